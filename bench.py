@@ -1,0 +1,461 @@
+"""Benchmark of the B200 spatial-query engine on the city workload.
+
+Workload (one GPU): 131,072 floorless box buildings (1,310,720 triangles) on a 363 x 362 lot
+grid, 1,000,000 rays from a plane 50 units above the tallest roof with cosine-weighted
+downward directions, 20,000 kNN (k=8) queries uniform in the scene bounds.  Seeded synthetic
+inputs generated by quarry.workloads (same bytes on every host).
+
+A step is one pass of the hot path over the resident inputs: trace the 1M rays (Morton
+order) through the tree.  `value` is rays per second over the timed steps (device time,
+CUDA events, L2 flushed between steps), `e2e` the same through the C ABI from pinned host
+buffers with the 32 MB ray upload and 8 MB result read-back inside the timed region.  The
+kNN pass and the build are timed beside it.  Every variant's results are compared bit for
+bit with each other, and the timed variant with quarry's own CPU reference on a sample.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload city|terrain] [--small]
+
+Multi-GPU: one process per GPU (torchrun); every rank builds its own replica of the scene
+and traces its own 1M rays (weak scaling, no data-path collective); time = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+sys.path.insert(0, str(ROOT / "quarry-gpu_b200"))
+
+METRIC = ("Mrays/s, Mqueries/s at bit-exact hash; batched vs per-scene loop; bwd/fwd ratio")
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="city", choices=["city", "terrain"])
+    ap.add_argument("--small", action="store_true", help="small inputs (profiling captures)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--only", default="", help="time only this variant (profiling)")
+    return ap.parse_args()
+
+
+def peaks() -> tuple[dict, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return json.loads(p.read_text()), "measured"
+    return PEAKS_FALLBACK, "fallback"
+
+
+def make_workload(name: str, small: bool, rank: int):
+    from quarry import workloads as w
+
+    seed = 1 + rank  # each rank traces its own rays over its own replica of the same scene
+    if name == "city":
+        b = 4096 if small else 131072
+        nr = 100_000 if small else 1_000_000
+        cfg = w.city_config(b, nr, 20_000, 1)
+        if rank:
+            lo, hi = w.bounds_of(cfg.tris)
+            cfg.rays = w.cosine_rays(nr, float(lo[0]), float(hi[0]), float(lo[1]), float(hi[1]),
+                                     cfg.top + 50.0, seed)
+        desc = {"workload": "city", "buildings": b, "triangles": int(cfg.tris.shape[0]),
+                "rays": nr, "knn_queries": 20_000, "k": 8}
+    else:
+        g = 64 if small else 256
+        nr = 100_000 if small else 1_000_000
+        cfg = w.terrain_config(g, nr, 20_000, seed)
+        desc = {"workload": "terrain", "grid": g, "triangles": int(cfg.tris.shape[0]),
+                "rays": nr, "closest_queries": 20_000}
+    return cfg, desc
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = Path(os.environ.get("TMPDIR", "/tmp")) / f"qk_clocks_{os.getpid()}.csv"
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+            # start timing only once the sampler is producing lines
+            deadline = time.time() + 10.0
+            while time.time() < deadline and self.path.stat().st_size == 0:
+                time.sleep(0.05)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self) -> dict:
+        if self.proc is None or not self.path.exists():
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        self.path.unlink(missing_ok=True)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def init_dist(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(world, value: float) -> float:
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------------------
+# CPU reference (quarry's own CPU code, compiled from its sources into oracle/_ref)
+# ---------------------------------------------------------------------------------------
+def cpu_reference_rays(tris, rays, threads: int):
+    import oracle
+
+    if oracle.REF_PATH.exists():
+        R = oracle.Reference()
+        out, ms, build_ms = R.raycast(tris, rays, threads)
+        return out, ms, build_ms, "reference"
+    # the oracle port when the reference could not be compiled on this machine
+    ref = oracle.LBVH("tri", tris)
+    t0 = time.perf_counter()
+    out = ref.raycast(rays, threads)
+    return out, (time.perf_counter() - t0) * 1e3, 0.0, "port"
+
+
+def reference_arm(args, world, rank):
+    """--impl reference: time quarry's CPU reference on the host cores (rank 0 only)."""
+    if rank != 0:
+        return
+    cfg, desc = make_workload(args.workload, args.small, 0)
+    threads = os.cpu_count() or 1
+    sample = min(len(cfg.rays), 200_000 if not args.small else 50_000)
+    rays = cfg.rays[:sample]
+    times = []
+    kind = "reference"
+    for i in range(args.warmup + args.steps):
+        _, ms, _, kind = cpu_reference_rays(cfg.tris, rays, threads)
+        if i >= args.warmup:
+            times.append(ms)
+    ms = float(np.mean(times))
+    value = sample / (ms * 1e-3) / 1e6
+    line = {"impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": "Mrays/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators)",
+            "config": desc,
+            "cpu_baseline": {"value": round(value, 3), "unit": "Mrays/s", "cores": threads,
+                             "kind": kind,
+                             "sample": f"first {sample} of the workload's rays per step, "
+                                       f"reference BVH built once per step (build excluded)"},
+            "e2e": {"value": round(value, 3), "unit": "Mrays/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------------------
+def main():
+    args = parse()
+    world, rank, local = init_dist(args)
+    if args.impl == "reference":
+        reference_arm(args, world, rank)
+        barrier(world)
+        return
+    import torch
+
+    import oracle
+    from quarry import capi
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    cfg, desc = make_workload(args.workload, args.small, rank)
+    nrays = cfg.rays.shape[0]
+
+    # ---- build (timed beside the step) ----
+    t_build = []
+    tree = None
+    for i in range(3):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        tree = capi.DeviceTree("tri", cfg.tris)
+        torch.cuda.synchronize()
+        t_build.append((time.perf_counter() - t0) * 1e3)
+    build_ms = float(min(t_build))
+    tree.build_wide()
+
+    rays_d = capi.to_device(cfg.rays, np.float32)
+    q_d = capi.to_device(cfg.queries, np.float32)
+    l2_flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+
+    variants = {"bin": 0, "bin_morton": capi.QK_ORDER_MORTON, "wide": capi.QK_WIDE,
+                "wide_morton": capi.QK_WIDE | capi.QK_ORDER_MORTON}
+    if args.only:
+        variants = {args.only: variants[args.only]}
+
+    # canonical per-ray visit counts on the binary LBVH (roofline algorithmic bytes)
+    stats = torch.zeros(4, dtype=torch.int64, device=dev)
+    base = tree.raycast(rays_d, capi.QK_ORDER_MORTON, stats=stats).clone()
+    s = stats.cpu().numpy()
+    node_tests, tri_tests, overflows = int(s[0]), int(s[1]), int(s[2])
+    if overflows:
+        raise RuntimeError(f"{overflows} rays overflowed the traversal stack")
+    p_int = (node_tests - tri_tests) / nrays
+    p_leaf = tri_tests / nrays
+    bytes_per_ray = 40.0 + 96.0 * p_int + (32.0 + 36.0) * p_leaf
+
+    # every variant must give the same bits
+    for name, flags in variants.items():
+        got = tree.raycast(rays_d, flags)
+        if not torch.equal(got, base):
+            raise RuntimeError(f"variant {name} differs from the binary Morton results")
+
+    def time_variant(flags, steps, warmup):
+        out = torch.empty(nrays, dtype=torch.int64, device=dev)
+        ws = torch.empty(capi.lib().qk_query_workspace_bytes(nrays, flags), dtype=torch.uint8,
+                         device=dev)
+        for _ in range(warmup):
+            tree.raycast(rays_d, flags, out=out, ws=ws)
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(steps)]
+        for e0, e1 in ev:
+            l2_flush.zero_()
+            e0.record()
+            tree.raycast(rays_d, flags, out=out, ws=ws)
+            e1.record()
+        torch.cuda.synchronize()
+        return [e0.elapsed_time(e1) for e0, e1 in ev]
+
+    results = {}
+    for name, flags in variants.items():
+        t = time_variant(flags, 10, 3)
+        results[name] = float(np.median(t))
+    best = min(results, key=results.get)
+    best_flags = variants[best]
+
+    # ---- the timed steps of the headline variant ----
+    barrier(world)
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        step_ms = time_variant(best_flags, args.steps, args.warmup)
+    clocks = clk.summary()
+    ms = float(np.sum(step_ms)) / args.steps
+    ms = max_over_ranks(world, ms)
+    value = world * nrays / (ms * 1e-3) / 1e6
+
+    # ---- roofline: traversal kernel alone on pre-sorted rays ----
+    # the engine's Morton order, recomputed on the host (quantize10 of src/gpu/morton.h), so
+    # the kernel alone can be timed on rays that are already in that order
+    trav_flags = best_flags & ~capi.QK_ORDER_MORTON
+    if best_flags & capi.QK_ORDER_MORTON:
+        o = cfg.rays[:, :3]
+        lo, hi = o.min(0), o.max(0)
+        qz = np.clip((o - lo) / np.where(hi > lo, hi - lo, 1), 0, 1)
+        qi = (qz * 1023 + 0.5).astype(np.uint32)
+
+        def spread(v):
+            v = v & 0x3FF
+            v = (v | (v << 16)) & 0x030000FF
+            v = (v | (v << 8)) & 0x0300F00F
+            v = (v | (v << 4)) & 0x030C30C3
+            v = (v | (v << 2)) & 0x09249249
+            return v
+
+        code = spread(qi[:, 0]) | (spread(qi[:, 1]) << 1) | (spread(qi[:, 2]) << 2)
+        order = np.argsort(code, kind="stable")
+        sorted_rays = capi.to_device(cfg.rays[order], np.float32)
+    else:
+        sorted_rays = rays_d
+    out = torch.empty(nrays, dtype=torch.int64, device=dev)
+    ws = torch.empty(capi.lib().qk_query_workspace_bytes(nrays, trav_flags), dtype=torch.uint8,
+                     device=dev)
+    for _ in range(3):
+        tree.raycast(sorted_rays, trav_flags, out=out, ws=ws)
+    kt = []
+    for _ in range(20):
+        l2_flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        tree.raycast(sorted_rays, trav_flags, out=out, ws=ws)
+        e1.record()
+        torch.cuda.synchronize()
+        kt.append(e0.elapsed_time(e1))
+    kernel_ms = float(np.median(kt))
+    pk, pk_kind = peaks()
+    achieved = bytes_per_ray * nrays / (kernel_ms * 1e-3) / 1e9
+    traffic = None
+    tfile = ROOT / "profiles" / f"traffic_{args.workload}.json"
+    if tfile.exists():
+        try:
+            traffic = json.loads(tfile.read_text()).get(best)
+        except Exception:
+            traffic = None
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": pk["hbm_gbs"],
+                "unit": "GB/s", "frac": round(achieved / pk["hbm_gbs"], 4),
+                "traffic": traffic, "peak_kind": pk_kind,
+                "kernel": "k_ray_wide" if trav_flags & capi.QK_WIDE else "k_ray_bin",
+                "kernel_ms": round(kernel_ms, 4),
+                "bytes_per_ray": round(bytes_per_ray, 1),
+                "canonical_counts": {"node_tests_per_ray": round(node_tests / nrays, 3),
+                                     "tri_tests_per_ray": round(p_leaf, 3)}}
+
+    # ---- kNN and build beside the step ----
+    k_out = torch.empty((q_d.shape[0], 8, 2), dtype=torch.int32, device=dev)
+    kflags = best_flags & (capi.QK_WIDE | capi.QK_ORDER_MORTON)
+    for _ in range(3):
+        tree.knn(q_d, 8, kflags, out=k_out)
+    kt = []
+    for _ in range(10):
+        l2_flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        tree.knn(q_d, 8, kflags, out=k_out)
+        e1.record()
+        torch.cuda.synchronize()
+        kt.append(e0.elapsed_time(e1))
+    knn_ms = float(np.median(kt))
+
+    # ---- e2e through the C ABI from pinned host buffers ----
+    host_rays = torch.from_numpy(np.ascontiguousarray(cfg.rays)).pin_memory()
+    host_out = torch.empty(nrays, dtype=torch.int64).pin_memory()
+    dev_rays = torch.empty((nrays, 8), dtype=torch.float32, device=dev)
+    e2e_ws = torch.empty(capi.lib().qk_query_workspace_bytes(nrays, best_flags),
+                         dtype=torch.uint8, device=dev)
+    for _ in range(3):
+        dev_rays.copy_(host_rays, non_blocking=True)
+        tree.raycast(dev_rays, best_flags, out=out, ws=e2e_ws)
+        host_out.copy_(out, non_blocking=True)
+    torch.cuda.synchronize()
+    e2e_t = []
+    for _ in range(min(args.steps, 50)):
+        l2_flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        dev_rays.copy_(host_rays, non_blocking=True)
+        tree.raycast(dev_rays, best_flags, out=out, ws=e2e_ws)
+        host_out.copy_(out, non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize()
+        e2e_t.append(e0.elapsed_time(e1))
+    e2e_ms = max_over_ranks(world, float(np.mean(e2e_t)))
+    e2e_value = world * nrays / (e2e_ms * 1e-3) / 1e6
+
+    result = host_out.numpy().view(np.uint64)
+    fp, hits = oracle.ray_hash(result)
+
+    line = None
+    if rank == 0:
+        cpu = None
+        parity = None
+        if not args.no_cpu_baseline:
+            threads = os.cpu_count() or 1
+            sample = min(nrays, 200_000 if not args.small else 50_000)
+            ref_out, ref_ms, ref_build, kind = cpu_reference_rays(cfg.tris, cfg.rays[:sample],
+                                                                  threads)
+            mism = int((ref_out != result[:sample]).sum())
+            parity = {"checked_rays": sample, "mismatches": mism, "against": kind}
+            if mism:
+                raise RuntimeError(f"{mism} of {sample} rays differ from the CPU reference")
+            cpu = {"value": round(sample / (ref_ms * 1e-3) / 1e6, 4), "unit": "Mrays/s",
+                   "cores": threads, "kind": kind,
+                   "sample": f"first {sample} of the {nrays} rays, reference BVH build "
+                             f"({ref_build:.0f} ms) excluded"}
+        line = {
+            "metric": METRIC, "value": round(value, 2), "unit": "Mrays/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded generators, identical bytes on every host)",
+            "config": {**desc, "builder": "lbvh", "variant": best,
+                       "l2": "flushed (256 MB write) between timed steps",
+                       "parallelism": f"replica x{world}, rays sharded per rank"},
+            "variants_ms": {k: round(v, 4) for k, v in results.items()},
+            "build_ms": round(build_ms, 3),
+            "knn": {"k": 8, "queries": int(q_d.shape[0]), "ms": round(knn_ms, 4),
+                    "mqueries_per_s": round(q_d.shape[0] / (knn_ms * 1e-3) / 1e6, 2)},
+            "fingerprint": f"0x{fp:016x}", "hits": int(hits), "parity": parity,
+            "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
+            "e2e": {"value": round(e2e_value, 2), "unit": "Mrays/s",
+                    "h2d_bytes_per_step": int(cfg.rays.nbytes),
+                    "d2h_bytes_per_step": int(nrays * 8)},
+            "gpu_launches": None,
+        }
+        # kernels of ours launched per timed step: keys + bounds + 4 sort passes x 5 + traversal
+        line["gpu_launches"] = args.steps * ((3 + 4 * 5 + 1) if best_flags & capi.QK_ORDER_MORTON else 1)
+        print(json.dumps(line), flush=True)
+    barrier(world)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

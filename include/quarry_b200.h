@@ -1,0 +1,187 @@
+/*
+ * quarry_b200.h -- C ABI of the B200 spatial-query engine.
+ *
+ * This is the boundary a foreign-function layer binds (ctypes, cffi, cgo, JNI).  Every entry
+ * point takes plain device pointers, element counts, a caller-provided device workspace and
+ * a CUDA stream passed as void* (NULL = legacy default stream), and returns a status code
+ * (QK_OK = 0).  Nothing here allocates device memory: callers size buffers with the *_bytes
+ * queries.  Launches are asynchronous on the given stream unless a comment says "syncs".
+ * No entry point keeps global state, so independent trees may be used from several host
+ * threads and streams at once.
+ *
+ * Data layouts follow quarry's API types (reference file:line):
+ *   triangle  9 floats  a.xyz b.xyz c.xyz                  src/core/geometry.h:91-101
+ *   point     3 floats                                     src/core/point_cloud.h:9-17
+ *   gaussian 10 floats  mean.xyz quat.xyzw scale.xyz       src/core/gaussian.h:12-20
+ *   ray       8 floats  origin.xyz dir.xyz tMin tMax       src/core/geometry.h:84-89
+ *   node     32 bytes   mn.xyz mx.xyz left right           src/gpu/gpu_node.h:9-14
+ *   wide    128 bytes   4 x {mn.xyz mx.xyz child pad}      src/gpu/gpu_node.h:46-57
+ *   ray result    uint64 (hit << 32) | bits(t)             src/gpu/gpu_bvh.h:91-97
+ *   query result  {uint32 dist2 bits, int32 id}, id -1 = none   src/gpu/gpu_bvh.h:250-253
+ *   radius CSR    int32 offsets[n+1], uint64 keys (bits(d2) << 32 | id), each segment
+ *                 ascending                                 src/gpu/gpu_bvh.h:296-301
+ */
+#ifndef QUARRY_B200_H
+#define QUARRY_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define QK_OK 0
+#define QK_ERR_INVALID 1     /* bad argument; see qk_last_error() */
+#define QK_ERR_CUDA 2        /* a CUDA call failed */
+#define QK_ERR_WORKSPACE 3   /* workspace smaller than the matching *_bytes query */
+#define QK_ERR_OVERFLOW 4    /* a traversal stack or a fixed table overflowed */
+#define QK_ERR_DEPTH 5       /* tree deeper than the traversal stacks support */
+
+/* ---- primitive kinds and builders ---- */
+#define QK_TRI 0
+#define QK_POINT 1
+#define QK_GAUSS 2
+#define QK_BUILD_LBVH 0
+#define QK_BUILD_SAH 1
+
+/* ---- query flags ---- */
+#define QK_ORDER_MORTON 1u       /* QueryOrder::Morton / RayOrder::Morton (origin keys) */
+#define QK_ORDER_DIRECTION 2u    /* RayOrder::MortonDirection (direction keys) */
+#define QK_WIDE 4u               /* traverse the 4-wide nodes */
+
+/*
+ * Device arrays of one tree.  The caller allocates every array (sizes from qk_tree_bytes)
+ * and qk_build / qk_refit fill them.  Mirrors GpuBVH (src/gpu/gpu_bvh.h:26-77):
+ *   nodes     2n-1 canonical 32-byte nodes (internal 0..n-2, leaf of slot s at n-1+s)
+ *   items     n primitives in leaf order (the API's d_tris)
+ *   prim_ids  n scene indices, prim_ids[slot]
+ *   parent    2n-1 parent links, -1 at the root
+ *   depth     2n-1 node depths (root 0)
+ *   bnodes    n-1 traversal nodes of 64 bytes (both child boxes inline)
+ *   leaves    n leaf payloads of 16*qk_leaf_vec4(kind) bytes
+ *   slot_of   n: inverse of prim_ids (scene index -> slot), written by the build
+ *   flags     n-1 ints of scratch for the bottom-up box pass
+ *   wide      4-wide nodes (capacity n-1), filled by qk_wide_build; wide_id n-1 ints
+ */
+typedef struct qk_tree {
+    int32_t kind;
+    int32_t n;
+    int32_t depth;       /* maximum node depth (set by qk_build) */
+    int32_t wide_count;  /* set by qk_wide_build, 0 when absent */
+    void* nodes;
+    void* items;
+    int32_t* prim_ids;
+    int32_t* parent;
+    int32_t* depth_arr;
+    void* bnodes;
+    void* leaves;
+    int32_t* slot_of;
+    int32_t* flags;
+    void* wide;
+    int32_t* wide_id;
+} qk_tree;
+
+/* Byte sizes of the arrays of a tree with n primitives (same order as qk_tree). */
+typedef struct qk_tree_sizes {
+    size_t nodes, items, prim_ids, parent, depth_arr, bnodes, leaves, slot_of, flags, wide,
+        wide_id;
+} qk_tree_sizes;
+
+/* ---- errors and device info ---- */
+const char* qk_status_string(int status);
+/* detail of the most recent failure on the calling host thread ("" if none) */
+const char* qk_last_error(void);
+/* gpuDescribe (src/gpu/gpu_bvh.h:100): writes "name sm_XY (N SM, G GiB)"; 0 when no device */
+int qk_describe(char* buf, int len);
+
+/* ---- sizes ---- */
+int qk_stride_floats(int kind);  /* 9, 3, 10 */
+int qk_leaf_vec4(int kind);      /* 3, 1, 3 */
+int qk_tree_bytes(int kind, int n, qk_tree_sizes* out);
+size_t qk_build_workspace_bytes(int kind, int n, int builder);
+size_t qk_query_workspace_bytes(int count, unsigned flags);
+size_t qk_radius_workspace_bytes(int count, unsigned flags);
+
+/*
+ * Build (buildBVHGPU / buildBVHSahGPU and the point / Gaussian variants,
+ * src/gpu/gpu_bvh.h:103-118).  items: n primitives in scene order (device).  Syncs on the
+ * stream to read the tree depth back into tree->depth.  sah_bins: SAH bin count (4..64),
+ * ignored by LBVH.  n >= 2.
+ */
+int qk_build(qk_tree* tree, int builder, int sah_bins, const void* items, void* workspace,
+             size_t workspace_bytes, void* stream);
+
+/* Full refit (refitBVHGPU without dirty list, src/gpu/gpu_bvh.h:141): items in scene order,
+ * same count; topology frozen; 4-wide nodes re-emitted when present. */
+int qk_refit(qk_tree* tree, const void* items, void* workspace, size_t workspace_bytes,
+             void* stream);
+
+/* Partial refit (refitBVHGPU with dirty list, src/gpu/gpu_bvh.h:145-146): dirty_ids are scene
+ * indices (device, count entries, each < n), dirty_items the new primitives for them (device,
+ * same order).  Only the ancestors of the dirty leaves are merged. */
+int qk_refit_dirty(qk_tree* tree, const int32_t* dirty_ids, const void* dirty_items, int count,
+                   void* workspace, size_t workspace_bytes, void* stream);
+
+/* 4-wide collapse (buildWideNodesGPU, src/gpu/gpu_bvh.h:229).  Syncs to read the count into
+ * tree->wide_count.  With tree->wide == NULL the call only computes wide_id and the count, so
+ * the caller can allocate wide_count * 128 bytes and call again to emit the nodes. */
+int qk_wide_build(qk_tree* tree, void* workspace, size_t workspace_bytes, void* stream);
+
+/*
+ * First-hit rays (raycastGPU, src/gpu/gpu_bvh.h:233-234).  rays: count rays (device);
+ * out: count uint64 results.  flags: QK_ORDER_* and QK_WIDE.  stats (nullable, device, 4
+ * uint64, accumulated): node tests, triangle tests, stack overflows, 0.
+ */
+int qk_raycast(const qk_tree* tree, const void* rays, int count, uint64_t* out, unsigned flags,
+               uint64_t* stats, void* workspace, size_t workspace_bytes, void* stream);
+
+/* Closest primitive per query point (closestPointGPU / closestVertexGPU /
+ * closestGaussianGPU, src/gpu/gpu_bvh.h:283-330).  points: count x 3 floats; out: count
+ * query results. */
+int qk_closest(const qk_tree* tree, const float* points, int count, void* out, unsigned flags,
+               uint64_t* stats, void* workspace, size_t workspace_bytes, void* stream);
+
+/* k nearest (kNearestGPU and variants, src/gpu/gpu_bvh.h:289-333): 1 <= k <= 32,
+ * stride >= k results per query, ascending by (dist2, id), missing slots id -1, dist2 0. */
+int qk_knn(const qk_tree* tree, const float* points, int count, int k, int stride, void* out,
+           unsigned flags, uint64_t* stats, void* workspace, size_t workspace_bytes,
+           void* stream);
+
+/*
+ * Radius query as CSR (radiusQueryGPU and variants, src/gpu/gpu_bvh.h:307-336), in two
+ * calls.  qk_radius_count writes counts and offsets[count+1] (offsets[count] = total) and
+ * copies the total to *total_host (syncs).  The caller then allocates keys[total] and calls
+ * qk_radius_fill with the same points, radius and flags, which writes every segment sorted
+ * by (dist2, id).  radius >= 0.
+ */
+int qk_radius_count(const qk_tree* tree, const float* points, int count, float radius,
+                    int32_t* offsets, int64_t* total_host, unsigned flags, uint64_t* stats,
+                    void* workspace, size_t workspace_bytes, void* stream);
+int qk_radius_fill(const qk_tree* tree, const float* points, int count, float radius,
+                   const int32_t* offsets, uint64_t* keys, unsigned flags, void* workspace,
+                   size_t workspace_bytes, void* stream);
+
+/*
+ * Structural check (validateBVHGPU and variants, src/gpu/gpu_bvh.h:347-349).  items: the
+ * scene-order primitives the tree should hold (device).  errors: 8 device ints, zeroed by
+ * the call, then [0] bad children or box, [1] bad leaf box, [2] bad reference count, [3] bad
+ * leaf id, [4] bad primitive map, [5] bad depth, [6] 4-wide node mismatch.
+ */
+int qk_validate(const qk_tree* tree, const void* items, int32_t* errors, void* workspace,
+                size_t workspace_bytes, void* stream);
+size_t qk_validate_workspace_bytes(int n);
+
+/* Stable LSD radix sort of 32-bit keys with 32-bit values over the low `bits` bits.  All
+ * four buffers hold n entries; the sorted result ends in keys_out / vals_out. */
+size_t qk_sort_workspace_bytes(int n);
+int qk_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
+                  uint32_t* vals_out, int n, int bits, void* workspace, size_t workspace_bytes,
+                  void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

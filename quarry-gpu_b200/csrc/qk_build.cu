@@ -1,0 +1,751 @@
+// qk_build.cu -- LBVH build, topology-frozen refit, 4-wide collapse and structural checks.
+//
+// LBVH (Karras 2012, as quarry's src/gpu/lbvh.cu:213-514 and 1954-2041 define it):
+//   1. centroid bounds: grid-stride min/max, warp shuffles, one ordered-uint atomic per block
+//   2. 30-bit Morton code of the quantized centroid, value = scene index
+//   3. stable radix sort on the code (equal codes keep index order = the reference's
+//      64-bit (code << 32 | index) key order)
+//   4. emit: one thread per slot writes the leaf (payload, canonical leaf node, prim id,
+//      inverse map) and, for slot < n-1, the internal node found by the Karras split
+//      search over the 64-bit keys
+//   5. bottom-up boxes in ONE launch: each leaf thread climbs its parent chain; an atomic
+//      visit counter per internal node lets the second arriving child compute the union
+//      (both children final) and carry on, the first one stops.  min/max is exact, so the
+//      boxes equal the reference's level-by-level refit bit for bit.  The same pass writes
+//      the 64-byte traversal node (both child boxes inline).
+//   6. depth of every node by walking its parent chain; the maximum is read back once.
+#include <cstdio>
+
+#include "qk_internal.cuh"
+
+namespace qk {
+
+namespace {
+
+__device__ __forceinline__ uint32_t spread10(uint32_t v) {
+    v &= 0x3ffu;
+    v = (v | (v << 16)) & 0x030000ffu;
+    v = (v | (v << 8)) & 0x0300f00fu;
+    v = (v | (v << 4)) & 0x030c30c3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+
+// quantize (lbvh.cu:285-290): (v - lo) / extent * 1023 + 0.5, clamped, truncated
+__device__ __forceinline__ uint32_t quant(float v, float lo, float extent) {
+    if (extent <= 0.0f) return 0;
+    const float q = (v - lo) / extent * 1023.0f + 0.5f;
+    return static_cast<uint32_t>(static_cast<int>(fminf(1023.0f, fmaxf(0.0f, q))));
+}
+
+__global__ void k_header_init(Header* h) {
+    if (threadIdx.x < 3) {
+        h->lo[threadIdx.x] = ord_f(kInf);
+        h->hi[threadIdx.x] = ord_f(-kInf);
+    }
+    if (threadIdx.x == 0) {
+        h->max_depth = 0;
+        h->counter = 0;
+        h->overflow = 0;
+        h->error = 0;
+        h->list_count[0] = 0;
+        h->list_count[1] = 0;
+    }
+}
+
+__device__ __forceinline__ float warp_min(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ __forceinline__ float warp_max(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+template <class Ops>
+__global__ __launch_bounds__(kBlock) void k_centroid_bounds(const float* __restrict__ items,
+                                                            int n, Header* __restrict__ h) {
+    float lo0 = kInf, lo1 = kInf, lo2 = kInf, hi0 = -kInf, hi1 = -kInf, hi2 = -kInf;
+    for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += kBlock * gridDim.x) {
+        const float3 c = Ops::centroid(items + static_cast<size_t>(i) * Ops::kFloats);
+        lo0 = fminf(lo0, c.x);
+        lo1 = fminf(lo1, c.y);
+        lo2 = fminf(lo2, c.z);
+        hi0 = fmaxf(hi0, c.x);
+        hi1 = fmaxf(hi1, c.y);
+        hi2 = fmaxf(hi2, c.z);
+    }
+    __shared__ float s[6][kBlock / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    lo0 = warp_min(lo0);
+    lo1 = warp_min(lo1);
+    lo2 = warp_min(lo2);
+    hi0 = warp_max(hi0);
+    hi1 = warp_max(hi1);
+    hi2 = warp_max(hi2);
+    if (lane == 0) {
+        s[0][warp] = lo0;
+        s[1][warp] = lo1;
+        s[2][warp] = lo2;
+        s[3][warp] = hi0;
+        s[4][warp] = hi1;
+        s[5][warp] = hi2;
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        float v = kInf;
+        for (int w = 0; w < kBlock / 32; ++w) v = fminf(v, s[threadIdx.x][w]);
+        atomicMin(&h->lo[threadIdx.x], ord_f(v));
+    } else if (threadIdx.x < 6) {
+        float v = -kInf;
+        for (int w = 0; w < kBlock / 32; ++w) v = fmaxf(v, s[threadIdx.x][w]);
+        atomicMax(&h->hi[threadIdx.x - 3], ord_f(v));
+    }
+}
+
+template <class Ops>
+__global__ __launch_bounds__(kBlock) void k_morton(const float* __restrict__ items, int n,
+                                                   const Header* __restrict__ h,
+                                                   uint32_t* __restrict__ codes,
+                                                   uint32_t* __restrict__ idx) {
+    const int i = blockIdx.x * kBlock + threadIdx.x;
+    if (i >= n) return;
+    const float lx = unord_f(h->lo[0]), ly = unord_f(h->lo[1]), lz = unord_f(h->lo[2]);
+    const float hx = unord_f(h->hi[0]), hy = unord_f(h->hi[1]), hz = unord_f(h->hi[2]);
+    const float3 c = Ops::centroid(items + static_cast<size_t>(i) * Ops::kFloats);
+    codes[i] = spread10(quant(c.x, lx, hx - lx)) | (spread10(quant(c.y, ly, hy - ly)) << 1) |
+               (spread10(quant(c.z, lz, hz - lz)) << 2);
+    idx[i] = static_cast<uint32_t>(i);
+}
+
+// 64-bit key of slot j: (code << 32) | scene index
+__device__ __forceinline__ uint64_t key64(const uint32_t* codes, const uint32_t* ids, int j) {
+    return (static_cast<uint64_t>(codes[j]) << 32) | ids[j];
+}
+
+// common-prefix length of keys a and b; -1 outside [0, n)
+__device__ __forceinline__ int cpl(const uint32_t* codes, const uint32_t* ids, int n, uint64_t ka,
+                                   int b) {
+    if (b < 0 || b >= n) return -1;
+    const uint64_t x = ka ^ key64(codes, ids, b);
+    return x == 0 ? 64 : __clzll(x);
+}
+
+__device__ __forceinline__ void write_box(Node* nd, Box b) {
+    float4* p = reinterpret_cast<float4*>(nd);
+    const float4 a = p[1];
+    p[0] = make_float4(b.lo.x, b.lo.y, b.lo.z, b.hi.x);
+    p[1] = make_float4(b.hi.y, b.hi.z, a.z, a.w);
+}
+
+template <class Ops>
+__global__ __launch_bounds__(kBlock) void k_emit(
+    const float* __restrict__ items, int n, const uint32_t* __restrict__ codes,
+    const uint32_t* __restrict__ ids, Node* __restrict__ nodes, float* __restrict__ sorted,
+    int* __restrict__ prim_ids, int* __restrict__ slot_of, int* __restrict__ parent,
+    BNode* __restrict__ bnodes, float4* __restrict__ leaves, int* __restrict__ flags) {
+    const int k = blockIdx.x * kBlock + threadIdx.x;
+    if (k >= n) return;
+    // leaf k
+    const int src = static_cast<int>(ids[k]);
+    float it[Ops::kFloats];
+#pragma unroll
+    for (int j = 0; j < Ops::kFloats; ++j) it[j] = items[static_cast<size_t>(src) * Ops::kFloats + j];
+#pragma unroll
+    for (int j = 0; j < Ops::kFloats; ++j) sorted[static_cast<size_t>(k) * Ops::kFloats + j] = it[j];
+    prim_ids[k] = src;
+    slot_of[src] = k;
+    const Box b = Ops::bounds(it);
+    float4* leafnode = reinterpret_cast<float4*>(nodes + (n - 1 + k));
+    leafnode[0] = make_float4(b.lo.x, b.lo.y, b.lo.z, b.hi.x);
+    leafnode[1] = make_float4(b.hi.y, b.hi.z, __int_as_float(-(k + 1)), __int_as_float(1));
+    float4 pay[Ops::kVec4];
+    Ops::pack(it, src, pay);
+#pragma unroll
+    for (int j = 0; j < Ops::kVec4; ++j) leaves[static_cast<size_t>(k) * Ops::kVec4 + j] = pay[j];
+    if (k == 0) parent[0] = -1;
+    if (k >= n - 1) return;
+
+    // internal node k (Karras 2012): direction, range end by exponential + binary search,
+    // then the split as the last index whose prefix with the first exceeds the node's
+    const uint64_t kk = key64(codes, ids, k);
+    const int dir = cpl(codes, ids, n, kk, k + 1) > cpl(codes, ids, n, kk, k - 1) ? 1 : -1;
+    const int dmin = cpl(codes, ids, n, kk, k - dir);
+    int lmax = 2;
+    while (cpl(codes, ids, n, kk, k + lmax * dir) > dmin) lmax *= 2;
+    int l = 0;
+    for (int t = lmax / 2; t > 0; t /= 2) {
+        if (cpl(codes, ids, n, kk, k + (l + t) * dir) > dmin) l += t;
+    }
+    const int j = k + l * dir;
+    const int first = min(k, j), last = max(k, j);
+    const int dnode = cpl(codes, ids, n, kk, j);
+    const uint64_t kf = key64(codes, ids, first);
+    int split = first;
+    int step = last - first;
+    do {
+        step = (step + 1) >> 1;
+        const int cand = split + step;
+        if (cand < last && cpl(codes, ids, n, kf, cand) > dnode) split = cand;
+    } while (step > 1);
+    const int left = split == first ? (n - 1 + split) : split;
+    const int right = split + 1 == last ? (n - 1 + split + 1) : split + 1;
+    nodes[k].left = left;
+    nodes[k].right = right;
+    parent[left] = k;
+    parent[right] = k;
+    const int lref = left >= n - 1 ? ~(left - (n - 1)) : left;
+    const int rref = right >= n - 1 ? ~(right - (n - 1)) : right;
+    bnodes[k].v3 = make_float4(__int_as_float(lref), __int_as_float(rref), 0.0f, 0.0f);
+    flags[k] = 0;
+}
+
+__device__ __forceinline__ Box load_box_cg(const Node* nd) {
+    const float4* p = reinterpret_cast<const float4*>(nd);
+    const float4 a = __ldcg(p), b = __ldcg(p + 1);
+    Box bx;
+    bx.lo = f3(a.x, a.y, a.z);
+    bx.hi = f3(a.w, b.x, b.y);
+    return bx;
+}
+
+// Complete internal node p from its two (final) children: canonical box + traversal node.
+__device__ __forceinline__ void finish_node(Node* __restrict__ nodes, BNode* __restrict__ bnodes,
+                                            int p) {
+    const int l = nodes[p].left, r = nodes[p].right;
+    const Box a = load_box_cg(nodes + l);
+    const Box b = load_box_cg(nodes + r);
+    Box u;
+    u.lo = f3(fmin_t(a.lo.x, b.lo.x), fmin_t(a.lo.y, b.lo.y), fmin_t(a.lo.z, b.lo.z));
+    u.hi = f3(fmax_t(a.hi.x, b.hi.x), fmax_t(a.hi.y, b.hi.y), fmax_t(a.hi.z, b.hi.z));
+    write_box(nodes + p, u);
+    BNode& bn = bnodes[p];
+    bn.v0 = make_float4(a.lo.x, a.lo.y, a.lo.z, a.hi.x);
+    bn.v1 = make_float4(a.hi.y, a.hi.z, b.lo.x, b.lo.y);
+    bn.v2 = make_float4(b.lo.z, b.hi.x, b.hi.y, b.hi.z);
+}
+
+// One thread per leaf climbs toward the root; flags[p] counts arrivals at internal node p.
+// The second arrival finishes p (both children final), resets the counter and continues.
+__global__ __launch_bounds__(kBlock) void k_bottom_up(Node* __restrict__ nodes,
+                                                     BNode* __restrict__ bnodes,
+                                                     const int* __restrict__ parent,
+                                                     int* __restrict__ flags, int n) {
+    const int k = blockIdx.x * kBlock + threadIdx.x;
+    if (k >= n) return;
+    int p = parent[n - 1 + k];
+    int guard = 0;
+    while (p >= 0 && guard++ < 4096) {
+        __threadfence();
+        if (atomicAdd(&flags[p], 1) == 0) return;
+        __threadfence();
+        finish_node(nodes, bnodes, p);
+        flags[p] = 0;
+        p = parent[p];
+    }
+}
+
+// depth = length of the parent chain (lbvh.cu:419-431); bounded by the node count
+__global__ __launch_bounds__(kBlock) void k_depth(const int* __restrict__ parent, int count,
+                                                 int* __restrict__ depth, Header* __restrict__ h) {
+    const int i = blockIdx.x * kBlock + threadIdx.x;
+    int d = 0;
+    if (i < count) {
+        int p = i;
+        while (p > 0 && d < count) {
+            p = parent[p];
+            ++d;
+        }
+        depth[i] = d;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) d = max(d, __shfl_xor_sync(0xffffffffu, d, o));
+    if ((threadIdx.x & 31) == 0 && d > 0) atomicMax(&h->max_depth, d);
+}
+
+// ---- refit ----
+template <class Ops>
+__global__ __launch_bounds__(kBlock) void k_refit_leaves(const float* __restrict__ items, int n,
+                                                         const int* __restrict__ prim_ids,
+                                                         Node* __restrict__ nodes,
+                                                         float* __restrict__ sorted,
+                                                         float4* __restrict__ leaves) {
+    const int k = blockIdx.x * kBlock + threadIdx.x;
+    if (k >= n) return;
+    const int src = prim_ids[k];
+    float it[Ops::kFloats];
+#pragma unroll
+    for (int j = 0; j < Ops::kFloats; ++j) it[j] = items[static_cast<size_t>(src) * Ops::kFloats + j];
+#pragma unroll
+    for (int j = 0; j < Ops::kFloats; ++j) sorted[static_cast<size_t>(k) * Ops::kFloats + j] = it[j];
+    write_box(nodes + (n - 1 + k), Ops::bounds(it));
+    float4 pay[Ops::kVec4];
+    Ops::pack(it, src, pay);
+#pragma unroll
+    for (int j = 0; j < Ops::kVec4; ++j) leaves[static_cast<size_t>(k) * Ops::kVec4 + j] = pay[j];
+}
+
+// Dirty refit, pass 1: write the moved leaves and mark ancestors.  flags[p] bit 0 / bit 1
+// record a dirty left / right child; a thread stops climbing at the first node another
+// thread already marked.  A repeated id (same leaf twice) is dropped via skip[].
+template <class Ops>
+__global__ __launch_bounds__(kBlock) void k_dirty_mark(
+    const int* __restrict__ ids, const float* __restrict__ items, int count, int n,
+    const int* __restrict__ slot_of, const int* __restrict__ parent, Node* __restrict__ nodes,
+    float* __restrict__ sorted, float4* __restrict__ leaves, int* __restrict__ flags,
+    int* __restrict__ skip, Header* __restrict__ h) {
+    const int i = blockIdx.x * kBlock + threadIdx.x;
+    if (i >= count) return;
+    const int id = ids[i];
+    if (id < 0 || id >= n) {
+        skip[i] = 1;
+        atomicAdd(&h->error, 1);
+        return;
+    }
+    const int slot = slot_of[id];
+    int node = n - 1 + slot;
+    int p = parent[node];
+    // claim the leaf: the first thread to set the child bit of its parent owns it
+    const int bit0 = nodes[p].left == node ? 1 : 2;
+    const int old0 = atomicOr(&flags[p], bit0);
+    if (old0 & bit0) {
+        skip[i] = 1;
+        return;
+    }
+    skip[i] = 0;
+    float it[Ops::kFloats];
+#pragma unroll
+    for (int j = 0; j < Ops::kFloats; ++j) it[j] = items[static_cast<size_t>(i) * Ops::kFloats + j];
+#pragma unroll
+    for (int j = 0; j < Ops::kFloats; ++j) sorted[static_cast<size_t>(slot) * Ops::kFloats + j] = it[j];
+    write_box(nodes + node, Ops::bounds(it));
+    float4 pay[Ops::kVec4];
+    Ops::pack(it, id, pay);
+#pragma unroll
+    for (int j = 0; j < Ops::kVec4; ++j) leaves[static_cast<size_t>(slot) * Ops::kVec4 + j] = pay[j];
+    if (old0 != 0) return;  // parent already marked by the sibling
+    int guard = 0;
+    while (guard++ < 4096) {
+        node = p;
+        p = parent[node];
+        if (p < 0) return;
+        const int bit = nodes[p].left == node ? 1 : 2;
+        if (atomicOr(&flags[p], bit) != 0) return;
+    }
+}
+
+// Dirty refit, pass 2: climb again; arrivals are counted in flags[p] >> 2 and the last of
+// the popcount(flags[p] & 3) dirty children finishes p, clears the word and continues.
+__global__ __launch_bounds__(kBlock) void k_dirty_merge(const int* __restrict__ ids, int count,
+                                                       int n, const int* __restrict__ slot_of,
+                                                       const int* __restrict__ parent,
+                                                       Node* __restrict__ nodes,
+                                                       BNode* __restrict__ bnodes,
+                                                       int* __restrict__ flags,
+                                                       const int* __restrict__ skip) {
+    const int i = blockIdx.x * kBlock + threadIdx.x;
+    if (i >= count || skip[i]) return;
+    int p = parent[n - 1 + slot_of[ids[i]]];
+    int guard = 0;
+    while (p >= 0 && guard++ < 4096) {
+        __threadfence();
+        const int old = atomicAdd(&flags[p], 4);
+        const int need = __popc(old & 3);
+        if ((old >> 2) + 1 < need) return;
+        __threadfence();
+        finish_node(nodes, bnodes, p);
+        flags[p] = 0;
+        p = parent[p];
+    }
+}
+
+// ---- 4-wide collapse (lbvh.cu:731-825): even-depth internal nodes ----
+__global__ __launch_bounds__(kBlock) void k_wide_flags(const int* __restrict__ depth, int m,
+                                                      int* __restrict__ flags) {
+    const int i = blockIdx.x * kBlock + threadIdx.x;
+    if (i < m) flags[i] = (depth[i] & 1) == 0 ? 1 : 0;
+}
+
+__device__ __forceinline__ void wide_fill(WideEntry& e, const Node& src, int child) {
+    e.mn[0] = src.mn[0];
+    e.mn[1] = src.mn[1];
+    e.mn[2] = src.mn[2];
+    e.mx[0] = src.mx[0];
+    e.mx[1] = src.mx[1];
+    e.mx[2] = src.mx[2];
+    e.child = child;
+    e.pad = 0;
+}
+
+__device__ void wide_node_of(const Node* __restrict__ nodes, int n, const int* __restrict__ wide_id,
+                             int i, WideNode& out) {
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+        out.c[s].mn[0] = out.c[s].mn[1] = out.c[s].mn[2] = kInf;
+        out.c[s].mx[0] = out.c[s].mx[1] = out.c[s].mx[2] = -kInf;
+        out.c[s].child = kEmptySlot;
+        out.c[s].pad = 0;
+    }
+    const int kids[2] = {nodes[i].left, nodes[i].right};
+    int slot = 0;
+    for (int k = 0; k < 2; ++k) {
+        const int c = kids[k];
+        if (c >= n - 1) {
+            wide_fill(out.c[slot++], nodes[c], nodes[c].left);
+            continue;
+        }
+        const int g[2] = {nodes[c].left, nodes[c].right};
+        for (int j = 0; j < 2; ++j) {
+            const int gc = g[j];
+            wide_fill(out.c[slot++], nodes[gc], gc >= n - 1 ? nodes[gc].left : wide_id[gc]);
+        }
+    }
+}
+
+__global__ __launch_bounds__(kBlock) void k_wide_emit(const Node* __restrict__ nodes, int n,
+                                                     const int* __restrict__ depth,
+                                                     const int* __restrict__ wide_id,
+                                                     WideNode* __restrict__ wide) {
+    const int i = blockIdx.x * kBlock + threadIdx.x;
+    if (i >= n - 1 || (depth[i] & 1) != 0) return;
+    WideNode out;
+    wide_node_of(nodes, n, wide_id, i, out);
+    wide[wide_id[i]] = out;
+}
+
+// ---- validation (lbvh.cu:613-729) ----
+__device__ __forceinline__ bool same_box(const Node& a, Box b) {
+    return a.mn[0] == b.lo.x && a.mn[1] == b.lo.y && a.mn[2] == b.lo.z && a.mx[0] == b.hi.x &&
+           a.mx[1] == b.hi.y && a.mx[2] == b.hi.z;
+}
+
+template <class Ops>
+__global__ __launch_bounds__(kBlock) void k_check_nodes(
+    const Node* __restrict__ nodes, const BNode* __restrict__ bnodes,
+    const float* __restrict__ sorted, int n, int* __restrict__ visited, int* __restrict__ err) {
+    const int i = blockIdx.x * kBlock + threadIdx.x;
+    const int count = 2 * n - 1;
+    if (i >= count) return;
+    const Node nd = nodes[i];
+    if (i < n - 1) {
+        if (nd.left < 0 || nd.left >= count || nd.right < 0 || nd.right >= count) {
+            atomicAdd(&err[0], 1);
+            return;
+        }
+        atomicAdd(&visited[nd.left], 1);
+        atomicAdd(&visited[nd.right], 1);
+        const Node l = nodes[nd.left], r = nodes[nd.right];
+        Box u;
+        u.lo = f3(fmin_t(l.mn[0], r.mn[0]), fmin_t(l.mn[1], r.mn[1]), fmin_t(l.mn[2], r.mn[2]));
+        u.hi = f3(fmax_t(l.mx[0], r.mx[0]), fmax_t(l.mx[1], r.mx[1]), fmax_t(l.mx[2], r.mx[2]));
+        if (!same_box(nd, u)) atomicAdd(&err[0], 1);
+        // the traversal node must mirror the canonical children
+        const BNode b = bnodes[i];
+        const int lref = nd.left >= n - 1 ? ~(nd.left - (n - 1)) : nd.left;
+        const int rref = nd.right >= n - 1 ? ~(nd.right - (n - 1)) : nd.right;
+        const bool ok = b.v0.x == l.mn[0] && b.v0.y == l.mn[1] && b.v0.z == l.mn[2] &&
+                        b.v0.w == l.mx[0] && b.v1.x == l.mx[1] && b.v1.y == l.mx[2] &&
+                        b.v1.z == r.mn[0] && b.v1.w == r.mn[1] && b.v2.x == r.mn[2] &&
+                        b.v2.y == r.mx[0] && b.v2.z == r.mx[1] && b.v2.w == r.mx[2] &&
+                        __float_as_int(b.v3.x) == lref && __float_as_int(b.v3.y) == rref;
+        if (!ok) atomicAdd(&err[0], 1);
+    } else {
+        const int slot = -nd.left - 1;
+        if (slot < 0 || slot >= n) {
+            atomicAdd(&err[0], 1);
+            return;
+        }
+        if (i != n - 1 + slot || nd.right != 1) atomicAdd(&err[3], 1);
+        if (!same_box(nd, Ops::bounds(sorted + static_cast<size_t>(slot) * Ops::kFloats)))
+            atomicAdd(&err[1], 1);
+    }
+}
+
+__global__ __launch_bounds__(kBlock) void k_check_refs(const int* __restrict__ visited, int count,
+                                                      int* __restrict__ err) {
+    const int i = blockIdx.x * kBlock + threadIdx.x;
+    if (i < count && visited[i] != (i == 0 ? 0 : 1)) atomicAdd(&err[2], 1);
+}
+
+template <class Ops>
+__global__ __launch_bounds__(kBlock) void k_check_perm(const int* __restrict__ prim_ids,
+                                                      const int* __restrict__ slot_of,
+                                                      const float* __restrict__ sorted,
+                                                      const float4* __restrict__ leaves,
+                                                      const float* __restrict__ items, int n,
+                                                      int* __restrict__ hist,
+                                                      int* __restrict__ err) {
+    const int s = blockIdx.x * kBlock + threadIdx.x;
+    if (s >= n) return;
+    const int id = prim_ids[s];
+    if (id < 0 || id >= n) {
+        atomicAdd(&err[4], 1);
+        return;
+    }
+    atomicAdd(&hist[id], 1);
+    int bad = slot_of[id] != s;
+    float it[Ops::kFloats];
+    for (int j = 0; j < Ops::kFloats; ++j) {
+        it[j] = sorted[static_cast<size_t>(s) * Ops::kFloats + j];
+        bad |= __float_as_uint(it[j]) != __float_as_uint(items[static_cast<size_t>(id) * Ops::kFloats + j]);
+    }
+    float4 pay[Ops::kVec4];
+    Ops::pack(it, id, pay);
+    for (int j = 0; j < Ops::kVec4; ++j) {
+        const float4 v = leaves[static_cast<size_t>(s) * Ops::kVec4 + j];
+        bad |= __float_as_uint(v.x) != __float_as_uint(pay[j].x) ||
+               __float_as_uint(v.y) != __float_as_uint(pay[j].y) ||
+               __float_as_uint(v.z) != __float_as_uint(pay[j].z) ||
+               __float_as_uint(v.w) != __float_as_uint(pay[j].w);
+    }
+    if (bad) atomicAdd(&err[4], 1);
+}
+
+__global__ __launch_bounds__(kBlock) void k_check_hist(const int* __restrict__ hist, int n,
+                                                      int* __restrict__ err) {
+    const int i = blockIdx.x * kBlock + threadIdx.x;
+    if (i < n && hist[i] != 1) atomicAdd(&err[4], 1);
+}
+
+__global__ __launch_bounds__(kBlock) void k_check_depth(const Node* __restrict__ nodes,
+                                                       const int* __restrict__ depth, int n,
+                                                       int* __restrict__ err) {
+    const int i = blockIdx.x * kBlock + threadIdx.x;
+    const int count = 2 * n - 1;
+    if (i >= count) return;
+    if (i == 0 && depth[0] != 0) atomicAdd(&err[5], 1);
+    if (i < n - 1) {
+        const int l = nodes[i].left, r = nodes[i].right;
+        if (l >= 0 && l < count && depth[l] != depth[i] + 1) atomicAdd(&err[5], 1);
+        if (r >= 0 && r < count && depth[r] != depth[i] + 1) atomicAdd(&err[5], 1);
+    }
+    if (depth[i] >= kStack) atomicAdd(&err[5], 1);
+}
+
+__global__ __launch_bounds__(kBlock) void k_check_wide(const Node* __restrict__ nodes, int n,
+                                                      const int* __restrict__ depth,
+                                                      const int* __restrict__ wide_id,
+                                                      const WideNode* __restrict__ wide,
+                                                      int* __restrict__ err) {
+    const int i = blockIdx.x * kBlock + threadIdx.x;
+    if (i >= n - 1 || (depth[i] & 1) != 0) return;
+    WideNode want;
+    wide_node_of(nodes, n, wide_id, i, want);
+    const WideNode got = wide[wide_id[i]];
+    const unsigned* a = reinterpret_cast<const unsigned*>(&want);
+    const unsigned* b = reinterpret_cast<const unsigned*>(&got);
+    int bad = 0;
+    for (int j = 0; j < 32; ++j) bad |= a[j] != b[j];
+    if (bad) atomicAdd(&err[6], 1);
+}
+
+template <class Ops>
+int build_lbvh(qk_tree* t, const void* items_v, void* ws, cudaStream_t s) {
+    const int n = t->n;
+    const float* items = static_cast<const float*>(items_v);
+    Carve c{static_cast<char*>(ws)};
+    Header* h = c.take<Header>(1);
+    uint32_t* codes = c.take<uint32_t>(n);
+    uint32_t* idx = c.take<uint32_t>(n);
+    uint32_t* codes_s = c.take<uint32_t>(n);
+    uint32_t* idx_s = c.take<uint32_t>(n);
+    void* sort_ws = c.take<char>(sort_ws_bytes(n));
+    Node* nodes = static_cast<Node*>(t->nodes);
+    BNode* bn = static_cast<BNode*>(t->bnodes);
+
+    k_header_init<<<1, 32, 0, s>>>(h);
+    const int grid = min(blocks_for(n), 148 * 8);
+    k_centroid_bounds<Ops><<<grid, kBlock, 0, s>>>(items, n, h);
+    k_morton<Ops><<<blocks_for(n), kBlock, 0, s>>>(items, n, h, codes, idx);
+    cudaError_t e = sort_pairs(codes, idx, codes_s, idx_s, n, 30, sort_ws, s);
+    if (e != cudaSuccess) return cuda_status(e, "build sort");
+    k_emit<Ops><<<blocks_for(n), kBlock, 0, s>>>(items, n, codes_s, idx_s, nodes,
+                                                  static_cast<float*>(t->items), t->prim_ids,
+                                                  t->slot_of, t->parent, bn,
+                                                  static_cast<float4*>(t->leaves), t->flags);
+    k_bottom_up<<<blocks_for(n), kBlock, 0, s>>>(nodes, bn, t->parent, t->flags, n);
+    k_depth<<<blocks_for(2 * n - 1), kBlock, 0, s>>>(t->parent, 2 * n - 1, t->depth_arr, h);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_status(e, "build kernels");
+    int depth = 0;
+    e = cudaMemcpyAsync(&depth, &h->max_depth, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_status(e, "build depth readback");
+    t->depth = depth;
+    t->wide_count = 0;
+    if (depth >= kStack) return fail(QK_ERR_DEPTH, "tree depth %d exceeds %d", depth, kStack - 1);
+    return QK_OK;
+}
+
+template <class Ops>
+int refit_impl(qk_tree* t, const void* items, cudaStream_t s) {
+    const int n = t->n;
+    k_refit_leaves<Ops><<<blocks_for(n), kBlock, 0, s>>>(
+        static_cast<const float*>(items), n, t->prim_ids, static_cast<Node*>(t->nodes),
+        static_cast<float*>(t->items), static_cast<float4*>(t->leaves));
+    k_bottom_up<<<blocks_for(n), kBlock, 0, s>>>(static_cast<Node*>(t->nodes),
+                                                 static_cast<BNode*>(t->bnodes), t->parent,
+                                                 t->flags, n);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_status(e, "refit");
+    if (t->wide_count > 0 && t->wide) return wide_emit_all(t, s);
+    return QK_OK;
+}
+
+template <class Ops>
+int refit_dirty_impl(qk_tree* t, const int* ids, const void* items, int count, void* ws,
+                     cudaStream_t s) {
+    const int n = t->n;
+    if (count <= 0) return QK_OK;
+    Carve c{static_cast<char*>(ws)};
+    Header* h = c.take<Header>(1);
+    int* skip = c.take<int>(count);
+    k_header_init<<<1, 32, 0, s>>>(h);
+    k_dirty_mark<Ops><<<blocks_for(count), kBlock, 0, s>>>(
+        ids, static_cast<const float*>(items), count, n, t->slot_of, t->parent,
+        static_cast<Node*>(t->nodes), static_cast<float*>(t->items),
+        static_cast<float4*>(t->leaves), t->flags, skip, h);
+    k_dirty_merge<<<blocks_for(count), kBlock, 0, s>>>(ids, count, n, t->slot_of, t->parent,
+                                                       static_cast<Node*>(t->nodes),
+                                                       static_cast<BNode*>(t->bnodes), t->flags,
+                                                       skip);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_status(e, "refit dirty");
+    if (t->wide_count > 0 && t->wide) return wide_emit_all(t, s);
+    return QK_OK;
+}
+
+template <class Ops>
+int validate_impl(const qk_tree* t, const void* items, int* err, void* ws, cudaStream_t s) {
+    const int n = t->n, count = 2 * n - 1;
+    Carve c{static_cast<char*>(ws)};
+    int* visited = c.take<int>(count);
+    int* hist = c.take<int>(n);
+    cudaMemsetAsync(err, 0, 8 * sizeof(int), s);
+    cudaMemsetAsync(visited, 0, sizeof(int) * count, s);
+    cudaMemsetAsync(hist, 0, sizeof(int) * n, s);
+    const Node* nodes = static_cast<const Node*>(t->nodes);
+    k_check_nodes<Ops><<<blocks_for(count), kBlock, 0, s>>>(
+        nodes, static_cast<const BNode*>(t->bnodes), static_cast<const float*>(t->items), n,
+        visited, err);
+    k_check_refs<<<blocks_for(count), kBlock, 0, s>>>(visited, count, err);
+    k_check_perm<Ops><<<blocks_for(n), kBlock, 0, s>>>(
+        t->prim_ids, t->slot_of, static_cast<const float*>(t->items),
+        static_cast<const float4*>(t->leaves), static_cast<const float*>(items), n, hist, err);
+    k_check_hist<<<blocks_for(n), kBlock, 0, s>>>(hist, n, err);
+    k_check_depth<<<blocks_for(count), kBlock, 0, s>>>(nodes, t->depth_arr, n, err);
+    if (t->wide_count > 0 && t->wide) {
+        k_check_wide<<<blocks_for(n - 1), kBlock, 0, s>>>(nodes, n, t->depth_arr, t->wide_id,
+                                                          static_cast<const WideNode*>(t->wide),
+                                                          err);
+    }
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? QK_OK : cuda_status(e, "validate");
+}
+
+}  // namespace
+
+size_t build_ws_bytes(int kind, int n, int builder) {
+    (void)kind;
+    (void)builder;
+    Carve c;
+    c.take<Header>(1);
+    c.take<uint32_t>(n);
+    c.take<uint32_t>(n);
+    c.take<uint32_t>(n);
+    c.take<uint32_t>(n);
+    c.take<char>(sort_ws_bytes(n));
+    size_t need = c.used;
+    // refit_dirty and wide_build share the build workspace
+    Carve d;
+    d.take<Header>(1);
+    d.take<int>(n);
+    if (d.used > need) need = d.used;
+    Carve w;
+    w.take<char>(scan_ws_bytes(n));
+    if (w.used > need) need = w.used;
+    return need;
+}
+
+int build_tree(qk_tree* t, int builder, int bins, const void* items, void* ws, size_t ws_bytes,
+               cudaStream_t s) {
+    (void)bins;
+    (void)ws_bytes;
+    if (builder != QK_BUILD_LBVH) return fail(QK_ERR_INVALID, "builder %d not available", builder);
+    switch (t->kind) {
+        case kTri: return build_lbvh<TriOps>(t, items, ws, s);
+        case kPoint: return build_lbvh<PointOps>(t, items, ws, s);
+        case kGauss: return build_lbvh<GaussOps>(t, items, ws, s);
+        default: return fail(QK_ERR_INVALID, "unknown primitive kind %d", t->kind);
+    }
+}
+
+int refit_tree(qk_tree* t, const void* items, cudaStream_t s) {
+    switch (t->kind) {
+        case kTri: return refit_impl<TriOps>(t, items, s);
+        case kPoint: return refit_impl<PointOps>(t, items, s);
+        case kGauss: return refit_impl<GaussOps>(t, items, s);
+        default: return fail(QK_ERR_INVALID, "unknown primitive kind %d", t->kind);
+    }
+}
+
+int refit_tree_dirty(qk_tree* t, const int* ids, const void* items, int count, void* ws,
+                     cudaStream_t s) {
+    switch (t->kind) {
+        case kTri: return refit_dirty_impl<TriOps>(t, ids, items, count, ws, s);
+        case kPoint: return refit_dirty_impl<PointOps>(t, ids, items, count, ws, s);
+        case kGauss: return refit_dirty_impl<GaussOps>(t, ids, items, count, ws, s);
+        default: return fail(QK_ERR_INVALID, "unknown primitive kind %d", t->kind);
+    }
+}
+
+int wide_emit_all(qk_tree* t, cudaStream_t s) {
+    const int n = t->n;
+    k_wide_emit<<<blocks_for(n - 1), kBlock, 0, s>>>(static_cast<const Node*>(t->nodes), n,
+                                                     t->depth_arr, t->wide_id,
+                                                     static_cast<WideNode*>(t->wide));
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? QK_OK : cuda_status(e, "wide emit");
+}
+
+int wide_build(qk_tree* t, void* ws, size_t ws_bytes, cudaStream_t s) {
+    (void)ws_bytes;
+    const int n = t->n, m = n - 1;
+    k_wide_flags<<<blocks_for(m), kBlock, 0, s>>>(t->depth_arr, m, t->flags);
+    // wide_id = exclusive scan of the flags; count = last prefix + last flag
+    cudaError_t e = scan_exclusive(t->flags, t->wide_id, m, false, ws, s);
+    if (e != cudaSuccess) return cuda_status(e, "wide scan");
+    int tail[2] = {0, 0};
+    e = cudaMemcpyAsync(&tail[0], t->wide_id + (m - 1), sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(&tail[1], t->flags + (m - 1), sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_status(e, "wide count readback");
+    // the flags are scratch of the bottom-up pass, which expects zeros
+    cudaMemsetAsync(t->flags, 0, sizeof(int) * static_cast<size_t>(m), s);
+    t->wide_count = tail[0] + tail[1];
+    if (t->wide_count <= 0) return fail(QK_ERR_INVALID, "no wide nodes");
+    // first call without a node buffer only sizes it
+    if (t->wide == nullptr) return QK_OK;
+    return wide_emit_all(t, s);
+}
+
+size_t validate_ws_bytes(int n) {
+    Carve c;
+    c.take<int>(2 * static_cast<size_t>(n));
+    c.take<int>(n);
+    return c.used;
+}
+
+int validate_tree(const qk_tree* t, const void* items, int* errors, void* ws, cudaStream_t s) {
+    switch (t->kind) {
+        case kTri: return validate_impl<TriOps>(t, items, errors, ws, s);
+        case kPoint: return validate_impl<PointOps>(t, items, errors, ws, s);
+        case kGauss: return validate_impl<GaussOps>(t, items, errors, ws, s);
+        default: return fail(QK_ERR_INVALID, "unknown primitive kind %d", t->kind);
+    }
+}
+
+}  // namespace qk

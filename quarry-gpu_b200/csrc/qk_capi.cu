@@ -1,0 +1,288 @@
+// qk_capi.cu -- extern "C" entry points (include/quarry_b200.h): argument checks, workspace
+// size checks and dispatch to the launchers.  Errors are reported as status codes with a
+// thread-local message; nothing here allocates device memory or keeps global state.
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+
+#include "qk_internal.cuh"
+
+namespace qk {
+
+namespace {
+thread_local char g_error[512] = "";
+}
+
+void set_error(const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(g_error, sizeof(g_error), fmt, ap);
+    va_end(ap);
+}
+
+int fail(int status, const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(g_error, sizeof(g_error), fmt, ap);
+    va_end(ap);
+    return status;
+}
+
+int cuda_status(cudaError_t e, const char* what) {
+    std::snprintf(g_error, sizeof(g_error), "CUDA %s: %s", what, cudaGetErrorString(e));
+    return QK_ERR_CUDA;
+}
+
+}  // namespace qk
+
+using namespace qk;
+
+namespace {
+
+int check_tree(const qk_tree* t, bool need_bnodes = true) {
+    if (!t) return fail(QK_ERR_INVALID, "tree is NULL");
+    if (t->kind < 0 || t->kind > 2) return fail(QK_ERR_INVALID, "unknown primitive kind %d", t->kind);
+    if (t->n < 2) return fail(QK_ERR_INVALID, "at least 2 primitives are required (n=%d)", t->n);
+    if (!t->nodes || !t->items || !t->prim_ids || !t->parent || !t->depth_arr || !t->leaves ||
+        !t->slot_of || !t->flags || (need_bnodes && !t->bnodes))
+        return fail(QK_ERR_INVALID, "tree has a NULL device array");
+    return QK_OK;
+}
+
+int check_ws(void* ws, size_t have, size_t need) {
+    if (need > 0 && (ws == nullptr || have < need))
+        return fail(QK_ERR_WORKSPACE, "workspace of %zu bytes is smaller than the %zu required",
+                    have, need);
+    return QK_OK;
+}
+
+int check_wide(const qk_tree* t, unsigned flags) {
+    if ((flags & QK_WIDE) && (t->wide == nullptr || t->wide_count <= 0))
+        return fail(QK_ERR_INVALID, "wide nodes not built");
+    if ((flags & QK_ORDER_MORTON) && (flags & QK_ORDER_DIRECTION))
+        return fail(QK_ERR_INVALID, "choose one of QK_ORDER_MORTON and QK_ORDER_DIRECTION");
+    return QK_OK;
+}
+
+cudaStream_t as_stream(void* s) { return static_cast<cudaStream_t>(s); }
+
+}  // namespace
+
+extern "C" {
+
+const char* qk_status_string(int status) {
+    switch (status) {
+        case QK_OK: return "ok";
+        case QK_ERR_INVALID: return "invalid argument";
+        case QK_ERR_CUDA: return "CUDA error";
+        case QK_ERR_WORKSPACE: return "workspace too small";
+        case QK_ERR_OVERFLOW: return "traversal stack overflow";
+        case QK_ERR_DEPTH: return "tree too deep";
+        default: return "unknown status";
+    }
+}
+
+const char* qk_last_error(void) { return g_error; }
+
+int qk_describe(char* buf, int len) {
+    int devices = 0;
+    if (cudaGetDeviceCount(&devices) != cudaSuccess || devices == 0) {
+        if (buf && len > 0) buf[0] = '\0';
+        cudaGetLastError();
+        return 0;
+    }
+    cudaDeviceProp prop{};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return 0;
+    if (buf && len > 0) {
+        std::snprintf(buf, static_cast<size_t>(len), "%s sm_%d%d (%d SM, %.1f GiB)", prop.name,
+                      prop.major, prop.minor, prop.multiProcessorCount,
+                      static_cast<double>(prop.totalGlobalMem) / (1024.0 * 1024.0 * 1024.0));
+    }
+    return 1;
+}
+
+int qk_stride_floats(int kind) { return kind == 0 ? 9 : kind == 1 ? 3 : kind == 2 ? 10 : 0; }
+int qk_leaf_vec4(int kind) { return kind == 0 ? 3 : kind == 1 ? 1 : kind == 2 ? 3 : 0; }
+
+int qk_tree_bytes(int kind, int n, qk_tree_sizes* out) {
+    if (!out) return fail(QK_ERR_INVALID, "sizes pointer is NULL");
+    if (kind < 0 || kind > 2) return fail(QK_ERR_INVALID, "unknown primitive kind %d", kind);
+    if (n < 2) return fail(QK_ERR_INVALID, "at least 2 primitives are required (n=%d)", n);
+    const size_t nn = static_cast<size_t>(n);
+    out->nodes = (2 * nn - 1) * sizeof(Node);
+    out->items = nn * qk_stride_floats(kind) * sizeof(float);
+    out->prim_ids = nn * sizeof(int32_t);
+    out->parent = (2 * nn - 1) * sizeof(int32_t);
+    out->depth_arr = (2 * nn - 1) * sizeof(int32_t);
+    out->bnodes = (nn - 1) * sizeof(BNode);
+    out->leaves = nn * qk_leaf_vec4(kind) * 16;
+    out->slot_of = nn * sizeof(int32_t);
+    out->flags = (nn - 1) * sizeof(int32_t);
+    out->wide = (nn - 1) * sizeof(WideNode);
+    out->wide_id = (nn - 1) * sizeof(int32_t);
+    return QK_OK;
+}
+
+size_t qk_build_workspace_bytes(int kind, int n, int builder) {
+    if (n < 2) return 0;
+    return build_ws_bytes(kind, n, builder);
+}
+
+size_t qk_query_workspace_bytes(int count, unsigned flags) {
+    (void)flags;
+    return count > 0 ? order_ws_bytes(count) : 0;
+}
+
+size_t qk_radius_workspace_bytes(int count, unsigned flags) {
+    return count > 0 ? radius_ws_bytes(count, flags) : 0;
+}
+
+int qk_build(qk_tree* tree, int builder, int sah_bins, const void* items, void* workspace,
+             size_t workspace_bytes, void* stream) {
+    int st = check_tree(tree);
+    if (st) return st;
+    if (!items) return fail(QK_ERR_INVALID, "items is NULL");
+    if (builder != QK_BUILD_LBVH && builder != QK_BUILD_SAH)
+        return fail(QK_ERR_INVALID, "builder must be QK_BUILD_LBVH or QK_BUILD_SAH");
+    if (builder == QK_BUILD_SAH && (sah_bins < 4 || sah_bins > 64))
+        return fail(QK_ERR_INVALID, "sah_bins must be in [4, 64]");
+    st = check_ws(workspace, workspace_bytes, build_ws_bytes(tree->kind, tree->n, builder));
+    if (st) return st;
+    return build_tree(tree, builder, sah_bins, items, workspace, workspace_bytes, as_stream(stream));
+}
+
+int qk_refit(qk_tree* tree, const void* items, void* workspace, size_t workspace_bytes,
+             void* stream) {
+    (void)workspace;
+    (void)workspace_bytes;
+    int st = check_tree(tree);
+    if (st) return st;
+    if (!items) return fail(QK_ERR_INVALID, "items is NULL");
+    return refit_tree(tree, items, as_stream(stream));
+}
+
+int qk_refit_dirty(qk_tree* tree, const int32_t* dirty_ids, const void* dirty_items, int count,
+                   void* workspace, size_t workspace_bytes, void* stream) {
+    int st = check_tree(tree);
+    if (st) return st;
+    if (count < 0) return fail(QK_ERR_INVALID, "negative dirty count");
+    if (count == 0) return QK_OK;
+    if (!dirty_ids || !dirty_items) return fail(QK_ERR_INVALID, "dirty arrays are NULL");
+    st = check_ws(workspace, workspace_bytes, build_ws_bytes(tree->kind, tree->n, 0));
+    if (st) return st;
+    if (count > tree->n) return fail(QK_ERR_INVALID, "more dirty entries than primitives");
+    return refit_tree_dirty(tree, dirty_ids, dirty_items, count, workspace, as_stream(stream));
+}
+
+int qk_wide_build(qk_tree* tree, void* workspace, size_t workspace_bytes, void* stream) {
+    int st = check_tree(tree);
+    if (st) return st;
+    if (!tree->wide_id) return fail(QK_ERR_INVALID, "wide_id is NULL");
+    st = check_ws(workspace, workspace_bytes, build_ws_bytes(tree->kind, tree->n, 0));
+    if (st) return st;
+    return wide_build(tree, workspace, workspace_bytes, as_stream(stream));
+}
+
+int qk_raycast(const qk_tree* tree, const void* rays, int count, uint64_t* out, unsigned flags,
+               uint64_t* stats, void* workspace, size_t workspace_bytes, void* stream) {
+    int st = check_tree(tree);
+    if (st) return st;
+    if (tree->kind != QK_TRI) return fail(QK_ERR_INVALID, "raycast needs a triangle tree");
+    if (count < 0) return fail(QK_ERR_INVALID, "negative ray count");
+    if (count > 0 && (!rays || !out)) return fail(QK_ERR_INVALID, "rays or out is NULL");
+    if ((st = check_wide(tree, flags))) return st;
+    if ((st = check_ws(workspace, workspace_bytes, order_ws_bytes(count)))) return st;
+    return ray_query(tree, rays, count, out, flags, stats, workspace, as_stream(stream));
+}
+
+int qk_closest(const qk_tree* tree, const float* points, int count, void* out, unsigned flags,
+               uint64_t* stats, void* workspace, size_t workspace_bytes, void* stream) {
+    int st = check_tree(tree);
+    if (st) return st;
+    if (count < 0) return fail(QK_ERR_INVALID, "negative query count");
+    if (count > 0 && (!points || !out)) return fail(QK_ERR_INVALID, "points or out is NULL");
+    if (flags & QK_ORDER_DIRECTION) return fail(QK_ERR_INVALID, "direction order is for rays");
+    if ((st = check_wide(tree, flags))) return st;
+    if ((st = check_ws(workspace, workspace_bytes, order_ws_bytes(count)))) return st;
+    return closest_query(tree, points, count, out, flags, stats, workspace, as_stream(stream));
+}
+
+int qk_knn(const qk_tree* tree, const float* points, int count, int k, int stride, void* out,
+           unsigned flags, uint64_t* stats, void* workspace, size_t workspace_bytes,
+           void* stream) {
+    int st = check_tree(tree);
+    if (st) return st;
+    if (k < 1 || k > kMaxKnn) return fail(QK_ERR_INVALID, "k must be in [1, 32]");
+    if (stride < k) return fail(QK_ERR_INVALID, "stride must be >= k");
+    if (count < 0) return fail(QK_ERR_INVALID, "negative query count");
+    if (count > 0 && (!points || !out)) return fail(QK_ERR_INVALID, "points or out is NULL");
+    if (flags & QK_ORDER_DIRECTION) return fail(QK_ERR_INVALID, "direction order is for rays");
+    if ((st = check_wide(tree, flags))) return st;
+    if ((st = check_ws(workspace, workspace_bytes, order_ws_bytes(count)))) return st;
+    return knn_query(tree, points, count, k, stride, out, flags, stats, workspace,
+                     as_stream(stream));
+}
+
+int qk_radius_count(const qk_tree* tree, const float* points, int count, float radius,
+                    int32_t* offsets, int64_t* total_host, unsigned flags, uint64_t* stats,
+                    void* workspace, size_t workspace_bytes, void* stream) {
+    int st = check_tree(tree);
+    if (st) return st;
+    if (!(radius >= 0.0f)) return fail(QK_ERR_INVALID, "radius must be >= 0");
+    if (count < 0) return fail(QK_ERR_INVALID, "negative query count");
+    if (!offsets || !total_host) return fail(QK_ERR_INVALID, "offsets or total is NULL");
+    if (count > 0 && !points) return fail(QK_ERR_INVALID, "points is NULL");
+    if (flags & QK_ORDER_DIRECTION) return fail(QK_ERR_INVALID, "direction order is for rays");
+    if ((st = check_wide(tree, flags))) return st;
+    if ((st = check_ws(workspace, workspace_bytes, radius_ws_bytes(count, flags)))) return st;
+    long long total = 0;
+    st = radius_count(tree, points, count, radius, offsets, &total, flags, stats, workspace,
+                      as_stream(stream));
+    *total_host = total;
+    return st;
+}
+
+int qk_radius_fill(const qk_tree* tree, const float* points, int count, float radius,
+                   const int32_t* offsets, uint64_t* keys, unsigned flags, void* workspace,
+                   size_t workspace_bytes, void* stream) {
+    int st = check_tree(tree);
+    if (st) return st;
+    if (!(radius >= 0.0f)) return fail(QK_ERR_INVALID, "radius must be >= 0");
+    if (count < 0) return fail(QK_ERR_INVALID, "negative query count");
+    if (count > 0 && (!points || !offsets)) return fail(QK_ERR_INVALID, "points or offsets is NULL");
+    if (flags & QK_ORDER_DIRECTION) return fail(QK_ERR_INVALID, "direction order is for rays");
+    if ((st = check_wide(tree, flags))) return st;
+    if ((st = check_ws(workspace, workspace_bytes, radius_ws_bytes(count, flags)))) return st;
+    return radius_fill(tree, points, count, radius, offsets, keys, flags, workspace,
+                       as_stream(stream));
+}
+
+size_t qk_validate_workspace_bytes(int n) { return n >= 2 ? validate_ws_bytes(n) : 0; }
+
+int qk_validate(const qk_tree* tree, const void* items, int32_t* errors, void* workspace,
+                size_t workspace_bytes, void* stream) {
+    int st = check_tree(tree);
+    if (st) return st;
+    if (!items || !errors) return fail(QK_ERR_INVALID, "items or errors is NULL");
+    if ((st = check_ws(workspace, workspace_bytes, validate_ws_bytes(tree->n)))) return st;
+    return validate_tree(tree, items, errors, workspace, as_stream(stream));
+}
+
+size_t qk_sort_workspace_bytes(int n) { return n > 0 ? sort_ws_bytes(n) : 0; }
+
+int qk_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* keys_out,
+                  uint32_t* vals_out, int n, int bits, void* workspace, size_t workspace_bytes,
+                  void* stream) {
+    if (n < 0 || bits < 1 || bits > 32) return fail(QK_ERR_INVALID, "bad n or bits");
+    if (n == 0) return QK_OK;
+    if (!keys_in || !vals_in || !keys_out || !vals_out) return fail(QK_ERR_INVALID, "NULL buffer");
+    int st = check_ws(workspace, workspace_bytes, sort_ws_bytes(n));
+    if (st) return st;
+    const cudaError_t e = sort_pairs(keys_in, vals_in, keys_out, vals_out, n, bits, workspace,
+                                     as_stream(stream));
+    return e == cudaSuccess ? QK_OK : cuda_status(e, "sort");
+}
+
+}  // extern "C"

@@ -1,0 +1,102 @@
+// qk_internal.cuh -- shared host/device plumbing of the engine: workspace carving, error
+// reporting, ordered-float atomics, and the launchers the C ABI (qk_capi.cu) calls.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+
+#include <cuda_runtime.h>
+
+#include "../../include/quarry_b200.h"
+#include "qk_device.cuh"
+
+namespace qk {
+
+constexpr int kBlock = 256;
+constexpr int kStack = 64;       // binary traversal stack (LBVH depth <= 63, SAH depth capped)
+constexpr int kStackWide = 128;  // 4-wide traversal stack (up to 3 far entries per level)
+constexpr int kMaxKnn = 32;
+constexpr int kSortTile = 4096;  // keys per radix-sort tile (256 threads x 16)
+constexpr int kScanBlock = 1024; // elements per scan block (256 threads x 4)
+
+inline int blocks_for(long long n, int per = kBlock) {
+    return static_cast<int>((n + per - 1) / per);
+}
+
+// Thread-local error detail behind qk_last_error().
+void set_error(const char* fmt, ...);
+int fail(int status, const char* fmt, ...);
+int cuda_status(cudaError_t e, const char* what);
+
+// Carves aligned sub-buffers out of one workspace.  With base == nullptr it only measures.
+struct Carve {
+    char* base = nullptr;
+    size_t used = 0;
+    template <typename T>
+    T* take(size_t count, size_t align = 256) {
+        used = (used + align - 1) / align * align;
+        T* p = base ? reinterpret_cast<T*>(base + used) : nullptr;
+        used += count * sizeof(T);
+        return p;
+    }
+};
+
+// IEEE-754 bits mapped to a monotone unsigned order, for atomicMin / atomicMax on floats.
+__device__ __forceinline__ unsigned ord_f(float f) {
+    const unsigned u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float unord_f(unsigned u) {
+    return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
+}
+
+// Per-call header at the start of every workspace: centroid / query bounds as ordered uints,
+// the maximum depth, a counter and the overflow / error words.
+struct Header {
+    unsigned lo[3];
+    unsigned hi[3];
+    int max_depth;
+    int counter;
+    int overflow;
+    int error;
+    int list_count[2];
+    int pad[4];
+};
+
+// ---- sort / scan (qk_sort.cu) ----
+size_t sort_ws_bytes(int n);
+cudaError_t sort_pairs(const uint32_t* kin, const uint32_t* vin, uint32_t* kout, uint32_t* vout,
+                       int n, int bits, void* ws, cudaStream_t s);
+size_t scan_ws_bytes(int n);
+// exclusive scan of n ints; writes the total to out[n] when write_total is set
+cudaError_t scan_exclusive(const int* in, int* out, int n, bool write_total, void* ws,
+                           cudaStream_t s);
+
+// ---- build / refit / wide / validate (qk_build.cu) ----
+size_t build_ws_bytes(int kind, int n, int builder);
+int build_tree(qk_tree* t, int builder, int bins, const void* items, void* ws, size_t ws_bytes,
+               cudaStream_t s);
+int refit_tree(qk_tree* t, const void* items, cudaStream_t s);
+int refit_tree_dirty(qk_tree* t, const int* ids, const void* items, int count, void* ws,
+                     cudaStream_t s);
+int wide_build(qk_tree* t, void* ws, size_t ws_bytes, cudaStream_t s);
+int wide_emit_all(qk_tree* t, cudaStream_t s);
+size_t validate_ws_bytes(int n);
+int validate_tree(const qk_tree* t, const void* items, int* errors, void* ws, cudaStream_t s);
+
+// ---- traversal (qk_query.cu) ----
+size_t order_ws_bytes(int count);
+int ray_query(const qk_tree* t, const void* rays, int count, uint64_t* out, unsigned flags,
+              uint64_t* stats, void* ws, cudaStream_t s);
+int closest_query(const qk_tree* t, const float* pts, int count, void* out, unsigned flags,
+                  uint64_t* stats, void* ws, cudaStream_t s);
+int knn_query(const qk_tree* t, const float* pts, int count, int k, int stride, void* out,
+              unsigned flags, uint64_t* stats, void* ws, cudaStream_t s);
+size_t radius_ws_bytes(int count, unsigned flags);
+int radius_count(const qk_tree* t, const float* pts, int count, float r, int* offsets,
+                 long long* total, unsigned flags, uint64_t* stats, void* ws, cudaStream_t s);
+int radius_fill(const qk_tree* t, const float* pts, int count, float r, const int* offsets,
+                uint64_t* keys, unsigned flags, void* ws, cudaStream_t s);
+
+}  // namespace qk

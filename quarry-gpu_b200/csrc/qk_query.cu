@@ -1,0 +1,1230 @@
+// qk_query.cu -- stack traversals for first-hit rays and closest / kNN / radius queries.
+//
+// One thread per ray or query point.  Binary traversal reads one 64-byte node (four 16-byte
+// vector loads) that holds both child boxes, so each level costs one dependent fetch; leaf
+// children are tested as soon as their box passes, near internal children are followed
+// directly and far ones pushed together with their entry bound, which is re-checked against
+// the current best when popped (the same test the reference's CPU traversal makes at pop
+// time, src/cpu/bvh.cpp:147-152, 230-234).  Pruning keeps the reference's rules exactly --
+// the slab test with its 1e-6 margins for rays and "bound <= best" for point queries
+// (src/gpu/raycast.cu:100-139, src/gpu/query.cu:74-116) -- which is what makes every result
+// independent of tree shape and visit order, and so bit-identical to the CPU reference.
+//
+// Morton ordering (RayOrder::Morton / QueryOrder::Morton) does not gather and scatter copies
+// of the inputs: the sorted permutation is handed to the traversal, thread i works on item
+// order[i] and writes its result in place.
+#include "qk_internal.cuh"
+
+namespace qk {
+
+namespace {
+
+// ---------------------------------------------------------------------------------------
+// Morton keys (src/gpu/morton.h:125-146) for query reordering
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t spread10q(uint32_t v) {
+    v &= 0x3ffu;
+    v = (v | (v << 16)) & 0x030000ffu;
+    v = (v | (v << 8)) & 0x0300f00fu;
+    v = (v | (v << 4)) & 0x030c30c3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+
+__device__ __forceinline__ uint32_t quantize10(float v, float lo, float hi) {
+    if (!(hi > lo)) return 0;
+    float f = (v - lo) / (hi - lo);
+    f = fminf(fmaxf(f, 0.0f), 1.0f);
+    return static_cast<uint32_t>(f * 1023.0f + 0.5f);
+}
+
+// bounds of the 3-float positions at `stride` floats apart (origins of rays or points)
+__global__ __launch_bounds__(kBlock) void k_pos_bounds(const float* __restrict__ p, int stride,
+                                                      int count, Header* __restrict__ h) {
+    float lo[3] = {kInf, kInf, kInf}, hi[3] = {-kInf, -kInf, -kInf};
+    for (int i = blockIdx.x * kBlock + threadIdx.x; i < count; i += kBlock * gridDim.x) {
+        for (int a = 0; a < 3; ++a) {
+            const float v = p[static_cast<size_t>(i) * stride + a];
+            lo[a] = fminf(lo[a], v);
+            hi[a] = fmaxf(hi[a], v);
+        }
+    }
+    for (int a = 0; a < 3; ++a) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            lo[a] = fminf(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], o));
+            hi[a] = fmaxf(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], o));
+        }
+    }
+    if ((threadIdx.x & 31) == 0) {
+        for (int a = 0; a < 3; ++a) {
+            atomicMin(&h->lo[a], ord_f(lo[a]));
+            atomicMax(&h->hi[a], ord_f(hi[a]));
+        }
+    }
+}
+
+__global__ void k_bounds_reset(Header* h, int fixed_unit) {
+    if (threadIdx.x < 3) {
+        h->lo[threadIdx.x] = ord_f(fixed_unit ? -1.0f : kInf);
+        h->hi[threadIdx.x] = ord_f(fixed_unit ? 1.0f : -kInf);
+    }
+    if (threadIdx.x == 0) {
+        h->overflow = 0;
+        h->list_count[0] = 0;
+        h->list_count[1] = 0;
+    }
+}
+
+__global__ __launch_bounds__(kBlock) void k_pos_keys(const float* __restrict__ p, int stride,
+                                                    int offset, int count,
+                                                    const Header* __restrict__ h,
+                                                    uint32_t* __restrict__ keys,
+                                                    uint32_t* __restrict__ idx) {
+    const int i = blockIdx.x * kBlock + threadIdx.x;
+    if (i >= count) return;
+    const float* q = p + static_cast<size_t>(i) * stride + offset;
+    const float lx = unord_f(h->lo[0]), ly = unord_f(h->lo[1]), lz = unord_f(h->lo[2]);
+    const float hx = unord_f(h->hi[0]), hy = unord_f(h->hi[1]), hz = unord_f(h->hi[2]);
+    keys[i] = spread10q(quantize10(q[0], lx, hx)) | (spread10q(quantize10(q[1], ly, hy)) << 1) |
+              (spread10q(quantize10(q[2], lz, hz)) << 2);
+    idx[i] = static_cast<uint32_t>(i);
+}
+
+// ---------------------------------------------------------------------------------------
+// statistics: warp-aggregated counters (src/gpu/raycast.cu:147-156)
+// ---------------------------------------------------------------------------------------
+template <bool kStats>
+__device__ __forceinline__ void flush_stats(bool active, int nodes, int leaves, bool overflow,
+                                            unsigned long long* stats) {
+    if (stats == nullptr) return;
+    const unsigned mask = __ballot_sync(0xffffffffu, active);
+    const unsigned ovf = __ballot_sync(0xffffffffu, overflow);
+    if (kStats) {
+        const int sn = __reduce_add_sync(0xffffffffu, nodes);
+        const int sl = __reduce_add_sync(0xffffffffu, leaves);
+        if ((threadIdx.x & 31) == 0 && mask) {
+            if (sn) atomicAdd(stats + 0, static_cast<unsigned long long>(sn));
+            if (sl) atomicAdd(stats + 1, static_cast<unsigned long long>(sl));
+        }
+    }
+    if ((threadIdx.x & 31) == 0 && ovf) atomicAdd(stats + 2, static_cast<unsigned long long>(__popc(ovf)));
+}
+
+__device__ __forceinline__ void load_bnode(const BNode* __restrict__ bn, int i, float3& llo,
+                                           float3& lhi, float3& rlo, float3& rhi, int& lref,
+                                           int& rref) {
+    const float4* p = reinterpret_cast<const float4*>(bn + i);
+    const float4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2), d = __ldg(p + 3);
+    llo = f3(a.x, a.y, a.z);
+    lhi = f3(a.w, b.x, b.y);
+    rlo = f3(b.z, b.w, c.x);
+    rhi = f3(c.y, c.z, c.w);
+    lref = __float_as_int(d.x);
+    rref = __float_as_int(d.y);
+}
+
+__device__ __forceinline__ Box root_box(const Node* __restrict__ nodes) {
+    const float4* p = reinterpret_cast<const float4*>(nodes);
+    const float4 a = __ldg(p), b = __ldg(p + 1);
+    Box bx;
+    bx.lo = f3(a.x, a.y, a.z);
+    bx.hi = f3(a.w, b.x, b.y);
+    return bx;
+}
+
+// ---------------------------------------------------------------------------------------
+// rays
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ void test_tri(const RayPre& R, const float4* __restrict__ leaves,
+                                         int slot, float& best, float& bound, bool& any) {
+    const float4 a = __ldg(leaves + 3 * slot), b = __ldg(leaves + 3 * slot + 1),
+                 c = __ldg(leaves + 3 * slot + 2);
+    float t;
+    if (ray_tri(R, f3(a.x, a.y, a.z), f3(b.x, b.y, b.z), f3(c.x, c.y, c.z), t) && t < best) {
+        best = t;
+        bound = best * kMarginMul + kMarginAdd;
+        any = true;
+    }
+}
+
+template <bool kStats>
+__global__ __launch_bounds__(kBlock) void k_ray_bin(const BNode* __restrict__ bn,
+                                                   const float4* __restrict__ leaves,
+                                                   const Node* __restrict__ nodes,
+                                                   const float4* __restrict__ rays,
+                                                   const uint32_t* __restrict__ order, int count,
+                                                   unsigned long long* __restrict__ out,
+                                                   int max_iter, unsigned long long* __restrict__ stats) {
+    const int i = blockIdx.x * kBlock + threadIdx.x;
+    const bool active = i < count;
+    int ntests = 0, ttests = 0;
+    bool overflow = false;
+    if (active) {
+        const int r = order ? static_cast<int>(order[i]) : i;
+        const RayPre R = prepare_ray(__ldg(rays + 2 * r), __ldg(rays + 2 * r + 1));
+        float best = R.tmax;
+        float bound = best * kMarginMul + kMarginAdd;
+        bool any = false;
+        const Box rb = root_box(nodes);
+        float te;
+        if (ray_box(R, rb.lo, rb.hi, bound, te)) {
+            ++ntests;
+            int stack[kStack];
+            float stackT[kStack];
+            int sp = 0;
+            int node = 0;
+            for (int iter = 0;; ++iter) {
+                if (iter >= max_iter) {
+                    overflow = true;
+                    break;
+                }
+                float3 llo, lhi, rlo, rhi;
+                int lref, rref;
+                load_bnode(bn, node, llo, lhi, rlo, rhi, lref, rref);
+                float tl, tr;
+                bool hl = ray_box(R, llo, lhi, bound, tl);
+                bool hr = ray_box(R, rlo, rhi, bound, tr);
+                ntests += static_cast<int>(hl) + static_cast<int>(hr);
+                if (hl && lref < 0) {
+                    ++ttests;
+                    test_tri(R, leaves, ~lref, best, bound, any);
+                    hl = false;
+                }
+                if (hr && rref < 0) {
+                    ++ttests;
+                    test_tri(R, leaves, ~rref, best, bound, any);
+                    hr = false;
+                }
+                if (hl && hr) {
+                    const bool lnear = tl <= tr;
+                    if (sp >= kStack) {
+                        overflow = true;
+                        break;
+                    }
+                    stack[sp] = lnear ? rref : lref;
+                    stackT[sp] = lnear ? tr : tl;
+                    ++sp;
+                    node = lnear ? lref : rref;
+                } else if (hl) {
+                    node = lref;
+                } else if (hr) {
+                    node = rref;
+                } else {
+                    // pop the next entry whose box could still hold a closer hit
+                    const float limit = bound * kMarginMul + kMarginAdd;
+                    node = -1;
+                    while (sp > 0) {
+                        --sp;
+                        if (!(stackT[sp] > limit)) {
+                            node = stack[sp];
+                            break;
+                        }
+                    }
+                    if (node < 0) break;
+                }
+            }
+        }
+        out[r] = any ? ((1ull << 32) | static_cast<unsigned long long>(__float_as_uint(best))) : 0ull;
+    }
+    flush_stats<kStats>(active, ntests, ttests, overflow, stats);
+}
+
+__device__ __forceinline__ void load_wide_entry(const WideNode* __restrict__ w, int node, int s,
+                                                float3& lo, float3& hi, int& child) {
+    const float4* p = reinterpret_cast<const float4*>(w + node) + 2 * s;
+    const float4 a = __ldg(p), b = __ldg(p + 1);
+    lo = f3(a.x, a.y, a.z);
+    hi = f3(a.w, b.x, b.y);
+    child = __float_as_int(b.z);
+}
+
+template <bool kStats>
+__global__ __launch_bounds__(kBlock) void k_ray_wide(const WideNode* __restrict__ wn,
+                                                    const float4* __restrict__ leaves,
+                                                    const float4* __restrict__ rays,
+                                                    const uint32_t* __restrict__ order, int count,
+                                                    unsigned long long* __restrict__ out,
+                                                    int max_iter, unsigned long long* __restrict__ stats) {
+    const int i = blockIdx.x * kBlock + threadIdx.x;
+    const bool active = i < count;
+    int ntests = 0, ttests = 0;
+    bool overflow = false;
+    if (active) {
+        const int r = order ? static_cast<int>(order[i]) : i;
+        const RayPre R = prepare_ray(__ldg(rays + 2 * r), __ldg(rays + 2 * r + 1));
+        float best = R.tmax;
+        float bound = best * kMarginMul + kMarginAdd;
+        bool any = false;
+        int stack[kStackWide];
+        float stackT[kStackWide];
+        int sp = 0;
+        int node = 0;  // the 4-wide root has no single box; start inside it (raycast.cu:182)
+        for (int iter = 0;; ++iter) {
+                if (iter >= max_iter) {
+                    overflow = true;
+                    break;
+                }
+            int child[4];
+            float key[4];
+            int hits = 0;
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+                float3 lo, hi;
+                int c;
+                load_wide_entry(wn, node, s, lo, hi, c);
+                float t;
+                if (c != kEmptySlot && ray_box(R, lo, hi, bound, t)) {
+                    ++ntests;
+                    int j = hits++;
+                    while (j > 0 && key[j - 1] > t) {
+                        key[j] = key[j - 1];
+                        child[j] = child[j - 1];
+                        --j;
+                    }
+                    key[j] = t;
+                    child[j] = c;
+                }
+            }
+            // leaves now, nearest first; internal children pushed far-first
+            int next = -1;
+            float nextT = 0.0f;
+            for (int j = 0; j < hits; ++j) {
+                if (child[j] < 0) {
+                    ++ttests;
+                    test_tri(R, leaves, ~child[j], best, bound, any);
+                }
+            }
+            for (int j = hits - 1; j >= 0; --j) {
+                if (child[j] < 0) continue;
+                if (next >= 0) {
+                    if (sp >= kStackWide) {
+                        overflow = true;
+                        break;
+                    }
+                    stack[sp] = next;
+                    stackT[sp] = nextT;
+                    ++sp;
+                }
+                next = child[j];
+                nextT = key[j];
+            }
+            if (overflow) break;
+            // `next` is the nearest internal child; the loop above pushed the farther ones
+            if (next >= 0) {
+                node = next;
+                continue;
+            }
+            const float limit = bound * kMarginMul + kMarginAdd;
+            node = -1;
+            while (sp > 0) {
+                --sp;
+                if (!(stackT[sp] > limit)) {
+                    node = stack[sp];
+                    break;
+                }
+            }
+            if (node < 0) break;
+        }
+        out[r] = any ? ((1ull << 32) | static_cast<unsigned long long>(__float_as_uint(best))) : 0ull;
+    }
+    flush_stats<kStats>(active, ntests, ttests, overflow, stats);
+}
+
+// ---------------------------------------------------------------------------------------
+// closest
+// ---------------------------------------------------------------------------------------
+template <class Ops>
+__device__ __forceinline__ void leaf_closest(float3 p, const float4* __restrict__ leaves, int slot,
+                                             float& best, int& best_id) {
+    int id;
+    const float d2 = Ops::dist2(p, leaves, slot, id);
+    if (best_id < 0 || closer(d2, id, best, best_id)) {
+        best = d2;
+        best_id = id;
+    }
+}
+
+template <class Ops, bool kStats>
+__global__ __launch_bounds__(kBlock) void k_closest_bin(const BNode* __restrict__ bn,
+                                                       const float4* __restrict__ leaves,
+                                                       const float* __restrict__ pts,
+                                                       const uint32_t* __restrict__ order,
+                                                       int count, uint2* __restrict__ out,
+                                                       int max_iter, unsigned long long* __restrict__ stats) {
+    const int i = blockIdx.x * kBlock + threadIdx.x;
+    const bool active = i < count;
+    int ntests = 0, ltests = 0;
+    bool overflow = false;
+    if (active) {
+        const int q = order ? static_cast<int>(order[i]) : i;
+        const float3 p = f3(pts[3 * q], pts[3 * q + 1], pts[3 * q + 2]);
+        float best = kInf;
+        int best_id = -1;
+        int stack[kStack];
+        float stackD[kStack];
+        int sp = 0;
+        int node = 0;
+        for (int iter = 0;; ++iter) {
+                if (iter >= max_iter) {
+                    overflow = true;
+                    break;
+                }
+            ++ntests;
+            float3 llo, lhi, rlo, rhi;
+            int lref, rref;
+            load_bnode(bn, node, llo, lhi, rlo, rhi, lref, rref);
+            const float dl = dist2_box(p, llo, lhi);
+            const float dr = dist2_box(p, rlo, rhi);
+            bool okl = best_id < 0 || dl <= best;
+            bool okr = best_id < 0 || dr <= best;
+            // leaves in near-first order so the second sees the tighter bound
+            const bool lfirst = dl <= dr;
+            if (lfirst) {
+                if (okl && lref < 0) { ++ltests; leaf_closest<Ops>(p, leaves, ~lref, best, best_id); okl = false; }
+                if (okr && rref < 0 && (best_id < 0 || dr <= best)) { ++ltests; leaf_closest<Ops>(p, leaves, ~rref, best, best_id); }
+                if (rref < 0) okr = false;
+            } else {
+                if (okr && rref < 0) { ++ltests; leaf_closest<Ops>(p, leaves, ~rref, best, best_id); okr = false; }
+                if (okl && lref < 0 && (best_id < 0 || dl <= best)) { ++ltests; leaf_closest<Ops>(p, leaves, ~lref, best, best_id); }
+                if (lref < 0) okl = false;
+            }
+            if (okl && okr) {
+                if (sp >= kStack) {
+                    overflow = true;
+                    break;
+                }
+                stack[sp] = lfirst ? rref : lref;
+                stackD[sp] = lfirst ? dr : dl;
+                ++sp;
+                node = lfirst ? lref : rref;
+            } else if (okl) {
+                node = lref;
+            } else if (okr) {
+                node = rref;
+            } else {
+                node = -1;
+                while (sp > 0) {
+                    --sp;
+                    if (best_id < 0 || stackD[sp] <= best) {
+                        node = stack[sp];
+                        break;
+                    }
+                }
+                if (node < 0) break;
+            }
+        }
+        out[q] = best_id >= 0 ? make_uint2(__float_as_uint(best), static_cast<unsigned>(best_id))
+                              : make_uint2(0u, 0xffffffffu);
+    }
+    flush_stats<kStats>(active, ntests, ltests, overflow, stats);
+}
+
+template <class Ops, bool kStats>
+__global__ __launch_bounds__(kBlock) void k_closest_wide(const WideNode* __restrict__ wn,
+                                                        const float4* __restrict__ leaves,
+                                                        const float* __restrict__ pts,
+                                                        const uint32_t* __restrict__ order,
+                                                        int count, uint2* __restrict__ out,
+                                                        int max_iter, unsigned long long* __restrict__ stats) {
+    const int i = blockIdx.x * kBlock + threadIdx.x;
+    const bool active = i < count;
+    int ntests = 0, ltests = 0;
+    bool overflow = false;
+    if (active) {
+        const int q = order ? static_cast<int>(order[i]) : i;
+        const float3 p = f3(pts[3 * q], pts[3 * q + 1], pts[3 * q + 2]);
+        float best = kInf;
+        int best_id = -1;
+        int stack[kStackWide];
+        float stackD[kStackWide];
+        int sp = 0;
+        int node = 0;
+        for (int iter = 0;; ++iter) {
+                if (iter >= max_iter) {
+                    overflow = true;
+                    break;
+                }
+            int child[4];
+            float key[4];
+            int hits = 0;
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+                float3 lo, hi;
+                int c;
+                load_wide_entry(wn, node, s, lo, hi, c);
+                if (c == kEmptySlot) continue;
+                const float d = dist2_box(p, lo, hi);
+                if (best_id >= 0 && d > best) continue;
+                ++ntests;
+                int j = hits++;
+                while (j > 0 && key[j - 1] > d) {
+                    key[j] = key[j - 1];
+                    child[j] = child[j - 1];
+                    --j;
+                }
+                key[j] = d;
+                child[j] = c;
+            }
+            for (int j = 0; j < hits; ++j) {
+                if (child[j] < 0 && (best_id < 0 || key[j] <= best)) {
+                    ++ltests;
+                    leaf_closest<Ops>(p, leaves, ~child[j], best, best_id);
+                }
+            }
+            int next = -1;
+            float nextD = 0.0f;
+            for (int j = hits - 1; j >= 0; --j) {
+                if (child[j] < 0) continue;
+                if (best_id >= 0 && key[j] > best) continue;
+                if (next >= 0) {
+                    if (sp >= kStackWide) {
+                        overflow = true;
+                        break;
+                    }
+                    stack[sp] = next;
+                    stackD[sp] = nextD;
+                    ++sp;
+                }
+                next = child[j];
+                nextD = key[j];
+            }
+            if (overflow) break;
+            if (next >= 0) {
+                node = next;
+                continue;
+            }
+            node = -1;
+            while (sp > 0) {
+                --sp;
+                if (best_id < 0 || stackD[sp] <= best) {
+                    node = stack[sp];
+                    break;
+                }
+            }
+            if (node < 0) break;
+        }
+        out[q] = best_id >= 0 ? make_uint2(__float_as_uint(best), static_cast<unsigned>(best_id))
+                              : make_uint2(0u, 0xffffffffu);
+    }
+    flush_stats<kStats>(active, ntests, ltests, overflow, stats);
+}
+
+// ---------------------------------------------------------------------------------------
+// kNN: the k best (dist2, id) pairs stay sorted in registers (unrolled insertion over a
+// compile-time capacity K >= k).  Empty slots hold (+inf, INT_MAX), so "strictly closer than
+// the k-th" is one comparison whether or not the table is full -- the reference's max-heap
+// replacement rule (src/cpu/bvh.cpp:284-299, src/gpu/query.cu:145-158).
+// ---------------------------------------------------------------------------------------
+template <int K>
+struct KnnTable {
+    float d[K];
+    int id[K];
+    float kd;  // dist2 of entry k-1 (the pruning threshold)
+    int kid;
+
+    __device__ __forceinline__ void init() {
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            d[j] = kInf;
+            id[j] = 0x7fffffff;
+        }
+        kd = kInf;
+        kid = 0x7fffffff;
+    }
+    __device__ __forceinline__ void insert(float xd, int xid, int k) {
+        if (!closer(xd, xid, kd, kid)) return;
+#pragma unroll
+        for (int j = K - 1; j > 0; --j) {
+            const bool shift = closer(xd, xid, d[j - 1], id[j - 1]);
+            const bool place = !shift && closer(xd, xid, d[j], id[j]);
+            const float nd = shift ? d[j - 1] : (place ? xd : d[j]);
+            const int ni = shift ? id[j - 1] : (place ? xid : id[j]);
+            d[j] = nd;
+            id[j] = ni;
+        }
+        if (closer(xd, xid, d[0], id[0])) {
+            d[0] = xd;
+            id[0] = xid;
+        }
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            if (j == k - 1) {
+                kd = d[j];
+                kid = id[j];
+            }
+        }
+    }
+    // prune test for a subtree bound: keep while the table is not full or bound <= k-th
+    __device__ __forceinline__ bool admits(float bound) const { return kid == 0x7fffffff || bound <= kd; }
+};
+
+template <class Ops, int K>
+__device__ __forceinline__ void leaf_knn(float3 p, const float4* __restrict__ leaves, int slot,
+                                         KnnTable<K>& tab, int k) {
+    int id;
+    const float d2 = Ops::dist2(p, leaves, slot, id);
+    tab.insert(d2, id, k);
+}
+
+template <int K>
+__device__ __forceinline__ void write_knn(const KnnTable<K>& tab, int k, uint2* __restrict__ dst) {
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+        if (j < k) {
+            const bool valid = tab.id[j] != 0x7fffffff;
+            dst[j] = valid ? make_uint2(__float_as_uint(tab.d[j]), static_cast<unsigned>(tab.id[j]))
+                           : make_uint2(0u, 0xffffffffu);
+        }
+    }
+}
+
+template <class Ops, int K, bool kStats>
+__global__ __launch_bounds__(kBlock) void k_knn_bin(const BNode* __restrict__ bn,
+                                                   const float4* __restrict__ leaves,
+                                                   const float* __restrict__ pts,
+                                                   const uint32_t* __restrict__ order, int count,
+                                                   int k, int stride, uint2* __restrict__ out,
+                                                   int max_iter, unsigned long long* __restrict__ stats) {
+    const int i = blockIdx.x * kBlock + threadIdx.x;
+    const bool active = i < count;
+    int ntests = 0, ltests = 0;
+    bool overflow = false;
+    if (active) {
+        const int q = order ? static_cast<int>(order[i]) : i;
+        const float3 p = f3(pts[3 * q], pts[3 * q + 1], pts[3 * q + 2]);
+        KnnTable<K> tab;
+        tab.init();
+        int stack[kStack];
+        float stackD[kStack];
+        int sp = 0;
+        int node = 0;
+        for (int iter = 0;; ++iter) {
+                if (iter >= max_iter) {
+                    overflow = true;
+                    break;
+                }
+            ++ntests;
+            float3 llo, lhi, rlo, rhi;
+            int lref, rref;
+            load_bnode(bn, node, llo, lhi, rlo, rhi, lref, rref);
+            const float dl = dist2_box(p, llo, lhi);
+            const float dr = dist2_box(p, rlo, rhi);
+            const bool lfirst = dl <= dr;
+            bool okl = tab.admits(dl);
+            bool okr = tab.admits(dr);
+            if (lfirst) {
+                if (okl && lref < 0) { ++ltests; leaf_knn<Ops, K>(p, leaves, ~lref, tab, k); okl = false; }
+                if (okr && rref < 0 && tab.admits(dr)) { ++ltests; leaf_knn<Ops, K>(p, leaves, ~rref, tab, k); }
+                if (rref < 0) okr = false;
+            } else {
+                if (okr && rref < 0) { ++ltests; leaf_knn<Ops, K>(p, leaves, ~rref, tab, k); okr = false; }
+                if (okl && lref < 0 && tab.admits(dl)) { ++ltests; leaf_knn<Ops, K>(p, leaves, ~lref, tab, k); }
+                if (lref < 0) okl = false;
+            }
+            if (okl && okr) {
+                if (sp >= kStack) {
+                    overflow = true;
+                    break;
+                }
+                stack[sp] = lfirst ? rref : lref;
+                stackD[sp] = lfirst ? dr : dl;
+                ++sp;
+                node = lfirst ? lref : rref;
+            } else if (okl) {
+                node = lref;
+            } else if (okr) {
+                node = rref;
+            } else {
+                node = -1;
+                while (sp > 0) {
+                    --sp;
+                    if (tab.admits(stackD[sp])) {
+                        node = stack[sp];
+                        break;
+                    }
+                }
+                if (node < 0) break;
+            }
+        }
+        write_knn<K>(tab, k, out + static_cast<size_t>(q) * stride);
+    }
+    flush_stats<kStats>(active, ntests, ltests, overflow, stats);
+}
+
+template <class Ops, int K, bool kStats>
+__global__ __launch_bounds__(kBlock) void k_knn_wide(const WideNode* __restrict__ wn,
+                                                    const float4* __restrict__ leaves,
+                                                    const float* __restrict__ pts,
+                                                    const uint32_t* __restrict__ order, int count,
+                                                    int k, int stride, uint2* __restrict__ out,
+                                                    int max_iter, unsigned long long* __restrict__ stats) {
+    const int i = blockIdx.x * kBlock + threadIdx.x;
+    const bool active = i < count;
+    int ntests = 0, ltests = 0;
+    bool overflow = false;
+    if (active) {
+        const int q = order ? static_cast<int>(order[i]) : i;
+        const float3 p = f3(pts[3 * q], pts[3 * q + 1], pts[3 * q + 2]);
+        KnnTable<K> tab;
+        tab.init();
+        int stack[kStackWide];
+        float stackD[kStackWide];
+        int sp = 0;
+        int node = 0;
+        for (int iter = 0;; ++iter) {
+                if (iter >= max_iter) {
+                    overflow = true;
+                    break;
+                }
+            int child[4];
+            float key[4];
+            int hits = 0;
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+                float3 lo, hi;
+                int c;
+                load_wide_entry(wn, node, s, lo, hi, c);
+                if (c == kEmptySlot) continue;
+                const float d = dist2_box(p, lo, hi);
+                if (!tab.admits(d)) continue;
+                ++ntests;
+                int j = hits++;
+                while (j > 0 && key[j - 1] > d) {
+                    key[j] = key[j - 1];
+                    child[j] = child[j - 1];
+                    --j;
+                }
+                key[j] = d;
+                child[j] = c;
+            }
+            for (int j = 0; j < hits; ++j) {
+                if (child[j] < 0 && tab.admits(key[j])) {
+                    ++ltests;
+                    leaf_knn<Ops, K>(p, leaves, ~child[j], tab, k);
+                }
+            }
+            int next = -1;
+            float nextD = 0.0f;
+            for (int j = hits - 1; j >= 0; --j) {
+                if (child[j] < 0 || !tab.admits(key[j])) continue;
+                if (next >= 0) {
+                    if (sp >= kStackWide) {
+                        overflow = true;
+                        break;
+                    }
+                    stack[sp] = next;
+                    stackD[sp] = nextD;
+                    ++sp;
+                }
+                next = child[j];
+                nextD = key[j];
+            }
+            if (overflow) break;
+            if (next >= 0) {
+                node = next;
+                continue;
+            }
+            node = -1;
+            while (sp > 0) {
+                --sp;
+                if (tab.admits(stackD[sp])) {
+                    node = stack[sp];
+                    break;
+                }
+            }
+            if (node < 0) break;
+        }
+        write_knn<K>(tab, k, out + static_cast<size_t>(q) * stride);
+    }
+    flush_stats<kStats>(active, ntests, ltests, overflow, stats);
+}
+
+// ---------------------------------------------------------------------------------------
+// radius: count, then fill at the scanned offsets, then sort every segment by (dist2, id).
+// Rule of src/gpu/query.cu:415-540: a box is entered when its squared distance <= r2, a
+// primitive kept when its dist2 <= r2.
+// ---------------------------------------------------------------------------------------
+template <class Ops, bool kFill, bool kStats>
+__global__ __launch_bounds__(kBlock) void k_radius_bin(
+    const BNode* __restrict__ bn, const float4* __restrict__ leaves, const Node* __restrict__ nodes,
+    const float* __restrict__ pts, const uint32_t* __restrict__ order, int count, float r2,
+    int* __restrict__ counts, const int* __restrict__ offsets,
+    unsigned long long* __restrict__ keys, int max_iter, unsigned long long* __restrict__ stats) {
+    const int i = blockIdx.x * kBlock + threadIdx.x;
+    const bool active = i < count;
+    int ntests = 0, ltests = 0;
+    bool overflow = false;
+    if (active) {
+        const int q = order ? static_cast<int>(order[i]) : i;
+        const float3 p = f3(pts[3 * q], pts[3 * q + 1], pts[3 * q + 2]);
+        int found = 0;
+        int write = kFill ? offsets[q] : 0;
+        const int end = kFill ? offsets[q + 1] : 0;  // never write past this query's segment
+        const Box rb = root_box(nodes);
+        if (dist2_box(p, rb.lo, rb.hi) <= r2) {
+            int stack[kStack];
+            int sp = 0;
+            int node = 0;
+            for (int iter = 0;; ++iter) {
+                if (iter >= max_iter) {
+                    overflow = true;
+                    break;
+                }
+                ++ntests;
+                float3 llo, lhi, rlo, rhi;
+                int lref, rref;
+                load_bnode(bn, node, llo, lhi, rlo, rhi, lref, rref);
+                bool okl = dist2_box(p, llo, lhi) <= r2;
+                bool okr = dist2_box(p, rlo, rhi) <= r2;
+                if (okl && lref < 0) {
+                    ++ltests;
+                    int id;
+                    const float d2 = Ops::dist2(p, leaves, ~lref, id);
+                    if (d2 <= r2) {
+                        if (kFill && write < end) keys[write++] = (static_cast<unsigned long long>(__float_as_uint(d2)) << 32) | static_cast<unsigned>(id);
+                        ++found;
+                    }
+                    okl = false;
+                }
+                if (okr && rref < 0) {
+                    ++ltests;
+                    int id;
+                    const float d2 = Ops::dist2(p, leaves, ~rref, id);
+                    if (d2 <= r2) {
+                        if (kFill && write < end) keys[write++] = (static_cast<unsigned long long>(__float_as_uint(d2)) << 32) | static_cast<unsigned>(id);
+                        ++found;
+                    }
+                    okr = false;
+                }
+                if (okl && okr) {
+                    if (sp >= kStack) {
+                        overflow = true;
+                        break;
+                    }
+                    stack[sp++] = rref;
+                    node = lref;
+                } else if (okl) {
+                    node = lref;
+                } else if (okr) {
+                    node = rref;
+                } else {
+                    if (sp == 0) break;
+                    node = stack[--sp];
+                }
+            }
+        }
+        if (!kFill) counts[q] = found;
+    }
+    flush_stats<kStats>(active, ntests, ltests, overflow, stats);
+}
+
+template <class Ops, bool kFill, bool kStats>
+__global__ __launch_bounds__(kBlock) void k_radius_wide(
+    const WideNode* __restrict__ wn, const float4* __restrict__ leaves,
+    const float* __restrict__ pts, const uint32_t* __restrict__ order, int count, float r2,
+    int* __restrict__ counts, const int* __restrict__ offsets,
+    unsigned long long* __restrict__ keys, int max_iter, unsigned long long* __restrict__ stats) {
+    const int i = blockIdx.x * kBlock + threadIdx.x;
+    const bool active = i < count;
+    int ntests = 0, ltests = 0;
+    bool overflow = false;
+    if (active) {
+        const int q = order ? static_cast<int>(order[i]) : i;
+        const float3 p = f3(pts[3 * q], pts[3 * q + 1], pts[3 * q + 2]);
+        int found = 0;
+        int write = kFill ? offsets[q] : 0;
+        const int end = kFill ? offsets[q + 1] : 0;  // never write past this query's segment
+        int stack[kStackWide];
+        int sp = 0;
+        int node = 0;
+        for (int iter = 0;; ++iter) {
+                if (iter >= max_iter) {
+                    overflow = true;
+                    break;
+                }
+            int next = -1;
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+                float3 lo, hi;
+                int c;
+                load_wide_entry(wn, node, s, lo, hi, c);
+                if (c == kEmptySlot || !(dist2_box(p, lo, hi) <= r2)) continue;
+                ++ntests;
+                if (c < 0) {
+                    ++ltests;
+                    int id;
+                    const float d2 = Ops::dist2(p, leaves, ~c, id);
+                    if (d2 <= r2) {
+                        if (kFill && write < end) keys[write++] = (static_cast<unsigned long long>(__float_as_uint(d2)) << 32) | static_cast<unsigned>(id);
+                        ++found;
+                    }
+                } else if (next < 0) {
+                    next = c;
+                } else if (sp < kStackWide) {
+                    stack[sp++] = c;
+                } else {
+                    overflow = true;
+                }
+            }
+            if (overflow) break;
+            if (next >= 0) {
+                node = next;
+            } else {
+                if (sp == 0) break;
+                node = stack[--sp];
+            }
+        }
+        if (!kFill) counts[q] = found;
+    }
+    flush_stats<kStats>(active, ntests, ltests, overflow, stats);
+}
+
+// ---- segment sort of the radius keys ----
+// all-ascending bitonic network: comparator (i, i ^ (2^j - 1)) then (i, i ^ stride) for
+// shrinking strides, smaller key to the lower index.  Indices >= m are virtual +inf and never
+// move, so a segment of any length sorts in place without padding writes.
+__device__ __forceinline__ void cswap(unsigned long long* a, int i, int j, int m) {
+    if (j < m) {
+        const unsigned long long x = a[i], y = a[j];
+        if (y < x) {
+            a[i] = y;
+            a[j] = x;
+        }
+    }
+}
+
+// one warp per segment of up to 32 keys, in registers
+__global__ __launch_bounds__(kBlock) void k_seg_sort_warp(const int* __restrict__ offsets, int count,
+                                                         unsigned long long* __restrict__ keys,
+                                                         int* __restrict__ medium,
+                                                         int* __restrict__ large,
+                                                         Header* __restrict__ h) {
+    const int lane = threadIdx.x & 31;
+    const int q = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
+    if (q >= count) return;
+    const int b = offsets[q];
+    const int m = offsets[q + 1] - b;
+    if (m <= 1) return;
+    if (m > 32) {
+        if (lane == 0) {
+            if (m <= 4096) medium[atomicAdd(&h->list_count[0], 1)] = q;
+            else large[atomicAdd(&h->list_count[1], 1)] = q;
+        }
+        return;
+    }
+    unsigned long long v = lane < m ? keys[b + lane] : ~0ull;
+    for (int size = 2; size <= 32; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            const int partner = (stride == (size >> 1)) ? (lane ^ (size - 1)) : (lane ^ stride);
+            const unsigned long long o = __shfl_sync(0xffffffffu, v, partner);
+            const bool lower = lane < partner;
+            v = lower ? (o < v ? o : v) : (o > v ? o : v);
+        }
+    }
+    if (lane < m) keys[b + lane] = v;
+}
+
+// one block per listed segment: shared memory (m <= 4096) or global memory in place
+template <bool kShared>
+__global__ __launch_bounds__(kBlock) void k_seg_sort_block(const int* __restrict__ offsets,
+                                                          unsigned long long* __restrict__ keys,
+                                                          const int* __restrict__ list,
+                                                          const Header* __restrict__ h, int which) {
+    __shared__ unsigned long long sm[kShared ? 4096 : 1];
+    const int n_list = h->list_count[which];
+    for (int e = blockIdx.x; e < n_list; e += gridDim.x) {
+        const int q = list[e];
+        const int b = offsets[q];
+        const int m = offsets[q + 1] - b;
+        unsigned long long* a = kShared ? sm : keys + b;
+        if (kShared) {
+            for (int t = threadIdx.x; t < m; t += kBlock) sm[t] = keys[b + t];
+            __syncthreads();
+        }
+        int pow2 = 1;
+        while (pow2 < m) pow2 <<= 1;
+        for (int size = 2; size <= pow2; size <<= 1) {
+            for (int stride = size >> 1; stride > 0; stride >>= 1) {
+                for (int t = threadIdx.x; t < pow2 / 2; t += kBlock) {
+                    // t-th comparator of this stage
+                    int i, j;
+                    if (stride == (size >> 1)) {
+                        const int blk = t / stride, off = t % stride;
+                        i = blk * size + off;
+                        j = blk * size + size - 1 - off;
+                    } else {
+                        const int blk = t / stride, off = t % stride;
+                        i = blk * 2 * stride + off;
+                        j = i + stride;
+                    }
+                    if (i < m) cswap(a, i, j, m);
+                }
+                __syncthreads();
+            }
+        }
+        if (kShared) {
+            for (int t = threadIdx.x; t < m; t += kBlock) keys[b + t] = sm[t];
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------------------
+struct OrderBufs {
+    Header* h = nullptr;
+    uint32_t* keys = nullptr;
+    uint32_t* idx = nullptr;
+    uint32_t* keys_s = nullptr;
+    uint32_t* idx_s = nullptr;
+    void* sort_ws = nullptr;
+};
+
+OrderBufs carve_order(Carve& c, int count) {
+    OrderBufs o;
+    o.h = c.take<Header>(1);
+    o.keys = c.take<uint32_t>(count);
+    o.idx = c.take<uint32_t>(count);
+    o.keys_s = c.take<uint32_t>(count);
+    o.idx_s = c.take<uint32_t>(count);
+    o.sort_ws = c.take<char>(sort_ws_bytes(count));
+    return o;
+}
+
+// Morton order of positions (stride floats apart, `offset` floats into each record);
+// returns the permutation or nullptr for input order.
+const uint32_t* make_order(const float* pos, int stride, int offset, int count, unsigned flags,
+                           OrderBufs& o, cudaStream_t s, int* status) {
+    *status = QK_OK;
+    if (!(flags & (QK_ORDER_MORTON | QK_ORDER_DIRECTION))) return nullptr;
+    const bool dir = (flags & QK_ORDER_DIRECTION) != 0;
+    k_bounds_reset<<<1, 32, 0, s>>>(o.h, dir ? 1 : 0);
+    if (!dir) {
+        const int grid = min(blocks_for(count), 148 * 4);
+        k_pos_bounds<<<grid, kBlock, 0, s>>>(pos + offset, stride, count, o.h);
+    }
+    k_pos_keys<<<blocks_for(count), kBlock, 0, s>>>(pos, stride, offset, count, o.h, o.keys, o.idx);
+    const cudaError_t e = sort_pairs(o.keys, o.idx, o.keys_s, o.idx_s, count, 30, o.sort_ws, s);
+    if (e != cudaSuccess) *status = cuda_status(e, "order sort");
+    return o.idx_s;
+}
+
+template <class Ops>
+int closest_impl(const qk_tree* t, const float* pts, int count, uint2* out, unsigned flags,
+                 unsigned long long* stats, const uint32_t* order, cudaStream_t s) {
+    const float4* leaves = static_cast<const float4*>(t->leaves);
+    const int g = blocks_for(count);
+    const bool wide = (flags & QK_WIDE) != 0;
+    const bool st = stats != nullptr;
+    if (wide) {
+        const WideNode* wn = static_cast<const WideNode*>(t->wide);
+        if (st) k_closest_wide<Ops, true><<<g, kBlock, 0, s>>>(wn, leaves, pts, order, count, out, t->n * 2 + 64, stats);
+        else k_closest_wide<Ops, false><<<g, kBlock, 0, s>>>(wn, leaves, pts, order, count, out, t->n * 2 + 64, stats);
+    } else {
+        const BNode* bn = static_cast<const BNode*>(t->bnodes);
+        if (st) k_closest_bin<Ops, true><<<g, kBlock, 0, s>>>(bn, leaves, pts, order, count, out, t->n * 2 + 64, stats);
+        else k_closest_bin<Ops, false><<<g, kBlock, 0, s>>>(bn, leaves, pts, order, count, out, t->n * 2 + 64, stats);
+    }
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? QK_OK : cuda_status(e, "closest");
+}
+
+template <class Ops, int K>
+void launch_knn(const qk_tree* t, const float* pts, int count, int k, int stride, uint2* out,
+                bool wide, unsigned long long* stats, const uint32_t* order, cudaStream_t s) {
+    const float4* leaves = static_cast<const float4*>(t->leaves);
+    const int g = blocks_for(count);
+    if (wide) {
+        const WideNode* wn = static_cast<const WideNode*>(t->wide);
+        if (stats) k_knn_wide<Ops, K, true><<<g, kBlock, 0, s>>>(wn, leaves, pts, order, count, k, stride, out, t->n * 2 + 64, stats);
+        else k_knn_wide<Ops, K, false><<<g, kBlock, 0, s>>>(wn, leaves, pts, order, count, k, stride, out, t->n * 2 + 64, stats);
+    } else {
+        const BNode* bn = static_cast<const BNode*>(t->bnodes);
+        if (stats) k_knn_bin<Ops, K, true><<<g, kBlock, 0, s>>>(bn, leaves, pts, order, count, k, stride, out, t->n * 2 + 64, stats);
+        else k_knn_bin<Ops, K, false><<<g, kBlock, 0, s>>>(bn, leaves, pts, order, count, k, stride, out, t->n * 2 + 64, stats);
+    }
+}
+
+template <class Ops>
+int knn_impl(const qk_tree* t, const float* pts, int count, int k, int stride, uint2* out,
+             unsigned flags, unsigned long long* stats, const uint32_t* order, cudaStream_t s) {
+    const bool wide = (flags & QK_WIDE) != 0;
+    if (k <= 4) launch_knn<Ops, 4>(t, pts, count, k, stride, out, wide, stats, order, s);
+    else if (k <= 8) launch_knn<Ops, 8>(t, pts, count, k, stride, out, wide, stats, order, s);
+    else if (k <= 16) launch_knn<Ops, 16>(t, pts, count, k, stride, out, wide, stats, order, s);
+    else launch_knn<Ops, 32>(t, pts, count, k, stride, out, wide, stats, order, s);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? QK_OK : cuda_status(e, "knn");
+}
+
+template <class Ops, bool kFill>
+int radius_launch(const qk_tree* t, const float* pts, int count, float r2, int* counts,
+                  const int* offsets, unsigned long long* keys, unsigned flags,
+                  unsigned long long* stats, const uint32_t* order, cudaStream_t s) {
+    const float4* leaves = static_cast<const float4*>(t->leaves);
+    const int g = blocks_for(count);
+    if (flags & QK_WIDE) {
+        const WideNode* wn = static_cast<const WideNode*>(t->wide);
+        if (stats) k_radius_wide<Ops, kFill, true><<<g, kBlock, 0, s>>>(wn, leaves, pts, order, count, r2, counts, offsets, keys, t->n * 2 + 64, stats);
+        else k_radius_wide<Ops, kFill, false><<<g, kBlock, 0, s>>>(wn, leaves, pts, order, count, r2, counts, offsets, keys, t->n * 2 + 64, stats);
+    } else {
+        const BNode* bn = static_cast<const BNode*>(t->bnodes);
+        const Node* nodes = static_cast<const Node*>(t->nodes);
+        if (stats) k_radius_bin<Ops, kFill, true><<<g, kBlock, 0, s>>>(bn, leaves, nodes, pts, order, count, r2, counts, offsets, keys, t->n * 2 + 64, stats);
+        else k_radius_bin<Ops, kFill, false><<<g, kBlock, 0, s>>>(bn, leaves, nodes, pts, order, count, r2, counts, offsets, keys, t->n * 2 + 64, stats);
+    }
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? QK_OK : cuda_status(e, "radius traversal");
+}
+
+template <bool kFill>
+int radius_dispatch(const qk_tree* t, const float* pts, int count, float r2, int* counts,
+                    const int* offsets, unsigned long long* keys, unsigned flags,
+                    unsigned long long* stats, const uint32_t* order, cudaStream_t s) {
+    switch (t->kind) {
+        case kTri: return radius_launch<TriOps, kFill>(t, pts, count, r2, counts, offsets, keys, flags, stats, order, s);
+        case kPoint: return radius_launch<PointOps, kFill>(t, pts, count, r2, counts, offsets, keys, flags, stats, order, s);
+        case kGauss: return radius_launch<GaussOps, kFill>(t, pts, count, r2, counts, offsets, keys, flags, stats, order, s);
+        default: return fail(QK_ERR_INVALID, "unknown primitive kind %d", t->kind);
+    }
+}
+
+}  // namespace
+
+size_t order_ws_bytes(int count) {
+    Carve c;
+    carve_order(c, count);
+    return c.used;
+}
+
+int ray_query(const qk_tree* t, const void* rays, int count, uint64_t* out, unsigned flags,
+              uint64_t* stats, void* ws, cudaStream_t s) {
+    if (count <= 0) return QK_OK;
+    Carve c{static_cast<char*>(ws)};
+    OrderBufs o = carve_order(c, count);
+    int st = QK_OK;
+    const bool dir = (flags & QK_ORDER_DIRECTION) != 0;
+    const uint32_t* order = make_order(static_cast<const float*>(rays), 8, dir ? 3 : 0, count,
+                                       flags, o, s, &st);
+    if (st != QK_OK) return st;
+    const float4* r4 = static_cast<const float4*>(rays);
+    auto* res = reinterpret_cast<unsigned long long*>(out);
+    auto* stt = reinterpret_cast<unsigned long long*>(stats);
+    const float4* leaves = static_cast<const float4*>(t->leaves);
+    const int g = blocks_for(count);
+    if (flags & QK_WIDE) {
+        const WideNode* wn = static_cast<const WideNode*>(t->wide);
+        if (stt) k_ray_wide<true><<<g, kBlock, 0, s>>>(wn, leaves, r4, order, count, res, t->n * 2 + 64, stt);
+        else k_ray_wide<false><<<g, kBlock, 0, s>>>(wn, leaves, r4, order, count, res, t->n * 2 + 64, stt);
+    } else {
+        const BNode* bn = static_cast<const BNode*>(t->bnodes);
+        const Node* nodes = static_cast<const Node*>(t->nodes);
+        if (stt) k_ray_bin<true><<<g, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, t->n * 2 + 64, stt);
+        else k_ray_bin<false><<<g, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, t->n * 2 + 64, stt);
+    }
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? QK_OK : cuda_status(e, "raycast");
+}
+
+int closest_query(const qk_tree* t, const float* pts, int count, void* out, unsigned flags,
+                  uint64_t* stats, void* ws, cudaStream_t s) {
+    if (count <= 0) return QK_OK;
+    Carve c{static_cast<char*>(ws)};
+    OrderBufs o = carve_order(c, count);
+    int st = QK_OK;
+    const uint32_t* order = make_order(pts, 3, 0, count, flags, o, s, &st);
+    if (st != QK_OK) return st;
+    auto* res = static_cast<uint2*>(out);
+    auto* stt = reinterpret_cast<unsigned long long*>(stats);
+    switch (t->kind) {
+        case kTri: return closest_impl<TriOps>(t, pts, count, res, flags, stt, order, s);
+        case kPoint: return closest_impl<PointOps>(t, pts, count, res, flags, stt, order, s);
+        case kGauss: return closest_impl<GaussOps>(t, pts, count, res, flags, stt, order, s);
+        default: return fail(QK_ERR_INVALID, "unknown primitive kind %d", t->kind);
+    }
+}
+
+int knn_query(const qk_tree* t, const float* pts, int count, int k, int stride, void* out,
+              unsigned flags, uint64_t* stats, void* ws, cudaStream_t s) {
+    if (count <= 0) return QK_OK;
+    Carve c{static_cast<char*>(ws)};
+    OrderBufs o = carve_order(c, count);
+    int st = QK_OK;
+    const uint32_t* order = make_order(pts, 3, 0, count, flags, o, s, &st);
+    if (st != QK_OK) return st;
+    auto* res = static_cast<uint2*>(out);
+    auto* stt = reinterpret_cast<unsigned long long*>(stats);
+    switch (t->kind) {
+        case kTri: return knn_impl<TriOps>(t, pts, count, k, stride, res, flags, stt, order, s);
+        case kPoint: return knn_impl<PointOps>(t, pts, count, k, stride, res, flags, stt, order, s);
+        case kGauss: return knn_impl<GaussOps>(t, pts, count, k, stride, res, flags, stt, order, s);
+        default: return fail(QK_ERR_INVALID, "unknown primitive kind %d", t->kind);
+    }
+}
+
+size_t radius_ws_bytes(int count, unsigned flags) {
+    (void)flags;
+    Carve c;
+    carve_order(c, count);
+    c.take<int>(count);            // counts
+    c.take<char>(scan_ws_bytes(count));
+    c.take<int>(count);            // medium segment list
+    c.take<int>(count);            // large segment list
+    return c.used;
+}
+
+int radius_count(const qk_tree* t, const float* pts, int count, float r, int* offsets,
+                 long long* total, unsigned flags, uint64_t* stats, void* ws, cudaStream_t s) {
+    *total = 0;
+    if (count <= 0) {
+        cudaMemsetAsync(offsets, 0, sizeof(int), s);
+        return QK_OK;
+    }
+    Carve c{static_cast<char*>(ws)};
+    OrderBufs o = carve_order(c, count);
+    int* counts = c.take<int>(count);
+    void* scan_ws = c.take<char>(scan_ws_bytes(count));
+    int st = QK_OK;
+    const uint32_t* order = make_order(pts, 3, 0, count, flags, o, s, &st);
+    if (st != QK_OK) return st;
+    st = radius_dispatch<false>(t, pts, count, r * r, counts, nullptr, nullptr, flags,
+                                reinterpret_cast<unsigned long long*>(stats), order, s);
+    if (st != QK_OK) return st;
+    cudaError_t e = scan_exclusive(counts, offsets, count, true, scan_ws, s);
+    if (e != cudaSuccess) return cuda_status(e, "radius scan");
+    int tot = 0;
+    e = cudaMemcpyAsync(&tot, offsets + count, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_status(e, "radius total readback");
+    *total = tot;
+    return QK_OK;
+}
+
+int radius_fill(const qk_tree* t, const float* pts, int count, float r, const int* offsets,
+                uint64_t* keys, unsigned flags, void* ws, cudaStream_t s) {
+    if (count <= 0) return QK_OK;
+    Carve c{static_cast<char*>(ws)};
+    OrderBufs o = carve_order(c, count);
+    c.take<int>(count);
+    c.take<char>(scan_ws_bytes(count));
+    int* medium = c.take<int>(count);
+    int* large = c.take<int>(count);
+    int st = QK_OK;
+    const uint32_t* order = make_order(pts, 3, 0, count, flags, o, s, &st);
+    if (st != QK_OK) return st;
+    auto* k64 = reinterpret_cast<unsigned long long*>(keys);
+    st = radius_dispatch<true>(t, pts, count, r * r, nullptr, offsets, k64, flags, nullptr, order, s);
+    if (st != QK_OK) return st;
+    // reset the segment lists (make_order only resets them on its Morton path)
+    k_bounds_reset<<<1, 32, 0, s>>>(o.h, 0);
+    k_seg_sort_warp<<<blocks_for(count, kBlock / 32), kBlock, 0, s>>>(offsets, count, k64, medium,
+                                                                      large, o.h);
+    k_seg_sort_block<true><<<148 * 2, kBlock, 0, s>>>(offsets, k64, medium, o.h, 0);
+    k_seg_sort_block<false><<<148, kBlock, 0, s>>>(offsets, k64, large, o.h, 1);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? QK_OK : cuda_status(e, "radius sort");
+}
+
+}  // namespace qk

@@ -1,0 +1,309 @@
+"""ctypes binding of the engine's C ABI (include/quarry_b200.h) over torch device memory.
+
+This is the foreign-function view of the engine: every call goes through an extern "C"
+entry point of libquarry_b200.so with plain device pointers, sizes, a workspace and a CUDA
+stream.  torch only provides device allocations and the current stream.
+
+There is no fallback: when the shared library is missing or no CUDA device is present the
+calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libquarry_b200.so"
+
+QK_OK = 0
+QK_TRI, QK_POINT, QK_GAUSS = 0, 1, 2
+QK_BUILD_LBVH, QK_BUILD_SAH = 0, 1
+QK_ORDER_MORTON, QK_ORDER_DIRECTION, QK_WIDE = 1, 2, 4
+KINDS = {"tri": QK_TRI, "point": QK_POINT, "gauss": QK_GAUSS}
+STRIDE = {QK_TRI: 9, QK_POINT: 3, QK_GAUSS: 10}
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_U = ctypes.c_uint
+_F = ctypes.c_float
+_SZ = ctypes.c_size_t
+
+
+class QkTree(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("n", ctypes.c_int32), ("depth", ctypes.c_int32),
+                ("wide_count", ctypes.c_int32), ("nodes", _P), ("items", _P), ("prim_ids", _P),
+                ("parent", _P), ("depth_arr", _P), ("bnodes", _P), ("leaves", _P),
+                ("slot_of", _P), ("flags", _P), ("wide", _P), ("wide_id", _P)]
+
+
+class QkTreeSizes(ctypes.Structure):
+    _fields_ = [(name, _SZ) for name in ("nodes", "items", "prim_ids", "parent", "depth_arr",
+                                          "bnodes", "leaves", "slot_of", "flags", "wide",
+                                          "wide_id")]
+
+
+EXPORTS = {
+    "qk_status_string": (ctypes.c_char_p, [_I]),
+    "qk_last_error": (ctypes.c_char_p, []),
+    "qk_describe": (_I, [ctypes.c_char_p, _I]),
+    "qk_stride_floats": (_I, [_I]),
+    "qk_leaf_vec4": (_I, [_I]),
+    "qk_tree_bytes": (_I, [_I, _I, ctypes.POINTER(QkTreeSizes)]),
+    "qk_build_workspace_bytes": (_SZ, [_I, _I, _I]),
+    "qk_query_workspace_bytes": (_SZ, [_I, _U]),
+    "qk_radius_workspace_bytes": (_SZ, [_I, _U]),
+    "qk_build": (_I, [ctypes.POINTER(QkTree), _I, _I, _P, _P, _SZ, _P]),
+    "qk_refit": (_I, [ctypes.POINTER(QkTree), _P, _P, _SZ, _P]),
+    "qk_refit_dirty": (_I, [ctypes.POINTER(QkTree), _P, _P, _I, _P, _SZ, _P]),
+    "qk_wide_build": (_I, [ctypes.POINTER(QkTree), _P, _SZ, _P]),
+    "qk_raycast": (_I, [ctypes.POINTER(QkTree), _P, _I, _P, _U, _P, _P, _SZ, _P]),
+    "qk_closest": (_I, [ctypes.POINTER(QkTree), _P, _I, _P, _U, _P, _P, _SZ, _P]),
+    "qk_knn": (_I, [ctypes.POINTER(QkTree), _P, _I, _I, _I, _P, _U, _P, _P, _SZ, _P]),
+    "qk_radius_count": (_I, [ctypes.POINTER(QkTree), _P, _I, _F, _P,
+                             ctypes.POINTER(ctypes.c_int64), _U, _P, _P, _SZ, _P]),
+    "qk_radius_fill": (_I, [ctypes.POINTER(QkTree), _P, _I, _F, _P, _P, _U, _P, _SZ, _P]),
+    "qk_validate": (_I, [ctypes.POINTER(QkTree), _P, _P, _P, _SZ, _P]),
+    "qk_validate_workspace_bytes": (_SZ, [_I]),
+    "qk_sort_workspace_bytes": (_SZ, [_I]),
+    "qk_sort_pairs": (_I, [_P, _P, _P, _P, _I, _I, _P, _SZ, _P]),
+}
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Load libquarry_b200.so and declare every export of include/quarry_b200.h."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"{LIB_PATH} is not built; run quarry-gpu_b200/build.py")
+        L = ctypes.CDLL(str(LIB_PATH))
+        for name, (res, args) in EXPORTS.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+class QkError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        L = lib()
+        msg = L.qk_last_error().decode(errors="replace")
+        super().__init__(f"{where}: {L.qk_status_string(status).decode()} ({msg})")
+        self.status = status
+
+
+def check(status: int, where: str) -> None:
+    if status != QK_OK:
+        raise QkError(status, where)
+
+
+def describe() -> str:
+    buf = ctypes.create_string_buffer(256)
+    return buf.value.decode() if lib().qk_describe(buf, 256) else ""
+
+
+# ---------------------------------------------------------------------------------------
+# torch-backed device objects
+# ---------------------------------------------------------------------------------------
+def _torch():
+    import torch
+
+    if not torch.cuda.is_available():
+        raise RuntimeError("the B200 engine needs a CUDA device")
+    return torch
+
+
+def _ptr(t) -> int | None:
+    return None if t is None else t.data_ptr()
+
+
+def _stream():
+    torch = _torch()
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _dev_bytes(nbytes: int):
+    torch = _torch()
+    return torch.empty(max(int(nbytes), 1), dtype=torch.uint8, device="cuda")
+
+
+def to_device(a: np.ndarray, dtype=None):
+    torch = _torch()
+    a = np.ascontiguousarray(a if dtype is None else a.astype(dtype, copy=False))
+    return torch.from_numpy(a).to("cuda")
+
+
+class Workspace:
+    """A growable device scratch buffer reused across calls."""
+
+    def __init__(self):
+        self.buf = None
+
+    def get(self, nbytes: int):
+        if self.buf is None or self.buf.numel() < nbytes:
+            self.buf = _dev_bytes(max(nbytes, 1 << 16))
+        return self.buf
+
+
+class DeviceTree:
+    """One tree: device arrays allocated from torch, filled by qk_build.
+
+    kind: "tri" | "point" | "gauss"; items: (n, stride) float32 in scene order (numpy or a
+    CUDA tensor).  builder: "lbvh" or "sah"."""
+
+    def __init__(self, kind: str, items, builder: str = "lbvh", sah_bins: int = 32):
+        torch = _torch()
+        L = lib()
+        self.kind = KINDS[kind]
+        if isinstance(items, np.ndarray):
+            items = to_device(items.reshape(-1, STRIDE[self.kind]), np.float32)
+        self.items_scene = items.reshape(-1, STRIDE[self.kind]).contiguous()
+        n = self.items_scene.shape[0]
+        self.n = n
+        sizes = QkTreeSizes()
+        check(L.qk_tree_bytes(self.kind, n, ctypes.byref(sizes)), "qk_tree_bytes")
+        self.arrays = {}
+        for name in ("nodes", "items", "prim_ids", "parent", "depth_arr", "bnodes", "leaves",
+                     "slot_of", "flags", "wide_id"):
+            self.arrays[name] = _dev_bytes(getattr(sizes, name))
+        self.arrays["flags"].zero_()
+        self.t = QkTree()
+        self.t.kind = self.kind
+        self.t.n = n
+        for name, buf in self.arrays.items():
+            setattr(self.t, name, buf.data_ptr())
+        self.t.wide = None
+        self.ws = Workspace()
+        self.builder = QK_BUILD_SAH if builder == "sah" else QK_BUILD_LBVH
+        self.sah_bins = sah_bins
+        self.build()
+        del torch
+
+    # ---- build / refit ----
+    def _build_ws(self):
+        nb = lib().qk_build_workspace_bytes(self.kind, self.n, self.builder)
+        return self.ws.get(nb), nb
+
+    def build(self) -> None:
+        ws, nb = self._build_ws()
+        check(lib().qk_build(ctypes.byref(self.t), self.builder, self.sah_bins,
+                             _ptr(self.items_scene), _ptr(ws), ws.numel(), _stream()), "qk_build")
+
+    @property
+    def depth(self) -> int:
+        return self.t.depth
+
+    def build_wide(self) -> int:
+        ws, _ = self._build_ws()
+        self.t.wide = None
+        check(lib().qk_wide_build(ctypes.byref(self.t), _ptr(ws), ws.numel(), _stream()),
+              "qk_wide_build (count)")
+        self.arrays["wide"] = _dev_bytes(self.t.wide_count * 128)
+        self.t.wide = self.arrays["wide"].data_ptr()
+        check(lib().qk_wide_build(ctypes.byref(self.t), _ptr(ws), ws.numel(), _stream()),
+              "qk_wide_build")
+        return self.t.wide_count
+
+    def refit(self, items) -> None:
+        if isinstance(items, np.ndarray):
+            items = to_device(items.reshape(-1, STRIDE[self.kind]), np.float32)
+        self.items_scene = items.reshape(-1, STRIDE[self.kind]).contiguous()
+        ws, _ = self._build_ws()
+        check(lib().qk_refit(ctypes.byref(self.t), _ptr(self.items_scene), _ptr(ws), ws.numel(),
+                             _stream()), "qk_refit")
+
+    def refit_dirty(self, ids, items_subset) -> None:
+        if isinstance(ids, np.ndarray):
+            ids = to_device(ids, np.int32)
+        if isinstance(items_subset, np.ndarray):
+            items_subset = to_device(items_subset.reshape(-1, STRIDE[self.kind]), np.float32)
+        ws, _ = self._build_ws()
+        check(lib().qk_refit_dirty(ctypes.byref(self.t), _ptr(ids), _ptr(items_subset),
+                                   int(ids.numel()), _ptr(ws), ws.numel(), _stream()),
+              "qk_refit_dirty")
+
+    # ---- read-back ----
+    def host(self, name: str, dtype, count: int | None = None) -> np.ndarray:
+        buf = self.arrays[name]
+        a = buf.cpu().numpy().view(dtype)
+        return a if count is None else a[:count]
+
+    def nodes_bytes(self) -> np.ndarray:
+        return self.arrays["nodes"].cpu().numpy()[: (2 * self.n - 1) * 32]
+
+    def validate(self) -> list[int]:
+        torch = _torch()
+        err = torch.zeros(8, dtype=torch.int32, device="cuda")
+        nb = lib().qk_validate_workspace_bytes(self.n)
+        ws = _dev_bytes(nb)
+        check(lib().qk_validate(ctypes.byref(self.t), _ptr(self.items_scene), _ptr(err), _ptr(ws),
+                                ws.numel(), _stream()), "qk_validate")
+        return err.cpu().tolist()
+
+    # ---- queries (device in, device out) ----
+    def raycast(self, rays, flags: int = 0, stats=None, out=None, ws=None):
+        torch = _torch()
+        count = rays.shape[0]
+        if out is None:
+            out = torch.empty(count, dtype=torch.int64, device="cuda")
+        nb = lib().qk_query_workspace_bytes(count, flags)
+        w = ws if ws is not None else self.ws.get(nb)
+        check(lib().qk_raycast(ctypes.byref(self.t), _ptr(rays), count, _ptr(out), flags,
+                               _ptr(stats), _ptr(w), w.numel(), _stream()), "qk_raycast")
+        return out
+
+    def closest(self, pts, flags: int = 0, stats=None, out=None):
+        torch = _torch()
+        count = pts.shape[0]
+        if out is None:
+            out = torch.empty((count, 2), dtype=torch.int32, device="cuda")
+        nb = lib().qk_query_workspace_bytes(count, flags)
+        w = self.ws.get(nb)
+        check(lib().qk_closest(ctypes.byref(self.t), _ptr(pts), count, _ptr(out), flags,
+                               _ptr(stats), _ptr(w), w.numel(), _stream()), "qk_closest")
+        return out
+
+    def knn(self, pts, k: int, flags: int = 0, stats=None, out=None, stride: int | None = None):
+        torch = _torch()
+        count = pts.shape[0]
+        stride = k if stride is None else stride
+        if out is None:
+            out = torch.empty((count, stride, 2), dtype=torch.int32, device="cuda")
+        nb = lib().qk_query_workspace_bytes(count, flags)
+        w = self.ws.get(nb)
+        check(lib().qk_knn(ctypes.byref(self.t), _ptr(pts), count, k, stride, _ptr(out), flags,
+                           _ptr(stats), _ptr(w), w.numel(), _stream()), "qk_knn")
+        return out
+
+    def radius(self, pts, r: float, flags: int = 0, stats=None):
+        torch = _torch()
+        count = pts.shape[0]
+        offsets = torch.empty(count + 1, dtype=torch.int32, device="cuda")
+        nb = lib().qk_radius_workspace_bytes(count, flags)
+        w = self.ws.get(nb)
+        total = ctypes.c_int64(0)
+        check(lib().qk_radius_count(ctypes.byref(self.t), _ptr(pts), count, float(r),
+                                    _ptr(offsets), ctypes.byref(total), flags, _ptr(stats),
+                                    _ptr(w), w.numel(), _stream()), "qk_radius_count")
+        keys = torch.empty(max(total.value, 1), dtype=torch.int64, device="cuda")
+        check(lib().qk_radius_fill(ctypes.byref(self.t), _ptr(pts), count, float(r),
+                                   _ptr(offsets), _ptr(keys), flags, _ptr(w), w.numel(),
+                                   _stream()), "qk_radius_fill")
+        return offsets, keys[: total.value]
+
+
+def sort_pairs(keys, vals, bits: int = 32):
+    """Stable radix sort of uint32 (key, value) tensors on the device (returns copies)."""
+    torch = _torch()
+    n = keys.numel()
+    kin, vin = keys.clone(), vals.clone()
+    kout, vout = torch.empty_like(kin), torch.empty_like(vin)
+    nb = lib().qk_sort_workspace_bytes(n)
+    ws = _dev_bytes(nb)
+    check(lib().qk_sort_pairs(_ptr(kin), _ptr(vin), _ptr(kout), _ptr(vout), n, bits, _ptr(ws),
+                              ws.numel(), _stream()), "qk_sort_pairs")
+    return kout, vout

@@ -1,0 +1,192 @@
+"""Seeded synthetic workloads of the engine's benchmark configurations (host side).
+
+The generators live in csrc/scenes.c (exported by libquarry_b200.so) and compute every
+transcendental from basic IEEE operations, so a seed yields the same bytes on any host.
+
+Workloads (sizes are the benchmark's; every generator takes smaller sizes for tests):
+  terrain   z-up height field on a grid x grid unit lattice, 2 triangles per cell
+            (4 sine octaves, amplitudes 8,4,2,1, frequencies 1/64..1/8), 1M downward rays
+            from z = +100 and 20k closest-point queries in the bounds padded by 2
+  city      131,072 floorless boxes (10 triangles each) on a 363 x 362 lot grid, footprint
+            sides U[1,8], log-normal heights (median 10, sigma 0.8); 1M rays from a plane 50
+            above the tallest roof with cosine-weighted downward directions; 20k kNN (k=8)
+  points    1,048,576 points on a noisy sphere (r=50, radial N(0,0.5)) or uniform in
+            [0,100]^3; 20k queries for closest / kNN8 / radius 1.0; a coherent 1% refit
+  gaussians 1,048,576 ellipsoids, means U[0,100]^3, log-uniform scales [0.05,1], uniform
+            rotations; 262,144 query points
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import capi
+
+_P = ctypes.c_void_p
+_sig_done = False
+
+
+def _lib():
+    global _sig_done
+    L = capi.lib()
+    if not _sig_done:
+        L.qs_cfg_terrain.restype = ctypes.c_int64
+        L.qs_cfg_terrain.argtypes = [ctypes.c_int, ctypes.c_uint64, _P]
+        L.qs_cfg_down_rays.restype = None
+        L.qs_cfg_down_rays.argtypes = [ctypes.c_int] + [ctypes.c_float] * 5 + [ctypes.c_uint64, _P]
+        L.qs_cfg_cosine_rays.restype = None
+        L.qs_cfg_cosine_rays.argtypes = [ctypes.c_int] + [ctypes.c_float] * 5 + [ctypes.c_uint64, _P]
+        L.qs_cfg_uniform_points.restype = None
+        L.qs_cfg_uniform_points.argtypes = [ctypes.c_int, _P, _P, ctypes.c_uint64, ctypes.c_uint64, _P]
+        L.qs_cfg_city.restype = ctypes.c_int64
+        L.qs_cfg_city.argtypes = [ctypes.c_int, ctypes.c_uint64, _P, _P]
+        L.qs_cfg_points.restype = None
+        L.qs_cfg_points.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_uint64, _P]
+        L.qs_cfg_coherent_motion.restype = None
+        L.qs_cfg_coherent_motion.argtypes = [_P, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                                             ctypes.c_uint64, _P, _P]
+        L.qs_cfg_gaussians.restype = None
+        L.qs_cfg_gaussians.argtypes = [ctypes.c_int, ctypes.c_float, ctypes.c_float,
+                                       ctypes.c_uint64, _P]
+        L.qs_log_uniform_int.restype = ctypes.c_int
+        L.qs_log_uniform_int.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int, ctypes.c_int]
+        L.qs_demo_mesh.restype = ctypes.c_int64
+        L.qs_demo_mesh.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint64,
+                                   ctypes.c_int, _P]
+        L.qs_demo_gaussians.restype = None
+        L.qs_demo_gaussians.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_uint64, _P]
+        for f in ("qs_det_sin", "qs_det_cos", "qs_det_log", "qs_det_exp"):
+            getattr(L, f).restype = ctypes.c_double
+            getattr(L, f).argtypes = [ctypes.c_double]
+        _sig_done = True
+    return L
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(_P)
+
+
+def bounds_of(tris: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    v = tris.reshape(-1, 3)
+    return v.min(axis=0), v.max(axis=0)
+
+
+def terrain(grid: int = 256, seed: int = 1) -> np.ndarray:
+    L = _lib()
+    n = L.qs_cfg_terrain(grid, seed, None)
+    t = np.zeros((n, 9), np.float32)
+    L.qs_cfg_terrain(grid, seed, _p(t))
+    return t
+
+
+def down_rays(count: int, x0: float, x1: float, y0: float, y1: float, z: float,
+              seed: int = 1) -> np.ndarray:
+    r = np.zeros((count, 8), np.float32)
+    _lib().qs_cfg_down_rays(count, x0, x1, y0, y1, z, seed, _p(r))
+    return r
+
+
+def cosine_rays(count: int, x0: float, x1: float, y0: float, y1: float, z: float,
+                seed: int = 1) -> np.ndarray:
+    r = np.zeros((count, 8), np.float32)
+    _lib().qs_cfg_cosine_rays(count, x0, x1, y0, y1, z, seed, _p(r))
+    return r
+
+
+def uniform_points(count: int, lo, hi, seed: int = 1, stream: int = 13) -> np.ndarray:
+    lo = np.ascontiguousarray(lo, np.float32)
+    hi = np.ascontiguousarray(hi, np.float32)
+    p = np.zeros((count, 3), np.float32)
+    _lib().qs_cfg_uniform_points(count, _p(lo), _p(hi), seed, stream, _p(p))
+    return p
+
+
+def city(buildings: int = 131072, seed: int = 1) -> tuple[np.ndarray, float]:
+    L = _lib()
+    n = L.qs_cfg_city(buildings, seed, None, None)
+    t = np.zeros((n, 9), np.float32)
+    top = ctypes.c_float(0.0)
+    L.qs_cfg_city(buildings, seed, _p(t), ctypes.byref(top))
+    return t, top.value
+
+
+def point_cloud(kind: str = "volume", count: int = 1048576, seed: int = 1) -> np.ndarray:
+    p = np.zeros((count, 3), np.float32)
+    _lib().qs_cfg_points(1 if kind == "volume" else 0, count, seed, _p(p))
+    return p
+
+
+def coherent_motion(pts: np.ndarray, fraction: float = 0.01, sigma: float = 0.05,
+                    seed: int = 1) -> tuple[np.ndarray, np.ndarray]:
+    pts = np.ascontiguousarray(pts, np.float32)
+    dirty = max(1, int(round(fraction * pts.shape[0])))
+    out = np.zeros_like(pts)
+    ids = np.zeros(dirty, np.int32)
+    _lib().qs_cfg_coherent_motion(_p(pts), pts.shape[0], dirty, sigma, seed, _p(out), _p(ids))
+    return out, ids
+
+
+def gaussians(count: int = 1048576, smin: float = 0.05, smax: float = 1.0,
+              seed: int = 1) -> np.ndarray:
+    g = np.zeros((count, 10), np.float32)
+    _lib().qs_cfg_gaussians(count, smin, smax, seed, _p(g))
+    return g
+
+
+def log_uniform_int(seed: int, stream: int, lo: int, hi: int) -> int:
+    return _lib().qs_log_uniform_int(seed, stream, lo, hi)
+
+
+def demo_mesh_tris(kind: int, grid: int, random_tris: int, seed: int, buildings: int) -> np.ndarray:
+    L = _lib()
+    n = L.qs_demo_mesh(kind, grid, random_tris, seed, buildings, None)
+    if n < 0:
+        raise ValueError("unknown demo mesh kind")
+    t = np.zeros((n, 9), np.float32)
+    L.qs_demo_mesh(kind, grid, random_tris, seed, buildings, _p(t))
+    return t
+
+
+def demo_gaussians(kind: int, count: int, seed: int) -> np.ndarray:
+    g = np.zeros((count, 10), np.float32)
+    _lib().qs_demo_gaussians(kind, count, seed, _p(g))
+    return g
+
+
+# ---------------------------------------------------------------------------------------
+# the benchmark configurations
+# ---------------------------------------------------------------------------------------
+@dataclass
+class TerrainConfig:
+    tris: np.ndarray
+    rays: np.ndarray
+    queries: np.ndarray
+
+
+def terrain_config(grid: int = 256, rays: int = 1_000_000, queries: int = 20_000,
+                   seed: int = 1) -> TerrainConfig:
+    tris = terrain(grid, seed)
+    lo, hi = bounds_of(tris)
+    r = down_rays(rays, 0.0, float(grid), 0.0, float(grid), 100.0, seed)
+    q = uniform_points(queries, lo - 2.0, hi + 2.0, seed, 13)
+    return TerrainConfig(tris, r, q)
+
+
+@dataclass
+class CityConfig:
+    tris: np.ndarray
+    rays: np.ndarray
+    queries: np.ndarray
+    top: float
+
+
+def city_config(buildings: int = 131072, rays: int = 1_000_000, queries: int = 20_000,
+                seed: int = 1) -> CityConfig:
+    tris, top = city(buildings, seed)
+    lo, hi = bounds_of(tris)
+    r = cosine_rays(rays, float(lo[0]), float(hi[0]), float(lo[1]), float(hi[1]), top + 50.0,
+                    seed)
+    q = uniform_points(queries, lo, hi, seed, 13)
+    return CityConfig(tris, r, q, top)

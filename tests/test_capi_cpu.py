@@ -1,0 +1,72 @@
+"""Host-side checks of the C ABI library (no GPU needed): it loads, exports every function
+include/quarry_b200.h declares, sizes buffers and rejects bad arguments with status codes."""
+from __future__ import annotations
+
+import ctypes
+import re
+from pathlib import Path
+
+import pytest
+
+from quarry import capi
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def declared_functions() -> list[str]:
+    names = []
+    for h in sorted((ROOT / "include").glob("*.h")):
+        text = h.read_text()
+        names += re.findall(r"^\s*(?:const\s+)?[A-Za-z_][A-Za-z0-9_ ]*\**\s+\**(qk_[a-z0-9_]+)\(",
+                            text, flags=re.M)
+    return sorted(set(names))
+
+
+def test_library_exports_every_declared_symbol():
+    names = declared_functions()
+    assert len(names) >= 20
+    lib = capi.lib()
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    assert set(names) <= set(capi.EXPORTS) | {"qk_status_string", "qk_last_error"}
+
+
+def test_sizes_and_status_strings():
+    L = capi.lib()
+    s = capi.QkTreeSizes()
+    assert L.qk_tree_bytes(capi.QK_TRI, 1000, ctypes.byref(s)) == 0
+    assert s.nodes == 1999 * 32 and s.items == 1000 * 36 and s.bnodes == 999 * 64
+    assert s.leaves == 1000 * 48
+    assert L.qk_tree_bytes(capi.QK_GAUSS, 10, ctypes.byref(s)) == 0 and s.items == 400
+    assert L.qk_tree_bytes(capi.QK_POINT, 1, ctypes.byref(s)) == capi.QK_ERR_INVALID if hasattr(capi, "QK_ERR_INVALID") else 1
+    assert L.qk_build_workspace_bytes(capi.QK_TRI, 1 << 20, 0) > 16 << 20
+    assert L.qk_query_workspace_bytes(1000, 1) > 0
+    assert L.qk_stride_floats(0) == 9 and L.qk_stride_floats(1) == 3 and L.qk_stride_floats(2) == 10
+    assert L.qk_status_string(0) == b"ok"
+
+
+def test_bad_arguments_are_rejected_without_touching_the_device():
+    L = capi.lib()
+    t = capi.QkTree()
+    t.kind = 0
+    t.n = 1
+    assert L.qk_build(ctypes.byref(t), 0, 0, None, None, 0, None) == 1
+    assert b"at least 2" in L.qk_last_error()
+    assert L.qk_build(None, 0, 0, None, None, 0, None) == 1
+    t.n = 100
+    t.kind = 7
+    assert L.qk_build(ctypes.byref(t), 0, 0, None, None, 0, None) == 1
+    assert L.qk_knn(None, None, 0, 0, 0, None, 0, None, None, 0, None) == 1
+    assert L.qk_sort_pairs(None, None, None, None, -1, 8, None, 0, None) == 1
+
+
+@pytest.mark.parametrize("k,stride", [(0, 1), (33, 40), (4, 3)])
+def test_knn_argument_checks(k, stride):
+    L = capi.lib()
+    t = capi.QkTree()
+    t.kind = 1
+    t.n = 10
+    for name in ("nodes", "items", "prim_ids", "parent", "depth_arr", "bnodes", "leaves",
+                 "slot_of", "flags"):
+        setattr(t, name, 16)  # never dereferenced: the checks run first
+    assert L.qk_knn(ctypes.byref(t), None, 0, k, stride, None, 0, None, None, 0, None) == 1

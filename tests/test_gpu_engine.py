@@ -1,0 +1,256 @@
+"""GPU parity of the engine through its C ABI (quarry.capi) against the oracle.
+
+Every check is bit-exact: node arrays and tree hashes against the oracle's restatement of
+the reference LBVH, ray results as (hit << 32 | bits(t)), query results as (dist2 bits, id),
+radius CSR keys, for binary and 4-wide traversal, input and Morton order.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import oracle
+from quarry import capi, workloads
+
+pytestmark = pytest.mark.gpu
+
+FLAG_SETS = [0, capi.QK_ORDER_MORTON, capi.QK_WIDE, capi.QK_ORDER_MORTON | capi.QK_WIDE]
+
+
+def _dev(a, dtype=np.float32):
+    return capi.to_device(np.ascontiguousarray(a), dtype)
+
+
+def _random_rays(lo, hi, n, seed):
+    """Rays from a sphere around the box toward jittered targets (some miss)."""
+    rng = np.random.default_rng(seed)
+    c = (lo + hi) / 2
+    ext = hi - lo
+    rad = 1.6 * float(np.linalg.norm(ext))
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    o = c + d * rad
+    tgt = c + (rng.random((n, 3)) * 2 - 1) * ext * 0.9
+    dirs = tgt - o
+    dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
+    rays = np.zeros((n, 8), np.float32)
+    rays[:, :3] = o
+    rays[:, 3:6] = dirs
+    rays[:, 6] = 1e-6
+    rays[:, 7] = rad * 4
+    return rays
+
+
+def _scenes():
+    terrain = workloads.terrain(48, 3)
+    mixed = workloads.demo_mesh_tris(2, 24, 1500, 7, 0)
+    city, _ = workloads.city(300, 5)
+    return {"terrain": terrain, "mixed": mixed, "city": city}
+
+
+SCENES = None
+
+
+def scenes():
+    global SCENES
+    if SCENES is None:
+        SCENES = _scenes()
+    return SCENES
+
+
+def _check_tree(tree: capi.DeviceTree, ref: oracle.LBVH):
+    n = tree.n
+    got_nodes = tree.nodes_bytes()
+    assert got_nodes.tobytes() == ref.nodes.tobytes(), "node array differs from the oracle"
+    assert np.array_equal(tree.host("prim_ids", np.int32, n), ref.prim_ids)
+    assert np.array_equal(tree.host("depth_arr", np.int32, 2 * n - 1), ref.depth_arr)
+    assert tree.depth == ref.depth
+    assert tree.validate() == [0] * 8
+
+
+# ---------------------------------------------------------------------------------------
+# radix sort
+# ---------------------------------------------------------------------------------------
+@pytest.mark.parametrize("n,bits", [(1, 8), (5, 30), (4096, 30), (4097, 30), (100_000, 32),
+                                    (300_000, 30)])
+def test_sort_pairs_stable(cuda, n, bits):
+    rng = np.random.default_rng(n)
+    keys = rng.integers(0, 2 ** bits if bits < 32 else 2 ** 32, size=n, dtype=np.uint64)
+    keys[: n // 3] = keys[0]  # many duplicates exercise stability
+    keys = keys.astype(np.uint32)
+    vals = np.arange(n, dtype=np.uint32)
+    kd, vd = capi.sort_pairs(_dev(keys.view(np.int32), np.int32), _dev(vals.view(np.int32), np.int32), bits)
+    order = np.argsort(keys & np.uint32((1 << bits) - 1 if bits < 32 else 0xFFFFFFFF), kind="stable")
+    assert np.array_equal(vd.cpu().numpy().view(np.uint32), vals[order])
+    assert np.array_equal(kd.cpu().numpy().view(np.uint32), keys[order])
+
+
+# ---------------------------------------------------------------------------------------
+# LBVH build == the reference algorithm (oracle restatement), bit for bit
+# ---------------------------------------------------------------------------------------
+@pytest.mark.parametrize("name", ["terrain", "mixed", "city"])
+def test_lbvh_triangles_match_oracle(cuda, name):
+    tris = scenes()[name]
+    tree = capi.DeviceTree("tri", tris)
+    _check_tree(tree, oracle.LBVH("tri", tris))
+
+
+@pytest.mark.parametrize("kind,n", [("point", 2), ("point", 3), ("point", 1000),
+                                    ("point", 50_000), ("gauss", 2), ("gauss", 5000)])
+def test_lbvh_points_gaussians_match_oracle(cuda, kind, n):
+    if kind == "point":
+        items = workloads.point_cloud("volume", n, 11)
+    else:
+        items = workloads.gaussians(n, 0.05, 1.0, 11)
+    tree = capi.DeviceTree(kind, items)
+    _check_tree(tree, oracle.LBVH(kind, items))
+
+
+def test_lbvh_duplicate_positions(cuda):
+    """All-coincident and repeated points: equal Morton codes ordered by index."""
+    pts = np.zeros((777, 3), np.float32)
+    pts[::3] = [1.0, 2.0, 3.0]
+    tree = capi.DeviceTree("point", pts)
+    _check_tree(tree, oracle.LBVH("point", pts))
+
+
+def test_wide_nodes_match_oracle(cuda):
+    tris = scenes()["terrain"]
+    tree = capi.DeviceTree("tri", tris)
+    count = tree.build_wide()
+    ref = oracle.LBVH("tri", tris)
+    wide, wide_id = ref.wide()
+    assert count == len(wide) // 4
+    got = tree.arrays["wide"].cpu().numpy()[: count * 128]
+    assert got.tobytes() == wide.tobytes()
+    assert np.array_equal(tree.host("wide_id", np.int32, tree.n - 1), wide_id)
+    assert tree.validate() == [0] * 8
+
+
+# ---------------------------------------------------------------------------------------
+# rays
+# ---------------------------------------------------------------------------------------
+@pytest.mark.parametrize("name", ["terrain", "mixed", "city"])
+def test_raycast_parity(cuda, name):
+    tris = scenes()[name]
+    lo, hi = workloads.bounds_of(tris)
+    ref = oracle.LBVH("tri", tris)
+    tree = capi.DeviceTree("tri", tris)
+    tree.build_wide()
+    ray_sets = [
+        workloads.down_rays(20_000, float(lo[0]), float(hi[0]), float(lo[1]), float(hi[1]),
+                            float(hi[2]) + 10.0, 9),
+        _random_rays(lo, hi, 20_000, 10),
+        workloads.cosine_rays(20_000, float(lo[0]), float(hi[0]), float(lo[1]), float(hi[1]),
+                              float(hi[2]) + 5.0, 12),
+    ]
+    for rays in ray_sets:
+        want = ref.raycast(rays)
+        d_rays = _dev(rays)
+        for flags in FLAG_SETS + [capi.QK_ORDER_DIRECTION, capi.QK_ORDER_DIRECTION | capi.QK_WIDE]:
+            got = tree.raycast(d_rays, flags).cpu().numpy().view(np.uint64)
+            assert np.array_equal(got, want), f"flags={flags}: {(got != want).sum()} rays differ"
+
+
+def test_raycast_stats_and_no_overflow(cuda):
+    tris = scenes()["terrain"]
+    tree = capi.DeviceTree("tri", tris)
+    lo, hi = workloads.bounds_of(tris)
+    rays = workloads.down_rays(5000, float(lo[0]), float(hi[0]), float(lo[1]), float(hi[1]), 50.0, 3)
+    stats = cuda.zeros(4, dtype=cuda.int64, device="cuda")
+    tree.raycast(_dev(rays), 0, stats=stats)
+    s = stats.cpu().numpy()
+    assert s[0] > 5000 and s[1] >= 5000 and s[2] == 0
+
+
+# ---------------------------------------------------------------------------------------
+# point queries over the three primitive kinds
+# ---------------------------------------------------------------------------------------
+def _items(kind):
+    if kind == "tri":
+        return scenes()["mixed"]
+    if kind == "point":
+        return workloads.point_cloud("sphere", 30_000, 4)
+    return workloads.gaussians(6000, 0.05, 1.0, 4)
+
+
+def _queries(items, kind, n, seed):
+    if kind == "tri":
+        lo, hi = workloads.bounds_of(items)
+    else:
+        lo, hi = items[:, :3].min(0), items[:, :3].max(0)
+    return workloads.uniform_points(n, lo - 1.0, hi + 1.0, seed, 21)
+
+
+@pytest.mark.parametrize("kind", ["tri", "point", "gauss"])
+def test_closest_knn_parity(cuda, kind):
+    items = _items(kind)
+    q = _queries(items, kind, 4000, 5)
+    ref = oracle.LBVH(kind, items)
+    tree = capi.DeviceTree(kind, items)
+    tree.build_wide()
+    dq = _dev(q)
+    want_c = ref.closest(q)
+    for flags in FLAG_SETS:
+        got = tree.closest(dq, flags).cpu().numpy().view(np.uint32)
+        assert np.array_equal(got, want_c), f"closest flags={flags}"
+    for k in (1, 3, 8, 16, 32):
+        want_k = ref.knn(q, k)
+        for flags in FLAG_SETS:
+            got = tree.knn(dq, k, flags).cpu().numpy().view(np.uint32)
+            assert np.array_equal(got, want_k), f"knn k={k} flags={flags}"
+    # wider stride than k pads only the first k entries of each row
+    got = tree.knn(dq, 5, 0, stride=9).cpu().numpy().view(np.uint32)
+    assert np.array_equal(got[:, :5], ref.knn(q, 5))
+
+
+@pytest.mark.parametrize("kind,r", [("tri", 2.5), ("point", 4.0), ("gauss", 1.5),
+                                    ("point", 0.0), ("point", 40.0)])
+def test_radius_parity(cuda, kind, r):
+    items = _items(kind)
+    q = _queries(items, kind, 1500, 6)
+    ref = oracle.LBVH(kind, items)
+    want_off, want_keys = ref.radius(q, r)
+    tree = capi.DeviceTree(kind, items)
+    tree.build_wide()
+    dq = _dev(q)
+    for flags in FLAG_SETS:
+        off, keys = tree.radius(dq, r, flags)
+        off = off.cpu().numpy().astype(np.int64)
+        keys = keys.cpu().numpy().view(np.uint64)
+        assert np.array_equal(off, want_off), f"offsets flags={flags}"
+        assert np.array_equal(keys, want_keys), f"keys flags={flags}"
+
+
+# ---------------------------------------------------------------------------------------
+# refit
+# ---------------------------------------------------------------------------------------
+@pytest.mark.parametrize("kind", ["tri", "point", "gauss"])
+def test_refit_full_and_dirty(cuda, kind):
+    items = _items(kind).copy()
+    tree = capi.DeviceTree(kind, items)
+    tree.build_wide()
+    ref = oracle.LBVH(kind, items)
+    rng = np.random.default_rng(3)
+    moved = items.copy()
+    moved[:, :3] += rng.normal(0, 0.05, size=(len(items), 3)).astype(np.float32)
+    if kind == "tri":
+        moved[:, 3:9] += rng.normal(0, 0.05, size=(len(items), 6)).astype(np.float32)
+    tree.refit(moved)
+    ref.refit(moved)
+    assert tree.nodes_bytes().tobytes() == ref.nodes.tobytes()
+    assert tree.validate() == [0] * 8
+    # partial: move a subset (with a repeated id) and refit only those
+    ids = np.unique(rng.integers(0, len(items), size=max(3, len(items) // 100))).astype(np.int32)
+    again = moved.copy()
+    again[ids, :3] += np.float32(0.5)
+    dup = np.concatenate([ids, ids[:1]])
+    tree.refit_dirty(dup, again[dup])
+    tree.items_scene = _dev(again)
+    ref.refit(again)
+    assert tree.nodes_bytes().tobytes() == ref.nodes.tobytes()
+    assert tree.validate() == [0] * 8
+    q = _queries(again, kind, 1000, 8)
+    for flags in (0, capi.QK_WIDE):
+        got = tree.closest(_dev(q), flags).cpu().numpy().view(np.uint32)
+        assert np.array_equal(got, ref.closest(q))

@@ -240,45 +240,41 @@ def main():
     cfg, desc = make_workload(args.workload, args.small, rank)
     nrays = cfg.rays.shape[0]
 
-    # ---- build (timed beside the step) ----
-    t_build = []
-    tree = None
-    for i in range(3):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        tree = capi.DeviceTree("tri", cfg.tris)
-        torch.cuda.synchronize()
-        t_build.append((time.perf_counter() - t0) * 1e3)
-    build_ms = float(min(t_build))
-    tree.build_wide()
+    # ---- builds (timed beside the step): LBVH and binned SAH with 32 bins ----
+    def timed_build(builder):
+        times, tr = [], None
+        for _ in range(3):
+            tr = None
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            tr = capi.DeviceTree("tri", cfg.tris, builder=builder, sah_bins=32)
+            torch.cuda.synchronize()
+            times.append((time.perf_counter() - t0) * 1e3)
+        tr.build_wide()
+        return tr, float(min(times))
+
+    trees, build_ms = {}, {}
+    for b in ("lbvh", "sah"):
+        trees[b], build_ms[b] = timed_build(b)
 
     rays_d = capi.to_device(cfg.rays, np.float32)
     q_d = capi.to_device(cfg.queries, np.float32)
     l2_flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
 
-    variants = {"bin": 0, "bin_morton": capi.QK_ORDER_MORTON, "wide": capi.QK_WIDE,
-                "wide_morton": capi.QK_WIDE | capi.QK_ORDER_MORTON}
+    modes = {"bin": 0, "bin_morton": capi.QK_ORDER_MORTON, "wide": capi.QK_WIDE,
+             "wide_morton": capi.QK_WIDE | capi.QK_ORDER_MORTON}
+    variants = {f"{b}_{m}": (b, f) for b in trees for m, f in modes.items()}
     if args.only:
         variants = {args.only: variants[args.only]}
 
-    # canonical per-ray visit counts on the binary LBVH (roofline algorithmic bytes)
-    stats = torch.zeros(4, dtype=torch.int64, device=dev)
-    base = tree.raycast(rays_d, capi.QK_ORDER_MORTON, stats=stats).clone()
-    s = stats.cpu().numpy()
-    node_tests, tri_tests, overflows = int(s[0]), int(s[1]), int(s[2])
-    if overflows:
-        raise RuntimeError(f"{overflows} rays overflowed the traversal stack")
-    p_int = (node_tests - tri_tests) / nrays
-    p_leaf = tri_tests / nrays
-    bytes_per_ray = 40.0 + 96.0 * p_int + (32.0 + 36.0) * p_leaf
-
+    base = trees["lbvh"].raycast(rays_d, 0).clone()
     # every variant must give the same bits
-    for name, flags in variants.items():
-        got = tree.raycast(rays_d, flags)
+    for name, (b, flags) in variants.items():
+        got = trees[b].raycast(rays_d, flags)
         if not torch.equal(got, base):
-            raise RuntimeError(f"variant {name} differs from the binary Morton results")
+            raise RuntimeError(f"variant {name} differs from the LBVH binary results")
 
-    def time_variant(flags, steps, warmup):
+    def time_variant(tree, flags, steps, warmup):
         out = torch.empty(nrays, dtype=torch.int64, device=dev)
         ws = torch.empty(capi.lib().qk_query_workspace_bytes(nrays, flags), dtype=torch.uint8,
                          device=dev)
@@ -295,17 +291,28 @@ def main():
         return [e0.elapsed_time(e1) for e0, e1 in ev]
 
     results = {}
-    for name, flags in variants.items():
-        t = time_variant(flags, 10, 3)
-        results[name] = float(np.median(t))
+    for name, (b, flags) in variants.items():
+        results[name] = float(np.median(time_variant(trees[b], flags, 10, 3)))
     best = min(results, key=results.get)
-    best_flags = variants[best]
+    best_builder, best_flags = variants[best]
+    tree = trees[best_builder]
+
+    # canonical per-ray visit counts: binary traversal of the timed tree (roofline bytes)
+    stats = torch.zeros(4, dtype=torch.int64, device=dev)
+    tree.raycast(rays_d, 0, stats=stats)
+    s = stats.cpu().numpy()
+    node_tests, tri_tests, overflows = int(s[0]), int(s[1]), int(s[2])
+    if overflows:
+        raise RuntimeError(f"{overflows} rays overflowed the traversal stack")
+    p_int = (node_tests - tri_tests) / nrays
+    p_leaf = tri_tests / nrays
+    bytes_per_ray = 40.0 + 96.0 * p_int + (32.0 + 36.0) * p_leaf
 
     # ---- the timed steps of the headline variant ----
     barrier(world)
     torch.cuda.synchronize()
     with Clocks(local) as clk:
-        step_ms = time_variant(best_flags, args.steps, args.warmup)
+        step_ms = time_variant(tree, best_flags, args.steps, args.warmup)
     clocks = clk.summary()
     ms = float(np.sum(step_ms)) / args.steps
     ms = max_over_ranks(world, ms)
@@ -362,6 +369,7 @@ def main():
                 "unit": "GB/s", "frac": round(achieved / pk["hbm_gbs"], 4),
                 "traffic": traffic, "peak_kind": pk_kind,
                 "kernel": "k_ray_wide" if trav_flags & capi.QK_WIDE else "k_ray_bin",
+                "tree": best_builder,
                 "kernel_ms": round(kernel_ms, 4),
                 "bytes_per_ray": round(bytes_per_ray, 1),
                 "canonical_counts": {"node_tests_per_ray": round(node_tests / nrays, 3),
@@ -433,11 +441,11 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded generators, identical bytes on every host)",
-            "config": {**desc, "builder": "lbvh", "variant": best,
+            "config": {**desc, "builder": best_builder, "sah_bins": 32, "variant": best,
                        "l2": "flushed (256 MB write) between timed steps",
                        "parallelism": f"replica x{world}, rays sharded per rank"},
             "variants_ms": {k: round(v, 4) for k, v in results.items()},
-            "build_ms": round(build_ms, 3),
+            "build_ms": {k: round(v, 3) for k, v in build_ms.items()},
             "knn": {"k": 8, "queries": int(q_d.shape[0]), "ms": round(knn_ms, 4),
                     "mqueries_per_s": round(q_d.shape[0] / (knn_ms * 1e-3) / 1e6, 2)},
             "fingerprint": f"0x{fp:016x}", "hits": int(hits), "parity": parity,

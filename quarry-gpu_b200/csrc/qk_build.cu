@@ -14,6 +14,7 @@
 //      boxes equal the reference's level-by-level refit bit for bit.  The same pass writes
 //      the 64-byte traversal node (both child boxes inline).
 //   6. depth of every node by walking its parent chain; the maximum is read back once.
+#include <algorithm>
 #include <cstdio>
 
 #include "qk_internal.cuh"
@@ -541,6 +542,27 @@ __global__ __launch_bounds__(kBlock) void k_check_wide(const Node* __restrict__ 
     if (bad) atomicAdd(&err[6], 1);
 }
 
+// Boxes (bottom-up), traversal nodes and depths of a tree whose links and leaves are set;
+// shared by the LBVH and SAH builders.  Reads the maximum depth back (syncs).
+int finish_tree(qk_tree* t, Header* h, cudaStream_t s) {
+    const int n = t->n;
+    k_bottom_up<<<blocks_for(n), kBlock, 0, s>>>(static_cast<Node*>(t->nodes),
+                                                 static_cast<BNode*>(t->bnodes), t->parent,
+                                                 t->flags, n);
+    cudaMemsetAsync(&h->max_depth, 0, sizeof(int), s);
+    k_depth<<<blocks_for(2 * n - 1), kBlock, 0, s>>>(t->parent, 2 * n - 1, t->depth_arr, h);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_status(e, "tree boxes");
+    int depth = 0;
+    e = cudaMemcpyAsync(&depth, &h->max_depth, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_status(e, "build depth readback");
+    t->depth = depth;
+    t->wide_count = 0;
+    if (depth >= kStack) return fail(QK_ERR_DEPTH, "tree depth %d exceeds %d", depth, kStack - 1);
+    return QK_OK;
+}
+
 template <class Ops>
 int build_lbvh(qk_tree* t, const void* items_v, void* ws, cudaStream_t s) {
     const int n = t->n;
@@ -565,18 +587,9 @@ int build_lbvh(qk_tree* t, const void* items_v, void* ws, cudaStream_t s) {
                                                   static_cast<float*>(t->items), t->prim_ids,
                                                   t->slot_of, t->parent, bn,
                                                   static_cast<float4*>(t->leaves), t->flags);
-    k_bottom_up<<<blocks_for(n), kBlock, 0, s>>>(nodes, bn, t->parent, t->flags, n);
-    k_depth<<<blocks_for(2 * n - 1), kBlock, 0, s>>>(t->parent, 2 * n - 1, t->depth_arr, h);
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_status(e, "build kernels");
-    int depth = 0;
-    e = cudaMemcpyAsync(&depth, &h->max_depth, sizeof(int), cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) return cuda_status(e, "build depth readback");
-    t->depth = depth;
-    t->wide_count = 0;
-    if (depth >= kStack) return fail(QK_ERR_DEPTH, "tree depth %d exceeds %d", depth, kStack - 1);
-    return QK_OK;
+    return finish_tree(t, h, s);
 }
 
 template <class Ops>
@@ -649,7 +662,6 @@ int validate_impl(const qk_tree* t, const void* items, int* err, void* ws, cudaS
 
 size_t build_ws_bytes(int kind, int n, int builder) {
     (void)kind;
-    (void)builder;
     Carve c;
     c.take<Header>(1);
     c.take<uint32_t>(n);
@@ -666,14 +678,19 @@ size_t build_ws_bytes(int kind, int n, int builder) {
     Carve w;
     w.take<char>(scan_ws_bytes(n));
     if (w.used > need) need = w.used;
+    if (builder == QK_BUILD_SAH) need = std::max(need, sah_ws_bytes(n));
     return need;
 }
 
 int build_tree(qk_tree* t, int builder, int bins, const void* items, void* ws, size_t ws_bytes,
                cudaStream_t s) {
-    (void)bins;
     (void)ws_bytes;
-    if (builder != QK_BUILD_LBVH) return fail(QK_ERR_INVALID, "builder %d not available", builder);
+    if (builder == QK_BUILD_SAH) {
+        cudaMemsetAsync(t->flags, 0, sizeof(int) * static_cast<size_t>(t->n - 1), s);
+        const int st = build_sah(t, bins, items, ws, s);
+        if (st != QK_OK) return st;
+        return finish_tree(t, static_cast<Header*>(ws), s);
+    }
     switch (t->kind) {
         case kTri: return build_lbvh<TriOps>(t, items, ws, s);
         case kPoint: return build_lbvh<PointOps>(t, items, ws, s);

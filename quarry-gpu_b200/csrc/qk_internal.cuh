@@ -77,6 +77,9 @@ cudaError_t scan_exclusive(const int* in, int* out, int n, bool write_total, voi
 size_t build_ws_bytes(int kind, int n, int builder);
 int build_tree(qk_tree* t, int builder, int bins, const void* items, void* ws, size_t ws_bytes,
                cudaStream_t s);
+// SAH topology (qk_sah.cu): fills links, parents, order-derived leaves; boxes come after
+size_t sah_ws_bytes(int n);
+int build_sah(qk_tree* t, int bins, const void* items, void* ws, cudaStream_t s);
 int refit_tree(qk_tree* t, const void* items, cudaStream_t s);
 int refit_tree_dirty(qk_tree* t, const int* ids, const void* items, int count, void* ws,
                      cudaStream_t s);

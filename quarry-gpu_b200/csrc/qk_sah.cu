@@ -1,0 +1,980 @@
+// qk_sah.cu -- top-down binned SAH builder (the reference's buildBVHSahGPU,
+// src/gpu/lbvh.cu:827-1291 and 1777-2135), organised for B200.
+//
+// The output keeps the LBVH numbering (internal nodes 0..n-2, leaf of slot s at n-1+s), so
+// boxes, traversal nodes, 4-wide collapse, refit and validation are shared with the LBVH.
+// Three tiers, all deterministic (commutative atomics for bins, stable partitions, node ids
+// from prefix sums or from sequential per-subtree counters):
+//   global   ranges of more than kBlockRange primitives, level by level: chunks of 4096
+//            primitives bin their centroids in shared memory (count + primitive box per bin,
+//            3 axes) and merge into per-range bins with ordered-uint atomics; one thread per
+//            range sweeps the bins for the cheapest area(L)*nL + area(R)*nR split; a stable
+//            partition by chunk-local block scans writes the new order.  Two host syncs per
+//            level.
+//   block    every range of at most kBlockRange primitives is handed to one thread block that
+//            gathers its centroids and boxes into shared memory and splits it with the same
+//            binned sweep until pieces reach 32 primitives; no global synchronisation.
+//   warp     pieces of at most 32 primitives are finished by one warp each with an exact
+//            sweep: for every axis the lanes sort by centroid (bitonic, ties by position), scan
+//            prefix and suffix boxes, and evaluate every split position.
+// Depth stays below the 64-entry traversal stacks: a split is only taken while
+// depth + ceil(log2(larger child)) <= kMaxDepth, otherwise the range is halved by count.
+#include "qk_internal.cuh"
+
+namespace qk {
+
+namespace {
+
+constexpr int kChunk = 4096;       // primitives binned per block at the global tier
+constexpr int kBlockRange = 1024;  // largest range built by one block
+constexpr int kWarpRange = 32;     // largest range finished by one warp
+constexpr int kMaxBins = 64;
+constexpr int kMaxDepth = 62;
+constexpr int kBinWords = 7;       // count, lo xyz, hi xyz
+
+struct Task {
+    int begin, end, node, depth;
+};
+
+__device__ __forceinline__ int ceil_log2(int c) { return c <= 1 ? 0 : 32 - __clz(c - 1); }
+
+__device__ __forceinline__ float half_area(float3 lo, float3 hi) {
+    const float dx = hi.x - lo.x, dy = hi.y - lo.y, dz = hi.z - lo.z;
+    return dx * dy + dy * dz + dz * dx;
+}
+
+__device__ __forceinline__ int bin_of(float c, float lo, float hi, int bins) {
+    const float ext = hi - lo;
+    if (!(ext > 0.0f)) return 0;
+    int b = __float2int_rd((c - lo) * (static_cast<float>(bins) / ext));
+    return b < 0 ? 0 : (b >= bins ? bins - 1 : b);
+}
+
+// child reference as the traversal nodes store it
+__device__ __forceinline__ int child_ref(int id, int n) { return id >= n - 1 ? ~(id - (n - 1)) : id; }
+
+__device__ __forceinline__ void link(Node* nodes, BNode* bn, int* parent, int node, int l, int r,
+                                     int n) {
+    nodes[node].left = l;
+    nodes[node].right = r;
+    parent[l] = node;
+    parent[r] = node;
+    bn[node].v3 = make_float4(__int_as_float(child_ref(l, n)), __int_as_float(child_ref(r, n)),
+                              0.0f, 0.0f);
+}
+
+// centroid and box of every primitive, in scene order
+template <class Ops>
+__global__ __launch_bounds__(kBlock) void k_prim_geom(const float* __restrict__ items, int n,
+                                                     float4* __restrict__ cen,
+                                                     float4* __restrict__ lo,
+                                                     float4* __restrict__ hi,
+                                                     int* __restrict__ order) {
+    const int i = blockIdx.x * kBlock + threadIdx.x;
+    if (i >= n) return;
+    const float* it = items + static_cast<size_t>(i) * Ops::kFloats;
+    const float3 c = Ops::centroid(it);
+    const Box b = Ops::bounds(it);
+    cen[i] = make_float4(c.x, c.y, c.z, 0.0f);
+    lo[i] = make_float4(b.lo.x, b.lo.y, b.lo.z, 0.0f);
+    hi[i] = make_float4(b.hi.x, b.hi.y, b.hi.z, 0.0f);
+    order[i] = i;
+}
+
+// ---------------------------------------------------------------------------------------
+// global tier
+// ---------------------------------------------------------------------------------------
+struct Level {
+    Task* tasks;        // current big tasks
+    int* chunk_task;    // chunk -> task
+    int* chunk_begin;
+    int* chunk_first;   // first chunk of each task
+    unsigned* cb;       // per task: centroid bounds lo xyz, hi xyz (ordered)
+    unsigned* bins;     // per task: 3 * bins * kBinWords
+    int* split;         // per task: axis * 256 + bin (-1 = count split)
+    int* left_count;    // per task
+    int* chunk_left;    // per chunk: left primitives, then exclusive prefix inside the task
+    int* counters;      // [0] chunks, [1] next big tasks, [2] block tasks, [3] internal base
+};
+
+// single block: chunk list of the current tasks, bin reset
+__global__ __launch_bounds__(1024) void k_level_prep(Level L, int ntask, int bins) {
+    __shared__ int carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int base = 0; base < ntask; base += 1024) {
+        const int t = base + threadIdx.x;
+        int nch = 0;
+        if (t < ntask) nch = (L.tasks[t].end - L.tasks[t].begin + kChunk - 1) / kChunk;
+        // block exclusive scan of nch (warp shuffles + shared totals)
+        __shared__ int wsum[32];
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        int v = nch;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane >= o) v += y;
+        }
+        if (lane == 31) wsum[warp] = v;
+        __syncthreads();
+        if (warp == 0) {
+            int s = wsum[lane];
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, s, o);
+                if (lane >= o) s += y;
+            }
+            wsum[lane] = s;
+        }
+        __syncthreads();
+        const int excl = carry + (warp ? wsum[warp - 1] : 0) + v - nch;
+        if (t < ntask) {
+            L.chunk_first[t] = excl;
+            for (int c = 0; c < nch; ++c) {
+                L.chunk_task[excl + c] = t;
+                L.chunk_begin[excl + c] = L.tasks[t].begin + c * kChunk;
+            }
+            for (int a = 0; a < 3; ++a) {
+                L.cb[6 * t + a] = ord_f(kInf);
+                L.cb[6 * t + 3 + a] = ord_f(-kInf);
+            }
+            unsigned* B = L.bins + static_cast<size_t>(t) * 3 * kMaxBins * kBinWords;
+            for (int j = 0; j < 3 * bins; ++j) {
+                B[j * kBinWords] = 0u;
+                for (int k = 0; k < 3; ++k) {
+                    B[j * kBinWords + 1 + k] = ord_f(kInf);
+                    B[j * kBinWords + 4 + k] = ord_f(-kInf);
+                }
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 1023) carry = excl + nch;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) L.counters[0] = carry;
+}
+
+__global__ __launch_bounds__(kBlock) void k_level_cbounds(Level L, const int* __restrict__ order,
+                                                         const float4* __restrict__ cen) {
+    const int c = blockIdx.x;
+    const int t = L.chunk_task[c];
+    const int b = L.chunk_begin[c];
+    const int e = min(b + kChunk, L.tasks[t].end);
+    float lo[3] = {kInf, kInf, kInf}, hi[3] = {-kInf, -kInf, -kInf};
+    for (int i = b + threadIdx.x; i < e; i += kBlock) {
+        const float4 p = cen[order[i]];
+        lo[0] = fminf(lo[0], p.x);
+        lo[1] = fminf(lo[1], p.y);
+        lo[2] = fminf(lo[2], p.z);
+        hi[0] = fmaxf(hi[0], p.x);
+        hi[1] = fmaxf(hi[1], p.y);
+        hi[2] = fmaxf(hi[2], p.z);
+    }
+    for (int a = 0; a < 3; ++a) {
+        for (int o = 16; o > 0; o >>= 1) {
+            lo[a] = fminf(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], o));
+            hi[a] = fmaxf(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], o));
+        }
+    }
+    if ((threadIdx.x & 31) == 0) {
+        for (int a = 0; a < 3; ++a) {
+            atomicMin(&L.cb[6 * t + a], ord_f(lo[a]));
+            atomicMax(&L.cb[6 * t + 3 + a], ord_f(hi[a]));
+        }
+    }
+}
+
+__global__ __launch_bounds__(kBlock) void k_level_bins(Level L, const int* __restrict__ order,
+                                                      const float4* __restrict__ cen,
+                                                      const float4* __restrict__ plo,
+                                                      const float4* __restrict__ phi, int bins) {
+    __shared__ unsigned sb[3 * kMaxBins * kBinWords];
+    for (int j = threadIdx.x; j < 3 * bins * kBinWords; j += kBlock) {
+        const int w = j % kBinWords;
+        sb[j] = w == 0 ? 0u : (w <= 3 ? ord_f(kInf) : ord_f(-kInf));
+    }
+    __syncthreads();
+    const int c = blockIdx.x;
+    const int t = L.chunk_task[c];
+    const int b = L.chunk_begin[c];
+    const int e = min(b + kChunk, L.tasks[t].end);
+    float clo[3], chi[3];
+    for (int a = 0; a < 3; ++a) {
+        clo[a] = unord_f(L.cb[6 * t + a]);
+        chi[a] = unord_f(L.cb[6 * t + 3 + a]);
+    }
+    for (int i = b + threadIdx.x; i < e; i += kBlock) {
+        const int p = order[i];
+        const float4 cc = cen[p], lo = plo[p], hi = phi[p];
+        const float cv[3] = {cc.x, cc.y, cc.z};
+        for (int a = 0; a < 3; ++a) {
+            unsigned* w = sb + (a * bins + bin_of(cv[a], clo[a], chi[a], bins)) * kBinWords;
+            atomicAdd(&w[0], 1u);
+            atomicMin(&w[1], ord_f(lo.x));
+            atomicMin(&w[2], ord_f(lo.y));
+            atomicMin(&w[3], ord_f(lo.z));
+            atomicMax(&w[4], ord_f(hi.x));
+            atomicMax(&w[5], ord_f(hi.y));
+            atomicMax(&w[6], ord_f(hi.z));
+        }
+    }
+    __syncthreads();
+    unsigned* B = L.bins + static_cast<size_t>(t) * 3 * kMaxBins * kBinWords;
+    for (int j = threadIdx.x; j < 3 * bins * kBinWords; j += kBlock) {
+        const int w = j % kBinWords;
+        if (w == 0) {
+            if (sb[j]) atomicAdd(&B[j], sb[j]);
+        } else if (w <= 3) {
+            atomicMin(&B[j], sb[j]);
+        } else {
+            atomicMax(&B[j], sb[j]);
+        }
+    }
+}
+
+// Sweep 3 x (bins - 1) candidate planes of one range given its bins (ordered-uint words).
+// Returns the chosen (axis, first right bin) as axis * 256 + bin and the left count, or -1
+// when no plane separates the centroids.
+__device__ int sweep_bins(const unsigned* B, int bins, int count, int* left_out) {
+    float best = kInf;
+    int best_split = -1, best_left = 0;
+    for (int a = 0; a < 3; ++a) {
+        // suffix boxes from the right
+        float3 slo[kMaxBins], shi[kMaxBins];
+        float3 rlo = f3(kInf, kInf, kInf), rhi = f3(-kInf, -kInf, -kInf);
+        for (int b = bins - 1; b >= 0; --b) {
+            const unsigned* w = B + (a * bins + b) * kBinWords;
+            if (w[0]) {
+                rlo = f3(fminf(rlo.x, unord_f(w[1])), fminf(rlo.y, unord_f(w[2])), fminf(rlo.z, unord_f(w[3])));
+                rhi = f3(fmaxf(rhi.x, unord_f(w[4])), fmaxf(rhi.y, unord_f(w[5])), fmaxf(rhi.z, unord_f(w[6])));
+            }
+            slo[b] = rlo;
+            shi[b] = rhi;
+        }
+        float3 llo = f3(kInf, kInf, kInf), lhi = f3(-kInf, -kInf, -kInf);
+        int lc = 0;
+        for (int b = 0; b < bins - 1; ++b) {
+            const unsigned* w = B + (a * bins + b) * kBinWords;
+            lc += static_cast<int>(w[0]);
+            if (w[0]) {
+                llo = f3(fminf(llo.x, unord_f(w[1])), fminf(llo.y, unord_f(w[2])), fminf(llo.z, unord_f(w[3])));
+                lhi = f3(fmaxf(lhi.x, unord_f(w[4])), fmaxf(lhi.y, unord_f(w[5])), fmaxf(lhi.z, unord_f(w[6])));
+            }
+            if (lc == 0 || lc == count) continue;
+            const float cost = half_area(llo, lhi) * static_cast<float>(lc) +
+                               half_area(slo[b + 1], shi[b + 1]) * static_cast<float>(count - lc);
+            if (cost < best) {
+                best = cost;
+                best_split = a * 256 + (b + 1);
+                best_left = lc;
+            }
+        }
+    }
+    *left_out = best_left;
+    return best_split;
+}
+
+__global__ __launch_bounds__(kBlock) void k_level_split(Level L, int ntask, int bins) {
+    const int t = blockIdx.x * kBlock + threadIdx.x;
+    if (t >= ntask) return;
+    const Task tk = L.tasks[t];
+    const int count = tk.end - tk.begin;
+    int lc = 0;
+    int s = sweep_bins(L.bins + static_cast<size_t>(t) * 3 * kMaxBins * kBinWords, bins, count, &lc);
+    if (s >= 0 && tk.depth + 1 + ceil_log2(max(lc, count - lc)) > kMaxDepth) s = -1;
+    if (s < 0) lc = count / 2;
+    L.split[t] = s;
+    L.left_count[t] = lc;
+}
+
+__device__ __forceinline__ bool goes_left(int split, int pos, int begin, int lc, float4 c,
+                                          const unsigned* cb, int bins) {
+    if (split < 0) return pos - begin < lc;
+    const int a = split >> 8;
+    const float v = a == 0 ? c.x : (a == 1 ? c.y : c.z);
+    return bin_of(v, unord_f(cb[a]), unord_f(cb[3 + a]), bins) < (split & 255);
+}
+
+// per chunk: count the primitives that go left
+__global__ __launch_bounds__(kBlock) void k_level_count_left(Level L, const int* __restrict__ order,
+                                                            const float4* __restrict__ cen,
+                                                            int bins) {
+    const int c = blockIdx.x;
+    const int t = L.chunk_task[c];
+    const Task tk = L.tasks[t];
+    const int b = L.chunk_begin[c];
+    const int e = min(b + kChunk, tk.end);
+    const int split = L.split[t], lc = L.left_count[t];
+    int cnt = 0;
+    for (int i = b + threadIdx.x; i < e; i += kBlock) {
+        cnt += goes_left(split, i, tk.begin, lc, cen[order[i]], L.cb + 6 * t, bins) ? 1 : 0;
+    }
+    cnt = __reduce_add_sync(0xffffffffu, cnt);
+    __shared__ int ws[kBlock / 32];
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = cnt;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int s = 0;
+        for (int w = 0; w < kBlock / 32; ++w) s += ws[w];
+        L.chunk_left[c] = s;
+    }
+}
+
+// per task: exclusive prefix of the chunk counts inside the task
+__global__ __launch_bounds__(kBlock) void k_level_prefix_left(Level L, int ntask) {
+    const int t = blockIdx.x * kBlock + threadIdx.x;
+    if (t >= ntask) return;
+    const int first = L.chunk_first[t];
+    const int nch = (L.tasks[t].end - L.tasks[t].begin + kChunk - 1) / kChunk;
+    int run = 0;
+    for (int c = 0; c < nch; ++c) {
+        const int v = L.chunk_left[first + c];
+        L.chunk_left[first + c] = run;
+        run += v;
+    }
+}
+
+// stable partition of each chunk into `out` (left block first, then right block)
+__global__ __launch_bounds__(kBlock) void k_level_partition(Level L, const int* __restrict__ order,
+                                                           int* __restrict__ out,
+                                                           const float4* __restrict__ cen,
+                                                           int bins) {
+    const int c = blockIdx.x;
+    const int t = L.chunk_task[c];
+    const Task tk = L.tasks[t];
+    const int b = L.chunk_begin[c];
+    const int e = min(b + kChunk, tk.end);
+    const int split = L.split[t], lc = L.left_count[t];
+    const int left_before = L.chunk_left[c];        // lefts in earlier chunks of this task
+    const int right_before = (b - tk.begin) - left_before;
+    __shared__ int wsum[kBlock / 32];
+    __shared__ int carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int base = b; base < e; base += kBlock) {
+        const int i = base + threadIdx.x;
+        int p = 0;
+        int f = 0;
+        if (i < e) {
+            p = order[i];
+            f = goes_left(split, i, tk.begin, lc, cen[p], L.cb + 6 * t, bins) ? 1 : 0;
+        }
+        int v = f;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane >= o) v += y;
+        }
+        if (lane == 31) wsum[warp] = v;
+        __syncthreads();
+        int wpre = 0, tot = 0;
+        for (int w = 0; w < kBlock / 32; ++w) {
+            if (w < warp) wpre += wsum[w];
+            tot += wsum[w];
+        }
+        const int lrank = carry + wpre + v - f;  // lefts before i inside this chunk
+        if (i < e) {
+            const int dst = f ? tk.begin + left_before + lrank
+                              : tk.begin + lc + right_before + (i - b - lrank);
+            out[dst] = p;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) carry += tot;
+        __syncthreads();
+    }
+}
+
+__global__ __launch_bounds__(kBlock) void k_level_copy(Level L, const int* __restrict__ src,
+                                                      int* __restrict__ dst) {
+    const int c = blockIdx.x;
+    const int t = L.chunk_task[c];
+    const int b = L.chunk_begin[c];
+    const int e = min(b + kChunk, L.tasks[t].end);
+    for (int i = b + threadIdx.x; i < e; i += kBlock) dst[i] = src[i];
+}
+
+// single block: node ids for the children (prefix sums over tasks), next big tasks and the
+// block-tier list
+__global__ __launch_bounds__(1024) void k_level_assign(Level L, int ntask, Task* __restrict__ next,
+                                                      Task* __restrict__ blocks, Node* nodes,
+                                                      BNode* bn, int* parent, int n) {
+    __shared__ int carry[3];
+    __shared__ int wsum[3][32];
+    if (threadIdx.x < 3) carry[threadIdx.x] = 0;
+    __syncthreads();
+    const int base_id = L.counters[3];
+    const int base_big = L.counters[1];
+    const int base_blk = L.counters[2];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int base = 0; base < ntask; base += 1024) {
+        const int t = base + threadIdx.x;
+        int lc = 0, rc = 0;
+        Task tk{0, 0, 0, 0};
+        if (t < ntask) {
+            tk = L.tasks[t];
+            lc = L.left_count[t];
+            rc = tk.end - tk.begin - lc;
+        }
+        int cnt[3];
+        cnt[0] = t < ntask ? (lc >= 2) + (rc >= 2) : 0;                           // internal ids
+        cnt[1] = t < ntask ? (lc > kBlockRange) + (rc > kBlockRange) : 0;         // big tasks
+        cnt[2] = t < ntask ? (lc >= 2 && lc <= kBlockRange) + (rc >= 2 && rc <= kBlockRange) : 0;
+        int ex[3];
+        for (int k = 0; k < 3; ++k) {
+            int v = cnt[k];
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, v, o);
+                if (lane >= o) v += y;
+            }
+            if (lane == 31) wsum[k][warp] = v;
+            ex[k] = v - cnt[k];
+        }
+        __syncthreads();
+        if (warp == 0) {
+            for (int k = 0; k < 3; ++k) {
+                int s = wsum[k][lane];
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int y = __shfl_up_sync(0xffffffffu, s, o);
+                    if (lane >= o) s += y;
+                }
+                wsum[k][lane] = s;
+            }
+        }
+        __syncthreads();
+        for (int k = 0; k < 3; ++k) ex[k] += carry[k] + (warp ? wsum[k][warp - 1] : 0);
+        if (t < ntask) {
+            const int lid = lc >= 2 ? base_id + ex[0] : n - 1 + tk.begin;
+            const int rid = rc >= 2 ? base_id + ex[0] + (lc >= 2) : n - 1 + tk.begin + lc;
+            link(nodes, bn, parent, tk.node, lid, rid, n);
+            int bi = base_big + ex[1], ki = base_blk + ex[2];
+            if (lc > kBlockRange) next[bi++] = Task{tk.begin, tk.begin + lc, lid, tk.depth + 1};
+            else if (lc >= 2) blocks[ki++] = Task{tk.begin, tk.begin + lc, lid, tk.depth + 1};
+            if (rc > kBlockRange) next[bi] = Task{tk.begin + lc, tk.end, rid, tk.depth + 1};
+            else if (rc >= 2) blocks[ki] = Task{tk.begin + lc, tk.end, rid, tk.depth + 1};
+        }
+        __syncthreads();
+        if (threadIdx.x == 1023) {
+            for (int k = 0; k < 3; ++k) carry[k] = ex[k] + cnt[k];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        L.counters[3] = base_id + carry[0];
+        L.counters[1] = base_big + carry[1];
+        L.counters[2] = base_blk + carry[2];
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// block tier: one block builds the subtree of one range of <= kBlockRange primitives.
+// Centroids and boxes stay at their load index in shared memory; splits permute `perm`
+// (position -> load index) only.
+// ---------------------------------------------------------------------------------------
+struct Piece {
+    int begin, count, node, depth, ids;  // ids: first reserved node id (warp pieces)
+};
+
+constexpr int kPieceCap = 128;  // block pieces pending (DFS: at most depth + 1)
+
+// Warp-level exact SAH over <= 32 primitives at positions [b, b + c) of the block's range.
+__device__ void warp_build(int* perm, const float4* sc, const float4* slo, const float4* shi,
+                           int b, int c, int node, int depth, int next_id, Node* nodes, BNode* bn,
+                           int* parent, int n, int gbase) {
+    const int lane = threadIdx.x & 31;
+    int stk_b[kWarpRange], stk_c[kWarpRange], stk_n[kWarpRange], stk_d[kWarpRange];
+    int top = 0;
+    stk_b[0] = b;
+    stk_c[0] = c;
+    stk_n[0] = node;
+    stk_d[0] = depth;
+    top = 1;
+    int guard = 0;
+    while (top > 0 && guard++ < 4 * kWarpRange) {
+        --top;
+        const int rb = stk_b[top], rc = stk_c[top], rn = stk_n[top], rd = stk_d[top];
+        const bool mine = lane < rc;
+        const int li = perm[rb + (mine ? lane : 0)];
+        const float4 cc = sc[li], lo = slo[li], hi = shi[li];
+        float best = kInf;
+        int best_axis = -1, best_k = rc / 2;
+        int rank_axis[3] = {lane, lane, lane};
+        for (int a = 0; a < 3; ++a) {
+            const float key = mine ? (a == 0 ? cc.x : (a == 1 ? cc.y : cc.z)) : kInf;
+            int rank = 0;
+            for (int j = 0; j < kWarpRange; ++j) {
+                const float kj = __shfl_sync(0xffffffffu, key, j);
+                if (j < rc && (kj < key || (kj == key && j < lane))) ++rank;
+            }
+            rank = mine ? rank : lane;
+            rank_axis[a] = rank;
+            // lane r takes the boxes of the item ranked r
+            int src = lane;
+            for (int j = 0; j < kWarpRange; ++j) {
+                const int rj = __shfl_sync(0xffffffffu, rank, j);
+                if (j < rc && rj == lane) src = j;
+            }
+            float3 blo = f3(__shfl_sync(0xffffffffu, lo.x, src), __shfl_sync(0xffffffffu, lo.y, src),
+                            __shfl_sync(0xffffffffu, lo.z, src));
+            float3 bhi = f3(__shfl_sync(0xffffffffu, hi.x, src), __shfl_sync(0xffffffffu, hi.y, src),
+                            __shfl_sync(0xffffffffu, hi.z, src));
+            if (lane >= rc) {
+                blo = f3(kInf, kInf, kInf);
+                bhi = f3(-kInf, -kInf, -kInf);
+            }
+            float3 plo = blo, phi = bhi, qlo = blo, qhi = bhi;
+            for (int o = 1; o < 32; o <<= 1) {
+                const float3 ulo = f3(__shfl_up_sync(0xffffffffu, plo.x, o), __shfl_up_sync(0xffffffffu, plo.y, o), __shfl_up_sync(0xffffffffu, plo.z, o));
+                const float3 uhi = f3(__shfl_up_sync(0xffffffffu, phi.x, o), __shfl_up_sync(0xffffffffu, phi.y, o), __shfl_up_sync(0xffffffffu, phi.z, o));
+                const float3 dlo = f3(__shfl_down_sync(0xffffffffu, qlo.x, o), __shfl_down_sync(0xffffffffu, qlo.y, o), __shfl_down_sync(0xffffffffu, qlo.z, o));
+                const float3 dhi = f3(__shfl_down_sync(0xffffffffu, qhi.x, o), __shfl_down_sync(0xffffffffu, qhi.y, o), __shfl_down_sync(0xffffffffu, qhi.z, o));
+                if (lane >= o) {
+                    plo = f3(fminf(plo.x, ulo.x), fminf(plo.y, ulo.y), fminf(plo.z, ulo.z));
+                    phi = f3(fmaxf(phi.x, uhi.x), fmaxf(phi.y, uhi.y), fmaxf(phi.z, uhi.z));
+                }
+                if (lane + o < 32) {
+                    qlo = f3(fminf(qlo.x, dlo.x), fminf(qlo.y, dlo.y), fminf(qlo.z, dlo.z));
+                    qhi = f3(fmaxf(qhi.x, dhi.x), fmaxf(qhi.y, dhi.y), fmaxf(qhi.z, dhi.z));
+                }
+            }
+            // split after sorted item `lane`: left [0, lane], right [lane + 1, rc)
+            const float3 rlo = f3(__shfl_down_sync(0xffffffffu, qlo.x, 1), __shfl_down_sync(0xffffffffu, qlo.y, 1), __shfl_down_sync(0xffffffffu, qlo.z, 1));
+            const float3 rhi = f3(__shfl_down_sync(0xffffffffu, qhi.x, 1), __shfl_down_sync(0xffffffffu, qhi.y, 1), __shfl_down_sync(0xffffffffu, qhi.z, 1));
+            const int kl = lane + 1;
+            float cost = kInf;
+            if (kl < rc && rd + 1 + ceil_log2(max(kl, rc - kl)) <= kMaxDepth) {
+                cost = half_area(plo, phi) * static_cast<float>(kl) +
+                       half_area(rlo, rhi) * static_cast<float>(rc - kl);
+            }
+            float bc = cost;
+            int bk = kl;
+            for (int o = 16; o > 0; o >>= 1) {
+                const float oc = __shfl_xor_sync(0xffffffffu, bc, o);
+                const int ok = __shfl_xor_sync(0xffffffffu, bk, o);
+                if (oc < bc || (oc == bc && ok < bk)) {
+                    bc = oc;
+                    bk = ok;
+                }
+            }
+            if (bc < best) {
+                best = bc;
+                best_axis = a;
+                best_k = bk;
+            }
+        }
+        // reorder the range by the chosen axis; with no finite cost halve the x order
+        const int r = rank_axis[best_axis < 0 ? 0 : best_axis];
+        __syncwarp();
+        if (mine) perm[rb + r] = li;
+        __syncwarp();
+        const int kl = best_k, kr = rc - best_k;
+        const int lid = kl >= 2 ? next_id++ : n - 1 + gbase + rb;
+        const int rid = kr >= 2 ? next_id++ : n - 1 + gbase + rb + kl;
+        if (lane == 0) link(nodes, bn, parent, rn, lid, rid, n);
+        if (kr >= 2 && top < kWarpRange) {
+            stk_b[top] = rb + kl;
+            stk_c[top] = kr;
+            stk_n[top] = rid;
+            stk_d[top] = rd + 1;
+            ++top;
+        }
+        if (kl >= 2 && top < kWarpRange) {
+            stk_b[top] = rb;
+            stk_c[top] = kl;
+            stk_n[top] = lid;
+            stk_d[top] = rd + 1;
+            ++top;
+        }
+        __syncwarp();
+    }
+}
+
+__global__ __launch_bounds__(kBlock) void k_block_build(const Task* __restrict__ tasks, int ntask,
+                                                       const int* __restrict__ id_base,
+                                                       int* __restrict__ order,
+                                                       const float4* __restrict__ cen,
+                                                       const float4* __restrict__ plo,
+                                                       const float4* __restrict__ phi, Node* nodes,
+                                                       BNode* bn, int* parent, int n, int bins,
+                                                       int* __restrict__ err) {
+    extern __shared__ float4 smem[];
+    float4* sc = smem;                                      // centroids   [kBlockRange]
+    float4* slo = sc + kBlockRange;                         // box lo      [kBlockRange]
+    float4* shi = slo + kBlockRange;                        // box hi      [kBlockRange]
+    int* perm = reinterpret_cast<int*>(shi + kBlockRange);  // position -> load index
+    int* tmp = perm + kBlockRange;                          // partition scratch
+    int* sid = tmp + kBlockRange;                           // load index -> scene index
+    __shared__ unsigned sb[3 * kMaxBins * kBinWords];
+    __shared__ Piece pieces[kPieceCap];
+    __shared__ Piece wpieces[kBlockRange / 2];
+    __shared__ int npieces, nw, next_id, wsum[kBlock / 32];
+    __shared__ unsigned sbu[6];
+    __shared__ float sbf[6];
+    __shared__ int s_split, s_left;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+
+    for (int ti = blockIdx.x; ti < ntask; ti += gridDim.x) {
+        const Task tk = tasks[ti];
+        const int count = tk.end - tk.begin;
+        if (count < 2 || count > kBlockRange) {
+            if (threadIdx.x == 0) atomicAdd(err, 1);
+            continue;
+        }
+        for (int i = threadIdx.x; i < count; i += kBlock) {
+            const int p = order[tk.begin + i];
+            sid[i] = p;
+            perm[i] = i;
+            sc[i] = cen[p];
+            slo[i] = plo[p];
+            shi[i] = phi[p];
+        }
+        if (threadIdx.x == 0) {
+            npieces = 0;
+            nw = 0;
+            next_id = id_base[ti];
+            if (count > kWarpRange) {
+                pieces[0] = Piece{0, count, tk.node, tk.depth, 0};
+                npieces = 1;
+            } else {
+                wpieces[0] = Piece{0, count, tk.node, tk.depth, id_base[ti]};
+                nw = 1;
+            }
+        }
+        __syncthreads();
+        int guard = 0;
+        while (npieces > 0 && guard++ < 2 * kBlockRange) {
+            const Piece pc = pieces[npieces - 1];
+            // centroid bounds of the piece
+            float lo[3] = {kInf, kInf, kInf}, hi[3] = {-kInf, -kInf, -kInf};
+            for (int i = threadIdx.x; i < pc.count; i += kBlock) {
+                const float4 c = sc[perm[pc.begin + i]];
+                lo[0] = fminf(lo[0], c.x);
+                lo[1] = fminf(lo[1], c.y);
+                lo[2] = fminf(lo[2], c.z);
+                hi[0] = fmaxf(hi[0], c.x);
+                hi[1] = fmaxf(hi[1], c.y);
+                hi[2] = fmaxf(hi[2], c.z);
+            }
+            for (int a = 0; a < 3; ++a) {
+                for (int o = 16; o > 0; o >>= 1) {
+                    lo[a] = fminf(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], o));
+                    hi[a] = fmaxf(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], o));
+                }
+            }
+            for (int j = threadIdx.x; j < 3 * bins * kBinWords; j += kBlock) {
+                const int w = j % kBinWords;
+                sb[j] = w == 0 ? 0u : (w <= 3 ? ord_f(kInf) : ord_f(-kInf));
+            }
+            if (threadIdx.x < 6) sbu[threadIdx.x] = threadIdx.x < 3 ? ord_f(kInf) : ord_f(-kInf);
+            __syncthreads();
+            if (threadIdx.x == 0) --npieces;
+            if (lane == 0) {
+                for (int a = 0; a < 3; ++a) {
+                    atomicMin(&sbu[a], ord_f(lo[a]));
+                    atomicMax(&sbu[3 + a], ord_f(hi[a]));
+                }
+            }
+            __syncthreads();
+            float cbl[3], cbh[3];
+            for (int a = 0; a < 3; ++a) {
+                cbl[a] = unord_f(sbu[a]);
+                cbh[a] = unord_f(sbu[3 + a]);
+            }
+            for (int i = threadIdx.x; i < pc.count; i += kBlock) {
+                const int li = perm[pc.begin + i];
+                const float4 c = sc[li], l = slo[li], h = shi[li];
+                const float cv[3] = {c.x, c.y, c.z};
+                for (int a = 0; a < 3; ++a) {
+                    unsigned* w = sb + (a * bins + bin_of(cv[a], cbl[a], cbh[a], bins)) * kBinWords;
+                    atomicAdd(&w[0], 1u);
+                    atomicMin(&w[1], ord_f(l.x));
+                    atomicMin(&w[2], ord_f(l.y));
+                    atomicMin(&w[3], ord_f(l.z));
+                    atomicMax(&w[4], ord_f(h.x));
+                    atomicMax(&w[5], ord_f(h.y));
+                    atomicMax(&w[6], ord_f(h.z));
+                }
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                int lc = 0;
+                int sp = sweep_bins(sb, bins, pc.count, &lc);
+                if (sp >= 0 && pc.depth + 1 + ceil_log2(max(lc, pc.count - lc)) > kMaxDepth) sp = -1;
+                if (sp < 0) lc = pc.count / 2;
+                s_split = sp;
+                s_left = lc;
+                for (int a = 0; a < 3; ++a) {
+                    sbf[a] = cbl[a];
+                    sbf[3 + a] = cbh[a];
+                }
+            }
+            __syncthreads();
+            const int split = s_split, lc = s_left;
+            // stable partition: destination of every position into tmp
+            int carry = 0;
+            for (int base = 0; base < pc.count; base += kBlock) {
+                const int i = base + threadIdx.x;
+                int f = 0;
+                if (i < pc.count) {
+                    if (split < 0) {
+                        f = i < lc;
+                    } else {
+                        const int a = split >> 8;
+                        const float4 c = sc[perm[pc.begin + i]];
+                        const float v = a == 0 ? c.x : (a == 1 ? c.y : c.z);
+                        f = bin_of(v, sbf[a], sbf[3 + a], bins) < (split & 255);
+                    }
+                }
+                int v = f;
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int y = __shfl_up_sync(0xffffffffu, v, o);
+                    if (lane >= o) v += y;
+                }
+                if (lane == 31) wsum[warp] = v;
+                __syncthreads();
+                int wpre = 0, tot = 0;
+                for (int w = 0; w < kBlock / 32; ++w) {
+                    if (w < warp) wpre += wsum[w];
+                    tot += wsum[w];
+                }
+                const int lrank = carry + wpre + v - f;
+                if (i < pc.count) tmp[pc.begin + (f ? lrank : lc + (i - lrank))] = perm[pc.begin + i];
+                __syncthreads();
+                carry += tot;
+            }
+            for (int i = threadIdx.x; i < pc.count; i += kBlock) perm[pc.begin + i] = tmp[pc.begin + i];
+            if (threadIdx.x == 0) {
+                const int rc = pc.count - lc;
+                const int lid = lc >= 2 ? next_id++ : n - 1 + tk.begin + pc.begin;
+                const int rid = rc >= 2 ? next_id++ : n - 1 + tk.begin + pc.begin + lc;
+                link(nodes, bn, parent, pc.node, lid, rid, n);
+                const Piece L = Piece{pc.begin, lc, lid, pc.depth + 1, 0};
+                const Piece R = Piece{pc.begin + lc, rc, rid, pc.depth + 1, 0};
+                for (int k = 0; k < 2; ++k) {
+                    Piece q = k == 0 ? R : L;
+                    if (q.count > kWarpRange) {
+                        if (npieces < kPieceCap) pieces[npieces++] = q;
+                        else atomicAdd(err, 1);
+                    } else if (q.count >= 2) {
+                        q.ids = next_id;
+                        next_id += q.count - 2;
+                        if (nw < kBlockRange / 2) wpieces[nw++] = q;
+                        else atomicAdd(err, 1);
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        if (threadIdx.x == 0 && npieces > 0) atomicAdd(err, 1);
+        __syncthreads();
+        const int total_w = nw;
+        for (int w = warp; w < total_w; w += kBlock / 32) {
+            const Piece q = wpieces[w];
+            warp_build(perm, sc, slo, shi, q.begin, q.count, q.node, q.depth, q.ids, nodes, bn,
+                       parent, n, tk.begin);
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < count; i += kBlock) order[tk.begin + i] = sid[perm[i]];
+        __syncthreads();
+    }
+}
+
+constexpr size_t kBlockSmem = 3 * kBlockRange * sizeof(float4) + 3 * kBlockRange * sizeof(int);
+
+// leaves of the final order: sorted items, ids, inverse map, canonical leaf nodes, payload
+template <class Ops>
+__global__ __launch_bounds__(kBlock) void k_sah_leaves(const float* __restrict__ items, int n,
+                                                      const int* __restrict__ order,
+                                                      Node* __restrict__ nodes,
+                                                      float* __restrict__ sorted,
+                                                      int* __restrict__ prim_ids,
+                                                      int* __restrict__ slot_of,
+                                                      float4* __restrict__ leaves) {
+    const int k = blockIdx.x * kBlock + threadIdx.x;
+    if (k >= n) return;
+    const int src = order[k];
+    float it[Ops::kFloats];
+#pragma unroll
+    for (int j = 0; j < Ops::kFloats; ++j) it[j] = items[static_cast<size_t>(src) * Ops::kFloats + j];
+#pragma unroll
+    for (int j = 0; j < Ops::kFloats; ++j) sorted[static_cast<size_t>(k) * Ops::kFloats + j] = it[j];
+    prim_ids[k] = src;
+    slot_of[src] = k;
+    const Box b = Ops::bounds(it);
+    float4* leaf = reinterpret_cast<float4*>(nodes + (n - 1 + k));
+    leaf[0] = make_float4(b.lo.x, b.lo.y, b.lo.z, b.hi.x);
+    leaf[1] = make_float4(b.hi.y, b.hi.z, __int_as_float(-(k + 1)), __int_as_float(1));
+    float4 pay[Ops::kVec4];
+    Ops::pack(it, src, pay);
+#pragma unroll
+    for (int j = 0; j < Ops::kVec4; ++j) leaves[static_cast<size_t>(k) * Ops::kVec4 + j] = pay[j];
+}
+
+__global__ void k_task_sizes(const Task* __restrict__ t, int m, int* __restrict__ out) {
+    const int i = blockIdx.x * kBlock + threadIdx.x;
+    if (i < m) out[i] = t[i].end - t[i].begin - 2;
+}
+
+__global__ void k_add_base(int* __restrict__ v, int m, const int* __restrict__ base) {
+    const int i = blockIdx.x * kBlock + threadIdx.x;
+    if (i < m) v[i] += base[3];
+}
+
+struct SahWs {
+    Header* h;
+    int* orderA;
+    int* orderB;
+    float4* cen;
+    float4* plo;
+    float4* phi;
+    Task* tasksA;
+    Task* tasksB;
+    Task* blocks;
+    int* id_base;
+    void* scan_ws;
+    Level L;
+};
+
+SahWs carve_sah(Carve& c, int n) {
+    const int max_big = n / (kBlockRange + 1) + 2;
+    const int max_chunks = n / kChunk + max_big + 2;
+    const int max_blocks = n / 2 + 2;
+    SahWs w;
+    w.h = c.take<Header>(1);
+    w.orderA = c.take<int>(n);
+    w.orderB = c.take<int>(n);
+    w.cen = c.take<float4>(n);
+    w.plo = c.take<float4>(n);
+    w.phi = c.take<float4>(n);
+    w.tasksA = c.take<Task>(max_big);
+    w.tasksB = c.take<Task>(max_big);
+    w.blocks = c.take<Task>(max_blocks);
+    w.id_base = c.take<int>(max_blocks + 1);
+    w.scan_ws = c.take<char>(scan_ws_bytes(max_blocks));
+    w.L.tasks = w.tasksA;
+    w.L.chunk_task = c.take<int>(max_chunks);
+    w.L.chunk_begin = c.take<int>(max_chunks);
+    w.L.chunk_first = c.take<int>(max_big);
+    w.L.cb = c.take<unsigned>(6 * static_cast<size_t>(max_big));
+    w.L.bins = c.take<unsigned>(static_cast<size_t>(max_big) * 3 * kMaxBins * kBinWords);
+    w.L.split = c.take<int>(max_big);
+    w.L.left_count = c.take<int>(max_big);
+    w.L.chunk_left = c.take<int>(max_chunks);
+    w.L.counters = c.take<int>(8);
+    return w;
+}
+
+template <class Ops>
+int build_sah_impl(qk_tree* t, int bins, const void* items_v, void* ws, cudaStream_t s) {
+    const int n = t->n;
+    const float* items = static_cast<const float*>(items_v);
+    Carve c{static_cast<char*>(ws)};
+    SahWs w = carve_sah(c, n);
+    Node* nodes = static_cast<Node*>(t->nodes);
+    BNode* bn = static_cast<BNode*>(t->bnodes);
+    int* err = &w.h->error;
+    cudaMemsetAsync(w.h, 0, sizeof(Header), s);
+    cudaMemsetAsync(t->parent, 0xff, sizeof(int) * (2 * static_cast<size_t>(n) - 1), s);
+    k_prim_geom<Ops><<<blocks_for(n), kBlock, 0, s>>>(items, n, w.cen, w.plo, w.phi, w.orderA);
+
+    // counters: [1] next big tasks, [2] block tasks, [3] next internal id
+    int init[8] = {0, 0, 0, 1, 0, 0, 0, 0};
+    Task root{0, n, 0, 0};
+    int nbig = 0, nblk = 0;
+    if (n > kBlockRange) {
+        cudaMemcpyAsync(w.tasksA, &root, sizeof(Task), cudaMemcpyHostToDevice, s);
+        nbig = 1;
+    } else {
+        cudaMemcpyAsync(w.blocks, &root, sizeof(Task), cudaMemcpyHostToDevice, s);
+        init[2] = 1;
+        nblk = 1;
+    }
+    cudaMemcpyAsync(w.L.counters, init, sizeof(init), cudaMemcpyHostToDevice, s);
+    Task* cur = w.tasksA;
+    Task* nxt = w.tasksB;
+    int* ord = w.orderA;
+    int* alt = w.orderB;
+    int level = 0;
+    while (nbig > 0) {
+        if (++level > kMaxDepth) return fail(QK_ERR_DEPTH, "SAH: too many levels");
+        w.L.tasks = cur;
+        k_level_prep<<<1, 1024, 0, s>>>(w.L, nbig, bins);
+        int nch = 0;
+        cudaError_t e = cudaMemcpyAsync(&nch, w.L.counters, sizeof(int), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return cuda_status(e, "SAH level prep");
+        k_level_cbounds<<<nch, kBlock, 0, s>>>(w.L, ord, w.cen);
+        k_level_bins<<<nch, kBlock, 0, s>>>(w.L, ord, w.cen, w.plo, w.phi, bins);
+        k_level_split<<<blocks_for(nbig), kBlock, 0, s>>>(w.L, nbig, bins);
+        k_level_count_left<<<nch, kBlock, 0, s>>>(w.L, ord, w.cen, bins);
+        k_level_prefix_left<<<blocks_for(nbig), kBlock, 0, s>>>(w.L, nbig);
+        k_level_partition<<<nch, kBlock, 0, s>>>(w.L, ord, alt, w.cen, bins);
+        k_level_copy<<<nch, kBlock, 0, s>>>(w.L, alt, ord);
+        // next big tasks start from zero each level; block tasks accumulate
+        cudaMemsetAsync(w.L.counters + 1, 0, sizeof(int), s);
+        k_level_assign<<<1, 1024, 0, s>>>(w.L, nbig, nxt, w.blocks, nodes, bn, t->parent, n);
+        int cnt[4] = {0, 0, 0, 0};
+        e = cudaMemcpyAsync(cnt, w.L.counters, sizeof(cnt), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return cuda_status(e, "SAH level");
+        nbig = cnt[1];
+        nblk = cnt[2];
+        Task* tmpt = cur;
+        cur = nxt;
+        nxt = tmpt;
+    }
+    if (nblk > 0) {
+        // reserved ids for the block subtrees: base + exclusive sum of (count - 2)
+        k_task_sizes<<<blocks_for(nblk), kBlock, 0, s>>>(w.blocks, nblk, w.id_base);
+        cudaError_t e = scan_exclusive(w.id_base, w.id_base, nblk, true, w.scan_ws, s);
+        if (e != cudaSuccess) return cuda_status(e, "SAH id scan");
+        int tail[2] = {0, 0};
+        e = cudaMemcpyAsync(&tail[0], w.id_base + nblk, sizeof(int), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&tail[1], w.L.counters + 3, sizeof(int), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return cuda_status(e, "SAH id readback");
+        if (tail[1] + tail[0] != n - 1) {
+            return fail(QK_ERR_INVALID, "SAH node accounting: %d + %d != %d", tail[1], tail[0], n - 1);
+        }
+        k_add_base<<<blocks_for(nblk), kBlock, 0, s>>>(w.id_base, nblk, w.L.counters);
+        const int grid = min(nblk, 148 * 4);
+        cudaFuncSetAttribute(k_block_build, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(kBlockSmem));
+        k_block_build<<<grid, kBlock, kBlockSmem, s>>>(w.blocks, nblk, w.id_base, ord, w.cen,
+                                                       w.plo, w.phi, nodes, bn, t->parent, n, bins,
+                                                       err);
+    } else {
+        int base = 0;
+        cudaMemcpyAsync(&base, w.L.counters + 3, sizeof(int), cudaMemcpyDeviceToHost, s);
+        cudaStreamSynchronize(s);
+        if (base != n - 1) return fail(QK_ERR_INVALID, "SAH node accounting: %d != %d", base, n - 1);
+    }
+    k_sah_leaves<Ops><<<blocks_for(n), kBlock, 0, s>>>(items, n, ord, nodes,
+                                                       static_cast<float*>(t->items), t->prim_ids,
+                                                       t->slot_of, static_cast<float4*>(t->leaves));
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_status(e, "SAH kernels");
+    int errors = 0;
+    e = cudaMemcpyAsync(&errors, err, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_status(e, "SAH readback");
+    if (errors) return fail(QK_ERR_OVERFLOW, "SAH block builder reported %d errors", errors);
+    return QK_OK;
+}
+
+}  // namespace
+
+size_t sah_ws_bytes(int n) {
+    Carve c;
+    carve_sah(c, n);
+    return c.used;
+}
+
+int build_sah(qk_tree* t, int bins, const void* items, void* ws, cudaStream_t s) {
+    if (bins < 4 || bins > kMaxBins) return fail(QK_ERR_INVALID, "sah_bins must be in [4, 64]");
+    switch (t->kind) {
+        case kTri: return build_sah_impl<TriOps>(t, bins, items, ws, s);
+        case kPoint: return build_sah_impl<PointOps>(t, bins, items, ws, s);
+        case kGauss: return build_sah_impl<GaussOps>(t, bins, items, ws, s);
+        default: return fail(QK_ERR_INVALID, "unknown primitive kind %d", t->kind);
+    }
+}
+
+}  // namespace qk

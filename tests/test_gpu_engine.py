@@ -254,3 +254,69 @@ def test_refit_full_and_dirty(cuda, kind):
     for flags in (0, capi.QK_WIDE):
         got = tree.closest(_dev(q), flags).cpu().numpy().view(np.uint32)
         assert np.array_equal(got, ref.closest(q))
+
+
+# ---------------------------------------------------------------------------------------
+# binned SAH builder: a different tree, identical query results
+# ---------------------------------------------------------------------------------------
+@pytest.mark.parametrize("kind,n,bins", [("tri", None, 16), ("tri", None, 32), ("point", 2, 32),
+                                         ("point", 3, 8), ("point", 700, 32),
+                                         ("point", 60_000, 32), ("gauss", 5000, 64)])
+def test_sah_tree_valid_and_results_identical(cuda, kind, n, bins):
+    if kind == "tri":
+        items = scenes()["city"]
+    elif kind == "point":
+        items = workloads.point_cloud("sphere", n, 5)
+    else:
+        items = workloads.gaussians(n, 0.05, 1.0, 5)
+    tree = capi.DeviceTree(kind, items, builder="sah", sah_bins=bins)
+    assert tree.validate() == [0] * 8
+    assert tree.depth <= 62
+    again = capi.DeviceTree(kind, items, builder="sah", sah_bins=bins)
+    assert again.nodes_bytes().tobytes() == tree.nodes_bytes().tobytes(), "SAH not deterministic"
+    ref = oracle.LBVH(kind, items)
+    if kind == "tri":
+        lo, hi = workloads.bounds_of(items)
+    else:
+        lo, hi = items[:, :3].min(0), items[:, :3].max(0)
+    q = workloads.uniform_points(2000, lo - 1, hi + 1, 3, 21)
+    tree.build_wide()
+    assert tree.validate() == [0] * 8
+    dq = _dev(q)
+    for flags in FLAG_SETS:
+        assert np.array_equal(tree.closest(dq, flags).cpu().numpy().view(np.uint32), ref.closest(q))
+        assert np.array_equal(tree.knn(dq, 8, flags).cpu().numpy().view(np.uint32), ref.knn(q, 8))
+    r = 3.0 if kind != "gauss" else 1.0
+    off, keys = tree.radius(dq, r)
+    woff, wkeys = ref.radius(q, r)
+    assert np.array_equal(off.cpu().numpy().astype(np.int64), woff)
+    assert np.array_equal(keys.cpu().numpy().view(np.uint64), wkeys)
+    if kind == "tri":
+        rays = workloads.cosine_rays(20_000, float(lo[0]), float(hi[0]), float(lo[1]),
+                                     float(hi[1]), float(hi[2]) + 5.0, 8)
+        want = ref.raycast(rays)
+        for flags in FLAG_SETS:
+            got = tree.raycast(_dev(rays), flags).cpu().numpy().view(np.uint64)
+            assert np.array_equal(got, want)
+
+
+def test_sah_city_large(cuda):
+    """The benchmark city at reduced size exercises the global SAH tier (> 1024 primitives
+    per range over several levels)."""
+    tris, top = workloads.city(20_000, 1)
+    tree = capi.DeviceTree("tri", tris, builder="sah", sah_bins=32)
+    assert tree.validate() == [0] * 8
+    lo, hi = workloads.bounds_of(tris)
+    rays = workloads.cosine_rays(50_000, float(lo[0]), float(hi[0]), float(lo[1]), float(hi[1]),
+                                 top + 50.0, 2)
+    ref = oracle.LBVH("tri", tris)
+    got = tree.raycast(_dev(rays)).cpu().numpy().view(np.uint64)
+    assert np.array_equal(got, ref.raycast(rays))
+    # the refit path works on SAH trees too
+    moved = tris.copy()
+    moved[:, 2::3] += np.float32(0.25)
+    tree.refit(moved)
+    ref.refit(moved)
+    assert tree.validate() == [0] * 8
+    got = tree.raycast(_dev(rays)).cpu().numpy().view(np.uint64)
+    assert np.array_equal(got, ref.raycast(rays))

@@ -44,7 +44,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=400)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="city", choices=["city", "terrain"])
+    ap.add_argument("--workload", default="city", choices=["city", "terrain", "grad"])
     ap.add_argument("--small", action="store_true", help="small inputs (profiling captures)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--only", default="", help="time only this variant (profiling)")
@@ -221,6 +221,91 @@ def reference_arm(args, world, rank):
 
 
 # ---------------------------------------------------------------------------------------
+# differentiable queries: forward and forward + backward time
+# ---------------------------------------------------------------------------------------
+def grad_arm(args, world, rank, local):
+    """1,048,576 Gaussians (means U[0,100]^3, log-uniform scales [0.05, 1], random rotations)
+    with 262,144 query points, loss = sum of point-to-ellipsoid distances; and 1M downward
+    rays on the 256 x 256 terrain, loss = sum of first-hit t, gradients to the vertices."""
+    import torch
+
+    from quarry import capi, workloads as w
+
+    torch.cuda.set_device(local)
+    small = args.small
+    ng, nq = (65_536, 16_384) if small else (1_048_576, 262_144)
+    g = torch.tensor(w.gaussians(ng, 0.05, 1.0, 1 + rank), device="cuda")
+    q = torch.tensor(w.uniform_points(nq, [0, 0, 0], [100, 100, 100], 1 + rank, 31), device="cuda")
+    flags = capi.QK_ORDER_MORTON
+    l2 = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+
+    def timed(fn, steps):
+        for _ in range(3):
+            fn()
+        ts = []
+        for _ in range(steps):
+            l2.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return float(np.median(ts))
+
+    state = {}
+
+    def g_build():
+        state["tree"] = capi.DeviceTree("gauss", g)
+
+    def g_fwd():
+        res = state["tree"].closest(q, flags)
+        state["res"] = res
+        state["d"] = torch.sqrt(res[:, 0].contiguous().view(torch.float32))
+
+    def g_bwd():
+        state["grads"] = state["tree"].distance_grad(q, state["res"])
+
+    g_build()
+    build_ms = timed(g_build, 5)
+    fwd_ms = timed(g_fwd, 10)
+    bwd_ms = timed(g_bwd, 10)
+
+    # triangles: 1M down rays on the terrain, loss = sum of t
+    tris = w.terrain(64 if small else 256, 1)
+    nr = 100_000 if small else 1_000_000
+    grid = 64 if small else 256
+    rays = capi.to_device(w.down_rays(nr, 0.0, float(grid), 0.0, float(grid), 100.0, 1), np.float32)
+    tri_tree = capi.DeviceTree("tri", tris)
+
+    def r_fwd():
+        state["out"], state["ids"] = tri_tree.raycast_ids(rays, flags)
+
+    def r_bwd():
+        state["rg"] = tri_tree.ray_t_grad(rays, state["ids"], None, with_rays=False)
+
+    r_fwd()
+    rf_ms = timed(r_fwd, 10)
+    rb_ms = timed(r_bwd, 10)
+    if rank == 0:
+        line = {"metric": METRIC, "value": round((fwd_ms + bwd_ms) / fwd_ms, 4),
+                "unit": "fwd+bwd / fwd (Gaussian closest distance)", "n_gpus": world,
+                "steps": 10, "warmup": 3, "ms_per_step": round(fwd_ms + bwd_ms, 4),
+                "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32 forward, f64 adjoint", "data": "synthetic (seeded generators)",
+                "config": {"workload": "gaussian distance + ray t gradients", "gaussians": ng,
+                           "queries": nq, "rays": nr, "terrain_grid": grid,
+                           "order": "morton", "l2": "flushed between timed steps"},
+                "gaussian": {"build_ms": round(build_ms, 3), "forward_ms": round(fwd_ms, 4),
+                             "backward_ms": round(bwd_ms, 4),
+                             "fwd_bwd_over_fwd": round((fwd_ms + bwd_ms) / fwd_ms, 4),
+                             "mqueries_per_s": round(nq / (fwd_ms * 1e-3) / 1e6, 2)},
+                "rays": {"forward_ms": round(rf_ms, 4), "backward_ms": round(rb_ms, 4),
+                         "fwd_bwd_over_fwd": round((rf_ms + rb_ms) / rf_ms, 4)}}
+        print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------------------
 def main():
@@ -228,6 +313,10 @@ def main():
     world, rank, local = init_dist(args)
     if args.impl == "reference":
         reference_arm(args, world, rank)
+        barrier(world)
+        return
+    if args.workload == "grad":
+        grad_arm(args, world, rank, local)
         barrier(world)
         return
     import torch

@@ -173,6 +173,37 @@ int qk_validate(const qk_tree* tree, const void* items, int32_t* errors, void* w
                 size_t workspace_bytes, void* stream);
 size_t qk_validate_workspace_bytes(int n);
 
+/* ---- differentiable queries (no counterpart in quarry, which has no backward pass) ---- */
+
+/* First-hit rays that also report the hit primitive: ids[count] = scene index (-1 on a
+ * miss); among primitives at the same t the smallest index.  The t results equal
+ * qk_raycast's bit for bit. */
+int qk_raycast_ids(const qk_tree* tree, const void* rays, int count, uint64_t* out, int32_t* ids,
+                   unsigned flags, void* workspace, size_t workspace_bytes, void* stream);
+
+size_t qk_grad_workspace_bytes(int count, int channels);
+
+/* Adjoint of d_i = |p_i - closest point of the selected primitive| (distance, not squared)
+ * for the selected primitive of qk_closest's results, recomputed in FP64.  grad_dist: count
+ * weights dL/dd_i (NULL = all ones).  Writes grad_points (count x 3) and grad_items (n x
+ * stride, scene order; summed over queries in query order, deterministic).  d = 0 (inside an
+ * ellipsoid, on a triangle) contributes 0. */
+int qk_distance_grad(const qk_tree* tree, const void* items, const float* points,
+                     const void* results, const float* grad_dist, int count, float* grad_points,
+                     float* grad_items, void* workspace, size_t workspace_bytes, void* stream);
+
+/* Adjoint of the first-hit t of the rays with respect to the hit triangles (grad_tris, n x 9,
+ * scene order, deterministic sums) and, when grad_rays is not NULL, the rays' origins and
+ * directions (count x 6).  ids from qk_raycast_ids; grad_t: dL/dt_i (NULL = all ones). */
+int qk_ray_t_grad(const qk_tree* tree, const void* items, const void* rays, const int32_t* ids,
+                  const float* grad_t, int count, float* grad_tris, float* grad_rays,
+                  void* workspace, size_t workspace_bytes, void* stream);
+
+/* Deterministic segmented sum: out[k, c] = sum over i in increasing order with keys[i] == k of
+ * values[i, c] (FP64 accumulation); keys < 0 are skipped.  1 <= channels <= 10. */
+int qk_segment_sum(const int32_t* keys, const float* values, int count, int channels, int segments,
+                   float* out, void* workspace, size_t workspace_bytes, void* stream);
+
 /* Stable LSD radix sort of 32-bit keys with 32-bit values over the low `bits` bits.  All
  * four buffers hold n entries; the sorted result ends in keys_out / vals_out. */
 size_t qk_sort_workspace_bytes(int n);

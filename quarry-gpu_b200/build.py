@@ -30,8 +30,8 @@ NVCC_FLAGS = [
     "-lineinfo", "-O3", "-std=c++17", "--fmad=false", "-Xcompiler", "-fPIC",
     "--expt-relaxed-constexpr", "-Xptxas", "-warn-spills",
 ]
-CU_SOURCES = ["qk_sort.cu", "qk_build.cu", "qk_sah.cu", "qk_query.cu", "qk_capi.cu",
-              "gpu_bvh.cu"]
+CU_SOURCES = ["qk_sort.cu", "qk_build.cu", "qk_sah.cu", "qk_query.cu", "qk_grad.cu",
+              "qk_capi.cu", "gpu_bvh.cu"]
 C_SOURCES = ["scenes.c"]
 LIB = OUT / "libquarry_b200.so"
 

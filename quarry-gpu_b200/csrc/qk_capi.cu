@@ -194,7 +194,61 @@ int qk_raycast(const qk_tree* tree, const void* rays, int count, uint64_t* out, 
     if (count > 0 && (!rays || !out)) return fail(QK_ERR_INVALID, "rays or out is NULL");
     if ((st = check_wide(tree, flags))) return st;
     if ((st = check_ws(workspace, workspace_bytes, order_ws_bytes(count)))) return st;
-    return ray_query(tree, rays, count, out, flags, stats, workspace, as_stream(stream));
+    return ray_query(tree, rays, count, out, nullptr, flags, stats, workspace, as_stream(stream));
+}
+
+int qk_raycast_ids(const qk_tree* tree, const void* rays, int count, uint64_t* out, int32_t* ids,
+                   unsigned flags, void* workspace, size_t workspace_bytes, void* stream) {
+    int st = check_tree(tree);
+    if (st) return st;
+    if (tree->kind != QK_TRI) return fail(QK_ERR_INVALID, "raycast needs a triangle tree");
+    if (count < 0) return fail(QK_ERR_INVALID, "negative ray count");
+    if (count > 0 && (!rays || !out || !ids)) return fail(QK_ERR_INVALID, "rays, out or ids is NULL");
+    if ((st = check_wide(tree, flags))) return st;
+    if ((st = check_ws(workspace, workspace_bytes, order_ws_bytes(count)))) return st;
+    return ray_query(tree, rays, count, out, ids, flags, nullptr, workspace, as_stream(stream));
+}
+
+size_t qk_grad_workspace_bytes(int count, int channels) {
+    return count > 0 ? grad_ws_bytes(count, channels < 10 ? 10 : channels) : 256;
+}
+
+int qk_distance_grad(const qk_tree* tree, const void* items, const float* points,
+                     const void* results, const float* grad_dist, int count, float* grad_points,
+                     float* grad_items, void* workspace, size_t workspace_bytes, void* stream) {
+    int st = check_tree(tree);
+    if (st) return st;
+    if (count < 0) return fail(QK_ERR_INVALID, "negative query count");
+    if (!items || !grad_items || (count > 0 && (!points || !results || !grad_points)))
+        return fail(QK_ERR_INVALID, "NULL array");
+    if ((st = check_ws(workspace, workspace_bytes, grad_ws_bytes(count, qk_stride_floats(tree->kind)))))
+        return st;
+    return closest_distance_grad(tree->kind, tree->n, items, points, results, grad_dist, count,
+                                 grad_points, grad_items, workspace, as_stream(stream));
+}
+
+int qk_ray_t_grad(const qk_tree* tree, const void* items, const void* rays, const int32_t* ids,
+                  const float* grad_t, int count, float* grad_tris, float* grad_rays,
+                  void* workspace, size_t workspace_bytes, void* stream) {
+    int st = check_tree(tree);
+    if (st) return st;
+    if (tree->kind != QK_TRI) return fail(QK_ERR_INVALID, "ray gradients need a triangle tree");
+    if (count < 0) return fail(QK_ERR_INVALID, "negative ray count");
+    if (!items || !grad_tris || (count > 0 && (!rays || !ids))) return fail(QK_ERR_INVALID, "NULL array");
+    if ((st = check_ws(workspace, workspace_bytes, grad_ws_bytes(count, 9)))) return st;
+    return ray_t_grad(tree->n, items, rays, ids, grad_t, count, grad_tris, grad_rays, workspace,
+                      as_stream(stream));
+}
+
+int qk_segment_sum(const int32_t* keys, const float* values, int count, int channels, int segments,
+                   float* out, void* workspace, size_t workspace_bytes, void* stream) {
+    if (count < 0 || segments < 0 || channels < 1 || channels > 10)
+        return fail(QK_ERR_INVALID, "bad count, segments or channels (1..10)");
+    if (segments > 0 && !out) return fail(QK_ERR_INVALID, "out is NULL");
+    if (count > 0 && (!keys || !values)) return fail(QK_ERR_INVALID, "NULL array");
+    int st = check_ws(workspace, workspace_bytes, grad_ws_bytes(count, 0));
+    if (st) return st;
+    return segment_sum(keys, values, count, channels, segments, out, workspace, as_stream(stream));
 }
 
 int qk_closest(const qk_tree* tree, const float* points, int count, void* out, unsigned flags,

@@ -90,8 +90,8 @@ int validate_tree(const qk_tree* t, const void* items, int* errors, void* ws, cu
 
 // ---- traversal (qk_query.cu) ----
 size_t order_ws_bytes(int count);
-int ray_query(const qk_tree* t, const void* rays, int count, uint64_t* out, unsigned flags,
-              uint64_t* stats, void* ws, cudaStream_t s);
+int ray_query(const qk_tree* t, const void* rays, int count, uint64_t* out, int* ids,
+              unsigned flags, uint64_t* stats, void* ws, cudaStream_t s);
 int closest_query(const qk_tree* t, const float* pts, int count, void* out, unsigned flags,
                   uint64_t* stats, void* ws, cudaStream_t s);
 int knn_query(const qk_tree* t, const float* pts, int count, int k, int stride, void* out,
@@ -101,5 +101,15 @@ int radius_count(const qk_tree* t, const float* pts, int count, float r, int* of
                  long long* total, unsigned flags, uint64_t* stats, void* ws, cudaStream_t s);
 int radius_fill(const qk_tree* t, const float* pts, int count, float r, const int* offsets,
                 uint64_t* keys, unsigned flags, void* ws, cudaStream_t s);
+
+// ---- adjoints (qk_grad.cu) ----
+size_t grad_ws_bytes(int count, int channels);
+int closest_distance_grad(int kind, int n, const void* items, const float* pts, const void* res,
+                          const float* gw, int count, float* gpts, float* gitems, void* ws,
+                          cudaStream_t s);
+int ray_t_grad(int n, const void* tris, const void* rays, const int* ids, const float* gw,
+               int count, float* gtris, float* grays, void* ws, cudaStream_t s);
+int segment_sum(const int* keys, const float* vals, int count, int channels, int nseg, float* out,
+                void* ws, cudaStream_t s);
 
 }  // namespace qk

@@ -136,15 +136,23 @@ __device__ __forceinline__ Box root_box(const Node* __restrict__ nodes) {
 // ---------------------------------------------------------------------------------------
 // rays
 // ---------------------------------------------------------------------------------------
+// Leaf test.  The first hit is taken even at t == tMax (the CPU reference accepts t <= tMax,
+// src/cpu/bvh.cpp:156-168); later hits only when closer.  Among hits at the same t the
+// smallest scene index is kept, so the reported primitive does not depend on visit order.
 __device__ __forceinline__ void test_tri(const RayPre& R, const float4* __restrict__ leaves,
-                                         int slot, float& best, float& bound, bool& any) {
+                                         int slot, float& best, float& bound, bool& any,
+                                         int& best_id) {
     const float4 a = __ldg(leaves + 3 * slot), b = __ldg(leaves + 3 * slot + 1),
                  c = __ldg(leaves + 3 * slot + 2);
     float t;
-    if (ray_tri(R, f3(a.x, a.y, a.z), f3(b.x, b.y, b.z), f3(c.x, c.y, c.z), t) && t < best) {
-        best = t;
-        bound = best * kMarginMul + kMarginAdd;
-        any = true;
+    if (ray_tri(R, f3(a.x, a.y, a.z), f3(b.x, b.y, b.z), f3(c.x, c.y, c.z), t)) {
+        const int id = __float_as_int(a.w);
+        if (!any || t < best || (t == best && id < best_id)) {
+            best = t;
+            bound = best * kMarginMul + kMarginAdd;
+            any = true;
+            best_id = id;
+        }
     }
 }
 
@@ -155,6 +163,7 @@ __global__ __launch_bounds__(kBlock) void k_ray_bin(const BNode* __restrict__ bn
                                                    const float4* __restrict__ rays,
                                                    const uint32_t* __restrict__ order, int count,
                                                    unsigned long long* __restrict__ out,
+                                                   int* __restrict__ ids,
                                                    int max_iter, unsigned long long* __restrict__ stats) {
     const int i = blockIdx.x * kBlock + threadIdx.x;
     const bool active = i < count;
@@ -166,6 +175,7 @@ __global__ __launch_bounds__(kBlock) void k_ray_bin(const BNode* __restrict__ bn
         float best = R.tmax;
         float bound = best * kMarginMul + kMarginAdd;
         bool any = false;
+        int best_id = -1;
         const Box rb = root_box(nodes);
         float te;
         if (ray_box(R, rb.lo, rb.hi, bound, te)) {
@@ -188,12 +198,12 @@ __global__ __launch_bounds__(kBlock) void k_ray_bin(const BNode* __restrict__ bn
                 ntests += static_cast<int>(hl) + static_cast<int>(hr);
                 if (hl && lref < 0) {
                     ++ttests;
-                    test_tri(R, leaves, ~lref, best, bound, any);
+                    test_tri(R, leaves, ~lref, best, bound, any, best_id);
                     hl = false;
                 }
                 if (hr && rref < 0) {
                     ++ttests;
-                    test_tri(R, leaves, ~rref, best, bound, any);
+                    test_tri(R, leaves, ~rref, best, bound, any, best_id);
                     hr = false;
                 }
                 if (hl && hr) {
@@ -226,6 +236,7 @@ __global__ __launch_bounds__(kBlock) void k_ray_bin(const BNode* __restrict__ bn
             }
         }
         out[r] = any ? ((1ull << 32) | static_cast<unsigned long long>(__float_as_uint(best))) : 0ull;
+        if (ids) ids[r] = best_id;
     }
     flush_stats<kStats>(active, ntests, ttests, overflow, stats);
 }
@@ -245,6 +256,7 @@ __global__ __launch_bounds__(kBlock) void k_ray_wide(const WideNode* __restrict_
                                                     const float4* __restrict__ rays,
                                                     const uint32_t* __restrict__ order, int count,
                                                     unsigned long long* __restrict__ out,
+                                                    int* __restrict__ ids,
                                                     int max_iter, unsigned long long* __restrict__ stats) {
     const int i = blockIdx.x * kBlock + threadIdx.x;
     const bool active = i < count;
@@ -256,6 +268,7 @@ __global__ __launch_bounds__(kBlock) void k_ray_wide(const WideNode* __restrict_
         float best = R.tmax;
         float bound = best * kMarginMul + kMarginAdd;
         bool any = false;
+        int best_id = -1;
         int stack[kStackWide];
         float stackT[kStackWide];
         int sp = 0;
@@ -292,7 +305,7 @@ __global__ __launch_bounds__(kBlock) void k_ray_wide(const WideNode* __restrict_
             for (int j = 0; j < hits; ++j) {
                 if (child[j] < 0) {
                     ++ttests;
-                    test_tri(R, leaves, ~child[j], best, bound, any);
+                    test_tri(R, leaves, ~child[j], best, bound, any, best_id);
                 }
             }
             for (int j = hits - 1; j >= 0; --j) {
@@ -327,6 +340,7 @@ __global__ __launch_bounds__(kBlock) void k_ray_wide(const WideNode* __restrict_
             if (node < 0) break;
         }
         out[r] = any ? ((1ull << 32) | static_cast<unsigned long long>(__float_as_uint(best))) : 0ull;
+        if (ids) ids[r] = best_id;
     }
     flush_stats<kStats>(active, ntests, ttests, overflow, stats);
 }
@@ -1099,8 +1113,8 @@ size_t order_ws_bytes(int count) {
     return c.used;
 }
 
-int ray_query(const qk_tree* t, const void* rays, int count, uint64_t* out, unsigned flags,
-              uint64_t* stats, void* ws, cudaStream_t s) {
+int ray_query(const qk_tree* t, const void* rays, int count, uint64_t* out, int* ids,
+              unsigned flags, uint64_t* stats, void* ws, cudaStream_t s) {
     if (count <= 0) return QK_OK;
     Carve c{static_cast<char*>(ws)};
     OrderBufs o = carve_order(c, count);
@@ -1116,13 +1130,13 @@ int ray_query(const qk_tree* t, const void* rays, int count, uint64_t* out, unsi
     const int g = blocks_for(count);
     if (flags & QK_WIDE) {
         const WideNode* wn = static_cast<const WideNode*>(t->wide);
-        if (stt) k_ray_wide<true><<<g, kBlock, 0, s>>>(wn, leaves, r4, order, count, res, t->n * 2 + 64, stt);
-        else k_ray_wide<false><<<g, kBlock, 0, s>>>(wn, leaves, r4, order, count, res, t->n * 2 + 64, stt);
+        if (stt) k_ray_wide<true><<<g, kBlock, 0, s>>>(wn, leaves, r4, order, count, res, ids, t->n * 2 + 64, stt);
+        else k_ray_wide<false><<<g, kBlock, 0, s>>>(wn, leaves, r4, order, count, res, ids, t->n * 2 + 64, stt);
     } else {
         const BNode* bn = static_cast<const BNode*>(t->bnodes);
         const Node* nodes = static_cast<const Node*>(t->nodes);
-        if (stt) k_ray_bin<true><<<g, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, t->n * 2 + 64, stt);
-        else k_ray_bin<false><<<g, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, t->n * 2 + 64, stt);
+        if (stt) k_ray_bin<true><<<g, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, ids, t->n * 2 + 64, stt);
+        else k_ray_bin<false><<<g, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, ids, t->n * 2 + 64, stt);
     }
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? QK_OK : cuda_status(e, "raycast");

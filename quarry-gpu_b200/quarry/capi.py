@@ -67,6 +67,11 @@ EXPORTS = {
     "qk_validate": (_I, [ctypes.POINTER(QkTree), _P, _P, _P, _SZ, _P]),
     "qk_validate_workspace_bytes": (_SZ, [_I]),
     "qk_sort_workspace_bytes": (_SZ, [_I]),
+    "qk_raycast_ids": (_I, [ctypes.POINTER(QkTree), _P, _I, _P, _P, _U, _P, _SZ, _P]),
+    "qk_grad_workspace_bytes": (_SZ, [_I, _I]),
+    "qk_distance_grad": (_I, [ctypes.POINTER(QkTree), _P, _P, _P, _P, _I, _P, _P, _P, _SZ, _P]),
+    "qk_ray_t_grad": (_I, [ctypes.POINTER(QkTree), _P, _P, _P, _P, _I, _P, _P, _P, _SZ, _P]),
+    "qk_segment_sum": (_I, [_P, _P, _I, _I, _I, _P, _P, _SZ, _P]),
     "qk_sort_pairs": (_I, [_P, _P, _P, _P, _I, _I, _P, _SZ, _P]),
 }
 
@@ -256,6 +261,41 @@ class DeviceTree:
                                _ptr(stats), _ptr(w), w.numel(), _stream()), "qk_raycast")
         return out
 
+    def raycast_ids(self, rays, flags: int = 0):
+        """First hits with the hit primitive (scene index, -1 on a miss)."""
+        torch = _torch()
+        count = rays.shape[0]
+        out = torch.empty(count, dtype=torch.int64, device="cuda")
+        ids = torch.empty(count, dtype=torch.int32, device="cuda")
+        w = self.ws.get(lib().qk_query_workspace_bytes(count, flags))
+        check(lib().qk_raycast_ids(ctypes.byref(self.t), _ptr(rays), count, _ptr(out), _ptr(ids),
+                                   flags, _ptr(w), w.numel(), _stream()), "qk_raycast_ids")
+        return out, ids
+
+    def distance_grad(self, pts, results, grad_dist=None):
+        """Adjoint of the distances of qk_closest's results: (grad_points, grad_items)."""
+        torch = _torch()
+        count = pts.shape[0]
+        gp = torch.empty((count, 3), dtype=torch.float32, device="cuda")
+        gi = torch.empty_like(self.items_scene)
+        w = _dev_bytes(lib().qk_grad_workspace_bytes(count, STRIDE[self.kind]))
+        check(lib().qk_distance_grad(ctypes.byref(self.t), _ptr(self.items_scene), _ptr(pts),
+                                     _ptr(results), _ptr(grad_dist), count, _ptr(gp), _ptr(gi),
+                                     _ptr(w), w.numel(), _stream()), "qk_distance_grad")
+        return gp, gi
+
+    def ray_t_grad(self, rays, ids, grad_t=None, with_rays: bool = True):
+        """Adjoint of the first-hit t: (grad_tris (n, 9), grad_rays (count, 6) or None)."""
+        torch = _torch()
+        count = rays.shape[0]
+        gt = torch.empty((self.n, 9), dtype=torch.float32, device="cuda")
+        gr = torch.empty((count, 6), dtype=torch.float32, device="cuda") if with_rays else None
+        w = _dev_bytes(lib().qk_grad_workspace_bytes(count, 9))
+        check(lib().qk_ray_t_grad(ctypes.byref(self.t), _ptr(self.items_scene), _ptr(rays),
+                                  _ptr(ids), _ptr(grad_t), count, _ptr(gt), _ptr(gr), _ptr(w),
+                                  w.numel(), _stream()), "qk_ray_t_grad")
+        return gt, gr
+
     def closest(self, pts, flags: int = 0, stats=None, out=None):
         torch = _torch()
         count = pts.shape[0]
@@ -294,6 +334,18 @@ class DeviceTree:
                                    _ptr(offsets), _ptr(keys), flags, _ptr(w), w.numel(),
                                    _stream()), "qk_radius_fill")
         return offsets, keys[: total.value]
+
+
+def segment_sum(keys, values, segments: int):
+    """Deterministic out[k] = sum of values[i] with keys[i] == k, in increasing i."""
+    torch = _torch()
+    count = keys.numel()
+    ch = values.shape[1] if values.dim() > 1 else 1
+    out = torch.empty((segments, ch), dtype=torch.float32, device="cuda")
+    w = _dev_bytes(lib().qk_grad_workspace_bytes(count, 0))
+    check(lib().qk_segment_sum(_ptr(keys), _ptr(values), count, ch, segments, _ptr(out), _ptr(w),
+                               w.numel(), _stream()), "qk_segment_sum")
+    return out
 
 
 def sort_pairs(keys, vals, bits: int = 32):

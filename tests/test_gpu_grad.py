@@ -1,0 +1,305 @@
+"""Gradients of the differentiable queries (quarry.torch) against FP64 references.
+
+Two references per result, both on the CPU in FP64 with the forward's selection held fixed:
+  * central finite differences (h = 1e-3) of FP64 restatements of the leaf tests, on 1,000
+    randomly drawn parameters;
+  * an analytic FP64 gradient written here from the geometry (envelope theorem for the
+    distances, plane-crossing derivative for t).
+Tolerances (relative error |g - g_ref| / max(|g_ref|, floor)): analytic <= 1e-4 everywhere;
+finite differences median <= 1e-4 and 99th percentile <= 1e-2 (the FD truncation error grows
+where a distance is tiny or a ray grazes its triangle).
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from quarry import workloads
+
+pytestmark = pytest.mark.gpu
+H = 1e-3
+
+
+# ---------------------------------------------------------------------------------------
+# FP64 restatements (selection fixed)
+# ---------------------------------------------------------------------------------------
+def quat_axes(q):
+    q = q / np.linalg.norm(q, axis=-1, keepdims=True)
+    x, y, z, w = q[..., 0], q[..., 1], q[..., 2], q[..., 3]
+    u = np.stack([1 - 2 * (y * y + z * z), 2 * (x * y + z * w), 2 * (x * z - y * w)], -1)
+    v = np.stack([2 * (x * y - z * w), 1 - 2 * (x * x + z * z), 2 * (y * z + x * w)], -1)
+    t = np.stack([2 * (x * z + y * w), 2 * (y * z - x * w), 1 - 2 * (x * x + y * y)], -1)
+    return u, v, t
+
+
+def ellipsoid_d(p, g):
+    """p (K,3), g (K,10) float64 -> (d, local point y, closest local x, scales, axes)."""
+    u, v, w = quat_axes(g[:, 3:7])
+    dp = p - g[:, 0:3]
+    y = np.stack([(dp * u).sum(-1), (dp * v).sum(-1), (dp * w).sum(-1)], -1)
+    s = g[:, 7:10]
+    inside = ((y / s) ** 2).sum(-1) <= 1.0
+    lo = np.zeros(len(p))
+    hi = 2 * s.max(-1) * np.linalg.norm(y, axis=-1)
+    for _ in range(200):
+        mid = 0.5 * (lo + hi)
+        f = ((s * y / (mid[:, None] + s * s)) ** 2).sum(-1) - 1
+        lo = np.where(f > 0, mid, lo)
+        hi = np.where(f > 0, hi, mid)
+    t = 0.5 * (lo + hi)
+    x = s * s * y / (t[:, None] + s * s)
+    d = np.where(inside, 0.0, np.linalg.norm(y - x, axis=-1))
+    return d, y, x, s, (u, v, w), dp
+
+
+def closest_tri(p, a, b, c):
+    """Vectorised Ericson closest point in FP64; returns (q, wa, wb, wc)."""
+    ab, ac, ap = b - a, c - a, p - a
+    d1, d2 = (ab * ap).sum(-1), (ac * ap).sum(-1)
+    bp = p - b
+    d3, d4 = (ab * bp).sum(-1), (ac * bp).sum(-1)
+    cp = p - c
+    d5, d6 = (ab * cp).sum(-1), (ac * cp).sum(-1)
+    vc = d1 * d4 - d3 * d2
+    vb = d5 * d2 - d1 * d6
+    va = d3 * d6 - d5 * d4
+    wb = np.zeros(len(p))
+    wc = np.zeros(len(p))
+    done = np.zeros(len(p), bool)
+
+    def put(mask, b_, c_):
+        nonlocal done
+        m = mask & ~done
+        wb[m] = b_[m] if np.ndim(b_) else b_
+        wc[m] = c_[m] if np.ndim(c_) else c_
+        done |= m
+
+    with np.errstate(divide="ignore", invalid="ignore"):
+        put((d1 <= 0) & (d2 <= 0), 0.0, 0.0)
+        put((d3 >= 0) & (d4 <= d3), 1.0, 0.0)
+        put((vc <= 0) & (d1 >= 0) & (d3 <= 0), d1 / (d1 - d3), np.zeros(len(p)))
+        put((d6 >= 0) & (d5 <= d6), 0.0, 1.0)
+        put((vb <= 0) & (d2 >= 0) & (d6 <= 0), np.zeros(len(p)), d2 / (d2 - d6))
+        tbc = (d4 - d3) / ((d4 - d3) + (d5 - d6))
+        put((va <= 0) & ((d4 - d3) >= 0) & ((d5 - d6) >= 0), 1.0 - tbc, tbc)
+        den = va + vb + vc
+        put(np.ones(len(p), bool), vb / den, vc / den)
+    wa = 1 - wb - wc
+    q = a * wa[:, None] + b * wb[:, None] + c * wc[:, None]
+    return q, wa, wb, wc
+
+
+def ray_t(o, d, a, b, c):
+    n = np.cross(b - a, c - a)
+    return ((n * (a - o)).sum(-1)) / ((n * d).sum(-1))
+
+
+def rel_err(g, ref, floor):
+    return np.abs(g - ref) / np.maximum(np.abs(ref), floor)
+
+
+# ---------------------------------------------------------------------------------------
+# Gaussians
+# ---------------------------------------------------------------------------------------
+def test_gaussian_distance_gradients(cuda):
+    import torch
+
+    import quarry.torch as qt
+
+    g = workloads.gaussians(20_000, 0.05, 1.0, 3)
+    q = workloads.uniform_points(8_000, [0, 0, 0], [100, 100, 100], 3, 31)
+    gt = torch.tensor(g, device="cuda")
+    pts = torch.tensor(q, device="cuda", requires_grad=True)
+    means = gt[:, 0:3].clone().requires_grad_(True)
+    rots = gt[:, 3:7].clone().requires_grad_(True)
+    scales = gt[:, 7:10].clone().requires_grad_(True)
+    d = qt.gaussian_distance(pts, means, rots, scales)
+    d.sum().backward()
+    # the forward's selection, read through the closest query of the same tree
+    from quarry import capi
+
+    tree = capi.DeviceTree("gauss", gt)
+    res = tree.closest(capi.to_device(q, np.float32)).cpu().numpy()
+    ids = res[:, 1].astype(np.int64)
+    assert np.all(ids >= 0)
+    G = g.astype(np.float64)
+    P = q.astype(np.float64)
+    dd, y, x, s, (u, v, w), dp = ellipsoid_d(P, G[ids])
+    assert np.allclose(d.detach().cpu().numpy(), dd, rtol=1e-5, atol=1e-5)
+
+    # analytic FP64 gradient
+    out = dd > 0
+    nl = np.zeros_like(y)
+    nl[out] = (y[out] - x[out]) / dd[out, None]
+    nw = nl[:, 0:1] * u + nl[:, 1:2] * v + nl[:, 2:3] * w
+    ref_p = nw
+    ref_m = np.zeros((len(g), 3))
+    np.add.at(ref_m, ids, -nw)
+    ref_s = np.zeros((len(g), 3))
+    np.add.at(ref_s, ids, -nl * x / s)
+    gp = pts.grad.cpu().numpy().astype(np.float64)
+    gm = means.grad.cpu().numpy().astype(np.float64)
+    gs = scales.grad.cpu().numpy().astype(np.float64)
+    gr = rots.grad.cpu().numpy().astype(np.float64)
+    assert np.max(rel_err(gp, ref_p, 1e-3)) <= 1e-4
+    assert np.max(rel_err(gm, ref_m, 1e-3)) <= 1e-4
+    assert np.max(rel_err(gs, ref_s, 1e-3)) <= 1e-4
+
+    # finite differences on 1,000 random parameters of selected Gaussians
+    rng = np.random.default_rng(5)
+    used = np.unique(ids[dd > 0])
+    picks = rng.choice(used, size=1000, replace=True)
+    comps = rng.integers(0, 10, size=1000)
+    errs = []
+    for gi, c in zip(picks, comps):
+        rows = np.nonzero(ids == gi)[0]
+        def loss(delta):
+            G2 = np.repeat(G[gi:gi + 1], len(rows), 0)
+            G2[:, c] += delta
+            return ellipsoid_d(P[rows], G2)[0].sum()
+        fd = (loss(H) - loss(-H)) / (2 * H)
+        got = (gm[gi, c] if c < 3 else gr[gi, c - 3] if c < 7 else gs[gi, c - 7])
+        errs.append(rel_err(np.array([got]), np.array([fd]), 1e-3)[0])
+    errs = np.array(errs)
+    print(f"gaussian FD rel err: median {np.median(errs):.2e} p99 {np.percentile(errs, 99):.2e} "
+          f"max {errs.max():.2e}")
+    assert np.median(errs) <= 1e-4
+    assert np.percentile(errs, 99) <= 1e-2
+
+
+# ---------------------------------------------------------------------------------------
+# triangles: closest distance and ray t
+# ---------------------------------------------------------------------------------------
+def _terrain_mesh(grid):
+    tris = workloads.terrain(grid, 1)
+    verts, inv = np.unique(tris.reshape(-1, 3), axis=0, return_inverse=True)
+    return verts.astype(np.float32), inv.reshape(-1, 3).astype(np.int32)
+
+
+def test_triangle_distance_gradients(cuda):
+    import torch
+
+    import quarry.torch as qt
+
+    verts, idx = _terrain_mesh(48)
+    lo, hi = verts.min(0), verts.max(0)
+    q = workloads.uniform_points(6_000, lo - 2, hi + 2, 4, 31)
+    V = torch.tensor(verts, device="cuda", requires_grad=True)
+    I = torch.tensor(idx, device="cuda")
+    pts = torch.tensor(q, device="cuda", requires_grad=True)
+    d = qt.triangle_distance(pts, V, I)
+    d.sum().backward()
+    from quarry import capi
+
+    tree = capi.DeviceTree("tri", verts[idx].reshape(-1, 9))
+    ids = tree.closest(capi.to_device(q, np.float32)).cpu().numpy()[:, 1].astype(np.int64)
+    Vd = verts.astype(np.float64)
+    P = q.astype(np.float64)
+    a, b, c = Vd[idx[ids, 0]], Vd[idx[ids, 1]], Vd[idx[ids, 2]]
+    qp, wa, wb, wc = closest_tri(P, a, b, c)
+    dd = np.linalg.norm(P - qp, axis=-1)
+    n = (P - qp) / dd[:, None]
+    ref_v = np.zeros_like(Vd)
+    for k, wk in enumerate((wa, wb, wc)):
+        np.add.at(ref_v, idx[ids, k], -wk[:, None] * n)
+    gv = V.grad.cpu().numpy().astype(np.float64)
+    gp = pts.grad.cpu().numpy().astype(np.float64)
+    assert np.max(rel_err(gp, n, 1e-3)) <= 1e-4
+    assert np.max(rel_err(gv, ref_v, 1e-3)) <= 1e-4
+    # FD on 1,000 random vertex coordinates touched by the selection
+    rng = np.random.default_rng(6)
+    touched = np.unique(idx[ids].reshape(-1))
+    errs = []
+    for vi, comp in zip(rng.choice(touched, 1000), rng.integers(0, 3, 1000)):
+        rows = np.nonzero((idx[ids] == vi).any(axis=1))[0]
+        def loss(delta):
+            V2 = Vd.copy()
+            V2[vi, comp] += delta
+            tri = idx[ids[rows]]
+            qq, _, _, _ = closest_tri(P[rows], V2[tri[:, 0]], V2[tri[:, 1]], V2[tri[:, 2]])
+            return np.linalg.norm(P[rows] - qq, axis=-1).sum()
+        fd = (loss(H) - loss(-H)) / (2 * H)
+        errs.append(rel_err(np.array([gv[vi, comp]]), np.array([fd]), 1e-3)[0])
+    errs = np.array(errs)
+    print(f"triangle distance FD rel err: median {np.median(errs):.2e} "
+          f"p99 {np.percentile(errs, 99):.2e}")
+    assert np.median(errs) <= 1e-4
+    assert np.percentile(errs, 99) <= 1e-2
+
+
+def test_ray_t_gradients(cuda):
+    import torch
+
+    import quarry.torch as qt
+
+    verts, idx = _terrain_mesh(64)
+    lo, hi = verts.min(0), verts.max(0)
+    rays = workloads.down_rays(50_000, float(lo[0]), float(hi[0]), float(lo[1]), float(hi[1]),
+                               100.0, 7)
+    V = torch.tensor(verts, device="cuda", requires_grad=True)
+    I = torch.tensor(idx, device="cuda")
+    o = torch.tensor(rays[:, 0:3], device="cuda", requires_grad=True)
+    dvec = torch.tensor(rays[:, 3:6], device="cuda", requires_grad=True)
+    t, hit = qt.ray_hit_t(o, dvec, V, I)
+    assert bool(hit.all())
+    t.sum().backward()
+    from quarry import capi
+
+    tree = capi.DeviceTree("tri", verts[idx].reshape(-1, 9))
+    r8 = capi.to_device(rays, np.float32)
+    _, ids_t = tree.raycast_ids(r8)
+    ids = ids_t.cpu().numpy().astype(np.int64)
+    Vd = verts.astype(np.float64)
+    O, D = rays[:, 0:3].astype(np.float64), rays[:, 3:6].astype(np.float64)
+    a, b, c = Vd[idx[ids, 0]], Vd[idx[ids, 1]], Vd[idx[ids, 2]]
+    tt = ray_t(O, D, a, b, c)
+    assert np.allclose(t.detach().cpu().numpy(), tt, rtol=1e-5, atol=1e-4)
+    nrm = np.cross(b - a, c - a)
+    nd = (nrm * D).sum(-1)
+    h = O + D * tt[:, None]
+    nn = (nrm * nrm).sum(-1)
+    u = (np.cross(h - a, c - a) * nrm).sum(-1) / nn
+    v = (np.cross(b - a, h - a) * nrm).sum(-1) / nn
+    k = nrm / nd[:, None]
+    ref_v = np.zeros_like(Vd)
+    for j, wj in enumerate((1 - u - v, u, v)):
+        np.add.at(ref_v, idx[ids, j], wj[:, None] * k)
+    gv = V.grad.cpu().numpy().astype(np.float64)
+    assert np.max(rel_err(gv, ref_v, 1e-3)) <= 1e-4
+    assert np.max(rel_err(o.grad.cpu().numpy(), -k, 1e-3)) <= 1e-4
+    assert np.max(rel_err(dvec.grad.cpu().numpy(), -tt[:, None] * k, 1e-3)) <= 1e-4
+    rng = np.random.default_rng(8)
+    touched = np.unique(idx[ids].reshape(-1))
+    errs = []
+    for vi, comp in zip(rng.choice(touched, 1000), rng.integers(0, 3, 1000)):
+        rows = np.nonzero((idx[ids] == vi).any(axis=1))[0]
+        def loss(delta):
+            V2 = Vd.copy()
+            V2[vi, comp] += delta
+            tri = idx[ids[rows]]
+            return ray_t(O[rows], D[rows], V2[tri[:, 0]], V2[tri[:, 1]], V2[tri[:, 2]]).sum()
+        fd = (loss(H) - loss(-H)) / (2 * H)
+        errs.append(rel_err(np.array([gv[vi, comp]]), np.array([fd]), 1e-3)[0])
+    errs = np.array(errs)
+    print(f"ray t FD rel err: median {np.median(errs):.2e} p99 {np.percentile(errs, 99):.2e}")
+    assert np.median(errs) <= 1e-4
+    assert np.percentile(errs, 99) <= 1e-2
+
+
+def test_segment_sum_is_deterministic(cuda):
+    import torch
+
+    from quarry import capi
+
+    rng = np.random.default_rng(1)
+    keys = rng.integers(-1, 500, 200_000).astype(np.int32)
+    vals = rng.normal(size=(200_000, 3)).astype(np.float32)
+    kt = torch.tensor(keys, device="cuda")
+    vt = torch.tensor(vals, device="cuda")
+    a = capi.segment_sum(kt, vt, 500).cpu().numpy()
+    b = capi.segment_sum(kt, vt, 500).cpu().numpy()
+    assert a.tobytes() == b.tobytes()
+    ref = np.zeros((500, 3))
+    m = keys >= 0
+    np.add.at(ref, keys[m], vals[m].astype(np.float64))
+    assert np.allclose(a, ref, rtol=1e-5, atol=1e-4)

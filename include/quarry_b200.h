@@ -204,6 +204,17 @@ int qk_ray_t_grad(const qk_tree* tree, const void* items, const void* rays, cons
 int qk_segment_sum(const int32_t* keys, const float* values, int count, int channels, int segments,
                    float* out, void* workspace, size_t workspace_bytes, void* stream);
 
+/* Allocation-free first-hit rays (no counterpart in quarry).  For callers that cannot
+ * allocate device memory when they trace (a host that reserves all device memory up front and
+ * forbids later allocations, or code without an allocator): same results as qk_raycast with
+ * the same flags, but the Morton-order scratch lives in a fixed array inside this library
+ * (4.5 MB per GPU that loads it, held until exit), so no workspace is passed.  At most
+ * 262,144 rays per call; larger counts return QK_ERR_INVALID.  The first call on each device
+ * looks the array up (make it before any stream capture).  Calls share the array: calls that
+ * overlap on the GPU race. */
+int qk_raycast_noalloc(const qk_tree* tree, const void* rays, int count, uint64_t* out,
+                       unsigned flags, void* stream);
+
 /* Stable LSD radix sort of 32-bit keys with 32-bit values over the low `bits` bits.  All
  * four buffers hold n entries; the sorted result ends in keys_out / vals_out. */
 size_t qk_sort_workspace_bytes(int n);

@@ -72,6 +72,7 @@ EXPORTS = {
     "qk_distance_grad": (_I, [ctypes.POINTER(QkTree), _P, _P, _P, _P, _I, _P, _P, _P, _SZ, _P]),
     "qk_ray_t_grad": (_I, [ctypes.POINTER(QkTree), _P, _P, _P, _P, _I, _P, _P, _P, _SZ, _P]),
     "qk_segment_sum": (_I, [_P, _P, _I, _I, _I, _P, _P, _SZ, _P]),
+    "qk_raycast_noalloc": (_I, [ctypes.POINTER(QkTree), _P, _I, _P, _U, _P]),
     "qk_sort_pairs": (_I, [_P, _P, _P, _P, _I, _I, _P, _SZ, _P]),
 }
 

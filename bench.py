@@ -350,8 +350,10 @@ def main():
     q_d = capi.to_device(cfg.queries, np.float32)
     l2_flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
 
-    modes = {"bin": 0, "bin_morton": capi.QK_ORDER_MORTON, "wide": capi.QK_WIDE,
-             "wide_morton": capi.QK_WIDE | capi.QK_ORDER_MORTON}
+    dyn, occ, mort = capi.QK_TUNE_DYNAMIC, capi.QK_TUNE_HIGH_OCC, capi.QK_ORDER_MORTON
+    modes = {"bin": 0, "bin_morton": mort, "wide": capi.QK_WIDE,
+             "wide_morton": capi.QK_WIDE | mort, "bin_occ": occ, "bin_morton_occ": mort | occ,
+             "bin_dyn": dyn, "bin_morton_dyn": mort | dyn, "bin_morton_dyn_occ": mort | dyn | occ}
     variants = {f"{b}_{m}": (b, f) for b in trees for m, f in modes.items()}
     if args.only:
         variants = {args.only: variants[args.only]}
@@ -457,7 +459,8 @@ def main():
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": pk["hbm_gbs"],
                 "unit": "GB/s", "frac": round(achieved / pk["hbm_gbs"], 4),
                 "traffic": traffic, "peak_kind": pk_kind,
-                "kernel": "k_ray_wide" if trav_flags & capi.QK_WIDE else "k_ray_bin",
+                "kernel": ("k_ray_wide" if trav_flags & capi.QK_WIDE else
+                           "k_ray_bin_dyn" if trav_flags & capi.QK_TUNE_DYNAMIC else "k_ray_bin"),
                 "tree": best_builder,
                 "kernel_ms": round(kernel_ms, 4),
                 "bytes_per_ray": round(bytes_per_ray, 1),
@@ -480,28 +483,31 @@ def main():
         kt.append(e0.elapsed_time(e1))
     knn_ms = float(np.median(kt))
 
-    # ---- e2e through the C ABI from pinned host buffers ----
+    # ---- e2e through the C ABI from pinned host buffers: qk_raycast_host uploads, traces and
+    # reads back in chunks over two streams, all inside the timed region ----
     host_rays = torch.from_numpy(np.ascontiguousarray(cfg.rays)).pin_memory()
     host_out = torch.empty(nrays, dtype=torch.int64).pin_memory()
     dev_rays = torch.empty((nrays, 8), dtype=torch.float32, device=dev)
-    e2e_ws = torch.empty(capi.lib().qk_query_workspace_bytes(nrays, best_flags),
+    chunks = 8
+    e2e_ws = torch.empty(capi.lib().qk_raycast_host_workspace_bytes(nrays, chunks),
                          dtype=torch.uint8, device=dev)
+    s0, s1 = torch.cuda.Stream(), torch.cuda.Stream()
     for _ in range(3):
-        dev_rays.copy_(host_rays, non_blocking=True)
-        tree.raycast(dev_rays, best_flags, out=out, ws=e2e_ws)
-        host_out.copy_(out, non_blocking=True)
+        tree.raycast_host(host_rays, host_out, dev_rays, out, best_flags, chunks, (s0, s1), e2e_ws)
     torch.cuda.synchronize()
     e2e_t = []
     for _ in range(min(args.steps, 50)):
         l2_flush.zero_()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        dev_rays.copy_(host_rays, non_blocking=True)
-        tree.raycast(dev_rays, best_flags, out=out, ws=e2e_ws)
-        host_out.copy_(out, non_blocking=True)
-        e1.record()
         torch.cuda.synchronize()
-        e2e_t.append(e0.elapsed_time(e1))
+        e0 = torch.cuda.Event(enable_timing=True)
+        e0.record(s0)
+        s1.wait_event(e0)
+        tree.raycast_host(host_rays, host_out, dev_rays, out, best_flags, chunks, (s0, s1), e2e_ws)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s0)
+        b.record(s1)
+        torch.cuda.synchronize()
+        e2e_t.append(max(e0.elapsed_time(a), e0.elapsed_time(b)))
     e2e_ms = max_over_ranks(world, float(np.mean(e2e_t)))
     e2e_value = world * nrays / (e2e_ms * 1e-3) / 1e6
 
@@ -541,7 +547,8 @@ def main():
             "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
             "e2e": {"value": round(e2e_value, 2), "unit": "Mrays/s",
                     "h2d_bytes_per_step": int(cfg.rays.nbytes),
-                    "d2h_bytes_per_step": int(nrays * 8)},
+                    "d2h_bytes_per_step": int(nrays * 8),
+                    "path": f"qk_raycast_host, {chunks} chunks over 2 streams, pinned host buffers"},
             "gpu_launches": None,
         }
         # kernels of ours launched per timed step: keys + bounds + 4 sort passes x 5 + traversal

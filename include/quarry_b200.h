@@ -50,6 +50,9 @@ extern "C" {
 #define QK_ORDER_MORTON 1u       /* QueryOrder::Morton / RayOrder::Morton (origin keys) */
 #define QK_ORDER_DIRECTION 2u    /* RayOrder::MortonDirection (direction keys) */
 #define QK_WIDE 4u               /* traverse the 4-wide nodes */
+/* tuning flags (same results, different schedules; chosen by the autotuner) */
+#define QK_TUNE_DYNAMIC 256u     /* persistent warps fetching new rays as lanes finish */
+#define QK_TUNE_HIGH_OCC 512u    /* register cap for 5 resident blocks of 256 per SM */
 
 /*
  * Device arrays of one tree.  The caller allocates every array (sizes from qk_tree_bytes)
@@ -136,6 +139,18 @@ int qk_wide_build(qk_tree* tree, void* workspace, size_t workspace_bytes, void* 
  */
 int qk_raycast(const qk_tree* tree, const void* rays, int count, uint64_t* out, unsigned flags,
                uint64_t* stats, void* workspace, size_t workspace_bytes, void* stream);
+
+/* First-hit rays from host memory (the whole raycastGPU round trip, src/gpu/gpu_bvh.h:217-237):
+ * rays are uploaded, traced and read back in `chunks` pieces alternating between two streams,
+ * so uploads, traversal and read-backs of different pieces overlap.  host_rays / host_out
+ * should be pinned (page-locked) for the copies to be asynchronous; dev_rays (count rays)
+ * and dev_out (count results) are device buffers; the workspace holds two chunk
+ * workspaces.  Results equal qk_raycast's.  Work is enqueued on stream0 / stream1; the
+ * caller synchronises them before reading host_out. */
+size_t qk_raycast_host_workspace_bytes(int count, int chunks);
+int qk_raycast_host(const qk_tree* tree, const void* host_rays, int count, uint64_t* host_out,
+                    void* dev_rays, uint64_t* dev_out, int chunks, unsigned flags, void* workspace,
+                    size_t workspace_bytes, void* stream0, void* stream1);
 
 /* Closest primitive per query point (closestPointGPU / closestVertexGPU /
  * closestGaussianGPU, src/gpu/gpu_bvh.h:283-330).  points: count x 3 floats; out: count

@@ -209,6 +209,52 @@ int qk_raycast_ids(const qk_tree* tree, const void* rays, int count, uint64_t* o
     return ray_query(tree, rays, count, out, ids, flags, nullptr, workspace, as_stream(stream));
 }
 
+size_t qk_raycast_host_workspace_bytes(int count, int chunks) {
+    if (count <= 0) return 0;
+    if (chunks < 1) chunks = 1;
+    const int per = (count + chunks - 1) / chunks;
+    return 2 * ((order_ws_bytes(per) + 255) / 256 * 256);
+}
+
+int qk_raycast_host(const qk_tree* tree, const void* host_rays, int count, uint64_t* host_out,
+                    void* dev_rays, uint64_t* dev_out, int chunks, unsigned flags, void* workspace,
+                    size_t workspace_bytes, void* stream0, void* stream1) {
+    int st = check_tree(tree);
+    if (st) return st;
+    if (tree->kind != QK_TRI) return fail(QK_ERR_INVALID, "raycast needs a triangle tree");
+    if (count < 0) return fail(QK_ERR_INVALID, "negative ray count");
+    if (count == 0) return QK_OK;
+    if (!host_rays || !host_out || !dev_rays || !dev_out)
+        return fail(QK_ERR_INVALID, "a ray or result buffer is NULL");
+    if ((st = check_wide(tree, flags))) return st;
+    if (chunks < 1) chunks = 1;
+    if (chunks > count) chunks = count;
+    if ((st = check_ws(workspace, workspace_bytes, qk_raycast_host_workspace_bytes(count, chunks))))
+        return st;
+    const int per = (count + chunks - 1) / chunks;
+    const size_t half = (order_ws_bytes(per) + 255) / 256 * 256;
+    cudaStream_t ss[2] = {as_stream(stream0), as_stream(stream1)};
+    // chunk c runs on stream c % 2 with workspace half c % 2: its upload overlaps the other
+    // stream's traversal, its read-back the next upload (separate copy engines)
+    for (int c = 0; c < chunks; ++c) {
+        const int b = c * per;
+        const int m = b + per <= count ? per : count - b;
+        if (m <= 0) break;
+        cudaStream_t s = ss[c & 1];
+        void* ws = static_cast<char*>(workspace) + (c & 1) * half;
+        const char* hr = static_cast<const char*>(host_rays) + static_cast<size_t>(b) * 32;
+        char* dr = static_cast<char*>(dev_rays) + static_cast<size_t>(b) * 32;
+        cudaError_t e = cudaMemcpyAsync(dr, hr, static_cast<size_t>(m) * 32, cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess) return cuda_status(e, "ray upload");
+        st = ray_query(tree, dr, m, dev_out + b, nullptr, flags, nullptr, ws, s);
+        if (st) return st;
+        e = cudaMemcpyAsync(host_out + b, dev_out + b, static_cast<size_t>(m) * 8,
+                            cudaMemcpyDeviceToHost, s);
+        if (e != cudaSuccess) return cuda_status(e, "result read-back");
+    }
+    return QK_OK;
+}
+
 size_t qk_grad_workspace_bytes(int count, int channels) {
     return count > 0 ? grad_ws_bytes(count, channels < 10 ? 10 : channels) : 256;
 }

@@ -156,8 +156,8 @@ __device__ __forceinline__ void test_tri(const RayPre& R, const float4* __restri
     }
 }
 
-template <bool kStats>
-__global__ __launch_bounds__(kBlock) void k_ray_bin(const BNode* __restrict__ bn,
+template <bool kStats, int kMinBlocks>
+__global__ __launch_bounds__(kBlock, kMinBlocks) void k_ray_bin(const BNode* __restrict__ bn,
                                                    const float4* __restrict__ leaves,
                                                    const Node* __restrict__ nodes,
                                                    const float4* __restrict__ rays,
@@ -239,6 +239,126 @@ __global__ __launch_bounds__(kBlock) void k_ray_bin(const BNode* __restrict__ bn
         if (ids) ids[r] = best_id;
     }
     flush_stats<kStats>(active, ntests, ttests, overflow, stats);
+}
+
+// Persistent variant with dynamic ray fetching (Aila & Laine 2009): a fixed grid of warps
+// loops; each iteration every lane makes one traversal step, and lanes whose ray finished
+// take the next rays from a global counter (one atomic per warp per refill).  Same per-ray
+// algorithm and results as k_ray_bin; it removes the idle lanes that wait for the longest
+// ray of their warp.
+template <bool kStats, int kMinBlocks>
+__global__ __launch_bounds__(kBlock, kMinBlocks) void k_ray_bin_dyn(
+    const BNode* __restrict__ bn, const float4* __restrict__ leaves, const Node* __restrict__ nodes,
+    const float4* __restrict__ rays, const uint32_t* __restrict__ order, int count,
+    unsigned long long* __restrict__ out, int* __restrict__ ids, int* __restrict__ counter,
+    int max_iter, unsigned long long* __restrict__ stats) {
+    const int lane = threadIdx.x & 31;
+    const unsigned lower = (1u << lane) - 1u;
+    int ntests = 0, ttests = 0;
+    bool overflow = false;
+    int r = -1;
+    bool done = false;
+    RayPre R;
+    float best = 0.0f, bound = 0.0f;
+    bool any = false;
+    int best_id = -1;
+    int stack[kStack];
+    float stackT[kStack];
+    int sp = 0, node = 0, iters = 0;
+    const Box rb = root_box(nodes);
+    for (int guard = 0; guard < (1 << 30); ++guard) {
+        const bool need = r < 0 && !done;
+        const unsigned needm = __ballot_sync(0xffffffffu, need);
+        if (needm) {
+            const int leader = __ffs(needm) - 1;
+            int base = 0;
+            if (lane == leader) base = atomicAdd(counter, __popc(needm));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (need) {
+                const int k = base + __popc(needm & lower);
+                if (k >= count) {
+                    done = true;
+                } else {
+                    r = order ? static_cast<int>(order[k]) : k;
+                    R = prepare_ray(__ldg(rays + 2 * r), __ldg(rays + 2 * r + 1));
+                    best = R.tmax;
+                    bound = best * kMarginMul + kMarginAdd;
+                    any = false;
+                    best_id = -1;
+                    sp = 0;
+                    node = 0;
+                    iters = 0;
+                    float te;
+                    if (ray_box(R, rb.lo, rb.hi, bound, te)) {
+                        ++ntests;
+                    } else {
+                        out[r] = 0ull;
+                        if (ids) ids[r] = -1;
+                        r = -1;
+                    }
+                }
+            }
+        }
+        if (__all_sync(0xffffffffu, done)) break;
+        if (r < 0) continue;
+        // one traversal step of this lane's ray
+        bool finished = false;
+        if (++iters > max_iter) {
+            overflow = true;
+            finished = true;
+        } else {
+            float3 llo, lhi, rlo, rhi;
+            int lref, rref;
+            load_bnode(bn, node, llo, lhi, rlo, rhi, lref, rref);
+            float tl, tr;
+            bool hl = ray_box(R, llo, lhi, bound, tl);
+            bool hr = ray_box(R, rlo, rhi, bound, tr);
+            ntests += static_cast<int>(hl) + static_cast<int>(hr);
+            if (hl && lref < 0) {
+                ++ttests;
+                test_tri(R, leaves, ~lref, best, bound, any, best_id);
+                hl = false;
+            }
+            if (hr && rref < 0) {
+                ++ttests;
+                test_tri(R, leaves, ~rref, best, bound, any, best_id);
+                hr = false;
+            }
+            if (hl && hr) {
+                const bool lnear = tl <= tr;
+                if (sp >= kStack) {
+                    overflow = true;
+                    finished = true;
+                } else {
+                    stack[sp] = lnear ? rref : lref;
+                    stackT[sp] = lnear ? tr : tl;
+                    ++sp;
+                    node = lnear ? lref : rref;
+                }
+            } else if (hl) {
+                node = lref;
+            } else if (hr) {
+                node = rref;
+            } else {
+                const float limit = bound * kMarginMul + kMarginAdd;
+                node = -1;
+                while (sp > 0) {
+                    --sp;
+                    if (!(stackT[sp] > limit)) {
+                        node = stack[sp];
+                        break;
+                    }
+                }
+                if (node < 0) finished = true;
+            }
+        }
+        if (finished) {
+            out[r] = any ? ((1ull << 32) | static_cast<unsigned long long>(__float_as_uint(best))) : 0ull;
+            if (ids) ids[r] = best_id;
+            r = -1;
+        }
+    }
+    flush_stats<kStats>(true, ntests, ttests, overflow, stats);
 }
 
 __device__ __forceinline__ void load_wide_entry(const WideNode* __restrict__ w, int node, int s,
@@ -1132,11 +1252,33 @@ int ray_query(const qk_tree* t, const void* rays, int count, uint64_t* out, int*
         const WideNode* wn = static_cast<const WideNode*>(t->wide);
         if (stt) k_ray_wide<true><<<g, kBlock, 0, s>>>(wn, leaves, r4, order, count, res, ids, t->n * 2 + 64, stt);
         else k_ray_wide<false><<<g, kBlock, 0, s>>>(wn, leaves, r4, order, count, res, ids, t->n * 2 + 64, stt);
+    } else if (flags & QK_TUNE_DYNAMIC) {
+        const BNode* bn = static_cast<const BNode*>(t->bnodes);
+        const Node* nodes = static_cast<const Node*>(t->nodes);
+        cudaMemsetAsync(&o.h->counter, 0, sizeof(int), s);
+        int sms = 148;
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const bool occ = (flags & QK_TUNE_HIGH_OCC) != 0;
+        const int grid = min(blocks_for(count), sms * (occ ? 5 : 4));
+        if (occ) {
+            if (stt) k_ray_bin_dyn<true, 5><<<grid, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, ids, &o.h->counter, t->n * 2 + 64, stt);
+            else k_ray_bin_dyn<false, 5><<<grid, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, ids, &o.h->counter, t->n * 2 + 64, stt);
+        } else {
+            if (stt) k_ray_bin_dyn<true, 4><<<grid, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, ids, &o.h->counter, t->n * 2 + 64, stt);
+            else k_ray_bin_dyn<false, 4><<<grid, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, ids, &o.h->counter, t->n * 2 + 64, stt);
+        }
     } else {
         const BNode* bn = static_cast<const BNode*>(t->bnodes);
         const Node* nodes = static_cast<const Node*>(t->nodes);
-        if (stt) k_ray_bin<true><<<g, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, ids, t->n * 2 + 64, stt);
-        else k_ray_bin<false><<<g, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, ids, t->n * 2 + 64, stt);
+        if (flags & QK_TUNE_HIGH_OCC) {
+            if (stt) k_ray_bin<true, 5><<<g, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, ids, t->n * 2 + 64, stt);
+            else k_ray_bin<false, 5><<<g, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, ids, t->n * 2 + 64, stt);
+        } else {
+            if (stt) k_ray_bin<true, 1><<<g, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, ids, t->n * 2 + 64, stt);
+            else k_ray_bin<false, 1><<<g, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, ids, t->n * 2 + 64, stt);
+        }
     }
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? QK_OK : cuda_status(e, "raycast");

@@ -21,6 +21,7 @@ QK_OK = 0
 QK_TRI, QK_POINT, QK_GAUSS = 0, 1, 2
 QK_BUILD_LBVH, QK_BUILD_SAH = 0, 1
 QK_ORDER_MORTON, QK_ORDER_DIRECTION, QK_WIDE = 1, 2, 4
+QK_TUNE_DYNAMIC, QK_TUNE_HIGH_OCC = 256, 512
 KINDS = {"tri": QK_TRI, "point": QK_POINT, "gauss": QK_GAUSS}
 STRIDE = {QK_TRI: 9, QK_POINT: 3, QK_GAUSS: 10}
 
@@ -73,6 +74,8 @@ EXPORTS = {
     "qk_ray_t_grad": (_I, [ctypes.POINTER(QkTree), _P, _P, _P, _P, _I, _P, _P, _P, _SZ, _P]),
     "qk_segment_sum": (_I, [_P, _P, _I, _I, _I, _P, _P, _SZ, _P]),
     "qk_raycast_noalloc": (_I, [ctypes.POINTER(QkTree), _P, _I, _P, _U, _P]),
+    "qk_raycast_host_workspace_bytes": (_SZ, [_I, _I]),
+    "qk_raycast_host": (_I, [ctypes.POINTER(QkTree), _P, _I, _P, _P, _P, _I, _U, _P, _SZ, _P, _P]),
     "qk_sort_pairs": (_I, [_P, _P, _P, _P, _I, _I, _P, _SZ, _P]),
 }
 
@@ -261,6 +264,21 @@ class DeviceTree:
         check(lib().qk_raycast(ctypes.byref(self.t), _ptr(rays), count, _ptr(out), flags,
                                _ptr(stats), _ptr(w), w.numel(), _stream()), "qk_raycast")
         return out
+
+    def raycast_host(self, host_rays, host_out, dev_rays, dev_out, flags: int = 0,
+                     chunks: int = 8, streams=None, ws=None):
+        """Pipelined host -> device -> host ray query over two streams (pinned buffers)."""
+        torch = _torch()
+        count = host_rays.shape[0]
+        if streams is None:
+            streams = (torch.cuda.Stream(), torch.cuda.Stream())
+        if ws is None:
+            ws = self.ws.get(lib().qk_raycast_host_workspace_bytes(count, chunks))
+        check(lib().qk_raycast_host(ctypes.byref(self.t), _ptr(host_rays), count, _ptr(host_out),
+                                    _ptr(dev_rays), _ptr(dev_out), chunks, flags, _ptr(ws),
+                                    ws.numel(), ctypes.c_void_p(streams[0].cuda_stream),
+                                    ctypes.c_void_p(streams[1].cuda_stream)), "qk_raycast_host")
+        return streams
 
     def raycast_ids(self, rays, flags: int = 0):
         """First hits with the hit primitive (scene index, -1 on a miss)."""

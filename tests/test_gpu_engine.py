@@ -320,3 +320,44 @@ def test_sah_city_large(cuda):
     assert tree.validate() == [0] * 8
     got = tree.raycast(_dev(rays)).cpu().numpy().view(np.uint64)
     assert np.array_equal(got, ref.raycast(rays))
+
+
+def test_raycast_host_pipeline_matches(cuda):
+    tris = scenes()["city"]
+    lo, hi = workloads.bounds_of(tris)
+    tree = capi.DeviceTree("tri", tris, builder="sah")
+    rays = workloads.cosine_rays(70_001, float(lo[0]), float(hi[0]), float(lo[1]), float(hi[1]),
+                                 float(hi[2]) + 5.0, 3)
+    want = tree.raycast(_dev(rays), capi.QK_ORDER_MORTON).cpu().numpy().view(np.uint64)
+    host_rays = cuda.from_numpy(rays).pin_memory()
+    for chunks in (1, 3, 8):
+        host_out = cuda.zeros(len(rays), dtype=cuda.int64).pin_memory()
+        dev_rays = cuda.empty((len(rays), 8), dtype=cuda.float32, device="cuda")
+        dev_out = cuda.empty(len(rays), dtype=cuda.int64, device="cuda")
+        tree.raycast_host(host_rays, host_out, dev_rays, dev_out, capi.QK_ORDER_MORTON, chunks)
+        cuda.cuda.synchronize()
+        assert np.array_equal(host_out.numpy().view(np.uint64), want)
+
+
+@pytest.mark.parametrize("tune", ["dyn", "occ", "dyn_occ"])
+@pytest.mark.parametrize("morton", [False, True])
+def test_raycast_tuning_flags_same_bits(cuda, tune, morton):
+    tris = scenes()["city"]
+    lo, hi = workloads.bounds_of(tris)
+    tree = capi.DeviceTree("tri", tris, builder="sah")
+    rays = workloads.cosine_rays(50_003, float(lo[0]), float(hi[0]), float(lo[1]), float(hi[1]),
+                                 float(hi[2]) + 5.0, 11)
+    flags = {"dyn": capi.QK_TUNE_DYNAMIC, "occ": capi.QK_TUNE_HIGH_OCC,
+             "dyn_occ": capi.QK_TUNE_DYNAMIC | capi.QK_TUNE_HIGH_OCC}[tune]
+    if morton:
+        flags |= capi.QK_ORDER_MORTON
+    rd = _dev(rays)
+    want, want_ids = tree.raycast_ids(rd, 0)
+    got, got_ids = tree.raycast_ids(rd, flags)
+    assert cuda.equal(got, want) and cuda.equal(got_ids, want_ids)
+    stats = cuda.zeros(4, dtype=cuda.int64, device="cuda")
+    tree.raycast(rd, flags, stats=stats)
+    base = cuda.zeros(4, dtype=cuda.int64, device="cuda")
+    tree.raycast(rd, 0, stats=base)
+    # same traversal per ray: identical node and triangle test counts
+    assert stats[:3].tolist() == base[:3].tolist()

@@ -237,6 +237,84 @@ int qk_sort_pairs(const uint32_t* keys_in, const uint32_t* vals_in, uint32_t* ke
                   uint32_t* vals_out, int n, int bits, void* workspace, size_t workspace_bytes,
                   void* stream);
 
+/*
+ * ---- Batched scenes (new; quarry has no batched API) ----
+ * A batch holds `scenes` trees of ONE primitive kind whose inputs are concatenated in one
+ * device array (scene s starts at item counts[0] + ... + counts[s-1]).  Every tree lives in
+ * a caller-allocated arena and is an ordinary qk_tree (qk_batch_tree), so every single-tree
+ * call above works on it too.  Under the batched schedule each phase of the build and of a
+ * query is ONE launch over all scenes; queries run persistent warps that take 32-query chunks
+ * of any scene from a shared counter (work stealing).  qk_batch_build and qk_batch_query
+ * with schedule QK_SCHEDULE_BATCHED only enqueue kernels and memsets, so a whole build +
+ * query sequence can be captured in one CUDA graph; qk_batch_create, qk_batch_sync,
+ * qk_batch_plan_create and qk_batch_plan_status synchronize.  QK_SCHEDULE_LOOP runs the same
+ * work as a per-scene loop over the single-tree calls (qk_build, qk_raycast, ...), with their
+ * per-scene synchronizations: the comparison schedule.  Results are bit-identical between
+ * the two schedules and to the single-tree calls.
+ */
+typedef struct qk_batch qk_batch;            /* opaque host object */
+typedef struct qk_batch_plan qk_batch_plan;  /* opaque host object */
+
+#define QK_SCHEDULE_BATCHED 0u
+#define QK_SCHEDULE_LOOP 1u
+
+#define QK_OP_RAY 0
+#define QK_OP_CLOSEST 1
+#define QK_OP_KNN 2
+#define QK_OP_RADIUS 3
+
+/* Launch shape of the persistent query kernels (chosen by the autotuner). */
+typedef struct qk_batch_tune {
+    int32_t block;          /* threads per block: 64, 128 or 256 */
+    int32_t blocks_per_sm;  /* persistent grid = SMs x blocks_per_sm (1..16) */
+    int32_t short_stack;    /* stack entries per thread held in shared memory (0..32) */
+    int32_t chunks_per_fetch; /* 32-query chunks a warp takes per counter fetch (1..64) */
+} qk_batch_tune;
+
+/* flags: QK_WIDE reserves and builds the 4-wide nodes of every scene. */
+size_t qk_batch_arena_bytes(int kind, const int32_t* counts, int scenes, unsigned flags);
+int qk_batch_create(qk_batch** out, int kind, const int32_t* counts, int scenes,
+                    const void* items, void* arena, size_t arena_bytes, unsigned flags,
+                    void* stream);
+/* Builds every scene's LBVH (and 4-wide nodes when created with QK_WIDE). */
+int qk_batch_build(qk_batch* batch, unsigned schedule, void* stream);
+/* Waits for the stream, reads every scene's depth / wide-node count back into its tree and
+ * reports QK_ERR_DEPTH when a scene is too deep for the traversal stack. */
+int qk_batch_sync(qk_batch* batch, void* stream);
+int qk_batch_tree(const qk_batch* batch, int scene, qk_tree* out);
+int qk_batch_scenes(const qk_batch* batch);
+void qk_batch_destroy(qk_batch* batch);
+
+/* A query plan: per-scene query counts of one operation (concatenated by scene in the
+ * inputs and outputs) and, for QK_OP_RADIUS, the per-scene radius (host floats).
+ * flags: QK_ORDER_MORTON (scene-major Morton order of the inputs, within each scene's
+ * bounds) and QK_WIDE (traverse the 4-wide nodes). */
+size_t qk_batch_plan_bytes(const qk_batch* batch, int op, const int32_t* counts,
+                           unsigned flags);
+int qk_batch_plan_create(qk_batch_plan** out, const qk_batch* batch, int op,
+                         const int32_t* counts, const float* params, void* mem, size_t bytes,
+                         unsigned flags, void* stream);
+typedef struct qk_batch_io {
+    const void* input;  /* rays (8 floats) or points (3 floats), device, concatenated by scene */
+    void* out;          /* RAY: uint64 per ray (qk_raycast layout); CLOSEST: 8 B per point;
+                           KNN: k x 8 B per point; RADIUS: uint64 keys, `capacity` entries */
+    int32_t* offsets;   /* RADIUS: CSR offsets into out, queries + scenes + 1 entries; batched
+                           schedule: one global CSR in the first queries + 1; loop schedule:
+                           scene s's own CSR (from 0) at offsets[q_begin(s) + s], its keys at
+                           out + (sum of earlier scenes' totals) */
+    int64_t capacity;   /* RADIUS: keys that fit in out */
+    int32_t k;          /* KNN: 1..32 */
+    int32_t pad;
+} qk_batch_io;
+int qk_batch_query(qk_batch_plan* plan, const qk_batch_io* io, const qk_batch_tune* tune,
+                   unsigned schedule, void* stream);
+/* Waits for the stream; radius_total: keys of the last radius query (-1 otherwise);
+ * overflows: traversals stopped by a stack or iteration limit.  QK_ERR_WORKSPACE when the
+ * radius keys exceeded the capacity (nothing was written past it). */
+int qk_batch_plan_status(qk_batch_plan* plan, int64_t* radius_total, int64_t* overflows,
+                         void* stream);
+void qk_batch_plan_destroy(qk_batch_plan* plan);
+
 #ifdef __cplusplus
 }
 #endif

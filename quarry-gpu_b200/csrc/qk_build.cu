@@ -18,26 +18,11 @@
 #include <cstdio>
 
 #include "qk_internal.cuh"
+#include "qk_build.cuh"
 
 namespace qk {
 
 namespace {
-
-__device__ __forceinline__ uint32_t spread10(uint32_t v) {
-    v &= 0x3ffu;
-    v = (v | (v << 16)) & 0x030000ffu;
-    v = (v | (v << 8)) & 0x0300f00fu;
-    v = (v | (v << 4)) & 0x030c30c3u;
-    v = (v | (v << 2)) & 0x09249249u;
-    return v;
-}
-
-// quantize (lbvh.cu:285-290): (v - lo) / extent * 1023 + 0.5, clamped, truncated
-__device__ __forceinline__ uint32_t quant(float v, float lo, float extent) {
-    if (extent <= 0.0f) return 0;
-    const float q = (v - lo) / extent * 1023.0f + 0.5f;
-    return static_cast<uint32_t>(static_cast<int>(fminf(1023.0f, fmaxf(0.0f, q))));
-}
 
 __global__ void k_header_init(Header* h) {
     if (threadIdx.x < 3) {
@@ -121,26 +106,6 @@ __global__ __launch_bounds__(kBlock) void k_morton(const float* __restrict__ ite
     idx[i] = static_cast<uint32_t>(i);
 }
 
-// 64-bit key of slot j: (code << 32) | scene index
-__device__ __forceinline__ uint64_t key64(const uint32_t* codes, const uint32_t* ids, int j) {
-    return (static_cast<uint64_t>(codes[j]) << 32) | ids[j];
-}
-
-// common-prefix length of keys a and b; -1 outside [0, n)
-__device__ __forceinline__ int cpl(const uint32_t* codes, const uint32_t* ids, int n, uint64_t ka,
-                                   int b) {
-    if (b < 0 || b >= n) return -1;
-    const uint64_t x = ka ^ key64(codes, ids, b);
-    return x == 0 ? 64 : __clzll(x);
-}
-
-__device__ __forceinline__ void write_box(Node* nd, Box b) {
-    float4* p = reinterpret_cast<float4*>(nd);
-    const float4 a = p[1];
-    p[0] = make_float4(b.lo.x, b.lo.y, b.lo.z, b.hi.x);
-    p[1] = make_float4(b.hi.y, b.hi.z, a.z, a.w);
-}
-
 template <class Ops>
 __global__ __launch_bounds__(kBlock) void k_emit(
     const float* __restrict__ items, int n, const uint32_t* __restrict__ codes,
@@ -149,103 +114,17 @@ __global__ __launch_bounds__(kBlock) void k_emit(
     BNode* __restrict__ bnodes, float4* __restrict__ leaves, int* __restrict__ flags) {
     const int k = blockIdx.x * kBlock + threadIdx.x;
     if (k >= n) return;
-    // leaf k
-    const int src = static_cast<int>(ids[k]);
-    float it[Ops::kFloats];
-#pragma unroll
-    for (int j = 0; j < Ops::kFloats; ++j) it[j] = items[static_cast<size_t>(src) * Ops::kFloats + j];
-#pragma unroll
-    for (int j = 0; j < Ops::kFloats; ++j) sorted[static_cast<size_t>(k) * Ops::kFloats + j] = it[j];
-    prim_ids[k] = src;
-    slot_of[src] = k;
-    const Box b = Ops::bounds(it);
-    float4* leafnode = reinterpret_cast<float4*>(nodes + (n - 1 + k));
-    leafnode[0] = make_float4(b.lo.x, b.lo.y, b.lo.z, b.hi.x);
-    leafnode[1] = make_float4(b.hi.y, b.hi.z, __int_as_float(-(k + 1)), __int_as_float(1));
-    float4 pay[Ops::kVec4];
-    Ops::pack(it, src, pay);
-#pragma unroll
-    for (int j = 0; j < Ops::kVec4; ++j) leaves[static_cast<size_t>(k) * Ops::kVec4 + j] = pay[j];
-    if (k == 0) parent[0] = -1;
-    if (k >= n - 1) return;
-
-    // internal node k (Karras 2012): direction, range end by exponential + binary search,
-    // then the split as the last index whose prefix with the first exceeds the node's
-    const uint64_t kk = key64(codes, ids, k);
-    const int dir = cpl(codes, ids, n, kk, k + 1) > cpl(codes, ids, n, kk, k - 1) ? 1 : -1;
-    const int dmin = cpl(codes, ids, n, kk, k - dir);
-    int lmax = 2;
-    while (cpl(codes, ids, n, kk, k + lmax * dir) > dmin) lmax *= 2;
-    int l = 0;
-    for (int t = lmax / 2; t > 0; t /= 2) {
-        if (cpl(codes, ids, n, kk, k + (l + t) * dir) > dmin) l += t;
-    }
-    const int j = k + l * dir;
-    const int first = min(k, j), last = max(k, j);
-    const int dnode = cpl(codes, ids, n, kk, j);
-    const uint64_t kf = key64(codes, ids, first);
-    int split = first;
-    int step = last - first;
-    do {
-        step = (step + 1) >> 1;
-        const int cand = split + step;
-        if (cand < last && cpl(codes, ids, n, kf, cand) > dnode) split = cand;
-    } while (step > 1);
-    const int left = split == first ? (n - 1 + split) : split;
-    const int right = split + 1 == last ? (n - 1 + split + 1) : split + 1;
-    nodes[k].left = left;
-    nodes[k].right = right;
-    parent[left] = k;
-    parent[right] = k;
-    const int lref = left >= n - 1 ? ~(left - (n - 1)) : left;
-    const int rref = right >= n - 1 ? ~(right - (n - 1)) : right;
-    bnodes[k].v3 = make_float4(__int_as_float(lref), __int_as_float(rref), 0.0f, 0.0f);
-    flags[k] = 0;
+    emit_slot<Ops>(items, n, codes, ids, nodes, sorted, prim_ids, slot_of, parent, bnodes, leaves, flags, k);
 }
 
-__device__ __forceinline__ Box load_box_cg(const Node* nd) {
-    const float4* p = reinterpret_cast<const float4*>(nd);
-    const float4 a = __ldcg(p), b = __ldcg(p + 1);
-    Box bx;
-    bx.lo = f3(a.x, a.y, a.z);
-    bx.hi = f3(a.w, b.x, b.y);
-    return bx;
-}
-
-// Complete internal node p from its two (final) children: canonical box + traversal node.
-__device__ __forceinline__ void finish_node(Node* __restrict__ nodes, BNode* __restrict__ bnodes,
-                                            int p) {
-    const int l = nodes[p].left, r = nodes[p].right;
-    const Box a = load_box_cg(nodes + l);
-    const Box b = load_box_cg(nodes + r);
-    Box u;
-    u.lo = f3(fmin_t(a.lo.x, b.lo.x), fmin_t(a.lo.y, b.lo.y), fmin_t(a.lo.z, b.lo.z));
-    u.hi = f3(fmax_t(a.hi.x, b.hi.x), fmax_t(a.hi.y, b.hi.y), fmax_t(a.hi.z, b.hi.z));
-    write_box(nodes + p, u);
-    BNode& bn = bnodes[p];
-    bn.v0 = make_float4(a.lo.x, a.lo.y, a.lo.z, a.hi.x);
-    bn.v1 = make_float4(a.hi.y, a.hi.z, b.lo.x, b.lo.y);
-    bn.v2 = make_float4(b.lo.z, b.hi.x, b.hi.y, b.hi.z);
-}
-
-// One thread per leaf climbs toward the root; flags[p] counts arrivals at internal node p.
-// The second arrival finishes p (both children final), resets the counter and continues.
+// One thread per leaf climbs toward the root (climb in qk_build.cuh).
 __global__ __launch_bounds__(kBlock) void k_bottom_up(Node* __restrict__ nodes,
                                                      BNode* __restrict__ bnodes,
                                                      const int* __restrict__ parent,
                                                      int* __restrict__ flags, int n) {
     const int k = blockIdx.x * kBlock + threadIdx.x;
     if (k >= n) return;
-    int p = parent[n - 1 + k];
-    int guard = 0;
-    while (p >= 0 && guard++ < 4096) {
-        __threadfence();
-        if (atomicAdd(&flags[p], 1) == 0) return;
-        __threadfence();
-        finish_node(nodes, bnodes, p);
-        flags[p] = 0;
-        p = parent[p];
-    }
+    climb(nodes, bnodes, parent, flags, n, k);
 }
 
 // depth = length of the parent chain (lbvh.cu:419-431); bounded by the node count
@@ -254,11 +133,7 @@ __global__ __launch_bounds__(kBlock) void k_depth(const int* __restrict__ parent
     const int i = blockIdx.x * kBlock + threadIdx.x;
     int d = 0;
     if (i < count) {
-        int p = i;
-        while (p > 0 && d < count) {
-            p = parent[p];
-            ++d;
-        }
+        d = chain_depth(parent, i, count);
         depth[i] = d;
     }
 #pragma unroll
@@ -367,42 +242,6 @@ __global__ __launch_bounds__(kBlock) void k_wide_flags(const int* __restrict__ d
                                                       int* __restrict__ flags) {
     const int i = blockIdx.x * kBlock + threadIdx.x;
     if (i < m) flags[i] = (depth[i] & 1) == 0 ? 1 : 0;
-}
-
-__device__ __forceinline__ void wide_fill(WideEntry& e, const Node& src, int child) {
-    e.mn[0] = src.mn[0];
-    e.mn[1] = src.mn[1];
-    e.mn[2] = src.mn[2];
-    e.mx[0] = src.mx[0];
-    e.mx[1] = src.mx[1];
-    e.mx[2] = src.mx[2];
-    e.child = child;
-    e.pad = 0;
-}
-
-__device__ void wide_node_of(const Node* __restrict__ nodes, int n, const int* __restrict__ wide_id,
-                             int i, WideNode& out) {
-#pragma unroll
-    for (int s = 0; s < 4; ++s) {
-        out.c[s].mn[0] = out.c[s].mn[1] = out.c[s].mn[2] = kInf;
-        out.c[s].mx[0] = out.c[s].mx[1] = out.c[s].mx[2] = -kInf;
-        out.c[s].child = kEmptySlot;
-        out.c[s].pad = 0;
-    }
-    const int kids[2] = {nodes[i].left, nodes[i].right};
-    int slot = 0;
-    for (int k = 0; k < 2; ++k) {
-        const int c = kids[k];
-        if (c >= n - 1) {
-            wide_fill(out.c[slot++], nodes[c], nodes[c].left);
-            continue;
-        }
-        const int g[2] = {nodes[c].left, nodes[c].right};
-        for (int j = 0; j < 2; ++j) {
-            const int gc = g[j];
-            wide_fill(out.c[slot++], nodes[gc], gc >= n - 1 ? nodes[gc].left : wide_id[gc]);
-        }
-    }
 }
 
 __global__ __launch_bounds__(kBlock) void k_wide_emit(const Node* __restrict__ nodes, int n,

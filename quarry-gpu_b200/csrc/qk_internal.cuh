@@ -101,6 +101,10 @@ int radius_count(const qk_tree* t, const float* pts, int count, float r, int* of
                  long long* total, unsigned flags, uint64_t* stats, void* ws, cudaStream_t s);
 int radius_fill(const qk_tree* t, const float* pts, int count, float r, const int* offsets,
                 uint64_t* keys, unsigned flags, void* ws, cudaStream_t s);
+// sorts every CSR segment [offsets[q], offsets[q+1]) of keys ascending; medium / large hold
+// count ints each; cap >= 0 skips the sort when offsets[count] > cap
+int radius_sort_segments(const int* offsets, int count, uint64_t* keys, int* medium, int* large,
+                         Header* h, long long cap, cudaStream_t s);
 
 // ---- adjoints (qk_grad.cu) ----
 size_t grad_ws_bytes(int count, int channels);

@@ -14,6 +14,7 @@
 // of the inputs: the sorted permutation is handed to the traversal, thread i works on item
 // order[i] and writes its result in place.
 #include "qk_internal.cuh"
+#include "qk_traverse.cuh"
 
 namespace qk {
 
@@ -92,70 +93,8 @@ __global__ __launch_bounds__(kBlock) void k_pos_keys(const float* __restrict__ p
 }
 
 // ---------------------------------------------------------------------------------------
-// statistics: warp-aggregated counters (src/gpu/raycast.cu:147-156)
+// single-tree kernels: one thread per ray / query point, bodies in qk_traverse.cuh
 // ---------------------------------------------------------------------------------------
-template <bool kStats>
-__device__ __forceinline__ void flush_stats(bool active, int nodes, int leaves, bool overflow,
-                                            unsigned long long* stats) {
-    if (stats == nullptr) return;
-    const unsigned mask = __ballot_sync(0xffffffffu, active);
-    const unsigned ovf = __ballot_sync(0xffffffffu, overflow);
-    if (kStats) {
-        const int sn = __reduce_add_sync(0xffffffffu, nodes);
-        const int sl = __reduce_add_sync(0xffffffffu, leaves);
-        if ((threadIdx.x & 31) == 0 && mask) {
-            if (sn) atomicAdd(stats + 0, static_cast<unsigned long long>(sn));
-            if (sl) atomicAdd(stats + 1, static_cast<unsigned long long>(sl));
-        }
-    }
-    if ((threadIdx.x & 31) == 0 && ovf) atomicAdd(stats + 2, static_cast<unsigned long long>(__popc(ovf)));
-}
-
-__device__ __forceinline__ void load_bnode(const BNode* __restrict__ bn, int i, float3& llo,
-                                           float3& lhi, float3& rlo, float3& rhi, int& lref,
-                                           int& rref) {
-    const float4* p = reinterpret_cast<const float4*>(bn + i);
-    const float4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2), d = __ldg(p + 3);
-    llo = f3(a.x, a.y, a.z);
-    lhi = f3(a.w, b.x, b.y);
-    rlo = f3(b.z, b.w, c.x);
-    rhi = f3(c.y, c.z, c.w);
-    lref = __float_as_int(d.x);
-    rref = __float_as_int(d.y);
-}
-
-__device__ __forceinline__ Box root_box(const Node* __restrict__ nodes) {
-    const float4* p = reinterpret_cast<const float4*>(nodes);
-    const float4 a = __ldg(p), b = __ldg(p + 1);
-    Box bx;
-    bx.lo = f3(a.x, a.y, a.z);
-    bx.hi = f3(a.w, b.x, b.y);
-    return bx;
-}
-
-// ---------------------------------------------------------------------------------------
-// rays
-// ---------------------------------------------------------------------------------------
-// Leaf test.  The first hit is taken even at t == tMax (the CPU reference accepts t <= tMax,
-// src/cpu/bvh.cpp:156-168); later hits only when closer.  Among hits at the same t the
-// smallest scene index is kept, so the reported primitive does not depend on visit order.
-__device__ __forceinline__ void test_tri(const RayPre& R, const float4* __restrict__ leaves,
-                                         int slot, float& best, float& bound, bool& any,
-                                         int& best_id) {
-    const float4 a = __ldg(leaves + 3 * slot), b = __ldg(leaves + 3 * slot + 1),
-                 c = __ldg(leaves + 3 * slot + 2);
-    float t;
-    if (ray_tri(R, f3(a.x, a.y, a.z), f3(b.x, b.y, b.z), f3(c.x, c.y, c.z), t)) {
-        const int id = __float_as_int(a.w);
-        if (!any || t < best || (t == best && id < best_id)) {
-            best = t;
-            bound = best * kMarginMul + kMarginAdd;
-            any = true;
-            best_id = id;
-        }
-    }
-}
-
 template <bool kStats, int kMinBlocks>
 __global__ __launch_bounds__(kBlock, kMinBlocks) void k_ray_bin(const BNode* __restrict__ bn,
                                                    const float4* __restrict__ leaves,
@@ -167,78 +106,16 @@ __global__ __launch_bounds__(kBlock, kMinBlocks) void k_ray_bin(const BNode* __r
                                                    int max_iter, unsigned long long* __restrict__ stats) {
     const int i = blockIdx.x * kBlock + threadIdx.x;
     const bool active = i < count;
-    int ntests = 0, ttests = 0;
-    bool overflow = false;
+    Trav tv;
     if (active) {
         const int r = order ? static_cast<int>(order[i]) : i;
         const RayPre R = prepare_ray(__ldg(rays + 2 * r), __ldg(rays + 2 * r + 1));
-        float best = R.tmax;
-        float bound = best * kMarginMul + kMarginAdd;
-        bool any = false;
-        int best_id = -1;
-        const Box rb = root_box(nodes);
-        float te;
-        if (ray_box(R, rb.lo, rb.hi, bound, te)) {
-            ++ntests;
-            int stack[kStack];
-            float stackT[kStack];
-            int sp = 0;
-            int node = 0;
-            for (int iter = 0;; ++iter) {
-                if (iter >= max_iter) {
-                    overflow = true;
-                    break;
-                }
-                float3 llo, lhi, rlo, rhi;
-                int lref, rref;
-                load_bnode(bn, node, llo, lhi, rlo, rhi, lref, rref);
-                float tl, tr;
-                bool hl = ray_box(R, llo, lhi, bound, tl);
-                bool hr = ray_box(R, rlo, rhi, bound, tr);
-                ntests += static_cast<int>(hl) + static_cast<int>(hr);
-                if (hl && lref < 0) {
-                    ++ttests;
-                    test_tri(R, leaves, ~lref, best, bound, any, best_id);
-                    hl = false;
-                }
-                if (hr && rref < 0) {
-                    ++ttests;
-                    test_tri(R, leaves, ~rref, best, bound, any, best_id);
-                    hr = false;
-                }
-                if (hl && hr) {
-                    const bool lnear = tl <= tr;
-                    if (sp >= kStack) {
-                        overflow = true;
-                        break;
-                    }
-                    stack[sp] = lnear ? rref : lref;
-                    stackT[sp] = lnear ? tr : tl;
-                    ++sp;
-                    node = lnear ? lref : rref;
-                } else if (hl) {
-                    node = lref;
-                } else if (hr) {
-                    node = rref;
-                } else {
-                    // pop the next entry whose box could still hold a closer hit
-                    const float limit = bound * kMarginMul + kMarginAdd;
-                    node = -1;
-                    while (sp > 0) {
-                        --sp;
-                        if (!(stackT[sp] > limit)) {
-                            node = stack[sp];
-                            break;
-                        }
-                    }
-                    if (node < 0) break;
-                }
-            }
-        }
-        out[r] = any ? ((1ull << 32) | static_cast<unsigned long long>(__float_as_uint(best))) : 0ull;
+        LocalStack<kStack> st;
+        int best_id;
+        out[r] = ray_bin_one(bn, leaves, root_box(nodes), R, max_iter, st, tv, best_id);
         if (ids) ids[r] = best_id;
     }
-    flush_stats<kStats>(active, ntests, ttests, overflow, stats);
+    flush_stats<kStats>(active, tv.nodes, tv.leaves, tv.overflow, stats);
 }
 
 // Persistent variant with dynamic ray fetching (Aila & Laine 2009): a fixed grid of warps
@@ -361,15 +238,6 @@ __global__ __launch_bounds__(kBlock, kMinBlocks) void k_ray_bin_dyn(
     flush_stats<kStats>(true, ntests, ttests, overflow, stats);
 }
 
-__device__ __forceinline__ void load_wide_entry(const WideNode* __restrict__ w, int node, int s,
-                                                float3& lo, float3& hi, int& child) {
-    const float4* p = reinterpret_cast<const float4*>(w + node) + 2 * s;
-    const float4 a = __ldg(p), b = __ldg(p + 1);
-    lo = f3(a.x, a.y, a.z);
-    hi = f3(a.w, b.x, b.y);
-    child = __float_as_int(b.z);
-}
-
 template <bool kStats>
 __global__ __launch_bounds__(kBlock) void k_ray_wide(const WideNode* __restrict__ wn,
                                                     const float4* __restrict__ leaves,
@@ -380,103 +248,16 @@ __global__ __launch_bounds__(kBlock) void k_ray_wide(const WideNode* __restrict_
                                                     int max_iter, unsigned long long* __restrict__ stats) {
     const int i = blockIdx.x * kBlock + threadIdx.x;
     const bool active = i < count;
-    int ntests = 0, ttests = 0;
-    bool overflow = false;
+    Trav tv;
     if (active) {
         const int r = order ? static_cast<int>(order[i]) : i;
         const RayPre R = prepare_ray(__ldg(rays + 2 * r), __ldg(rays + 2 * r + 1));
-        float best = R.tmax;
-        float bound = best * kMarginMul + kMarginAdd;
-        bool any = false;
-        int best_id = -1;
-        int stack[kStackWide];
-        float stackT[kStackWide];
-        int sp = 0;
-        int node = 0;  // the 4-wide root has no single box; start inside it (raycast.cu:182)
-        for (int iter = 0;; ++iter) {
-                if (iter >= max_iter) {
-                    overflow = true;
-                    break;
-                }
-            int child[4];
-            float key[4];
-            int hits = 0;
-#pragma unroll
-            for (int s = 0; s < 4; ++s) {
-                float3 lo, hi;
-                int c;
-                load_wide_entry(wn, node, s, lo, hi, c);
-                float t;
-                if (c != kEmptySlot && ray_box(R, lo, hi, bound, t)) {
-                    ++ntests;
-                    int j = hits++;
-                    while (j > 0 && key[j - 1] > t) {
-                        key[j] = key[j - 1];
-                        child[j] = child[j - 1];
-                        --j;
-                    }
-                    key[j] = t;
-                    child[j] = c;
-                }
-            }
-            // leaves now, nearest first; internal children pushed far-first
-            int next = -1;
-            float nextT = 0.0f;
-            for (int j = 0; j < hits; ++j) {
-                if (child[j] < 0) {
-                    ++ttests;
-                    test_tri(R, leaves, ~child[j], best, bound, any, best_id);
-                }
-            }
-            for (int j = hits - 1; j >= 0; --j) {
-                if (child[j] < 0) continue;
-                if (next >= 0) {
-                    if (sp >= kStackWide) {
-                        overflow = true;
-                        break;
-                    }
-                    stack[sp] = next;
-                    stackT[sp] = nextT;
-                    ++sp;
-                }
-                next = child[j];
-                nextT = key[j];
-            }
-            if (overflow) break;
-            // `next` is the nearest internal child; the loop above pushed the farther ones
-            if (next >= 0) {
-                node = next;
-                continue;
-            }
-            const float limit = bound * kMarginMul + kMarginAdd;
-            node = -1;
-            while (sp > 0) {
-                --sp;
-                if (!(stackT[sp] > limit)) {
-                    node = stack[sp];
-                    break;
-                }
-            }
-            if (node < 0) break;
-        }
-        out[r] = any ? ((1ull << 32) | static_cast<unsigned long long>(__float_as_uint(best))) : 0ull;
+        LocalStack<kStackWide> st;
+        int best_id;
+        out[r] = ray_wide_one(wn, leaves, R, max_iter, st, tv, best_id);
         if (ids) ids[r] = best_id;
     }
-    flush_stats<kStats>(active, ntests, ttests, overflow, stats);
-}
-
-// ---------------------------------------------------------------------------------------
-// closest
-// ---------------------------------------------------------------------------------------
-template <class Ops>
-__device__ __forceinline__ void leaf_closest(float3 p, const float4* __restrict__ leaves, int slot,
-                                             float& best, int& best_id) {
-    int id;
-    const float d2 = Ops::dist2(p, leaves, slot, id);
-    if (best_id < 0 || closer(d2, id, best, best_id)) {
-        best = d2;
-        best_id = id;
-    }
+    flush_stats<kStats>(active, tv.nodes, tv.leaves, tv.overflow, stats);
 }
 
 template <class Ops, bool kStats>
@@ -488,70 +269,14 @@ __global__ __launch_bounds__(kBlock) void k_closest_bin(const BNode* __restrict_
                                                        int max_iter, unsigned long long* __restrict__ stats) {
     const int i = blockIdx.x * kBlock + threadIdx.x;
     const bool active = i < count;
-    int ntests = 0, ltests = 0;
-    bool overflow = false;
+    Trav tv;
     if (active) {
         const int q = order ? static_cast<int>(order[i]) : i;
         const float3 p = f3(pts[3 * q], pts[3 * q + 1], pts[3 * q + 2]);
-        float best = kInf;
-        int best_id = -1;
-        int stack[kStack];
-        float stackD[kStack];
-        int sp = 0;
-        int node = 0;
-        for (int iter = 0;; ++iter) {
-                if (iter >= max_iter) {
-                    overflow = true;
-                    break;
-                }
-            ++ntests;
-            float3 llo, lhi, rlo, rhi;
-            int lref, rref;
-            load_bnode(bn, node, llo, lhi, rlo, rhi, lref, rref);
-            const float dl = dist2_box(p, llo, lhi);
-            const float dr = dist2_box(p, rlo, rhi);
-            bool okl = best_id < 0 || dl <= best;
-            bool okr = best_id < 0 || dr <= best;
-            // leaves in near-first order so the second sees the tighter bound
-            const bool lfirst = dl <= dr;
-            if (lfirst) {
-                if (okl && lref < 0) { ++ltests; leaf_closest<Ops>(p, leaves, ~lref, best, best_id); okl = false; }
-                if (okr && rref < 0 && (best_id < 0 || dr <= best)) { ++ltests; leaf_closest<Ops>(p, leaves, ~rref, best, best_id); }
-                if (rref < 0) okr = false;
-            } else {
-                if (okr && rref < 0) { ++ltests; leaf_closest<Ops>(p, leaves, ~rref, best, best_id); okr = false; }
-                if (okl && lref < 0 && (best_id < 0 || dl <= best)) { ++ltests; leaf_closest<Ops>(p, leaves, ~lref, best, best_id); }
-                if (lref < 0) okl = false;
-            }
-            if (okl && okr) {
-                if (sp >= kStack) {
-                    overflow = true;
-                    break;
-                }
-                stack[sp] = lfirst ? rref : lref;
-                stackD[sp] = lfirst ? dr : dl;
-                ++sp;
-                node = lfirst ? lref : rref;
-            } else if (okl) {
-                node = lref;
-            } else if (okr) {
-                node = rref;
-            } else {
-                node = -1;
-                while (sp > 0) {
-                    --sp;
-                    if (best_id < 0 || stackD[sp] <= best) {
-                        node = stack[sp];
-                        break;
-                    }
-                }
-                if (node < 0) break;
-            }
-        }
-        out[q] = best_id >= 0 ? make_uint2(__float_as_uint(best), static_cast<unsigned>(best_id))
-                              : make_uint2(0u, 0xffffffffu);
+        LocalStack<kStack> st;
+        out[q] = closest_bin_one<Ops>(bn, leaves, p, max_iter, st, tv);
     }
-    flush_stats<kStats>(active, ntests, ltests, overflow, stats);
+    flush_stats<kStats>(active, tv.nodes, tv.leaves, tv.overflow, stats);
 }
 
 template <class Ops, bool kStats>
@@ -563,154 +288,14 @@ __global__ __launch_bounds__(kBlock) void k_closest_wide(const WideNode* __restr
                                                         int max_iter, unsigned long long* __restrict__ stats) {
     const int i = blockIdx.x * kBlock + threadIdx.x;
     const bool active = i < count;
-    int ntests = 0, ltests = 0;
-    bool overflow = false;
+    Trav tv;
     if (active) {
         const int q = order ? static_cast<int>(order[i]) : i;
         const float3 p = f3(pts[3 * q], pts[3 * q + 1], pts[3 * q + 2]);
-        float best = kInf;
-        int best_id = -1;
-        int stack[kStackWide];
-        float stackD[kStackWide];
-        int sp = 0;
-        int node = 0;
-        for (int iter = 0;; ++iter) {
-                if (iter >= max_iter) {
-                    overflow = true;
-                    break;
-                }
-            int child[4];
-            float key[4];
-            int hits = 0;
-#pragma unroll
-            for (int s = 0; s < 4; ++s) {
-                float3 lo, hi;
-                int c;
-                load_wide_entry(wn, node, s, lo, hi, c);
-                if (c == kEmptySlot) continue;
-                const float d = dist2_box(p, lo, hi);
-                if (best_id >= 0 && d > best) continue;
-                ++ntests;
-                int j = hits++;
-                while (j > 0 && key[j - 1] > d) {
-                    key[j] = key[j - 1];
-                    child[j] = child[j - 1];
-                    --j;
-                }
-                key[j] = d;
-                child[j] = c;
-            }
-            for (int j = 0; j < hits; ++j) {
-                if (child[j] < 0 && (best_id < 0 || key[j] <= best)) {
-                    ++ltests;
-                    leaf_closest<Ops>(p, leaves, ~child[j], best, best_id);
-                }
-            }
-            int next = -1;
-            float nextD = 0.0f;
-            for (int j = hits - 1; j >= 0; --j) {
-                if (child[j] < 0) continue;
-                if (best_id >= 0 && key[j] > best) continue;
-                if (next >= 0) {
-                    if (sp >= kStackWide) {
-                        overflow = true;
-                        break;
-                    }
-                    stack[sp] = next;
-                    stackD[sp] = nextD;
-                    ++sp;
-                }
-                next = child[j];
-                nextD = key[j];
-            }
-            if (overflow) break;
-            if (next >= 0) {
-                node = next;
-                continue;
-            }
-            node = -1;
-            while (sp > 0) {
-                --sp;
-                if (best_id < 0 || stackD[sp] <= best) {
-                    node = stack[sp];
-                    break;
-                }
-            }
-            if (node < 0) break;
-        }
-        out[q] = best_id >= 0 ? make_uint2(__float_as_uint(best), static_cast<unsigned>(best_id))
-                              : make_uint2(0u, 0xffffffffu);
+        LocalStack<kStackWide> st;
+        out[q] = closest_wide_one<Ops>(wn, leaves, p, max_iter, st, tv);
     }
-    flush_stats<kStats>(active, ntests, ltests, overflow, stats);
-}
-
-// ---------------------------------------------------------------------------------------
-// kNN: the k best (dist2, id) pairs stay sorted in registers (unrolled insertion over a
-// compile-time capacity K >= k).  Empty slots hold (+inf, INT_MAX), so "strictly closer than
-// the k-th" is one comparison whether or not the table is full -- the reference's max-heap
-// replacement rule (src/cpu/bvh.cpp:284-299, src/gpu/query.cu:145-158).
-// ---------------------------------------------------------------------------------------
-template <int K>
-struct KnnTable {
-    float d[K];
-    int id[K];
-    float kd;  // dist2 of entry k-1 (the pruning threshold)
-    int kid;
-
-    __device__ __forceinline__ void init() {
-#pragma unroll
-        for (int j = 0; j < K; ++j) {
-            d[j] = kInf;
-            id[j] = 0x7fffffff;
-        }
-        kd = kInf;
-        kid = 0x7fffffff;
-    }
-    __device__ __forceinline__ void insert(float xd, int xid, int k) {
-        if (!closer(xd, xid, kd, kid)) return;
-#pragma unroll
-        for (int j = K - 1; j > 0; --j) {
-            const bool shift = closer(xd, xid, d[j - 1], id[j - 1]);
-            const bool place = !shift && closer(xd, xid, d[j], id[j]);
-            const float nd = shift ? d[j - 1] : (place ? xd : d[j]);
-            const int ni = shift ? id[j - 1] : (place ? xid : id[j]);
-            d[j] = nd;
-            id[j] = ni;
-        }
-        if (closer(xd, xid, d[0], id[0])) {
-            d[0] = xd;
-            id[0] = xid;
-        }
-#pragma unroll
-        for (int j = 0; j < K; ++j) {
-            if (j == k - 1) {
-                kd = d[j];
-                kid = id[j];
-            }
-        }
-    }
-    // prune test for a subtree bound: keep while the table is not full or bound <= k-th
-    __device__ __forceinline__ bool admits(float bound) const { return kid == 0x7fffffff || bound <= kd; }
-};
-
-template <class Ops, int K>
-__device__ __forceinline__ void leaf_knn(float3 p, const float4* __restrict__ leaves, int slot,
-                                         KnnTable<K>& tab, int k) {
-    int id;
-    const float d2 = Ops::dist2(p, leaves, slot, id);
-    tab.insert(d2, id, k);
-}
-
-template <int K>
-__device__ __forceinline__ void write_knn(const KnnTable<K>& tab, int k, uint2* __restrict__ dst) {
-#pragma unroll
-    for (int j = 0; j < K; ++j) {
-        if (j < k) {
-            const bool valid = tab.id[j] != 0x7fffffff;
-            dst[j] = valid ? make_uint2(__float_as_uint(tab.d[j]), static_cast<unsigned>(tab.id[j]))
-                           : make_uint2(0u, 0xffffffffu);
-        }
-    }
+    flush_stats<kStats>(active, tv.nodes, tv.leaves, tv.overflow, stats);
 }
 
 template <class Ops, int K, bool kStats>
@@ -722,68 +307,16 @@ __global__ __launch_bounds__(kBlock) void k_knn_bin(const BNode* __restrict__ bn
                                                    int max_iter, unsigned long long* __restrict__ stats) {
     const int i = blockIdx.x * kBlock + threadIdx.x;
     const bool active = i < count;
-    int ntests = 0, ltests = 0;
-    bool overflow = false;
+    Trav tv;
     if (active) {
         const int q = order ? static_cast<int>(order[i]) : i;
         const float3 p = f3(pts[3 * q], pts[3 * q + 1], pts[3 * q + 2]);
+        LocalStack<kStack> st;
         KnnTable<K> tab;
-        tab.init();
-        int stack[kStack];
-        float stackD[kStack];
-        int sp = 0;
-        int node = 0;
-        for (int iter = 0;; ++iter) {
-                if (iter >= max_iter) {
-                    overflow = true;
-                    break;
-                }
-            ++ntests;
-            float3 llo, lhi, rlo, rhi;
-            int lref, rref;
-            load_bnode(bn, node, llo, lhi, rlo, rhi, lref, rref);
-            const float dl = dist2_box(p, llo, lhi);
-            const float dr = dist2_box(p, rlo, rhi);
-            const bool lfirst = dl <= dr;
-            bool okl = tab.admits(dl);
-            bool okr = tab.admits(dr);
-            if (lfirst) {
-                if (okl && lref < 0) { ++ltests; leaf_knn<Ops, K>(p, leaves, ~lref, tab, k); okl = false; }
-                if (okr && rref < 0 && tab.admits(dr)) { ++ltests; leaf_knn<Ops, K>(p, leaves, ~rref, tab, k); }
-                if (rref < 0) okr = false;
-            } else {
-                if (okr && rref < 0) { ++ltests; leaf_knn<Ops, K>(p, leaves, ~rref, tab, k); okr = false; }
-                if (okl && lref < 0 && tab.admits(dl)) { ++ltests; leaf_knn<Ops, K>(p, leaves, ~lref, tab, k); }
-                if (lref < 0) okl = false;
-            }
-            if (okl && okr) {
-                if (sp >= kStack) {
-                    overflow = true;
-                    break;
-                }
-                stack[sp] = lfirst ? rref : lref;
-                stackD[sp] = lfirst ? dr : dl;
-                ++sp;
-                node = lfirst ? lref : rref;
-            } else if (okl) {
-                node = lref;
-            } else if (okr) {
-                node = rref;
-            } else {
-                node = -1;
-                while (sp > 0) {
-                    --sp;
-                    if (tab.admits(stackD[sp])) {
-                        node = stack[sp];
-                        break;
-                    }
-                }
-                if (node < 0) break;
-            }
-        }
+        knn_bin_one<Ops, K>(bn, leaves, p, k, max_iter, st, tv, tab);
         write_knn<K>(tab, k, out + static_cast<size_t>(q) * stride);
     }
-    flush_stats<kStats>(active, ntests, ltests, overflow, stats);
+    flush_stats<kStats>(active, tv.nodes, tv.leaves, tv.overflow, stats);
 }
 
 template <class Ops, int K, bool kStats>
@@ -795,90 +328,19 @@ __global__ __launch_bounds__(kBlock) void k_knn_wide(const WideNode* __restrict_
                                                     int max_iter, unsigned long long* __restrict__ stats) {
     const int i = blockIdx.x * kBlock + threadIdx.x;
     const bool active = i < count;
-    int ntests = 0, ltests = 0;
-    bool overflow = false;
+    Trav tv;
     if (active) {
         const int q = order ? static_cast<int>(order[i]) : i;
         const float3 p = f3(pts[3 * q], pts[3 * q + 1], pts[3 * q + 2]);
+        LocalStack<kStackWide> st;
         KnnTable<K> tab;
-        tab.init();
-        int stack[kStackWide];
-        float stackD[kStackWide];
-        int sp = 0;
-        int node = 0;
-        for (int iter = 0;; ++iter) {
-                if (iter >= max_iter) {
-                    overflow = true;
-                    break;
-                }
-            int child[4];
-            float key[4];
-            int hits = 0;
-#pragma unroll
-            for (int s = 0; s < 4; ++s) {
-                float3 lo, hi;
-                int c;
-                load_wide_entry(wn, node, s, lo, hi, c);
-                if (c == kEmptySlot) continue;
-                const float d = dist2_box(p, lo, hi);
-                if (!tab.admits(d)) continue;
-                ++ntests;
-                int j = hits++;
-                while (j > 0 && key[j - 1] > d) {
-                    key[j] = key[j - 1];
-                    child[j] = child[j - 1];
-                    --j;
-                }
-                key[j] = d;
-                child[j] = c;
-            }
-            for (int j = 0; j < hits; ++j) {
-                if (child[j] < 0 && tab.admits(key[j])) {
-                    ++ltests;
-                    leaf_knn<Ops, K>(p, leaves, ~child[j], tab, k);
-                }
-            }
-            int next = -1;
-            float nextD = 0.0f;
-            for (int j = hits - 1; j >= 0; --j) {
-                if (child[j] < 0 || !tab.admits(key[j])) continue;
-                if (next >= 0) {
-                    if (sp >= kStackWide) {
-                        overflow = true;
-                        break;
-                    }
-                    stack[sp] = next;
-                    stackD[sp] = nextD;
-                    ++sp;
-                }
-                next = child[j];
-                nextD = key[j];
-            }
-            if (overflow) break;
-            if (next >= 0) {
-                node = next;
-                continue;
-            }
-            node = -1;
-            while (sp > 0) {
-                --sp;
-                if (tab.admits(stackD[sp])) {
-                    node = stack[sp];
-                    break;
-                }
-            }
-            if (node < 0) break;
-        }
+        knn_wide_one<Ops, K>(wn, leaves, p, k, max_iter, st, tv, tab);
         write_knn<K>(tab, k, out + static_cast<size_t>(q) * stride);
     }
-    flush_stats<kStats>(active, ntests, ltests, overflow, stats);
+    flush_stats<kStats>(active, tv.nodes, tv.leaves, tv.overflow, stats);
 }
 
-// ---------------------------------------------------------------------------------------
-// radius: count, then fill at the scanned offsets, then sort every segment by (dist2, id).
-// Rule of src/gpu/query.cu:415-540: a box is entered when its squared distance <= r2, a
-// primitive kept when its dist2 <= r2.
-// ---------------------------------------------------------------------------------------
+// radius: count, then fill at the scanned offsets, then sort every segment by (dist2, id)
 template <class Ops, bool kFill, bool kStats>
 __global__ __launch_bounds__(kBlock) void k_radius_bin(
     const BNode* __restrict__ bn, const float4* __restrict__ leaves, const Node* __restrict__ nodes,
@@ -887,70 +349,18 @@ __global__ __launch_bounds__(kBlock) void k_radius_bin(
     unsigned long long* __restrict__ keys, int max_iter, unsigned long long* __restrict__ stats) {
     const int i = blockIdx.x * kBlock + threadIdx.x;
     const bool active = i < count;
-    int ntests = 0, ltests = 0;
-    bool overflow = false;
+    Trav tv;
     if (active) {
         const int q = order ? static_cast<int>(order[i]) : i;
         const float3 p = f3(pts[3 * q], pts[3 * q + 1], pts[3 * q + 2]);
-        int found = 0;
-        int write = kFill ? offsets[q] : 0;
+        const int write = kFill ? offsets[q] : 0;
         const int end = kFill ? offsets[q + 1] : 0;  // never write past this query's segment
-        const Box rb = root_box(nodes);
-        if (dist2_box(p, rb.lo, rb.hi) <= r2) {
-            int stack[kStack];
-            int sp = 0;
-            int node = 0;
-            for (int iter = 0;; ++iter) {
-                if (iter >= max_iter) {
-                    overflow = true;
-                    break;
-                }
-                ++ntests;
-                float3 llo, lhi, rlo, rhi;
-                int lref, rref;
-                load_bnode(bn, node, llo, lhi, rlo, rhi, lref, rref);
-                bool okl = dist2_box(p, llo, lhi) <= r2;
-                bool okr = dist2_box(p, rlo, rhi) <= r2;
-                if (okl && lref < 0) {
-                    ++ltests;
-                    int id;
-                    const float d2 = Ops::dist2(p, leaves, ~lref, id);
-                    if (d2 <= r2) {
-                        if (kFill && write < end) keys[write++] = (static_cast<unsigned long long>(__float_as_uint(d2)) << 32) | static_cast<unsigned>(id);
-                        ++found;
-                    }
-                    okl = false;
-                }
-                if (okr && rref < 0) {
-                    ++ltests;
-                    int id;
-                    const float d2 = Ops::dist2(p, leaves, ~rref, id);
-                    if (d2 <= r2) {
-                        if (kFill && write < end) keys[write++] = (static_cast<unsigned long long>(__float_as_uint(d2)) << 32) | static_cast<unsigned>(id);
-                        ++found;
-                    }
-                    okr = false;
-                }
-                if (okl && okr) {
-                    if (sp >= kStack) {
-                        overflow = true;
-                        break;
-                    }
-                    stack[sp++] = rref;
-                    node = lref;
-                } else if (okl) {
-                    node = lref;
-                } else if (okr) {
-                    node = rref;
-                } else {
-                    if (sp == 0) break;
-                    node = stack[--sp];
-                }
-            }
-        }
+        LocalStack<kStack> st;
+        const int found = radius_bin_one<Ops, kFill>(bn, leaves, root_box(nodes), p, r2, write,
+                                                     end, keys, max_iter, st, tv);
         if (!kFill) counts[q] = found;
     }
-    flush_stats<kStats>(active, ntests, ltests, overflow, stats);
+    flush_stats<kStats>(active, tv.nodes, tv.leaves, tv.overflow, stats);
 }
 
 template <class Ops, bool kFill, bool kStats>
@@ -961,57 +371,18 @@ __global__ __launch_bounds__(kBlock) void k_radius_wide(
     unsigned long long* __restrict__ keys, int max_iter, unsigned long long* __restrict__ stats) {
     const int i = blockIdx.x * kBlock + threadIdx.x;
     const bool active = i < count;
-    int ntests = 0, ltests = 0;
-    bool overflow = false;
+    Trav tv;
     if (active) {
         const int q = order ? static_cast<int>(order[i]) : i;
         const float3 p = f3(pts[3 * q], pts[3 * q + 1], pts[3 * q + 2]);
-        int found = 0;
-        int write = kFill ? offsets[q] : 0;
-        const int end = kFill ? offsets[q + 1] : 0;  // never write past this query's segment
-        int stack[kStackWide];
-        int sp = 0;
-        int node = 0;
-        for (int iter = 0;; ++iter) {
-                if (iter >= max_iter) {
-                    overflow = true;
-                    break;
-                }
-            int next = -1;
-#pragma unroll
-            for (int s = 0; s < 4; ++s) {
-                float3 lo, hi;
-                int c;
-                load_wide_entry(wn, node, s, lo, hi, c);
-                if (c == kEmptySlot || !(dist2_box(p, lo, hi) <= r2)) continue;
-                ++ntests;
-                if (c < 0) {
-                    ++ltests;
-                    int id;
-                    const float d2 = Ops::dist2(p, leaves, ~c, id);
-                    if (d2 <= r2) {
-                        if (kFill && write < end) keys[write++] = (static_cast<unsigned long long>(__float_as_uint(d2)) << 32) | static_cast<unsigned>(id);
-                        ++found;
-                    }
-                } else if (next < 0) {
-                    next = c;
-                } else if (sp < kStackWide) {
-                    stack[sp++] = c;
-                } else {
-                    overflow = true;
-                }
-            }
-            if (overflow) break;
-            if (next >= 0) {
-                node = next;
-            } else {
-                if (sp == 0) break;
-                node = stack[--sp];
-            }
-        }
+        const int write = kFill ? offsets[q] : 0;
+        const int end = kFill ? offsets[q + 1] : 0;
+        LocalStack<kStackWide> st;
+        const int found = radius_wide_one<Ops, kFill>(wn, leaves, p, r2, write, end, keys,
+                                                      max_iter, st, tv);
         if (!kFill) counts[q] = found;
     }
-    flush_stats<kStats>(active, ntests, ltests, overflow, stats);
+    flush_stats<kStats>(active, tv.nodes, tv.leaves, tv.overflow, stats);
 }
 
 // ---- segment sort of the radius keys ----
@@ -1029,14 +400,16 @@ __device__ __forceinline__ void cswap(unsigned long long* a, int i, int j, int m
 }
 
 // one warp per segment of up to 32 keys, in registers
+// (cap >= 0: nothing is sorted when the keys overran a buffer of cap entries)
 __global__ __launch_bounds__(kBlock) void k_seg_sort_warp(const int* __restrict__ offsets, int count,
                                                          unsigned long long* __restrict__ keys,
                                                          int* __restrict__ medium,
                                                          int* __restrict__ large,
-                                                         Header* __restrict__ h) {
+                                                         Header* __restrict__ h, long long cap) {
     const int lane = threadIdx.x & 31;
     const int q = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
     if (q >= count) return;
+    if (cap >= 0 && offsets[count] > cap) return;
     const int b = offsets[q];
     const int m = offsets[q + 1] - b;
     if (m <= 1) return;
@@ -1374,11 +747,17 @@ int radius_fill(const qk_tree* t, const float* pts, int count, float r, const in
     st = radius_dispatch<true>(t, pts, count, r * r, nullptr, offsets, k64, flags, nullptr, order, s);
     if (st != QK_OK) return st;
     // reset the segment lists (make_order only resets them on its Morton path)
-    k_bounds_reset<<<1, 32, 0, s>>>(o.h, 0);
+    return radius_sort_segments(offsets, count, keys, medium, large, o.h, -1, s);
+}
+
+int radius_sort_segments(const int* offsets, int count, uint64_t* keys, int* medium, int* large,
+                         Header* h, long long cap, cudaStream_t s) {
+    auto* k64 = reinterpret_cast<unsigned long long*>(keys);
+    k_bounds_reset<<<1, 32, 0, s>>>(h, 0);
     k_seg_sort_warp<<<blocks_for(count, kBlock / 32), kBlock, 0, s>>>(offsets, count, k64, medium,
-                                                                      large, o.h);
-    k_seg_sort_block<true><<<148 * 2, kBlock, 0, s>>>(offsets, k64, medium, o.h, 0);
-    k_seg_sort_block<false><<<148, kBlock, 0, s>>>(offsets, k64, large, o.h, 1);
+                                                                      large, h, cap);
+    k_seg_sort_block<true><<<148 * 2, kBlock, 0, s>>>(offsets, k64, medium, h, 0);
+    k_seg_sort_block<false><<<148, kBlock, 0, s>>>(offsets, k64, large, h, 1);
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? QK_OK : cuda_status(e, "radius sort");
 }

@@ -1,0 +1,760 @@
+// qk_traverse.cuh -- per-query stack traversals shared by the single-tree kernels
+// (qk_query.cu) and the batched persistent kernels (qk_batch.cu).
+//
+// Each function runs one ray or query point through one tree to completion.  Binary nodes
+// are 64-byte BNodes (both child boxes inline, four 16-byte loads); 4-wide nodes are 128-byte
+// WideNodes.  Pruning follows the reference's rules exactly: the slab test with its 1e-6
+// margins for rays, "bound <= best" for closest / kNN, "dist2 <= r2" for radius
+// (src/gpu/raycast.cu:100-139, src/gpu/query.cu:74-116, 415-540), so every result is
+// independent of tree shape and visit order.
+//
+// The stack is a template policy: LocalStack keeps every entry in local memory (the
+// single-tree kernels), SplitStack keeps the first `sh` entries of every thread in shared
+// memory (entry e of thread t at base[e * stride + t], conflict-free) and the rest in local
+// memory -- the short-stack depth the batch autotuner chooses at run time.
+#pragma once
+
+#include "qk_internal.cuh"
+
+namespace qk {
+
+struct Trav {
+    int nodes = 0;
+    int leaves = 0;
+    bool overflow = false;
+};
+
+template <int kCap>
+struct LocalStack {
+    static constexpr int kSize = kCap;
+    int node[kCap];
+    float key[kCap];
+    __device__ __forceinline__ void put(int i, int n, float k) {
+        node[i] = n;
+        key[i] = k;
+    }
+    __device__ __forceinline__ void put_node(int i, int n) { node[i] = n; }
+    __device__ __forceinline__ int get_node(int i) const { return node[i]; }
+    __device__ __forceinline__ float get_key(int i) const { return key[i]; }
+};
+
+template <int kCap>
+struct SplitStack {
+    static constexpr int kSize = kCap;
+    int* snode;   // this thread's column of the shared-memory part
+    float* skey;
+    int sh;       // entries kept in shared memory
+    int stride;   // threads per block
+    int node[kCap];
+    float key[kCap];
+    __device__ __forceinline__ void put(int i, int n, float k) {
+        if (i < sh) {
+            snode[i * stride] = n;
+            skey[i * stride] = k;
+        } else {
+            node[i] = n;
+            key[i] = k;
+        }
+    }
+    __device__ __forceinline__ void put_node(int i, int n) {
+        if (i < sh) snode[i * stride] = n;
+        else node[i] = n;
+    }
+    __device__ __forceinline__ int get_node(int i) const { return i < sh ? snode[i * stride] : node[i]; }
+    __device__ __forceinline__ float get_key(int i) const { return i < sh ? skey[i * stride] : key[i]; }
+};
+
+// ---------------------------------------------------------------------------------------
+// node and leaf loads
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ void load_bnode(const BNode* __restrict__ bn, int i, float3& llo,
+                                           float3& lhi, float3& rlo, float3& rhi, int& lref,
+                                           int& rref) {
+    const float4* p = reinterpret_cast<const float4*>(bn + i);
+    const float4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2), d = __ldg(p + 3);
+    llo = f3(a.x, a.y, a.z);
+    lhi = f3(a.w, b.x, b.y);
+    rlo = f3(b.z, b.w, c.x);
+    rhi = f3(c.y, c.z, c.w);
+    lref = __float_as_int(d.x);
+    rref = __float_as_int(d.y);
+}
+
+__device__ __forceinline__ Box root_box(const Node* __restrict__ nodes) {
+    const float4* p = reinterpret_cast<const float4*>(nodes);
+    const float4 a = __ldg(p), b = __ldg(p + 1);
+    Box bx;
+    bx.lo = f3(a.x, a.y, a.z);
+    bx.hi = f3(a.w, b.x, b.y);
+    return bx;
+}
+
+__device__ __forceinline__ void load_wide_entry(const WideNode* __restrict__ w, int node, int s,
+                                                float3& lo, float3& hi, int& child) {
+    const float4* p = reinterpret_cast<const float4*>(w + node) + 2 * s;
+    const float4 a = __ldg(p), b = __ldg(p + 1);
+    lo = f3(a.x, a.y, a.z);
+    hi = f3(a.w, b.x, b.y);
+    child = __float_as_int(b.z);
+}
+
+// statistics: warp-aggregated counters (src/gpu/raycast.cu:147-156)
+template <bool kStats>
+__device__ __forceinline__ void flush_stats(bool active, int nodes, int leaves, bool overflow,
+                                            unsigned long long* stats) {
+    if (stats == nullptr) return;
+    const unsigned mask = __ballot_sync(0xffffffffu, active);
+    const unsigned ovf = __ballot_sync(0xffffffffu, overflow);
+    if (kStats) {
+        const int sn = __reduce_add_sync(0xffffffffu, nodes);
+        const int sl = __reduce_add_sync(0xffffffffu, leaves);
+        if ((threadIdx.x & 31) == 0 && mask) {
+            if (sn) atomicAdd(stats + 0, static_cast<unsigned long long>(sn));
+            if (sl) atomicAdd(stats + 1, static_cast<unsigned long long>(sl));
+        }
+    }
+    if ((threadIdx.x & 31) == 0 && ovf) atomicAdd(stats + 2, static_cast<unsigned long long>(__popc(ovf)));
+}
+
+// ---------------------------------------------------------------------------------------
+// rays
+// ---------------------------------------------------------------------------------------
+// Leaf test.  The first hit is taken even at t == tMax (the CPU reference accepts t <= tMax,
+// src/cpu/bvh.cpp:156-168); later hits only when closer.  Among hits at the same t the
+// smallest scene index is kept, so the reported primitive does not depend on visit order.
+__device__ __forceinline__ void test_tri(const RayPre& R, const float4* __restrict__ leaves,
+                                         int slot, float& best, float& bound, bool& any,
+                                         int& best_id) {
+    const float4 a = __ldg(leaves + 3 * slot), b = __ldg(leaves + 3 * slot + 1),
+                 c = __ldg(leaves + 3 * slot + 2);
+    float t;
+    if (ray_tri(R, f3(a.x, a.y, a.z), f3(b.x, b.y, b.z), f3(c.x, c.y, c.z), t)) {
+        const int id = __float_as_int(a.w);
+        if (!any || t < best || (t == best && id < best_id)) {
+            best = t;
+            bound = best * kMarginMul + kMarginAdd;
+            any = true;
+            best_id = id;
+        }
+    }
+}
+
+__device__ __forceinline__ unsigned long long pack_hit(bool any, float best) {
+    return any ? ((1ull << 32) | static_cast<unsigned long long>(__float_as_uint(best))) : 0ull;
+}
+
+// First hit in a binary tree: near child followed, far child pushed with its entry bound,
+// which is re-checked against the current best when popped (src/cpu/bvh.cpp:147-152).
+template <class St>
+__device__ __forceinline__ unsigned long long ray_bin_one(const BNode* __restrict__ bn,
+                                                          const float4* __restrict__ leaves,
+                                                          const Box& rb, const RayPre& R,
+                                                          int max_iter, St& st, Trav& tv,
+                                                          int& best_id) {
+    float best = R.tmax;
+    float bound = best * kMarginMul + kMarginAdd;
+    bool any = false;
+    best_id = -1;
+    float te;
+    if (!ray_box(R, rb.lo, rb.hi, bound, te)) return 0ull;
+    ++tv.nodes;
+    int sp = 0;
+    int node = 0;
+    for (int iter = 0;; ++iter) {
+        if (iter >= max_iter) {
+            tv.overflow = true;
+            break;
+        }
+        float3 llo, lhi, rlo, rhi;
+        int lref, rref;
+        load_bnode(bn, node, llo, lhi, rlo, rhi, lref, rref);
+        float tl, tr;
+        bool hl = ray_box(R, llo, lhi, bound, tl);
+        bool hr = ray_box(R, rlo, rhi, bound, tr);
+        tv.nodes += static_cast<int>(hl) + static_cast<int>(hr);
+        if (hl && lref < 0) {
+            ++tv.leaves;
+            test_tri(R, leaves, ~lref, best, bound, any, best_id);
+            hl = false;
+        }
+        if (hr && rref < 0) {
+            ++tv.leaves;
+            test_tri(R, leaves, ~rref, best, bound, any, best_id);
+            hr = false;
+        }
+        if (hl && hr) {
+            const bool lnear = tl <= tr;
+            if (sp >= St::kSize) {
+                tv.overflow = true;
+                break;
+            }
+            st.put(sp, lnear ? rref : lref, lnear ? tr : tl);
+            ++sp;
+            node = lnear ? lref : rref;
+        } else if (hl) {
+            node = lref;
+        } else if (hr) {
+            node = rref;
+        } else {
+            // pop the next entry whose box could still hold a closer hit
+            const float limit = bound * kMarginMul + kMarginAdd;
+            node = -1;
+            while (sp > 0) {
+                --sp;
+                if (!(st.get_key(sp) > limit)) {
+                    node = st.get_node(sp);
+                    break;
+                }
+            }
+            if (node < 0) break;
+        }
+    }
+    return pack_hit(any, best);
+}
+
+// First hit in a 4-wide tree: hit slots sorted by entry t, leaves tested nearest first,
+// the nearest internal child followed and the others pushed far-first.
+template <class St>
+__device__ __forceinline__ unsigned long long ray_wide_one(const WideNode* __restrict__ wn,
+                                                           const float4* __restrict__ leaves,
+                                                           const RayPre& R, int max_iter, St& st,
+                                                           Trav& tv, int& best_id) {
+    float best = R.tmax;
+    float bound = best * kMarginMul + kMarginAdd;
+    bool any = false;
+    best_id = -1;
+    int sp = 0;
+    int node = 0;  // the 4-wide root has no single box; start inside it (raycast.cu:182)
+    for (int iter = 0;; ++iter) {
+        if (iter >= max_iter) {
+            tv.overflow = true;
+            break;
+        }
+        int child[4];
+        float key[4];
+        int hits = 0;
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            float3 lo, hi;
+            int c;
+            load_wide_entry(wn, node, s, lo, hi, c);
+            float t;
+            if (c != kEmptySlot && ray_box(R, lo, hi, bound, t)) {
+                ++tv.nodes;
+                int j = hits++;
+                while (j > 0 && key[j - 1] > t) {
+                    key[j] = key[j - 1];
+                    child[j] = child[j - 1];
+                    --j;
+                }
+                key[j] = t;
+                child[j] = c;
+            }
+        }
+        int next = -1;
+        float nextT = 0.0f;
+        for (int j = 0; j < hits; ++j) {
+            if (child[j] < 0) {
+                ++tv.leaves;
+                test_tri(R, leaves, ~child[j], best, bound, any, best_id);
+            }
+        }
+        for (int j = hits - 1; j >= 0; --j) {
+            if (child[j] < 0) continue;
+            if (next >= 0) {
+                if (sp >= St::kSize) {
+                    tv.overflow = true;
+                    break;
+                }
+                st.put(sp, next, nextT);
+                ++sp;
+            }
+            next = child[j];
+            nextT = key[j];
+        }
+        if (tv.overflow) break;
+        if (next >= 0) {
+            node = next;
+            continue;
+        }
+        const float limit = bound * kMarginMul + kMarginAdd;
+        node = -1;
+        while (sp > 0) {
+            --sp;
+            if (!(st.get_key(sp) > limit)) {
+                node = st.get_node(sp);
+                break;
+            }
+        }
+        if (node < 0) break;
+    }
+    return pack_hit(any, best);
+}
+
+// ---------------------------------------------------------------------------------------
+// closest
+// ---------------------------------------------------------------------------------------
+template <class Ops>
+__device__ __forceinline__ void leaf_closest(float3 p, const float4* __restrict__ leaves, int slot,
+                                             float& best, int& best_id) {
+    int id;
+    const float d2 = Ops::dist2(p, leaves, slot, id);
+    if (best_id < 0 || closer(d2, id, best, best_id)) {
+        best = d2;
+        best_id = id;
+    }
+}
+
+__device__ __forceinline__ uint2 pack_closest(float best, int best_id) {
+    return best_id >= 0 ? make_uint2(__float_as_uint(best), static_cast<unsigned>(best_id))
+                        : make_uint2(0u, 0xffffffffu);
+}
+
+template <class Ops, class St>
+__device__ __forceinline__ uint2 closest_bin_one(const BNode* __restrict__ bn,
+                                                 const float4* __restrict__ leaves, float3 p,
+                                                 int max_iter, St& st, Trav& tv) {
+    float best = kInf;
+    int best_id = -1;
+    int sp = 0;
+    int node = 0;
+    for (int iter = 0;; ++iter) {
+        if (iter >= max_iter) {
+            tv.overflow = true;
+            break;
+        }
+        ++tv.nodes;
+        float3 llo, lhi, rlo, rhi;
+        int lref, rref;
+        load_bnode(bn, node, llo, lhi, rlo, rhi, lref, rref);
+        const float dl = dist2_box(p, llo, lhi);
+        const float dr = dist2_box(p, rlo, rhi);
+        bool okl = best_id < 0 || dl <= best;
+        bool okr = best_id < 0 || dr <= best;
+        // leaves in near-first order so the second sees the tighter bound
+        const bool lfirst = dl <= dr;
+        if (lfirst) {
+            if (okl && lref < 0) { ++tv.leaves; leaf_closest<Ops>(p, leaves, ~lref, best, best_id); okl = false; }
+            if (okr && rref < 0 && (best_id < 0 || dr <= best)) { ++tv.leaves; leaf_closest<Ops>(p, leaves, ~rref, best, best_id); }
+            if (rref < 0) okr = false;
+        } else {
+            if (okr && rref < 0) { ++tv.leaves; leaf_closest<Ops>(p, leaves, ~rref, best, best_id); okr = false; }
+            if (okl && lref < 0 && (best_id < 0 || dl <= best)) { ++tv.leaves; leaf_closest<Ops>(p, leaves, ~lref, best, best_id); }
+            if (lref < 0) okl = false;
+        }
+        if (okl && okr) {
+            if (sp >= St::kSize) {
+                tv.overflow = true;
+                break;
+            }
+            st.put(sp, lfirst ? rref : lref, lfirst ? dr : dl);
+            ++sp;
+            node = lfirst ? lref : rref;
+        } else if (okl) {
+            node = lref;
+        } else if (okr) {
+            node = rref;
+        } else {
+            node = -1;
+            while (sp > 0) {
+                --sp;
+                if (best_id < 0 || st.get_key(sp) <= best) {
+                    node = st.get_node(sp);
+                    break;
+                }
+            }
+            if (node < 0) break;
+        }
+    }
+    return pack_closest(best, best_id);
+}
+
+template <class Ops, class St>
+__device__ __forceinline__ uint2 closest_wide_one(const WideNode* __restrict__ wn,
+                                                  const float4* __restrict__ leaves, float3 p,
+                                                  int max_iter, St& st, Trav& tv) {
+    float best = kInf;
+    int best_id = -1;
+    int sp = 0;
+    int node = 0;
+    for (int iter = 0;; ++iter) {
+        if (iter >= max_iter) {
+            tv.overflow = true;
+            break;
+        }
+        int child[4];
+        float key[4];
+        int hits = 0;
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            float3 lo, hi;
+            int c;
+            load_wide_entry(wn, node, s, lo, hi, c);
+            if (c == kEmptySlot) continue;
+            const float d = dist2_box(p, lo, hi);
+            if (best_id >= 0 && d > best) continue;
+            ++tv.nodes;
+            int j = hits++;
+            while (j > 0 && key[j - 1] > d) {
+                key[j] = key[j - 1];
+                child[j] = child[j - 1];
+                --j;
+            }
+            key[j] = d;
+            child[j] = c;
+        }
+        for (int j = 0; j < hits; ++j) {
+            if (child[j] < 0 && (best_id < 0 || key[j] <= best)) {
+                ++tv.leaves;
+                leaf_closest<Ops>(p, leaves, ~child[j], best, best_id);
+            }
+        }
+        int next = -1;
+        float nextD = 0.0f;
+        for (int j = hits - 1; j >= 0; --j) {
+            if (child[j] < 0) continue;
+            if (best_id >= 0 && key[j] > best) continue;
+            if (next >= 0) {
+                if (sp >= St::kSize) {
+                    tv.overflow = true;
+                    break;
+                }
+                st.put(sp, next, nextD);
+                ++sp;
+            }
+            next = child[j];
+            nextD = key[j];
+        }
+        if (tv.overflow) break;
+        if (next >= 0) {
+            node = next;
+            continue;
+        }
+        node = -1;
+        while (sp > 0) {
+            --sp;
+            if (best_id < 0 || st.get_key(sp) <= best) {
+                node = st.get_node(sp);
+                break;
+            }
+        }
+        if (node < 0) break;
+    }
+    return pack_closest(best, best_id);
+}
+
+// ---------------------------------------------------------------------------------------
+// kNN: the k best (dist2, id) pairs stay sorted in registers (unrolled insertion over a
+// compile-time capacity K >= k).  Empty slots hold (+inf, INT_MAX), so "strictly closer than
+// the k-th" is one comparison whether or not the table is full -- the reference's max-heap
+// replacement rule (src/cpu/bvh.cpp:284-299, src/gpu/query.cu:145-158).
+// ---------------------------------------------------------------------------------------
+template <int K>
+struct KnnTable {
+    float d[K];
+    int id[K];
+    float kd;  // dist2 of entry k-1 (the pruning threshold)
+    int kid;
+
+    __device__ __forceinline__ void init() {
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            d[j] = kInf;
+            id[j] = 0x7fffffff;
+        }
+        kd = kInf;
+        kid = 0x7fffffff;
+    }
+    __device__ __forceinline__ void insert(float xd, int xid, int k) {
+        if (!closer(xd, xid, kd, kid)) return;
+#pragma unroll
+        for (int j = K - 1; j > 0; --j) {
+            const bool shift = closer(xd, xid, d[j - 1], id[j - 1]);
+            const bool place = !shift && closer(xd, xid, d[j], id[j]);
+            const float nd = shift ? d[j - 1] : (place ? xd : d[j]);
+            const int ni = shift ? id[j - 1] : (place ? xid : id[j]);
+            d[j] = nd;
+            id[j] = ni;
+        }
+        if (closer(xd, xid, d[0], id[0])) {
+            d[0] = xd;
+            id[0] = xid;
+        }
+#pragma unroll
+        for (int j = 0; j < K; ++j) {
+            if (j == k - 1) {
+                kd = d[j];
+                kid = id[j];
+            }
+        }
+    }
+    // prune test for a subtree bound: keep while the table is not full or bound <= k-th
+    __device__ __forceinline__ bool admits(float bound) const { return kid == 0x7fffffff || bound <= kd; }
+};
+
+template <class Ops, int K>
+__device__ __forceinline__ void leaf_knn(float3 p, const float4* __restrict__ leaves, int slot,
+                                         KnnTable<K>& tab, int k) {
+    int id;
+    const float d2 = Ops::dist2(p, leaves, slot, id);
+    tab.insert(d2, id, k);
+}
+
+template <int K>
+__device__ __forceinline__ void write_knn(const KnnTable<K>& tab, int k, uint2* __restrict__ dst) {
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+        if (j < k) {
+            const bool valid = tab.id[j] != 0x7fffffff;
+            dst[j] = valid ? make_uint2(__float_as_uint(tab.d[j]), static_cast<unsigned>(tab.id[j]))
+                           : make_uint2(0u, 0xffffffffu);
+        }
+    }
+}
+
+template <class Ops, int K, class St>
+__device__ __forceinline__ void knn_bin_one(const BNode* __restrict__ bn,
+                                            const float4* __restrict__ leaves, float3 p, int k,
+                                            int max_iter, St& st, Trav& tv, KnnTable<K>& tab) {
+    tab.init();
+    int sp = 0;
+    int node = 0;
+    for (int iter = 0;; ++iter) {
+        if (iter >= max_iter) {
+            tv.overflow = true;
+            break;
+        }
+        ++tv.nodes;
+        float3 llo, lhi, rlo, rhi;
+        int lref, rref;
+        load_bnode(bn, node, llo, lhi, rlo, rhi, lref, rref);
+        const float dl = dist2_box(p, llo, lhi);
+        const float dr = dist2_box(p, rlo, rhi);
+        const bool lfirst = dl <= dr;
+        bool okl = tab.admits(dl);
+        bool okr = tab.admits(dr);
+        if (lfirst) {
+            if (okl && lref < 0) { ++tv.leaves; leaf_knn<Ops, K>(p, leaves, ~lref, tab, k); okl = false; }
+            if (okr && rref < 0 && tab.admits(dr)) { ++tv.leaves; leaf_knn<Ops, K>(p, leaves, ~rref, tab, k); }
+            if (rref < 0) okr = false;
+        } else {
+            if (okr && rref < 0) { ++tv.leaves; leaf_knn<Ops, K>(p, leaves, ~rref, tab, k); okr = false; }
+            if (okl && lref < 0 && tab.admits(dl)) { ++tv.leaves; leaf_knn<Ops, K>(p, leaves, ~lref, tab, k); }
+            if (lref < 0) okl = false;
+        }
+        if (okl && okr) {
+            if (sp >= St::kSize) {
+                tv.overflow = true;
+                break;
+            }
+            st.put(sp, lfirst ? rref : lref, lfirst ? dr : dl);
+            ++sp;
+            node = lfirst ? lref : rref;
+        } else if (okl) {
+            node = lref;
+        } else if (okr) {
+            node = rref;
+        } else {
+            node = -1;
+            while (sp > 0) {
+                --sp;
+                if (tab.admits(st.get_key(sp))) {
+                    node = st.get_node(sp);
+                    break;
+                }
+            }
+            if (node < 0) break;
+        }
+    }
+}
+
+template <class Ops, int K, class St>
+__device__ __forceinline__ void knn_wide_one(const WideNode* __restrict__ wn,
+                                             const float4* __restrict__ leaves, float3 p, int k,
+                                             int max_iter, St& st, Trav& tv, KnnTable<K>& tab) {
+    tab.init();
+    int sp = 0;
+    int node = 0;
+    for (int iter = 0;; ++iter) {
+        if (iter >= max_iter) {
+            tv.overflow = true;
+            break;
+        }
+        int child[4];
+        float key[4];
+        int hits = 0;
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            float3 lo, hi;
+            int c;
+            load_wide_entry(wn, node, s, lo, hi, c);
+            if (c == kEmptySlot) continue;
+            const float d = dist2_box(p, lo, hi);
+            if (!tab.admits(d)) continue;
+            ++tv.nodes;
+            int j = hits++;
+            while (j > 0 && key[j - 1] > d) {
+                key[j] = key[j - 1];
+                child[j] = child[j - 1];
+                --j;
+            }
+            key[j] = d;
+            child[j] = c;
+        }
+        for (int j = 0; j < hits; ++j) {
+            if (child[j] < 0 && tab.admits(key[j])) {
+                ++tv.leaves;
+                leaf_knn<Ops, K>(p, leaves, ~child[j], tab, k);
+            }
+        }
+        int next = -1;
+        float nextD = 0.0f;
+        for (int j = hits - 1; j >= 0; --j) {
+            if (child[j] < 0 || !tab.admits(key[j])) continue;
+            if (next >= 0) {
+                if (sp >= St::kSize) {
+                    tv.overflow = true;
+                    break;
+                }
+                st.put(sp, next, nextD);
+                ++sp;
+            }
+            next = child[j];
+            nextD = key[j];
+        }
+        if (tv.overflow) break;
+        if (next >= 0) {
+            node = next;
+            continue;
+        }
+        node = -1;
+        while (sp > 0) {
+            --sp;
+            if (tab.admits(st.get_key(sp))) {
+                node = st.get_node(sp);
+                break;
+            }
+        }
+        if (node < 0) break;
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// radius: a box is entered when its squared distance <= r2, a primitive kept when its
+// dist2 <= r2 (src/gpu/query.cu:415-540).  The fill pass writes (bits(d2) << 32 | id) keys
+// from `write` on and never past `end`; both passes return the number found.
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long radius_key(float d2, int id) {
+    return (static_cast<unsigned long long>(__float_as_uint(d2)) << 32) | static_cast<unsigned>(id);
+}
+
+template <class Ops, bool kFill, class St>
+__device__ __forceinline__ int radius_bin_one(const BNode* __restrict__ bn,
+                                              const float4* __restrict__ leaves, const Box& rb,
+                                              float3 p, float r2, int write, int end,
+                                              unsigned long long* __restrict__ keys,
+                                              int max_iter, St& st, Trav& tv) {
+    int found = 0;
+    if (!(dist2_box(p, rb.lo, rb.hi) <= r2)) return 0;
+    int sp = 0;
+    int node = 0;
+    for (int iter = 0;; ++iter) {
+        if (iter >= max_iter) {
+            tv.overflow = true;
+            break;
+        }
+        ++tv.nodes;
+        float3 llo, lhi, rlo, rhi;
+        int lref, rref;
+        load_bnode(bn, node, llo, lhi, rlo, rhi, lref, rref);
+        bool okl = dist2_box(p, llo, lhi) <= r2;
+        bool okr = dist2_box(p, rlo, rhi) <= r2;
+        if (okl && lref < 0) {
+            ++tv.leaves;
+            int id;
+            const float d2 = Ops::dist2(p, leaves, ~lref, id);
+            if (d2 <= r2) {
+                if (kFill && write < end) keys[write++] = radius_key(d2, id);
+                ++found;
+            }
+            okl = false;
+        }
+        if (okr && rref < 0) {
+            ++tv.leaves;
+            int id;
+            const float d2 = Ops::dist2(p, leaves, ~rref, id);
+            if (d2 <= r2) {
+                if (kFill && write < end) keys[write++] = radius_key(d2, id);
+                ++found;
+            }
+            okr = false;
+        }
+        if (okl && okr) {
+            if (sp >= St::kSize) {
+                tv.overflow = true;
+                break;
+            }
+            st.put_node(sp++, rref);
+            node = lref;
+        } else if (okl) {
+            node = lref;
+        } else if (okr) {
+            node = rref;
+        } else {
+            if (sp == 0) break;
+            node = st.get_node(--sp);
+        }
+    }
+    return found;
+}
+
+template <class Ops, bool kFill, class St>
+__device__ __forceinline__ int radius_wide_one(const WideNode* __restrict__ wn,
+                                               const float4* __restrict__ leaves, float3 p,
+                                               float r2, int write, int end,
+                                               unsigned long long* __restrict__ keys,
+                                               int max_iter, St& st, Trav& tv) {
+    int found = 0;
+    int sp = 0;
+    int node = 0;
+    for (int iter = 0;; ++iter) {
+        if (iter >= max_iter) {
+            tv.overflow = true;
+            break;
+        }
+        int next = -1;
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            float3 lo, hi;
+            int c;
+            load_wide_entry(wn, node, s, lo, hi, c);
+            if (c == kEmptySlot || !(dist2_box(p, lo, hi) <= r2)) continue;
+            ++tv.nodes;
+            if (c < 0) {
+                ++tv.leaves;
+                int id;
+                const float d2 = Ops::dist2(p, leaves, ~c, id);
+                if (d2 <= r2) {
+                    if (kFill && write < end) keys[write++] = radius_key(d2, id);
+                    ++found;
+                }
+            } else if (next < 0) {
+                next = c;
+            } else if (sp < St::kSize) {
+                st.put_node(sp++, c);
+            } else {
+                tv.overflow = true;
+            }
+        }
+        if (tv.overflow) break;
+        if (next >= 0) {
+            node = next;
+        } else {
+            if (sp == 0) break;
+            node = st.get_node(--sp);
+        }
+    }
+    return found;
+}
+
+}  // namespace qk

@@ -22,6 +22,8 @@ QK_TRI, QK_POINT, QK_GAUSS = 0, 1, 2
 QK_BUILD_LBVH, QK_BUILD_SAH = 0, 1
 QK_ORDER_MORTON, QK_ORDER_DIRECTION, QK_WIDE = 1, 2, 4
 QK_TUNE_DYNAMIC, QK_TUNE_HIGH_OCC = 256, 512
+QK_SCHEDULE_BATCHED, QK_SCHEDULE_LOOP = 0, 1
+QK_OP_RAY, QK_OP_CLOSEST, QK_OP_KNN, QK_OP_RADIUS = 0, 1, 2, 3
 KINDS = {"tri": QK_TRI, "point": QK_POINT, "gauss": QK_GAUSS}
 STRIDE = {QK_TRI: 9, QK_POINT: 3, QK_GAUSS: 10}
 
@@ -44,6 +46,19 @@ class QkTreeSizes(ctypes.Structure):
                                           "bnodes", "leaves", "slot_of", "flags", "wide",
                                           "wide_id")]
 
+
+class QkBatchTune(ctypes.Structure):
+    _fields_ = [("block", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32),
+                ("short_stack", ctypes.c_int32), ("chunks_per_fetch", ctypes.c_int32)]
+
+
+class QkBatchIo(ctypes.Structure):
+    _fields_ = [("input", _P), ("out", _P), ("offsets", _P), ("capacity", ctypes.c_int64),
+                ("k", ctypes.c_int32), ("pad", ctypes.c_int32)]
+
+
+_PP = ctypes.POINTER(ctypes.c_void_p)
+_I64P = ctypes.POINTER(ctypes.c_int64)
 
 EXPORTS = {
     "qk_status_string": (ctypes.c_char_p, [_I]),
@@ -77,6 +92,18 @@ EXPORTS = {
     "qk_raycast_host_workspace_bytes": (_SZ, [_I, _I]),
     "qk_raycast_host": (_I, [ctypes.POINTER(QkTree), _P, _I, _P, _P, _P, _I, _U, _P, _SZ, _P, _P]),
     "qk_sort_pairs": (_I, [_P, _P, _P, _P, _I, _I, _P, _SZ, _P]),
+    "qk_batch_arena_bytes": (_SZ, [_I, _P, _I, _U]),
+    "qk_batch_create": (_I, [_PP, _I, _P, _I, _P, _P, _SZ, _U, _P]),
+    "qk_batch_build": (_I, [_P, _U, _P]),
+    "qk_batch_sync": (_I, [_P, _P]),
+    "qk_batch_tree": (_I, [_P, _I, ctypes.POINTER(QkTree)]),
+    "qk_batch_scenes": (_I, [_P]),
+    "qk_batch_destroy": (None, [_P]),
+    "qk_batch_plan_bytes": (_SZ, [_P, _I, _P, _U]),
+    "qk_batch_plan_create": (_I, [_PP, _P, _I, _P, _P, _P, _SZ, _U, _P]),
+    "qk_batch_query": (_I, [_P, ctypes.POINTER(QkBatchIo), ctypes.POINTER(QkBatchTune), _U, _P]),
+    "qk_batch_plan_status": (_I, [_P, _I64P, _I64P, _P]),
+    "qk_batch_plan_destroy": (None, [_P]),
 }
 
 _lib = None
@@ -378,3 +405,131 @@ def sort_pairs(keys, vals, bits: int = 32):
     check(lib().qk_sort_pairs(_ptr(kin), _ptr(vin), _ptr(kout), _ptr(vout), n, bits, _ptr(ws),
                               ws.numel(), _stream()), "qk_sort_pairs")
     return kout, vout
+
+
+# ---------------------------------------------------------------------------------------
+# batched scenes
+# ---------------------------------------------------------------------------------------
+class Batch:
+    """Scenes of one primitive kind built and queried together (qk_batch_*).
+
+    scenes: list of (n_s, stride) float32 arrays (numpy or CUDA tensors).  wide=True also
+    builds every scene's 4-wide nodes."""
+
+    def __init__(self, kind: str, scenes, wide: bool = False):
+        torch = _torch()
+        self.kind = KINDS[kind]
+        st = STRIDE[self.kind]
+        parts = [np.asarray(a, np.float32).reshape(-1, st) if isinstance(a, np.ndarray)
+                 else a.reshape(-1, st) for a in scenes]
+        self.counts = np.array([p.shape[0] for p in parts], dtype=np.int32)
+        if isinstance(parts[0], np.ndarray):
+            self.items = to_device(np.concatenate(parts, axis=0), np.float32)
+        else:
+            self.items = torch.cat(parts, dim=0).contiguous()
+        self.scenes = len(parts)
+        self.offsets = np.concatenate([[0], np.cumsum(self.counts)]).astype(np.int64)
+        self.flags = QK_WIDE if wide else 0
+        L = lib()
+        nb = L.qk_batch_arena_bytes(self.kind, self.counts.ctypes.data, self.scenes, self.flags)
+        if nb == 0:
+            raise QkError(1, "qk_batch_arena_bytes")
+        self.arena = _dev_bytes(nb)
+        self.h = ctypes.c_void_p()
+        check(L.qk_batch_create(ctypes.byref(self.h), self.kind, self.counts.ctypes.data,
+                                self.scenes, _ptr(self.items), _ptr(self.arena), nb, self.flags,
+                                _stream()), "qk_batch_create")
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h is not None and h.value and _lib is not None:
+            _lib.qk_batch_destroy(h)
+            self.h = None
+
+    def build(self, schedule: int = QK_SCHEDULE_BATCHED) -> None:
+        check(lib().qk_batch_build(self.h, schedule, _stream()), "qk_batch_build")
+
+    def sync(self) -> None:
+        check(lib().qk_batch_sync(self.h, _stream()), "qk_batch_sync")
+
+    def tree(self, s: int) -> QkTree:
+        t = QkTree()
+        check(lib().qk_batch_tree(self.h, s, ctypes.byref(t)), "qk_batch_tree")
+        return t
+
+    def view(self, s: int) -> "DeviceTree":
+        """Scene s as a DeviceTree (no copy): single-tree queries, validation, read-back."""
+        t = self.tree(s)
+        v = DeviceTree.__new__(DeviceTree)
+        v.kind = self.kind
+        v.n = t.n
+        v.t = t
+        v.items_scene = self.items[int(self.offsets[s]):int(self.offsets[s + 1])]
+        sizes = QkTreeSizes()
+        check(lib().qk_tree_bytes(self.kind, t.n, ctypes.byref(sizes)), "qk_tree_bytes")
+        base = self.arena.data_ptr()
+        v.arrays = {}
+        for name in ("nodes", "items", "prim_ids", "parent", "depth_arr", "bnodes", "leaves",
+                     "slot_of", "flags", "wide", "wide_id"):
+            ptr = getattr(t, name)
+            if ptr:
+                off = ptr - base
+                v.arrays[name] = self.arena[off:off + getattr(sizes, name)]
+        v.ws = Workspace()
+        v.builder = QK_BUILD_LBVH
+        v.sah_bins = 32
+        v.owner = self
+        return v
+
+    def plan(self, op: int, counts, params=None, flags: int = 0) -> "BatchPlan":
+        return BatchPlan(self, op, counts, params, flags)
+
+
+class BatchPlan:
+    """Per-scene query counts of one operation over a Batch (qk_batch_plan_*)."""
+
+    def __init__(self, batch: Batch, op: int, counts, params=None, flags: int = 0):
+        L = lib()
+        self.batch = batch
+        self.op = op
+        self.counts = np.ascontiguousarray(counts, dtype=np.int32)
+        self.total = int(self.counts.sum())
+        self.q_off = np.concatenate([[0], np.cumsum(self.counts)]).astype(np.int64)
+        self.params = None if params is None else np.ascontiguousarray(params, dtype=np.float32)
+        nb = L.qk_batch_plan_bytes(batch.h, op, self.counts.ctypes.data, flags)
+        self.mem = _dev_bytes(nb)
+        self.h = ctypes.c_void_p()
+        check(L.qk_batch_plan_create(ctypes.byref(self.h), batch.h, op, self.counts.ctypes.data,
+                                     None if self.params is None else self.params.ctypes.data,
+                                     _ptr(self.mem), nb, flags, _stream()), "qk_batch_plan_create")
+
+    def __del__(self):
+        h = getattr(self, "h", None)
+        if h is not None and h.value and _lib is not None:
+            _lib.qk_batch_plan_destroy(h)
+            self.h = None
+
+    def query(self, inputs, out, offsets=None, capacity: int = 0, k: int = 0, tune=None,
+              schedule: int = QK_SCHEDULE_BATCHED) -> None:
+        io = QkBatchIo()
+        io.input = _ptr(inputs)
+        io.out = _ptr(out)
+        io.offsets = _ptr(offsets)
+        io.capacity = int(capacity)
+        io.k = int(k)
+        tp = None
+        if tune is not None:
+            t = QkBatchTune()
+            t.block, t.blocks_per_sm, t.short_stack, t.chunks_per_fetch = (
+                int(tune["block"]), int(tune["blocks_per_sm"]), int(tune["short_stack"]),
+                int(tune["chunks_per_fetch"]))
+            tp = ctypes.byref(t)
+        check(lib().qk_batch_query(self.h, ctypes.byref(io), tp, schedule, _stream()),
+              "qk_batch_query")
+
+    def status(self) -> tuple[int, int]:
+        tot = ctypes.c_int64(0)
+        ovf = ctypes.c_int64(0)
+        check(lib().qk_batch_plan_status(self.h, ctypes.byref(tot), ctypes.byref(ovf), _stream()),
+              "qk_batch_plan_status")
+        return tot.value, ovf.value

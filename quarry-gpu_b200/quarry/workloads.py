@@ -14,6 +14,9 @@ Workloads (sizes are the benchmark's; every generator takes smaller sizes for te
             [0,100]^3; 20k queries for closest / kNN8 / radius 1.0; a coherent 1% refit
   gaussians 1,048,576 ellipsoids, means U[0,100]^3, log-uniform scales [0.05,1], uniform
             rotations; 262,144 query points
+  batch     256 scenes of uneven size: 128 terrains of 1k..500k triangles and 128 uniform
+            clouds of 4k..1M points (log-uniform), each with 1k..100k queries split into
+            closest / kNN16 / radius (r = 0.02 x diagonal), terrains also with as many rays
 """
 from __future__ import annotations
 
@@ -190,3 +193,64 @@ def city_config(buildings: int = 131072, rays: int = 1_000_000, queries: int = 2
                     seed)
     q = uniform_points(queries, lo, hi, seed, 13)
     return CityConfig(tris, r, q, top)
+
+
+@dataclass
+class BatchScene:
+    """One scene of the batched workload: primitives and its four query sets."""
+    kind: str              # "tri" (terrain) or "point" (uniform cloud)
+    items: np.ndarray      # (n, 9) triangles or (n, 3) points
+    closest: np.ndarray    # (q1, 3)
+    knn: np.ndarray        # (q2, 3)
+    radius: np.ndarray     # (q3, 3)
+    r: float               # 0.02 x the scene's bounding-box diagonal
+    rays: np.ndarray       # (q, 8) downward rays (terrain scenes), (0, 8) otherwise
+
+
+@dataclass
+class BatchConfig:
+    terrains: list
+    clouds: list
+    k: int
+
+
+def batch_scene_sizes(index: int, prim_range: tuple[int, int],
+                      query_range: tuple[int, int]) -> tuple[int, int]:
+    """Primitive and query counts of scene `index` (seed 1000 + index, log-uniform)."""
+    seed = 1000 + index
+    return (log_uniform_int(seed, 1, prim_range[0], prim_range[1]),
+            log_uniform_int(seed, 2, query_range[0], query_range[1]))
+
+
+def batch_config(terrains: int = 128, clouds: int = 128,
+                 tri_range: tuple[int, int] = (1_000, 500_000),
+                 point_range: tuple[int, int] = (4_000, 1_000_000),
+                 query_range: tuple[int, int] = (1_000, 100_000), k: int = 16) -> BatchConfig:
+    """The batched uneven workload: `terrains` height-field meshes (scenes 0..terrains-1) and
+    `clouds` uniform point clouds (the following scene indices).  Scene i uses seed 1000 + i;
+    its Q queries are uniform in its bounds, the first third closest, the next third kNN, the
+    rest radius at r = 0.02 x diagonal; terrain scenes also get Q rays straight down from
+    z = +100."""
+    out_t, out_c = [], []
+    for i in range(terrains + clouds):
+        is_tri = i < terrains
+        n, q = batch_scene_sizes(i, tri_range if is_tri else point_range, query_range)
+        seed = 1000 + i
+        if is_tri:
+            grid = max(2, int(round((n / 2) ** 0.5)))
+            items = terrain(grid, seed)
+            lo, hi = bounds_of(items)
+        else:
+            items = point_cloud("volume", n, seed)
+            lo, hi = items.min(axis=0), items.max(axis=0)
+        pts = uniform_points(q, lo, hi, seed, 13)
+        a, b = q // 3, 2 * (q // 3)
+        diag = float(np.sqrt(np.sum((hi.astype(np.float64) - lo.astype(np.float64)) ** 2)))
+        r = float(np.float32(0.02 * diag))
+        if is_tri:
+            rays = down_rays(q, float(lo[0]), float(hi[0]), float(lo[1]), float(hi[1]), 100.0, seed)
+        else:
+            rays = np.zeros((0, 8), np.float32)
+        sc = BatchScene("tri" if is_tri else "point", items, pts[:a], pts[a:b], pts[b:], r, rays)
+        (out_t if is_tri else out_c).append(sc)
+    return BatchConfig(out_t, out_c, k)

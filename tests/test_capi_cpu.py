@@ -70,3 +70,49 @@ def test_knn_argument_checks(k, stride):
                  "slot_of", "flags"):
         setattr(t, name, 16)  # never dereferenced: the checks run first
     assert L.qk_knn(ctypes.byref(t), None, 0, k, stride, None, 0, None, None, 0, None) == 1
+
+
+def test_batch_sizes_and_argument_checks():
+    L = capi.lib()
+    counts = (ctypes.c_int32 * 3)(1000, 5000, 2)
+    a = L.qk_batch_arena_bytes(capi.QK_TRI, counts, 3, 0)
+    w = L.qk_batch_arena_bytes(capi.QK_TRI, counts, 3, capi.QK_WIDE)
+    # at least the three trees' arrays, and the 4-wide fields only when asked for
+    s = capi.QkTreeSizes()
+    need = 0
+    for n in (1000, 5000, 2):
+        L.qk_tree_bytes(capi.QK_TRI, n, ctypes.byref(s))
+        need += s.nodes + s.items + s.bnodes + s.leaves
+    assert a > need and w > a + (999 + 4999 + 1) * 128
+    bad = (ctypes.c_int32 * 2)(1000, 1)
+    assert L.qk_batch_arena_bytes(capi.QK_TRI, bad, 2, 0) == 0
+    h = ctypes.c_void_p()
+    assert L.qk_batch_create(ctypes.byref(h), capi.QK_TRI, bad, 2, 16, 256, 1 << 30, 0, None) == 1
+    assert b"at least 2" in L.qk_last_error()
+    # unaligned arena, unknown flags, too-small arena: rejected before any device call
+    assert L.qk_batch_create(ctypes.byref(h), capi.QK_TRI, counts, 3, 16, 260, a, 0, None) == 1
+    assert L.qk_batch_create(ctypes.byref(h), capi.QK_TRI, counts, 3, 16, 256, a, 8, None) == 1
+    assert L.qk_batch_create(ctypes.byref(h), capi.QK_TRI, counts, 3, 16, 256, a - 1, 0, None) == 3
+    assert not h.value
+    assert L.qk_batch_query(None, None, None, 0, None) == 1
+    assert L.qk_batch_plan_status(None, None, None, None) == 1
+
+
+def test_batch_workload_sizes_are_seeded():
+    from quarry import workloads
+
+    sizes = [workloads.batch_scene_sizes(i, (1_000, 500_000), (1_000, 100_000)) for i in range(256)]
+    assert sizes == [workloads.batch_scene_sizes(i, (1_000, 500_000), (1_000, 100_000))
+                     for i in range(256)]
+    n = [s[0] for s in sizes]
+    q = [s[1] for s in sizes]
+    assert min(n) >= 1_000 and max(n) <= 500_000 and min(q) >= 1_000 and max(q) <= 100_000
+    # log-uniform: about half the draws below the geometric midpoint
+    assert 80 < sum(x < (1_000 * 500_000) ** 0.5 for x in n) < 176
+    cfg = workloads.batch_config(terrains=2, clouds=2, tri_range=(1_000, 4_000),
+                                 point_range=(4_000, 8_000), query_range=(30, 90))
+    for sc in cfg.terrains + cfg.clouds:
+        q3 = sc.closest.shape[0] + sc.knn.shape[0] + sc.radius.shape[0]
+        assert sc.closest.shape[0] == sc.knn.shape[0] == q3 // 3
+        assert sc.r > 0
+        assert sc.rays.shape[0] == (q3 if sc.kind == "tri" else 0)

@@ -41,14 +41,20 @@ PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default 400; 20 for --workload batch)")
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="city", choices=["city", "terrain", "grad"])
+    ap.add_argument("--workload", default="city", choices=["city", "terrain", "grad", "batch"])
+    ap.add_argument("--tune-cache", default=None, help="autotuner JSON (default: user cache)")
+    ap.add_argument("--retune", action="store_true", help="ignore cached autotuner choices")
     ap.add_argument("--small", action="store_true", help="small inputs (profiling captures)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--only", default="", help="time only this variant (profiling)")
-    return ap.parse_args()
+    args = ap.parse_args()
+    if args.steps is None:
+        args.steps = 20 if args.workload == "batch" else 400
+    return args
 
 
 def peaks() -> tuple[dict, str]:
@@ -306,6 +312,187 @@ def grad_arm(args, world, rank, local):
 
 
 # ---------------------------------------------------------------------------------------
+# batched uneven scenes: one CUDA graph per step vs the per-scene launch loop
+# ---------------------------------------------------------------------------------------
+def batch_arm(args, world, rank, local):
+    """256 scenes (128 terrains of 1k..500k triangles, 128 uniform clouds of 4k..1M points,
+    1k..100k queries each: closest / kNN16 / radius at 0.02 x diagonal, plus as many rays on
+    the terrains).  A step builds every tree and answers every query.  Batched: one CUDA graph
+    of one-launch-per-phase kernels (launch shapes from the autotuner).  Loop: the same work
+    through the single-tree calls, scene after scene.  Each rank runs its own 256 scenes."""
+    import torch
+
+    import oracle
+    from quarry import autotune, pipeline, workloads as w
+
+    torch.cuda.set_device(local)
+    kw = {}
+    if args.small:
+        kw = dict(terrains=16, clouds=16, tri_range=(1_000, 50_000),
+                  point_range=(4_000, 100_000), query_range=(1_000, 10_000))
+    t0 = time.perf_counter()
+    cfg = w.batch_config(first_seed=1000 + 100_000 * rank, **kw)
+    gen_s = time.perf_counter() - t0
+    pipe = pipeline.BatchPipeline(cfg.terrains, cfg.clouds, cfg.k)
+    pipe.size_radius_outputs()
+    tuner = autotune.Autotuner(args.tune_cache)
+    tune_report = pipe.tune(tuner, force=args.retune)
+    pipe.size_radius_outputs()
+    pipe.capture()
+    for _ in range(max(args.warmup, 3)):
+        pipe.replay()
+    torch.cuda.synchronize()
+    pipe.sync()
+
+    # ---- batched: K graph replays (inputs are GBs, larger than L2) ----
+    barrier(world)
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    with Clocks(local) as clk:
+        for e0, e1 in ev:
+            e0.record()
+            pipe.replay()
+            e1.record()
+        torch.cuda.synchronize()
+    clocks = clk.summary()
+    batched_ms = max_over_ranks(world, float(np.mean([a.elapsed_time(b) for a, b in ev])))
+    pipe.sync()
+    got = pipe.results()
+
+    # ---- the per-scene launch loop, same layouts and orders ----
+    loop_steps = 2 if args.small else 3
+    pipe.run_loop()
+    torch.cuda.synchronize()
+    lt = []
+    for _ in range(loop_steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        pipe.run_loop()
+        e1.record()
+        torch.cuda.synchronize()
+        lt.append(e0.elapsed_time(e1))
+    loop_ms = max_over_ranks(world, float(np.mean(lt)))
+    loop = pipe.results(loop_layout=True)
+    mism = []
+    for key, per in got.items():
+        for i, (a, b) in enumerate(zip(per, loop[key])):
+            same = (np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+                    if isinstance(a, tuple) else np.array_equal(a, b))
+            if not same:
+                mism.append(f"{key}[{i}]")
+    if mism:
+        raise RuntimeError(f"batched and loop results differ: {mism[:8]}")
+
+    # ---- end to end: inputs uploaded from pinned host memory, results read back ----
+    host_in = [(t, torch.empty(t.shape, dtype=t.dtype).pin_memory().copy_(t.cpu()))
+               for t in [b.items for b in pipe.batches.values()] + [ph.inputs for ph in pipe.phases]]
+    outs = []
+    for ph in pipe.phases:
+        outs.append((ph.out, torch.empty(ph.out.shape, dtype=ph.out.dtype).pin_memory()))
+        if ph.offsets is not None:
+            outs.append((ph.offsets, torch.empty(ph.offsets.shape, dtype=ph.offsets.dtype).pin_memory()))
+    h2d = int(sum(h.numel() * h.element_size() for _, h in host_in))
+    d2h = int(sum(h.numel() * h.element_size() for _, h in outs))
+
+    def e2e_step():
+        for d, h in host_in:
+            d.copy_(h, non_blocking=True)
+        pipe.replay()
+        for d, h in outs:
+            h.copy_(d, non_blocking=True)
+
+    e2e_step()
+    torch.cuda.synchronize()
+    et = []
+    for _ in range(min(args.steps, 5)):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        e2e_step()
+        e1.record()
+        torch.cuda.synchronize()
+        et.append(e0.elapsed_time(e1))
+    e2e_ms = max_over_ranks(world, float(np.mean(et)))
+    nq = pipe.query_count()
+
+    line = None
+    if rank == 0:
+        # ---- quarry's CPU reference on sample scenes: smallest, median and largest of each kind
+        threads = os.cpu_count() or 1
+        checked, cpu_q, cpu_ms = [], 0, 0.0
+        have_ref = oracle.REF_PATH.exists()
+        R = oracle.Reference() if have_ref else None
+        for kind, scenes in (("tri", cfg.terrains), ("point", cfg.clouds)):
+            order = np.argsort([s.items.shape[0] for s in scenes], kind="stable")
+            for i in sorted({int(order[0]), int(order[len(order) // 2]), int(order[-1])}):
+                sc = scenes[i]
+                if R is not None:
+                    want = {"closest": R.closest(kind, sc.items, sc.closest, threads),
+                            "knn": R.knn(kind, sc.items, sc.knn, cfg.k, threads),
+                            "radius": R.radius(kind, sc.items, sc.radius, float(sc.r), threads)}
+                    if kind == "tri":
+                        want["rays"] = R.raycast(sc.items, sc.rays, threads)
+                    for name, wv in want.items():
+                        cpu_ms += wv[-2] if name != "radius" else wv[-1]
+                    res = {k: (v[0] if k != "radius" else (v[0], v[1])) for k, v in want.items()}
+                else:
+                    ref = oracle.LBVH(kind, sc.items)
+                    ta = time.perf_counter()
+                    res = {"closest": ref.closest(sc.closest, threads),
+                           "knn": ref.knn(sc.knn, cfg.k, threads),
+                           "radius": ref.radius(sc.radius, float(sc.r), threads)}
+                    if kind == "tri":
+                        res["rays"] = ref.raycast(sc.rays, threads)
+                    cpu_ms += (time.perf_counter() - ta) * 1e3
+                for name, wv in res.items():
+                    g = got[f"{kind}_{name}"][i]
+                    ok = (np.array_equal(g[0], wv[0]) and np.array_equal(g[1], wv[1])
+                          if name == "radius" else np.array_equal(g, wv))
+                    if not ok:
+                        raise RuntimeError(f"{kind} scene {i} {name} differs from the CPU reference")
+                    cpu_q += len(g[0]) - 1 if name == "radius" else len(g)
+                checked.append(f"{kind}[{i}] n={sc.items.shape[0]}")
+        speedup = loop_ms / batched_ms
+        line = {
+            "metric": METRIC, "value": round(speedup, 3), "unit": "x (per-scene loop / batched)",
+            "n_gpus": world, "steps": args.steps, "warmup": max(args.warmup, 3),
+            "ms_per_step": round(batched_ms, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded generators, identical bytes on every host)",
+            "config": {"workload": "batch", "scenes": len(cfg.terrains) + len(cfg.clouds),
+                       "terrains": len(cfg.terrains), "clouds": len(cfg.clouds),
+                       "triangles": int(sum(s.items.shape[0] for s in cfg.terrains)),
+                       "points": int(sum(s.items.shape[0] for s in cfg.clouds)),
+                       "queries": nq, "k": cfg.k,
+                       "l2": "inputs and trees (GBs) larger than L2; no flush",
+                       "parallelism": f"{world} rank(s), each its own 256 scenes",
+                       "step": "build every tree + every query of every scene"},
+            "batched": {"ms": round(batched_ms, 3),
+                        "mqueries_per_s": round(world * nq / (batched_ms * 1e-3) / 1e6, 2),
+                        "graph_kernel_nodes": pipe.graph_kernel_nodes()},
+            "loop": {"ms": round(loop_ms, 3), "steps": loop_steps,
+                     "mqueries_per_s": round(world * nq / (loop_ms * 1e-3) / 1e6, 2)},
+            "autotune": tune_report, "tune_cache": str(tuner.path),
+            "parity": {"batched_vs_loop": "all scenes bit-identical",
+                       "cpu_reference_scenes": checked,
+                       "against": "reference" if have_ref else "port"},
+            "roofline": None,
+            "cpu_baseline": {"value": round(cpu_q / (cpu_ms * 1e-3) / 1e6, 4) if cpu_ms else None,
+                             "unit": "Mqueries/s", "cores": threads,
+                             "kind": "reference" if have_ref else "port",
+                             "sample": "queries of the smallest, median and largest scene of "
+                                       "each kind; CPU tree builds excluded"},
+            "clocks": clocks,
+            "e2e": {"value": round(world * nq / (e2e_ms * 1e-3) / 1e6, 2), "unit": "Mqueries/s",
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "path": "pinned host inputs -> graph replay -> pinned host outputs"},
+            "generate_s": round(gen_s, 1),
+            "gpu_launches": (pipe.graph_kernel_nodes() or 0) * args.steps,
+        }
+        print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------------------
 def main():
@@ -317,6 +504,10 @@ def main():
         return
     if args.workload == "grad":
         grad_arm(args, world, rank, local)
+        barrier(world)
+        return
+    if args.workload == "batch":
+        batch_arm(args, world, rank, local)
         barrier(world)
         return
     import torch

@@ -527,9 +527,12 @@ class BatchPlan:
         check(lib().qk_batch_query(self.h, ctypes.byref(io), tp, schedule, _stream()),
               "qk_batch_query")
 
-    def status(self) -> tuple[int, int]:
+    def status(self, raise_on_overrun: bool = True) -> tuple[int, int]:
+        """(radius keys of the last query or -1, traversals stopped by a limit); raises on a
+        radius capacity overrun unless raise_on_overrun is False."""
         tot = ctypes.c_int64(0)
         ovf = ctypes.c_int64(0)
-        check(lib().qk_batch_plan_status(self.h, ctypes.byref(tot), ctypes.byref(ovf), _stream()),
-              "qk_batch_plan_status")
+        st = lib().qk_batch_plan_status(self.h, ctypes.byref(tot), ctypes.byref(ovf), _stream())
+        if st != QK_OK and (raise_on_overrun or st != 3):
+            check(st, "qk_batch_plan_status")
         return tot.value, ovf.value

@@ -215,9 +215,9 @@ class BatchConfig:
 
 
 def batch_scene_sizes(index: int, prim_range: tuple[int, int],
-                      query_range: tuple[int, int]) -> tuple[int, int]:
-    """Primitive and query counts of scene `index` (seed 1000 + index, log-uniform)."""
-    seed = 1000 + index
+                      query_range: tuple[int, int], first_seed: int = 1000) -> tuple[int, int]:
+    """Primitive and query counts of scene `index` (seed first_seed + index, log-uniform)."""
+    seed = first_seed + index
     return (log_uniform_int(seed, 1, prim_range[0], prim_range[1]),
             log_uniform_int(seed, 2, query_range[0], query_range[1]))
 
@@ -225,17 +225,20 @@ def batch_scene_sizes(index: int, prim_range: tuple[int, int],
 def batch_config(terrains: int = 128, clouds: int = 128,
                  tri_range: tuple[int, int] = (1_000, 500_000),
                  point_range: tuple[int, int] = (4_000, 1_000_000),
-                 query_range: tuple[int, int] = (1_000, 100_000), k: int = 16) -> BatchConfig:
+                 query_range: tuple[int, int] = (1_000, 100_000), k: int = 16,
+                 first_seed: int = 1000) -> BatchConfig:
     """The batched uneven workload: `terrains` height-field meshes (scenes 0..terrains-1) and
-    `clouds` uniform point clouds (the following scene indices).  Scene i uses seed 1000 + i;
+    `clouds` uniform point clouds (the following scene indices).  Scene i uses seed
+    first_seed + i;
     its Q queries are uniform in its bounds, the first third closest, the next third kNN, the
     rest radius at r = 0.02 x diagonal; terrain scenes also get Q rays straight down from
     z = +100."""
     out_t, out_c = [], []
     for i in range(terrains + clouds):
         is_tri = i < terrains
-        n, q = batch_scene_sizes(i, tri_range if is_tri else point_range, query_range)
-        seed = 1000 + i
+        n, q = batch_scene_sizes(i, tri_range if is_tri else point_range, query_range,
+                                 first_seed)
+        seed = first_seed + i
         if is_tri:
             grid = max(2, int(round((n / 2) ** 0.5)))
             items = terrain(grid, seed)

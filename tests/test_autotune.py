@@ -94,3 +94,26 @@ def test_engine_spaces_are_consistent():
     for b in autotune.BATCH_SPACE["block"]:
         for s in autotune.BATCH_SPACE["short_stack"]:
             assert b * s * 8 <= 48 * 1024
+
+
+def test_shipped_choices_are_a_fallback(tmp_path):
+    shipped = tmp_path / "shipped.json"
+    shipped.write_text(json.dumps({"version": autotune.VERSION, "entries": {
+        "dev|w": {"params": {"a": 3, "b": "x", "c": 2}, "ms": 2.0}}}))
+    timer, calls = fake_timer(separable)
+    tu = autotune.Autotuner(tmp_path / "cache.json", timer=timer, device="dev", shipped=shipped)
+    res = tu.search("w", SPACE, run=lambda p: None)
+    assert res.cached and res.source == "shipped" and res.params["a"] == 3 and not calls
+    # force measures and the measured choice then shadows the shipped one
+    res = tu.search("w", SPACE, run=lambda p: None, force=True)
+    assert not res.cached and res.params == {"a": 2, "b": "y", "c": 1}
+    assert tu.search("w", SPACE, run=lambda p: None).source == "cache"
+
+
+def test_shipped_b200_table_is_valid():
+    data = json.loads(autotune.SHIPPED.read_text())
+    assert data["version"] == autotune.VERSION and data["entries"]
+    for key, e in data["entries"].items():
+        assert "|batch:" in key
+        p = e["params"]
+        assert all(p[k] in v for k, v in autotune.BATCH_SPACE.items()), (key, p)

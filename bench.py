@@ -45,7 +45,7 @@ def parse():
                     help="timed steps (default 400; 20 for --workload batch)")
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="city", choices=["city", "terrain", "grad", "batch"])
+    ap.add_argument("--workload", default="city", choices=["city", "terrain", "grad", "batch", "points"])
     ap.add_argument("--tune-cache", default=None, help="autotuner JSON (default: user cache)")
     ap.add_argument("--retune", action="store_true", help="ignore cached autotuner choices")
     ap.add_argument("--small", action="store_true", help="small inputs (profiling captures)")
@@ -312,6 +312,231 @@ def grad_arm(args, world, rank, local):
 
 
 # ---------------------------------------------------------------------------------------
+# point clouds: closest / kNN8 / radius 1.0 and the 1% coherent refit
+# ---------------------------------------------------------------------------------------
+def points_arm(args, world, rank, local):
+    """1,048,576 points on a noisy sphere (r=50, radial N(0,0.5)) and 1,048,576 uniform in
+    [0,100]^3; per cloud 20,000 queries uniform in its bounds for closest, kNN (k=8) and
+    radius (r=1.0).  A step answers all six query sets (L2 flushed before each step).  The
+    refit moves a spatially coherent 1% of the points by N(0, 0.05) per axis."""
+    import torch
+
+    import oracle
+    from quarry import capi, workloads as w
+
+    torch.cuda.set_device(local)
+    n = 65_536 if args.small else 1_048_576
+    nq, k, r = 20_000, 8, 1.0
+    seed = 1 + rank
+    l2 = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    clouds = {}
+    for kind in ("surface", "volume"):
+        pts = w.point_cloud(kind, n, seed)
+        lo, hi = pts.min(axis=0), pts.max(axis=0)
+        q = w.uniform_points(nq, lo, hi, seed, 13)
+        tree = capi.DeviceTree("point", pts)
+        tree.build_wide()
+        clouds[kind] = {"pts": pts, "q": q, "q_d": capi.to_device(q, np.float32), "tree": tree}
+
+    def timed(fn, steps, warm=3):
+        for _ in range(warm):
+            fn()
+        ts = []
+        for _ in range(steps):
+            l2.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return ts
+
+    outs = {}
+
+    def step(flags):
+        for kind, c in clouds.items():
+            t = c["tree"]
+            outs[(kind, "closest")] = t.closest(c["q_d"], flags)
+            outs[(kind, "knn")] = t.knn(c["q_d"], k, flags)
+            outs[(kind, "radius")] = t.radius(c["q_d"], r, flags)
+
+    def snapshot():
+        return {key: ((v[0].cpu().numpy(), v[1].cpu().numpy()) if isinstance(v, tuple)
+                      else v.cpu().numpy()) for key, v in outs.items()}
+
+    variants = {"bin": 0, "bin_morton": capi.QK_ORDER_MORTON, "wide": capi.QK_WIDE,
+                "wide_morton": capi.QK_WIDE | capi.QK_ORDER_MORTON,
+                "split": capi.QK_TUNE_SPLIT, "split_morton": capi.QK_TUNE_SPLIT | capi.QK_ORDER_MORTON}
+    step(0)
+    base = snapshot()
+    vms = {}
+    for name, f in variants.items():
+        step(f)
+        got = snapshot()
+        for key in base:
+            a, b = base[key], got[key]
+            same = (np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+                    if isinstance(a, tuple) else np.array_equal(a, b))
+            if not same:
+                raise RuntimeError(f"variant {name} differs on {key}")
+        vms[name] = float(np.median(timed(lambda: step(f), 5)))
+    best = min(vms, key=vms.get)
+    flags = variants[best]
+
+    barrier(world)
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        ts = timed(lambda: step(flags), args.steps, args.warmup)
+    clocks = clk.summary()
+    ms = max_over_ranks(world, float(np.mean(ts)))
+    queries = 2 * 3 * nq
+    value = world * queries / (ms * 1e-3) / 1e6
+
+    # per-operation kernel times and the canonical visit counts (binary LBVH) for the roofline
+    per_op = {}
+    for op in ("closest", "knn", "radius"):
+        def one(op=op):
+            for c in clouds.values():
+                t = c["tree"]
+                if op == "closest":
+                    t.closest(c["q_d"], flags)
+                elif op == "knn":
+                    t.knn(c["q_d"], k, flags)
+                else:
+                    t.radius(c["q_d"], r, flags)
+        per_op[op] = float(np.median(timed(one, 20)))
+    stats = torch.zeros(4, dtype=torch.int64, device="cuda")
+    for c in clouds.values():
+        c["tree"].knn(c["q_d"], k, 0, stats=stats)
+    st = stats.cpu().numpy()
+    p_leaf = st[1] / (2 * nq)
+    p_int = (st[0] - st[1]) / (2 * nq)
+    bytes_per_q = 12 + 8 * k + 96 * p_int + (32 + 12 + 4) * p_leaf
+    pk, pk_kind = peaks()
+    achieved = bytes_per_q * 2 * nq / (per_op["knn"] * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": pk["hbm_gbs"],
+                "unit": "GB/s", "frac": round(achieved / pk["hbm_gbs"], 4), "traffic": None,
+                "peak_kind": pk_kind,
+                "kernel": ("k_knn_wide" if flags & capi.QK_WIDE else
+                           "k_knn_split" if flags & capi.QK_TUNE_SPLIT else "k_knn_bin"),
+                "kernel_ms": round(per_op["knn"], 4), "bytes_per_query": round(float(bytes_per_q), 1),
+                "canonical_counts": {"internal_pops_per_query": round(float(p_int), 2),
+                                     "leaf_tests_per_query": round(float(p_leaf), 2)}}
+
+    # ---- refit: 1% coherent motion, dirty refit vs full refit vs rebuild ----
+    refit = {}
+    for kind, c in clouds.items():
+        moved, ids = w.coherent_motion(c["pts"], 0.01, 0.05, seed)
+        t = c["tree"]
+        ids_d = capi.to_device(ids, np.int32)
+        sub_moved = capi.to_device(moved[ids], np.float32)
+        sub_orig = capi.to_device(c["pts"][ids], np.float32)
+        flip = [0]
+
+        def dirty():
+            t.refit_dirty(ids_d, sub_moved if flip[0] % 2 == 0 else sub_orig)
+            flip[0] += 1
+
+        d_ms = float(np.median(timed(dirty, 10, 2)))
+        if flip[0] % 2 == 1:  # leave the tree on the moved points
+            pass
+        else:
+            t.refit_dirty(ids_d, sub_moved)
+        moved_d = capi.to_device(moved, np.float32)
+        f_ms = float(np.median(timed(lambda: t.refit(moved_d), 10, 2)))
+        fresh = capi.DeviceTree("point", moved_d)
+        b_ms = float(np.median(timed(lambda: fresh.build(), 5, 1)))
+        fresh.build_wide()
+        a = t.knn(c["q_d"], k, flags).cpu().numpy()
+        b = fresh.knn(c["q_d"], k, flags).cpu().numpy()
+        ref = oracle.LBVH("point", moved)
+        want = ref.knn(c["q"], k)
+        if not (np.array_equal(a.view(np.uint32), want) and np.array_equal(b.view(np.uint32), want)):
+            raise RuntimeError(f"{kind}: refit kNN differs from the rebuild or the oracle")
+        ca = t.closest(c["q_d"], flags).cpu().numpy().view(np.uint32)
+        if not np.array_equal(ca, ref.closest(c["q"])):
+            raise RuntimeError(f"{kind}: refit closest differs from the oracle")
+        refit[kind] = {"dirty": int(ids.size), "dirty_refit_ms": round(d_ms, 4),
+                       "full_refit_ms": round(f_ms, 4), "rebuild_ms": round(b_ms, 4),
+                       "knn_fingerprint_after_refit": f"0x{oracle.knn_hash(want):016x}"}
+        t.refit(capi.to_device(c["pts"], np.float32))
+
+    # ---- end to end: queries from pinned host memory, results read back ----
+    host_q = {kind: torch.from_numpy(c["q"]).pin_memory() for kind, c in clouds.items()}
+
+    def e2e():
+        total = 0
+        for kind, c in clouds.items():
+            qd = host_q[kind].to("cuda", non_blocking=True)
+            t = c["tree"]
+            a = t.closest(qd, flags)
+            b = t.knn(qd, k, flags)
+            off, keys = t.radius(qd, r, flags)
+            a.cpu(), b.cpu(), off.cpu(), keys.cpu()
+            total += int(keys.numel())
+        return total
+
+    et = timed(e2e, 10)
+    e2e_ms = max_over_ranks(world, float(np.mean(et)))
+    radius_keys = sum(int(outs[(kind, "radius")][1].numel()) for kind in clouds)
+
+    line = None
+    if rank == 0:
+        # quarry's CPU reference on the same queries, all host threads
+        threads = os.cpu_count() or 1
+        parity, cpu_ms, kind_ref = {}, 0.0, "port"
+        if oracle.REF_PATH.exists():
+            R = oracle.Reference()
+            kind_ref = "reference"
+            for kind, c in clouds.items():
+                cw, cms, _ = R.closest("point", c["pts"], c["q"], threads)
+                kw_, kms, _ = R.knn("point", c["pts"], c["q"], k, threads)
+                ro, rk, rms = R.radius("point", c["pts"], c["q"], r, threads)
+                cpu_ms += cms + kms + rms
+                ok = (np.array_equal(outs[(kind, "closest")].cpu().numpy().view(np.uint32), cw)
+                      and np.array_equal(outs[(kind, "knn")].cpu().numpy().view(np.uint32), kw_)
+                      and np.array_equal(outs[(kind, "radius")][0].cpu().numpy(), ro)
+                      and np.array_equal(outs[(kind, "radius")][1].cpu().numpy().view(np.uint64), rk))
+                if not ok:
+                    raise RuntimeError(f"{kind}: results differ from the CPU reference")
+                parity[kind] = {"closest": f"0x{oracle.closest_hash(cw):016x}",
+                                "knn": f"0x{oracle.knn_hash(kw_):016x}",
+                                "radius": f"0x{oracle.radius_hash(ro, rk):016x}"}
+        line = {
+            "metric": METRIC, "value": round(value, 2), "unit": "Mqueries/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded generators, identical bytes on every host)",
+            "config": {"workload": "points", "points_per_cloud": n, "clouds": ["surface", "volume"],
+                       "queries_per_op": nq, "k": k, "radius": r, "builder": "lbvh",
+                       "variant": best, "l2": "flushed (256 MB write) between timed steps",
+                       "parallelism": f"replica x{world}"},
+            "variants_ms": {kk: round(v, 4) for kk, v in vms.items()},
+            "per_op_ms": {kk: round(v, 4) for kk, v in per_op.items()},
+            "radius_results": radius_keys, "refit": refit,
+            "parity": {"against": kind_ref, "fingerprints": parity,
+                       "variants": "all layouts / orders / schedules bit-identical"},
+            "roofline": roofline,
+            "cpu_baseline": {"value": round(queries / (cpu_ms * 1e-3) / 1e6, 4) if cpu_ms else None,
+                             "unit": "Mqueries/s", "cores": threads, "kind": kind_ref,
+                             "sample": "all 120,000 queries of the step; CPU tree builds excluded"},
+            "clocks": clocks,
+            "e2e": {"value": round(world * queries / (e2e_ms * 1e-3) / 1e6, 2),
+                    "unit": "Mqueries/s", "h2d_bytes_per_step": 2 * nq * 12,
+                    "d2h_bytes_per_step": 2 * nq * (8 + 8 * k + 4) + 8 * radius_keys,
+                    "path": "pinned queries -> qk_closest / qk_knn / qk_radius_count+fill -> host"},
+            "gpu_launches": None,
+        }
+        morton = 24 if flags & capi.QK_ORDER_MORTON else 0
+        # per cloud: closest + kNN (1 + order), radius count (1 + scan 3 + order) + fill (1 +
+        # order) + 4 segment-sort launches
+        line["gpu_launches"] = args.steps * 2 * ((1 + morton) * 2 + (4 + morton) + (1 + morton) + 4)
+        print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------------------
 # batched uneven scenes: one CUDA graph per step vs the per-scene launch loop
 # ---------------------------------------------------------------------------------------
 def batch_arm(args, world, rank, local):
@@ -422,7 +647,8 @@ def batch_arm(args, world, rank, local):
         checked, cpu_q, cpu_ms = [], 0, 0.0
         have_ref = oracle.REF_PATH.exists()
         R = oracle.Reference() if have_ref else None
-        for kind, scenes in (("tri", cfg.terrains), ("point", cfg.clouds)):
+        sample_sets = () if args.no_cpu_baseline else (("tri", cfg.terrains), ("point", cfg.clouds))
+        for kind, scenes in sample_sets:
             order = np.argsort([s.items.shape[0] for s in scenes], kind="stable")
             for i in sorted({int(order[0]), int(order[len(order) // 2]), int(order[-1])}):
                 sc = scenes[i]
@@ -508,6 +734,10 @@ def main():
         return
     if args.workload == "batch":
         batch_arm(args, world, rank, local)
+        barrier(world)
+        return
+    if args.workload == "points":
+        points_arm(args, world, rank, local)
         barrier(world)
         return
     import torch
@@ -660,19 +890,27 @@ def main():
 
     # ---- kNN and build beside the step ----
     k_out = torch.empty((q_d.shape[0], 8, 2), dtype=torch.int32, device=dev)
-    kflags = best_flags & (capi.QK_WIDE | capi.QK_ORDER_MORTON)
-    for _ in range(3):
-        tree.knn(q_d, 8, kflags, out=k_out)
-    kt = []
-    for _ in range(10):
-        l2_flush.zero_()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        tree.knn(q_d, 8, kflags, out=k_out)
-        e1.record()
-        torch.cuda.synchronize()
-        kt.append(e0.elapsed_time(e1))
-    knn_ms = float(np.median(kt))
+    knn_base = tree.knn(q_d, 8, 0).clone()
+    knn_ms_by = {}
+    for kname, kf in (("layout_of_rays", best_flags & (capi.QK_WIDE | capi.QK_ORDER_MORTON)),
+                      ("split", capi.QK_TUNE_SPLIT),
+                      ("split_morton", capi.QK_TUNE_SPLIT | capi.QK_ORDER_MORTON)):
+        for _ in range(3):
+            tree.knn(q_d, 8, kf, out=k_out)
+        if not torch.equal(k_out, knn_base):
+            raise RuntimeError(f"kNN variant {kname} differs")
+        kt = []
+        for _ in range(10):
+            l2_flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            tree.knn(q_d, 8, kf, out=k_out)
+            e1.record()
+            torch.cuda.synchronize()
+            kt.append(e0.elapsed_time(e1))
+        knn_ms_by[kname] = float(np.median(kt))
+    knn_variant = min(knn_ms_by, key=knn_ms_by.get)
+    knn_ms = knn_ms_by[knn_variant]
 
     # ---- e2e through the C ABI from pinned host buffers: qk_raycast_host uploads, traces and
     # reads back in chunks over two streams, all inside the timed region ----
@@ -733,6 +971,8 @@ def main():
             "variants_ms": {k: round(v, 4) for k, v in results.items()},
             "build_ms": {k: round(v, 3) for k, v in build_ms.items()},
             "knn": {"k": 8, "queries": int(q_d.shape[0]), "ms": round(knn_ms, 4),
+                    "variant": knn_variant,
+                    "variants_ms": {kk: round(v, 4) for kk, v in knn_ms_by.items()},
                     "mqueries_per_s": round(q_d.shape[0] / (knn_ms * 1e-3) / 1e6, 2)},
             "fingerprint": f"0x{fp:016x}", "hits": int(hits), "parity": parity,
             "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,

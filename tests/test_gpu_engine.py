@@ -361,3 +361,45 @@ def test_raycast_tuning_flags_same_bits(cuda, tune, morton):
     tree.raycast(rd, 0, stats=base)
     # same traversal per ray: identical node and triangle test counts
     assert stats[:3].tolist() == base[:3].tolist()
+
+
+@pytest.mark.parametrize("kind", ["tri", "point", "gauss"])
+@pytest.mark.parametrize("n", [2, 3, 5, 40, 20_000])
+def test_split_queries_same_bits(cuda, kind, n):
+    """One warp per query over 32 disjoint subtrees: closest, kNN and radius equal the
+    one-thread-per-query kernels, including trees shallower than the split levels."""
+    rng = np.random.default_rng(n)
+    if kind == "tri":
+        items = rng.uniform(0, 10, (n, 9)).astype(np.float32)
+    elif kind == "point":
+        items = workloads.point_cloud("surface", n, 3) if n > 100 else rng.uniform(0, 10, (n, 3)).astype(np.float32)
+    else:
+        items = workloads.gaussians(n, 0.05, 1.0, 5)
+        items[:, :3] *= 0.1
+    tree = capi.DeviceTree(kind, items)
+    lo = np.asarray(items).reshape(n, -1)[:, :3].min(0) - 1
+    hi = np.asarray(items).reshape(n, -1)[:, :3].max(0) + 1
+    q = _dev(workloads.uniform_points(3_001, lo, hi, 7, 13))
+    for extra in (0, capi.QK_ORDER_MORTON):
+        f = capi.QK_TUNE_SPLIT | extra
+        assert cuda.equal(tree.closest(q, f), tree.closest(q, 0))
+        for k in (1, 8, 16):
+            assert cuda.equal(tree.knn(q, k, f), tree.knn(q, k, 0)), (k, extra)
+        r = float(np.linalg.norm(hi - lo)) * 0.05
+        o1, k1 = tree.radius(q, r, f)
+        o0, k0 = tree.radius(q, r, 0)
+        assert cuda.equal(o1, o0) and cuda.equal(k1, k0)
+    stats = cuda.zeros(4, dtype=cuda.int64, device="cuda")
+    tree.knn(q, 8, capi.QK_TUNE_SPLIT, stats=stats)
+    assert int(stats[2]) == 0
+
+
+def test_split_knn_sphere_matches_oracle(cuda):
+    pts = workloads.point_cloud("surface", 100_000, 2)
+    q = workloads.uniform_points(2_000, pts.min(0), pts.max(0), 2, 13)
+    tree = capi.DeviceTree("point", pts)
+    ref = oracle.LBVH("point", pts)
+    got = tree.knn(_dev(q), 8, capi.QK_TUNE_SPLIT).cpu().numpy().view(np.uint32)
+    assert np.array_equal(got, ref.knn(q, 8))
+    got = tree.closest(_dev(q), capi.QK_TUNE_SPLIT).cpu().numpy().view(np.uint32)
+    assert np.array_equal(got, ref.closest(q))

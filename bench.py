@@ -57,6 +57,18 @@ def parse():
     return args
 
 
+def profiled_traffic(workload: str, variant: str):
+    """DRAM bytes of one launch of this variant's kernel from the ncu summary in profiles/."""
+    p = ROOT / "profiles" / "traffic.md"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        cells = [c.strip() for c in line.strip().strip("|").split("|")]
+        if len(cells) >= 4 and cells[0] == workload and cells[1] == variant and cells[3].isdigit():
+            return int(cells[3])
+    return None
+
+
 def peaks() -> tuple[dict, str]:
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -870,13 +882,7 @@ def main():
     kernel_ms = float(np.median(kt))
     pk, pk_kind = peaks()
     achieved = bytes_per_ray * nrays / (kernel_ms * 1e-3) / 1e9
-    traffic = None
-    tfile = ROOT / "profiles" / f"traffic_{args.workload}.json"
-    if tfile.exists():
-        try:
-            traffic = json.loads(tfile.read_text()).get(best)
-        except Exception:
-            traffic = None
+    traffic = profiled_traffic(args.workload, best)
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": pk["hbm_gbs"],
                 "unit": "GB/s", "frac": round(achieved / pk["hbm_gbs"], 4),
                 "traffic": traffic, "peak_kind": pk_kind,

@@ -157,38 +157,29 @@ class Clocks:
                 "samples": len(sm), "reasons": sorted(reasons)}
 
 
+_RANKS = None
+
+
 def init_dist(args):
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import datetime
+    """One process per GPU over NCCL (quarry.dist); world 1 needs no process group."""
+    global _RANKS
+    from quarry import dist
 
-        import torch
-        import torch.distributed as dist
-
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
-    return world, rank, local
+    _RANKS = dist.init(backend="nccl" if int(os.environ.get("WORLD_SIZE", "1")) > 1 else None)
+    return _RANKS.world, _RANKS.rank, _RANKS.local
 
 
 def barrier(world):
-    if world > 1:
-        import torch.distributed as dist
+    from quarry import dist
 
-        dist.barrier()
+    if _RANKS is not None:
+        dist.barrier(_RANKS)
 
 
 def max_over_ranks(world, value: float) -> float:
-    if world == 1:
-        return value
-    import torch
-    import torch.distributed as dist
+    from quarry import dist
 
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    return dist.max_over_ranks(_RANKS, value) if _RANKS is not None else float(value)
 
 
 # ---------------------------------------------------------------------------------------
@@ -575,6 +566,7 @@ def batch_arm(args, world, rank, local):
     tuner = autotune.Autotuner(args.tune_cache)
     tune_report = pipe.tune(tuner, force=args.retune)
     pipe.size_radius_outputs()
+    tune_report["builder"] = pipe.tune_builder(tuner, force=args.retune)
     pipe.capture()
     for _ in range(max(args.warmup, 3)):
         pipe.replay()
@@ -704,6 +696,7 @@ def batch_arm(args, world, rank, local):
                        "queries": nq, "k": cfg.k,
                        "l2": "inputs and trees (GBs) larger than L2; no flush",
                        "parallelism": f"{world} rank(s), each its own 256 scenes",
+                       "builder": pipe.builder,
                        "step": "build every tree + every query of every scene"},
             "batched": {"ms": round(batched_ms, 3),
                         "mqueries_per_s": round(world * nq / (batched_ms * 1e-3) / 1e6, 2),
@@ -736,22 +729,27 @@ def batch_arm(args, world, rank, local):
 def main():
     args = parse()
     world, rank, local = init_dist(args)
-    if args.impl == "reference":
-        reference_arm(args, world, rank)
+    try:
+        if args.impl == "reference":
+            reference_arm(args, world, rank)
+        elif args.workload == "grad":
+            grad_arm(args, world, rank, local)
+        elif args.workload == "batch":
+            batch_arm(args, world, rank, local)
+        elif args.workload == "points":
+            points_arm(args, world, rank, local)
+        else:
+            rays_arm(args, world, rank, local)
         barrier(world)
-        return
-    if args.workload == "grad":
-        grad_arm(args, world, rank, local)
-        barrier(world)
-        return
-    if args.workload == "batch":
-        batch_arm(args, world, rank, local)
-        barrier(world)
-        return
-    if args.workload == "points":
-        points_arm(args, world, rank, local)
-        barrier(world)
-        return
+    finally:
+        from quarry import dist
+
+        if _RANKS is not None:
+            dist.destroy(_RANKS)
+
+
+def rays_arm(args, world, rank, local):
+    """City (default) or terrain: rays through the engine, the timed step."""
     import torch
 
     import oracle
@@ -991,11 +989,6 @@ def main():
         # kernels of ours launched per timed step: keys + bounds + 4 sort passes x 5 + traversal
         line["gpu_launches"] = args.steps * ((3 + 4 * 5 + 1) if best_flags & capi.QK_ORDER_MORTON else 1)
         print(json.dumps(line), flush=True)
-    barrier(world)
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.destroy_process_group()
 
 
 if __name__ == "__main__":

@@ -280,6 +280,10 @@ int qk_batch_create(qk_batch** out, int kind, const int32_t* counts, int scenes,
                     void* stream);
 /* Builds every scene's LBVH (and 4-wide nodes when created with QK_WIDE). */
 int qk_batch_build(qk_batch* batch, unsigned schedule, void* stream);
+/* Builds every scene with the binned SAH builder (sah_bins 4..64), scene after scene: the
+ * SAH level loop reads counts back, so this call synchronizes and cannot be captured.  The
+ * trees stay in the arena and serve every batched query like the LBVH ones. */
+int qk_batch_build_sah(qk_batch* batch, int sah_bins, void* stream);
 /* Waits for the stream, reads every scene's depth / wide-node count back into its tree and
  * reports QK_ERR_DEPTH when a scene is too deep for the traversal stack. */
 int qk_batch_sync(qk_batch* batch, void* stream);

@@ -596,7 +596,7 @@ BatchLayout batch_layout(int kind, const int32_t* counts, int scenes, unsigned f
     L.sort_ws = take(sort_ws_bytes(static_cast<int>(n)));
     const long long span = static_cast<long long>(L.field_bytes[8] / sizeof(int));
     L.scan_ws = take((flags & QK_WIDE) ? scan_ws_bytes(static_cast<int>(span)) : 0);
-    L.single_ws_bytes = std::max(build_ws_bytes(kind, max_n, QK_BUILD_LBVH),
+    L.single_ws_bytes = std::max(build_ws_bytes(kind, max_n, QK_BUILD_SAH),
                                  scan_ws_bytes(max_n));
     L.single_ws = take(L.single_ws_bytes);
     L.total = c.used;
@@ -639,11 +639,11 @@ int batch_build_impl(qk_batch* b, cudaStream_t s) {
     return e == cudaSuccess ? QK_OK : cuda_status(e, "batch build");
 }
 
-int batch_build_loop(qk_batch* b, cudaStream_t s) {
+int batch_build_loop(qk_batch* b, int builder, int bins, cudaStream_t s) {
     for (int i = 0; i < b->scenes; ++i) {
         qk_tree& t = b->trees[i];
         const float* in = b->items + static_cast<size_t>(b->prim_off[i]) * qk_stride_floats(b->kind);
-        int st = build_tree(&t, QK_BUILD_LBVH, 0, in, b->single_ws, b->single_ws_bytes, s);
+        int st = build_tree(&t, builder, bins, in, b->single_ws, b->single_ws_bytes, s);
         if (st != QK_OK) return st;
         if (b->flags & QK_WIDE) {
             st = wide_build(&t, b->single_ws, b->single_ws_bytes, s);
@@ -941,7 +941,7 @@ int qk_batch_build(qk_batch* b, unsigned schedule, void* stream) {
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     if (schedule == QK_SCHEDULE_LOOP) {
         b->built_by_loop = true;
-        return batch_build_loop(b, s);
+        return batch_build_loop(b, QK_BUILD_LBVH, 0, s);
     }
     if (schedule != QK_SCHEDULE_BATCHED) return fail(QK_ERR_INVALID, "unknown schedule %u", schedule);
     b->built_by_loop = false;
@@ -951,6 +951,13 @@ int qk_batch_build(qk_batch* b, unsigned schedule, void* stream) {
         case kGauss: return batch_build_impl<GaussOps>(b, s);
         default: return fail(QK_ERR_INVALID, "unknown primitive kind %d", b->kind);
     }
+}
+
+int qk_batch_build_sah(qk_batch* b, int sah_bins, void* stream) {
+    if (!b) return fail(QK_ERR_INVALID, "batch is NULL");
+    if (sah_bins < 4 || sah_bins > 64) return fail(QK_ERR_INVALID, "sah_bins must be in [4, 64]");
+    b->built_by_loop = true;
+    return batch_build_loop(b, QK_BUILD_SAH, sah_bins, static_cast<cudaStream_t>(stream));
 }
 
 int qk_batch_sync(qk_batch* b, void* stream) {

@@ -95,6 +95,7 @@ EXPORTS = {
     "qk_batch_arena_bytes": (_SZ, [_I, _P, _I, _U]),
     "qk_batch_create": (_I, [_PP, _I, _P, _I, _P, _P, _SZ, _U, _P]),
     "qk_batch_build": (_I, [_P, _U, _P]),
+    "qk_batch_build_sah": (_I, [_P, _I, _P]),
     "qk_batch_sync": (_I, [_P, _P]),
     "qk_batch_tree": (_I, [_P, _I, ctypes.POINTER(QkTree)]),
     "qk_batch_scenes": (_I, [_P]),
@@ -448,6 +449,10 @@ class Batch:
 
     def build(self, schedule: int = QK_SCHEDULE_BATCHED) -> None:
         check(lib().qk_batch_build(self.h, schedule, _stream()), "qk_batch_build")
+
+    def build_sah(self, bins: int = 32) -> None:
+        """Every scene with the binned SAH builder, scene by scene (synchronizes)."""
+        check(lib().qk_batch_build_sah(self.h, bins, _stream()), "qk_batch_build_sah")
 
     def sync(self) -> None:
         check(lib().qk_batch_sync(self.h, _stream()), "qk_batch_sync")

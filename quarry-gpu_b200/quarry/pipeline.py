@@ -72,8 +72,15 @@ class BatchPipeline:
                                          dict(autotune.BATCH_START), {}))
         self.graph = None
         self.streams = None
+        self.builder = "lbvh"   # or "sah<bins>": per-scene SAH builds, outside the graph
 
     # ---- objects ----
+    def build_trees(self, kind: str) -> None:
+        if self.builder == "lbvh":
+            self.batches[kind].build()
+        else:
+            self.batches[kind].build_sah(int(self.builder[3:]))
+
     def _make_batches(self):
         for kind, sc in self.scenes.items():
             if sc:
@@ -161,9 +168,10 @@ class BatchPipeline:
         torch = self.torch
         kinds = [k for k in ("tri", "point") if k in self.batches]
         main = torch.cuda.current_stream()
+        in_graph = self.builder == "lbvh"
         if streams is None:
             for kind in kinds:
-                self.batches[kind].build()
+                self.build_trees(kind)
                 for ph in self.phases:
                     if ph.kind == kind:
                         self.run_phase(ph)
@@ -172,7 +180,8 @@ class BatchPipeline:
             s.wait_stream(main)
         for kind, s in zip(kinds, streams):
             with torch.cuda.stream(s):
-                self.batches[kind].build()
+                if in_graph:
+                    self.batches[kind].build()
                 for ph in self.phases:
                     if ph.kind == kind:
                         self.run_phase(ph)
@@ -199,7 +208,37 @@ class BatchPipeline:
         torch.cuda.synchronize()
 
     def replay(self) -> None:
+        """One step: the graph (builds included with the batched LBVH); per-scene SAH builds,
+        which synchronize, run before it."""
+        if self.builder != "lbvh":
+            for kind in self.batches:
+                self.build_trees(kind)
         self.graph.replay()
+
+    def tune_builder(self, tuner: autotune.Autotuner, force: bool = False,
+                     repeats: int = 2) -> dict:
+        """Chooses the builder (batched LBVH, or per-scene SAH with 8 / 16 / 32 bins) by the
+        time of a whole step: every build plus every query phase with its tuned shape."""
+        sig = "batch-step:" + "|".join(self.signature(ph) for ph in self.phases)
+
+        def run(params):
+            self.builder = params["builder"]
+            self.step()
+
+        def fp(params):
+            return tuple(self.fingerprint(ph) for ph in self.phases)
+
+        res = tuner.search(sig, {"builder": ["lbvh", "sah8", "sah16", "sah32"]}, run,
+                           fingerprint=fp, start={"builder": "lbvh"}, repeats=repeats,
+                           force=force, tolerance=0.0)
+        self.builder = res.params["builder"]
+        for kind in self.batches:
+            self.build_trees(kind)
+        self.sync()
+        tuner.save()
+        return {"params": res.params, "ms": round(res.ms, 3), "cached": res.cached,
+                "source": res.source, "points": [(t["params"]["builder"], t["ms"])
+                                                 for t in res.trials]}
 
     def graph_kernel_nodes(self) -> int | None:
         """Kernel nodes in the captured graph (None when the runtime bindings are missing)."""
@@ -232,7 +271,10 @@ class BatchPipeline:
         for kind in ("tri", "point"):
             if kind not in self.batches:
                 continue
-            self.batches[kind].build(capi.QK_SCHEDULE_LOOP)
+            if self.builder == "lbvh":
+                self.batches[kind].build(capi.QK_SCHEDULE_LOOP)
+            else:
+                self.build_trees(kind)
             for ph in self.phases:
                 if ph.kind == kind:
                     self.run_phase(ph, schedule=capi.QK_SCHEDULE_LOOP)

@@ -114,6 +114,9 @@ def test_shipped_b200_table_is_valid():
     data = json.loads(autotune.SHIPPED.read_text())
     assert data["version"] == autotune.VERSION and data["entries"]
     for key, e in data["entries"].items():
-        assert "|batch:" in key
         p = e["params"]
+        if "|batch-step:" in key:
+            assert p["builder"] in ("lbvh", "sah8", "sah16", "sah32")
+            continue
+        assert "|batch:" in key
         assert all(p[k] in v for k, v in autotune.BATCH_SPACE.items()), (key, p)

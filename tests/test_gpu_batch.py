@@ -166,3 +166,22 @@ def test_batch_graph_capture_replays(cuda):
         cuda.cuda.synchronize()
         assert np.array_equal(out.cpu().numpy().view(np.uint64), want)
     b.sync()
+
+
+@pytest.mark.parametrize("bins", [8, 32])
+def test_batch_sah_trees_give_oracle_results(cuda, bins):
+    """Per-scene SAH builds into the batch arena: valid trees whose batched query results
+    equal the oracle's (results do not depend on the tree)."""
+    cfg = small_config()
+    b = capi.Batch("tri", [s.items for s in cfg.terrains], wide=True)
+    b.build_sah(bins)
+    b.sync()
+    for i in range(len(cfg.terrains)):
+        assert b.view(i).validate() == [0] * 8
+    rays, counts = _queries(cfg.terrains, "rays")
+    for flags in (0, capi.QK_WIDE | capi.QK_ORDER_MORTON):
+        plan = b.plan(capi.QK_OP_RAY, counts, flags=flags)
+        out = cuda.zeros(rays.shape[0], dtype=cuda.int64, device="cuda")
+        plan.query(_dev(rays), out)
+        want = np.concatenate([oracle.LBVH("tri", s.items).raycast(s.rays) for s in cfg.terrains])
+        assert np.array_equal(out.cpu().numpy().view(np.uint64), want)

@@ -761,17 +761,22 @@ def rays_arm(args, world, rank, local):
     nrays = cfg.rays.shape[0]
 
     # ---- builds (timed beside the step): LBVH and binned SAH with 32 bins ----
+    tris_d = capi.to_device(cfg.tris, np.float32)
+
     def timed_build(builder):
-        times, tr = [], None
-        for _ in range(3):
-            tr = None
+        """Device build time (CUDA events) of qk_build from device-resident triangles; the
+        call includes its depth read-back (and the SAH level read-backs)."""
+        tr = capi.DeviceTree("tri", tris_d, builder=builder, sah_bins=32)
+        times = []
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            tr.build()
+            e1.record()
             torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            tr = capi.DeviceTree("tri", cfg.tris, builder=builder, sah_bins=32)
-            torch.cuda.synchronize()
-            times.append((time.perf_counter() - t0) * 1e3)
+            times.append(e0.elapsed_time(e1))
         tr.build_wide()
-        return tr, float(min(times))
+        return tr, float(np.median(times))
 
     trees, build_ms = {}, {}
     for b in ("lbvh", "sah"):
@@ -784,7 +789,8 @@ def rays_arm(args, world, rank, local):
     dyn, occ, mort = capi.QK_TUNE_DYNAMIC, capi.QK_TUNE_HIGH_OCC, capi.QK_ORDER_MORTON
     modes = {"bin": 0, "bin_morton": mort, "wide": capi.QK_WIDE,
              "wide_morton": capi.QK_WIDE | mort, "bin_occ": occ, "bin_morton_occ": mort | occ,
-             "bin_dyn": dyn, "bin_morton_dyn": mort | dyn, "bin_morton_dyn_occ": mort | dyn | occ}
+             "bin_dyn": dyn, "bin_morton_dyn": mort | dyn, "bin_morton_dyn_occ": mort | dyn | occ,
+             "bin_sm": capi.QK_TUNE_SHORT_STACK, "bin_occ_sm": occ | capi.QK_TUNE_SHORT_STACK}
     variants = {f"{b}_{m}": (b, f) for b in trees for m, f in modes.items()}
     if args.only:
         variants = {args.only: variants[args.only]}

@@ -53,6 +53,7 @@ extern "C" {
 /* tuning flags (same results, different schedules; chosen by the autotuner) */
 #define QK_TUNE_DYNAMIC 256u     /* persistent warps fetching new rays as lanes finish */
 #define QK_TUNE_HIGH_OCC 512u    /* register cap for 5 resident blocks of 256 per SM */
+#define QK_TUNE_SHORT_STACK 2048u /* binary rays: top 8 stack entries per thread in shared memory */
 #define QK_TUNE_SPLIT 1024u      /* closest / kNN / radius on binary nodes: one warp per query,
                                     lanes on disjoint subtrees sharing the pruning bound */
 

@@ -95,7 +95,7 @@ __global__ __launch_bounds__(kBlock) void k_pos_keys(const float* __restrict__ p
 // ---------------------------------------------------------------------------------------
 // single-tree kernels: one thread per ray / query point, bodies in qk_traverse.cuh
 // ---------------------------------------------------------------------------------------
-template <bool kStats, int kMinBlocks>
+template <bool kStats, int kMinBlocks, int kShort = 0>
 __global__ __launch_bounds__(kBlock, kMinBlocks) void k_ray_bin(const BNode* __restrict__ bn,
                                                    const float4* __restrict__ leaves,
                                                    const Node* __restrict__ nodes,
@@ -110,9 +110,21 @@ __global__ __launch_bounds__(kBlock, kMinBlocks) void k_ray_bin(const BNode* __r
     if (active) {
         const int r = order ? static_cast<int>(order[i]) : i;
         const RayPre R = prepare_ray(__ldg(rays + 2 * r), __ldg(rays + 2 * r + 1));
-        LocalStack<kStack> st;
         int best_id;
-        out[r] = ray_bin_one(bn, leaves, root_box(nodes), R, max_iter, st, tv, best_id);
+        if constexpr (kShort > 0) {
+            // the top kShort entries of every thread's stack in shared memory
+            __shared__ int sn[kShort * kBlock];
+            __shared__ float sk[kShort * kBlock];
+            SplitStack<kStack> st;
+            st.snode = sn + threadIdx.x;
+            st.skey = sk + threadIdx.x;
+            st.sh = kShort;
+            st.stride = kBlock;
+            out[r] = ray_bin_one(bn, leaves, root_box(nodes), R, max_iter, st, tv, best_id);
+        } else {
+            LocalStack<kStack> st;
+            out[r] = ray_bin_one(bn, leaves, root_box(nodes), R, max_iter, st, tv, best_id);
+        }
         if (ids) ids[r] = best_id;
     }
     flush_stats<kStats>(active, tv.nodes, tv.leaves, tv.overflow, stats);
@@ -1018,7 +1030,13 @@ int ray_query(const qk_tree* t, const void* rays, int count, uint64_t* out, int*
     } else {
         const BNode* bn = static_cast<const BNode*>(t->bnodes);
         const Node* nodes = static_cast<const Node*>(t->nodes);
-        if (flags & QK_TUNE_HIGH_OCC) {
+        if ((flags & QK_TUNE_HIGH_OCC) && (flags & QK_TUNE_SHORT_STACK)) {
+            if (stt) k_ray_bin<true, 5, 8><<<g, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, ids, t->n * 2 + 64, stt);
+            else k_ray_bin<false, 5, 8><<<g, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, ids, t->n * 2 + 64, stt);
+        } else if (flags & QK_TUNE_SHORT_STACK) {
+            if (stt) k_ray_bin<true, 1, 8><<<g, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, ids, t->n * 2 + 64, stt);
+            else k_ray_bin<false, 1, 8><<<g, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, ids, t->n * 2 + 64, stt);
+        } else if (flags & QK_TUNE_HIGH_OCC) {
             if (stt) k_ray_bin<true, 5><<<g, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, ids, t->n * 2 + 64, stt);
             else k_ray_bin<false, 5><<<g, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, ids, t->n * 2 + 64, stt);
         } else {

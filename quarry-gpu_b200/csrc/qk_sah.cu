@@ -230,59 +230,147 @@ __global__ __launch_bounds__(kBlock) void k_level_bins(Level L, const int* __res
     }
 }
 
-// Sweep 3 x (bins - 1) candidate planes of one range given its bins (ordered-uint words).
-// Returns the chosen (axis, first right bin) as axis * 256 + bin and the left count, or -1
-// when no plane separates the centroids.
-__device__ int sweep_bins(const unsigned* B, int bins, int count, int* left_out) {
+// Sweep of 3 x (bins - 1) candidate planes of one range given its bins (ordered-uint words),
+// by one warp: plane b (between bins b-1 and b) costs area(left) * nL + area(right) * nR over
+// the bins' primitive boxes; planes with an empty side are skipped; the cheapest wins, ties
+// to the lowest axis and then the lowest plane.  Returns axis * 256 + plane and the left
+// count, or -1 when no plane separates the centroids.
+// Lane l owns bins 2l and 2l+1; prefix and suffix boxes and counts come from warp scans (min /
+// max and integer sums are exact, so every cost equals a sequential sweep's).  All 32 lanes
+// call it; all get the result.
+__device__ int warp_sweep_bins(const unsigned* B, int bins, int count, int* left_out) {
+    const int lane = threadIdx.x & 31;
     float best = kInf;
     int best_split = -1, best_left = 0;
+    const float3 elo = f3(kInf, kInf, kInf), ehi = f3(-kInf, -kInf, -kInf);
+    auto uni = [](float3& lo, float3& hi, float3 l2, float3 h2) {
+        lo = f3(fminf(lo.x, l2.x), fminf(lo.y, l2.y), fminf(lo.z, l2.z));
+        hi = f3(fmaxf(hi.x, h2.x), fmaxf(hi.y, h2.y), fmaxf(hi.z, h2.z));
+    };
+    auto shfl3 = [](float3 v, int src) {
+        return f3(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src),
+                  __shfl_sync(0xffffffffu, v.z, src));
+    };
     for (int a = 0; a < 3; ++a) {
-        // suffix boxes from the right
-        float3 slo[kMaxBins], shi[kMaxBins];
-        float3 rlo = f3(kInf, kInf, kInf), rhi = f3(-kInf, -kInf, -kInf);
-        for (int b = bins - 1; b >= 0; --b) {
-            const unsigned* w = B + (a * bins + b) * kBinWords;
-            if (w[0]) {
-                rlo = f3(fminf(rlo.x, unord_f(w[1])), fminf(rlo.y, unord_f(w[2])), fminf(rlo.z, unord_f(w[3])));
-                rhi = f3(fmaxf(rhi.x, unord_f(w[4])), fmaxf(rhi.y, unord_f(w[5])), fmaxf(rhi.z, unord_f(w[6])));
+        float3 lo[2], hi[2];
+        int c[2];
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const int b = 2 * lane + k;
+            lo[k] = elo;
+            hi[k] = ehi;
+            c[k] = 0;
+            if (b < bins) {
+                const unsigned* w = B + (a * bins + b) * kBinWords;
+                c[k] = static_cast<int>(w[0]);
+                if (c[k]) {
+                    lo[k] = f3(unord_f(w[1]), unord_f(w[2]), unord_f(w[3]));
+                    hi[k] = f3(unord_f(w[4]), unord_f(w[5]), unord_f(w[6]));
+                }
             }
-            slo[b] = rlo;
-            shi[b] = rhi;
         }
-        float3 llo = f3(kInf, kInf, kInf), lhi = f3(-kInf, -kInf, -kInf);
-        int lc = 0;
-        for (int b = 0; b < bins - 1; ++b) {
-            const unsigned* w = B + (a * bins + b) * kBinWords;
-            lc += static_cast<int>(w[0]);
-            if (w[0]) {
-                llo = f3(fminf(llo.x, unord_f(w[1])), fminf(llo.y, unord_f(w[2])), fminf(llo.z, unord_f(w[3])));
-                lhi = f3(fmaxf(lhi.x, unord_f(w[4])), fmaxf(lhi.y, unord_f(w[5])), fmaxf(lhi.z, unord_f(w[6])));
+        // lane totals, exclusive prefix from the lower lanes, exclusive suffix from the upper
+        float3 tlo = lo[0], thi = hi[0];
+        uni(tlo, thi, lo[1], hi[1]);
+        const int tc = c[0] + c[1];
+        float3 plo = tlo, phi = thi;
+        int pc = tc;
+        float3 qlo = tlo, qhi = thi;
+        int qc = tc;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const float3 ul = shfl3(plo, max(lane - o, 0)), uh = shfl3(phi, max(lane - o, 0));
+            const int ucnt = __shfl_sync(0xffffffffu, pc, max(lane - o, 0));
+            const float3 dl = shfl3(qlo, min(lane + o, 31)), dh = shfl3(qhi, min(lane + o, 31));
+            const int dcnt = __shfl_sync(0xffffffffu, qc, min(lane + o, 31));
+            if (lane >= o) {
+                uni(plo, phi, ul, uh);
+                pc += ucnt;
             }
-            if (lc == 0 || lc == count) continue;
-            const float cost = half_area(llo, lhi) * static_cast<float>(lc) +
-                               half_area(slo[b + 1], shi[b + 1]) * static_cast<float>(count - lc);
-            if (cost < best) {
-                best = cost;
-                best_split = a * 256 + (b + 1);
-                best_left = lc;
+            if (lane + o < 32) {
+                uni(qlo, qhi, dl, dh);
+                qc += dcnt;
             }
+        }
+        // exclusive = inclusive of the neighbour
+        float3 xlo = shfl3(plo, max(lane - 1, 0)), xhi = shfl3(phi, max(lane - 1, 0));
+        int xc = __shfl_sync(0xffffffffu, pc, max(lane - 1, 0));
+        float3 ylo = shfl3(qlo, min(lane + 1, 31)), yhi = shfl3(qhi, min(lane + 1, 31));
+        int yc = __shfl_sync(0xffffffffu, qc, min(lane + 1, 31));
+        if (lane == 0) {
+            xlo = elo;
+            xhi = ehi;
+            xc = 0;
+        }
+        if (lane == 31) {
+            ylo = elo;
+            yhi = ehi;
+            yc = 0;
+        }
+        // left prefix through bin 2l and 2l+1; right suffix from bin 2l+1 and 2l+2
+        float3 l0lo = xlo, l0hi = xhi;
+        uni(l0lo, l0hi, lo[0], hi[0]);
+        const int l0c = xc + c[0];
+        float3 l1lo = l0lo, l1hi = l0hi;
+        uni(l1lo, l1hi, lo[1], hi[1]);
+        const int l1c = l0c + c[1];
+        float3 r1lo = ylo, r1hi = yhi;  // suffix from bin 2l+1
+        uni(r1lo, r1hi, lo[1], hi[1]);
+        const float3 r2lo = ylo, r2hi = yhi;  // suffix from bin 2l+2
+        float lcost = kInf;
+        int lsplit = 0x7fffffff, lleft = 0;
+        // plane after bin 2l (valid when 2l <= bins - 2)
+        if (2 * lane <= bins - 2 && l0c != 0 && l0c != count) {
+            lcost = half_area(l0lo, l0hi) * static_cast<float>(l0c) +
+                    half_area(r1lo, r1hi) * static_cast<float>(count - l0c);
+            lsplit = 2 * lane + 1;
+            lleft = l0c;
+        }
+        if (2 * lane + 1 <= bins - 2 && l1c != 0 && l1c != count) {
+            const float cost = half_area(l1lo, l1hi) * static_cast<float>(l1c) +
+                               half_area(r2lo, r2hi) * static_cast<float>(count - l1c);
+            if (cost < lcost) {
+                lcost = cost;
+                lsplit = 2 * lane + 2;
+                lleft = l1c;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const float oc = __shfl_xor_sync(0xffffffffu, lcost, o);
+            const int os = __shfl_xor_sync(0xffffffffu, lsplit, o);
+            const int ol = __shfl_xor_sync(0xffffffffu, lleft, o);
+            if (oc < lcost || (oc == lcost && os < lsplit)) {
+                lcost = oc;
+                lsplit = os;
+                lleft = ol;
+            }
+        }
+        if (lcost < best) {
+            best = lcost;
+            best_split = a * 256 + lsplit;
+            best_left = lleft;
         }
     }
     *left_out = best_left;
     return best_split;
 }
 
+// one warp per range
 __global__ __launch_bounds__(kBlock) void k_level_split(Level L, int ntask, int bins) {
-    const int t = blockIdx.x * kBlock + threadIdx.x;
+    const int t = (blockIdx.x * kBlock + threadIdx.x) >> 5;
     if (t >= ntask) return;
     const Task tk = L.tasks[t];
     const int count = tk.end - tk.begin;
     int lc = 0;
-    int s = sweep_bins(L.bins + static_cast<size_t>(t) * 3 * kMaxBins * kBinWords, bins, count, &lc);
+    int s = warp_sweep_bins(L.bins + static_cast<size_t>(t) * 3 * kMaxBins * kBinWords, bins,
+                            count, &lc);
     if (s >= 0 && tk.depth + 1 + ceil_log2(max(lc, count - lc)) > kMaxDepth) s = -1;
     if (s < 0) lc = count / 2;
-    L.split[t] = s;
-    L.left_count[t] = lc;
+    if ((threadIdx.x & 31) == 0) {
+        L.split[t] = s;
+        L.left_count[t] = lc;
+    }
 }
 
 __device__ __forceinline__ bool goes_left(int split, int pos, int begin, int lc, float4 c,
@@ -473,6 +561,9 @@ struct Piece {
 };
 
 constexpr int kPieceCap = 128;  // block pieces pending (DFS: at most depth + 1)
+constexpr int kMediumRange = 256;  // pieces of 33..256 primitives go to one warp each
+constexpr int kWarpStack = 16;     // pending pieces > 32 inside one medium piece
+constexpr int kMediumCap = kBlockRange / (kWarpRange + 1) + 1;
 
 // Warp-level exact SAH over <= 32 primitives at positions [b, b + c) of the block's range.
 __device__ void warp_build(int* perm, const float4* sc, const float4* slo, const float4* shi,
@@ -586,6 +677,119 @@ __device__ void warp_build(int* perm, const float4* sc, const float4* slo, const
     }
 }
 
+// One warp builds the subtree of a medium piece (33..kMediumRange primitives) with the block
+// tier's algorithm -- centroid bounds, binned SAH (warp-private bins), stable partition --
+// recursing until pieces reach 32, which it finishes with warp_build.  Node ids come from
+// the piece's reserved range (root.ids: count - 2 ids) in a fixed order, so the tree does
+// not depend on how warps are scheduled.
+__device__ void warp_piece_tree(Piece root, int* perm, int* tmp, const float4* sc,
+                                const float4* slo, const float4* shi, unsigned* wb, Piece* wstk,
+                                int bins, Node* nodes, BNode* bn, int* parent, int n, int gbase,
+                                int* err) {
+    const int lane = threadIdx.x & 31;
+    int next = root.ids;
+    if (lane == 0) wstk[0] = root;
+    int top = 1;
+    __syncwarp();
+    int guard = 0;
+    while (top > 0 && guard++ < 4 * kMediumRange) {
+        const Piece pc = wstk[top - 1];
+        --top;
+        __syncwarp();
+        float lo[3] = {kInf, kInf, kInf}, hi[3] = {-kInf, -kInf, -kInf};
+        for (int i = lane; i < pc.count; i += 32) {
+            const float4 c = sc[perm[pc.begin + i]];
+            lo[0] = fminf(lo[0], c.x);
+            lo[1] = fminf(lo[1], c.y);
+            lo[2] = fminf(lo[2], c.z);
+            hi[0] = fmaxf(hi[0], c.x);
+            hi[1] = fmaxf(hi[1], c.y);
+            hi[2] = fmaxf(hi[2], c.z);
+        }
+        for (int a = 0; a < 3; ++a) {
+            for (int o = 16; o > 0; o >>= 1) {
+                lo[a] = fminf(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], o));
+                hi[a] = fmaxf(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], o));
+            }
+        }
+        for (int j = lane; j < 3 * bins * kBinWords; j += 32) {
+            const int w = j % kBinWords;
+            wb[j] = w == 0 ? 0u : (w <= 3 ? ord_f(kInf) : ord_f(-kInf));
+        }
+        __syncwarp();
+        for (int i = lane; i < pc.count; i += 32) {
+            const int li = perm[pc.begin + i];
+            const float4 c = sc[li], l = slo[li], h = shi[li];
+            const float cv[3] = {c.x, c.y, c.z};
+            for (int a = 0; a < 3; ++a) {
+                unsigned* w = wb + (a * bins + bin_of(cv[a], lo[a], hi[a], bins)) * kBinWords;
+                atomicAdd(&w[0], 1u);
+                atomicMin(&w[1], ord_f(l.x));
+                atomicMin(&w[2], ord_f(l.y));
+                atomicMin(&w[3], ord_f(l.z));
+                atomicMax(&w[4], ord_f(h.x));
+                atomicMax(&w[5], ord_f(h.y));
+                atomicMax(&w[6], ord_f(h.z));
+            }
+        }
+        __syncwarp();
+        int lc = 0;
+        int sp = warp_sweep_bins(wb, bins, pc.count, &lc);
+        if (sp >= 0 && pc.depth + 1 + ceil_log2(max(lc, pc.count - lc)) > kMaxDepth) sp = -1;
+        if (sp < 0) lc = pc.count / 2;
+        // stable partition: left side in position order, then the right side
+        int carry = 0;
+        for (int base = 0; base < pc.count; base += 32) {
+            const int i = base + lane;
+            bool f = false;
+            if (i < pc.count) {
+                if (sp < 0) {
+                    f = i < lc;
+                } else {
+                    const int a = sp >> 8;
+                    const float4 c = sc[perm[pc.begin + i]];
+                    const float v = a == 0 ? c.x : (a == 1 ? c.y : c.z);
+                    f = bin_of(v, lo[a], hi[a], bins) < (sp & 255);
+                }
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, f);
+            const int lrank = carry + __popc(m & ((1u << lane) - 1u));
+            if (i < pc.count) tmp[pc.begin + (f ? lrank : lc + (i - lrank))] = perm[pc.begin + i];
+            carry += __popc(m);
+        }
+        __syncwarp();
+        for (int i = lane; i < pc.count; i += 32) perm[pc.begin + i] = tmp[pc.begin + i];
+        __syncwarp();
+        const int rc = pc.count - lc;
+        const int lid = lc >= 2 ? next++ : n - 1 + gbase + pc.begin;
+        const int rid = rc >= 2 ? next++ : n - 1 + gbase + pc.begin + lc;
+        if (lane == 0) link(nodes, bn, parent, pc.node, lid, rid, n);
+        const Piece L = Piece{pc.begin, lc, lid, pc.depth + 1, 0};
+        const Piece R = Piece{pc.begin + lc, rc, rid, pc.depth + 1, 0};
+        for (int k = 0; k < 2; ++k) {
+            const Piece q = k == 0 ? L : R;
+            if (q.count >= 2 && q.count <= kWarpRange) {
+                warp_build(perm, sc, slo, shi, q.begin, q.count, q.node, q.depth, next, nodes, bn,
+                           parent, n, gbase);
+                next += q.count - 2;
+            }
+        }
+        for (int k = 0; k < 2; ++k) {
+            const Piece q = k == 0 ? R : L;
+            if (q.count > kWarpRange) {
+                if (top < kWarpStack) {
+                    if (lane == 0) wstk[top] = q;
+                    ++top;
+                } else if (lane == 0) {
+                    atomicAdd(err, 1);
+                }
+            }
+        }
+        __syncwarp();
+    }
+    if (top > 0 && lane == 0) atomicAdd(err, 1);
+}
+
 __global__ __launch_bounds__(kBlock) void k_block_build(const Task* __restrict__ tasks, int ntask,
                                                        const int* __restrict__ id_base,
                                                        int* __restrict__ order,
@@ -601,14 +805,20 @@ __global__ __launch_bounds__(kBlock) void k_block_build(const Task* __restrict__
     int* perm = reinterpret_cast<int*>(shi + kBlockRange);  // position -> load index
     int* tmp = perm + kBlockRange;                          // partition scratch
     int* sid = tmp + kBlockRange;                           // load index -> scene index
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned* wbins = reinterpret_cast<unsigned*>(sid + kBlockRange) +
+                      static_cast<size_t>(warp) * 3 * bins * kBinWords;  // this warp's bins
+    Piece* wstk = reinterpret_cast<Piece*>(reinterpret_cast<unsigned*>(sid + kBlockRange) +
+                                           static_cast<size_t>(kBlock / 32) * 3 * bins * kBinWords) +
+                  warp * kWarpStack;
     __shared__ unsigned sb[3 * kMaxBins * kBinWords];
     __shared__ Piece pieces[kPieceCap];
     __shared__ Piece wpieces[kBlockRange / 2];
-    __shared__ int npieces, nw, next_id, wsum[kBlock / 32];
+    __shared__ Piece mpieces[kMediumCap];
+    __shared__ int npieces, nw, nm, next_id, wsum[kBlock / 32];
     __shared__ unsigned sbu[6];
     __shared__ float sbf[6];
     __shared__ int s_split, s_left;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
     for (int ti = blockIdx.x; ti < ntask; ti += gridDim.x) {
         const Task tk = tasks[ti];
@@ -628,10 +838,14 @@ __global__ __launch_bounds__(kBlock) void k_block_build(const Task* __restrict__
         if (threadIdx.x == 0) {
             npieces = 0;
             nw = 0;
+            nm = 0;
             next_id = id_base[ti];
-            if (count > kWarpRange) {
+            if (count > kMediumRange) {
                 pieces[0] = Piece{0, count, tk.node, tk.depth, 0};
                 npieces = 1;
+            } else if (count > kWarpRange) {
+                mpieces[0] = Piece{0, count, tk.node, tk.depth, id_base[ti]};
+                nm = 1;
             } else {
                 wpieces[0] = Piece{0, count, tk.node, tk.depth, id_base[ti]};
                 nw = 1;
@@ -693,16 +907,18 @@ __global__ __launch_bounds__(kBlock) void k_block_build(const Task* __restrict__
                 }
             }
             __syncthreads();
-            if (threadIdx.x == 0) {
+            if (warp == 0) {
                 int lc = 0;
-                int sp = sweep_bins(sb, bins, pc.count, &lc);
+                int sp = warp_sweep_bins(sb, bins, pc.count, &lc);
                 if (sp >= 0 && pc.depth + 1 + ceil_log2(max(lc, pc.count - lc)) > kMaxDepth) sp = -1;
                 if (sp < 0) lc = pc.count / 2;
-                s_split = sp;
-                s_left = lc;
-                for (int a = 0; a < 3; ++a) {
-                    sbf[a] = cbl[a];
-                    sbf[3 + a] = cbh[a];
+                if (lane == 0) {
+                    s_split = sp;
+                    s_left = lc;
+                    for (int a = 0; a < 3; ++a) {
+                        sbf[a] = cbl[a];
+                        sbf[3 + a] = cbh[a];
+                    }
                 }
             }
             __syncthreads();
@@ -749,8 +965,13 @@ __global__ __launch_bounds__(kBlock) void k_block_build(const Task* __restrict__
                 const Piece R = Piece{pc.begin + lc, rc, rid, pc.depth + 1, 0};
                 for (int k = 0; k < 2; ++k) {
                     Piece q = k == 0 ? R : L;
-                    if (q.count > kWarpRange) {
+                    if (q.count > kMediumRange) {
                         if (npieces < kPieceCap) pieces[npieces++] = q;
+                        else atomicAdd(err, 1);
+                    } else if (q.count > kWarpRange) {
+                        q.ids = next_id;
+                        next_id += q.count - 2;
+                        if (nm < kMediumCap) mpieces[nm++] = q;
                         else atomicAdd(err, 1);
                     } else if (q.count >= 2) {
                         q.ids = next_id;
@@ -764,6 +985,11 @@ __global__ __launch_bounds__(kBlock) void k_block_build(const Task* __restrict__
         }
         if (threadIdx.x == 0 && npieces > 0) atomicAdd(err, 1);
         __syncthreads();
+        const int total_m = nm;
+        for (int m = warp; m < total_m; m += kBlock / 32)
+            warp_piece_tree(mpieces[m], perm, tmp, sc, slo, shi, wbins, wstk, bins, nodes, bn,
+                            parent, n, tk.begin, err);
+        __syncthreads();
         const int total_w = nw;
         for (int w = warp; w < total_w; w += kBlock / 32) {
             const Piece q = wpieces[w];
@@ -776,7 +1002,14 @@ __global__ __launch_bounds__(kBlock) void k_block_build(const Task* __restrict__
     }
 }
 
-constexpr size_t kBlockSmem = 3 * kBlockRange * sizeof(float4) + 3 * kBlockRange * sizeof(int);
+constexpr size_t kBlockSmemBase = 3 * kBlockRange * sizeof(float4) + 3 * kBlockRange * sizeof(int);
+
+// dynamic shared memory of k_block_build: the range arrays plus every warp's bins and stack
+size_t block_smem(int bins) {
+    return kBlockSmemBase + static_cast<size_t>(kBlock / 32) *
+                                (3 * static_cast<size_t>(bins) * kBinWords * sizeof(unsigned) +
+                                 kWarpStack * sizeof(Piece));
+}
 
 // leaves of the final order: sorted items, ids, inverse map, canonical leaf nodes, payload
 template <class Ops>
@@ -902,7 +1135,7 @@ int build_sah_impl(qk_tree* t, int bins, const void* items_v, void* ws, cudaStre
         if (e != cudaSuccess) return cuda_status(e, "SAH level prep");
         k_level_cbounds<<<nch, kBlock, 0, s>>>(w.L, ord, w.cen);
         k_level_bins<<<nch, kBlock, 0, s>>>(w.L, ord, w.cen, w.plo, w.phi, bins);
-        k_level_split<<<blocks_for(nbig), kBlock, 0, s>>>(w.L, nbig, bins);
+        k_level_split<<<blocks_for(static_cast<long long>(nbig) * 32), kBlock, 0, s>>>(w.L, nbig, bins);
         k_level_count_left<<<nch, kBlock, 0, s>>>(w.L, ord, w.cen, bins);
         k_level_prefix_left<<<blocks_for(nbig), kBlock, 0, s>>>(w.L, nbig);
         k_level_partition<<<nch, kBlock, 0, s>>>(w.L, ord, alt, w.cen, bins);
@@ -935,9 +1168,10 @@ int build_sah_impl(qk_tree* t, int bins, const void* items_v, void* ws, cudaStre
         }
         k_add_base<<<blocks_for(nblk), kBlock, 0, s>>>(w.id_base, nblk, w.L.counters);
         const int grid = min(nblk, 148 * 4);
+        const size_t smem = block_smem(bins);
         cudaFuncSetAttribute(k_block_build, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(kBlockSmem));
-        k_block_build<<<grid, kBlock, kBlockSmem, s>>>(w.blocks, nblk, w.id_base, ord, w.cen,
+                             static_cast<int>(block_smem(kMaxBins)));
+        k_block_build<<<grid, kBlock, smem, s>>>(w.blocks, nblk, w.id_base, ord, w.cen,
                                                        w.plo, w.phi, nodes, bn, t->parent, n, bins,
                                                        err);
     } else {

@@ -206,7 +206,7 @@ RAY_SPACE = {
     "builder": ["sah32", "lbvh", "sah16", "sah8"],
     "layout": ["bin", "wide"],
     "order": ["input", "morton"],
-    "schedule": ["occ", "plain", "dyn", "dyn_occ"],
+    "schedule": ["occ", "plain", "dyn", "dyn_occ", "sm", "occ_sm"],
 }
 
 
@@ -223,5 +223,7 @@ def ray_flags(p: dict) -> int:
         f |= capi.QK_ORDER_MORTON
     if p["layout"] == "bin":
         f |= {"plain": 0, "occ": capi.QK_TUNE_HIGH_OCC, "dyn": capi.QK_TUNE_DYNAMIC,
-              "dyn_occ": capi.QK_TUNE_DYNAMIC | capi.QK_TUNE_HIGH_OCC}[p["schedule"]]
+              "dyn_occ": capi.QK_TUNE_DYNAMIC | capi.QK_TUNE_HIGH_OCC,
+              "sm": capi.QK_TUNE_SHORT_STACK,
+              "occ_sm": capi.QK_TUNE_HIGH_OCC | capi.QK_TUNE_SHORT_STACK}[p["schedule"]]
     return f

@@ -339,7 +339,7 @@ def test_raycast_host_pipeline_matches(cuda):
         assert np.array_equal(host_out.numpy().view(np.uint64), want)
 
 
-@pytest.mark.parametrize("tune", ["dyn", "occ", "dyn_occ"])
+@pytest.mark.parametrize("tune", ["dyn", "occ", "dyn_occ", "sm", "occ_sm"])
 @pytest.mark.parametrize("morton", [False, True])
 def test_raycast_tuning_flags_same_bits(cuda, tune, morton):
     tris = scenes()["city"]
@@ -348,7 +348,9 @@ def test_raycast_tuning_flags_same_bits(cuda, tune, morton):
     rays = workloads.cosine_rays(50_003, float(lo[0]), float(hi[0]), float(lo[1]), float(hi[1]),
                                  float(hi[2]) + 5.0, 11)
     flags = {"dyn": capi.QK_TUNE_DYNAMIC, "occ": capi.QK_TUNE_HIGH_OCC,
-             "dyn_occ": capi.QK_TUNE_DYNAMIC | capi.QK_TUNE_HIGH_OCC}[tune]
+             "dyn_occ": capi.QK_TUNE_DYNAMIC | capi.QK_TUNE_HIGH_OCC,
+             "sm": capi.QK_TUNE_SHORT_STACK,
+             "occ_sm": capi.QK_TUNE_HIGH_OCC | capi.QK_TUNE_SHORT_STACK}[tune]
     if morton:
         flags |= capi.QK_ORDER_MORTON
     rd = _dev(rays)

@@ -97,7 +97,7 @@ struct Level {
     int* counters;      // [0] chunks, [1] next big tasks, [2] block tasks, [3] internal base
 };
 
-// single block: chunk list of the current tasks, bin reset
+// single block: chunk list of the current tasks
 __global__ __launch_bounds__(1024) void k_level_prep(Level L, int ntask, int bins) {
     __shared__ int carry;
     if (threadIdx.x == 0) carry = 0;
@@ -132,24 +132,23 @@ __global__ __launch_bounds__(1024) void k_level_prep(Level L, int ntask, int bin
                 L.chunk_task[excl + c] = t;
                 L.chunk_begin[excl + c] = L.tasks[t].begin + c * kChunk;
             }
-            for (int a = 0; a < 3; ++a) {
-                L.cb[6 * t + a] = ord_f(kInf);
-                L.cb[6 * t + 3 + a] = ord_f(-kInf);
-            }
-            unsigned* B = L.bins + static_cast<size_t>(t) * 3 * kMaxBins * kBinWords;
-            for (int j = 0; j < 3 * bins; ++j) {
-                B[j * kBinWords] = 0u;
-                for (int k = 0; k < 3; ++k) {
-                    B[j * kBinWords + 1 + k] = ord_f(kInf);
-                    B[j * kBinWords + 4 + k] = ord_f(-kInf);
-                }
-            }
         }
         __syncthreads();
         if (threadIdx.x == 1023) carry = excl + nch;
         __syncthreads();
     }
     if (threadIdx.x == 0) L.counters[0] = carry;
+}
+
+// one block per range: reset its centroid bounds and bins
+__global__ __launch_bounds__(kBlock) void k_level_reset(Level L, int bins) {
+    const int t = blockIdx.x;
+    if (threadIdx.x < 6) L.cb[6 * t + threadIdx.x] = threadIdx.x < 3 ? ord_f(kInf) : ord_f(-kInf);
+    unsigned* B = L.bins + static_cast<size_t>(t) * 3 * kMaxBins * kBinWords;
+    for (int j = threadIdx.x; j < 3 * bins * kBinWords; j += kBlock) {
+        const int w = j % kBinWords;
+        B[j] = w == 0 ? 0u : (w <= 3 ? ord_f(kInf) : ord_f(-kInf));
+    }
 }
 
 __global__ __launch_bounds__(kBlock) void k_level_cbounds(Level L, const int* __restrict__ order,
@@ -566,51 +565,64 @@ constexpr int kWarpStack = 16;     // pending pieces > 32 inside one medium piec
 constexpr int kMediumCap = kBlockRange / (kWarpRange + 1) + 1;
 
 // Warp-level exact SAH over <= 32 primitives at positions [b, b + c) of the block's range.
+// Each primitive stays in the lane that loaded it ("item" = that lane's index).  The items are
+// ranked once per axis by centroid (ties by position); ord[a] in lane p is the item at
+// position p of the axis-a order.  Every node owns the same position segment [s, s + m) in
+// all three orders: its split sweeps each axis order with warp scans (left box of the first
+// r + 1 items, right box of the rest) and takes the cheapest plane (lowest axis, then lowest
+// plane, on ties; a count split when no plane is allowed by the depth limit), and the three
+// orders are then stably partitioned by side, so the children own [s, s + k) and
+// [s + k, s + m) again.  Two-item nodes split 1 | 1 without a sweep.  At the end position p
+// of the axis-0 order is leaf slot b + p.  `scratch` holds 32 ints of this warp.
 __device__ void warp_build(int* perm, const float4* sc, const float4* slo, const float4* shi,
                            int b, int c, int node, int depth, int next_id, Node* nodes, BNode* bn,
-                           int* parent, int n, int gbase) {
+                           int* parent, int n, int gbase, int* scratch) {
     const int lane = threadIdx.x & 31;
-    int stk_b[kWarpRange], stk_c[kWarpRange], stk_n[kWarpRange], stk_d[kWarpRange];
-    int top = 0;
-    stk_b[0] = b;
-    stk_c[0] = c;
+    const bool mine = lane < c;
+    const int li = perm[b + (mine ? lane : 0)];
+    const float4 cc = sc[li], blo = slo[li], bhi = shi[li];
+    int ord[3];
+    for (int a = 0; a < 3; ++a) {
+        const float key = mine ? (a == 0 ? cc.x : (a == 1 ? cc.y : cc.z)) : kInf;
+        int rank = 0;
+        for (int j = 0; j < kWarpRange; ++j) {
+            const float kj = __shfl_sync(0xffffffffu, key, j);
+            if (j < c && (kj < key || (kj == key && j < lane))) ++rank;
+        }
+        if (mine) scratch[rank] = lane;
+        __syncwarp();
+        ord[a] = mine ? scratch[lane] : lane;
+        __syncwarp();
+    }
+    int stk_s[kWarpRange], stk_m[kWarpRange], stk_n[kWarpRange], stk_d[kWarpRange];
+    stk_s[0] = 0;
+    stk_m[0] = c;
     stk_n[0] = node;
     stk_d[0] = depth;
-    top = 1;
+    int top = 1;
     int guard = 0;
+    const float3 elo = f3(kInf, kInf, kInf), ehi = f3(-kInf, -kInf, -kInf);
     while (top > 0 && guard++ < 4 * kWarpRange) {
         --top;
-        const int rb = stk_b[top], rc = stk_c[top], rn = stk_n[top], rd = stk_d[top];
-        const bool mine = lane < rc;
-        const int li = perm[rb + (mine ? lane : 0)];
-        const float4 cc = sc[li], lo = slo[li], hi = shi[li];
+        const int s = stk_s[top], m = stk_m[top], rn = stk_n[top], rd = stk_d[top];
+        if (m == 2) {
+            if (lane == 0) link(nodes, bn, parent, rn, n - 1 + gbase + b + s, n - 1 + gbase + b + s + 1, n);
+            continue;
+        }
         float best = kInf;
-        int best_axis = -1, best_k = rc / 2;
-        int rank_axis[3] = {lane, lane, lane};
+        int best_axis = -1, best_k = m / 2;
+        const int r = lane;
         for (int a = 0; a < 3; ++a) {
-            const float key = mine ? (a == 0 ? cc.x : (a == 1 ? cc.y : cc.z)) : kInf;
-            int rank = 0;
-            for (int j = 0; j < kWarpRange; ++j) {
-                const float kj = __shfl_sync(0xffffffffu, key, j);
-                if (j < rc && (kj < key || (kj == key && j < lane))) ++rank;
+            const int it = __shfl_sync(0xffffffffu, ord[a], min(s + r, 31));
+            float3 lo = f3(__shfl_sync(0xffffffffu, blo.x, it), __shfl_sync(0xffffffffu, blo.y, it),
+                           __shfl_sync(0xffffffffu, blo.z, it));
+            float3 hi = f3(__shfl_sync(0xffffffffu, bhi.x, it), __shfl_sync(0xffffffffu, bhi.y, it),
+                           __shfl_sync(0xffffffffu, bhi.z, it));
+            if (r >= m) {
+                lo = elo;
+                hi = ehi;
             }
-            rank = mine ? rank : lane;
-            rank_axis[a] = rank;
-            // lane r takes the boxes of the item ranked r
-            int src = lane;
-            for (int j = 0; j < kWarpRange; ++j) {
-                const int rj = __shfl_sync(0xffffffffu, rank, j);
-                if (j < rc && rj == lane) src = j;
-            }
-            float3 blo = f3(__shfl_sync(0xffffffffu, lo.x, src), __shfl_sync(0xffffffffu, lo.y, src),
-                            __shfl_sync(0xffffffffu, lo.z, src));
-            float3 bhi = f3(__shfl_sync(0xffffffffu, hi.x, src), __shfl_sync(0xffffffffu, hi.y, src),
-                            __shfl_sync(0xffffffffu, hi.z, src));
-            if (lane >= rc) {
-                blo = f3(kInf, kInf, kInf);
-                bhi = f3(-kInf, -kInf, -kInf);
-            }
-            float3 plo = blo, phi = bhi, qlo = blo, qhi = bhi;
+            float3 plo = lo, phi = hi, qlo = lo, qhi = hi;
             for (int o = 1; o < 32; o <<= 1) {
                 const float3 ulo = f3(__shfl_up_sync(0xffffffffu, plo.x, o), __shfl_up_sync(0xffffffffu, plo.y, o), __shfl_up_sync(0xffffffffu, plo.z, o));
                 const float3 uhi = f3(__shfl_up_sync(0xffffffffu, phi.x, o), __shfl_up_sync(0xffffffffu, phi.y, o), __shfl_up_sync(0xffffffffu, phi.z, o));
@@ -625,14 +637,14 @@ __device__ void warp_build(int* perm, const float4* sc, const float4* slo, const
                     qhi = f3(fmaxf(qhi.x, dhi.x), fmaxf(qhi.y, dhi.y), fmaxf(qhi.z, dhi.z));
                 }
             }
-            // split after sorted item `lane`: left [0, lane], right [lane + 1, rc)
+            // plane after position r: left r + 1 items, right the rest
             const float3 rlo = f3(__shfl_down_sync(0xffffffffu, qlo.x, 1), __shfl_down_sync(0xffffffffu, qlo.y, 1), __shfl_down_sync(0xffffffffu, qlo.z, 1));
             const float3 rhi = f3(__shfl_down_sync(0xffffffffu, qhi.x, 1), __shfl_down_sync(0xffffffffu, qhi.y, 1), __shfl_down_sync(0xffffffffu, qhi.z, 1));
-            const int kl = lane + 1;
+            const int kl = r + 1;
             float cost = kInf;
-            if (kl < rc && rd + 1 + ceil_log2(max(kl, rc - kl)) <= kMaxDepth) {
+            if (kl < m && rd + 1 + ceil_log2(max(kl, m - kl)) <= kMaxDepth) {
                 cost = half_area(plo, phi) * static_cast<float>(kl) +
-                       half_area(rlo, rhi) * static_cast<float>(rc - kl);
+                       half_area(rlo, rhi) * static_cast<float>(m - kl);
             }
             float bc = cost;
             int bk = kl;
@@ -650,31 +662,50 @@ __device__ void warp_build(int* perm, const float4* sc, const float4* slo, const
                 best_k = bk;
             }
         }
-        // reorder the range by the chosen axis; with no finite cost halve the x order
-        const int r = rank_axis[best_axis < 0 ? 0 : best_axis];
-        __syncwarp();
-        if (mine) perm[rb + r] = li;
-        __syncwarp();
-        const int kl = best_k, kr = rc - best_k;
-        const int lid = kl >= 2 ? next_id++ : n - 1 + gbase + rb;
-        const int rid = kr >= 2 ? next_id++ : n - 1 + gbase + rb + kl;
+        const int axis = best_axis < 0 ? 0 : best_axis;
+        const int k = best_k;
+        // items of the left side (bit per item), then a stable partition of every order
+        const int ax_ord = axis == 0 ? ord[0] : (axis == 1 ? ord[1] : ord[2]);
+        const int it = __shfl_sync(0xffffffffu, ax_ord, min(s + r, 31));
+        const unsigned leftmask = __reduce_or_sync(0xffffffffu, (r < k) ? (1u << it) : 0u);
+        const bool inseg = lane >= s && lane < s + m;
+        const unsigned segmask = __ballot_sync(0xffffffffu, inseg);
+        for (int a = 0; a < 3; ++a) {
+            const int item = ord[a];
+            const bool left = inseg && ((leftmask >> item) & 1u);
+            const unsigned lm = __ballot_sync(0xffffffffu, left);
+            const int below = __popc(lm & ((1u << lane) - 1u));
+            const int segbelow = __popc(segmask & ((1u << lane) - 1u));  // = lane - s in the segment
+            const int pos = left ? s + below : s + k + (segbelow - below);
+            if (inseg) scratch[pos] = item;
+            __syncwarp();
+            if (inseg) ord[a] = scratch[lane];
+            __syncwarp();
+        }
+        const int kr = m - k;
+        const int lid = k >= 2 ? next_id++ : n - 1 + gbase + b + s;
+        const int rid = kr >= 2 ? next_id++ : n - 1 + gbase + b + s + k;
         if (lane == 0) link(nodes, bn, parent, rn, lid, rid, n);
         if (kr >= 2 && top < kWarpRange) {
-            stk_b[top] = rb + kl;
-            stk_c[top] = kr;
+            stk_s[top] = s + k;
+            stk_m[top] = kr;
             stk_n[top] = rid;
             stk_d[top] = rd + 1;
             ++top;
         }
-        if (kl >= 2 && top < kWarpRange) {
-            stk_b[top] = rb;
-            stk_c[top] = kl;
+        if (k >= 2 && top < kWarpRange) {
+            stk_s[top] = s;
+            stk_m[top] = k;
             stk_n[top] = lid;
             stk_d[top] = rd + 1;
             ++top;
         }
-        __syncwarp();
     }
+    // leaf order: position p of the axis-0 order
+    const int src = __shfl_sync(0xffffffffu, li, ord[0]);
+    __syncwarp();
+    if (mine) perm[b + lane] = src;
+    __syncwarp();
 }
 
 // One warp builds the subtree of a medium piece (33..kMediumRange primitives) with the block
@@ -684,8 +715,8 @@ __device__ void warp_build(int* perm, const float4* sc, const float4* slo, const
 // not depend on how warps are scheduled.
 __device__ void warp_piece_tree(Piece root, int* perm, int* tmp, const float4* sc,
                                 const float4* slo, const float4* shi, unsigned* wb, Piece* wstk,
-                                int bins, Node* nodes, BNode* bn, int* parent, int n, int gbase,
-                                int* err) {
+                                int* scratch, int bins, Node* nodes, BNode* bn, int* parent, int n,
+                                int gbase, int* err) {
     const int lane = threadIdx.x & 31;
     int next = root.ids;
     if (lane == 0) wstk[0] = root;
@@ -770,7 +801,7 @@ __device__ void warp_piece_tree(Piece root, int* perm, int* tmp, const float4* s
             const Piece q = k == 0 ? L : R;
             if (q.count >= 2 && q.count <= kWarpRange) {
                 warp_build(perm, sc, slo, shi, q.begin, q.count, q.node, q.depth, next, nodes, bn,
-                           parent, n, gbase);
+                           parent, n, gbase, scratch);
                 next += q.count - 2;
             }
         }
@@ -808,9 +839,10 @@ __global__ __launch_bounds__(kBlock) void k_block_build(const Task* __restrict__
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     unsigned* wbins = reinterpret_cast<unsigned*>(sid + kBlockRange) +
                       static_cast<size_t>(warp) * 3 * bins * kBinWords;  // this warp's bins
-    Piece* wstk = reinterpret_cast<Piece*>(reinterpret_cast<unsigned*>(sid + kBlockRange) +
-                                           static_cast<size_t>(kBlock / 32) * 3 * bins * kBinWords) +
-                  warp * kWarpStack;
+    Piece* wstk_all = reinterpret_cast<Piece*>(reinterpret_cast<unsigned*>(sid + kBlockRange) +
+                                               static_cast<size_t>(kBlock / 32) * 3 * bins * kBinWords);
+    Piece* wstk = wstk_all + warp * kWarpStack;
+    int* wscratch = reinterpret_cast<int*>(wstk_all + (kBlock / 32) * kWarpStack) + warp * 32;
     __shared__ unsigned sb[3 * kMaxBins * kBinWords];
     __shared__ Piece pieces[kPieceCap];
     __shared__ Piece wpieces[kBlockRange / 2];
@@ -987,14 +1019,14 @@ __global__ __launch_bounds__(kBlock) void k_block_build(const Task* __restrict__
         __syncthreads();
         const int total_m = nm;
         for (int m = warp; m < total_m; m += kBlock / 32)
-            warp_piece_tree(mpieces[m], perm, tmp, sc, slo, shi, wbins, wstk, bins, nodes, bn,
-                            parent, n, tk.begin, err);
+            warp_piece_tree(mpieces[m], perm, tmp, sc, slo, shi, wbins, wstk, wscratch, bins,
+                            nodes, bn, parent, n, tk.begin, err);
         __syncthreads();
         const int total_w = nw;
         for (int w = warp; w < total_w; w += kBlock / 32) {
             const Piece q = wpieces[w];
             warp_build(perm, sc, slo, shi, q.begin, q.count, q.node, q.depth, q.ids, nodes, bn,
-                       parent, n, tk.begin);
+                       parent, n, tk.begin, wscratch);
         }
         __syncthreads();
         for (int i = threadIdx.x; i < count; i += kBlock) order[tk.begin + i] = sid[perm[i]];
@@ -1008,7 +1040,7 @@ constexpr size_t kBlockSmemBase = 3 * kBlockRange * sizeof(float4) + 3 * kBlockR
 size_t block_smem(int bins) {
     return kBlockSmemBase + static_cast<size_t>(kBlock / 32) *
                                 (3 * static_cast<size_t>(bins) * kBinWords * sizeof(unsigned) +
-                                 kWarpStack * sizeof(Piece));
+                                 kWarpStack * sizeof(Piece) + 32 * sizeof(int));
 }
 
 // leaves of the final order: sorted items, ids, inverse map, canonical leaf nodes, payload
@@ -1129,6 +1161,7 @@ int build_sah_impl(qk_tree* t, int bins, const void* items_v, void* ws, cudaStre
         if (++level > kMaxDepth) return fail(QK_ERR_DEPTH, "SAH: too many levels");
         w.L.tasks = cur;
         k_level_prep<<<1, 1024, 0, s>>>(w.L, nbig, bins);
+        k_level_reset<<<nbig, kBlock, 0, s>>>(w.L, bins);
         int nch = 0;
         cudaError_t e = cudaMemcpyAsync(&nch, w.L.counters, sizeof(int), cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);

@@ -754,6 +754,8 @@ __global__ __launch_bounds__(kBlock) void k_radius_split(
 }
 
 // ---- segment sort of the radius keys ----
+constexpr int kWarpSortMax = 1024;   // largest segment sorted by one warp
+constexpr int kWarpSortBlock = 128;  // threads per block of the warp sort
 // all-ascending bitonic network: comparator (i, i ^ (2^j - 1)) then (i, i ^ stride) for
 // shrinking strides, smaller key to the lower index.  Indices >= m are virtual +inf and never
 // move, so a segment of any length sorts in place without padding writes.
@@ -783,7 +785,7 @@ __global__ __launch_bounds__(kBlock) void k_seg_sort_warp(const int* __restrict_
     if (m <= 1) return;
     if (m > 32) {
         if (lane == 0) {
-            if (m <= 4096) medium[atomicAdd(&h->list_count[0], 1)] = q;
+            if (m <= kWarpSortMax) medium[atomicAdd(&h->list_count[0], 1)] = q;
             else large[atomicAdd(&h->list_count[1], 1)] = q;
         }
         return;
@@ -800,45 +802,82 @@ __global__ __launch_bounds__(kBlock) void k_seg_sort_warp(const int* __restrict_
     if (lane < m) keys[b + lane] = v;
 }
 
-// one block per listed segment: shared memory (m <= 4096) or global memory in place
-template <bool kShared>
+// t-th comparator (i, j) of the bitonic stage (size, stride)
+__device__ __forceinline__ void bitonic_pair(int t, int size, int stride, int& i, int& j) {
+    const int blk = t / stride, off = t % stride;
+    if (stride == (size >> 1)) {
+        i = blk * size + off;
+        j = blk * size + size - 1 - off;
+    } else {
+        i = blk * 2 * stride + off;
+        j = i + stride;
+    }
+}
+
+// one warp per listed segment of 33..kWarpSortMax keys, sorted in the warp's shared memory
+// (only warp barriers between stages)
+__global__ __launch_bounds__(kWarpSortBlock) void k_seg_sort_warp_smem(
+    const int* __restrict__ offsets, unsigned long long* __restrict__ keys,
+    const int* __restrict__ list, const Header* __restrict__ h) {
+    __shared__ unsigned long long sm[kWarpSortBlock / 32][kWarpSortMax];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    unsigned long long* a = sm[w];
+    const int n_list = h->list_count[0];
+    const int warps = gridDim.x * (kWarpSortBlock / 32);
+    for (int e = blockIdx.x * (kWarpSortBlock / 32) + w; e < n_list; e += warps) {
+        const int q = list[e];
+        const int b = offsets[q];
+        const int m = min(offsets[q + 1] - b, kWarpSortMax);
+        for (int t = lane; t < m; t += 32) a[t] = keys[b + t];
+        int pow2 = 32;
+        while (pow2 < m) pow2 <<= 1;
+        __syncwarp();
+        for (int size = 2; size <= pow2; size <<= 1) {
+            for (int stride = size >> 1; stride > 0; stride >>= 1) {
+                for (int t = lane; t < pow2 / 2; t += 32) {
+                    int i, j;
+                    bitonic_pair(t, size, stride, i, j);
+                    if (i < m) cswap(a, i, j, m);
+                }
+                __syncwarp();
+            }
+        }
+        for (int t = lane; t < m; t += 32) keys[b + t] = a[t];
+        __syncwarp();
+    }
+}
+
+// one block per listed segment of more than kWarpSortMax keys: in shared memory up to 4096,
+// in place in global memory beyond
 __global__ __launch_bounds__(kBlock) void k_seg_sort_block(const int* __restrict__ offsets,
                                                           unsigned long long* __restrict__ keys,
                                                           const int* __restrict__ list,
-                                                          const Header* __restrict__ h, int which) {
-    __shared__ unsigned long long sm[kShared ? 4096 : 1];
-    const int n_list = h->list_count[which];
+                                                          const Header* __restrict__ h) {
+    __shared__ unsigned long long sm[4096];
+    const int n_list = h->list_count[1];
     for (int e = blockIdx.x; e < n_list; e += gridDim.x) {
         const int q = list[e];
         const int b = offsets[q];
         const int m = offsets[q + 1] - b;
-        unsigned long long* a = kShared ? sm : keys + b;
-        if (kShared) {
+        const bool shared = m <= 4096;
+        unsigned long long* a = shared ? sm : keys + b;
+        if (shared) {
             for (int t = threadIdx.x; t < m; t += kBlock) sm[t] = keys[b + t];
-            __syncthreads();
         }
+        __syncthreads();
         int pow2 = 1;
         while (pow2 < m) pow2 <<= 1;
         for (int size = 2; size <= pow2; size <<= 1) {
             for (int stride = size >> 1; stride > 0; stride >>= 1) {
                 for (int t = threadIdx.x; t < pow2 / 2; t += kBlock) {
-                    // t-th comparator of this stage
                     int i, j;
-                    if (stride == (size >> 1)) {
-                        const int blk = t / stride, off = t % stride;
-                        i = blk * size + off;
-                        j = blk * size + size - 1 - off;
-                    } else {
-                        const int blk = t / stride, off = t % stride;
-                        i = blk * 2 * stride + off;
-                        j = i + stride;
-                    }
+                    bitonic_pair(t, size, stride, i, j);
                     if (i < m) cswap(a, i, j, m);
                 }
                 __syncthreads();
             }
         }
-        if (kShared) {
+        if (shared) {
             for (int t = threadIdx.x; t < m; t += kBlock) keys[b + t] = sm[t];
         }
         __syncthreads();
@@ -1152,8 +1191,8 @@ int radius_sort_segments(const int* offsets, int count, uint64_t* keys, int* med
     k_bounds_reset<<<1, 32, 0, s>>>(h, 0);
     k_seg_sort_warp<<<blocks_for(count, kBlock / 32), kBlock, 0, s>>>(offsets, count, k64, medium,
                                                                       large, h, cap);
-    k_seg_sort_block<true><<<148 * 2, kBlock, 0, s>>>(offsets, k64, medium, h, 0);
-    k_seg_sort_block<false><<<148, kBlock, 0, s>>>(offsets, k64, large, h, 1);
+    k_seg_sort_warp_smem<<<148 * 8, kWarpSortBlock, 0, s>>>(offsets, k64, medium, h);
+    k_seg_sort_block<<<148 * 2, kBlock, 0, s>>>(offsets, k64, large, h);
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? QK_OK : cuda_status(e, "radius sort");
 }

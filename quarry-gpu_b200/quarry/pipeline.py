@@ -234,7 +234,7 @@ class BatchPipeline:
         self.builder = res.params["builder"]
         for kind in self.batches:
             self.build_trees(kind)
-        self.sync()
+            self.batches[kind].sync()
         tuner.save()
         return {"params": res.params, "ms": round(res.ms, 3), "cached": res.cached,
                 "source": res.source, "points": [(t["params"]["builder"], t["ms"])

@@ -405,3 +405,27 @@ def test_split_knn_sphere_matches_oracle(cuda):
     assert np.array_equal(got, ref.knn(q, 8))
     got = tree.closest(_dev(q), capi.QK_TUNE_SPLIT).cpu().numpy().view(np.uint32)
     assert np.array_equal(got, ref.closest(q))
+
+
+def test_radius_segment_sizes_all_sort_paths(cuda):
+    """Segments of 0..32 keys (warp registers), 33..1024 (warp shared memory), 1025..4096
+    (block shared memory) and more (block, global memory) all come out sorted as the oracle's."""
+    rng = np.random.default_rng(21)
+    pts = rng.uniform(0, 4, (60_000, 3)).astype(np.float32)
+    q = rng.uniform(0.5, 3.5, (400, 3)).astype(np.float32)
+    tree = capi.DeviceTree("point", pts)
+    ref = oracle.LBVH("point", pts)
+    dq = _dev(q)
+    for r in (0.15, 0.4, 0.75, 1.1):
+        want_off, want_keys = ref.radius(q, r)
+        sizes = np.diff(want_off)
+        for flags in (0, capi.QK_TUNE_SPLIT, capi.QK_ORDER_MORTON):
+            off, keys = tree.radius(dq, r, flags)
+            assert np.array_equal(off.cpu().numpy().astype(np.int64), want_off)
+            assert np.array_equal(keys.cpu().numpy().view(np.uint64), want_keys), (r, flags)
+        if r == 1.1:
+            assert sizes.max() > 4096
+        if r == 0.4:
+            assert ((sizes > 32) & (sizes <= 1024)).any()
+        if r == 0.75:
+            assert ((sizes > 1024) & (sizes <= 4096)).any()

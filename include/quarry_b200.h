@@ -272,6 +272,8 @@ typedef struct qk_batch_tune {
     int32_t blocks_per_sm;  /* persistent grid = SMs x blocks_per_sm (1..16) */
     int32_t short_stack;    /* stack entries per thread held in shared memory (0..32) */
     int32_t chunks_per_fetch; /* 32-query chunks a warp takes per counter fetch (1..64) */
+    int32_t split;          /* 1: closest / kNN / radius with one warp per query (binary
+                               nodes; see QK_TUNE_SPLIT); 0: one thread per query */
 } qk_batch_tune;
 
 /* flags: QK_WIDE reserves and builds the 4-wide nodes of every scene. */

@@ -339,6 +339,97 @@ __global__ __launch_bounds__(256) void k_bq(Q q, QArgs a) {
 
 __device__ __forceinline__ int max_iter_of(const qk_tree& t) { return t.n * 2 + 64; }
 
+// Split schedule of the persistent kernel: a warp takes chunks the same way, then answers
+// their queries one after another with the whole warp (qk_traverse.cuh *_split_one).
+template <class Q>
+__global__ __launch_bounds__(256) void k_bq_split(Q q, QArgs a) {
+    if (!q.enabled()) return;
+    Trav tv;
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        int c0 = 0;
+        if (lane == 0) c0 = atomicAdd(a.counter, a.per_fetch);
+        c0 = __shfl_sync(0xffffffffu, c0, 0);
+        if (c0 >= a.nchunks) break;
+        const int c1 = min(c0 + a.per_fetch, a.nchunks);
+        for (int c = c0; c < c1; ++c) {
+            const int2 ch = __ldg(a.chunks + c);
+            const int s = ch.x;
+            const int base = __ldg(a.q_off + s);
+            const int m = min(32, __ldg(a.q_off + s + 1) - base - ch.y);
+            for (int j = 0; j < m; ++j) {
+                const int pos = base + ch.y + j;
+                const int qi = a.order ? static_cast<int>(__ldg(a.order + pos)) : pos;
+                q.run_split(a.tab[s], s, qi, lane, tv);
+            }
+        }
+    }
+    flush_stats<false>(true, 0, 0, tv.overflow, a.stats);
+}
+
+template <class Ops>
+struct QClosestSplit {
+    const float* pts;
+    uint2* out;
+    __device__ bool enabled() const { return true; }
+    __device__ __forceinline__ void run_split(const BScene& sc, int, int q, int lane, Trav& tv) const {
+        const float3 p = f3(pts[3 * q], pts[3 * q + 1], pts[3 * q + 2]);
+        const uint2 r = closest_split_one<Ops>(static_cast<const BNode*>(sc.t.bnodes),
+                                               static_cast<const float4*>(sc.t.leaves), p, lane,
+                                               max_iter_of(sc.t), tv);
+        if (lane == 0) out[q] = r;
+    }
+};
+
+template <class Ops>
+struct QKnnSplit {
+    const float* pts;
+    uint2* out;
+    int k;
+    __device__ bool enabled() const { return true; }
+    __device__ __forceinline__ void run_split(const BScene& sc, int, int q, int lane, Trav& tv) const {
+        const float3 p = f3(pts[3 * q], pts[3 * q + 1], pts[3 * q + 2]);
+        WarpTable tab;
+        knn_split_one<Ops>(static_cast<const BNode*>(sc.t.bnodes),
+                           static_cast<const float4*>(sc.t.leaves), p, k, lane,
+                           max_iter_of(sc.t), tv, tab);
+        if (lane < k) out[static_cast<size_t>(q) * k + lane] = warp_table_entry(tab);
+    }
+};
+
+template <class Ops, bool kFill>
+struct QRadiusSplit {
+    const float* pts;
+    const float* radius;
+    int* counts;
+    int* lane_counts;  // queries x 32
+    const int* offsets;
+    unsigned long long* keys;
+    const int* total;
+    long long cap;
+    __device__ bool enabled() const { return !kFill || static_cast<long long>(*total) <= cap; }
+    __device__ __forceinline__ void run_split(const BScene& sc, int s, int q, int lane, Trav& tv) const {
+        const float3 p = f3(pts[3 * q], pts[3 * q + 1], pts[3 * q + 2]);
+        const float r = __ldg(radius + s);
+        const float r2 = r * r;
+        int write = 0, end = 0;
+        if (kFill) {
+            const int mine = lane_counts[static_cast<size_t>(q) * 32 + lane];
+            write = offsets[q] + warp_exclusive(mine, lane);
+            end = min(write + mine, offsets[q + 1]);
+        }
+        const int found = radius_split_one<Ops, kFill>(static_cast<const BNode*>(sc.t.bnodes),
+                                                       static_cast<const float4*>(sc.t.leaves),
+                                                       p, r2, lane, write, end, keys,
+                                                       max_iter_of(sc.t), tv);
+        if (!kFill) {
+            lane_counts[static_cast<size_t>(q) * 32 + lane] = found;
+            const int t = __reduce_add_sync(0xffffffffu, found);
+            if (lane == 0) counts[q] = t;
+        }
+    }
+};
+
 template <bool kWide>
 struct QRay {
     using Stack = SplitStack<kWide ? kStackWide : kStack>;
@@ -520,6 +611,7 @@ struct qk_batch_plan {
     void* scan_ws = nullptr;
     int* medium = nullptr;
     int* large = nullptr;
+    int* lane_counts = nullptr;
     void* loop_ws = nullptr;
     size_t loop_ws_bytes = 0;
     int sms = 148;
@@ -656,7 +748,7 @@ int batch_build_loop(qk_batch* b, int builder, int bins, cudaStream_t s) {
 // ---- queries ----
 struct PlanLayout {
     size_t qoff, chunks, counter, params, stats, hdr, keys, idx, keys_s, idx_s, sort_ws, counts,
-        scan_ws, medium, large, loop_ws, loop_ws_bytes, total;
+        scan_ws, medium, large, lane_counts, loop_ws, loop_ws_bytes, total;
     int nchunks;
 };
 
@@ -694,6 +786,7 @@ PlanLayout plan_layout(int op, const int32_t* counts, int scenes, unsigned flags
         L.scan_ws = take(scan_ws_bytes(n));
         L.medium = take(sizeof(int) * n);
         L.large = take(sizeof(int) * n);
+        L.lane_counts = take(sizeof(int) * static_cast<size_t>(n) * 32);
     }
     L.loop_ws_bytes = op == QK_OP_RADIUS ? radius_ws_bytes(max_q, flags) : order_ws_bytes(max_q);
     L.loop_ws = take(L.loop_ws_bytes);
@@ -728,6 +821,57 @@ int launch_bq(const Q& q, const qk_batch_plan* p, const qk_batch_tune& tune, cud
     k_bq<Q><<<grid, tune.block, smem, s>>>(q, a);
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? QK_OK : cuda_status(e, "batched query");
+}
+
+template <class Q>
+int launch_bq_split(const Q& q, const qk_batch_plan* p, const qk_batch_tune& tune,
+                    cudaStream_t s) {
+    QArgs a;
+    a.tab = p->b->d_tab;
+    a.chunks = p->d_chunks;
+    a.nchunks = p->nchunks;
+    a.q_off = p->d_qoff;
+    a.order = (p->flags & QK_ORDER_MORTON) ? p->idx_s : nullptr;
+    a.counter = p->d_counter;
+    a.per_fetch = tune.chunks_per_fetch;
+    a.short_stack = 0;
+    a.stats = p->d_stats;
+    const int grid = p->sms * tune.blocks_per_sm;
+    cudaMemsetAsync(p->d_counter, 0, sizeof(int), s);
+    k_bq_split<Q><<<grid, tune.block, 0, s>>>(q, a);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? QK_OK : cuda_status(e, "batched split query");
+}
+
+// closest / kNN / radius with one warp per query (binary nodes)
+template <class Ops>
+int batch_query_split(qk_batch_plan* p, const qk_batch_io& io, const qk_batch_tune& tune,
+                      cudaStream_t s) {
+    const int N = p->total;
+    const float* pts = static_cast<const float*>(io.input);
+    switch (p->op) {
+        case QK_OP_CLOSEST:
+            return launch_bq_split(QClosestSplit<Ops>{pts, static_cast<uint2*>(io.out)}, p, tune, s);
+        case QK_OP_KNN:
+            return launch_bq_split(QKnnSplit<Ops>{pts, static_cast<uint2*>(io.out), io.k}, p, tune, s);
+        case QK_OP_RADIUS: {
+            auto* keys = static_cast<unsigned long long*>(io.out);
+            QRadiusSplit<Ops, false> qc{pts, p->d_params, p->counts, p->lane_counts, nullptr,
+                                        nullptr, nullptr, -1};
+            int st = launch_bq_split(qc, p, tune, s);
+            if (st != QK_OK) return st;
+            const cudaError_t e = scan_exclusive(p->counts, io.offsets, N, true, p->scan_ws, s);
+            if (e != cudaSuccess) return cuda_status(e, "batched radius scan");
+            QRadiusSplit<Ops, true> qf{pts, p->d_params, nullptr, p->lane_counts, io.offsets, keys,
+                                       io.offsets + N, io.capacity};
+            st = launch_bq_split(qf, p, tune, s);
+            if (st != QK_OK) return st;
+            return radius_sort_segments(io.offsets, N, static_cast<uint64_t*>(io.out), p->medium,
+                                        p->large, p->d_hdr, io.capacity, s);
+        }
+        default:
+            return fail(QK_ERR_INVALID, "the split schedule serves closest, kNN and radius");
+    }
 }
 
 template <class Ops, bool kWide>
@@ -1055,6 +1199,7 @@ int qk_batch_plan_create(qk_batch_plan** out, const qk_batch* b, int op, const i
         p->scan_ws = base + L.scan_ws;
         p->medium = reinterpret_cast<int*>(base + L.medium);
         p->large = reinterpret_cast<int*>(base + L.large);
+        p->lane_counts = reinterpret_cast<int*>(base + L.lane_counts);
     }
     p->loop_ws = base + L.loop_ws;
     p->loop_ws_bytes = L.loop_ws_bytes;
@@ -1103,8 +1248,10 @@ int qk_batch_query(qk_batch_plan* p, const qk_batch_io* io, const qk_batch_tune*
     p->radius_total = -1;
     if (schedule == QK_SCHEDULE_LOOP) return batch_query_loop(p, *io, s);
     if (schedule != QK_SCHEDULE_BATCHED) return fail(QK_ERR_INVALID, "unknown schedule %u", schedule);
-    qk_batch_tune t = {128, 4, 8, 4};
+    qk_batch_tune t = {128, 4, 8, 4, 0};
     if (tune) t = *tune;
+    if (t.split && (p->op == QK_OP_RAY || (p->flags & QK_WIDE)))
+        return fail(QK_ERR_INVALID, "the split schedule serves closest, kNN and radius on binary nodes");
     if ((t.block != 64 && t.block != 128 && t.block != 256) || t.blocks_per_sm < 1 ||
         t.blocks_per_sm > 16 || t.short_stack < 0 || t.short_stack > kMaxShortStack ||
         t.chunks_per_fetch < 1 || t.chunks_per_fetch > 64)
@@ -1127,6 +1274,14 @@ int qk_batch_query(qk_batch_plan* p, const qk_batch_io* io, const qk_batch_tune*
         if (e != cudaSuccess) return cuda_status(e, "batched query order");
     }
     const bool wide = (p->flags & QK_WIDE) != 0;
+    if (t.split) {
+        switch (p->b->kind) {
+            case kTri: return batch_query_split<TriOps>(p, *io, t, s);
+            case kPoint: return batch_query_split<PointOps>(p, *io, t, s);
+            case kGauss: return batch_query_split<GaussOps>(p, *io, t, s);
+            default: return fail(QK_ERR_INVALID, "unknown primitive kind %d", p->b->kind);
+        }
+    }
     switch (p->b->kind) {
         case kTri: return wide ? batch_query_kind<TriOps, true>(p, *io, t, s)
                                : batch_query_kind<TriOps, false>(p, *io, t, s);

@@ -757,4 +757,324 @@ __device__ __forceinline__ int radius_wide_one(const WideNode* __restrict__ wn,
     return found;
 }
 
+// ---------------------------------------------------------------------------------------
+// split mode (QK_TUNE_SPLIT): one warp per query point.  The top kSplitLevels levels of the
+// binary tree are descended with lane l taking child bit ((l >> level) & 1), so the 32 lanes
+// own 32 disjoint subtrees (a leaf met on the way belongs to the lowest lane that reaches
+// it); each lane then runs the ordinary depth-first traversal of its subtree.  After every
+// step the warp shares its pruning bound by shuffles, so a query whose search touches much of
+// the tree (a point near the centre of a spherical shell) is spread over 32 lanes.  The
+// subtrees partition the leaves and the shared bound only ever comes from found candidates,
+// so results equal the one-thread-per-query kernels bit for bit.
+// ---------------------------------------------------------------------------------------
+constexpr int kSplitLevels = 5;
+
+__device__ __forceinline__ void warp_min_lex(float& d, int& id) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const float od = __shfl_xor_sync(0xffffffffu, d, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, id, o);
+        if (closer(od, oi, d, id)) {
+            d = od;
+            id = oi;
+        }
+    }
+}
+
+// Forced descent of lane `lane` from the root: returns the subtree root the lane owns (an
+// internal node) or -1; a leaf met on the way is handed to `on_leaf` by its owning lane.
+// `keep(box)` decides whether a child box can still hold a result.
+template <class Leaf, class Keep>
+__device__ __forceinline__ int split_descend(const BNode* __restrict__ bn, int lane, Leaf on_leaf,
+                                             Keep keep) {
+    int node = 0;
+    for (int d = 0; d < kSplitLevels; ++d) {
+        float3 llo, lhi, rlo, rhi;
+        int lref, rref;
+        load_bnode(bn, node, llo, lhi, rlo, rhi, lref, rref);
+        const bool right = ((lane >> d) & 1) != 0;
+        const int ref = right ? rref : lref;
+        const float3 lo = right ? rlo : llo;
+        const float3 hi = right ? rhi : lhi;
+        if (ref < 0) {
+            if ((lane >> (d + 1)) == 0 && keep(lo, hi)) on_leaf(~ref);
+            return -1;
+        }
+        if (!keep(lo, hi)) return -1;
+        node = ref;
+    }
+    return node;
+}
+
+template <class Ops>
+__device__ __forceinline__ uint2 closest_split_one(const BNode* __restrict__ bn,
+                                                   const float4* __restrict__ leaves, float3 p,
+                                                   int lane, int max_iter, Trav& tv) {
+    float best = kInf;
+    int best_id = 0x7fffffff;
+    auto on_leaf = [&](int slot) {
+        ++tv.leaves;
+        int id;
+        const float d2 = Ops::dist2(p, leaves, slot, id);
+        if (closer(d2, id, best, best_id)) {
+            best = d2;
+            best_id = id;
+        }
+    };
+    int node = split_descend(bn, lane, on_leaf, [](float3, float3) { return true; });
+    warp_min_lex(best, best_id);
+    LocalStack<kStack> st;
+    int sp = 0;
+    bool active = node >= 0;
+    for (int iter = 0; __any_sync(0xffffffffu, active); ++iter) {
+        if (active) {
+            if (iter >= max_iter) {
+                tv.overflow = true;
+                active = false;
+            } else {
+                ++tv.nodes;
+                float3 llo, lhi, rlo, rhi;
+                int lref, rref;
+                load_bnode(bn, node, llo, lhi, rlo, rhi, lref, rref);
+                const float dl = dist2_box(p, llo, lhi);
+                const float dr = dist2_box(p, rlo, rhi);
+                bool okl = dl <= best;
+                bool okr = dr <= best;
+                const bool lfirst = dl <= dr;
+                if (lfirst) {
+                    if (okl && lref < 0) { on_leaf(~lref); okl = false; }
+                    if (okr && rref < 0 && dr <= best) on_leaf(~rref);
+                    if (rref < 0) okr = false;
+                } else {
+                    if (okr && rref < 0) { on_leaf(~rref); okr = false; }
+                    if (okl && lref < 0 && dl <= best) on_leaf(~lref);
+                    if (lref < 0) okl = false;
+                }
+                if (okl && okr) {
+                    if (sp >= kStack) {
+                        tv.overflow = true;
+                        active = false;
+                    } else {
+                        st.put(sp++, lfirst ? rref : lref, lfirst ? dr : dl);
+                        node = lfirst ? lref : rref;
+                    }
+                } else if (okl) {
+                    node = lref;
+                } else if (okr) {
+                    node = rref;
+                } else {
+                    node = -1;
+                    while (sp > 0) {
+                        --sp;
+                        if (st.get_key(sp) <= best) {
+                            node = st.get_node(sp);
+                            break;
+                        }
+                    }
+                    if (node < 0) active = false;
+                }
+            }
+        }
+        warp_min_lex(best, best_id);
+    }
+    return best_id != 0x7fffffff ? make_uint2(__float_as_uint(best), static_cast<unsigned>(best_id))
+                                 : make_uint2(0u, 0xffffffffu);
+}
+
+// kNN, split: the k best candidates form ONE warp-wide sorted table, entry j held by lane j
+// (k <= 32), so every lane prunes with the exact k-th distance of everything found so far.
+// After each traversal step the lanes' new leaf candidates (up to two per lane) are inserted
+// one at a time: a ballot gives the insertion rank, a shuffle shifts the tail down.
+struct WarpTable {
+    float d;   // this lane's entry
+    int id;
+    float kd;  // entry k-1, broadcast
+    int kid;
+    __device__ __forceinline__ void init() {
+        d = kInf;
+        id = 0x7fffffff;
+        kd = kInf;
+        kid = 0x7fffffff;
+    }
+    __device__ __forceinline__ bool admits(float bound) const {
+        return kid == 0x7fffffff || bound <= kd;
+    }
+    // whole warp; x is the same on every lane
+    __device__ __forceinline__ void insert(float xd, int xid, int k, int lane) {
+        if (!closer(xd, xid, kd, kid)) return;
+        const unsigned before = __ballot_sync(0xffffffffu, lane < k && closer(d, id, xd, xid));
+        const int pos = __popc(before);
+        const float pd = __shfl_up_sync(0xffffffffu, d, 1);
+        const int pid = __shfl_up_sync(0xffffffffu, id, 1);
+        if (lane < k) {
+            if (lane == pos) {
+                d = xd;
+                id = xid;
+            } else if (lane > pos) {
+                d = pd;
+                id = pid;
+            }
+        }
+        kd = __shfl_sync(0xffffffffu, d, k - 1);
+        kid = __shfl_sync(0xffffffffu, id, k - 1);
+    }
+};
+
+// the warp's table holds the query's k best on return (entry j in lane j)
+template <class Ops>
+__device__ __forceinline__ void knn_split_one(const BNode* __restrict__ bn,
+                                              const float4* __restrict__ leaves, float3 p, int k,
+                                              int lane, int max_iter, Trav& tv, WarpTable& tab) {
+    tab.init();
+    tab.init();
+    // up to two pending leaf candidates per lane, inserted by the whole warp
+    float cd[2];
+    int cid[2];
+    bool has[2] = {false, false};
+    auto leaf = [&](int slot, int c) {
+        ++tv.leaves;
+        cd[c] = Ops::dist2(p, leaves, slot, cid[c]);
+        has[c] = true;
+    };
+    auto flush = [&]() {
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            unsigned m = __ballot_sync(0xffffffffu, has[c]);
+            while (m) {
+                const int src = __ffs(m) - 1;
+                const float xd = __shfl_sync(0xffffffffu, cd[c], src);
+                const int xid = __shfl_sync(0xffffffffu, cid[c], src);
+                tab.insert(xd, xid, k, lane);
+                m &= m - 1;
+            }
+            has[c] = false;
+        }
+    };
+    int node = split_descend(bn, lane, [&](int slot) { leaf(slot, 0); },
+                             [](float3, float3) { return true; });
+    flush();
+    LocalStack<kStack> st;
+    int sp = 0;
+    bool active = node >= 0;
+    for (int iter = 0; __any_sync(0xffffffffu, active); ++iter) {
+        if (active) {
+            if (iter >= max_iter) {
+                tv.overflow = true;
+                active = false;
+            } else {
+                ++tv.nodes;
+                float3 llo, lhi, rlo, rhi;
+                int lref, rref;
+                load_bnode(bn, node, llo, lhi, rlo, rhi, lref, rref);
+                const float dl = dist2_box(p, llo, lhi);
+                const float dr = dist2_box(p, rlo, rhi);
+                const bool lfirst = dl <= dr;
+                bool okl = tab.admits(dl);
+                bool okr = tab.admits(dr);
+                if (okl && lref < 0) { leaf(~lref, 0); okl = false; }
+                if (okr && rref < 0) { leaf(~rref, 1); okr = false; }
+                if (okl && okr) {
+                    if (sp >= kStack) {
+                        tv.overflow = true;
+                        active = false;
+                    } else {
+                        st.put(sp++, lfirst ? rref : lref, lfirst ? dr : dl);
+                        node = lfirst ? lref : rref;
+                    }
+                } else if (okl) {
+                    node = lref;
+                } else if (okr) {
+                    node = rref;
+                } else {
+                    node = -1;
+                    while (sp > 0) {
+                        --sp;
+                        if (tab.admits(st.get_key(sp))) {
+                            node = st.get_node(sp);
+                            break;
+                        }
+                    }
+                    if (node < 0) active = false;
+                }
+            }
+        }
+        flush();
+    }
+}
+
+__device__ __forceinline__ uint2 warp_table_entry(const WarpTable& tab) {
+    return tab.id != 0x7fffffff ? make_uint2(__float_as_uint(tab.d), static_cast<unsigned>(tab.id))
+                                : make_uint2(0u, 0xffffffffu);
+}
+
+// radius, split: returns this lane's count; the fill pass writes the lane's keys from
+// `write` on, never past `end` (the query's offset plus the counts of the lower lanes)
+template <class Ops, bool kFill>
+__device__ __forceinline__ int radius_split_one(const BNode* __restrict__ bn,
+                                                const float4* __restrict__ leaves, float3 p,
+                                                float r2, int lane, int write, int end,
+                                                unsigned long long* __restrict__ keys,
+                                                int max_iter, Trav& tv) {
+    int found = 0;
+    auto keep = [&](float3 lo, float3 hi) { return dist2_box(p, lo, hi) <= r2; };
+    auto on_leaf = [&](int slot) {
+        ++tv.leaves;
+        int id;
+        const float d2 = Ops::dist2(p, leaves, slot, id);
+        if (d2 <= r2) {
+            if (kFill && write < end) keys[write++] = radius_key(d2, id);
+            ++found;
+        }
+    };
+    int node = split_descend(bn, lane, on_leaf, keep);
+    LocalStack<kStack> st;
+    int sp = 0;
+    for (int iter = 0; node >= 0; ++iter) {
+        if (iter >= max_iter) {
+            tv.overflow = true;
+            break;
+        }
+        ++tv.nodes;
+        float3 llo, lhi, rlo, rhi;
+        int lref, rref;
+        load_bnode(bn, node, llo, lhi, rlo, rhi, lref, rref);
+        bool okl = keep(llo, lhi);
+        bool okr = keep(rlo, rhi);
+        if (okl && lref < 0) {
+            on_leaf(~lref);
+            okl = false;
+        }
+        if (okr && rref < 0) {
+            on_leaf(~rref);
+            okr = false;
+        }
+        if (okl && okr) {
+            if (sp >= kStack) {
+                tv.overflow = true;
+                break;
+            }
+            st.put_node(sp++, rref);
+            node = lref;
+        } else if (okl) {
+            node = lref;
+        } else if (okr) {
+            node = rref;
+        } else {
+            node = sp > 0 ? st.get_node(--sp) : -1;
+        }
+    }
+    return found;
+}
+
+// exclusive prefix over the lanes of `v`
+__device__ __forceinline__ int warp_exclusive(int v, int lane) {
+    int incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += u;
+    }
+    return incl - v;
+}
+
 }  // namespace qk

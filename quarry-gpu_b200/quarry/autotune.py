@@ -191,15 +191,28 @@ BATCH_SPACE = {
     "blocks_per_sm": [6, 4, 8, 2],
     "short_stack": [8, 0, 16],
     "chunks_per_fetch": [1, 4, 16],
+    "split": [0, 1],                       # one warp per query (closest / kNN / radius)
 }
 
 BATCH_START = {"flags": 1, "block": 128, "blocks_per_sm": 6, "short_stack": 8,
-               "chunks_per_fetch": 1}
+               "chunks_per_fetch": 1, "split": 0}
 
 
 def batch_launch(params: dict) -> dict:
     """The qk_batch_tune fields of a batch point."""
-    return {k: params[k] for k in ("block", "blocks_per_sm", "short_stack", "chunks_per_fetch")}
+    out = {k: params[k] for k in ("block", "blocks_per_sm", "short_stack", "chunks_per_fetch")}
+    out["split"] = params.get("split", 0)
+    return out
+
+
+def batch_valid(op: str):
+    """Points of BATCH_SPACE an operation accepts: the split schedule serves closest, kNN and
+    radius on binary nodes."""
+    def ok(p: dict) -> bool:
+        if not p.get("split", 0):
+            return True
+        return op != "rays" and not (p["flags"] & 4)
+    return ok
 
 
 RAY_SPACE = {

@@ -49,7 +49,8 @@ class QkTreeSizes(ctypes.Structure):
 
 class QkBatchTune(ctypes.Structure):
     _fields_ = [("block", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32),
-                ("short_stack", ctypes.c_int32), ("chunks_per_fetch", ctypes.c_int32)]
+                ("short_stack", ctypes.c_int32), ("chunks_per_fetch", ctypes.c_int32),
+                ("split", ctypes.c_int32)]
 
 
 class QkBatchIo(ctypes.Structure):
@@ -528,6 +529,7 @@ class BatchPlan:
             t.block, t.blocks_per_sm, t.short_stack, t.chunks_per_fetch = (
                 int(tune["block"]), int(tune["blocks_per_sm"]), int(tune["short_stack"]),
                 int(tune["chunks_per_fetch"]))
+            t.split = int(tune.get("split", 0))
             tp = ctypes.byref(t)
         check(lib().qk_batch_query(self.h, ctypes.byref(io), tp, schedule, _stream()),
               "qk_batch_query")

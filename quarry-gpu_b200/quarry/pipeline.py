@@ -130,7 +130,7 @@ class BatchPipeline:
     def signature(self, ph: Phase) -> str:
         n = int(sum(s.items.shape[0] for s in self.scenes[ph.kind]))
         return (f"batch:{ph.kind}:{ph.name}:scenes={len(ph.counts)}:prims={n}:"
-                f"queries={int(ph.counts.sum())}:k={self.k}")
+                f"queries={int(ph.counts.sum())}:k={self.k}:space=2")
 
     def tune(self, tuner: autotune.Autotuner, force: bool = False, repeats: int = 3) -> dict:
         report = {}
@@ -140,7 +140,8 @@ class BatchPipeline:
 
             res = tuner.search(self.signature(ph), autotune.BATCH_SPACE, run,
                                fingerprint=lambda params, ph=ph: self.fingerprint(ph),
-                               start=autotune.BATCH_START, repeats=repeats, force=force)
+                               start=autotune.BATCH_START, valid=autotune.batch_valid(ph.name),
+                               repeats=repeats, force=force)
             ph.params = dict(res.params)
             report[f"{ph.kind}_{ph.name}"] = {"params": res.params, "ms": round(res.ms, 4),
                                               "cached": res.cached, "source": res.source,

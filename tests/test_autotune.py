@@ -84,10 +84,18 @@ def test_invalid_points_are_skipped(tmp_path):
     assert all(c["b"] != "z" for c in calls)
 
 
+def test_batch_split_validity():
+    ok = autotune.batch_valid("rays")
+    assert ok({"flags": 1, "split": 0}) and not ok({"flags": 1, "split": 1})
+    ok = autotune.batch_valid("knn")
+    assert ok({"flags": 1, "split": 1}) and not ok({"flags": 5, "split": 1})
+    assert autotune.batch_launch({**autotune.BATCH_START, "split": 1})["split"] == 1
+
+
 def test_engine_spaces_are_consistent():
     assert all(autotune.BATCH_START[k] in v for k, v in autotune.BATCH_SPACE.items())
     assert set(autotune.batch_launch(autotune.BATCH_START)) == {
-        "block", "blocks_per_sm", "short_stack", "chunks_per_fetch"}
+        "block", "blocks_per_sm", "short_stack", "chunks_per_fetch", "split"}
     assert autotune.ray_valid({"layout": "wide", "schedule": "plain"})
     assert not autotune.ray_valid({"layout": "wide", "schedule": "dyn"})
     # the shared-memory short stack stays within 48 KB for every block size
@@ -119,4 +127,5 @@ def test_shipped_b200_table_is_valid():
             assert p["builder"] in ("lbvh", "sah8", "sah16", "sah32")
             continue
         assert "|batch:" in key
-        assert all(p[k] in v for k, v in autotune.BATCH_SPACE.items()), (key, p)
+        assert all(p.get(k, autotune.BATCH_START[k]) in v
+                   for k, v in autotune.BATCH_SPACE.items()), (key, p)

@@ -58,6 +58,7 @@ def _queries(cfg_scenes, field):
 
 TUNES = [None, {"block": 64, "blocks_per_sm": 8, "short_stack": 0, "chunks_per_fetch": 1},
          {"block": 256, "blocks_per_sm": 2, "short_stack": 16, "chunks_per_fetch": 8}]
+SPLIT = {"block": 128, "blocks_per_sm": 6, "short_stack": 0, "chunks_per_fetch": 2, "split": 1}
 
 
 @pytest.mark.parametrize("flags", [0, capi.QK_ORDER_MORTON, capi.QK_WIDE,
@@ -85,16 +86,19 @@ def test_batch_closest_knn_match_oracle(cuda, kind, flags, schedule):
     pts, counts = _queries(scenes, "closest")
     plan = b.plan(capi.QK_OP_CLOSEST, counts, flags=flags)
     out = cuda.zeros((pts.shape[0], 2), dtype=cuda.int32, device="cuda")
-    for tune in (TUNES if schedule == capi.QK_SCHEDULE_BATCHED else [None]):
+    tunes = TUNES + ([SPLIT] if not flags & capi.QK_WIDE else [])
+    for tune in (tunes if schedule == capi.QK_SCHEDULE_BATCHED else [None]):
         plan.query(_dev(pts), out, tune=tune, schedule=schedule)
         want = np.concatenate([oracle.LBVH(kind, s.items).closest(s.closest) for s in scenes])
         assert np.array_equal(out.cpu().numpy().view(np.uint32), want)
     pts, counts = _queries(scenes, "knn")
     plan = b.plan(capi.QK_OP_KNN, counts, flags=flags)
-    out = cuda.zeros((pts.shape[0], cfg.k, 2), dtype=cuda.int32, device="cuda")
-    plan.query(_dev(pts), out, k=cfg.k, schedule=schedule, tune=TUNES[2] if schedule == 0 else None)
     want = np.concatenate([oracle.LBVH(kind, s.items).knn(s.knn, cfg.k) for s in scenes])
-    assert np.array_equal(out.cpu().numpy().view(np.uint32), want)
+    tunes = [TUNES[2]] + ([SPLIT] if not flags & capi.QK_WIDE else [])
+    for tune in (tunes if schedule == capi.QK_SCHEDULE_BATCHED else [None]):
+        out = cuda.zeros((pts.shape[0], cfg.k, 2), dtype=cuda.int32, device="cuda")
+        plan.query(_dev(pts), out, k=cfg.k, schedule=schedule, tune=tune)
+        assert np.array_equal(out.cpu().numpy().view(np.uint32), want)
 
 
 @pytest.mark.parametrize("kind", ["tri", "point"])
@@ -109,7 +113,9 @@ def test_batch_radius_matches_oracle(cuda, kind, flags, schedule):
     total = sum(int(w[0][-1]) for w in want)
     keys = cuda.zeros(total + 16, dtype=cuda.int64, device="cuda")
     offsets = cuda.zeros(pts.shape[0] + len(scenes) + 1, dtype=cuda.int32, device="cuda")
-    plan.query(_dev(pts), keys, offsets=offsets, capacity=keys.numel(), schedule=schedule)
+    tune = SPLIT if schedule == capi.QK_SCHEDULE_BATCHED and not flags & capi.QK_WIDE else None
+    plan.query(_dev(pts), keys, offsets=offsets, capacity=keys.numel(), schedule=schedule,
+               tune=tune)
     got_total, ovf = plan.status()
     assert got_total == total and ovf == 0
     off = offsets.cpu().numpy().astype(np.int64)

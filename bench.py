@@ -277,6 +277,20 @@ def grad_arm(args, world, rank, local):
 
     g_build()
     build_ms = timed(g_build, 5)
+    # forward schedule: every variant returns the same bits; the fastest is timed
+    state["tree"].build_wide()
+    fwd_variants = {"morton": capi.QK_ORDER_MORTON, "input": 0,
+                    "split_morton": capi.QK_ORDER_MORTON | capi.QK_TUNE_SPLIT,
+                    "wide_morton": capi.QK_ORDER_MORTON | capi.QK_WIDE}
+    base = state["tree"].closest(q, 0).clone()
+    fwd_by = {}
+    for name, f in fwd_variants.items():
+        if not torch.equal(state["tree"].closest(q, f), base):
+            raise RuntimeError(f"Gaussian closest variant {name} differs")
+        flags = f
+        fwd_by[name] = timed(g_fwd, 5)
+    fwd_variant = min(fwd_by, key=fwd_by.get)
+    flags = fwd_variants[fwd_variant]
     fwd_ms = timed(g_fwd, 10)
     bwd_ms = timed(g_bwd, 10)
 
@@ -288,7 +302,7 @@ def grad_arm(args, world, rank, local):
     tri_tree = capi.DeviceTree("tri", tris)
 
     def r_fwd():
-        state["out"], state["ids"] = tri_tree.raycast_ids(rays, flags)
+        state["out"], state["ids"] = tri_tree.raycast_ids(rays, capi.QK_ORDER_MORTON)
 
     def r_bwd():
         state["rg"] = tri_tree.ray_t_grad(rays, state["ids"], None, with_rays=False)
@@ -306,6 +320,8 @@ def grad_arm(args, world, rank, local):
                            "queries": nq, "rays": nr, "terrain_grid": grid,
                            "order": "morton", "l2": "flushed between timed steps"},
                 "gaussian": {"build_ms": round(build_ms, 3), "forward_ms": round(fwd_ms, 4),
+                             "forward_variant": fwd_variant,
+                             "forward_variants_ms": {k: round(v, 4) for k, v in fwd_by.items()},
                              "backward_ms": round(bwd_ms, 4),
                              "fwd_bwd_over_fwd": round((fwd_ms + bwd_ms) / fwd_ms, 4),
                              "mqueries_per_s": round(nq / (fwd_ms * 1e-3) / 1e6, 2)},

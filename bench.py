@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--small", action="store_true", help="small inputs (profiling captures)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--only", default="", help="time only this variant (profiling)")
+    ap.add_argument("--dump", default="", help="also write the inputs as QRYD / QRCD files "
+                                                "into this directory (for other engines)")
     args = ap.parse_args()
     if args.steps is None:
         args.steps = 20 if args.workload == "batch" else 400
@@ -356,6 +358,11 @@ def points_arm(args, world, rank, local):
         tree = capi.DeviceTree("point", pts)
         tree.build_wide()
         clouds[kind] = {"pts": pts, "q": q, "q_d": capi.to_device(q, np.float32), "tree": tree}
+        if args.dump and rank == 0:
+            from quarry import dumps
+
+            Path(args.dump).mkdir(parents=True, exist_ok=True)
+            dumps.write_qrcd(Path(args.dump) / f"points_{kind}.qrcd", pts, q)
 
     def timed(fn, steps, warm=3):
         for _ in range(warm):
@@ -775,6 +782,11 @@ def rays_arm(args, world, rank, local):
     dev = torch.device("cuda", local)
     cfg, desc = make_workload(args.workload, args.small, rank)
     nrays = cfg.rays.shape[0]
+    if args.dump and rank == 0:
+        from quarry import dumps
+
+        Path(args.dump).mkdir(parents=True, exist_ok=True)
+        dumps.write_qryd(Path(args.dump) / f"{args.workload}.qryd", cfg.tris, cfg.queries)
 
     # ---- builds (timed beside the step): LBVH and binned SAH with 32 bins ----
     tris_d = capi.to_device(cfg.tris, np.float32)

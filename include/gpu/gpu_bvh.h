@@ -234,3 +234,9 @@ std::string validateGaussianBVHGPU(const GpuBVH& bvh, const GaussianCloud& cloud
 
 // 64-bit FNV-1a over the node array bytes: the determinism gate.
 uint64_t treeHashGPU(const GpuBVH& bvh);
+
+// Additive (no quarry counterpart): the tree's device arrays as the C ABI sees them
+// (include/quarry_b200.h), for callers that query it with their own device buffers and
+// stream -- the zero-copy path of the Python module.  Valid while `bvh` lives and is not
+// rebuilt; wide nodes appear once buildWideNodesGPU has run.
+const struct qk_tree* gpuTreeView(const GpuBVH& bvh);

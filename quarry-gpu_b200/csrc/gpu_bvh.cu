@@ -738,6 +738,8 @@ std::string validateGaussianBVHGPU(const GpuBVH& bvh, const GaussianCloud& cloud
                        static_cast<int>(cloud.gaussians.size()), cloud.bounds);
 }
 
+const qk_tree* gpuTreeView(const GpuBVH& bvh) { return &implOf(bvh)->t; }
+
 uint64_t treeHashGPU(const GpuBVH& bvh) {
     std::vector<unsigned char> bytes(static_cast<size_t>(bvh.nodeCount) * 32);
     if (!bytes.empty()) {

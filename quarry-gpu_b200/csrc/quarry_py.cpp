@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "gpu/gpu_bvh.h"
+#include "quarry_b200.h"
 
 namespace py = pybind11;
 
@@ -606,6 +607,18 @@ void commonProps(py::class_<C>& c) {
         .def_property_readonly("bounds", [](const C& s) { return boundsDict(s.bounds); })
         .def_property_readonly("build_stats", [](const C& s) { return s.buildStats(); })
         .def("validate", &C::validate, "Check tree invariants; empty string means pass")
+        .def("_tree_view",
+             [](C& s, bool wide) {
+                 s.ensureWide(wide);
+                 const qk_tree* t = gpuTreeView(s.bvh);
+                 auto u = [](const void* p) { return reinterpret_cast<uintptr_t>(p); };
+                 return py::make_tuple(t->kind, t->n, t->depth, t->wide_count, u(t->nodes),
+                                       u(t->items), u(t->prim_ids), u(t->parent), u(t->depth_arr),
+                                       u(t->bnodes), u(t->leaves), u(t->slot_of), u(t->flags),
+                                       u(t->wide), u(t->wide_id));
+             },
+             py::arg("wide") = false,
+             "Device arrays of the tree (C ABI qk_tree fields) for the zero-copy CUDA path")
         .def("closest", &C::closest, py::arg("points"), py::arg("order") = "input",
              py::arg("wide") = false,
              "Return (dist2 float32[N], index int32[N]); index is -1 on a miss")

@@ -17,6 +17,9 @@ try:
         demo_mesh,
         describe,
     )
+    from . import zerocopy as _zerocopy
+
+    _zerocopy.install(Scene, PointCloud, GaussianCloud)
 except ImportError as _e:  # the extension is built by quarry-gpu_b200/build.py
     _import_error = _e
 

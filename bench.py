@@ -393,7 +393,8 @@ def points_arm(args, world, rank, local):
 
     variants = {"bin": 0, "bin_morton": capi.QK_ORDER_MORTON, "wide": capi.QK_WIDE,
                 "wide_morton": capi.QK_WIDE | capi.QK_ORDER_MORTON,
-                "split": capi.QK_TUNE_SPLIT, "split_morton": capi.QK_TUNE_SPLIT | capi.QK_ORDER_MORTON}
+                "split": capi.QK_TUNE_SPLIT, "split_morton": capi.QK_TUNE_SPLIT | capi.QK_ORDER_MORTON,
+                "leaf4": capi.QK_TUNE_LEAF4, "leaf4_morton": capi.QK_TUNE_LEAF4 | capi.QK_ORDER_MORTON}
     step(0)
     base = snapshot()
     vms = {}
@@ -818,7 +819,9 @@ def rays_arm(args, world, rank, local):
     modes = {"bin": 0, "bin_morton": mort, "wide": capi.QK_WIDE,
              "wide_morton": capi.QK_WIDE | mort, "bin_occ": occ, "bin_morton_occ": mort | occ,
              "bin_dyn": dyn, "bin_morton_dyn": mort | dyn, "bin_morton_dyn_occ": mort | dyn | occ,
-             "bin_sm": capi.QK_TUNE_SHORT_STACK, "bin_occ_sm": occ | capi.QK_TUNE_SHORT_STACK}
+             "bin_sm": capi.QK_TUNE_SHORT_STACK, "bin_occ_sm": occ | capi.QK_TUNE_SHORT_STACK,
+             "bin_leaf4": capi.QK_TUNE_LEAF4, "bin_occ_leaf4": occ | capi.QK_TUNE_LEAF4,
+             "bin_morton_occ_leaf4": mort | occ | capi.QK_TUNE_LEAF4}
     variants = {f"{b}_{m}": (b, f) for b in trees for m, f in modes.items()}
     if args.only:
         variants = {args.only: variants[args.only]}
@@ -932,7 +935,9 @@ def rays_arm(args, world, rank, local):
     knn_ms_by = {}
     for kname, kf in (("layout_of_rays", best_flags & (capi.QK_WIDE | capi.QK_ORDER_MORTON)),
                       ("split", capi.QK_TUNE_SPLIT),
-                      ("split_morton", capi.QK_TUNE_SPLIT | capi.QK_ORDER_MORTON)):
+                      ("split_morton", capi.QK_TUNE_SPLIT | capi.QK_ORDER_MORTON),
+                      ("leaf4", capi.QK_TUNE_LEAF4),
+                      ("leaf4_morton", capi.QK_TUNE_LEAF4 | capi.QK_ORDER_MORTON)):
         for _ in range(3):
             tree.knn(q_d, 8, kf, out=k_out)
         if not torch.equal(k_out, knn_base):

@@ -54,6 +54,8 @@ extern "C" {
 #define QK_TUNE_DYNAMIC 256u     /* persistent warps fetching new rays as lanes finish */
 #define QK_TUNE_HIGH_OCC 512u    /* register cap for 5 resident blocks of 256 per SM */
 #define QK_TUNE_SHORT_STACK 2048u /* binary rays: top 8 stack entries per thread in shared memory */
+#define QK_TUNE_LEAF4 4096u      /* binary nodes: child subtrees of 2..4 primitives are tested
+                                    as leaves (skips their inner boxes) */
 #define QK_TUNE_SPLIT 1024u      /* closest / kNN / radius on binary nodes: one warp per query,
                                     lanes on disjoint subtrees sharing the pruning bound */
 

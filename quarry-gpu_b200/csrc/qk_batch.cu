@@ -206,14 +206,18 @@ __global__ __launch_bounds__(kBlock) void k_bt_emit(const BScene* __restrict__ t
     }
 }
 
+// ranges: one int2 per primitive of the batch (scene s's internal nodes at prim_off(s))
 __global__ __launch_bounds__(kBlock) void k_bt_bottom_up(const BScene* __restrict__ tab,
-                                                         const int2* __restrict__ chunks) {
+                                                         const int2* __restrict__ chunks,
+                                                         int2* __restrict__ ranges) {
     const int2 ch = chunks[blockIdx.x];
-    const qk_tree& t = tab[ch.x].t;
+    const BScene& sc = tab[ch.x];
+    const qk_tree& t = sc.t;
     const int n = t.n;
     const int end = min(n, ch.y + kBuildChunk);
     for (int k = ch.y + threadIdx.x; k < end; k += kBlock)
-        climb(static_cast<Node*>(t.nodes), static_cast<BNode*>(t.bnodes), t.parent, t.flags, n, k);
+        climb(static_cast<Node*>(t.nodes), static_cast<BNode*>(t.bnodes), t.parent, t.flags, n, k,
+              ranges + sc.prim_off);
 }
 
 __global__ __launch_bounds__(kBlock) void k_bt_depth(const BScene* __restrict__ tab,
@@ -716,7 +720,8 @@ int batch_build_impl(qk_batch* b, cudaStream_t s) {
     // idx_f = codes_s; gather codes into codes, local ids into idx_s
     k_bt_gather<<<C, kBlock, 0, s>>>(b->d_tab, b->d_chunks, keep, codes_s, codes, idx_s);
     k_bt_emit<Ops><<<C, kBlock, 0, s>>>(b->d_tab, b->d_chunks, codes, idx_s);
-    k_bt_bottom_up<<<C, kBlock, 0, s>>>(b->d_tab, b->d_chunks);
+    // the code buffers are free again: their 2N uint32 (256-byte aligned) hold N int2 ranges
+    k_bt_bottom_up<<<C, kBlock, 0, s>>>(b->d_tab, b->d_chunks, reinterpret_cast<int2*>(codes));
     k_bt_depth<<<C, kBlock, 0, s>>>(b->d_tab, b->d_chunks, b->d_hdr);
     if (b->flags & QK_WIDE) {
         k_bt_wide_flags<<<C, kBlock, 0, s>>>(b->d_tab, b->d_chunks);

@@ -121,10 +121,11 @@ __global__ __launch_bounds__(kBlock) void k_emit(
 __global__ __launch_bounds__(kBlock) void k_bottom_up(Node* __restrict__ nodes,
                                                      BNode* __restrict__ bnodes,
                                                      const int* __restrict__ parent,
-                                                     int* __restrict__ flags, int n) {
+                                                     int* __restrict__ flags, int n,
+                                                     int2* __restrict__ ranges) {
     const int k = blockIdx.x * kBlock + threadIdx.x;
     if (k >= n) return;
-    climb(nodes, bnodes, parent, flags, n, k);
+    climb(nodes, bnodes, parent, flags, n, k, ranges);
 }
 
 // depth = length of the parent chain (lbvh.cu:419-431); bounded by the node count
@@ -231,7 +232,7 @@ __global__ __launch_bounds__(kBlock) void k_dirty_merge(const int* __restrict__ 
         const int need = __popc(old & 3);
         if ((old >> 2) + 1 < need) return;
         __threadfence();
-        finish_node(nodes, bnodes, p);
+        finish_node(nodes, bnodes, p, n, nullptr);
         flags[p] = 0;
         p = parent[p];
     }
@@ -383,11 +384,11 @@ __global__ __launch_bounds__(kBlock) void k_check_wide(const Node* __restrict__ 
 
 // Boxes (bottom-up), traversal nodes and depths of a tree whose links and leaves are set;
 // shared by the LBVH and SAH builders.  Reads the maximum depth back (syncs).
-int finish_tree(qk_tree* t, Header* h, cudaStream_t s) {
+int finish_tree(qk_tree* t, Header* h, int2* ranges, cudaStream_t s) {
     const int n = t->n;
     k_bottom_up<<<blocks_for(n), kBlock, 0, s>>>(static_cast<Node*>(t->nodes),
                                                  static_cast<BNode*>(t->bnodes), t->parent,
-                                                 t->flags, n);
+                                                 t->flags, n, ranges);
     cudaMemsetAsync(&h->max_depth, 0, sizeof(int), s);
     k_depth<<<blocks_for(2 * n - 1), kBlock, 0, s>>>(t->parent, 2 * n - 1, t->depth_arr, h);
     cudaError_t e = cudaGetLastError();
@@ -428,7 +429,7 @@ int build_lbvh(qk_tree* t, const void* items_v, void* ws, cudaStream_t s) {
                                                   static_cast<float4*>(t->leaves), t->flags);
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_status(e, "build kernels");
-    return finish_tree(t, h, s);
+    return finish_tree(t, h, build_ranges(ws, t->kind, n, QK_BUILD_LBVH), s);
 }
 
 template <class Ops>
@@ -439,7 +440,7 @@ int refit_impl(qk_tree* t, const void* items, cudaStream_t s) {
         static_cast<float*>(t->items), static_cast<float4*>(t->leaves));
     k_bottom_up<<<blocks_for(n), kBlock, 0, s>>>(static_cast<Node*>(t->nodes),
                                                  static_cast<BNode*>(t->bnodes), t->parent,
-                                                 t->flags, n);
+                                                 t->flags, n, nullptr);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_status(e, "refit");
     if (t->wide_count > 0 && t->wide) return wide_emit_all(t, s);
@@ -499,7 +500,8 @@ int validate_impl(const qk_tree* t, const void* items, int* err, void* ws, cudaS
 
 }  // namespace
 
-size_t build_ws_bytes(int kind, int n, int builder) {
+// workspace of the builders themselves; the bottom-up ranges follow it
+size_t build_core_bytes(int kind, int n, int builder) {
     (void)kind;
     Carve c;
     c.take<Header>(1);
@@ -521,6 +523,16 @@ size_t build_ws_bytes(int kind, int n, int builder) {
     return need;
 }
 
+size_t build_ws_bytes(int kind, int n, int builder) {
+    return (build_core_bytes(kind, n, builder) + 255) / 256 * 256 + sizeof(int2) * static_cast<size_t>(n);
+}
+
+// the int2 per internal node the bottom-up pass records leaf-slot ranges in
+int2* build_ranges(void* ws, int kind, int n, int builder) {
+    return reinterpret_cast<int2*>(static_cast<char*>(ws) +
+                                   (build_core_bytes(kind, n, builder) + 255) / 256 * 256);
+}
+
 int build_tree(qk_tree* t, int builder, int bins, const void* items, void* ws, size_t ws_bytes,
                cudaStream_t s) {
     (void)ws_bytes;
@@ -528,7 +540,7 @@ int build_tree(qk_tree* t, int builder, int bins, const void* items, void* ws, s
         cudaMemsetAsync(t->flags, 0, sizeof(int) * static_cast<size_t>(t->n - 1), s);
         const int st = build_sah(t, bins, items, ws, s);
         if (st != QK_OK) return st;
-        return finish_tree(t, static_cast<Header*>(ws), s);
+        return finish_tree(t, static_cast<Header*>(ws), build_ranges(ws, t->kind, t->n, QK_BUILD_SAH), s);
     }
     switch (t->kind) {
         case kTri: return build_lbvh<TriOps>(t, items, ws, s);

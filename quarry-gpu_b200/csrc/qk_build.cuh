@@ -113,10 +113,34 @@ __device__ __forceinline__ Box load_box_cg(const Node* nd) {
     return bx;
 }
 
+// Small-subtree code of a child (traversal node words v3.z / v3.w): a subtree of 2..kLeafMax
+// leaves on contiguous slots is (first slot << 2) | (leaves - 1); anything else is 0.
+constexpr int kLeafMax = 4;
+
+__device__ __forceinline__ int small_code(int c, int n, int2 range) {
+    return (c < n - 1 && range.y >= 2 && range.y <= kLeafMax) ? ((range.x << 2) | (range.y - 1)) : 0;
+}
+
+__device__ __forceinline__ int2 child_range(const int2* ranges, int c, int n) {
+    return c >= n - 1 ? make_int2(c - (n - 1), 1) : __ldcg(ranges + c);
+}
+
 // Complete internal node p from its two (final) children: canonical box + traversal node.
+// With `ranges` (one int2 per internal node) the node's leaf-slot range (first, count; count
+// 0 when the slots are not contiguous) is recorded and the children's small-subtree codes
+// are written; without (refit) the codes are kept.
 __device__ __forceinline__ void finish_node(Node* __restrict__ nodes, BNode* __restrict__ bnodes,
-                                            int p) {
+                                            int p, int n, int2* __restrict__ ranges) {
     const int l = nodes[p].left, r = nodes[p].right;
+    if (ranges) {
+        const int2 rl = child_range(ranges, l, n), rr = child_range(ranges, r, n);
+        const int first = min(rl.x, rr.x);
+        int count = rl.y + rr.y;
+        if (rl.y <= 0 || rr.y <= 0 || max(rl.x + rl.y, rr.x + rr.y) - first != count) count = 0;
+        ranges[p] = make_int2(first, count);
+        *reinterpret_cast<float2*>(&bnodes[p].v3.z) =
+            make_float2(__int_as_float(small_code(l, n, rl)), __int_as_float(small_code(r, n, rr)));
+    }
     const Box a = load_box_cg(nodes + l);
     const Box b = load_box_cg(nodes + r);
     Box u;
@@ -133,14 +157,14 @@ __device__ __forceinline__ void finish_node(Node* __restrict__ nodes, BNode* __r
 // second arrival finishes p (both children final), resets the counter and continues.
 __device__ __forceinline__ void climb(Node* __restrict__ nodes, BNode* __restrict__ bnodes,
                                       const int* __restrict__ parent, int* __restrict__ flags,
-                                      int n, int k) {
+                                      int n, int k, int2* __restrict__ ranges) {
     int p = parent[n - 1 + k];
     int guard = 0;
     while (p >= 0 && guard++ < 4096) {
         __threadfence();
         if (atomicAdd(&flags[p], 1) == 0) return;
         __threadfence();
-        finish_node(nodes, bnodes, p);
+        finish_node(nodes, bnodes, p, n, ranges);
         flags[p] = 0;
         p = parent[p];
     }

@@ -42,7 +42,9 @@ static_assert(sizeof(Node) == 32, "node is 32 bytes");
 //   v0 = L.mn.x L.mn.y L.mn.z L.mx.x
 //   v1 = L.mx.y L.mx.z R.mn.x R.mn.y
 //   v2 = R.mn.z R.mx.x R.mx.y R.mx.z
-//   v3 = left   right  0      0
+//   v3 = left   right  lsmall rsmall
+// lsmall / rsmall: 0, or (first slot << 2) | (leaves - 1) when that child's subtree holds 2..4
+// leaves on contiguous slots (written by the bottom-up pass, kept by refits).
 struct alignas(64) BNode {
     float4 v0, v1, v2, v3;
 };

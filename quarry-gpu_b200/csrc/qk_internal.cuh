@@ -75,6 +75,8 @@ cudaError_t scan_exclusive(const int* in, int* out, int n, bool write_total, voi
 
 // ---- build / refit / wide / validate (qk_build.cu) ----
 size_t build_ws_bytes(int kind, int n, int builder);
+// the bottom-up pass's range scratch inside a build workspace
+int2* build_ranges(void* ws, int kind, int n, int builder);
 int build_tree(qk_tree* t, int builder, int bins, const void* items, void* ws, size_t ws_bytes,
                cudaStream_t s);
 // SAH topology (qk_sah.cu): fills links, parents, order-derived leaves; boxes come after

@@ -95,7 +95,7 @@ __global__ __launch_bounds__(kBlock) void k_pos_keys(const float* __restrict__ p
 // ---------------------------------------------------------------------------------------
 // single-tree kernels: one thread per ray / query point, bodies in qk_traverse.cuh
 // ---------------------------------------------------------------------------------------
-template <bool kStats, int kMinBlocks, int kShort = 0>
+template <bool kStats, int kMinBlocks, int kShort = 0, bool kLeaf4 = false>
 __global__ __launch_bounds__(kBlock, kMinBlocks) void k_ray_bin(const BNode* __restrict__ bn,
                                                    const float4* __restrict__ leaves,
                                                    const Node* __restrict__ nodes,
@@ -123,7 +123,8 @@ __global__ __launch_bounds__(kBlock, kMinBlocks) void k_ray_bin(const BNode* __r
             out[r] = ray_bin_one(bn, leaves, root_box(nodes), R, max_iter, st, tv, best_id);
         } else {
             LocalStack<kStack> st;
-            out[r] = ray_bin_one(bn, leaves, root_box(nodes), R, max_iter, st, tv, best_id);
+            out[r] = ray_bin_one<LocalStack<kStack>, kLeaf4>(bn, leaves, root_box(nodes), R,
+                                                             max_iter, st, tv, best_id);
         }
         if (ids) ids[r] = best_id;
     }
@@ -272,7 +273,7 @@ __global__ __launch_bounds__(kBlock) void k_ray_wide(const WideNode* __restrict_
     flush_stats<kStats>(active, tv.nodes, tv.leaves, tv.overflow, stats);
 }
 
-template <class Ops, bool kStats>
+template <class Ops, bool kStats, bool kLeaf4 = false>
 __global__ __launch_bounds__(kBlock) void k_closest_bin(const BNode* __restrict__ bn,
                                                        const float4* __restrict__ leaves,
                                                        const float* __restrict__ pts,
@@ -286,7 +287,7 @@ __global__ __launch_bounds__(kBlock) void k_closest_bin(const BNode* __restrict_
         const int q = order ? static_cast<int>(order[i]) : i;
         const float3 p = f3(pts[3 * q], pts[3 * q + 1], pts[3 * q + 2]);
         LocalStack<kStack> st;
-        out[q] = closest_bin_one<Ops>(bn, leaves, p, max_iter, st, tv);
+        out[q] = closest_bin_one<Ops, LocalStack<kStack>, kLeaf4>(bn, leaves, p, max_iter, st, tv);
     }
     flush_stats<kStats>(active, tv.nodes, tv.leaves, tv.overflow, stats);
 }
@@ -310,7 +311,7 @@ __global__ __launch_bounds__(kBlock) void k_closest_wide(const WideNode* __restr
     flush_stats<kStats>(active, tv.nodes, tv.leaves, tv.overflow, stats);
 }
 
-template <class Ops, int K, bool kStats>
+template <class Ops, int K, bool kStats, bool kLeaf4 = false>
 __global__ __launch_bounds__(kBlock) void k_knn_bin(const BNode* __restrict__ bn,
                                                    const float4* __restrict__ leaves,
                                                    const float* __restrict__ pts,
@@ -325,7 +326,7 @@ __global__ __launch_bounds__(kBlock) void k_knn_bin(const BNode* __restrict__ bn
         const float3 p = f3(pts[3 * q], pts[3 * q + 1], pts[3 * q + 2]);
         LocalStack<kStack> st;
         KnnTable<K> tab;
-        knn_bin_one<Ops, K>(bn, leaves, p, k, max_iter, st, tv, tab);
+        knn_bin_one<Ops, K, LocalStack<kStack>, kLeaf4>(bn, leaves, p, k, max_iter, st, tv, tab);
         write_knn<K>(tab, k, out + static_cast<size_t>(q) * stride);
     }
     flush_stats<kStats>(active, tv.nodes, tv.leaves, tv.overflow, stats);
@@ -353,7 +354,7 @@ __global__ __launch_bounds__(kBlock) void k_knn_wide(const WideNode* __restrict_
 }
 
 // radius: count, then fill at the scanned offsets, then sort every segment by (dist2, id)
-template <class Ops, bool kFill, bool kStats>
+template <class Ops, bool kFill, bool kStats, bool kLeaf4 = false>
 __global__ __launch_bounds__(kBlock) void k_radius_bin(
     const BNode* __restrict__ bn, const float4* __restrict__ leaves, const Node* __restrict__ nodes,
     const float* __restrict__ pts, const uint32_t* __restrict__ order, int count, float r2,
@@ -368,8 +369,8 @@ __global__ __launch_bounds__(kBlock) void k_radius_bin(
         const int write = kFill ? offsets[q] : 0;
         const int end = kFill ? offsets[q + 1] : 0;  // never write past this query's segment
         LocalStack<kStack> st;
-        const int found = radius_bin_one<Ops, kFill>(bn, leaves, root_box(nodes), p, r2, write,
-                                                     end, keys, max_iter, st, tv);
+        const int found = radius_bin_one<Ops, kFill, LocalStack<kStack>, kLeaf4>(
+            bn, leaves, root_box(nodes), p, r2, write, end, keys, max_iter, st, tv);
         if (!kFill) counts[q] = found;
     }
     flush_stats<kStats>(active, tv.nodes, tv.leaves, tv.overflow, stats);
@@ -658,6 +659,10 @@ int closest_impl(const qk_tree* t, const float* pts, int count, uint2* out, unsi
         const int gs = blocks_for(static_cast<long long>(count) * 32);
         if (st) k_closest_split<Ops, true><<<gs, kBlock, 0, s>>>(bn, leaves, pts, order, count, out, t->n * 2 + 64, stats);
         else k_closest_split<Ops, false><<<gs, kBlock, 0, s>>>(bn, leaves, pts, order, count, out, t->n * 2 + 64, stats);
+    } else if (flags & QK_TUNE_LEAF4) {
+        const BNode* bn = static_cast<const BNode*>(t->bnodes);
+        if (st) k_closest_bin<Ops, true, true><<<g, kBlock, 0, s>>>(bn, leaves, pts, order, count, out, t->n * 2 + 64, stats);
+        else k_closest_bin<Ops, false, true><<<g, kBlock, 0, s>>>(bn, leaves, pts, order, count, out, t->n * 2 + 64, stats);
     } else {
         const BNode* bn = static_cast<const BNode*>(t->bnodes);
         if (st) k_closest_bin<Ops, true><<<g, kBlock, 0, s>>>(bn, leaves, pts, order, count, out, t->n * 2 + 64, stats);
@@ -669,8 +674,8 @@ int closest_impl(const qk_tree* t, const float* pts, int count, uint2* out, unsi
 
 template <class Ops, int K>
 void launch_knn(const qk_tree* t, const float* pts, int count, int k, int stride, uint2* out,
-                bool wide, bool split, unsigned long long* stats, const uint32_t* order,
-                cudaStream_t s) {
+                bool wide, bool split, bool leaf4, unsigned long long* stats,
+                const uint32_t* order, cudaStream_t s) {
     const float4* leaves = static_cast<const float4*>(t->leaves);
     const int g = blocks_for(count);
     if (split && !wide) {
@@ -682,6 +687,10 @@ void launch_knn(const qk_tree* t, const float* pts, int count, int k, int stride
         const WideNode* wn = static_cast<const WideNode*>(t->wide);
         if (stats) k_knn_wide<Ops, K, true><<<g, kBlock, 0, s>>>(wn, leaves, pts, order, count, k, stride, out, t->n * 2 + 64, stats);
         else k_knn_wide<Ops, K, false><<<g, kBlock, 0, s>>>(wn, leaves, pts, order, count, k, stride, out, t->n * 2 + 64, stats);
+    } else if (leaf4) {
+        const BNode* bn = static_cast<const BNode*>(t->bnodes);
+        if (stats) k_knn_bin<Ops, K, true, true><<<g, kBlock, 0, s>>>(bn, leaves, pts, order, count, k, stride, out, t->n * 2 + 64, stats);
+        else k_knn_bin<Ops, K, false, true><<<g, kBlock, 0, s>>>(bn, leaves, pts, order, count, k, stride, out, t->n * 2 + 64, stats);
     } else {
         const BNode* bn = static_cast<const BNode*>(t->bnodes);
         if (stats) k_knn_bin<Ops, K, true><<<g, kBlock, 0, s>>>(bn, leaves, pts, order, count, k, stride, out, t->n * 2 + 64, stats);
@@ -694,10 +703,11 @@ int knn_impl(const qk_tree* t, const float* pts, int count, int k, int stride, u
              unsigned flags, unsigned long long* stats, const uint32_t* order, cudaStream_t s) {
     const bool wide = (flags & QK_WIDE) != 0;
     const bool split = (flags & QK_TUNE_SPLIT) != 0;
-    if (k <= 4) launch_knn<Ops, 4>(t, pts, count, k, stride, out, wide, split, stats, order, s);
-    else if (k <= 8) launch_knn<Ops, 8>(t, pts, count, k, stride, out, wide, split, stats, order, s);
-    else if (k <= 16) launch_knn<Ops, 16>(t, pts, count, k, stride, out, wide, split, stats, order, s);
-    else launch_knn<Ops, 32>(t, pts, count, k, stride, out, wide, split, stats, order, s);
+    const bool leaf4 = (flags & QK_TUNE_LEAF4) != 0;
+    if (k <= 4) launch_knn<Ops, 4>(t, pts, count, k, stride, out, wide, split, leaf4, stats, order, s);
+    else if (k <= 8) launch_knn<Ops, 8>(t, pts, count, k, stride, out, wide, split, leaf4, stats, order, s);
+    else if (k <= 16) launch_knn<Ops, 16>(t, pts, count, k, stride, out, wide, split, leaf4, stats, order, s);
+    else launch_knn<Ops, 32>(t, pts, count, k, stride, out, wide, split, leaf4, stats, order, s);
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? QK_OK : cuda_status(e, "knn");
 }
@@ -717,6 +727,11 @@ int radius_launch(const qk_tree* t, const float* pts, int count, float r2, int* 
         const WideNode* wn = static_cast<const WideNode*>(t->wide);
         if (stats) k_radius_wide<Ops, kFill, true><<<g, kBlock, 0, s>>>(wn, leaves, pts, order, count, r2, counts, offsets, keys, t->n * 2 + 64, stats);
         else k_radius_wide<Ops, kFill, false><<<g, kBlock, 0, s>>>(wn, leaves, pts, order, count, r2, counts, offsets, keys, t->n * 2 + 64, stats);
+    } else if (flags & QK_TUNE_LEAF4) {
+        const BNode* bn = static_cast<const BNode*>(t->bnodes);
+        const Node* nodes = static_cast<const Node*>(t->nodes);
+        if (stats) k_radius_bin<Ops, kFill, true, true><<<g, kBlock, 0, s>>>(bn, leaves, nodes, pts, order, count, r2, counts, offsets, keys, t->n * 2 + 64, stats);
+        else k_radius_bin<Ops, kFill, false, true><<<g, kBlock, 0, s>>>(bn, leaves, nodes, pts, order, count, r2, counts, offsets, keys, t->n * 2 + 64, stats);
     } else {
         const BNode* bn = static_cast<const BNode*>(t->bnodes);
         const Node* nodes = static_cast<const Node*>(t->nodes);
@@ -792,6 +807,12 @@ int ray_query(const qk_tree* t, const void* rays, int count, uint64_t* out, int*
         } else if (flags & QK_TUNE_SHORT_STACK) {
             if (stt) k_ray_bin<true, 1, 8><<<g, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, ids, t->n * 2 + 64, stt);
             else k_ray_bin<false, 1, 8><<<g, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, ids, t->n * 2 + 64, stt);
+        } else if ((flags & QK_TUNE_HIGH_OCC) && (flags & QK_TUNE_LEAF4)) {
+            if (stt) k_ray_bin<true, 5, 0, true><<<g, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, ids, t->n * 2 + 64, stt);
+            else k_ray_bin<false, 5, 0, true><<<g, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, ids, t->n * 2 + 64, stt);
+        } else if (flags & QK_TUNE_LEAF4) {
+            if (stt) k_ray_bin<true, 1, 0, true><<<g, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, ids, t->n * 2 + 64, stt);
+            else k_ray_bin<false, 1, 0, true><<<g, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, ids, t->n * 2 + 64, stt);
         } else if (flags & QK_TUNE_HIGH_OCC) {
             if (stt) k_ray_bin<true, 5><<<g, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, ids, t->n * 2 + 64, stt);
             else k_ray_bin<false, 5><<<g, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, ids, t->n * 2 + 64, stt);

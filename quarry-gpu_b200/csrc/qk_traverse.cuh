@@ -80,6 +80,23 @@ __device__ __forceinline__ void load_bnode(const BNode* __restrict__ bn, int i, 
     rref = __float_as_int(d.y);
 }
 
+// load_bnode plus the children's small-subtree codes (v3.z / v3.w): 0, or (first slot << 2)
+// | (leaves - 1) for a child subtree of 2..4 leaves on contiguous slots
+__device__ __forceinline__ void load_bnode_small(const BNode* __restrict__ bn, int i, float3& llo,
+                                                 float3& lhi, float3& rlo, float3& rhi,
+                                                 int& lref, int& rref, int& lsm, int& rsm) {
+    const float4* p = reinterpret_cast<const float4*>(bn + i);
+    const float4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2), d = __ldg(p + 3);
+    llo = f3(a.x, a.y, a.z);
+    lhi = f3(a.w, b.x, b.y);
+    rlo = f3(b.z, b.w, c.x);
+    rhi = f3(c.y, c.z, c.w);
+    lref = __float_as_int(d.x);
+    rref = __float_as_int(d.y);
+    lsm = __float_as_int(d.z);
+    rsm = __float_as_int(d.w);
+}
+
 __device__ __forceinline__ Box root_box(const Node* __restrict__ nodes) {
     const float4* p = reinterpret_cast<const float4*>(nodes);
     const float4 a = __ldg(p), b = __ldg(p + 1);
@@ -145,7 +162,7 @@ __device__ __forceinline__ unsigned long long pack_hit(bool any, float best) {
 
 // First hit in a binary tree: near child followed, far child pushed with its entry bound,
 // which is re-checked against the current best when popped (src/cpu/bvh.cpp:147-152).
-template <class St>
+template <class St, bool kLeaf4 = false>
 __device__ __forceinline__ unsigned long long ray_bin_one(const BNode* __restrict__ bn,
                                                           const float4* __restrict__ leaves,
                                                           const Box& rb, const RayPre& R,
@@ -166,8 +183,9 @@ __device__ __forceinline__ unsigned long long ray_bin_one(const BNode* __restric
             break;
         }
         float3 llo, lhi, rlo, rhi;
-        int lref, rref;
-        load_bnode(bn, node, llo, lhi, rlo, rhi, lref, rref);
+        int lref, rref, lsm = 0, rsm = 0;
+        if constexpr (kLeaf4) load_bnode_small(bn, node, llo, lhi, rlo, rhi, lref, rref, lsm, rsm);
+        else load_bnode(bn, node, llo, lhi, rlo, rhi, lref, rref);
         float tl, tr;
         bool hl = ray_box(R, llo, lhi, bound, tl);
         bool hr = ray_box(R, rlo, rhi, bound, tr);
@@ -181,6 +199,29 @@ __device__ __forceinline__ unsigned long long ray_bin_one(const BNode* __restric
             ++tv.leaves;
             test_tri(R, leaves, ~rref, best, bound, any, best_id);
             hr = false;
+        }
+        if constexpr (kLeaf4) {
+            // subtrees of 2..4 triangles: test them now, the nearer first, the farther only
+            // while its entry still passes the current bound
+            const bool sl = hl && lsm != 0, sr = hr && rsm != 0;
+            if (sl || sr) {
+                const bool lnear = tl <= tr;
+#pragma unroll
+                for (int pass = 0; pass < 2; ++pass) {
+                    const bool left = (pass == 0) == lnear;
+                    const int code = left ? (sl ? lsm : 0) : (sr ? rsm : 0);
+                    const float te = left ? tl : tr;
+                    if (code && !(te > bound * kMarginMul + kMarginAdd)) {
+                        const int first = code >> 2, cnt = (code & 3) + 1;
+                        for (int j = 0; j < cnt; ++j) {
+                            ++tv.leaves;
+                            test_tri(R, leaves, first + j, best, bound, any, best_id);
+                        }
+                    }
+                }
+                if (sl) hl = false;
+                if (sr) hr = false;
+            }
         }
         if (hl && hr) {
             const bool lnear = tl <= tr;
@@ -310,7 +351,7 @@ __device__ __forceinline__ uint2 pack_closest(float best, int best_id) {
                         : make_uint2(0u, 0xffffffffu);
 }
 
-template <class Ops, class St>
+template <class Ops, class St, bool kLeaf4 = false>
 __device__ __forceinline__ uint2 closest_bin_one(const BNode* __restrict__ bn,
                                                  const float4* __restrict__ leaves, float3 p,
                                                  int max_iter, St& st, Trav& tv) {
@@ -325,8 +366,9 @@ __device__ __forceinline__ uint2 closest_bin_one(const BNode* __restrict__ bn,
         }
         ++tv.nodes;
         float3 llo, lhi, rlo, rhi;
-        int lref, rref;
-        load_bnode(bn, node, llo, lhi, rlo, rhi, lref, rref);
+        int lref, rref, lsm = 0, rsm = 0;
+        if constexpr (kLeaf4) load_bnode_small(bn, node, llo, lhi, rlo, rhi, lref, rref, lsm, rsm);
+        else load_bnode(bn, node, llo, lhi, rlo, rhi, lref, rref);
         const float dl = dist2_box(p, llo, lhi);
         const float dr = dist2_box(p, rlo, rhi);
         bool okl = best_id < 0 || dl <= best;
@@ -341,6 +383,26 @@ __device__ __forceinline__ uint2 closest_bin_one(const BNode* __restrict__ bn,
             if (okr && rref < 0) { ++tv.leaves; leaf_closest<Ops>(p, leaves, ~rref, best, best_id); okr = false; }
             if (okl && lref < 0 && (best_id < 0 || dl <= best)) { ++tv.leaves; leaf_closest<Ops>(p, leaves, ~lref, best, best_id); }
             if (lref < 0) okl = false;
+        }
+        if constexpr (kLeaf4) {
+            const bool sl = okl && lsm != 0, sr = okr && rsm != 0;
+            if (sl || sr) {
+#pragma unroll
+                for (int pass = 0; pass < 2; ++pass) {
+                    const bool left = (pass == 0) == lfirst;
+                    const int code = left ? (sl ? lsm : 0) : (sr ? rsm : 0);
+                    const float dbox = left ? dl : dr;
+                    if (code && (best_id < 0 || dbox <= best)) {
+                        const int first = code >> 2, cnt = (code & 3) + 1;
+                        for (int j = 0; j < cnt; ++j) {
+                            ++tv.leaves;
+                            leaf_closest<Ops>(p, leaves, first + j, best, best_id);
+                        }
+                    }
+                }
+                if (sl) okl = false;
+                if (sr) okr = false;
+            }
         }
         if (okl && okr) {
             if (sp >= St::kSize) {
@@ -512,7 +574,7 @@ __device__ __forceinline__ void write_knn(const KnnTable<K>& tab, int k, uint2* 
     }
 }
 
-template <class Ops, int K, class St>
+template <class Ops, int K, class St, bool kLeaf4 = false>
 __device__ __forceinline__ void knn_bin_one(const BNode* __restrict__ bn,
                                             const float4* __restrict__ leaves, float3 p, int k,
                                             int max_iter, St& st, Trav& tv, KnnTable<K>& tab) {
@@ -526,8 +588,9 @@ __device__ __forceinline__ void knn_bin_one(const BNode* __restrict__ bn,
         }
         ++tv.nodes;
         float3 llo, lhi, rlo, rhi;
-        int lref, rref;
-        load_bnode(bn, node, llo, lhi, rlo, rhi, lref, rref);
+        int lref, rref, lsm = 0, rsm = 0;
+        if constexpr (kLeaf4) load_bnode_small(bn, node, llo, lhi, rlo, rhi, lref, rref, lsm, rsm);
+        else load_bnode(bn, node, llo, lhi, rlo, rhi, lref, rref);
         const float dl = dist2_box(p, llo, lhi);
         const float dr = dist2_box(p, rlo, rhi);
         const bool lfirst = dl <= dr;
@@ -541,6 +604,26 @@ __device__ __forceinline__ void knn_bin_one(const BNode* __restrict__ bn,
             if (okr && rref < 0) { ++tv.leaves; leaf_knn<Ops, K>(p, leaves, ~rref, tab, k); okr = false; }
             if (okl && lref < 0 && tab.admits(dl)) { ++tv.leaves; leaf_knn<Ops, K>(p, leaves, ~lref, tab, k); }
             if (lref < 0) okl = false;
+        }
+        if constexpr (kLeaf4) {
+            const bool sl = okl && lsm != 0, sr = okr && rsm != 0;
+            if (sl || sr) {
+#pragma unroll
+                for (int pass = 0; pass < 2; ++pass) {
+                    const bool left = (pass == 0) == lfirst;
+                    const int code = left ? (sl ? lsm : 0) : (sr ? rsm : 0);
+                    const float dbox = left ? dl : dr;
+                    if (code && tab.admits(dbox)) {
+                        const int first = code >> 2, cnt = (code & 3) + 1;
+                        for (int j = 0; j < cnt; ++j) {
+                            ++tv.leaves;
+                            leaf_knn<Ops, K>(p, leaves, first + j, tab, k);
+                        }
+                    }
+                }
+                if (sl) okl = false;
+                if (sr) okr = false;
+            }
         }
         if (okl && okr) {
             if (sp >= St::kSize) {
@@ -648,7 +731,7 @@ __device__ __forceinline__ unsigned long long radius_key(float d2, int id) {
     return (static_cast<unsigned long long>(__float_as_uint(d2)) << 32) | static_cast<unsigned>(id);
 }
 
-template <class Ops, bool kFill, class St>
+template <class Ops, bool kFill, class St, bool kLeaf4 = false>
 __device__ __forceinline__ int radius_bin_one(const BNode* __restrict__ bn,
                                               const float4* __restrict__ leaves, const Box& rb,
                                               float3 p, float r2, int write, int end,
@@ -665,8 +748,9 @@ __device__ __forceinline__ int radius_bin_one(const BNode* __restrict__ bn,
         }
         ++tv.nodes;
         float3 llo, lhi, rlo, rhi;
-        int lref, rref;
-        load_bnode(bn, node, llo, lhi, rlo, rhi, lref, rref);
+        int lref, rref, lsm = 0, rsm = 0;
+        if constexpr (kLeaf4) load_bnode_small(bn, node, llo, lhi, rlo, rhi, lref, rref, lsm, rsm);
+        else load_bnode(bn, node, llo, lhi, rlo, rhi, lref, rref);
         bool okl = dist2_box(p, llo, lhi) <= r2;
         bool okr = dist2_box(p, rlo, rhi) <= r2;
         if (okl && lref < 0) {
@@ -688,6 +772,26 @@ __device__ __forceinline__ int radius_bin_one(const BNode* __restrict__ bn,
                 ++found;
             }
             okr = false;
+        }
+        if constexpr (kLeaf4) {
+#pragma unroll
+            for (int pass = 0; pass < 2; ++pass) {
+                const int code = pass == 0 ? (okl ? lsm : 0) : (okr ? rsm : 0);
+                if (code) {
+                    const int first = code >> 2, cnt = (code & 3) + 1;
+                    for (int j = 0; j < cnt; ++j) {
+                        ++tv.leaves;
+                        int id;
+                        const float d2 = Ops::dist2(p, leaves, first + j, id);
+                        if (d2 <= r2) {
+                            if (kFill && write < end) keys[write++] = radius_key(d2, id);
+                            ++found;
+                        }
+                    }
+                }
+            }
+            if (lsm) okl = false;
+            if (rsm) okr = false;
         }
         if (okl && okr) {
             if (sp >= St::kSize) {

@@ -219,7 +219,7 @@ RAY_SPACE = {
     "builder": ["sah32", "lbvh", "sah16", "sah8"],
     "layout": ["bin", "wide"],
     "order": ["input", "morton"],
-    "schedule": ["occ", "plain", "dyn", "dyn_occ", "sm", "occ_sm"],
+    "schedule": ["occ", "plain", "dyn", "dyn_occ", "sm", "occ_sm", "leaf4", "occ_leaf4"],
 }
 
 
@@ -238,5 +238,7 @@ def ray_flags(p: dict) -> int:
         f |= {"plain": 0, "occ": capi.QK_TUNE_HIGH_OCC, "dyn": capi.QK_TUNE_DYNAMIC,
               "dyn_occ": capi.QK_TUNE_DYNAMIC | capi.QK_TUNE_HIGH_OCC,
               "sm": capi.QK_TUNE_SHORT_STACK,
-              "occ_sm": capi.QK_TUNE_HIGH_OCC | capi.QK_TUNE_SHORT_STACK}[p["schedule"]]
+              "occ_sm": capi.QK_TUNE_HIGH_OCC | capi.QK_TUNE_SHORT_STACK,
+              "leaf4": capi.QK_TUNE_LEAF4,
+              "occ_leaf4": capi.QK_TUNE_HIGH_OCC | capi.QK_TUNE_LEAF4}[p["schedule"]]
     return f

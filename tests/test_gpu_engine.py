@@ -396,6 +396,93 @@ def test_split_queries_same_bits(cuda, kind, n):
     assert int(stats[2]) == 0
 
 
+def _check_small_codes(tree: capi.DeviceTree):
+    """Traversal-node words v3.z / v3.w: (first slot << 2) | (leaves - 1) for a child subtree
+    of 2..4 leaves on contiguous slots, else 0 (leaf children always 0)."""
+    n = tree.n
+    nodes = tree.nodes_bytes().view(np.int32).reshape(2 * n - 1, 8)
+    bn = tree.host("bnodes", np.int32, (n - 1) * 16).reshape(n - 1, 16)
+    depth = tree.host("depth_arr", np.int32, 2 * n - 1)
+    first = np.zeros(2 * n - 1, np.int64)
+    last = np.zeros(2 * n - 1, np.int64)
+    count = np.zeros(2 * n - 1, np.int64)
+    first[n - 1:] = last[n - 1:] = np.arange(n)
+    count[n - 1:] = 1
+    for p in sorted(range(n - 1), key=lambda i: -int(depth[i])):
+        l, r = nodes[p, 6], nodes[p, 7]
+        first[p] = min(first[l], first[r])
+        last[p] = max(last[l], last[r])
+        count[p] = count[l] + count[r]
+    contiguous = last - first + 1 == count
+    small = 0
+    for p in range(n - 1):
+        for c, word in ((nodes[p, 6], bn[p, 14]), (nodes[p, 7], bn[p, 15])):
+            want = 0
+            if c < n - 1 and contiguous[c] and 2 <= count[c] <= 4:
+                want = (int(first[c]) << 2) | int(count[c] - 1)
+                small += 1
+            assert int(word) == want, (p, c)
+    return small
+
+
+@pytest.mark.parametrize("kind", ["tri", "point", "gauss"])
+@pytest.mark.parametrize("builder", ["lbvh", "sah"])
+def test_leaf4_small_subtrees_same_bits(cuda, kind, builder):
+    """Child subtrees of 2..4 primitives tested as leaves: same results as the plain binary
+    traversal for every query kind, after a refit too (codes depend on the topology only)."""
+    items = _items(kind)
+    tree = capi.DeviceTree(kind, items, builder=builder)
+    assert _check_small_codes(tree) > tree.n // 8
+    ref = oracle.LBVH(kind, items)
+    qh = _queries(items, kind, 3_001, 5)
+    q = _dev(qh)
+    lo, hi = qh.min(0), qh.max(0)
+    r = float(np.linalg.norm(hi - lo)) * 0.04
+    rays = _dev(_random_rays(lo, hi, 20_001, 6)) if kind == "tri" else None
+
+    def same(t):
+        for extra in (0, capi.QK_ORDER_MORTON):
+            f = capi.QK_TUNE_LEAF4 | extra
+            assert cuda.equal(t.closest(q, f), t.closest(q, 0)), extra
+            for k in (1, 8, 16):
+                assert cuda.equal(t.knn(q, k, f), t.knn(q, k, 0)), (k, extra)
+            o1, k1 = t.radius(q, r, f)
+            o0, k0 = t.radius(q, r, 0)
+            assert cuda.equal(o1, o0) and cuda.equal(k1, k0)
+            if rays is not None:
+                for tune in (0, capi.QK_TUNE_HIGH_OCC):
+                    want, want_ids = t.raycast_ids(rays, extra)
+                    got, got_ids = t.raycast_ids(rays, f | tune)
+                    assert cuda.equal(got, want) and cuda.equal(got_ids, want_ids)
+
+    same(tree)
+    got = tree.closest(q, capi.QK_TUNE_LEAF4).cpu().numpy().view(np.uint32)
+    assert np.array_equal(got, ref.closest(qh))
+    moved = items.copy()
+    moved[:, :3] += np.random.default_rng(9).normal(0, 0.05, (len(items), 3)).astype(np.float32)
+    tree.refit(moved)
+    _check_small_codes(tree)
+    same(tree)
+    ref.refit(moved)
+    got = tree.knn(q, 8, capi.QK_TUNE_LEAF4).cpu().numpy().view(np.uint32)
+    assert np.array_equal(got, ref.knn(qh, 8))
+
+
+@pytest.mark.parametrize("n", [2, 3, 4, 5, 9])
+def test_leaf4_tiny_trees(cuda, n):
+    rng = np.random.default_rng(n)
+    pts = rng.uniform(0, 1, (n, 3)).astype(np.float32)
+    tree = capi.DeviceTree("point", pts)
+    _check_small_codes(tree)
+    q = _dev(rng.uniform(-0.5, 1.5, (257, 3)).astype(np.float32))
+    f = capi.QK_TUNE_LEAF4
+    assert cuda.equal(tree.closest(q, f), tree.closest(q, 0))
+    assert cuda.equal(tree.knn(q, min(n, 4), f), tree.knn(q, min(n, 4), 0))
+    o1, k1 = tree.radius(q, 0.5, f)
+    o0, k0 = tree.radius(q, 0.5, 0)
+    assert cuda.equal(o1, o0) and cuda.equal(k1, k0)
+
+
 def test_split_knn_sphere_matches_oracle(cuda):
     pts = workloads.point_cloud("surface", 100_000, 2)
     q = workloads.uniform_points(2_000, pts.min(0), pts.max(0), 2, 13)

@@ -132,6 +132,55 @@ int qk_refit(qk_tree* tree, const void* items, void* workspace, size_t workspace
 int qk_refit_dirty(qk_tree* tree, const int32_t* dirty_ids, const void* dirty_items, int count,
                    void* workspace, size_t workspace_bytes, void* stream);
 
+/*
+ * Topology edit (updateBVHGPU / updatePointBVHGPU / updateGaussianBVHGPU,
+ * src/gpu/gpu_bvh.h:182-213; GpuTopoEdit semantics).  The new scene is the old one's
+ * survivors in their order (old scene indices `deleted` removed), new primitives at the new
+ * indices `inserted`, and `appended` more at its end; `moved` lists new indices whose geometry
+ * changed.  All index arrays are device int32 arrays; deleted and inserted ascending and
+ * unique; extra_items holds the n_inserted + appended new primitives (the inserted ones in
+ * ascending index order, then the appended ones) and moved_items the n_moved moved ones.
+ *
+ * Only the small subtrees the edit touches are rebuilt (SAH over each); the rest is relinked
+ * and renumbered.  new_tree: arrays for n_new = n_old - n_deleted + n_inserted + appended
+ * primitives, of the same kind, none shared with old_tree; its wide layer is not built.
+ * Query results on it equal those of a fresh build of the new scene.  Syncs.  When the plan
+ * declines (the edit touches too much of the tree, a subtree would outgrow the forest
+ * builder, or the root would change) info->rebuild is set, new_tree is left unwritten and the
+ * caller rebuilds from the whole new scene.  cut_size: largest subtree a touched leaf may
+ * rebuild (2..1024; 0 = n_old / (8 x edited primitives) clamped to 8..256, so the rebuilt
+ * subtrees hold about an eighth of the tree).
+ */
+typedef struct qk_topo_edit {
+    const int32_t* deleted;
+    int n_deleted;
+    const int32_t* inserted;
+    int n_inserted;
+    int appended;
+    const int32_t* moved;
+    int n_moved;
+    const void* extra_items;
+    const void* moved_items;
+} qk_topo_edit;
+
+typedef struct qk_topo_info {
+    int rebuild;         /* 1: the plan declined; new_tree untouched */
+    int cuts;            /* subtrees rebuilt */
+    int old_leaves;      /* leaves under them before the edit */
+    int new_leaves;      /* ... after it */
+    int max_cut;         /* largest rebuilt subtree after the edit */
+    int spliced;         /* internal nodes removed because one side became empty */
+    int depth;           /* depth of the new tree */
+    int reason;          /* why the plan declined: 1 the root is a subtree to rebuild, 2 the
+                            root loses a side, 3 a subtree exceeds 1024 leaves, 4 more than a
+                            quarter of the leaves, 5 depth */
+} qk_topo_info;
+
+size_t qk_update_workspace_bytes(int kind, int n_old, int n_new, int n_extra);
+int qk_update_topology(const qk_tree* old_tree, qk_tree* new_tree, const qk_topo_edit* edit,
+                       int cut_size, int sah_bins, qk_topo_info* info, void* workspace,
+                       size_t workspace_bytes, void* stream);
+
 /* 4-wide collapse (buildWideNodesGPU, src/gpu/gpu_bvh.h:229).  Syncs to read the count into
  * tree->wide_count.  With tree->wide == NULL the call only computes wide_id and the count, so
  * the caller can allocate wide_count * 128 bytes and call again to emit the nodes. */

@@ -31,7 +31,7 @@ NVCC_FLAGS = [
     "--expt-relaxed-constexpr", "-Xptxas", "-warn-spills",
 ]
 CU_SOURCES = ["qk_sort.cu", "qk_build.cu", "qk_sah.cu", "qk_query.cu", "qk_grad.cu",
-              "qk_capi.cu", "qk_noalloc.cu", "qk_batch.cu", "gpu_bvh.cu"]
+              "qk_capi.cu", "qk_noalloc.cu", "qk_batch.cu", "qk_topo.cu", "gpu_bvh.cu"]
 C_SOURCES = ["scenes.c"]
 LIB = OUT / "libquarry_b200.so"
 

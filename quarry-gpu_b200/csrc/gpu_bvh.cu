@@ -64,18 +64,49 @@ struct Timer {
     }
 };
 
-// Device state behind GpuBVH::impl.
+constexpr int kTreeArrays = 10;
+
+// Device state behind GpuBVH::impl.  Topology edits write the new tree into the spare array
+// set and swap, so steady updates allocate nothing.
 struct Impl {
     qk_tree t{};
-    void* arrays[11] = {};
+    void* arrays[kTreeArrays] = {};
+    int cap = 0;                     // primitives the arrays hold
+    void* spare[kTreeArrays] = {};
+    int spareCap = 0;
     void* ws = nullptr;
     size_t wsBytes = 0;
     void* stage = nullptr;  // scene-order upload buffer (refit, validate)
     size_t stageBytes = 0;
+    void* upd = nullptr;    // topology-edit workspace and edit script
+    size_t updBytes = 0;
     int builder = QK_BUILD_LBVH;
     int bins = 32;
-    bool hadWide = false;
+    int baseDepth = 0;      // depth after the last full build (topology-edit depth budget)
 };
+
+void allocTreeArrays(int kind, int cap, void* arrays[kTreeArrays]) {
+    qk_tree_sizes sz{};
+    qkOk(qk_tree_bytes(kind, cap, &sz), "tree sizes");
+    const size_t sizes[kTreeArrays] = {sz.nodes, sz.bnodes, sz.items, sz.prim_ids, sz.parent,
+                                       sz.depth_arr, sz.leaves, sz.slot_of, sz.flags, sz.wide_id};
+    for (int i = 0; i < kTreeArrays; ++i) arrays[i] = devAlloc(sizes[i], "tree arrays");
+}
+
+void bindTree(qk_tree& t, int kind, int n, void* const arrays[kTreeArrays]) {
+    t.kind = kind;
+    t.n = n;
+    t.nodes = arrays[0];
+    t.bnodes = arrays[1];
+    t.items = arrays[2];
+    t.prim_ids = static_cast<int32_t*>(arrays[3]);
+    t.parent = static_cast<int32_t*>(arrays[4]);
+    t.depth_arr = static_cast<int32_t*>(arrays[5]);
+    t.leaves = arrays[6];
+    t.slot_of = static_cast<int32_t*>(arrays[7]);
+    t.flags = static_cast<int32_t*>(arrays[8]);
+    t.wide_id = static_cast<int32_t*>(arrays[9]);
+}
 
 Impl* implOf(const GpuBVH& bvh) {
     if (!bvh.impl) throw std::runtime_error("GpuBVH is not built");
@@ -105,8 +136,10 @@ void syncPublic(GpuBVH& bvh, Impl* im) {
 void freeImpl(Impl* im) {
     if (!im) return;
     for (void*& p : im->arrays) devFree(p);
+    for (void*& p : im->spare) devFree(p);
     devFree(im->ws);
     devFree(im->stage);
+    devFree(im->upd);
     if (im->t.wide) {
         void* w = im->t.wide;
         cudaFree(w);
@@ -120,26 +153,12 @@ GpuBVH buildImpl(int kind, const void* host, size_t itemBytes, int n, int builde
     auto* im = new Impl;
     GpuBVH bvh;
     try {
-        qk_tree_sizes sz{};
-        qkOk(qk_tree_bytes(kind, n, &sz), "tree sizes");
-        const size_t sizes[] = {sz.nodes, sz.items, sz.prim_ids, sz.parent, sz.depth_arr,
-                                sz.bnodes, sz.leaves, sz.slot_of, sz.flags, sz.wide_id};
-        for (int i = 0; i < 10; ++i) im->arrays[i] = devAlloc(sizes[i], "tree arrays");
+        allocTreeArrays(kind, n, im->arrays);
+        im->cap = n;
         qk_tree& t = im->t;
-        t.kind = kind;
-        t.n = n;
-        t.nodes = im->arrays[0];
-        t.items = im->arrays[1];
-        t.prim_ids = static_cast<int32_t*>(im->arrays[2]);
-        t.parent = static_cast<int32_t*>(im->arrays[3]);
-        t.depth_arr = static_cast<int32_t*>(im->arrays[4]);
-        t.bnodes = im->arrays[5];
-        t.leaves = im->arrays[6];
-        t.slot_of = static_cast<int32_t*>(im->arrays[7]);
-        t.flags = static_cast<int32_t*>(im->arrays[8]);
-        t.wide_id = static_cast<int32_t*>(im->arrays[9]);
+        bindTree(t, kind, n, im->arrays);
         t.wide = nullptr;
-        cudaOk(cudaMemset(t.flags, 0, sz.flags), "flags");
+        cudaOk(cudaMemset(t.flags, 0, sizeof(int32_t) * static_cast<size_t>(n - 1)), "flags");
         im->builder = builder;
         im->wsBytes = qk_build_workspace_bytes(kind, n, builder);
         im->ws = devAlloc(im->wsBytes, "build workspace");
@@ -155,6 +174,7 @@ GpuBVH buildImpl(int kind, const void* host, size_t itemBytes, int n, int builde
             timings->totalMs = ms;
         }
         bvh.sah = builder == QK_BUILD_SAH;
+        im->baseDepth = t.depth;
         bvh.impl = im;
         syncPublic(bvh, im);
     } catch (...) {
@@ -239,6 +259,12 @@ void checkEdit(int nOld, const GpuTopoEdit& edit, size_t newSize) {
     }
 }
 
+// Depth a topology edit may add over the last full build before the tree is rebuilt to
+// rebalance it (quarry's kTopoDepthSlack, src/gpu/lbvh.cu:2543-2545).
+constexpr int kTopoDepthSlack = 6;
+
+size_t alignUp(size_t b) { return (b + 255) / 256 * 256; }
+
 template <typename Item>
 double updateImpl(GpuBVH& bvh, int kind, const std::vector<Item>& items, const GpuTopoEdit& edit,
                   GpuTopoUpdateTimings* timings) {
@@ -251,6 +277,7 @@ double updateImpl(GpuBVH& bvh, int kind, const std::vector<Item>& items, const G
     t->deleted = static_cast<int>(edit.deleted.size());
     t->inserted = static_cast<int>(edit.inserted.size());
     t->appended = edit.appended;
+    t->moved = static_cast<int>(edit.moved.size());
     if (edit.deleted.empty() && edit.inserted.empty() && edit.appended == 0) {
         GpuRefitTimings rt;
         t->refitMs = refitImpl<Item>(bvh, items, &edit.moved, &rt);
@@ -259,24 +286,107 @@ double updateImpl(GpuBVH& bvh, int kind, const std::vector<Item>& items, const G
         t->newDepth = bvh.depth;
         return t->totalMs;
     }
-    // the primitive set changed: rebuild with the tree's own builder (results equal a fresh
-    // build by construction) and restore the 4-wide layer when the tree had one
     const bool wide = im->t.wide != nullptr;
-    const int builder = im->builder;
+    const int nOld = im->t.n;
+    const int nNew = static_cast<int>(items.size());
+    const int nIns = static_cast<int>(edit.inserted.size());
+    const int nDel = static_cast<int>(edit.deleted.size());
+    const int nMov = static_cast<int>(edit.moved.size());
+    const int extra = nIns + edit.appended;
     Timer timer;
-    GpuBVH fresh = buildImpl(kind, items.data(), sizeof(Item), static_cast<int>(items.size()),
-                             builder, nullptr);
-    destroyBVHGPU(bvh);
-    bvh = fresh;
+
+    // rebuild with the tree's own builder (results equal a fresh build by construction) and
+    // restore the 4-wide layer when the tree had one
+    auto rebuildAll = [&]() -> double {
+        const int builder = im->builder;
+        GpuBVH fresh = buildImpl(kind, items.data(), sizeof(Item), nNew, builder, nullptr);
+        destroyBVHGPU(bvh);
+        bvh = fresh;
+        im = implOf(bvh);
+        double wideMs = 0.0;
+        if (wide) wideMs = buildWideNodesGPU(bvh);
+        t->totalMs = timer.stop();
+        t->wideMs = wideMs;
+        t->surgeryMs = t->totalMs - wideMs;
+        t->surgeryRoots = 1;
+        t->rebuiltLeaves = bvh.primCount;
+        t->newDepth = bvh.depth;
+        t->fullRebuild = true;
+        return t->totalMs;
+    };
+    // more than half of the primitives change: a rebuild costs about as much
+    if (nDel + extra > nOld / 2) return rebuildAll();
+
+    // the edit script and only the primitives it brings, in one upload
+    const size_t oDel = 0, oIns = alignUp(sizeof(int) * nDel);
+    const size_t oMov = oIns + alignUp(sizeof(int) * nIns);
+    const size_t oExtra = oMov + alignUp(sizeof(int) * nMov);
+    const size_t oMoved = oExtra + alignUp(sizeof(Item) * extra);
+    const size_t scriptBytes = oMoved + alignUp(sizeof(Item) * nMov);
+    std::vector<char> script(scriptBytes);
+    if (nDel) std::memcpy(script.data() + oDel, edit.deleted.data(), sizeof(int) * nDel);
+    if (nIns) std::memcpy(script.data() + oIns, edit.inserted.data(), sizeof(int) * nIns);
+    if (nMov) std::memcpy(script.data() + oMov, edit.moved.data(), sizeof(int) * nMov);
+    Item* ex = reinterpret_cast<Item*>(script.data() + oExtra);
+    for (int k = 0; k < nIns; ++k) ex[k] = items[static_cast<size_t>(edit.inserted[k])];
+    for (int k = 0; k < edit.appended; ++k)
+        ex[nIns + k] = items[static_cast<size_t>(nNew - edit.appended + k)];
+    Item* mv = reinterpret_cast<Item*>(script.data() + oMoved);
+    for (int k = 0; k < nMov; ++k) mv[k] = items[static_cast<size_t>(edit.moved[k])];
+    const size_t wsBytes = alignUp(qk_update_workspace_bytes(kind, nOld, nNew, extra));
+    if (im->updBytes < wsBytes + scriptBytes) {
+        devFree(im->upd);
+        im->updBytes = wsBytes + scriptBytes;
+        im->upd = devAlloc(im->updBytes, "topology workspace");
+    }
+    char* dScript = static_cast<char*>(im->upd) + wsBytes;
+    cudaOk(cudaMemcpy(dScript, script.data(), scriptBytes, cudaMemcpyHostToDevice), "H2D edit");
+    Timer surgery;
+
+    if (im->spareCap < nNew) {
+        for (void*& p : im->spare) devFree(p);
+        im->spareCap = nNew + nNew / 8 + 16;
+        allocTreeArrays(kind, im->spareCap, im->spare);
+    }
+    qk_tree nt{};
+    bindTree(nt, kind, nNew, im->spare);
+    qk_topo_edit ed{};
+    ed.deleted = reinterpret_cast<const int32_t*>(dScript + oDel);
+    ed.n_deleted = nDel;
+    ed.inserted = reinterpret_cast<const int32_t*>(dScript + oIns);
+    ed.n_inserted = nIns;
+    ed.appended = edit.appended;
+    ed.moved = reinterpret_cast<const int32_t*>(dScript + oMov);
+    ed.n_moved = nMov;
+    ed.extra_items = dScript + oExtra;
+    ed.moved_items = dScript + oMoved;
+    qk_topo_info info{};
+    qkOk(qk_update_topology(&im->t, &nt, &ed, 0, im->bins, &info, im->upd, wsBytes, nullptr),
+         "topology update");
+    if (info.rebuild || nt.depth > im->baseDepth + kTopoDepthSlack) return rebuildAll();
+    t->surgeryMs = surgery.stop();
+
+    nt.wide = im->t.wide;  // reused by the wide rebuild below (or freed with the tree)
+    nt.wide_count = 0;
+    im->t = nt;
+    for (int i = 0; i < kTreeArrays; ++i) std::swap(im->arrays[i], im->spare[i]);
+    std::swap(im->cap, im->spareCap);
+    const size_t buildWs = qk_build_workspace_bytes(kind, nNew, im->builder);
+    if (buildWs > im->wsBytes) {
+        devFree(im->ws);
+        im->wsBytes = buildWs;
+        im->ws = devAlloc(im->wsBytes, "build workspace");
+    }
+    syncPublic(bvh, im);
     double wideMs = 0.0;
     if (wide) wideMs = buildWideNodesGPU(bvh);
     t->totalMs = timer.stop();
     t->wideMs = wideMs;
-    t->surgeryMs = t->totalMs - wideMs;
-    t->surgeryRoots = 1;
-    t->rebuiltLeaves = bvh.primCount;
+    t->uploadMs = t->totalMs - t->surgeryMs - wideMs;
+    t->surgeryRoots = info.cuts;
+    t->rebuiltLeaves = info.new_leaves;
     t->newDepth = bvh.depth;
-    t->fullRebuild = true;
+    t->fullRebuild = false;
     return t->totalMs;
 }
 

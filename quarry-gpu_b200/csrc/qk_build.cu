@@ -500,6 +500,10 @@ int validate_impl(const qk_tree* t, const void* items, int* err, void* ws, cudaS
 
 }  // namespace
 
+int finish_tree_boxes(qk_tree* t, Header* h, int2* ranges, cudaStream_t s) {
+    return finish_tree(t, h, ranges, s);
+}
+
 // workspace of the builders themselves; the bottom-up ranges follow it
 size_t build_core_bytes(int kind, int n, int builder) {
     (void)kind;

@@ -176,6 +176,43 @@ int qk_refit_dirty(qk_tree* tree, const int32_t* dirty_ids, const void* dirty_it
     return refit_tree_dirty(tree, dirty_ids, dirty_items, count, workspace, as_stream(stream));
 }
 
+size_t qk_update_workspace_bytes(int kind, int n_old, int n_new, int n_extra) {
+    if (kind < 0 || kind > 2 || n_old < 2 || n_new < 2 || n_extra < 0) return 0;
+    return update_ws_bytes(kind, n_old, n_new, n_extra);
+}
+
+int qk_update_topology(const qk_tree* old_tree, qk_tree* new_tree, const qk_topo_edit* edit,
+                       int cut_size, int sah_bins, qk_topo_info* info, void* workspace,
+                       size_t workspace_bytes, void* stream) {
+    int st = check_tree(old_tree);
+    if (st) return st;
+    if ((st = check_tree(new_tree))) return st;
+    if (!edit || !info) return fail(QK_ERR_INVALID, "edit or info is NULL");
+    if (new_tree->kind != old_tree->kind)
+        return fail(QK_ERR_INVALID, "new tree kind %d differs from %d", new_tree->kind, old_tree->kind);
+    if (new_tree->nodes == old_tree->nodes || new_tree->items == old_tree->items ||
+        new_tree->leaves == old_tree->leaves || new_tree->bnodes == old_tree->bnodes ||
+        new_tree->prim_ids == old_tree->prim_ids || new_tree->parent == old_tree->parent)
+        return fail(QK_ERR_INVALID, "new tree shares arrays with the old tree");
+    if (edit->n_deleted < 0 || edit->n_inserted < 0 || edit->appended < 0 || edit->n_moved < 0)
+        return fail(QK_ERR_INVALID, "negative edit counts");
+    const long long n_new = static_cast<long long>(old_tree->n) - edit->n_deleted +
+                            edit->n_inserted + edit->appended;
+    if (n_new != new_tree->n)
+        return fail(QK_ERR_INVALID, "the edit leaves %lld primitives, the new tree has %d", n_new,
+                    new_tree->n);
+    const int n_extra = edit->n_inserted + edit->appended;
+    if ((edit->n_deleted && !edit->deleted) || (edit->n_inserted && !edit->inserted) ||
+        (edit->n_moved && (!edit->moved || !edit->moved_items)) || (n_extra && !edit->extra_items))
+        return fail(QK_ERR_INVALID, "edit array is NULL");
+    if (sah_bins < 4 || sah_bins > 64) return fail(QK_ERR_INVALID, "sah_bins must be in [4, 64]");
+    st = check_ws(workspace, workspace_bytes,
+                  update_ws_bytes(old_tree->kind, old_tree->n, new_tree->n, n_extra));
+    if (st) return st;
+    return update_topology(old_tree, new_tree, edit, cut_size, sah_bins, info, workspace,
+                           as_stream(stream));
+}
+
 int qk_wide_build(qk_tree* tree, void* workspace, size_t workspace_bytes, void* stream) {
     int st = check_tree(tree);
     if (st) return st;

@@ -855,6 +855,7 @@ __global__ __launch_bounds__(kBlock) void k_block_build(const Task* __restrict__
     for (int ti = blockIdx.x; ti < ntask; ti += gridDim.x) {
         const Task tk = tasks[ti];
         const int count = tk.end - tk.begin;
+        if (tk.node < 0) continue;  // a forest slot with nothing to build (0 or 1 primitive)
         if (count < 2 || count > kBlockRange) {
             if (threadIdx.x == 0) atomicAdd(err, 1);
             continue;
@@ -1232,6 +1233,21 @@ size_t sah_ws_bytes(int n) {
     Carve c;
     carve_sah(c, n);
     return c.used;
+}
+
+int sah_forest(const int4* tasks, int ntask, const int* id_base, int* order, const float4* cen,
+               const float4* plo, const float4* phi, qk_tree* t, int bins, int* err,
+               cudaStream_t s) {
+    static_assert(sizeof(Task) == sizeof(int4), "forest tasks are {begin, end, node, depth}");
+    if (bins < 4 || bins > kMaxBins) return fail(QK_ERR_INVALID, "sah_bins must be in [4, 64]");
+    if (ntask <= 0) return QK_OK;
+    cudaFuncSetAttribute(k_block_build, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         static_cast<int>(block_smem(kMaxBins)));
+    k_block_build<<<min(ntask, 148 * 4), kBlock, block_smem(bins), s>>>(
+        reinterpret_cast<const Task*>(tasks), ntask, id_base, order, cen, plo, phi,
+        static_cast<Node*>(t->nodes), static_cast<BNode*>(t->bnodes), t->parent, t->n, bins, err);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? QK_OK : cuda_status(e, "SAH forest");
 }
 
 int build_sah(qk_tree* t, int bins, const void* items, void* ws, cudaStream_t s) {

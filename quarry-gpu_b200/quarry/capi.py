@@ -59,6 +59,18 @@ class QkBatchIo(ctypes.Structure):
                 ("k", ctypes.c_int32), ("pad", ctypes.c_int32)]
 
 
+class QkTopoEdit(ctypes.Structure):
+    _fields_ = [("deleted", _P), ("n_deleted", ctypes.c_int32), ("inserted", _P),
+                ("n_inserted", ctypes.c_int32), ("appended", ctypes.c_int32), ("moved", _P),
+                ("n_moved", ctypes.c_int32), ("extra_items", _P), ("moved_items", _P)]
+
+
+class QkTopoInfo(ctypes.Structure):
+    _fields_ = [(name, ctypes.c_int32) for name in ("rebuild", "cuts", "old_leaves",
+                                                    "new_leaves", "max_cut", "spliced", "depth",
+                                                    "reason")]
+
+
 _PP = ctypes.POINTER(ctypes.c_void_p)
 _I64P = ctypes.POINTER(ctypes.c_int64)
 
@@ -76,6 +88,10 @@ EXPORTS = {
     "qk_refit": (_I, [ctypes.POINTER(QkTree), _P, _P, _SZ, _P]),
     "qk_refit_dirty": (_I, [ctypes.POINTER(QkTree), _P, _P, _I, _P, _SZ, _P]),
     "qk_wide_build": (_I, [ctypes.POINTER(QkTree), _P, _SZ, _P]),
+    "qk_update_workspace_bytes": (_SZ, [_I, _I, _I, _I]),
+    "qk_update_topology": (_I, [ctypes.POINTER(QkTree), ctypes.POINTER(QkTree),
+                                ctypes.POINTER(QkTopoEdit), _I, _I, ctypes.POINTER(QkTopoInfo),
+                                _P, _SZ, _P]),
     "qk_raycast": (_I, [ctypes.POINTER(QkTree), _P, _I, _P, _U, _P, _P, _SZ, _P]),
     "qk_closest": (_I, [ctypes.POINTER(QkTree), _P, _I, _P, _U, _P, _P, _SZ, _P]),
     "qk_knn": (_I, [ctypes.POINTER(QkTree), _P, _I, _I, _I, _P, _U, _P, _P, _SZ, _P]),
@@ -203,24 +219,28 @@ class DeviceTree:
         self.items_scene = items.reshape(-1, STRIDE[self.kind]).contiguous()
         n = self.items_scene.shape[0]
         self.n = n
-        sizes = QkTreeSizes()
-        check(L.qk_tree_bytes(self.kind, n, ctypes.byref(sizes)), "qk_tree_bytes")
-        self.arrays = {}
-        for name in ("nodes", "items", "prim_ids", "parent", "depth_arr", "bnodes", "leaves",
-                     "slot_of", "flags", "wide_id"):
-            self.arrays[name] = _dev_bytes(getattr(sizes, name))
-        self.arrays["flags"].zero_()
-        self.t = QkTree()
-        self.t.kind = self.kind
-        self.t.n = n
-        for name, buf in self.arrays.items():
-            setattr(self.t, name, buf.data_ptr())
-        self.t.wide = None
+        self.arrays, self.t = self._alloc(n)
         self.ws = Workspace()
         self.builder = QK_BUILD_SAH if builder == "sah" else QK_BUILD_LBVH
         self.sah_bins = sah_bins
         self.build()
-        del torch
+        del torch, L
+
+    def _alloc(self, n: int):
+        sizes = QkTreeSizes()
+        check(lib().qk_tree_bytes(self.kind, n, ctypes.byref(sizes)), "qk_tree_bytes")
+        arrays = {}
+        for name in ("nodes", "items", "prim_ids", "parent", "depth_arr", "bnodes", "leaves",
+                     "slot_of", "flags", "wide_id"):
+            arrays[name] = _dev_bytes(getattr(sizes, name))
+        arrays["flags"].zero_()
+        t = QkTree()
+        t.kind = self.kind
+        t.n = n
+        for name, buf in arrays.items():
+            setattr(t, name, buf.data_ptr())
+        t.wide = None
+        return arrays, t
 
     # ---- build / refit ----
     def _build_ws(self):
@@ -264,6 +284,38 @@ class DeviceTree:
         check(lib().qk_refit_dirty(ctypes.byref(self.t), _ptr(ids), _ptr(items_subset),
                                    int(ids.numel()), _ptr(ws), ws.numel(), _stream()),
               "qk_refit_dirty")
+
+    def update_topology(self, new_items, deleted=(), inserted=(), moved=(), cut_size: int = 0):
+        """Topology edit (qk_update_topology) toward the new scene `new_items` (scene order):
+        deleted old indices, inserted new indices, moved new indices; the appended count
+        follows from the sizes.  Surgery when the plan accepts, else a full rebuild.  Returns
+        the plan's qk_topo_info fields as a dict.  The wide layer is dropped."""
+        torch = _torch()
+        if isinstance(new_items, np.ndarray):
+            new_items = to_device(new_items.reshape(-1, STRIDE[self.kind]), np.float32)
+        new_items = new_items.reshape(-1, STRIDE[self.kind]).contiguous()
+        n_new = new_items.shape[0]
+        dele = torch.as_tensor(np.asarray(deleted, np.int32).reshape(-1), device="cuda")
+        ins = torch.as_tensor(np.asarray(inserted, np.int32).reshape(-1), device="cuda")
+        mov = torch.as_tensor(np.asarray(moved, np.int32).reshape(-1), device="cuda")
+        appended = n_new - self.n + dele.numel() - ins.numel()
+        extra_idx = torch.cat([ins.long(), torch.arange(n_new - appended, n_new, device="cuda")])
+        extra = new_items[extra_idx].contiguous()
+        moved_items = new_items[mov.long()].contiguous()
+        e = QkTopoEdit(_ptr(dele), dele.numel(), _ptr(ins), ins.numel(), int(appended), _ptr(mov),
+                       mov.numel(), _ptr(extra), _ptr(moved_items))
+        arrays, t = self._alloc(n_new)
+        nb = lib().qk_update_workspace_bytes(self.kind, self.n, n_new, int(extra.shape[0]))
+        ws = _dev_bytes(nb)
+        info = QkTopoInfo()
+        check(lib().qk_update_topology(ctypes.byref(self.t), ctypes.byref(t), ctypes.byref(e),
+                                       int(cut_size), self.sah_bins, ctypes.byref(info), _ptr(ws),
+                                       ws.numel(), _stream()), "qk_update_topology")
+        out = {name: getattr(info, name) for name, _ in QkTopoInfo._fields_}
+        self.arrays, self.t, self.n, self.items_scene = arrays, t, n_new, new_items
+        if info.rebuild:
+            self.build()
+        return out
 
     # ---- read-back ----
     def host(self, name: str, dtype, count: int | None = None) -> np.ndarray:

@@ -333,6 +333,65 @@ def grad_arm(args, world, rank, local):
 
 
 # ---------------------------------------------------------------------------------------
+# topology edits: subtree surgery against a rebuild of the edited scene
+# ---------------------------------------------------------------------------------------
+def topology_timing(kind, items, builder, bins, queries_d, seed, timed_ms, rays_d=None):
+    """1% edits of quarry's GpuTopoEdit kind (a quarter each deleted, inserted, appended and
+    moved), "cluster" (around one spot) and "scatter" (uniform): qk_update_topology on the
+    built tree against qk_build of the edited scene, both device-timed with the scripts
+    already resident.  The edited tree must answer closest / kNN (and rays) like the rebuild."""
+    import ctypes
+
+    import torch
+
+    from quarry import capi, workloads as w
+
+    out = {}
+    for mode in ("cluster", "scatter"):
+        new, dele, ins, mov = w.topology_edit(items, 0.01, mode, seed)
+        base = capi.DeviceTree(kind, items, builder=builder, sah_bins=bins)
+        n_new = len(new)
+        new_d = capi.to_device(new, np.float32)
+        dele_d, ins_d, mov_d = (capi.to_device(a, np.int32) for a in (dele, ins, mov))
+        app = n_new - len(items) + len(dele) - len(ins)
+        tail = torch.arange(n_new - app, n_new, device="cuda")
+        extra = new_d[torch.cat([ins_d.long(), tail])].contiguous()
+        moved_items = new_d[mov_d.long()].contiguous()
+        e = capi.QkTopoEdit(dele_d.data_ptr(), len(dele), ins_d.data_ptr(), len(ins), app,
+                            mov_d.data_ptr(), len(mov), extra.data_ptr(), moved_items.data_ptr())
+        arrays, nt = base._alloc(n_new)
+        nb = capi.lib().qk_update_workspace_bytes(base.kind, base.n, n_new, int(extra.shape[0]))
+        ws = torch.empty(nb, dtype=torch.uint8, device="cuda")
+        info = capi.QkTopoInfo()
+
+        def surgery():
+            capi.check(capi.lib().qk_update_topology(
+                ctypes.byref(base.t), ctypes.byref(nt), ctypes.byref(e), 0, bins,
+                ctypes.byref(info), ws.data_ptr(), nb, capi._stream()), "qk_update_topology")
+
+        s_ms = timed_ms(surgery)
+        fresh = capi.DeviceTree(kind, new_d, builder=builder, sah_bins=bins)
+        b_ms = timed_ms(fresh.build)
+        entry = {"edited": int(len(dele) + len(ins) + app + len(mov)), "surgery_ms": round(s_ms, 4),
+                 "rebuild_ms": round(b_ms, 4), "ratio": round(s_ms / b_ms, 3),
+                 "rebuilt_subtrees": info.cuts, "rebuilt_leaves": info.new_leaves,
+                 "spliced": info.spliced, "fallback": bool(info.rebuild)}
+        if not info.rebuild:
+            base.update_topology(new_d, dele, ins, mov)
+            same = (torch.equal(base.closest(queries_d), fresh.closest(queries_d)) and
+                    torch.equal(base.knn(queries_d, 8), fresh.knn(queries_d, 8)))
+            if rays_d is not None:
+                same = same and torch.equal(base.raycast(rays_d), fresh.raycast(rays_d))
+            if not same:
+                raise RuntimeError(f"topology {mode}: edited tree answers differently")
+            entry["depth"] = base.depth
+            entry["fresh_depth"] = fresh.depth
+        out[f"{mode}_1pct"] = entry
+        del base, fresh, arrays, ws
+    return out
+
+
+# ---------------------------------------------------------------------------------------
 # point clouds: closest / kNN8 / radius 1.0 and the 1% coherent refit
 # ---------------------------------------------------------------------------------------
 def points_arm(args, world, rank, local):
@@ -489,6 +548,11 @@ def points_arm(args, world, rank, local):
                        "knn_fingerprint_after_refit": f"0x{oracle.knn_hash(want):016x}"}
         t.refit(capi.to_device(c["pts"], np.float32))
 
+    # ---- topology edits (1%, cluster / scatter) on the surface cloud's LBVH ----
+    topology = topology_timing("point", clouds["surface"]["pts"], "lbvh", 32,
+                               clouds["surface"]["q_d"], seed,
+                               lambda fn: float(np.median(timed(fn, 5, 2))))
+
     # ---- end to end: queries from pinned host memory, results read back ----
     host_q = {kind: torch.from_numpy(c["q"]).pin_memory() for kind, c in clouds.items()}
 
@@ -542,7 +606,7 @@ def points_arm(args, world, rank, local):
                        "parallelism": f"replica x{world}"},
             "variants_ms": {kk: round(v, 4) for kk, v in vms.items()},
             "per_op_ms": {kk: round(v, 4) for kk, v in per_op.items()},
-            "radius_results": radius_keys, "refit": refit,
+            "radius_results": radius_keys, "refit": refit, "topology": topology,
             "parity": {"against": kind_ref, "fingerprints": parity,
                        "variants": "all layouts / orders / schedules bit-identical"},
             "roofline": roofline,
@@ -955,6 +1019,26 @@ def rays_arm(args, world, rank, local):
     knn_variant = min(knn_ms_by, key=knn_ms_by.get)
     knn_ms = knn_ms_by[knn_variant]
 
+    # ---- topology edits on the SAH tree (the surgery path; results checked at full size) ----
+    def med_ms(fn, steps=5):
+        for _ in range(2):
+            fn()
+        ts = []
+        for _ in range(steps):
+            l2_flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return float(np.median(ts))
+
+    topology = None
+    if args.workload == "city":
+        topology = topology_timing("tri", cfg.tris, "sah", 32, q_d, 1 + rank, med_ms,
+                                   rays_d[:200_000])
+
     # ---- e2e through the C ABI from pinned host buffers: qk_raycast_host uploads, traces and
     # reads back in chunks over two streams, all inside the timed region ----
     host_rays = torch.from_numpy(np.ascontiguousarray(cfg.rays)).pin_memory()
@@ -1025,6 +1109,7 @@ def rays_arm(args, world, rank, local):
                     "variants_ms": {kk: round(v, 4) for kk, v in knn_ms_by.items()},
                     "mqueries_per_s": round(q_d.shape[0] / (knn_ms * 1e-3) / 1e6, 2)},
             "fingerprint": f"0x{fp:016x}", "hits": int(hits), "parity": parity,
+            "topology": topology,
             "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
             "e2e": {"value": round(e2e_value, 2), "unit": "Mrays/s",
                     "h2d_bytes_per_step": int(cfg.rays.nbytes),

@@ -227,11 +227,9 @@ __global__ __launch_bounds__(kBlock) void k_dirty_merge(const int* __restrict__ 
     int p = parent[n - 1 + slot_of[ids[i]]];
     int guard = 0;
     while (p >= 0 && guard++ < 4096) {
-        __threadfence();
-        const int old = atomicAdd(&flags[p], 4);
+        const int old = arrive_add(&flags[p], 4);
         const int need = __popc(old & 3);
         if ((old >> 2) + 1 < need) return;
-        __threadfence();
         finish_node(nodes, bnodes, p, n, nullptr);
         flags[p] = 0;
         p = parent[p];

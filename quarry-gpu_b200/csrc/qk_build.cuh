@@ -161,9 +161,7 @@ __device__ __forceinline__ void climb(Node* __restrict__ nodes, BNode* __restric
     int p = parent[n - 1 + k];
     int guard = 0;
     while (p >= 0 && guard++ < 4096) {
-        __threadfence();
-        if (atomicAdd(&flags[p], 1) == 0) return;
-        __threadfence();
+        if (arrive_add(&flags[p], 1) == 0) return;
         finish_node(nodes, bnodes, p, n, ranges);
         flags[p] = 0;
         p = parent[p];

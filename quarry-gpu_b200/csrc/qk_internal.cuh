@@ -42,6 +42,19 @@ struct Carve {
     }
 };
 
+// Arrival counter of the bottom-up passes: one acquire-release add at device scope.  The
+// release half publishes the arriving thread's earlier writes (its child's box) before the
+// count changes; the acquire half makes the other arrivals' writes visible to the thread that
+// goes on to merge the node.  Replaces a full fence on each side of a relaxed atomicAdd.
+__device__ __forceinline__ int arrive_add(int* counter, int v) {
+    int old;
+    asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], %2;"
+                 : "=r"(old)
+                 : "l"(counter), "r"(v)
+                 : "memory");
+    return old;
+}
+
 // IEEE-754 bits mapped to a monotone unsigned order, for atomicMin / atomicMax on floats.
 __device__ __forceinline__ unsigned ord_f(float f) {
     const unsigned u = __float_as_uint(f);

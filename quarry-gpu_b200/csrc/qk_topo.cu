@@ -248,9 +248,7 @@ __global__ __launch_bounds__(kBlock) void k_topo_ranges(const Node* __restrict__
     int p = parent[n - 1 + k];
     int guard = 0;
     while (p >= 0 && guard++ < 4096) {
-        __threadfence();
-        if (atomicAdd(&visit[p], 1) == 0) return;
-        __threadfence();
+        if (arrive_add(&visit[p], 1) == 0) return;
         const int l = nodes[p].left, r = nodes[p].right;
         const int2 a = l >= n - 1 ? make_int2(l - (n - 1), 1) : __ldcg(range + l);
         const int2 b = r >= n - 1 ? make_int2(r - (n - 1), 1) : __ldcg(range + r);
@@ -527,22 +525,31 @@ __global__ __launch_bounds__(kBlock) void k_topo_stage_cuts(
     }
 }
 
-// new primitives, sorted by cut: after the cut's first-slot survivor (when it survives)
+// cut node of every new primitive -> its cut's rank in the cut list
+__global__ __launch_bounds__(kBlock) void k_topo_extra_rank(const int* __restrict__ cut_rank,
+                                                           int n_extra, uint32_t* __restrict__ key) {
+    const int k = blockIdx.x * kBlock + threadIdx.x;
+    if (k < n_extra) key[k] = static_cast<uint32_t>(cut_rank[key[k]]);
+}
+
+// new primitives, sorted by cut rank: after the cut's first-slot survivor (when it survives)
 template <class Ops>
 __global__ __launch_bounds__(kBlock) void k_topo_stage_extra(
     EditDev e, const qk_tree old_t, const uint32_t* __restrict__ key, const uint32_t* __restrict__ val,
-    const int2* __restrict__ range, const int* __restrict__ xs, const int* __restrict__ del_flag,
-    float* st_items, int* st_id, float4* cen, float4* plo, float4* phi, int* order, int* err) {
+    const int* __restrict__ list, const int2* __restrict__ range, const int* __restrict__ xs,
+    const int* __restrict__ del_flag, float* st_items, int* st_id, float4* cen, float4* plo,
+    float4* phi, int* order, int* err) {
     const int i = blockIdx.x * kBlock + threadIdx.x;
     const int n_extra = e.n_ins + e.appended;
     if (i >= n_extra) return;
-    const int c = static_cast<int>(key[i]);
+    const int ck = static_cast<int>(key[i]);
     int lo = 0, hi = i;  // first sorted entry of this cut
     while (lo < hi) {
         const int mid = (lo + hi) >> 1;
-        if (static_cast<int>(key[mid]) < c) lo = mid + 1;
+        if (static_cast<int>(key[mid]) < ck) lo = mid + 1;
         else hi = mid;
     }
+    const int c = list[ck];
     const int2 r = node_range(range, c, e.n_old);
     const int first_kept = del_flag[old_t.prim_ids[r.x]] ? 0 : 1;
     const int k = static_cast<int>(val[i]);
@@ -687,14 +694,16 @@ int update_impl(const qk_tree* old_t, qk_tree* new_t, const qk_topo_edit* ed, in
                                                        w.order, w.tasks, w.id_base, eerr);
     }
     if (n_extra > 0) {
-        // new primitives grouped by cut in index order (stable), so the forest is deterministic
+        // new primitives grouped by cut (dense cut rank as the key) in index order (stable),
+        // so the forest is deterministic
+        k_topo_extra_rank<<<blocks_for(n_extra), kBlock, 0, s>>>(w.cut_mark, n_extra, w.ext_key);
         int bits = 1;
-        while (bits < 32 && (1ll << bits) < nn) ++bits;
+        while (bits < 32 && (1ll << bits) < plan.cuts) ++bits;
         err = sort_pairs(w.ext_key, w.ext_val, w.ext_key_s, w.ext_val_s, n_extra, bits, w.sort_ws, s);
         if (err != cudaSuccess) return cuda_status(err, "topology extra sort");
         k_topo_stage_extra<Ops><<<blocks_for(n_extra), kBlock, 0, s>>>(
-            e, *old_t, w.ext_key_s, w.ext_val_s, w.range, w.wslot, w.del_flag, w.st_items, w.st_id,
-            w.cen, w.plo, w.phi, w.order, eerr);
+            e, *old_t, w.ext_key_s, w.ext_val_s, w.cut_list, w.range, w.wslot, w.del_flag,
+            w.st_items, w.st_id, w.cen, w.plo, w.phi, w.order, eerr);
     }
     if (plan.cuts > 0) {
         const int st = sah_forest(w.tasks, plan.cuts, w.id_base, w.order, w.cen, w.plo, w.phi,

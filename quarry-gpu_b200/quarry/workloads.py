@@ -257,3 +257,63 @@ def batch_config(terrains: int = 128, clouds: int = 128,
         sc = BatchScene("tri" if is_tri else "point", items, pts[:a], pts[a:b], pts[b:], r, rays)
         (out_t if is_tri else out_c).append(sc)
     return BatchConfig(out_t, out_c, k)
+
+
+def _centroids(items: np.ndarray) -> np.ndarray:
+    if items.shape[1] == 9:
+        return items.reshape(-1, 3, 3).mean(axis=1)
+    return items[:, :3]
+
+
+def topology_edit(items: np.ndarray, fraction: float = 0.01, mode: str = "cluster",
+                  seed: int = 1):
+    """A GpuTopoEdit script over `items` (n, stride) touching `fraction` of them: a quarter
+    deleted, a quarter inserted at random new indices, a quarter appended, a quarter moved.
+    "cluster" draws every touched primitive from the ones nearest a random anchor (and new
+    primitives as shifted copies of them); "scatter" draws them uniformly.  Returns (new scene,
+    deleted old indices, inserted new indices, moved new indices), index arrays ascending."""
+    rng = np.random.default_rng(seed)
+    items = np.ascontiguousarray(items, np.float32)
+    n = items.shape[0]
+    q = max(1, int(round(fraction * n / 4)))
+    cen = _centroids(items)
+    if mode == "cluster":
+        anchor = cen[rng.integers(n)]
+        pool = np.argsort(((cen - anchor) ** 2).sum(axis=1), kind="stable")[: 4 * q]
+    elif mode == "scatter":
+        pool = np.arange(n)
+    else:
+        raise ValueError("mode must be 'cluster' or 'scatter'")
+    deleted = np.sort(rng.choice(pool, q, replace=False)).astype(np.int32)
+    ext = 0.05 * float(np.linalg.norm(cen.max(axis=0) - cen.min(axis=0))) / max(n, 1) ** (1 / 3)
+
+    def fresh(count):
+        src = items[rng.choice(pool, count)].copy()
+        shift = rng.normal(0.0, ext, (count, 3)).astype(np.float32)
+        if items.shape[1] == 9:
+            src += np.tile(shift, 3)
+        else:
+            src[:, :3] += shift
+        return src
+
+    survivors = np.delete(items, deleted, axis=0)
+    n_new = n - q + 2 * q
+    tail = n_new - q
+    inserted = np.sort(rng.choice(tail, q, replace=False)).astype(np.int32)
+    new = np.empty((n_new, items.shape[1]), np.float32)
+    keep = np.ones(tail, bool)
+    keep[inserted] = False
+    new[:tail][keep] = survivors
+    new[inserted] = fresh(q)
+    new[tail:] = fresh(q)
+    # moved: survivors from the pool, at their new indices
+    old_to_new = np.full(n, -1, np.int64)
+    old_to_new[np.setdiff1d(np.arange(n), deleted)] = np.flatnonzero(keep)
+    cand = old_to_new[np.setdiff1d(pool, deleted)]
+    moved = np.sort(rng.choice(cand, min(q, cand.size), replace=False)).astype(np.int32)
+    shift = rng.normal(0.0, ext, (moved.size, 3)).astype(np.float32)
+    if items.shape[1] == 9:
+        new[moved] += np.tile(shift, 3)
+    else:
+        new[moved, :3] += shift
+    return new, deleted, inserted, moved

@@ -386,9 +386,48 @@ def topology_timing(kind, items, builder, bins, queries_d, seed, timed_ms, rays_
                 raise RuntimeError(f"topology {mode}: edited tree answers differently")
             entry["depth"] = base.depth
             entry["fresh_depth"] = fresh.depth
+        if mode == "cluster":
+            entry["api"] = topology_api_wall(kind, items, new, dele, ins, mov, builder)
         out[f"{mode}_1pct"] = entry
         del base, fresh, arrays, ws
     return out
+
+
+def topology_api_wall(kind, items, new, dele, ins, mov, builder, rounds=4):
+    """Host wall time through the module (the C++ updateBVHGPU: it uploads only the edit
+    script and the primitives it brings, and reuses its arrays from the previous edit) in
+    steady state -- one object takes `rounds` further 1% edits of the same kind after the first
+    (which allocates), the later ones timed -- against constructing the object from the whole
+    edited scene (conversion, allocation, upload, build).  Medians."""
+    import time
+
+    import torch
+
+    import quarry
+    from quarry import workloads as w
+
+    wrap = (lambda a: a.reshape(-1, 3, 3)) if kind == "tri" else (lambda a: a)
+    make = {"tri": lambda a: quarry.Scene(wrap(a), builder=builder),
+            "point": lambda a: quarry.PointCloud(a, builder=builder)}[kind]
+    obj = make(items)
+    obj.update_topology(wrap(new), deleted=dele, moved=mov, inserted=ins)
+    cur = new
+    upd, reb, full = [], [], 0
+    for r in range(rounds):
+        nxt, d2, i2, m2 = w.topology_edit(cur, 0.01, "cluster", 100 + r)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        tm = obj.update_topology(wrap(nxt), deleted=d2, moved=m2, inserted=i2)
+        upd.append((time.perf_counter() - t0) * 1e3)
+        full += int(bool(tm["full_rebuild"]))
+        t0 = time.perf_counter()
+        fresh = make(nxt)
+        reb.append((time.perf_counter() - t0) * 1e3)
+        del fresh
+        cur = nxt
+    u, r = float(np.median(upd[1:])), float(np.median(reb[1:]))
+    return {"update_wall_ms": round(u, 3), "rebuild_wall_ms": round(r, 3), "ratio": round(u / r, 3),
+            "full_rebuilds": full, "rounds": rounds, "timed": "rounds 2..n, cluster 1% each"}
 
 
 # ---------------------------------------------------------------------------------------

@@ -828,7 +828,7 @@ __global__ __launch_bounds__(kBlock) void k_block_build(const Task* __restrict__
                                                        const float4* __restrict__ plo,
                                                        const float4* __restrict__ phi, Node* nodes,
                                                        BNode* bn, int* parent, int n, int bins,
-                                                       int* __restrict__ err) {
+                                                       int* __restrict__ err, int skip_small = 0) {
     extern __shared__ float4 smem[];
     float4* sc = smem;                                      // centroids   [kBlockRange]
     float4* slo = sc + kBlockRange;                         // box lo      [kBlockRange]
@@ -856,6 +856,7 @@ __global__ __launch_bounds__(kBlock) void k_block_build(const Task* __restrict__
         const Task tk = tasks[ti];
         const int count = tk.end - tk.begin;
         if (tk.node < 0) continue;  // a forest slot with nothing to build (0 or 1 primitive)
+        if (skip_small && count <= kWarpRange) continue;  // built by k_warp_forest
         if (count < 2 || count > kBlockRange) {
             if (threadIdx.x == 0) atomicAdd(err, 1);
             continue;
@@ -1032,6 +1033,27 @@ __global__ __launch_bounds__(kBlock) void k_block_build(const Task* __restrict__
         __syncthreads();
         for (int i = threadIdx.x; i < count; i += kBlock) order[tk.begin + i] = sid[perm[i]];
         __syncthreads();
+    }
+}
+
+// Forest tasks of 2..32 primitives, one warp each (warp_build over the global arrays: `order`
+// plays the block tier's position -> load index map, leaf slots start at the task's begin).
+__global__ __launch_bounds__(kBlock) void k_warp_forest(const Task* __restrict__ tasks, int ntask,
+                                                       const int* __restrict__ id_base,
+                                                       int* __restrict__ order,
+                                                       const float4* __restrict__ cen,
+                                                       const float4* __restrict__ plo,
+                                                       const float4* __restrict__ phi, Node* nodes,
+                                                       BNode* bn, int* parent, int n) {
+    __shared__ int scratch[kBlock / 32][32];
+    const int w = (blockIdx.x * kBlock + threadIdx.x) >> 5;
+    const int nw = (gridDim.x * kBlock) >> 5;
+    for (int ti = w; ti < ntask; ti += nw) {
+        const Task tk = tasks[ti];
+        const int count = tk.end - tk.begin;
+        if (tk.node < 0 || count < 2 || count > kWarpRange) continue;
+        warp_build(order, cen, plo, phi, tk.begin, count, tk.node, tk.depth, id_base[ti], nodes, bn,
+                   parent, n, 0, scratch[threadIdx.x >> 5]);
     }
 }
 
@@ -1235,17 +1257,23 @@ size_t sah_ws_bytes(int n) {
     return c.used;
 }
 
-int sah_forest(const int4* tasks, int ntask, const int* id_base, int* order, const float4* cen,
-               const float4* plo, const float4* phi, qk_tree* t, int bins, int* err,
-               cudaStream_t s) {
+int sah_forest(const int4* tasks, int ntask, int max_count, const int* id_base, int* order,
+               const float4* cen, const float4* plo, const float4* phi, qk_tree* t, int bins,
+               int* err, cudaStream_t s) {
     static_assert(sizeof(Task) == sizeof(int4), "forest tasks are {begin, end, node, depth}");
     if (bins < 4 || bins > kMaxBins) return fail(QK_ERR_INVALID, "sah_bins must be in [4, 64]");
     if (ntask <= 0) return QK_OK;
-    cudaFuncSetAttribute(k_block_build, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         static_cast<int>(block_smem(kMaxBins)));
-    k_block_build<<<min(ntask, 148 * 4), kBlock, block_smem(bins), s>>>(
-        reinterpret_cast<const Task*>(tasks), ntask, id_base, order, cen, plo, phi,
-        static_cast<Node*>(t->nodes), static_cast<BNode*>(t->bnodes), t->parent, t->n, bins, err);
+    const Task* tk = reinterpret_cast<const Task*>(tasks);
+    Node* nodes = static_cast<Node*>(t->nodes);
+    BNode* bn = static_cast<BNode*>(t->bnodes);
+    k_warp_forest<<<min(blocks_for(static_cast<long long>(ntask) * 32), 148 * 8), kBlock, 0, s>>>(
+        tk, ntask, id_base, order, cen, plo, phi, nodes, bn, t->parent, t->n);
+    if (max_count > kWarpRange) {
+        cudaFuncSetAttribute(k_block_build, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(block_smem(kMaxBins)));
+        k_block_build<<<min(ntask, 148 * 4), kBlock, block_smem(bins), s>>>(
+            tk, ntask, id_base, order, cen, plo, phi, nodes, bn, t->parent, t->n, bins, err, 1);
+    }
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? QK_OK : cuda_status(e, "SAH forest");
 }

@@ -5,7 +5,8 @@
 //
 // Every subtree of the engine's trees covers a contiguous run of leaf slots (LBVH and SAH
 // both emit them that way, and this pass keeps it so).  Plan, one host synchronisation:
-//   * a bottom-up pass records (first slot, leaf count) of every old internal node;
+//   * every old internal node's (first slot, leaf count) comes from its leftmost and rightmost
+//     leaves;
 //   * a cut is a maximal subtree of at most S leaves (its parent holds more), so the cuts
 //     partition the leaves.  A deleted leaf rebuilds its cut.  A new primitive descends from
 //     the root toward the child whose box grows least and joins the cut it reaches: new
@@ -56,7 +57,6 @@ struct TopoWs {
     Header* h;
     int* del_flag;     // n_old: old scene index deleted
     int2* range;       // n_old - 1: (first slot, leaves) of every old internal node
-    int* visit;        // n_old - 1: bottom-up arrival counters
     int* wslot;        // n_old + 1: slot weights, then new slot starts (exclusive scan)
     int* cut_mark;     // 2 n_old: 1 for a cut node; then the cut list index (scan)
     int* cut_extra;    // 2 n_old - 1: new primitives per cut node
@@ -89,7 +89,6 @@ TopoWs carve_topo(Carve& c, int kind, int n_old, int n_new, int n_extra) {
     w.h = c.take<Header>(1);
     w.del_flag = c.take<int>(n_old);
     w.range = c.take<int2>(n_old);
-    w.visit = c.take<int>(n_old);
     w.wslot = c.take<int>(n_old + 1);
     w.cut_mark = c.take<int>(2 * static_cast<size_t>(n_old));
     w.cut_extra = c.take<int>(2 * static_cast<size_t>(n_old));
@@ -236,27 +235,25 @@ __global__ __launch_bounds__(kBlock) void k_topo_check(EditDev e, int* __restric
     }
 }
 
-// (first slot, leaves) of every old internal node: the bottom-up arrival scheme of the box
-// pass, on ranges only
+// (first slot, leaves) of every old internal node.  Every subtree covers an ordered
+// contiguous run of slots (left child's run first), so its run is [leftmost leaf, rightmost
+// leaf]: two descents, no atomics.  k_topo_weights verifies the assumption node by node; a
+// run that comes out inverted is recorded as empty and reported.
 __global__ __launch_bounds__(kBlock) void k_topo_ranges(const Node* __restrict__ nodes,
-                                                       const int* __restrict__ parent,
-                                                       int* __restrict__ visit,
                                                        int2* __restrict__ range, int n,
                                                        TopoPlan* __restrict__ plan) {
-    const int k = blockIdx.x * kBlock + threadIdx.x;
-    if (k >= n) return;
-    int p = parent[n - 1 + k];
-    int guard = 0;
-    while (p >= 0 && guard++ < 4096) {
-        if (arrive_add(&visit[p], 1) == 0) return;
-        const int l = nodes[p].left, r = nodes[p].right;
-        const int2 a = l >= n - 1 ? make_int2(l - (n - 1), 1) : __ldcg(range + l);
-        const int2 b = r >= n - 1 ? make_int2(r - (n - 1), 1) : __ldcg(range + r);
-        const int first = min(a.x, b.x), cnt = a.y + b.y;
-        if (max(a.x + a.y, b.x + b.y) - first != cnt) atomicAdd(&plan->noncontig, 1);
-        range[p] = make_int2(first, cnt);
-        p = parent[p];
+    const int v = blockIdx.x * kBlock + threadIdx.x;
+    if (v >= n - 1) return;
+    int a = v, b = v;
+    for (int guard = 0; a < n - 1 && guard < 4096; ++guard) a = nodes[a].left;
+    for (int guard = 0; b < n - 1 && guard < 4096; ++guard) b = nodes[b].right;
+    const int first = a - (n - 1), last = b - (n - 1);
+    if (a < n - 1 || b < n - 1 || last < first) {
+        atomicAdd(&plan->noncontig, 1);
+        range[v] = make_int2(0, 0);
+        return;
     }
+    range[v] = make_int2(first, last - first + 1);
 }
 
 __global__ __launch_bounds__(kBlock) void k_topo_kept(const int* __restrict__ prim_ids,
@@ -375,6 +372,12 @@ __global__ __launch_bounds__(kBlock) void k_topo_weights(const Node* __restrict_
     if (v >= 2 * n - 1) return;
     const bool is_cut = cut_rank[v + 1] != cut_rank[v];
     const int m = new_count(range, xs, v, n);
+    if (v < n - 1) {
+        const int2 r = range[v];
+        const int2 rl = node_range(range, nodes[v].left, n);
+        const int2 rr = node_range(range, nodes[v].right, n);
+        if (rl.x != r.x || rr.x != rl.x + rl.y || rl.y + rr.y != r.y) atomicAdd(&plan->noncontig, 1);
+    }
     int wt = 0;
     if (is_cut) {
         wt = m > 1 ? m - 1 : 0;
@@ -608,15 +611,13 @@ int update_impl(const qk_tree* old_t, qk_tree* new_t, const qk_topo_edit* ed, in
 
     cudaMemsetAsync(w.plan, 0, sizeof(TopoPlan), s);
     cudaMemsetAsync(w.del_flag, 0, sizeof(int) * n_old, s);
-    cudaMemsetAsync(w.visit, 0, sizeof(int) * n_old, s);
     cudaMemsetAsync(w.cut_mark, 0, sizeof(int) * 2 * static_cast<size_t>(n_old), s);
     cudaMemsetAsync(w.cut_extra, 0, sizeof(int) * 2 * static_cast<size_t>(n_old), s);
     cudaMemsetAsync(w.cut_of_slot, 0xff, sizeof(int) * n_old, s);
     const int checks = std::max(std::max(e.n_del, e.n_ins), std::max(e.n_mov, 1));
     k_topo_check<<<blocks_for(checks), kBlock, 0, s>>>(e, w.del_flag, w.shifts, w.plan);
-    k_topo_ranges<<<blocks_for(n_old), kBlock, 0, s>>>(static_cast<const Node*>(old_t->nodes),
-                                                       old_t->parent, w.visit, w.range, n_old,
-                                                       w.plan);
+    k_topo_ranges<<<blocks_for(n_old - 1), kBlock, 0, s>>>(static_cast<const Node*>(old_t->nodes),
+                                                           w.range, n_old, w.plan);
     k_topo_kept<<<blocks_for(n_old + 1), kBlock, 0, s>>>(old_t->prim_ids, w.del_flag, n_old,
                                                          w.wslot);
     if (e.n_del > 0)
@@ -706,8 +707,8 @@ int update_impl(const qk_tree* old_t, qk_tree* new_t, const qk_topo_edit* ed, in
             w.st_items, w.st_id, w.cen, w.plo, w.phi, w.order, eerr);
     }
     if (plan.cuts > 0) {
-        const int st = sah_forest(w.tasks, plan.cuts, w.id_base, w.order, w.cen, w.plo, w.phi,
-                                  new_t, bins, eerr, s);
+        const int st = sah_forest(w.tasks, plan.cuts, plan.max_new, w.id_base, w.order, w.cen,
+                                  w.plo, w.phi, new_t, bins, eerr, s);
         if (st != QK_OK) return st;
         k_topo_cut_leaves<Ops><<<grid, kBlock, 0, s>>>(w.tasks, ncut_p, w.order, w.st_items,
                                                        w.st_id, *new_t, eerr);

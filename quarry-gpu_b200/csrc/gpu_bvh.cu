@@ -335,8 +335,11 @@ double updateImpl(GpuBVH& bvh, int kind, const std::vector<Item>& items, const G
     for (int k = 0; k < nMov; ++k) mv[k] = items[static_cast<size_t>(edit.moved[k])];
     const size_t wsBytes = alignUp(qk_update_workspace_bytes(kind, nOld, nNew, extra));
     if (im->updBytes < wsBytes + scriptBytes) {
+        // headroom for the next edits (scenes that grow a little per edit reuse it)
         devFree(im->upd);
-        im->updBytes = wsBytes + scriptBytes;
+        im->updBytes = alignUp(qk_update_workspace_bytes(kind, nOld + nOld / 8, nNew + nNew / 8,
+                                                         extra + extra / 8 + 64)) +
+                       scriptBytes + scriptBytes / 8;
         im->upd = devAlloc(im->updBytes, "topology workspace");
     }
     char* dScript = static_cast<char*>(im->upd) + wsBytes;
@@ -371,10 +374,9 @@ double updateImpl(GpuBVH& bvh, int kind, const std::vector<Item>& items, const G
     im->t = nt;
     for (int i = 0; i < kTreeArrays; ++i) std::swap(im->arrays[i], im->spare[i]);
     std::swap(im->cap, im->spareCap);
-    const size_t buildWs = qk_build_workspace_bytes(kind, nNew, im->builder);
-    if (buildWs > im->wsBytes) {
+    if (qk_build_workspace_bytes(kind, nNew, im->builder) > im->wsBytes) {
         devFree(im->ws);
-        im->wsBytes = buildWs;
+        im->wsBytes = qk_build_workspace_bytes(kind, nNew + nNew / 8, im->builder);
         im->ws = devAlloc(im->wsBytes, "build workspace");
     }
     syncPublic(bvh, im);

@@ -111,10 +111,69 @@ __global__ __launch_bounds__(kBlock) void k_emit(
     const float* __restrict__ items, int n, const uint32_t* __restrict__ codes,
     const uint32_t* __restrict__ ids, Node* __restrict__ nodes, float* __restrict__ sorted,
     int* __restrict__ prim_ids, int* __restrict__ slot_of, int* __restrict__ parent,
-    BNode* __restrict__ bnodes, float4* __restrict__ leaves, int* __restrict__ flags) {
+    BNode* __restrict__ bnodes, float4* __restrict__ leaves, int* __restrict__ flags,
+    int2* __restrict__ ranges) {
     const int k = blockIdx.x * kBlock + threadIdx.x;
     if (k >= n) return;
-    emit_slot<Ops>(items, n, codes, ids, nodes, sorted, prim_ids, slot_of, parent, bnodes, leaves, flags, k);
+    emit_slot<Ops>(items, n, codes, ids, nodes, sorted, prim_ids, slot_of, parent, bnodes, leaves,
+                   flags, k, ranges);
+}
+
+// (first slot, leaves) of every internal node of a tree whose subtrees cover ordered
+// contiguous slot runs (every builder here emits them so): leftmost and rightmost leaf.
+__global__ __launch_bounds__(kBlock) void k_ranges_descent(const Node* __restrict__ nodes, int n,
+                                                          int2* __restrict__ ranges) {
+    const int v = blockIdx.x * kBlock + threadIdx.x;
+    if (v >= n - 1) return;
+    int a = v, b = v;
+    for (int guard = 0; a < n - 1 && guard < 4096; ++guard) a = nodes[a].left;
+    for (int guard = 0; b < n - 1 && guard < 4096; ++guard) b = nodes[b].right;
+    const int first = a - (n - 1), last = b - (n - 1);
+    ranges[v] = make_int2(first, last >= first ? last - first + 1 : 0);
+}
+
+// Bottom-up boxes with known slot ranges.  Block b's threads start at the leaves of slots
+// [256 b, 256 b + 256).  A node whose whole range lies in those slots has both children
+// finished by this block, so its two arrivals meet in a shared-memory counter (indexed by the
+// node's split gap, the last slot of its left child, unique per internal node) behind block
+// fences; only nodes spanning blocks take the device-scope counter in flags[].
+__global__ __launch_bounds__(kBlock) void k_bottom_up_ranged(Node* __restrict__ nodes,
+                                                            BNode* __restrict__ bnodes,
+                                                            const int* __restrict__ parent,
+                                                            int* __restrict__ flags, int n,
+                                                            const int2* __restrict__ ranges) {
+    __shared__ int arrivals[kBlock];
+    const int base = blockIdx.x * kBlock;
+    arrivals[threadIdx.x] = 0;
+    __syncthreads();
+    const int k = base + threadIdx.x;
+    if (k >= n) return;
+    int c = n - 1 + k;
+    int2 rc = make_int2(k, 1);
+    int p = parent[c];
+    for (int guard = 0; p >= 0 && guard < 4096; ++guard) {
+        const int2 rp = ranges[p];
+        const bool local = rp.x >= base && rp.x + rp.y <= base + kBlock;
+        int old;
+        if (local) {
+            const int gap = nodes[p].left == c ? rc.x + rc.y - 1 : rc.x - 1;
+            __threadfence_block();
+            old = atomicAdd(&arrivals[gap - base], 1);
+            __threadfence_block();
+        } else {
+            old = arrive_add(&flags[p], 1);
+        }
+        if (old == 0) return;
+        if (local) {
+            finish_node_ranged<true>(nodes, bnodes, p, n, ranges);
+        } else {
+            finish_node_ranged<false>(nodes, bnodes, p, n, ranges);
+            flags[p] = 0;
+        }
+        c = p;
+        rc = rp;
+        p = parent[p];
+    }
 }
 
 // One thread per leaf climbs toward the root (climb in qk_build.cuh).
@@ -381,12 +440,15 @@ __global__ __launch_bounds__(kBlock) void k_check_wide(const Node* __restrict__ 
 }
 
 // Boxes (bottom-up), traversal nodes and depths of a tree whose links and leaves are set;
-// shared by the LBVH and SAH builders.  Reads the maximum depth back (syncs).
-int finish_tree(qk_tree* t, Header* h, int2* ranges, cudaStream_t s) {
+// shared by the LBVH and SAH builders and topology edits.  `ranges` (one int2 per internal
+// node) holds the slot ranges when ranges_ready (the LBVH emit writes them), else they are
+// derived first.  Reads the maximum depth back (syncs).
+int finish_tree(qk_tree* t, Header* h, int2* ranges, bool ranges_ready, cudaStream_t s) {
     const int n = t->n;
-    k_bottom_up<<<blocks_for(n), kBlock, 0, s>>>(static_cast<Node*>(t->nodes),
-                                                 static_cast<BNode*>(t->bnodes), t->parent,
-                                                 t->flags, n, ranges);
+    Node* nodes = static_cast<Node*>(t->nodes);
+    if (!ranges_ready) k_ranges_descent<<<blocks_for(n - 1), kBlock, 0, s>>>(nodes, n, ranges);
+    k_bottom_up_ranged<<<blocks_for(n), kBlock, 0, s>>>(nodes, static_cast<BNode*>(t->bnodes),
+                                                        t->parent, t->flags, n, ranges);
     cudaMemsetAsync(&h->max_depth, 0, sizeof(int), s);
     k_depth<<<blocks_for(2 * n - 1), kBlock, 0, s>>>(t->parent, 2 * n - 1, t->depth_arr, h);
     cudaError_t e = cudaGetLastError();
@@ -421,13 +483,14 @@ int build_lbvh(qk_tree* t, const void* items_v, void* ws, cudaStream_t s) {
     k_morton<Ops><<<blocks_for(n), kBlock, 0, s>>>(items, n, h, codes, idx);
     cudaError_t e = sort_pairs(codes, idx, codes_s, idx_s, n, 30, sort_ws, s);
     if (e != cudaSuccess) return cuda_status(e, "build sort");
+    int2* ranges = build_ranges(ws, t->kind, n, QK_BUILD_LBVH);
     k_emit<Ops><<<blocks_for(n), kBlock, 0, s>>>(items, n, codes_s, idx_s, nodes,
                                                   static_cast<float*>(t->items), t->prim_ids,
                                                   t->slot_of, t->parent, bn,
-                                                  static_cast<float4*>(t->leaves), t->flags);
+                                                  static_cast<float4*>(t->leaves), t->flags, ranges);
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_status(e, "build kernels");
-    return finish_tree(t, h, build_ranges(ws, t->kind, n, QK_BUILD_LBVH), s);
+    return finish_tree(t, h, ranges, true, s);
 }
 
 template <class Ops>
@@ -499,7 +562,7 @@ int validate_impl(const qk_tree* t, const void* items, int* err, void* ws, cudaS
 }  // namespace
 
 int finish_tree_boxes(qk_tree* t, Header* h, int2* ranges, cudaStream_t s) {
-    return finish_tree(t, h, ranges, s);
+    return finish_tree(t, h, ranges, false, s);
 }
 
 // workspace of the builders themselves; the bottom-up ranges follow it
@@ -542,7 +605,8 @@ int build_tree(qk_tree* t, int builder, int bins, const void* items, void* ws, s
         cudaMemsetAsync(t->flags, 0, sizeof(int) * static_cast<size_t>(t->n - 1), s);
         const int st = build_sah(t, bins, items, ws, s);
         if (st != QK_OK) return st;
-        return finish_tree(t, static_cast<Header*>(ws), build_ranges(ws, t->kind, t->n, QK_BUILD_SAH), s);
+        return finish_tree(t, static_cast<Header*>(ws), build_ranges(ws, t->kind, t->n, QK_BUILD_SAH),
+                           false, s);
     }
     switch (t->kind) {
         case kTri: return build_lbvh<TriOps>(t, items, ws, s);

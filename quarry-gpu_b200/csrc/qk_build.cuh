@@ -49,7 +49,8 @@ __device__ __forceinline__ void emit_slot(
     const float* __restrict__ items, int n, const uint32_t* __restrict__ codes,
     const uint32_t* __restrict__ ids, Node* __restrict__ nodes, float* __restrict__ sorted,
     int* __restrict__ prim_ids, int* __restrict__ slot_of, int* __restrict__ parent,
-    BNode* __restrict__ bnodes, float4* __restrict__ leaves, int* __restrict__ flags, int k) {
+    BNode* __restrict__ bnodes, float4* __restrict__ leaves, int* __restrict__ flags, int k,
+    int2* __restrict__ ranges = nullptr) {
     // leaf k
     const int src = static_cast<int>(ids[k]);
     float it[Ops::kFloats];
@@ -83,6 +84,7 @@ __device__ __forceinline__ void emit_slot(
     }
     const int j = k + l * dir;
     const int first = min(k, j), last = max(k, j);
+    if (ranges) ranges[k] = make_int2(first, last - first + 1);
     const int dnode = cpl(codes, ids, n, kk, j);
     const uint64_t kf = key64(codes, ids, first);
     int split = first;
@@ -143,6 +145,40 @@ __device__ __forceinline__ void finish_node(Node* __restrict__ nodes, BNode* __r
     }
     const Box a = load_box_cg(nodes + l);
     const Box b = load_box_cg(nodes + r);
+    Box u;
+    u.lo = f3(fmin_t(a.lo.x, b.lo.x), fmin_t(a.lo.y, b.lo.y), fmin_t(a.lo.z, b.lo.z));
+    u.hi = f3(fmax_t(a.hi.x, b.hi.x), fmax_t(a.hi.y, b.hi.y), fmax_t(a.hi.z, b.hi.z));
+    write_box(nodes + p, u);
+    BNode& bn = bnodes[p];
+    bn.v0 = make_float4(a.lo.x, a.lo.y, a.lo.z, a.hi.x);
+    bn.v1 = make_float4(a.hi.y, a.hi.z, b.lo.x, b.lo.y);
+    bn.v2 = make_float4(b.lo.z, b.hi.x, b.hi.y, b.hi.z);
+}
+
+__device__ __forceinline__ Box load_box_ca(const Node* nd) {
+    const float4* p = reinterpret_cast<const float4*>(nd);
+    const float4 a = __ldca(p), b = __ldca(p + 1);
+    Box bx;
+    bx.lo = f3(a.x, a.y, a.z);
+    bx.hi = f3(a.w, b.x, b.y);
+    return bx;
+}
+
+// Complete internal node p from its two final children when every internal node's slot range
+// is already known (`ranges`): box, traversal node and the children's small-subtree codes.
+// kLocal: both children were finished by threads of this block, whose writes a plain load
+// sees after the block fence; otherwise they are read from L2.
+template <bool kLocal>
+__device__ __forceinline__ void finish_node_ranged(Node* __restrict__ nodes,
+                                                   BNode* __restrict__ bnodes, int p, int n,
+                                                   const int2* __restrict__ ranges) {
+    const int l = nodes[p].left, r = nodes[p].right;
+    const int2 rl = l >= n - 1 ? make_int2(l - (n - 1), 1) : ranges[l];
+    const int2 rr = r >= n - 1 ? make_int2(r - (n - 1), 1) : ranges[r];
+    *reinterpret_cast<float2*>(&bnodes[p].v3.z) =
+        make_float2(__int_as_float(small_code(l, n, rl)), __int_as_float(small_code(r, n, rr)));
+    const Box a = kLocal ? load_box_ca(nodes + l) : load_box_cg(nodes + l);
+    const Box b = kLocal ? load_box_ca(nodes + r) : load_box_cg(nodes + r);
     Box u;
     u.lo = f3(fmin_t(a.lo.x, b.lo.x), fmin_t(a.lo.y, b.lo.y), fmin_t(a.lo.z, b.lo.z));
     u.hi = f3(fmax_t(a.hi.x, b.hi.x), fmax_t(a.hi.y, b.hi.y), fmax_t(a.hi.z, b.hi.z));

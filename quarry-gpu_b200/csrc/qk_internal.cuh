@@ -98,11 +98,11 @@ int build_sah(qk_tree* t, int bins, const void* items, void* ws, cudaStream_t s)
 // Forest of independent ranges for the SAH builder's lower tiers (qk_sah.cu): task i =
 // {begin, end, node, depth} over positions of `order` (indices into cen / plo / phi), its
 // internal nodes below `node` numbered from id_base[i]; node < 0 skips the task.  Leaf of
-// position p is n-1+p of t.  Ranges of 2..1024 primitives, at most max_count: those of up to
-// 32 take one warp each, larger ones one block each.
+// position p is n-1+p of t; tmp: partition scratch like `order`.  Ranges of 2..1024
+// primitives, at most max_count: those of up to 256 take one warp each, larger ones a block.
 int sah_forest(const int4* tasks, int ntask, int max_count, const int* id_base, int* order,
-               const float4* cen, const float4* plo, const float4* phi, qk_tree* t, int bins,
-               int* err, cudaStream_t s);
+               int* tmp, const float4* cen, const float4* plo, const float4* phi, qk_tree* t,
+               int bins, int* err, cudaStream_t s);
 // boxes, traversal nodes and depths of a tree whose links and leaves are set (syncs)
 int finish_tree_boxes(qk_tree* t, Header* h, int2* ranges, cudaStream_t s);
 // topology edits (qk_topo.cu)

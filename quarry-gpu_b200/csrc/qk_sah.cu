@@ -5,15 +5,17 @@
 // boxes, traversal nodes, 4-wide collapse, refit and validation are shared with the LBVH.
 // Three tiers, all deterministic (commutative atomics for bins, stable partitions, node ids
 // from prefix sums or from sequential per-subtree counters):
-//   global   ranges of more than kBlockRange primitives, level by level: chunks of 4096
+//   global   ranges of more than kTaskRange primitives, level by level: chunks of 4096
 //            primitives bin their centroids in shared memory (count + primitive box per bin,
 //            3 axes) and merge into per-range bins with ordered-uint atomics; one thread per
 //            range sweeps the bins for the cheapest area(L)*nL + area(R)*nR split; a stable
 //            partition by chunk-local block scans writes the new order.  Two host syncs per
 //            level.
-//   block    every range of at most kBlockRange primitives is handed to one thread block that
-//            gathers its centroids and boxes into shared memory and splits it with the same
-//            binned sweep until pieces reach 32 primitives; no global synchronisation.
+//   warp     every range of at most kTaskRange (256) primitives is handed to one warp
+//            (k_warp_tasks): binned SAH with warp-private bins down to 32 primitives
+//            (warp_piece_tree), then the exact sweep below; no block barriers, no global
+//            synchronisation.  The block tier (k_block_build: one thread block per range of up
+//            to 1024 in shared memory) now only builds forest tasks above 256 (topology edits).
 //   warp     pieces of at most 32 primitives are finished by one warp each with an exact
 //            sweep: for every axis the lanes sort by centroid (bitonic, ties by position), scan
 //            prefix and suffix boxes, and evaluate every split position.
@@ -26,7 +28,8 @@ namespace qk {
 namespace {
 
 constexpr int kChunk = 4096;       // primitives binned per block at the global tier
-constexpr int kBlockRange = 1024;  // largest range built by one block
+constexpr int kBlockRange = 1024;  // largest range built by one block (forest tasks)
+constexpr int kTaskRange = 256;    // largest range the global tier hands to one warp
 constexpr int kWarpRange = 32;     // largest range finished by one warp
 constexpr int kMaxBins = 64;
 constexpr int kMaxDepth = 62;
@@ -502,8 +505,8 @@ __global__ __launch_bounds__(1024) void k_level_assign(Level L, int ntask, Task*
         }
         int cnt[3];
         cnt[0] = t < ntask ? (lc >= 2) + (rc >= 2) : 0;                           // internal ids
-        cnt[1] = t < ntask ? (lc > kBlockRange) + (rc > kBlockRange) : 0;         // big tasks
-        cnt[2] = t < ntask ? (lc >= 2 && lc <= kBlockRange) + (rc >= 2 && rc <= kBlockRange) : 0;
+        cnt[1] = t < ntask ? (lc > kTaskRange) + (rc > kTaskRange) : 0;           // big tasks
+        cnt[2] = t < ntask ? (lc >= 2 && lc <= kTaskRange) + (rc >= 2 && rc <= kTaskRange) : 0;
         int ex[3];
         for (int k = 0; k < 3; ++k) {
             int v = cnt[k];
@@ -532,9 +535,9 @@ __global__ __launch_bounds__(1024) void k_level_assign(Level L, int ntask, Task*
             const int rid = rc >= 2 ? base_id + ex[0] + (lc >= 2) : n - 1 + tk.begin + lc;
             link(nodes, bn, parent, tk.node, lid, rid, n);
             int bi = base_big + ex[1], ki = base_blk + ex[2];
-            if (lc > kBlockRange) next[bi++] = Task{tk.begin, tk.begin + lc, lid, tk.depth + 1};
+            if (lc > kTaskRange) next[bi++] = Task{tk.begin, tk.begin + lc, lid, tk.depth + 1};
             else if (lc >= 2) blocks[ki++] = Task{tk.begin, tk.begin + lc, lid, tk.depth + 1};
-            if (rc > kBlockRange) next[bi] = Task{tk.begin + lc, tk.end, rid, tk.depth + 1};
+            if (rc > kTaskRange) next[bi] = Task{tk.begin + lc, tk.end, rid, tk.depth + 1};
             else if (rc >= 2) blocks[ki] = Task{tk.begin + lc, tk.end, rid, tk.depth + 1};
         }
         __syncthreads();
@@ -856,7 +859,7 @@ __global__ __launch_bounds__(kBlock) void k_block_build(const Task* __restrict__
         const Task tk = tasks[ti];
         const int count = tk.end - tk.begin;
         if (tk.node < 0) continue;  // a forest slot with nothing to build (0 or 1 primitive)
-        if (skip_small && count <= kWarpRange) continue;  // built by k_warp_forest
+        if (skip_small && count <= kTaskRange) continue;  // built by k_warp_tasks
         if (count < 2 || count > kBlockRange) {
             if (threadIdx.x == 0) atomicAdd(err, 1);
             continue;
@@ -1036,25 +1039,49 @@ __global__ __launch_bounds__(kBlock) void k_block_build(const Task* __restrict__
     }
 }
 
-// Forest tasks of 2..32 primitives, one warp each (warp_build over the global arrays: `order`
-// plays the block tier's position -> load index map, leaf slots start at the task's begin).
-__global__ __launch_bounds__(kBlock) void k_warp_forest(const Task* __restrict__ tasks, int ntask,
-                                                       const int* __restrict__ id_base,
-                                                       int* __restrict__ order,
-                                                       const float4* __restrict__ cen,
-                                                       const float4* __restrict__ plo,
-                                                       const float4* __restrict__ phi, Node* nodes,
-                                                       BNode* bn, int* parent, int n) {
-    __shared__ int scratch[kBlock / 32][32];
+// Tasks of 2..kTaskRange primitives, one warp each, over global arrays: `order` maps positions
+// to primitive indices (cen / plo / phi), `tmp` is partition scratch of the same size.  A task
+// of up to 32 goes straight to warp_build, a larger one through warp_piece_tree; node ids come
+// from the task's reserved range, so the tree does not depend on scheduling.  No block-wide
+// barriers: each warp works on its own task.
+__global__ __launch_bounds__(kBlock) void k_warp_tasks(const Task* __restrict__ tasks, int ntask,
+                                                      const int* __restrict__ id_base,
+                                                      int* __restrict__ order, int* __restrict__ tmp,
+                                                      const float4* __restrict__ cen,
+                                                      const float4* __restrict__ plo,
+                                                      const float4* __restrict__ phi, Node* nodes,
+                                                      BNode* bn, int* parent, int n, int bins,
+                                                      int* __restrict__ err) {
+    extern __shared__ unsigned wsm[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned* wb = wsm + static_cast<size_t>(warp) * 3 * bins * kBinWords;
+    Piece* wstk_all = reinterpret_cast<Piece*>(wsm + static_cast<size_t>(kBlock / 32) * 3 * bins * kBinWords);
+    Piece* wstk = wstk_all + warp * kWarpStack;
+    int* scratch = reinterpret_cast<int*>(wstk_all + (kBlock / 32) * kWarpStack) + warp * 32;
     const int w = (blockIdx.x * kBlock + threadIdx.x) >> 5;
     const int nw = (gridDim.x * kBlock) >> 5;
     for (int ti = w; ti < ntask; ti += nw) {
         const Task tk = tasks[ti];
         const int count = tk.end - tk.begin;
-        if (tk.node < 0 || count < 2 || count > kWarpRange) continue;
-        warp_build(order, cen, plo, phi, tk.begin, count, tk.node, tk.depth, id_base[ti], nodes, bn,
-                   parent, n, 0, scratch[threadIdx.x >> 5]);
+        if (tk.node < 0 || count < 2 || count > kTaskRange) {
+            if (tk.node >= 0 && count > kTaskRange && lane == 0) atomicAdd(err, 1);
+            continue;
+        }
+        if (count <= kWarpRange) {
+            warp_build(order, cen, plo, phi, tk.begin, count, tk.node, tk.depth, id_base[ti], nodes,
+                       bn, parent, n, 0, scratch);
+        } else {
+            warp_piece_tree(Piece{tk.begin, count, tk.node, tk.depth, id_base[ti]}, order, tmp, cen,
+                            plo, phi, wb, wstk, scratch, bins, nodes, bn, parent, n, 0, err);
+        }
     }
+}
+
+// dynamic shared memory of k_warp_tasks: every warp's bins, piece stack and scratch
+size_t warp_tasks_smem(int bins) {
+    return static_cast<size_t>(kBlock / 32) *
+           (3 * static_cast<size_t>(bins) * kBinWords * sizeof(unsigned) + kWarpStack * sizeof(Piece) +
+            32 * sizeof(int));
 }
 
 constexpr size_t kBlockSmemBase = 3 * kBlockRange * sizeof(float4) + 3 * kBlockRange * sizeof(int);
@@ -1121,7 +1148,7 @@ struct SahWs {
 };
 
 SahWs carve_sah(Carve& c, int n) {
-    const int max_big = n / (kBlockRange + 1) + 2;
+    const int max_big = n / (kTaskRange + 1) + 2;
     const int max_chunks = n / kChunk + max_big + 2;
     const int max_blocks = n / 2 + 2;
     SahWs w;
@@ -1166,7 +1193,7 @@ int build_sah_impl(qk_tree* t, int bins, const void* items_v, void* ws, cudaStre
     int init[8] = {0, 0, 0, 1, 0, 0, 0, 0};
     Task root{0, n, 0, 0};
     int nbig = 0, nblk = 0;
-    if (n > kBlockRange) {
+    if (n > kTaskRange) {
         cudaMemcpyAsync(w.tasksA, &root, sizeof(Task), cudaMemcpyHostToDevice, s);
         nbig = 1;
     } else {
@@ -1223,13 +1250,10 @@ int build_sah_impl(qk_tree* t, int bins, const void* items_v, void* ws, cudaStre
             return fail(QK_ERR_INVALID, "SAH node accounting: %d + %d != %d", tail[1], tail[0], n - 1);
         }
         k_add_base<<<blocks_for(nblk), kBlock, 0, s>>>(w.id_base, nblk, w.L.counters);
-        const int grid = min(nblk, 148 * 4);
-        const size_t smem = block_smem(bins);
-        cudaFuncSetAttribute(k_block_build, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(block_smem(kMaxBins)));
-        k_block_build<<<grid, kBlock, smem, s>>>(w.blocks, nblk, w.id_base, ord, w.cen,
-                                                       w.plo, w.phi, nodes, bn, t->parent, n, bins,
-                                                       err);
+        // every range of at most kTaskRange primitives: one warp each (`alt` is free scratch)
+        k_warp_tasks<<<min(blocks_for(static_cast<long long>(nblk) * 32), 148 * 8), kBlock,
+                       warp_tasks_smem(bins), s>>>(w.blocks, nblk, w.id_base, ord, alt, w.cen,
+                                                   w.plo, w.phi, nodes, bn, t->parent, n, bins, err);
     } else {
         int base = 0;
         cudaMemcpyAsync(&base, w.L.counters + 3, sizeof(int), cudaMemcpyDeviceToHost, s);
@@ -1258,17 +1282,18 @@ size_t sah_ws_bytes(int n) {
 }
 
 int sah_forest(const int4* tasks, int ntask, int max_count, const int* id_base, int* order,
-               const float4* cen, const float4* plo, const float4* phi, qk_tree* t, int bins,
-               int* err, cudaStream_t s) {
+               int* tmp, const float4* cen, const float4* plo, const float4* phi, qk_tree* t,
+               int bins, int* err, cudaStream_t s) {
     static_assert(sizeof(Task) == sizeof(int4), "forest tasks are {begin, end, node, depth}");
     if (bins < 4 || bins > kMaxBins) return fail(QK_ERR_INVALID, "sah_bins must be in [4, 64]");
     if (ntask <= 0) return QK_OK;
     const Task* tk = reinterpret_cast<const Task*>(tasks);
     Node* nodes = static_cast<Node*>(t->nodes);
     BNode* bn = static_cast<BNode*>(t->bnodes);
-    k_warp_forest<<<min(blocks_for(static_cast<long long>(ntask) * 32), 148 * 8), kBlock, 0, s>>>(
-        tk, ntask, id_base, order, cen, plo, phi, nodes, bn, t->parent, t->n);
-    if (max_count > kWarpRange) {
+    k_warp_tasks<<<min(blocks_for(static_cast<long long>(ntask) * 32), 148 * 8), kBlock,
+                   warp_tasks_smem(bins), s>>>(tk, ntask, id_base, order, tmp, cen, plo, phi, nodes,
+                                               bn, t->parent, t->n, bins, err);
+    if (max_count > kTaskRange) {
         cudaFuncSetAttribute(k_block_build, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              static_cast<int>(block_smem(kMaxBins)));
         k_block_build<<<min(ntask, 148 * 4), kBlock, block_smem(bins), s>>>(

@@ -76,6 +76,7 @@ struct TopoWs {
     float* st_items;   // n_new staged records
     int* st_id;        // n_new staged new scene indices
     int* order;        // n_new
+    int* tmp;          // n_new: partition scratch of the forest builders
     int2* new_range;   // n_new - 1: bottom-up ranges of the new tree
     void* sort_ws;
     void* scan_ws;
@@ -108,6 +109,7 @@ TopoWs carve_topo(Carve& c, int kind, int n_old, int n_new, int n_extra) {
     w.st_items = c.take<float>(static_cast<size_t>(n_new) * fl);
     w.st_id = c.take<int>(n_new);
     w.order = c.take<int>(n_new);
+    w.tmp = c.take<int>(n_new);
     w.new_range = c.take<int2>(n_new);
     w.sort_ws = c.take<char>(sort_ws_bytes(n_extra + 1));
     w.scan_ws = c.take<char>(scan_ws_bytes(2 * n_old + 1));
@@ -707,8 +709,8 @@ int update_impl(const qk_tree* old_t, qk_tree* new_t, const qk_topo_edit* ed, in
             w.st_items, w.st_id, w.cen, w.plo, w.phi, w.order, eerr);
     }
     if (plan.cuts > 0) {
-        const int st = sah_forest(w.tasks, plan.cuts, plan.max_new, w.id_base, w.order, w.cen,
-                                  w.plo, w.phi, new_t, bins, eerr, s);
+        const int st = sah_forest(w.tasks, plan.cuts, plan.max_new, w.id_base, w.order, w.tmp,
+                                  w.cen, w.plo, w.phi, new_t, bins, eerr, s);
         if (st != QK_OK) return st;
         k_topo_cut_leaves<Ops><<<grid, kBlock, 0, s>>>(w.tasks, ncut_p, w.order, w.st_items,
                                                        w.st_id, *new_t, eerr);

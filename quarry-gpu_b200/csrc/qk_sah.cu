@@ -588,9 +588,9 @@ __device__ void warp_build(int* perm, const float4* sc, const float4* slo, const
     for (int a = 0; a < 3; ++a) {
         const float key = mine ? (a == 0 ? cc.x : (a == 1 ? cc.y : cc.z)) : kInf;
         int rank = 0;
-        for (int j = 0; j < kWarpRange; ++j) {
+        for (int j = 0; j < c; ++j) {  // c is warp-uniform: only the piece's lanes are ranked
             const float kj = __shfl_sync(0xffffffffu, key, j);
-            if (j < c && (kj < key || (kj == key && j < lane))) ++rank;
+            if (kj < key || (kj == key && j < lane)) ++rank;
         }
         if (mine) scratch[rank] = lane;
         __syncwarp();
@@ -626,7 +626,8 @@ __device__ void warp_build(int* perm, const float4* sc, const float4* slo, const
                 hi = ehi;
             }
             float3 plo = lo, phi = hi, qlo = lo, qhi = hi;
-            for (int o = 1; o < 32; o <<= 1) {
+            // scans over the node's m positions only (lanes >= m hold empty boxes): log2(m) steps
+            for (int o = 1; o < m; o <<= 1) {
                 const float3 ulo = f3(__shfl_up_sync(0xffffffffu, plo.x, o), __shfl_up_sync(0xffffffffu, plo.y, o), __shfl_up_sync(0xffffffffu, plo.z, o));
                 const float3 uhi = f3(__shfl_up_sync(0xffffffffu, phi.x, o), __shfl_up_sync(0xffffffffu, phi.y, o), __shfl_up_sync(0xffffffffu, phi.z, o));
                 const float3 dlo = f3(__shfl_down_sync(0xffffffffu, qlo.x, o), __shfl_down_sync(0xffffffffu, qlo.y, o), __shfl_down_sync(0xffffffffu, qlo.z, o));
@@ -651,7 +652,9 @@ __device__ void warp_build(int* perm, const float4* sc, const float4* slo, const
             }
             float bc = cost;
             int bk = kl;
-            for (int o = 16; o > 0; o >>= 1) {
+            int span = 1;  // lanes holding candidates: below m, rounded up to a power of two
+            while (span < m) span <<= 1;
+            for (int o = span >> 1; o > 0; o >>= 1) {
                 const float oc = __shfl_xor_sync(0xffffffffu, bc, o);
                 const int ok = __shfl_xor_sync(0xffffffffu, bk, o);
                 if (oc < bc || (oc == bc && ok < bk)) {
@@ -659,6 +662,9 @@ __device__ void warp_build(int* perm, const float4* sc, const float4* slo, const
                     bk = ok;
                 }
             }
+            // lanes [0, span) hold the winner; every lane takes it from lane 0
+            bc = __shfl_sync(0xffffffffu, bc, 0);
+            bk = __shfl_sync(0xffffffffu, bk, 0);
             if (bc < best) {
                 best = bc;
                 best_axis = a;

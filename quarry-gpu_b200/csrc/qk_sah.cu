@@ -1050,7 +1050,7 @@ __global__ __launch_bounds__(kBlock) void k_block_build(const Task* __restrict__
 // of up to 32 goes straight to warp_build, a larger one through warp_piece_tree; node ids come
 // from the task's reserved range, so the tree does not depend on scheduling.  No block-wide
 // barriers: each warp works on its own task.
-__global__ __launch_bounds__(kBlock) void k_warp_tasks(const Task* __restrict__ tasks, int ntask,
+__global__ __launch_bounds__(kBlock, 4) void k_warp_tasks(const Task* __restrict__ tasks, int ntask,
                                                       const int* __restrict__ id_base,
                                                       int* __restrict__ order, int* __restrict__ tmp,
                                                       const float4* __restrict__ cen,

@@ -203,21 +203,55 @@ __global__ __launch_bounds__(kBlock) void k_level_bins(Level L, const int* __res
         clo[a] = unord_f(L.cb[6 * t + a]);
         chi[a] = unord_f(L.cb[6 * t + 3 + a]);
     }
-    for (int i = b + threadIdx.x; i < e; i += kBlock) {
+    // Each thread bins a contiguous run of positions.  Partitioned ranges keep nearby
+    // primitives together, so consecutive positions mostly fall in the same bin: the thread
+    // accumulates a bin's count and box in registers and issues the shared-memory atomics only
+    // when the bin changes (count, min and max are exact in any grouping).
+    const int per = (e - b + kBlock - 1) / kBlock;
+    const int i0 = b + threadIdx.x * per, i1 = min(i0 + per, e);
+    int cur[3] = {-1, -1, -1};
+    unsigned acc[3][kBinWords];
+    auto flush = [&](int a) {
+        unsigned* w = sb + (a * bins + cur[a]) * kBinWords;
+        atomicAdd(&w[0], acc[a][0]);
+        atomicMin(&w[1], acc[a][1]);
+        atomicMin(&w[2], acc[a][2]);
+        atomicMin(&w[3], acc[a][3]);
+        atomicMax(&w[4], acc[a][4]);
+        atomicMax(&w[5], acc[a][5]);
+        atomicMax(&w[6], acc[a][6]);
+    };
+    for (int i = i0; i < i1; ++i) {
         const int p = order[i];
         const float4 cc = cen[p], lo = plo[p], hi = phi[p];
         const float cv[3] = {cc.x, cc.y, cc.z};
+#pragma unroll
         for (int a = 0; a < 3; ++a) {
-            unsigned* w = sb + (a * bins + bin_of(cv[a], clo[a], chi[a], bins)) * kBinWords;
-            atomicAdd(&w[0], 1u);
-            atomicMin(&w[1], ord_f(lo.x));
-            atomicMin(&w[2], ord_f(lo.y));
-            atomicMin(&w[3], ord_f(lo.z));
-            atomicMax(&w[4], ord_f(hi.x));
-            atomicMax(&w[5], ord_f(hi.y));
-            atomicMax(&w[6], ord_f(hi.z));
+            const int bin = bin_of(cv[a], clo[a], chi[a], bins);
+            if (bin != cur[a]) {
+                if (cur[a] >= 0) flush(a);
+                cur[a] = bin;
+                acc[a][0] = 1u;
+                acc[a][1] = ord_f(lo.x);
+                acc[a][2] = ord_f(lo.y);
+                acc[a][3] = ord_f(lo.z);
+                acc[a][4] = ord_f(hi.x);
+                acc[a][5] = ord_f(hi.y);
+                acc[a][6] = ord_f(hi.z);
+            } else {
+                acc[a][0] += 1u;
+                acc[a][1] = min(acc[a][1], ord_f(lo.x));
+                acc[a][2] = min(acc[a][2], ord_f(lo.y));
+                acc[a][3] = min(acc[a][3], ord_f(lo.z));
+                acc[a][4] = max(acc[a][4], ord_f(hi.x));
+                acc[a][5] = max(acc[a][5], ord_f(hi.y));
+                acc[a][6] = max(acc[a][6], ord_f(hi.z));
+            }
         }
     }
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+        if (cur[a] >= 0) flush(a);
     __syncthreads();
     unsigned* B = L.bins + static_cast<size_t>(t) * 3 * kMaxBins * kBinWords;
     for (int j = threadIdx.x; j < 3 * bins * kBinWords; j += kBlock) {

@@ -456,9 +456,12 @@ def points_arm(args, world, rank, local):
         pts = w.point_cloud(kind, n, seed)
         lo, hi = pts.min(axis=0), pts.max(axis=0)
         q = w.uniform_points(nq, lo, hi, seed, 13)
-        tree = capi.DeviceTree("point", pts)
-        tree.build_wide()
-        clouds[kind] = {"pts": pts, "q": q, "q_d": capi.to_device(q, np.float32), "tree": tree}
+        trees = {}
+        for bname, builder, bins in (("lbvh", "lbvh", 32), ("sah8", "sah", 8), ("sah32", "sah", 32)):
+            trees[bname] = capi.DeviceTree("point", pts, builder=builder, sah_bins=bins)
+            trees[bname].build_wide()
+        clouds[kind] = {"pts": pts, "q": q, "q_d": capi.to_device(q, np.float32),
+                        "tree": trees["lbvh"], "trees": trees}
         if args.dump and rank == 0:
             from quarry import dumps
 
@@ -480,42 +483,55 @@ def points_arm(args, world, rank, local):
         return ts
 
     outs = {}
+    ops = ("closest", "knn", "radius")
 
-    def step(flags):
-        for kind, c in clouds.items():
-            t = c["tree"]
-            outs[(kind, "closest")] = t.closest(c["q_d"], flags)
-            outs[(kind, "knn")] = t.knn(c["q_d"], k, flags)
-            outs[(kind, "radius")] = t.radius(c["q_d"], r, flags)
+    def run(kind, op, tree, flags):
+        c = clouds[kind]
+        if op == "closest":
+            outs[(kind, op)] = tree.closest(c["q_d"], flags)
+        elif op == "knn":
+            outs[(kind, op)] = tree.knn(c["q_d"], k, flags)
+        else:
+            outs[(kind, op)] = tree.radius(c["q_d"], r, flags)
 
-    def snapshot():
-        return {key: ((v[0].cpu().numpy(), v[1].cpu().numpy()) if isinstance(v, tuple)
-                      else v.cpu().numpy()) for key, v in outs.items()}
+    def snapshot(key):
+        v = outs[key]
+        return (v[0].cpu().numpy(), v[1].cpu().numpy()) if isinstance(v, tuple) else v.cpu().numpy()
 
+    def same(a, b):
+        return (np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+                if isinstance(a, tuple) else np.array_equal(a, b))
+
+    # Every (cloud, operation) takes its fastest (tree, schedule): the sphere shell's queries
+    # have a heavy tail that the warp-per-query kernels spread out, the uniform cloud's do not.
+    # All candidates must return the bits of the LBVH thread-per-query run.
     variants = {"bin": 0, "bin_morton": capi.QK_ORDER_MORTON, "wide": capi.QK_WIDE,
                 "wide_morton": capi.QK_WIDE | capi.QK_ORDER_MORTON,
                 "split": capi.QK_TUNE_SPLIT, "split_morton": capi.QK_TUNE_SPLIT | capi.QK_ORDER_MORTON,
                 "leaf4": capi.QK_TUNE_LEAF4, "leaf4_morton": capi.QK_TUNE_LEAF4 | capi.QK_ORDER_MORTON}
-    step(0)
-    base = snapshot()
-    vms = {}
-    for name, f in variants.items():
-        step(f)
-        got = snapshot()
-        for key in base:
-            a, b = base[key], got[key]
-            same = (np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
-                    if isinstance(a, tuple) else np.array_equal(a, b))
-            if not same:
-                raise RuntimeError(f"variant {name} differs on {key}")
-        vms[name] = float(np.median(timed(lambda: step(f), 5)))
-    best = min(vms, key=vms.get)
-    flags = variants[best]
+    vms, plan = {}, {}
+    for kind, c in clouds.items():
+        for op in ops:
+            run(kind, op, c["trees"]["lbvh"], 0)
+            base = snapshot((kind, op))
+            for bname, tree in c["trees"].items():
+                for vname, f in variants.items():
+                    run(kind, op, tree, f)
+                    if not same(base, snapshot((kind, op))):
+                        raise RuntimeError(f"{kind} {op}: {bname}/{vname} differs")
+                    t = float(np.median(timed(lambda: run(kind, op, tree, f), 5)))
+                    vms[f"{kind}/{op}/{bname}/{vname}"] = t
+                    if (kind, op) not in plan or t < plan[(kind, op)][2]:
+                        plan[(kind, op)] = (bname, vname, t)
+
+    def step():
+        for (kind, op), (bname, vname, _) in plan.items():
+            run(kind, op, clouds[kind]["trees"][bname], variants[vname])
 
     barrier(world)
     torch.cuda.synchronize()
     with Clocks(local) as clk:
-        ts = timed(lambda: step(flags), args.steps, args.warmup)
+        ts = timed(step, args.steps, args.warmup)
     clocks = clk.summary()
     ms = max_over_ranks(world, float(np.mean(ts)))
     queries = 2 * 3 * nq
@@ -523,16 +539,11 @@ def points_arm(args, world, rank, local):
 
     # per-operation kernel times and the canonical visit counts (binary LBVH) for the roofline
     per_op = {}
-    for op in ("closest", "knn", "radius"):
+    for op in ops:
         def one(op=op):
-            for c in clouds.values():
-                t = c["tree"]
-                if op == "closest":
-                    t.closest(c["q_d"], flags)
-                elif op == "knn":
-                    t.knn(c["q_d"], k, flags)
-                else:
-                    t.radius(c["q_d"], r, flags)
+            for kind in clouds:
+                bname, vname, _ = plan[(kind, op)]
+                run(kind, op, clouds[kind]["trees"][bname], variants[vname])
         per_op[op] = float(np.median(timed(one, 20)))
     stats = torch.zeros(4, dtype=torch.int64, device="cuda")
     for c in clouds.values():
@@ -543,11 +554,17 @@ def points_arm(args, world, rank, local):
     bytes_per_q = 12 + 8 * k + 96 * p_int + (32 + 12 + 4) * p_leaf
     pk, pk_kind = peaks()
     achieved = bytes_per_q * 2 * nq / (per_op["knn"] * 1e-3) / 1e9
+
+    def kernel_of(op, vname):
+        f = variants[vname]
+        return ("k_%s_wide" if f & capi.QK_WIDE else "k_%s_split" if f & capi.QK_TUNE_SPLIT
+                else "k_%s_bin") % op
+
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": pk["hbm_gbs"],
                 "unit": "GB/s", "frac": round(achieved / pk["hbm_gbs"], 4), "traffic": None,
                 "peak_kind": pk_kind,
-                "kernel": ("k_knn_wide" if flags & capi.QK_WIDE else
-                           "k_knn_split" if flags & capi.QK_TUNE_SPLIT else "k_knn_bin"),
+                "kernel": ", ".join(f"{kernel_of('knn', plan[(kind, 'knn')][1])} ({kind})"
+                                    for kind in clouds),
                 "kernel_ms": round(per_op["knn"], 4), "bytes_per_query": round(float(bytes_per_q), 1),
                 "canonical_counts": {"internal_pops_per_query": round(float(p_int), 2),
                                      "leaf_tests_per_query": round(float(p_leaf), 2)}}
@@ -576,13 +593,13 @@ def points_arm(args, world, rank, local):
         fresh = capi.DeviceTree("point", moved_d)
         b_ms = float(np.median(timed(lambda: fresh.build(), 5, 1)))
         fresh.build_wide()
-        a = t.knn(c["q_d"], k, flags).cpu().numpy()
-        b = fresh.knn(c["q_d"], k, flags).cpu().numpy()
+        a = t.knn(c["q_d"], k, 0).cpu().numpy()
+        b = fresh.knn(c["q_d"], k, 0).cpu().numpy()
         ref = oracle.LBVH("point", moved)
         want = ref.knn(c["q"], k)
         if not (np.array_equal(a.view(np.uint32), want) and np.array_equal(b.view(np.uint32), want)):
             raise RuntimeError(f"{kind}: refit kNN differs from the rebuild or the oracle")
-        ca = t.closest(c["q_d"], flags).cpu().numpy().view(np.uint32)
+        ca = t.closest(c["q_d"], 0).cpu().numpy().view(np.uint32)
         if not np.array_equal(ca, ref.closest(c["q"])):
             raise RuntimeError(f"{kind}: refit closest differs from the oracle")
         refit[kind] = {"dirty": int(ids.size), "dirty_refit_ms": round(d_ms, 4),
@@ -602,10 +619,12 @@ def points_arm(args, world, rank, local):
         total = 0
         for kind, c in clouds.items():
             qd = host_q[kind].to("cuda", non_blocking=True)
-            t = c["tree"]
-            a = t.closest(qd, flags)
-            b = t.knn(qd, k, flags)
-            off, keys = t.radius(qd, r, flags)
+            tc, fc = c["trees"][plan[(kind, "closest")][0]], variants[plan[(kind, "closest")][1]]
+            tk, fk = c["trees"][plan[(kind, "knn")][0]], variants[plan[(kind, "knn")][1]]
+            tr, fr = c["trees"][plan[(kind, "radius")][0]], variants[plan[(kind, "radius")][1]]
+            a = tc.closest(qd, fc)
+            b = tk.knn(qd, k, fk)
+            off, keys = tr.radius(qd, r, fr)
             a.cpu(), b.cpu(), off.cpu(), keys.cpu()
             total += int(keys.numel())
         return total
@@ -643,14 +662,15 @@ def points_arm(args, world, rank, local):
             "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded generators, identical bytes on every host)",
             "config": {"workload": "points", "points_per_cloud": n, "clouds": ["surface", "volume"],
-                       "queries_per_op": nq, "k": k, "radius": r, "builder": "lbvh",
-                       "variant": best, "l2": "flushed (256 MB write) between timed steps",
+                       "queries_per_op": nq, "k": k, "radius": r,
+                       "plan": {f"{kind}/{op}": f"{b}/{v}" for (kind, op), (b, v, _) in plan.items()},
+                       "l2": "flushed (256 MB write) between timed steps",
                        "parallelism": f"replica x{world}"},
             "variants_ms": {kk: round(v, 4) for kk, v in vms.items()},
             "per_op_ms": {kk: round(v, 4) for kk, v in per_op.items()},
             "radius_results": radius_keys, "refit": refit, "topology": topology,
             "parity": {"against": kind_ref, "fingerprints": parity,
-                       "variants": "all layouts / orders / schedules bit-identical"},
+                       "variants": "all trees / layouts / orders / schedules bit-identical"},
             "roofline": roofline,
             "cpu_baseline": {"value": round(queries / (cpu_ms * 1e-3) / 1e6, 4) if cpu_ms else None,
                              "unit": "Mqueries/s", "cores": threads, "kind": kind_ref,
@@ -662,10 +682,13 @@ def points_arm(args, world, rank, local):
                     "path": "pinned queries -> qk_closest / qk_knn / qk_radius_count+fill -> host"},
             "gpu_launches": None,
         }
-        morton = 24 if flags & capi.QK_ORDER_MORTON else 0
-        # per cloud: closest + kNN (1 + order), radius count (1 + scan 3 + order) + fill (1 +
-        # order) + 4 segment-sort launches
-        line["gpu_launches"] = args.steps * 2 * ((1 + morton) * 2 + (4 + morton) + (1 + morton) + 4)
+        # per cloud: closest, kNN (1 + order each), radius count (1 + scan 3 + order) + fill
+        # (1 + order) + 4 segment-sort launches; a Morton order is 24 launches
+        launches = 0
+        for (kind, op), (_, vname, _) in plan.items():
+            morton = 24 if variants[vname] & capi.QK_ORDER_MORTON else 0
+            launches += (1 + morton) if op != "radius" else (4 + morton) + (1 + morton) + 4
+        line["gpu_launches"] = args.steps * launches
         print(json.dumps(line), flush=True)
 
 

@@ -509,13 +509,17 @@ def points_arm(args, world, rank, local):
                 "wide_morton": capi.QK_WIDE | capi.QK_ORDER_MORTON,
                 "split": capi.QK_TUNE_SPLIT, "split_morton": capi.QK_TUNE_SPLIT | capi.QK_ORDER_MORTON,
                 "leaf4": capi.QK_TUNE_LEAF4, "leaf4_morton": capi.QK_TUNE_LEAF4 | capi.QK_ORDER_MORTON}
+    radius_variants = {"stash": capi.QK_TUNE_STASH,
+                       "stash_morton": capi.QK_TUNE_STASH | capi.QK_ORDER_MORTON,
+                       "stash_leaf4": capi.QK_TUNE_STASH | capi.QK_TUNE_LEAF4}
     vms, plan = {}, {}
     for kind, c in clouds.items():
         for op in ops:
             run(kind, op, c["trees"]["lbvh"], 0)
             base = snapshot((kind, op))
+            cands = {**variants, **radius_variants} if op == "radius" else variants
             for bname, tree in c["trees"].items():
-                for vname, f in variants.items():
+                for vname, f in cands.items():
                     run(kind, op, tree, f)
                     if not same(base, snapshot((kind, op))):
                         raise RuntimeError(f"{kind} {op}: {bname}/{vname} differs")
@@ -523,6 +527,8 @@ def points_arm(args, world, rank, local):
                     vms[f"{kind}/{op}/{bname}/{vname}"] = t
                     if (kind, op) not in plan or t < plan[(kind, op)][2]:
                         plan[(kind, op)] = (bname, vname, t)
+
+    variants.update(radius_variants)
 
     def step():
         for (kind, op), (bname, vname, _) in plan.items():

@@ -56,6 +56,10 @@ extern "C" {
 #define QK_TUNE_SHORT_STACK 2048u /* binary rays: top 8 stack entries per thread in shared memory */
 #define QK_TUNE_LEAF4 4096u      /* binary nodes: child subtrees of 2..4 primitives are tested
                                     as leaves (skips their inner boxes) */
+#define QK_TUNE_STASH 8192u     /* radius, binary thread-per-query: the count pass keeps each
+                                    query's first 16 keys in the workspace and the fill pass
+                                    traverses again only for queries with more (pass the same
+                                    workspace and flags to qk_radius_count and qk_radius_fill) */
 #define QK_TUNE_SPLIT 1024u      /* closest / kNN / radius on binary nodes: one warp per query,
                                     lanes on disjoint subtrees sharing the pruning bound */
 

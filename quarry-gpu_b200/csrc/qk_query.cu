@@ -20,6 +20,11 @@ namespace qk {
 
 namespace {
 
+// canonical nodes of the leaves (leaf of slot s at n-1+s): their boxes are the leaf boxes
+inline const Node* leaf_nodes(const qk_tree* t) {
+    return static_cast<const Node*>(t->nodes) + (t->n - 1);
+}
+
 // ---------------------------------------------------------------------------------------
 // Morton keys (src/gpu/morton.h:125-146) for query reordering
 // ---------------------------------------------------------------------------------------
@@ -103,7 +108,8 @@ __global__ __launch_bounds__(kBlock, kMinBlocks) void k_ray_bin(const BNode* __r
                                                    const uint32_t* __restrict__ order, int count,
                                                    unsigned long long* __restrict__ out,
                                                    int* __restrict__ ids,
-                                                   int max_iter, unsigned long long* __restrict__ stats) {
+                                                   int max_iter, unsigned long long* __restrict__ stats,
+                                                   const Node* __restrict__ lnodes = nullptr) {
     const int i = blockIdx.x * kBlock + threadIdx.x;
     const bool active = i < count;
     Trav tv;
@@ -124,7 +130,7 @@ __global__ __launch_bounds__(kBlock, kMinBlocks) void k_ray_bin(const BNode* __r
         } else {
             LocalStack<kStack> st;
             out[r] = ray_bin_one<LocalStack<kStack>, kLeaf4>(bn, leaves, root_box(nodes), R,
-                                                             max_iter, st, tv, best_id);
+                                                             max_iter, st, tv, best_id, lnodes);
         }
         if (ids) ids[r] = best_id;
     }
@@ -279,7 +285,8 @@ __global__ __launch_bounds__(kBlock) void k_closest_bin(const BNode* __restrict_
                                                        const float* __restrict__ pts,
                                                        const uint32_t* __restrict__ order,
                                                        int count, uint2* __restrict__ out,
-                                                       int max_iter, unsigned long long* __restrict__ stats) {
+                                                       int max_iter, unsigned long long* __restrict__ stats,
+                                                       const Node* __restrict__ lnodes = nullptr) {
     const int i = blockIdx.x * kBlock + threadIdx.x;
     const bool active = i < count;
     Trav tv;
@@ -287,7 +294,8 @@ __global__ __launch_bounds__(kBlock) void k_closest_bin(const BNode* __restrict_
         const int q = order ? static_cast<int>(order[i]) : i;
         const float3 p = f3(pts[3 * q], pts[3 * q + 1], pts[3 * q + 2]);
         LocalStack<kStack> st;
-        out[q] = closest_bin_one<Ops, LocalStack<kStack>, kLeaf4>(bn, leaves, p, max_iter, st, tv);
+        out[q] = closest_bin_one<Ops, LocalStack<kStack>, kLeaf4>(bn, leaves, p, max_iter, st, tv,
+                                                                  lnodes);
     }
     flush_stats<kStats>(active, tv.nodes, tv.leaves, tv.overflow, stats);
 }
@@ -317,7 +325,8 @@ __global__ __launch_bounds__(kBlock) void k_knn_bin(const BNode* __restrict__ bn
                                                    const float* __restrict__ pts,
                                                    const uint32_t* __restrict__ order, int count,
                                                    int k, int stride, uint2* __restrict__ out,
-                                                   int max_iter, unsigned long long* __restrict__ stats) {
+                                                   int max_iter, unsigned long long* __restrict__ stats,
+                                                   const Node* __restrict__ lnodes = nullptr) {
     const int i = blockIdx.x * kBlock + threadIdx.x;
     const bool active = i < count;
     Trav tv;
@@ -326,7 +335,8 @@ __global__ __launch_bounds__(kBlock) void k_knn_bin(const BNode* __restrict__ bn
         const float3 p = f3(pts[3 * q], pts[3 * q + 1], pts[3 * q + 2]);
         LocalStack<kStack> st;
         KnnTable<K> tab;
-        knn_bin_one<Ops, K, LocalStack<kStack>, kLeaf4>(bn, leaves, p, k, max_iter, st, tv, tab);
+        knn_bin_one<Ops, K, LocalStack<kStack>, kLeaf4>(bn, leaves, p, k, max_iter, st, tv, tab,
+                                                        lnodes);
         write_knn<K>(tab, k, out + static_cast<size_t>(q) * stride);
     }
     flush_stats<kStats>(active, tv.nodes, tv.leaves, tv.overflow, stats);
@@ -359,7 +369,8 @@ __global__ __launch_bounds__(kBlock) void k_radius_bin(
     const BNode* __restrict__ bn, const float4* __restrict__ leaves, const Node* __restrict__ nodes,
     const float* __restrict__ pts, const uint32_t* __restrict__ order, int count, float r2,
     int* __restrict__ counts, const int* __restrict__ offsets,
-    unsigned long long* __restrict__ keys, int max_iter, unsigned long long* __restrict__ stats) {
+    unsigned long long* __restrict__ keys, int max_iter, unsigned long long* __restrict__ stats,
+    const Node* __restrict__ lnodes = nullptr) {
     const int i = blockIdx.x * kBlock + threadIdx.x;
     const bool active = i < count;
     Trav tv;
@@ -370,10 +381,57 @@ __global__ __launch_bounds__(kBlock) void k_radius_bin(
         const int end = kFill ? offsets[q + 1] : 0;  // never write past this query's segment
         LocalStack<kStack> st;
         const int found = radius_bin_one<Ops, kFill, LocalStack<kStack>, kLeaf4>(
-            bn, leaves, root_box(nodes), p, r2, write, end, keys, max_iter, st, tv);
+            bn, leaves, root_box(nodes), p, r2, write, end, keys, max_iter, st, tv, lnodes);
         if (!kFill) counts[q] = found;
     }
     flush_stats<kStats>(active, tv.nodes, tv.leaves, tv.overflow, stats);
+}
+
+// Radius with a stash (QK_TUNE_STASH): the count pass also keeps each query's first kStash
+// keys (the traversal runs in fill mode into the query's stash slots and counts every match);
+// the fill pass then copies the stash for queries with at most kStash results and traverses
+// again only for the others.  The keys are the same, and the segment sort orders them.
+constexpr int kStash = 16;
+
+template <class Ops, bool kStats, bool kLeaf4 = false>
+__global__ __launch_bounds__(kBlock) void k_radius_count_stash(
+    const BNode* __restrict__ bn, const float4* __restrict__ leaves, const Node* __restrict__ nodes,
+    const float* __restrict__ pts, const uint32_t* __restrict__ order, int count, float r2,
+    int* __restrict__ counts, unsigned long long* __restrict__ stash, int max_iter,
+    unsigned long long* __restrict__ stats, const Node* __restrict__ lnodes = nullptr) {
+    const int i = blockIdx.x * kBlock + threadIdx.x;
+    const bool active = i < count;
+    Trav tv;
+    if (active) {
+        const int q = order ? static_cast<int>(order[i]) : i;
+        const float3 p = f3(pts[3 * q], pts[3 * q + 1], pts[3 * q + 2]);
+        const int write = q * kStash;
+        LocalStack<kStack> st;
+        counts[q] = radius_bin_one<Ops, true, LocalStack<kStack>, kLeaf4>(
+            bn, leaves, root_box(nodes), p, r2, write, write + kStash, stash, max_iter, st, tv, lnodes);
+    }
+    flush_stats<kStats>(active, tv.nodes, tv.leaves, tv.overflow, stats);
+}
+
+template <class Ops, bool kLeaf4 = false>
+__global__ __launch_bounds__(kBlock) void k_radius_fill_stash(
+    const BNode* __restrict__ bn, const float4* __restrict__ leaves, const Node* __restrict__ nodes,
+    const float* __restrict__ pts, const uint32_t* __restrict__ order, int count, float r2,
+    const int* __restrict__ offsets, const unsigned long long* __restrict__ stash,
+    unsigned long long* __restrict__ keys, int max_iter, const Node* __restrict__ lnodes = nullptr) {
+    const int i = blockIdx.x * kBlock + threadIdx.x;
+    if (i >= count) return;
+    const int q = order ? static_cast<int>(order[i]) : i;
+    const int begin = offsets[q], end = offsets[q + 1];
+    if (end - begin <= kStash) {
+        for (int j = 0; j < end - begin; ++j) keys[begin + j] = stash[static_cast<size_t>(q) * kStash + j];
+        return;
+    }
+    const float3 p = f3(pts[3 * q], pts[3 * q + 1], pts[3 * q + 2]);
+    Trav tv;
+    LocalStack<kStack> st;
+    radius_bin_one<Ops, true, LocalStack<kStack>, kLeaf4>(bn, leaves, root_box(nodes), p, r2, begin,
+                                                          end, keys, max_iter, st, tv, lnodes);
 }
 
 template <class Ops, bool kFill, bool kStats>
@@ -381,7 +439,8 @@ __global__ __launch_bounds__(kBlock) void k_radius_wide(
     const WideNode* __restrict__ wn, const float4* __restrict__ leaves,
     const float* __restrict__ pts, const uint32_t* __restrict__ order, int count, float r2,
     int* __restrict__ counts, const int* __restrict__ offsets,
-    unsigned long long* __restrict__ keys, int max_iter, unsigned long long* __restrict__ stats) {
+    unsigned long long* __restrict__ keys, int max_iter, unsigned long long* __restrict__ stats,
+    const Node* __restrict__ lnodes = nullptr) {
     const int i = blockIdx.x * kBlock + threadIdx.x;
     const bool active = i < count;
     Trav tv;
@@ -661,8 +720,8 @@ int closest_impl(const qk_tree* t, const float* pts, int count, uint2* out, unsi
         else k_closest_split<Ops, false><<<gs, kBlock, 0, s>>>(bn, leaves, pts, order, count, out, t->n * 2 + 64, stats);
     } else if (flags & QK_TUNE_LEAF4) {
         const BNode* bn = static_cast<const BNode*>(t->bnodes);
-        if (st) k_closest_bin<Ops, true, true><<<g, kBlock, 0, s>>>(bn, leaves, pts, order, count, out, t->n * 2 + 64, stats);
-        else k_closest_bin<Ops, false, true><<<g, kBlock, 0, s>>>(bn, leaves, pts, order, count, out, t->n * 2 + 64, stats);
+        if (st) k_closest_bin<Ops, true, true><<<g, kBlock, 0, s>>>(bn, leaves, pts, order, count, out, t->n * 2 + 64, stats, leaf_nodes(t));
+        else k_closest_bin<Ops, false, true><<<g, kBlock, 0, s>>>(bn, leaves, pts, order, count, out, t->n * 2 + 64, stats, leaf_nodes(t));
     } else {
         const BNode* bn = static_cast<const BNode*>(t->bnodes);
         if (st) k_closest_bin<Ops, true><<<g, kBlock, 0, s>>>(bn, leaves, pts, order, count, out, t->n * 2 + 64, stats);
@@ -689,8 +748,8 @@ void launch_knn(const qk_tree* t, const float* pts, int count, int k, int stride
         else k_knn_wide<Ops, K, false><<<g, kBlock, 0, s>>>(wn, leaves, pts, order, count, k, stride, out, t->n * 2 + 64, stats);
     } else if (leaf4) {
         const BNode* bn = static_cast<const BNode*>(t->bnodes);
-        if (stats) k_knn_bin<Ops, K, true, true><<<g, kBlock, 0, s>>>(bn, leaves, pts, order, count, k, stride, out, t->n * 2 + 64, stats);
-        else k_knn_bin<Ops, K, false, true><<<g, kBlock, 0, s>>>(bn, leaves, pts, order, count, k, stride, out, t->n * 2 + 64, stats);
+        if (stats) k_knn_bin<Ops, K, true, true><<<g, kBlock, 0, s>>>(bn, leaves, pts, order, count, k, stride, out, t->n * 2 + 64, stats, leaf_nodes(t));
+        else k_knn_bin<Ops, K, false, true><<<g, kBlock, 0, s>>>(bn, leaves, pts, order, count, k, stride, out, t->n * 2 + 64, stats, leaf_nodes(t));
     } else {
         const BNode* bn = static_cast<const BNode*>(t->bnodes);
         if (stats) k_knn_bin<Ops, K, true><<<g, kBlock, 0, s>>>(bn, leaves, pts, order, count, k, stride, out, t->n * 2 + 64, stats);
@@ -730,8 +789,8 @@ int radius_launch(const qk_tree* t, const float* pts, int count, float r2, int* 
     } else if (flags & QK_TUNE_LEAF4) {
         const BNode* bn = static_cast<const BNode*>(t->bnodes);
         const Node* nodes = static_cast<const Node*>(t->nodes);
-        if (stats) k_radius_bin<Ops, kFill, true, true><<<g, kBlock, 0, s>>>(bn, leaves, nodes, pts, order, count, r2, counts, offsets, keys, t->n * 2 + 64, stats);
-        else k_radius_bin<Ops, kFill, false, true><<<g, kBlock, 0, s>>>(bn, leaves, nodes, pts, order, count, r2, counts, offsets, keys, t->n * 2 + 64, stats);
+        if (stats) k_radius_bin<Ops, kFill, true, true><<<g, kBlock, 0, s>>>(bn, leaves, nodes, pts, order, count, r2, counts, offsets, keys, t->n * 2 + 64, stats, leaf_nodes(t));
+        else k_radius_bin<Ops, kFill, false, true><<<g, kBlock, 0, s>>>(bn, leaves, nodes, pts, order, count, r2, counts, offsets, keys, t->n * 2 + 64, stats, leaf_nodes(t));
     } else {
         const BNode* bn = static_cast<const BNode*>(t->bnodes);
         const Node* nodes = static_cast<const Node*>(t->nodes);
@@ -808,11 +867,11 @@ int ray_query(const qk_tree* t, const void* rays, int count, uint64_t* out, int*
             if (stt) k_ray_bin<true, 1, 8><<<g, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, ids, t->n * 2 + 64, stt);
             else k_ray_bin<false, 1, 8><<<g, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, ids, t->n * 2 + 64, stt);
         } else if ((flags & QK_TUNE_HIGH_OCC) && (flags & QK_TUNE_LEAF4)) {
-            if (stt) k_ray_bin<true, 5, 0, true><<<g, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, ids, t->n * 2 + 64, stt);
-            else k_ray_bin<false, 5, 0, true><<<g, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, ids, t->n * 2 + 64, stt);
+            if (stt) k_ray_bin<true, 5, 0, true><<<g, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, ids, t->n * 2 + 64, stt, leaf_nodes(t));
+            else k_ray_bin<false, 5, 0, true><<<g, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, ids, t->n * 2 + 64, stt, leaf_nodes(t));
         } else if (flags & QK_TUNE_LEAF4) {
-            if (stt) k_ray_bin<true, 1, 0, true><<<g, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, ids, t->n * 2 + 64, stt);
-            else k_ray_bin<false, 1, 0, true><<<g, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, ids, t->n * 2 + 64, stt);
+            if (stt) k_ray_bin<true, 1, 0, true><<<g, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, ids, t->n * 2 + 64, stt, leaf_nodes(t));
+            else k_ray_bin<false, 1, 0, true><<<g, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, ids, t->n * 2 + 64, stt, leaf_nodes(t));
         } else if (flags & QK_TUNE_HIGH_OCC) {
             if (stt) k_ray_bin<true, 5><<<g, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, ids, t->n * 2 + 64, stt);
             else k_ray_bin<false, 5><<<g, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, ids, t->n * 2 + 64, stt);
@@ -861,6 +920,11 @@ int knn_query(const qk_tree* t, const float* pts, int count, int k, int stride, 
     }
 }
 
+// the stash applies to the binary thread-per-query traversal only
+bool use_stash(unsigned flags) {
+    return (flags & QK_TUNE_STASH) && !(flags & (QK_TUNE_SPLIT | QK_WIDE));
+}
+
 size_t radius_ws_bytes(int count, unsigned flags) {
     Carve c;
     carve_order(c, count);
@@ -869,7 +933,45 @@ size_t radius_ws_bytes(int count, unsigned flags) {
     c.take<int>(count);            // medium segment list
     c.take<int>(count);            // large segment list
     if (flags & QK_TUNE_SPLIT) c.take<int>(static_cast<size_t>(count) * 32);  // lane counts
+    if (use_stash(flags)) c.take<unsigned long long>(static_cast<size_t>(count) * kStash);
     return c.used;
+}
+
+template <class Ops>
+int radius_stash_launch(const qk_tree* t, const float* pts, int count, float r2, int* counts,
+                        const int* offsets, unsigned long long* stash, unsigned long long* keys,
+                        unsigned flags, unsigned long long* stats, const uint32_t* order,
+                        bool fill, cudaStream_t s) {
+    const BNode* bn = static_cast<const BNode*>(t->bnodes);
+    const Node* nodes = static_cast<const Node*>(t->nodes);
+    const float4* leaves = static_cast<const float4*>(t->leaves);
+    const int g = blocks_for(count);
+    const int it = t->n * 2 + 64;
+    const bool leaf4 = (flags & QK_TUNE_LEAF4) != 0;
+    if (fill) {
+        if (leaf4) k_radius_fill_stash<Ops, true><<<g, kBlock, 0, s>>>(bn, leaves, nodes, pts, order, count, r2, offsets, stash, keys, it, leaf_nodes(t));
+        else k_radius_fill_stash<Ops><<<g, kBlock, 0, s>>>(bn, leaves, nodes, pts, order, count, r2, offsets, stash, keys, it);
+    } else if (leaf4) {
+        if (stats) k_radius_count_stash<Ops, true, true><<<g, kBlock, 0, s>>>(bn, leaves, nodes, pts, order, count, r2, counts, stash, it, stats, leaf_nodes(t));
+        else k_radius_count_stash<Ops, false, true><<<g, kBlock, 0, s>>>(bn, leaves, nodes, pts, order, count, r2, counts, stash, it, stats, leaf_nodes(t));
+    } else {
+        if (stats) k_radius_count_stash<Ops, true><<<g, kBlock, 0, s>>>(bn, leaves, nodes, pts, order, count, r2, counts, stash, it, stats);
+        else k_radius_count_stash<Ops, false><<<g, kBlock, 0, s>>>(bn, leaves, nodes, pts, order, count, r2, counts, stash, it, stats);
+    }
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? QK_OK : cuda_status(e, "radius traversal (stash)");
+}
+
+int radius_stash_dispatch(const qk_tree* t, const float* pts, int count, float r2, int* counts,
+                          const int* offsets, unsigned long long* stash, unsigned long long* keys,
+                          unsigned flags, unsigned long long* stats, const uint32_t* order,
+                          bool fill, cudaStream_t s) {
+    switch (t->kind) {
+        case kTri: return radius_stash_launch<TriOps>(t, pts, count, r2, counts, offsets, stash, keys, flags, stats, order, fill, s);
+        case kPoint: return radius_stash_launch<PointOps>(t, pts, count, r2, counts, offsets, stash, keys, flags, stats, order, fill, s);
+        case kGauss: return radius_stash_launch<GaussOps>(t, pts, count, r2, counts, offsets, stash, keys, flags, stats, order, fill, s);
+        default: return fail(QK_ERR_INVALID, "unknown primitive kind %d", t->kind);
+    }
 }
 
 int radius_count(const qk_tree* t, const float* pts, int count, float r, int* offsets,
@@ -886,11 +988,17 @@ int radius_count(const qk_tree* t, const float* pts, int count, float r, int* of
     c.take<int>(count);
     c.take<int>(count);
     int* lane_counts = (flags & QK_TUNE_SPLIT) ? c.take<int>(static_cast<size_t>(count) * 32) : nullptr;
+    unsigned long long* stash =
+        use_stash(flags) ? c.take<unsigned long long>(static_cast<size_t>(count) * kStash) : nullptr;
     int st = QK_OK;
     const uint32_t* order = make_order(pts, 3, 0, count, flags, o, s, &st);
     if (st != QK_OK) return st;
-    st = radius_dispatch<false>(t, pts, count, r * r, counts, lane_counts, nullptr, nullptr, flags,
-                                reinterpret_cast<unsigned long long*>(stats), order, s);
+    if (stash)
+        st = radius_stash_dispatch(t, pts, count, r * r, counts, nullptr, stash, nullptr, flags,
+                                   reinterpret_cast<unsigned long long*>(stats), order, false, s);
+    else
+        st = radius_dispatch<false>(t, pts, count, r * r, counts, lane_counts, nullptr, nullptr, flags,
+                                    reinterpret_cast<unsigned long long*>(stats), order, s);
     if (st != QK_OK) return st;
     cudaError_t e = scan_exclusive(counts, offsets, count, true, scan_ws, s);
     if (e != cudaSuccess) return cuda_status(e, "radius scan");
@@ -912,12 +1020,18 @@ int radius_fill(const qk_tree* t, const float* pts, int count, float r, const in
     int* medium = c.take<int>(count);
     int* large = c.take<int>(count);
     int* lane_counts = (flags & QK_TUNE_SPLIT) ? c.take<int>(static_cast<size_t>(count) * 32) : nullptr;
+    unsigned long long* stash =
+        use_stash(flags) ? c.take<unsigned long long>(static_cast<size_t>(count) * kStash) : nullptr;
     int st = QK_OK;
     const uint32_t* order = make_order(pts, 3, 0, count, flags, o, s, &st);
     if (st != QK_OK) return st;
     auto* k64 = reinterpret_cast<unsigned long long*>(keys);
-    st = radius_dispatch<true>(t, pts, count, r * r, nullptr, lane_counts, offsets, k64, flags,
-                               nullptr, order, s);
+    if (stash)
+        st = radius_stash_dispatch(t, pts, count, r * r, nullptr, offsets, stash, k64, flags, nullptr,
+                                   order, true, s);
+    else
+        st = radius_dispatch<true>(t, pts, count, r * r, nullptr, lane_counts, offsets, k64, flags,
+                                   nullptr, order, s);
     if (st != QK_OK) return st;
     // reset the segment lists (make_order only resets them on its Morton path)
     return radius_sort_segments(offsets, count, keys, medium, large, o.h, -1, s);

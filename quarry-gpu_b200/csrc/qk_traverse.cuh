@@ -97,6 +97,16 @@ __device__ __forceinline__ void load_bnode_small(const BNode* __restrict__ bn, i
     rsm = __float_as_int(d.w);
 }
 
+// box of the leaf in slot s; lnodes = the canonical nodes of the leaves (nodes + n - 1)
+__device__ __forceinline__ Box leaf_box(const Node* __restrict__ lnodes, int s) {
+    const float4* p = reinterpret_cast<const float4*>(lnodes + s);
+    const float4 a = __ldg(p), b = __ldg(p + 1);
+    Box bx;
+    bx.lo = f3(a.x, a.y, a.z);
+    bx.hi = f3(a.w, b.x, b.y);
+    return bx;
+}
+
 __device__ __forceinline__ Box root_box(const Node* __restrict__ nodes) {
     const float4* p = reinterpret_cast<const float4*>(nodes);
     const float4 a = __ldg(p), b = __ldg(p + 1);
@@ -167,7 +177,8 @@ __device__ __forceinline__ unsigned long long ray_bin_one(const BNode* __restric
                                                           const float4* __restrict__ leaves,
                                                           const Box& rb, const RayPre& R,
                                                           int max_iter, St& st, Trav& tv,
-                                                          int& best_id) {
+                                                          int& best_id,
+                                                          const Node* __restrict__ lnodes = nullptr) {
     float best = R.tmax;
     float bound = best * kMarginMul + kMarginAdd;
     bool any = false;
@@ -214,6 +225,10 @@ __device__ __forceinline__ unsigned long long ray_bin_one(const BNode* __restric
                     if (code && !(te > bound * kMarginMul + kMarginAdd)) {
                         const int first = code >> 2, cnt = (code & 3) + 1;
                         for (int j = 0; j < cnt; ++j) {
+                            // the leaf's own box first, as a descent would test it
+                            const Box lb = leaf_box(lnodes, first + j);
+                            float tb;
+                            if (!ray_box(R, lb.lo, lb.hi, bound, tb)) continue;
                             ++tv.leaves;
                             test_tri(R, leaves, first + j, best, bound, any, best_id);
                         }
@@ -354,7 +369,8 @@ __device__ __forceinline__ uint2 pack_closest(float best, int best_id) {
 template <class Ops, class St, bool kLeaf4 = false>
 __device__ __forceinline__ uint2 closest_bin_one(const BNode* __restrict__ bn,
                                                  const float4* __restrict__ leaves, float3 p,
-                                                 int max_iter, St& st, Trav& tv) {
+                                                 int max_iter, St& st, Trav& tv,
+                                                 const Node* __restrict__ lnodes = nullptr) {
     float best = kInf;
     int best_id = -1;
     int sp = 0;
@@ -395,6 +411,8 @@ __device__ __forceinline__ uint2 closest_bin_one(const BNode* __restrict__ bn,
                     if (code && (best_id < 0 || dbox <= best)) {
                         const int first = code >> 2, cnt = (code & 3) + 1;
                         for (int j = 0; j < cnt; ++j) {
+                            const Box lb = leaf_box(lnodes, first + j);
+                            if (!(best_id < 0 || dist2_box(p, lb.lo, lb.hi) <= best)) continue;
                             ++tv.leaves;
                             leaf_closest<Ops>(p, leaves, first + j, best, best_id);
                         }
@@ -577,7 +595,8 @@ __device__ __forceinline__ void write_knn(const KnnTable<K>& tab, int k, uint2* 
 template <class Ops, int K, class St, bool kLeaf4 = false>
 __device__ __forceinline__ void knn_bin_one(const BNode* __restrict__ bn,
                                             const float4* __restrict__ leaves, float3 p, int k,
-                                            int max_iter, St& st, Trav& tv, KnnTable<K>& tab) {
+                                            int max_iter, St& st, Trav& tv, KnnTable<K>& tab,
+                                            const Node* __restrict__ lnodes = nullptr) {
     tab.init();
     int sp = 0;
     int node = 0;
@@ -616,6 +635,8 @@ __device__ __forceinline__ void knn_bin_one(const BNode* __restrict__ bn,
                     if (code && tab.admits(dbox)) {
                         const int first = code >> 2, cnt = (code & 3) + 1;
                         for (int j = 0; j < cnt; ++j) {
+                            const Box lb = leaf_box(lnodes, first + j);
+                            if (!tab.admits(dist2_box(p, lb.lo, lb.hi))) continue;
                             ++tv.leaves;
                             leaf_knn<Ops, K>(p, leaves, first + j, tab, k);
                         }
@@ -736,7 +757,8 @@ __device__ __forceinline__ int radius_bin_one(const BNode* __restrict__ bn,
                                               const float4* __restrict__ leaves, const Box& rb,
                                               float3 p, float r2, int write, int end,
                                               unsigned long long* __restrict__ keys,
-                                              int max_iter, St& st, Trav& tv) {
+                                              int max_iter, St& st, Trav& tv,
+                                              const Node* __restrict__ lnodes = nullptr) {
     int found = 0;
     if (!(dist2_box(p, rb.lo, rb.hi) <= r2)) return 0;
     int sp = 0;
@@ -780,6 +802,8 @@ __device__ __forceinline__ int radius_bin_one(const BNode* __restrict__ bn,
                 if (code) {
                     const int first = code >> 2, cnt = (code & 3) + 1;
                     for (int j = 0; j < cnt; ++j) {
+                        const Box lb = leaf_box(lnodes, first + j);
+                        if (!(dist2_box(p, lb.lo, lb.hi) <= r2)) continue;
                         ++tv.leaves;
                         int id;
                         const float d2 = Ops::dist2(p, leaves, first + j, id);

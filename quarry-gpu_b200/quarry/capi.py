@@ -23,6 +23,7 @@ QK_BUILD_LBVH, QK_BUILD_SAH = 0, 1
 QK_ORDER_MORTON, QK_ORDER_DIRECTION, QK_WIDE = 1, 2, 4
 QK_TUNE_DYNAMIC, QK_TUNE_HIGH_OCC, QK_TUNE_SPLIT, QK_TUNE_SHORT_STACK = 256, 512, 1024, 2048
 QK_TUNE_LEAF4 = 4096
+QK_TUNE_STASH = 8192
 QK_SCHEDULE_BATCHED, QK_SCHEDULE_LOOP = 0, 1
 QK_OP_RAY, QK_OP_CLOSEST, QK_OP_KNN, QK_OP_RADIUS = 0, 1, 2, 3
 KINDS = {"tri": QK_TRI, "point": QK_POINT, "gauss": QK_GAUSS}

@@ -437,7 +437,7 @@ def test_leaf4_small_subtrees_same_bits(cuda, kind, builder):
     qh = _queries(items, kind, 3_001, 5)
     q = _dev(qh)
     lo, hi = qh.min(0), qh.max(0)
-    r = float(np.linalg.norm(hi - lo)) * 0.04
+    radii = [float(np.linalg.norm(hi - lo)) * f for f in (0.04, 0.2)]
     rays = _dev(_random_rays(lo, hi, 20_001, 6)) if kind == "tri" else None
 
     def same(t):
@@ -446,9 +446,12 @@ def test_leaf4_small_subtrees_same_bits(cuda, kind, builder):
             assert cuda.equal(t.closest(q, f), t.closest(q, 0)), extra
             for k in (1, 8, 16):
                 assert cuda.equal(t.knn(q, k, f), t.knn(q, k, 0)), (k, extra)
-            o1, k1 = t.radius(q, r, f)
-            o0, k0 = t.radius(q, r, 0)
-            assert cuda.equal(o1, o0) and cuda.equal(k1, k0)
+            # the wide radius reaches leaves whose own box fails the radius although their
+            # primitive's computed distance passes it (Gaussians): leaf4 must skip them too
+            for r in radii:
+                o1, k1 = t.radius(q, r, f)
+                o0, k0 = t.radius(q, r, 0)
+                assert cuda.equal(o1, o0) and cuda.equal(k1, k0), r
             if rays is not None:
                 for tune in (0, capi.QK_TUNE_HIGH_OCC):
                     want, want_ids = t.raycast_ids(rays, extra)
@@ -494,6 +497,28 @@ def test_split_knn_sphere_matches_oracle(cuda):
     assert np.array_equal(got, ref.closest(q))
 
 
+@pytest.mark.parametrize("kind", ["tri", "point", "gauss"])
+def test_radius_stash_same_csr(cuda, kind):
+    """Radius with the count pass's 16-key stash: the same CSR as the two-traversal path, with
+    segments below, at and above the stash size (and empty ones)."""
+    items = _items(kind)
+    tree = capi.DeviceTree(kind, items)
+    q = _queries(items, kind, 4_001, 31)
+    dq = _dev(q)
+    lo, hi = q.min(0), q.max(0)
+    seen = set()
+    for frac in (0.002, 0.03, 0.08, 0.2):
+        r = float(np.linalg.norm(hi - lo)) * frac
+        o0, k0 = tree.radius(dq, r, 0)
+        sizes = np.diff(o0.cpu().numpy())
+        seen |= {0 if z == 0 else (1 if z <= 16 else 2) for z in np.unique(sizes)}
+        for f in (capi.QK_TUNE_STASH, capi.QK_TUNE_STASH | capi.QK_ORDER_MORTON,
+                  capi.QK_TUNE_STASH | capi.QK_TUNE_LEAF4):
+            o1, k1 = tree.radius(dq, r, f)
+            assert cuda.equal(o1, o0) and cuda.equal(k1, k0), (frac, f)
+    assert seen == {0, 1, 2}  # empty segments, segments within the stash and beyond it
+
+
 def test_radius_segment_sizes_all_sort_paths(cuda):
     """Segments of 0..32 keys (warp registers), 33..1024 (warp shared memory), 1025..4096
     (block shared memory) and more (block, global memory) all come out sorted as the oracle's."""
@@ -506,7 +531,8 @@ def test_radius_segment_sizes_all_sort_paths(cuda):
     for r in (0.15, 0.4, 0.75, 1.1):
         want_off, want_keys = ref.radius(q, r)
         sizes = np.diff(want_off)
-        for flags in (0, capi.QK_TUNE_SPLIT, capi.QK_ORDER_MORTON):
+        for flags in (0, capi.QK_TUNE_SPLIT, capi.QK_ORDER_MORTON, capi.QK_TUNE_STASH,
+                      capi.QK_TUNE_STASH | capi.QK_ORDER_MORTON):
             off, keys = tree.radius(dq, r, flags)
             assert np.array_equal(off.cpu().numpy().astype(np.int64), want_off)
             assert np.array_equal(keys.cpu().numpy().view(np.uint64), want_keys), (r, flags)

@@ -156,6 +156,7 @@ __global__ __launch_bounds__(kBlock) void k_level_reset(Level L, int bins) {
 
 __global__ __launch_bounds__(kBlock) void k_level_cbounds(Level L, const int* __restrict__ order,
                                                          const float4* __restrict__ cen) {
+    if (static_cast<int>(blockIdx.x) >= L.counters[0]) return;  // grid sized by a bound
     const int c = blockIdx.x;
     const int t = L.chunk_task[c];
     const int b = L.chunk_begin[c];
@@ -189,6 +190,7 @@ __global__ __launch_bounds__(kBlock) void k_level_bins(Level L, const int* __res
                                                       const float4* __restrict__ plo,
                                                       const float4* __restrict__ phi, int bins) {
     __shared__ unsigned sb[3 * kMaxBins * kBinWords];
+    if (static_cast<int>(blockIdx.x) >= L.counters[0]) return;  // grid sized by a bound
     for (int j = threadIdx.x; j < 3 * bins * kBinWords; j += kBlock) {
         const int w = j % kBinWords;
         sb[j] = w == 0 ? 0u : (w <= 3 ? ord_f(kInf) : ord_f(-kInf));
@@ -421,6 +423,7 @@ __device__ __forceinline__ bool goes_left(int split, int pos, int begin, int lc,
 __global__ __launch_bounds__(kBlock) void k_level_count_left(Level L, const int* __restrict__ order,
                                                             const float4* __restrict__ cen,
                                                             int bins) {
+    if (static_cast<int>(blockIdx.x) >= L.counters[0]) return;  // grid sized by a bound
     const int c = blockIdx.x;
     const int t = L.chunk_task[c];
     const Task tk = L.tasks[t];
@@ -461,6 +464,7 @@ __global__ __launch_bounds__(kBlock) void k_level_partition(Level L, const int* 
                                                            int* __restrict__ out,
                                                            const float4* __restrict__ cen,
                                                            int bins) {
+    if (static_cast<int>(blockIdx.x) >= L.counters[0]) return;  // grid sized by a bound
     const int c = blockIdx.x;
     const int t = L.chunk_task[c];
     const Task tk = L.tasks[t];
@@ -508,6 +512,7 @@ __global__ __launch_bounds__(kBlock) void k_level_partition(Level L, const int* 
 
 __global__ __launch_bounds__(kBlock) void k_level_copy(Level L, const int* __restrict__ src,
                                                       int* __restrict__ dst) {
+    if (static_cast<int>(blockIdx.x) >= L.counters[0]) return;  // grid sized by a bound
     const int c = blockIdx.x;
     const int t = L.chunk_task[c];
     const int b = L.chunk_begin[c];
@@ -1252,10 +1257,10 @@ int build_sah_impl(qk_tree* t, int bins, const void* items_v, void* ws, cudaStre
         w.L.tasks = cur;
         k_level_prep<<<1, 1024, 0, s>>>(w.L, nbig, bins);
         k_level_reset<<<nbig, kBlock, 0, s>>>(w.L, bins);
-        int nch = 0;
-        cudaError_t e = cudaMemcpyAsync(&nch, w.L.counters, sizeof(int), cudaMemcpyDeviceToHost, s);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-        if (e != cudaSuccess) return cuda_status(e, "SAH level prep");
+        // chunk kernels: grid sized by a bound on the chunk count (every task spans at most
+        // size / kChunk + 1 chunks); blocks beyond the count k_level_prep wrote return at once
+        const int nch = n / kChunk + nbig + 1;
+        cudaError_t e;
         k_level_cbounds<<<nch, kBlock, 0, s>>>(w.L, ord, w.cen);
         k_level_bins<<<nch, kBlock, 0, s>>>(w.L, ord, w.cen, w.plo, w.phi, bins);
         k_level_split<<<blocks_for(static_cast<long long>(nbig) * 32), kBlock, 0, s>>>(w.L, nbig, bins);

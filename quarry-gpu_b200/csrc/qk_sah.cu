@@ -9,8 +9,8 @@
 //            primitives bin their centroids in shared memory (count + primitive box per bin,
 //            3 axes) and merge into per-range bins with ordered-uint atomics; one thread per
 //            range sweeps the bins for the cheapest area(L)*nL + area(R)*nR split; a stable
-//            partition by chunk-local block scans writes the new order.  Two host syncs per
-//            level.
+//            partition by chunk-local block scans writes the new order.  One host sync per
+//            level (the next level's range count); chunk grids are sized by a bound.
 //   warp     every range of at most kTaskRange (256) primitives is handed to one warp
 //            (k_warp_tasks): binned SAH with warp-private bins down to 32 primitives
 //            (warp_piece_tree), then the exact sweep below; no block barriers, no global

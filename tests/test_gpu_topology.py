@@ -224,3 +224,44 @@ def test_python_update_topology_uses_surgery(cuda):
     for a, b in zip(scene.raycast(rays[:, :3], rays[:, 3:6]),
                     fresh.raycast(rays[:, :3], rays[:, 3:6])):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("kind", ["point", "gauss"])
+def test_python_clouds_update_topology_rounds(cuda, kind):
+    """PointCloud / GaussianCloud.update_topology (updatePointBVHGPU / updateGaussianBVHGPU):
+    three mixed edits in a row on one object (the C++ layer reuses its spare arrays and keeps
+    the 4-wide layer), each answering like a freshly built object, wide queries included."""
+    import quarry
+
+    rng = np.random.default_rng(43)
+    items = _items(kind, 20_000, 14)
+
+    def make(a):
+        if kind == "point":
+            return quarry.PointCloud(a)
+        return quarry.GaussianCloud(a[:, :3].copy(), a[:, 3:7].copy(), a[:, 7:10].copy())
+
+    def update(obj, a, dele, ins, mov):
+        if kind == "point":
+            return obj.update_topology(a, deleted=dele, moved=mov, inserted=ins)
+        return obj.update_topology(a[:, :3].copy(), a[:, 3:7].copy(), a[:, 7:10].copy(),
+                                   deleted=dele, moved=mov, inserted=ins)
+
+    obj = make(items)
+    lo, hi = items[:, :3].min(0), items[:, :3].max(0)
+    q = workloads.uniform_points(1_000, lo - 1.0, hi + 1.0, 5, 21)
+    obj.closest(q, wide=True)  # builds the 4-wide layer
+    for step in range(3):
+        new, dele, ins, mov = make_edit(kind, items, rng, 30, 15, 10 + 5 * step, 20)
+        tm = update(obj, new, dele, ins, mov)
+        assert tm["full_rebuild"] is False, (step, tm)
+        assert obj.validate() == ""
+        fresh = make(new)
+        for wide in (False, True):
+            for a, b in zip(obj.closest(q, wide=wide), fresh.closest(q, wide=wide)):
+                assert np.array_equal(a, b), (step, wide)
+            for a, b in zip(obj.knn(q, 8, wide=wide), fresh.knn(q, 8, wide=wide)):
+                assert np.array_equal(a, b), (step, wide)
+        for a, b in zip(obj.radius(q, 2.0), fresh.radius(q, 2.0)):
+            assert np.array_equal(a, b), step
+        items = new

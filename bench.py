@@ -1165,6 +1165,14 @@ def rays_arm(args, world, rank, local):
                    "cores": threads, "kind": kind,
                    "sample": f"first {sample} of the {nrays} rays, reference BVH build "
                              f"({ref_build:.0f} ms) excluded"}
+            # the same reference on one host thread (a smaller sample)
+            one = min(sample, 50_000)
+            one_out, one_ms, _, _ = cpu_reference_rays(cfg.tris, cfg.rays[:one], 1)
+            if int((one_out != result[:one]).sum()):
+                raise RuntimeError("single-thread CPU reference differs")
+            cpu["single_thread"] = {"value": round(one / (one_ms * 1e-3) / 1e6, 4),
+                                    "unit": "Mrays/s", "cores": 1,
+                                    "sample": f"first {one} rays, BVH build excluded"}
         line = {
             "metric": METRIC, "value": round(value, 2), "unit": "Mrays/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),

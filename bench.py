@@ -78,6 +78,33 @@ def peaks() -> tuple[dict, str]:
     return PEAKS_FALLBACK, "fallback"
 
 
+def coherent_order(rays: np.ndarray) -> np.ndarray:
+    """The engine's coherent ray order (QK_ORDER_COHERENT), recomputed on the host: a Morton
+    key over origin and direction, the non-flat axes (bounds of 4,096 rays spaced count /
+    4,096 apart) with b bits each, b * axes <= log2(bucket count), the bucket count at most
+    32,768 and count / 4; ties keep input order."""
+    n = rays.shape[0]
+    kb = 4
+    while (2 << kb) <= 32768 and (2 << kb) <= n // 4:
+        kb += 1
+    x = rays[:, :6].astype(np.float32)
+    samples = min(n, 4096)
+    pick = x[np.arange(samples, dtype=np.int64) * (n // samples)]
+    lo, hi = pick.min(0), pick.max(0)
+    ext = hi - lo
+    live = [a for a in range(6) if ext[a] > 0 and np.isfinite(ext[a])]
+    if not live:
+        return np.arange(n)
+    bits = min(kb // len(live), 10)
+    q = [np.clip((x[:, a] - lo[a]) * np.float32((1 << bits) / ext[a]), 0,
+                 (1 << bits) - 1).astype(np.uint32) for a in live]
+    key = np.zeros(n, np.uint32)
+    for bit in range(bits - 1, -1, -1):
+        for qa in q:
+            key = (key << np.uint32(1)) | ((qa >> np.uint32(bit)) & np.uint32(1))
+    return np.argsort(key, kind="stable")
+
+
 def make_workload(name: str, small: bool, rank: int):
     from quarry import workloads as w
 
@@ -508,10 +535,13 @@ def points_arm(args, world, rank, local):
     variants = {"bin": 0, "bin_morton": capi.QK_ORDER_MORTON, "wide": capi.QK_WIDE,
                 "wide_morton": capi.QK_WIDE | capi.QK_ORDER_MORTON,
                 "split": capi.QK_TUNE_SPLIT, "split_morton": capi.QK_TUNE_SPLIT | capi.QK_ORDER_MORTON,
-                "leaf4": capi.QK_TUNE_LEAF4, "leaf4_morton": capi.QK_TUNE_LEAF4 | capi.QK_ORDER_MORTON}
+                "leaf4": capi.QK_TUNE_LEAF4, "leaf4_morton": capi.QK_TUNE_LEAF4 | capi.QK_ORDER_MORTON,
+                "bin_coh": capi.QK_ORDER_COHERENT, "split_coh": capi.QK_TUNE_SPLIT | capi.QK_ORDER_COHERENT,
+                "leaf4_coh": capi.QK_TUNE_LEAF4 | capi.QK_ORDER_COHERENT}
     radius_variants = {"stash": capi.QK_TUNE_STASH,
                        "stash_morton": capi.QK_TUNE_STASH | capi.QK_ORDER_MORTON,
-                       "stash_leaf4": capi.QK_TUNE_STASH | capi.QK_TUNE_LEAF4}
+                       "stash_leaf4": capi.QK_TUNE_STASH | capi.QK_TUNE_LEAF4,
+                       "stash_coh": capi.QK_TUNE_STASH | capi.QK_ORDER_COHERENT}
     vms, plan = {}, {}
     for kind, c in clouds.items():
         for op in ops:
@@ -689,10 +719,12 @@ def points_arm(args, world, rank, local):
             "gpu_launches": None,
         }
         # per cloud: closest, kNN (1 + order each), radius count (1 + scan 3 + order) + fill
-        # (1 + order) + 4 segment-sort launches; a Morton order is 24 launches
+        # (1 + order) + 4 segment-sort launches; a Morton order is 24 launches, a coherent
+        # order 4 (grid, keys, scan, scatter)
         launches = 0
         for (kind, op), (_, vname, _) in plan.items():
-            morton = 24 if variants[vname] & capi.QK_ORDER_MORTON else 0
+            morton = (24 if variants[vname] & capi.QK_ORDER_MORTON else
+                      4 if variants[vname] & capi.QK_ORDER_COHERENT else 0)
             launches += (1 + morton) if op != "radius" else (4 + morton) + (1 + morton) + 4
         line["gpu_launches"] = args.steps * launches
         print(json.dumps(line), flush=True)
@@ -951,12 +983,15 @@ def rays_arm(args, world, rank, local):
     l2_flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
 
     dyn, occ, mort = capi.QK_TUNE_DYNAMIC, capi.QK_TUNE_HIGH_OCC, capi.QK_ORDER_MORTON
+    coh = capi.QK_ORDER_COHERENT
     modes = {"bin": 0, "bin_morton": mort, "wide": capi.QK_WIDE,
              "wide_morton": capi.QK_WIDE | mort, "bin_occ": occ, "bin_morton_occ": mort | occ,
              "bin_dyn": dyn, "bin_morton_dyn": mort | dyn, "bin_morton_dyn_occ": mort | dyn | occ,
              "bin_sm": capi.QK_TUNE_SHORT_STACK, "bin_occ_sm": occ | capi.QK_TUNE_SHORT_STACK,
              "bin_leaf4": capi.QK_TUNE_LEAF4, "bin_occ_leaf4": occ | capi.QK_TUNE_LEAF4,
-             "bin_morton_occ_leaf4": mort | occ | capi.QK_TUNE_LEAF4}
+             "bin_morton_occ_leaf4": mort | occ | capi.QK_TUNE_LEAF4,
+             "bin_coh": coh, "bin_coh_occ": coh | occ, "bin_coh_dyn_occ": coh | dyn | occ,
+             "bin_coh_occ_leaf4": coh | occ | capi.QK_TUNE_LEAF4, "wide_coh": capi.QK_WIDE | coh}
     variants = {f"{b}_{m}": (b, f) for b in trees for m, f in modes.items()}
     if args.only:
         variants = {args.only: variants[args.only]}
@@ -1015,8 +1050,10 @@ def rays_arm(args, world, rank, local):
     # ---- roofline: traversal kernel alone on pre-sorted rays ----
     # the engine's Morton order, recomputed on the host (quantize10 of src/gpu/morton.h), so
     # the kernel alone can be timed on rays that are already in that order
-    trav_flags = best_flags & ~capi.QK_ORDER_MORTON
-    if best_flags & capi.QK_ORDER_MORTON:
+    trav_flags = best_flags & ~(capi.QK_ORDER_MORTON | capi.QK_ORDER_COHERENT)
+    if best_flags & capi.QK_ORDER_COHERENT:
+        sorted_rays = capi.to_device(cfg.rays[coherent_order(cfg.rays)], np.float32)
+    elif best_flags & capi.QK_ORDER_MORTON:
         o = cfg.rays[:, :3]
         lo, hi = o.min(0), o.max(0)
         qz = np.clip((o - lo) / np.where(hi > lo, hi - lo, 1), 0, 1)
@@ -1111,37 +1148,45 @@ def rays_arm(args, world, rank, local):
                                    rays_d[:200_000])
 
     # ---- e2e through the C ABI from pinned host buffers: qk_raycast_host uploads, traces and
-    # reads back in chunks over two streams, all inside the timed region ----
+    # reads back in chunks (uploads, traversals and read-backs on three streams), all inside
+    # the timed region ----
     host_rays = torch.from_numpy(np.ascontiguousarray(cfg.rays)).pin_memory()
     host_out = torch.empty(nrays, dtype=torch.int64).pin_memory()
     dev_rays = torch.empty((nrays, 8), dtype=torch.float32, device=dev)
-    s0, s1 = torch.cuda.Stream(), torch.cuda.Stream()
+    streams = tuple(torch.cuda.Stream() for _ in range(4))
 
-    def e2e_times(chunks, steps):
+    def e2e_times(chunks, steps, flags):
         ws = torch.empty(capi.lib().qk_raycast_host_workspace_bytes(nrays, chunks),
                          dtype=torch.uint8, device=dev)
         for _ in range(3):
-            tree.raycast_host(host_rays, host_out, dev_rays, out, best_flags, chunks, (s0, s1), ws)
+            tree.raycast_host(host_rays, host_out, dev_rays, out, flags, chunks, streams, ws)
         torch.cuda.synchronize()
         ts = []
         for _ in range(steps):
             l2_flush.zero_()
             torch.cuda.synchronize()
             e0 = torch.cuda.Event(enable_timing=True)
-            e0.record(s0)
-            s1.wait_event(e0)
-            tree.raycast_host(host_rays, host_out, dev_rays, out, best_flags, chunks, (s0, s1), ws)
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a.record(s0)
-            b.record(s1)
+            e0.record(streams[0])
+            for x in streams[1:]:
+                x.wait_event(e0)
+            tree.raycast_host(host_rays, host_out, dev_rays, out, flags, chunks, streams, ws)
+            ends = [torch.cuda.Event(enable_timing=True) for _ in streams]
+            for ev, x in zip(ends, streams):
+                ev.record(x)
             torch.cuda.synchronize()
-            ts.append(max(e0.elapsed_time(a), e0.elapsed_time(b)))
+            ts.append(max(e0.elapsed_time(ev) for ev in ends))
         return ts
 
-    # the chunk count of the pipeline is chosen by measurement (same bits for every count)
-    chunk_ms = {c: float(np.median(e2e_times(c, 10))) for c in (2, 4, 8, 16)}
-    chunks = min(chunk_ms, key=chunk_ms.get)
-    e2e_t = e2e_times(chunks, min(args.steps, 50))
+    # the chunk count and the ray order of the pipeline are chosen by measurement (same bits
+    # for every choice): per chunk, an order costs a fixed few tens of microseconds
+    orders = {"timed variant": best_flags,
+              "input order": best_flags & ~(capi.QK_ORDER_MORTON | capi.QK_ORDER_COHERENT)}
+    chunk_ms = {f"{c} chunks, {o}": float(np.median(e2e_times(c, 10, f)))
+                for o, f in orders.items() for c in (2, 4, 8, 16)}
+    e2e_pick = min(chunk_ms, key=chunk_ms.get)
+    chunks = int(e2e_pick.split()[0])
+    e2e_flags = orders[e2e_pick.split(", ", 1)[1]]
+    e2e_t = e2e_times(chunks, min(args.steps, 50), e2e_flags)
     e2e_ms = max_over_ranks(world, float(np.mean(e2e_t)))
     e2e_value = world * nrays / (e2e_ms * 1e-3) / 1e6
 
@@ -1193,12 +1238,20 @@ def rays_arm(args, world, rank, local):
             "e2e": {"value": round(e2e_value, 2), "unit": "Mrays/s",
                     "h2d_bytes_per_step": int(cfg.rays.nbytes),
                     "d2h_bytes_per_step": int(nrays * 8),
-                    "path": f"qk_raycast_host, {chunks} chunks over 2 streams, pinned host buffers",
-                    "chunks_ms": {str(k): round(v, 4) for k, v in chunk_ms.items()}},
+                    "path": f"qk_raycast_host, {e2e_pick}: uploads, traversals alternating "
+                            "over two streams, read-backs, pinned host buffers",
+                    "flags": e2e_flags,
+                    "chunks_ms": {k: round(v, 4) for k, v in chunk_ms.items()}},
             "gpu_launches": None,
         }
-        # kernels of ours launched per timed step: keys + bounds + 4 sort passes x 5 + traversal
-        line["gpu_launches"] = args.steps * ((3 + 4 * 5 + 1) if best_flags & capi.QK_ORDER_MORTON else 1)
+        # kernels of ours launched per timed step: Morton = reset + bounds + keys + 4 sort
+        # passes x 5 + traversal; coherent = grid + keys + scan + scatter + traversal
+        per_step = 1
+        if best_flags & capi.QK_ORDER_MORTON:
+            per_step = 3 + 4 * 5 + 1
+        elif best_flags & capi.QK_ORDER_COHERENT:
+            per_step = 4 + 1
+        line["gpu_launches"] = args.steps * per_step
         print(json.dumps(line), flush=True)
 
 

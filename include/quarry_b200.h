@@ -50,6 +50,10 @@ extern "C" {
 #define QK_ORDER_MORTON 1u       /* QueryOrder::Morton / RayOrder::Morton (origin keys) */
 #define QK_ORDER_DIRECTION 2u    /* RayOrder::MortonDirection (direction keys) */
 #define QK_WIDE 4u               /* traverse the 4-wide nodes */
+#define QK_ORDER_COHERENT 8u     /* engine order (no quarry counterpart): a counting sort on
+                                    a Morton key of at most 15 bits over origin and direction
+                                    (rays) or position (queries); same results as input order;
+                                    batches under 64 keep input order */
 /* tuning flags (same results, different schedules; chosen by the autotuner) */
 #define QK_TUNE_DYNAMIC 256u     /* persistent warps fetching new rays as lanes finish */
 #define QK_TUNE_HIGH_OCC 512u    /* register cap for 5 resident blocks of 256 per SM */
@@ -199,16 +203,21 @@ int qk_raycast(const qk_tree* tree, const void* rays, int count, uint64_t* out, 
                uint64_t* stats, void* workspace, size_t workspace_bytes, void* stream);
 
 /* First-hit rays from host memory (the whole raycastGPU round trip, src/gpu/gpu_bvh.h:217-237):
- * rays are uploaded, traced and read back in `chunks` pieces alternating between two streams,
- * so uploads, traversal and read-backs of different pieces overlap.  host_rays / host_out
- * should be pinned (page-locked) for the copies to be asynchronous; dev_rays (count rays)
- * and dev_out (count results) are device buffers; the workspace holds two chunk
- * workspaces.  Results equal qk_raycast's.  Work is enqueued on stream0 / stream1; the
- * caller synchronises them before reading host_out. */
+ * rays are uploaded, traced and read back in `chunks` pieces: the uploads on upload_stream,
+ * the traversals alternating between trace_stream0 and trace_stream1 (a traversal can start
+ * while the one before drains), the read-backs on readback_stream, so the upload of one
+ * piece overlaps the traversal of the one before and the read-back of the one before that.
+ * host_rays / host_out should be pinned (page-locked) for the copies to be asynchronous;
+ * dev_rays (count rays) and dev_out (count results) are device buffers; the workspace holds
+ * two chunk workspaces.  Results equal qk_raycast's.  Every read-back waits for its
+ * traversal and follows the earlier read-backs, and every traversal waits for its upload,
+ * so synchronising readback_stream covers all the work before host_out is read.  The
+ * streams may coincide (the pieces then run one after another). */
 size_t qk_raycast_host_workspace_bytes(int count, int chunks);
 int qk_raycast_host(const qk_tree* tree, const void* host_rays, int count, uint64_t* host_out,
                     void* dev_rays, uint64_t* dev_out, int chunks, unsigned flags, void* workspace,
-                    size_t workspace_bytes, void* stream0, void* stream1);
+                    size_t workspace_bytes, void* upload_stream, void* trace_stream0,
+                    void* trace_stream1, void* readback_stream);
 
 /* Closest primitive per query point (closestPointGPU / closestVertexGPU /
  * closestGaussianGPU, src/gpu/gpu_bvh.h:283-330).  points: count x 3 floats; out: count

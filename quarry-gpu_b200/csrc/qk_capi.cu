@@ -59,8 +59,9 @@ int check_ws(void* ws, size_t have, size_t need) {
 int check_wide(const qk_tree* t, unsigned flags) {
     if ((flags & QK_WIDE) && (t->wide == nullptr || t->wide_count <= 0))
         return fail(QK_ERR_INVALID, "wide nodes not built");
-    if ((flags & QK_ORDER_MORTON) && (flags & QK_ORDER_DIRECTION))
-        return fail(QK_ERR_INVALID, "choose one of QK_ORDER_MORTON and QK_ORDER_DIRECTION");
+    if (__builtin_popcount(flags & (QK_ORDER_MORTON | QK_ORDER_DIRECTION | QK_ORDER_COHERENT)) > 1)
+        return fail(QK_ERR_INVALID,
+                    "choose one of QK_ORDER_MORTON, QK_ORDER_DIRECTION and QK_ORDER_COHERENT");
     return QK_OK;
 }
 
@@ -255,7 +256,8 @@ size_t qk_raycast_host_workspace_bytes(int count, int chunks) {
 
 int qk_raycast_host(const qk_tree* tree, const void* host_rays, int count, uint64_t* host_out,
                     void* dev_rays, uint64_t* dev_out, int chunks, unsigned flags, void* workspace,
-                    size_t workspace_bytes, void* stream0, void* stream1) {
+                    size_t workspace_bytes, void* upload_stream, void* trace_stream0,
+                    void* trace_stream1, void* readback_stream) {
     int st = check_tree(tree);
     if (st) return st;
     if (tree->kind != QK_TRI) return fail(QK_ERR_INVALID, "raycast needs a triangle tree");
@@ -270,26 +272,49 @@ int qk_raycast_host(const qk_tree* tree, const void* host_rays, int count, uint6
         return st;
     const int per = (count + chunks - 1) / chunks;
     const size_t half = (order_ws_bytes(per) + 255) / 256 * 256;
-    cudaStream_t ss[2] = {as_stream(stream0), as_stream(stream1)};
-    // chunk c runs on stream c % 2 with workspace half c % 2: its upload overlaps the other
-    // stream's traversal, its read-back the next upload (separate copy engines)
-    for (int c = 0; c < chunks; ++c) {
+    cudaStream_t up = as_stream(upload_stream), rb = as_stream(readback_stream);
+    cudaStream_t tr[2] = {as_stream(trace_stream0), as_stream(trace_stream1)};
+    // The uploads follow one another on the host-to-device copy engine and the read-backs on
+    // the device-to-host engine; chunk c is traced on trace stream c % 2 with workspace half
+    // c % 2, so a traversal can start while the previous one drains its last rays.  Chunk c's
+    // traversal waits for its upload, its read-back for its traversal.  A wait takes the
+    // event's latest record at the time of the call, so one event per edge serves every chunk.
+    cudaEvent_t uploaded = nullptr, traced = nullptr;
+    cudaError_t e = cudaEventCreateWithFlags(&uploaded, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&traced, cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+        if (uploaded) cudaEventDestroy(uploaded);
+        return cuda_status(e, "pipeline events");
+    }
+    for (int c = 0; c < chunks && st == QK_OK; ++c) {
         const int b = c * per;
         const int m = b + per <= count ? per : count - b;
         if (m <= 0) break;
-        cudaStream_t s = ss[c & 1];
+        cudaStream_t ts = tr[c & 1];
         void* ws = static_cast<char*>(workspace) + (c & 1) * half;
         const char* hr = static_cast<const char*>(host_rays) + static_cast<size_t>(b) * 32;
         char* dr = static_cast<char*>(dev_rays) + static_cast<size_t>(b) * 32;
-        cudaError_t e = cudaMemcpyAsync(dr, hr, static_cast<size_t>(m) * 32, cudaMemcpyHostToDevice, s);
-        if (e != cudaSuccess) return cuda_status(e, "ray upload");
-        st = ray_query(tree, dr, m, dev_out + b, nullptr, flags, nullptr, ws, s);
-        if (st) return st;
-        e = cudaMemcpyAsync(host_out + b, dev_out + b, static_cast<size_t>(m) * 8,
-                            cudaMemcpyDeviceToHost, s);
-        if (e != cudaSuccess) return cuda_status(e, "result read-back");
+        e = cudaMemcpyAsync(dr, hr, static_cast<size_t>(m) * 32, cudaMemcpyHostToDevice, up);
+        if (e == cudaSuccess) e = cudaEventRecord(uploaded, up);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(ts, uploaded, 0);
+        if (e != cudaSuccess) {
+            st = cuda_status(e, "ray upload");
+            break;
+        }
+        st = ray_query(tree, dr, m, dev_out + b, nullptr, flags, nullptr, ws, ts);
+        if (st) break;
+        e = cudaEventRecord(traced, ts);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(rb, traced, 0);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(host_out + b, dev_out + b, static_cast<size_t>(m) * 8,
+                                cudaMemcpyDeviceToHost, rb);
+        if (e != cudaSuccess) st = cuda_status(e, "result read-back");
     }
-    return QK_OK;
+    // destroying an event that pending waits still reference is allowed: its resources are
+    // released once the work completes
+    cudaEventDestroy(uploaded);
+    cudaEventDestroy(traced);
+    return st;
 }
 
 size_t qk_grad_workspace_bytes(int count, int channels) {

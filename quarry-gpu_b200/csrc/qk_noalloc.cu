@@ -68,8 +68,9 @@ extern "C" int qk_raycast_noalloc(const qk_tree* tree, const void* rays, int cou
     if (count > 0 && (!rays || !out)) return fail(QK_ERR_INVALID, "rays or out is NULL");
     if ((flags & QK_WIDE) && (tree->wide == nullptr || tree->wide_count <= 0))
         return fail(QK_ERR_INVALID, "wide nodes not built");
-    if ((flags & QK_ORDER_MORTON) && (flags & QK_ORDER_DIRECTION))
-        return fail(QK_ERR_INVALID, "choose one of QK_ORDER_MORTON and QK_ORDER_DIRECTION");
+    if (__builtin_popcount(flags & (QK_ORDER_MORTON | QK_ORDER_DIRECTION | QK_ORDER_COHERENT)) > 1)
+        return fail(QK_ERR_INVALID,
+                    "choose one of QK_ORDER_MORTON, QK_ORDER_DIRECTION and QK_ORDER_COHERENT");
     if (count == 0) return QK_OK;
     if (order_ws_bytes(count) > kNoAllocScratchBytes)
         return fail(QK_ERR_WORKSPACE, "noalloc scratch too small for %d rays", count);

@@ -98,6 +98,237 @@ __global__ __launch_bounds__(kBlock) void k_pos_keys(const float* __restrict__ p
 }
 
 // ---------------------------------------------------------------------------------------
+// Coherent order (QK_ORDER_COHERENT): a counting sort of the records on a Morton key over
+// the first `dims` floats of each record (origin xyz and direction xyz of a ray, the
+// position of a query point).  The key spans the bounds of an evenly spaced sample of the
+// records; axes whose bounds are flat or not finite are left out, and the others get b bits
+// each, b the largest with b * axes <= log2(bucket count), interleaved most significant bit
+// first.  Rays that start close together and point the same way get neighbouring threads,
+// so a warp walks fewer distinct nodes.  The key pass takes each record's rank in its bucket
+// with one atomic; the order inside a bucket follows the atomics and may differ between
+// runs, and results never depend on it (the traversal keeps the lexicographic minimum).
+// ---------------------------------------------------------------------------------------
+constexpr int kCohMaxBuckets = 1 << 15;  // one block scans them
+constexpr int kCohMinCount = 64;         // smaller batches keep input order
+constexpr int kCohSample = 4096;         // evenly spaced records whose bounds set the key
+constexpr int kCohThreads = 1024;        // the grid and scan blocks
+constexpr int kCohItems = 4;             // records per thread in the key and scatter kernels
+
+// key parameters: q_a = min((v_a - lo_a) * scale_a, 2^bits - 1) for the axes in `live`
+struct CohGrid {
+    float lo[6];
+    float scale[6];  // 2^bits / extent
+    uint32_t live;   // bit a set for an axis that takes part
+    int bits;        // bits per axis
+};
+
+// the first D floats of record i: rays are 8-float records (two 16-byte loads), query
+// points 3-float records
+template <int D>
+__device__ __forceinline__ void coh_load(const float* __restrict__ p, int i, float (&v)[6]) {
+    if constexpr (D == 6) {
+        const float4* r = reinterpret_cast<const float4*>(p) + 2 * static_cast<size_t>(i);
+        const float4 a = __ldg(r), b = __ldg(r + 1);
+        v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y;
+    } else {
+        const float* r = p + 3 * static_cast<size_t>(i);
+        v[0] = __ldg(r); v[1] = __ldg(r + 1); v[2] = __ldg(r + 2);
+        v[3] = v[4] = v[5] = 0.0f;
+    }
+}
+
+// One block: bounds of kCohSample records spaced count / kCohSample apart (records outside
+// them fall into the edge cells), then the key parameters for `key_bits` bits.
+template <int D>
+__global__ __launch_bounds__(kCohThreads) void k_coh_grid(const float* __restrict__ p, int count,
+                                                         int key_bits, CohGrid* __restrict__ g) {
+    __shared__ float part[kCohThreads / 32][12];
+    __shared__ float bound[12];
+    const int samples = min(count, kCohSample);
+    const int step = count / samples;  // samples * step <= count
+    float lo[6], hi[6];
+#pragma unroll
+    for (int a = 0; a < 6; ++a) {
+        lo[a] = kInf;
+        hi[a] = -kInf;
+    }
+#pragma unroll 4
+    for (int j = threadIdx.x; j < samples; j += kCohThreads) {
+        float v[6];
+        coh_load<D>(p, j * step, v);
+#pragma unroll
+        for (int a = 0; a < D; ++a) {
+            lo[a] = fminf(lo[a], v[a]);
+            hi[a] = fmaxf(hi[a], v[a]);
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            lo[a] = fminf(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], o));
+            hi[a] = fmaxf(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], o));
+        }
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+#pragma unroll
+        for (int a = 0; a < 6; ++a) {
+            part[warp][a] = lo[a];
+            part[warp][6 + a] = hi[a];
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < 12) {
+        const bool is_lo = threadIdx.x < 6;
+        float m = part[0][threadIdx.x];
+        for (int w = 1; w < kCohThreads / 32; ++w)
+            m = is_lo ? fminf(m, part[w][threadIdx.x]) : fmaxf(m, part[w][threadIdx.x]);
+        bound[threadIdx.x] = m;
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    uint32_t live = 0;
+    int axes = 0;
+    for (int a = 0; a < D; ++a) {
+        const float ext = bound[6 + a] - bound[a];
+        if (ext > 0.0f && ext < kInf) {
+            live |= 1u << a;
+            ++axes;
+        }
+    }
+    const int bits = axes ? min(key_bits / axes, 10) : 0;
+    for (int a = 0; a < 6; ++a) {
+        const bool on = (live >> a) & 1u;
+        g->lo[a] = on ? bound[a] : 0.0f;
+        g->scale[a] = on ? static_cast<float>(1 << bits) / (bound[6 + a] - bound[a]) : 0.0f;
+    }
+    g->live = live;
+    g->bits = bits;
+}
+
+// key of every record and its rank in its bucket (one atomic per record; the kCohItems
+// atomics of a thread are issued before any of their results is stored)
+template <int D>
+__global__ __launch_bounds__(kBlock) void k_coh_keys(const float* __restrict__ p, int count,
+                                                    const CohGrid* __restrict__ g,
+                                                    uint32_t* __restrict__ keys,
+                                                    uint32_t* __restrict__ ranks,
+                                                    uint32_t* __restrict__ hist) {
+    float lo[6], scale[6];
+#pragma unroll
+    for (int a = 0; a < 6; ++a) {
+        lo[a] = g->lo[a];
+        scale[a] = g->scale[a];
+    }
+    const uint32_t live = g->live;
+    const int bits = g->bits;
+    const float top = static_cast<float>((1 << bits) - 1);
+    const int base = blockIdx.x * (kBlock * kCohItems) + threadIdx.x;
+    uint32_t key[kCohItems], rank[kCohItems];
+#pragma unroll
+    for (int k = 0; k < kCohItems; ++k) {
+        const int i = base + k * kBlock;
+        key[k] = 0;
+        rank[k] = 0;
+        if (i < count) {
+            float v[6];
+            coh_load<D>(p, i, v);
+            uint32_t q[6];
+#pragma unroll
+            for (int a = 0; a < 6; ++a) {
+                // fmaxf / fminf also send a NaN coordinate to cell 0
+                q[a] = a < D ? static_cast<uint32_t>(
+                                   fminf(fmaxf((v[a] - lo[a]) * scale[a], 0.0f), top))
+                             : 0u;
+            }
+            uint32_t kk = 0;
+            for (int bit = bits - 1; bit >= 0; --bit) {
+#pragma unroll
+                for (int a = 0; a < D; ++a) {
+                    if ((live >> a) & 1u) kk = (kk << 1) | ((q[a] >> bit) & 1u);
+                }
+            }
+            key[k] = kk;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < kCohItems; ++k) {
+        if (base + k * kBlock < count) rank[k] = atomicAdd(&hist[key[k]], 1u);
+    }
+#pragma unroll
+    for (int k = 0; k < kCohItems; ++k) {
+        const int i = base + k * kBlock;
+        if (i < count) {
+            keys[i] = key[k];
+            ranks[i] = rank[k];
+        }
+    }
+}
+
+// exclusive scan of the bucket counts by one block (buckets <= kCohMaxBuckets): warp w
+// scans buckets [1024 w, 1024 w + 1024) in 32 coalesced steps after the warps' totals
+// have been scanned
+__global__ __launch_bounds__(kCohThreads) void k_coh_scan(uint32_t* __restrict__ hist,
+                                                         int buckets) {
+    constexpr int kWarps = kCohThreads / 32;
+    constexpr int kSteps = kCohMaxBuckets / kCohThreads;
+    __shared__ uint32_t warp_base[kWarps];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int seg = warp * (kCohMaxBuckets / kWarps);
+    uint32_t v[kSteps];
+    uint32_t tot = 0;
+#pragma unroll
+    for (int j = 0; j < kSteps; ++j) {
+        const int idx = seg + j * 32 + lane;
+        v[j] = idx < buckets ? hist[idx] : 0u;
+        tot += v[j];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
+    if (lane == 0) warp_base[warp] = tot;
+    __syncthreads();
+    if (warp == 0) {
+        const uint32_t w = warp_base[lane];
+        uint32_t inc = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += y;
+        }
+        warp_base[lane] = inc - w;
+    }
+    __syncthreads();
+    uint32_t carry = warp_base[warp];
+#pragma unroll
+    for (int j = 0; j < kSteps; ++j) {
+        uint32_t inc = v[j];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+            if (lane >= o) inc += y;
+        }
+        const int idx = seg + j * 32 + lane;
+        if (idx < buckets) hist[idx] = carry + inc - v[j];
+        carry += __shfl_sync(0xffffffffu, inc, 31);
+    }
+}
+
+// each record goes to its bucket's start plus its rank
+__global__ __launch_bounds__(kBlock) void k_coh_scatter(const uint32_t* __restrict__ keys,
+                                                       const uint32_t* __restrict__ ranks,
+                                                       int count,
+                                                       const uint32_t* __restrict__ start,
+                                                       uint32_t* __restrict__ order) {
+    const int base = blockIdx.x * (kBlock * kCohItems) + threadIdx.x;
+#pragma unroll
+    for (int k = 0; k < kCohItems; ++k) {
+        const int i = base + k * kBlock;
+        if (i < count) order[start[keys[i]] + ranks[i]] = static_cast<uint32_t>(i);
+    }
+}
+
+// ---------------------------------------------------------------------------------------
 // single-tree kernels: one thread per ray / query point, bodies in qk_traverse.cuh
 // ---------------------------------------------------------------------------------------
 template <bool kStats, int kMinBlocks, int kShort = 0, bool kLeaf4 = false>
@@ -686,9 +917,38 @@ OrderBufs carve_order(Carve& c, int count) {
 
 // Morton order of positions (stride floats apart, `offset` floats into each record);
 // returns the permutation or nullptr for input order.
+// Coherent order of the records (rays: 6 floats of origin and direction; points: 3) by the
+// counting sort above.  The buffers of the Morton sort hold it: keys in o.keys, ranks in
+// o.idx, the bucket counts and the key parameters in o.keys_s (at most count / 4 buckets,
+// so they and the 14 parameter words fit in its count words), the order in o.idx_s.
+const uint32_t* make_coherent_order(const float* pos, int stride, int count, OrderBufs& o,
+                                    cudaStream_t s, int* status) {
+    if (count < kCohMinCount || (stride != 8 && stride != 3)) return nullptr;
+    int key_bits = 4;
+    while ((2 << key_bits) <= kCohMaxBuckets && (2 << key_bits) <= count / 4) ++key_bits;
+    const int buckets = 1 << key_bits;
+    uint32_t* hist = o.keys_s;
+    CohGrid* grid = reinterpret_cast<CohGrid*>(o.keys_s + buckets);
+    cudaMemsetAsync(hist, 0, sizeof(uint32_t) * static_cast<size_t>(buckets), s);
+    const int g = blocks_for(count, kBlock * kCohItems);
+    if (stride == 8) {
+        k_coh_grid<6><<<1, kCohThreads, 0, s>>>(pos, count, key_bits, grid);
+        k_coh_keys<6><<<g, kBlock, 0, s>>>(pos, count, grid, o.keys, o.idx, hist);
+    } else {
+        k_coh_grid<3><<<1, kCohThreads, 0, s>>>(pos, count, key_bits, grid);
+        k_coh_keys<3><<<g, kBlock, 0, s>>>(pos, count, grid, o.keys, o.idx, hist);
+    }
+    k_coh_scan<<<1, kCohThreads, 0, s>>>(hist, buckets);
+    k_coh_scatter<<<g, kBlock, 0, s>>>(o.keys, o.idx, count, hist, o.idx_s);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) *status = cuda_status(e, "coherent order");
+    return o.idx_s;
+}
+
 const uint32_t* make_order(const float* pos, int stride, int offset, int count, unsigned flags,
                            OrderBufs& o, cudaStream_t s, int* status) {
     *status = QK_OK;
+    if (flags & QK_ORDER_COHERENT) return make_coherent_order(pos, stride, count, o, s, status);
     if (!(flags & (QK_ORDER_MORTON | QK_ORDER_DIRECTION))) return nullptr;
     const bool dir = (flags & QK_ORDER_DIRECTION) != 0;
     k_bounds_reset<<<1, 32, 0, s>>>(o.h, dir ? 1 : 0);

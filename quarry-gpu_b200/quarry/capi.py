@@ -20,7 +20,7 @@ LIB_PATH = HERE / "libquarry_b200.so"
 QK_OK = 0
 QK_TRI, QK_POINT, QK_GAUSS = 0, 1, 2
 QK_BUILD_LBVH, QK_BUILD_SAH = 0, 1
-QK_ORDER_MORTON, QK_ORDER_DIRECTION, QK_WIDE = 1, 2, 4
+QK_ORDER_MORTON, QK_ORDER_DIRECTION, QK_WIDE, QK_ORDER_COHERENT = 1, 2, 4, 8
 QK_TUNE_DYNAMIC, QK_TUNE_HIGH_OCC, QK_TUNE_SPLIT, QK_TUNE_SHORT_STACK = 256, 512, 1024, 2048
 QK_TUNE_LEAF4 = 4096
 QK_TUNE_STASH = 8192
@@ -109,7 +109,8 @@ EXPORTS = {
     "qk_segment_sum": (_I, [_P, _P, _I, _I, _I, _P, _P, _SZ, _P]),
     "qk_raycast_noalloc": (_I, [ctypes.POINTER(QkTree), _P, _I, _P, _U, _P]),
     "qk_raycast_host_workspace_bytes": (_SZ, [_I, _I]),
-    "qk_raycast_host": (_I, [ctypes.POINTER(QkTree), _P, _I, _P, _P, _P, _I, _U, _P, _SZ, _P, _P]),
+    "qk_raycast_host": (_I, [ctypes.POINTER(QkTree), _P, _I, _P, _P, _P, _I, _U, _P, _SZ, _P, _P,
+                             _P, _P]),
     "qk_sort_pairs": (_I, [_P, _P, _P, _P, _I, _I, _P, _SZ, _P]),
     "qk_batch_arena_bytes": (_SZ, [_I, _P, _I, _U]),
     "qk_batch_create": (_I, [_PP, _I, _P, _I, _P, _P, _SZ, _U, _P]),
@@ -350,17 +351,19 @@ class DeviceTree:
 
     def raycast_host(self, host_rays, host_out, dev_rays, dev_out, flags: int = 0,
                      chunks: int = 8, streams=None, ws=None):
-        """Pipelined host -> device -> host ray query over two streams (pinned buffers)."""
+        """Pipelined host -> device -> host ray query (pinned buffers): uploads on
+        streams[0], traversals alternating between streams[1] and [2], read-backs on
+        streams[3]; synchronise streams[3] before reading host_out."""
         torch = _torch()
         count = host_rays.shape[0]
         if streams is None:
-            streams = (torch.cuda.Stream(), torch.cuda.Stream())
+            streams = tuple(torch.cuda.Stream() for _ in range(4))
         if ws is None:
             ws = self.ws.get(lib().qk_raycast_host_workspace_bytes(count, chunks))
         check(lib().qk_raycast_host(ctypes.byref(self.t), _ptr(host_rays), count, _ptr(host_out),
                                     _ptr(dev_rays), _ptr(dev_out), chunks, flags, _ptr(ws),
-                                    ws.numel(), ctypes.c_void_p(streams[0].cuda_stream),
-                                    ctypes.c_void_p(streams[1].cuda_stream)), "qk_raycast_host")
+                                    ws.numel(), *(ctypes.c_void_p(x.cuda_stream) for x in streams)),
+              "qk_raycast_host")
         return streams
 
     def raycast_ids(self, rays, flags: int = 0):

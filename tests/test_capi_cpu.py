@@ -116,3 +116,17 @@ def test_batch_workload_sizes_are_seeded():
         assert sc.closest.shape[0] == sc.knn.shape[0] == q3 // 3
         assert sc.r > 0
         assert sc.rays.shape[0] == (q3 if sc.kind == "tri" else 0)
+
+
+def test_header_constants_match_python():
+    """Every QK_* value the header defines equals the Python module's constant of that name."""
+    import re
+
+    text = (Path(__file__).resolve().parents[1] / "include" / "quarry_b200.h").read_text()
+    defs = {m.group(1): int(m.group(2)) for m in
+            re.finditer(r"^#define (QK_\w+) (\d+)u?\b", text, re.M)}
+    assert defs["QK_ORDER_COHERENT"] == 8
+    shared = [k for k in defs if hasattr(capi, k)]
+    assert len(shared) >= 15
+    for k in shared:
+        assert getattr(capi, k) == defs[k], k

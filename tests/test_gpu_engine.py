@@ -14,7 +14,8 @@ from quarry import capi, workloads
 
 pytestmark = pytest.mark.gpu
 
-FLAG_SETS = [0, capi.QK_ORDER_MORTON, capi.QK_WIDE, capi.QK_ORDER_MORTON | capi.QK_WIDE]
+FLAG_SETS = [0, capi.QK_ORDER_MORTON, capi.QK_WIDE, capi.QK_ORDER_MORTON | capi.QK_WIDE,
+             capi.QK_ORDER_COHERENT, capi.QK_ORDER_COHERENT | capi.QK_WIDE]
 
 
 def _dev(a, dtype=np.float32):
@@ -330,18 +331,22 @@ def test_raycast_host_pipeline_matches(cuda):
                                  float(hi[2]) + 5.0, 3)
     want = tree.raycast(_dev(rays), capi.QK_ORDER_MORTON).cpu().numpy().view(np.uint64)
     host_rays = cuda.from_numpy(rays).pin_memory()
-    for chunks in (1, 3, 8):
+    one = cuda.cuda.Stream()
+    for chunks, streams in ((1, None), (3, None), (8, None), (32, None), (5, (one,) * 4)):
         host_out = cuda.zeros(len(rays), dtype=cuda.int64).pin_memory()
         dev_rays = cuda.empty((len(rays), 8), dtype=cuda.float32, device="cuda")
         dev_out = cuda.empty(len(rays), dtype=cuda.int64, device="cuda")
-        tree.raycast_host(host_rays, host_out, dev_rays, dev_out, capi.QK_ORDER_MORTON, chunks)
-        cuda.cuda.synchronize()
+        streams = tree.raycast_host(host_rays, host_out, dev_rays, dev_out,
+                                    capi.QK_ORDER_MORTON, chunks, streams)
+        # the read-back stream's last copy depends on every earlier step
+        streams[3].synchronize()
         assert np.array_equal(host_out.numpy().view(np.uint64), want)
+        cuda.cuda.synchronize()
 
 
 @pytest.mark.parametrize("tune", ["dyn", "occ", "dyn_occ", "sm", "occ_sm"])
-@pytest.mark.parametrize("morton", [False, True])
-def test_raycast_tuning_flags_same_bits(cuda, tune, morton):
+@pytest.mark.parametrize("order", [0, capi.QK_ORDER_MORTON, capi.QK_ORDER_COHERENT])
+def test_raycast_tuning_flags_same_bits(cuda, tune, order):
     tris = scenes()["city"]
     lo, hi = workloads.bounds_of(tris)
     tree = capi.DeviceTree("tri", tris, builder="sah")
@@ -351,8 +356,7 @@ def test_raycast_tuning_flags_same_bits(cuda, tune, morton):
              "dyn_occ": capi.QK_TUNE_DYNAMIC | capi.QK_TUNE_HIGH_OCC,
              "sm": capi.QK_TUNE_SHORT_STACK,
              "occ_sm": capi.QK_TUNE_HIGH_OCC | capi.QK_TUNE_SHORT_STACK}[tune]
-    if morton:
-        flags |= capi.QK_ORDER_MORTON
+    flags |= order
     rd = _dev(rays)
     want, want_ids = tree.raycast_ids(rd, 0)
     got, got_ids = tree.raycast_ids(rd, flags)
@@ -363,6 +367,44 @@ def test_raycast_tuning_flags_same_bits(cuda, tune, morton):
     tree.raycast(rd, 0, stats=base)
     # same traversal per ray: identical node and triangle test counts
     assert stats[:3].tolist() == base[:3].tolist()
+
+
+@pytest.mark.parametrize("count", [0, 1, 63, 64, 65, 8191, 8192, 70_001])
+def test_coherent_order_same_bits(cuda, count):
+    """QK_ORDER_COHERENT (a counting sort on origin / direction or position keys) returns the
+    input order's bits for rays, closest, kNN and radius: below 64 records (input order), at
+    the bucket-count steps, with flat axes (a common origin; identical query points) and
+    with non-finite coordinates in the batch."""
+    tris = scenes()["city"]
+    lo, hi = workloads.bounds_of(tris)
+    tree = capi.DeviceTree("tri", tris, builder="sah")
+    rays = workloads.cosine_rays(max(count, 1), float(lo[0]), float(hi[0]), float(lo[1]),
+                                 float(hi[1]), float(hi[2]) + 5.0, 5)[:count]
+    rng = np.random.default_rng(count)
+    pts = rng.uniform(lo - 2, hi + 2, (count, 3)).astype(np.float32)
+    if count >= 64:
+        rays[: count // 3, :3] = rays[0, :3]   # a third share one origin
+        pts[: count // 4] = pts[0]            # a quarter of the queries coincide
+        rays[1, 0] = np.nan
+        pts[2, 1] = np.inf
+    variants = [(rays, pts)]
+    if count >= 64:
+        flat = rays.copy()
+        flat[:, :3] = flat[0, :3]             # every origin equal: three flat axes
+        same = np.repeat(pts[:1], count, axis=0)
+        variants.append((flat, same))
+    for r, p in variants:
+        rd, pd = _dev(r), _dev(p)
+        assert cuda.equal(tree.raycast(rd, capi.QK_ORDER_COHERENT), tree.raycast(rd, 0))
+        assert cuda.equal(tree.raycast(rd, capi.QK_ORDER_COHERENT | capi.QK_TUNE_DYNAMIC),
+                          tree.raycast(rd, 0))
+        if count == 0:
+            continue
+        assert cuda.equal(tree.closest(pd, capi.QK_ORDER_COHERENT), tree.closest(pd, 0))
+        assert cuda.equal(tree.knn(pd, 4, capi.QK_ORDER_COHERENT), tree.knn(pd, 4, 0))
+        want = tree.radius(pd, 3.0, 0)
+        got = tree.radius(pd, 3.0, capi.QK_ORDER_COHERENT | capi.QK_TUNE_STASH)
+        assert all(cuda.equal(a, b) for a, b in zip(got, want))
 
 
 @pytest.mark.parametrize("kind", ["tri", "point", "gauss"])

@@ -310,7 +310,9 @@ def grad_arm(args, world, rank, local):
     state["tree"].build_wide()
     fwd_variants = {"morton": capi.QK_ORDER_MORTON, "input": 0,
                     "split_morton": capi.QK_ORDER_MORTON | capi.QK_TUNE_SPLIT,
-                    "wide_morton": capi.QK_ORDER_MORTON | capi.QK_WIDE}
+                    "wide_morton": capi.QK_ORDER_MORTON | capi.QK_WIDE,
+                    "coherent": capi.QK_ORDER_COHERENT,
+                    "wide_coherent": capi.QK_ORDER_COHERENT | capi.QK_WIDE}
     base = state["tree"].closest(q, 0).clone()
     fwd_by = {}
     for name, f in fwd_variants.items():
@@ -330,12 +332,28 @@ def grad_arm(args, world, rank, local):
     rays = capi.to_device(w.down_rays(nr, 0.0, float(grid), 0.0, float(grid), 100.0, 1), np.float32)
     tri_tree = capi.DeviceTree("tri", tris)
 
+    ray_flags = {"morton": capi.QK_ORDER_MORTON, "coherent": capi.QK_ORDER_COHERENT}
+    state["rflags"] = capi.QK_ORDER_MORTON
+
     def r_fwd():
-        state["out"], state["ids"] = tri_tree.raycast_ids(rays, capi.QK_ORDER_MORTON)
+        state["out"], state["ids"] = tri_tree.raycast_ids(rays, state["rflags"])
 
     def r_bwd():
         state["rg"] = tri_tree.ray_t_grad(rays, state["ids"], None, with_rays=False)
 
+    # the ray order is chosen by measurement too (same hits and ids for both)
+    r_by, r_base = {}, None
+    for name, f in ray_flags.items():
+        state["rflags"] = f
+        r_fwd()
+        got = (state["out"].clone(), state["ids"].clone())
+        if r_base is None:
+            r_base = got
+        elif not (torch.equal(got[0], r_base[0]) and torch.equal(got[1], r_base[1])):
+            raise RuntimeError(f"ray order {name} differs")
+        r_by[name] = timed(r_fwd, 5)
+    ray_order = min(r_by, key=r_by.get)
+    state["rflags"] = ray_flags[ray_order]
     r_fwd()
     rf_ms = timed(r_fwd, 10)
     rb_ms = timed(r_bwd, 10)
@@ -347,7 +365,8 @@ def grad_arm(args, world, rank, local):
                 "dtype": "f32 forward, f64 adjoint", "data": "synthetic (seeded generators)",
                 "config": {"workload": "gaussian distance + ray t gradients", "gaussians": ng,
                            "queries": nq, "rays": nr, "terrain_grid": grid,
-                           "order": "morton", "l2": "flushed between timed steps"},
+                           "order": "fastest of the variants below",
+                           "l2": "flushed between timed steps"},
                 "gaussian": {"build_ms": round(build_ms, 3), "forward_ms": round(fwd_ms, 4),
                              "forward_variant": fwd_variant,
                              "forward_variants_ms": {k: round(v, 4) for k, v in fwd_by.items()},
@@ -355,6 +374,8 @@ def grad_arm(args, world, rank, local):
                              "fwd_bwd_over_fwd": round((fwd_ms + bwd_ms) / fwd_ms, 4),
                              "mqueries_per_s": round(nq / (fwd_ms * 1e-3) / 1e6, 2)},
                 "rays": {"forward_ms": round(rf_ms, 4), "backward_ms": round(rb_ms, 4),
+                         "order": ray_order,
+                         "forward_orders_ms": {k: round(v, 4) for k, v in r_by.items()},
                          "fwd_bwd_over_fwd": round((rf_ms + rb_ms) / rf_ms, 4)}}
         print(json.dumps(line), flush=True)
 
@@ -1155,11 +1176,20 @@ def rays_arm(args, world, rank, local):
     dev_rays = torch.empty((nrays, 8), dtype=torch.float32, device=dev)
     streams = tuple(torch.cuda.Stream() for _ in range(4))
 
-    def e2e_times(chunks, steps, flags):
-        ws = torch.empty(capi.lib().qk_raycast_host_workspace_bytes(nrays, chunks),
-                         dtype=torch.uint8, device=dev)
-        for _ in range(3):
+    def e2e_call(chunks, flags, ws):
+        if chunks == 0:
+            # zero-copy: the traversal reads the pinned rays and writes the pinned results
+            with torch.cuda.stream(streams[0]):
+                tree.raycast_mapped(host_rays, host_out, flags, ws)
+        else:
             tree.raycast_host(host_rays, host_out, dev_rays, out, flags, chunks, streams, ws)
+
+    def e2e_times(chunks, steps, flags):
+        nb = (capi.lib().qk_query_workspace_bytes(nrays, flags) if chunks == 0 else
+              capi.lib().qk_raycast_host_workspace_bytes(nrays, chunks))
+        ws = torch.empty(nb, dtype=torch.uint8, device=dev)
+        for _ in range(3):
+            e2e_call(chunks, flags, ws)
         torch.cuda.synchronize()
         ts = []
         for _ in range(steps):
@@ -1169,7 +1199,7 @@ def rays_arm(args, world, rank, local):
             e0.record(streams[0])
             for x in streams[1:]:
                 x.wait_event(e0)
-            tree.raycast_host(host_rays, host_out, dev_rays, out, flags, chunks, streams, ws)
+            e2e_call(chunks, flags, ws)
             ends = [torch.cuda.Event(enable_timing=True) for _ in streams]
             for ev, x in zip(ends, streams):
                 ev.record(x)
@@ -1177,16 +1207,20 @@ def rays_arm(args, world, rank, local):
             ts.append(max(e0.elapsed_time(ev) for ev in ends))
         return ts
 
-    # the chunk count and the ray order of the pipeline are chosen by measurement (same bits
-    # for every choice): per chunk, an order costs a fixed few tens of microseconds
+    # the transfer scheme (copy pipeline with 2-16 chunks, or zero-copy through mapped pinned
+    # memory) and the ray order are chosen by measurement (same bits for every choice): per
+    # chunk, an order costs a fixed few tens of microseconds
     orders = {"timed variant": best_flags,
               "input order": best_flags & ~(capi.QK_ORDER_MORTON | capi.QK_ORDER_COHERENT)}
-    chunk_ms = {f"{c} chunks, {o}": float(np.median(e2e_times(c, 10, f)))
-                for o, f in orders.items() for c in (2, 4, 8, 16)}
+    schemes = {"zero-copy": 0, **{f"{c} chunks": c for c in (2, 4, 8, 16)}}
+    chunk_ms = {f"{sc}, {o}": float(np.median(e2e_times(c, 10, f)))
+                for o, f in orders.items() for sc, c in schemes.items()}
     e2e_pick = min(chunk_ms, key=chunk_ms.get)
-    chunks = int(e2e_pick.split()[0])
+    chunks = schemes[e2e_pick.split(", ")[0]]
     e2e_flags = orders[e2e_pick.split(", ", 1)[1]]
     e2e_t = e2e_times(chunks, min(args.steps, 50), e2e_flags)
+    if not np.array_equal(host_out.numpy(), tree.raycast(rays_d, 0).cpu().numpy()):
+        raise RuntimeError("e2e results differ from the device-resident run")
     e2e_ms = max_over_ranks(world, float(np.mean(e2e_t)))
     e2e_value = world * nrays / (e2e_ms * 1e-3) / 1e6
 
@@ -1238,8 +1272,10 @@ def rays_arm(args, world, rank, local):
             "e2e": {"value": round(e2e_value, 2), "unit": "Mrays/s",
                     "h2d_bytes_per_step": int(cfg.rays.nbytes),
                     "d2h_bytes_per_step": int(nrays * 8),
-                    "path": f"qk_raycast_host, {e2e_pick}: uploads, traversals alternating "
-                            "over two streams, read-backs, pinned host buffers",
+                    "path": (f"qk_raycast_mapped, {e2e_pick}: the traversal reads pinned "
+                             "host rays and writes pinned host results" if chunks == 0 else
+                             f"qk_raycast_host, {e2e_pick}: uploads, traversals alternating "
+                             "over two streams, read-backs, pinned host buffers"),
                     "flags": e2e_flags,
                     "chunks_ms": {k: round(v, 4) for k, v in chunk_ms.items()}},
             "gpu_launches": None,

@@ -219,6 +219,17 @@ int qk_raycast_host(const qk_tree* tree, const void* host_rays, int count, uint6
                     size_t workspace_bytes, void* upload_stream, void* trace_stream0,
                     void* trace_stream1, void* readback_stream);
 
+/* First-hit rays read from and written to page-locked host memory by the traversal kernel
+ * itself (zero-copy; the rest of the raycastGPU round trip, src/gpu/gpu_bvh.h:217-237): each
+ * ray crosses the host link once, as the thread that traces it loads it, and each result
+ * once, as it is stored, so transfers and traversal overlap inside one launch.  host_rays
+ * and host_out must be page-locked memory mapped into the device's address space (pinned
+ * allocations under unified addressing are); anything else returns QK_ERR_INVALID before
+ * any launch.  Flags and workspace as qk_raycast; an order flag makes the key pass read the
+ * rays over the link too.  Results equal qk_raycast's once the stream is synchronised. */
+int qk_raycast_mapped(const qk_tree* tree, const void* host_rays, int count, uint64_t* host_out,
+                      unsigned flags, void* workspace, size_t workspace_bytes, void* stream);
+
 /* Closest primitive per query point (closestPointGPU / closestVertexGPU /
  * closestGaussianGPU, src/gpu/gpu_bvh.h:283-330).  points: count x 3 floats; out: count
  * query results. */

@@ -247,6 +247,38 @@ int qk_raycast_ids(const qk_tree* tree, const void* rays, int count, uint64_t* o
     return ray_query(tree, rays, count, out, ids, flags, nullptr, workspace, as_stream(stream));
 }
 
+namespace {
+// device alias of page-locked, mapped host memory, or nullptr
+void* mapped_alias(const void* host) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, host) != cudaSuccess) {
+        cudaGetLastError();  // clear the (non-sticky) error the query left
+        return nullptr;
+    }
+    return a.type == cudaMemoryTypeHost ? a.devicePointer : nullptr;
+}
+}  // namespace
+
+int qk_raycast_mapped(const qk_tree* tree, const void* host_rays, int count, uint64_t* host_out,
+                      unsigned flags, void* workspace, size_t workspace_bytes, void* stream) {
+    int st = check_tree(tree);
+    if (st) return st;
+    if (tree->kind != QK_TRI) return fail(QK_ERR_INVALID, "raycast needs a triangle tree");
+    if (count < 0) return fail(QK_ERR_INVALID, "negative ray count");
+    if (count == 0) return QK_OK;
+    if (!host_rays || !host_out) return fail(QK_ERR_INVALID, "rays or out is NULL");
+    void* rays_d = mapped_alias(host_rays);
+    void* out_d = mapped_alias(host_out);
+    if (!rays_d || !out_d)
+        return fail(QK_ERR_INVALID, "host_rays and host_out must be page-locked, mapped host memory");
+    if ((reinterpret_cast<uintptr_t>(rays_d) & 15u) || (reinterpret_cast<uintptr_t>(out_d) & 7u))
+        return fail(QK_ERR_INVALID, "rays must be 16-byte and results 8-byte aligned");
+    if ((st = check_wide(tree, flags))) return st;
+    if ((st = check_ws(workspace, workspace_bytes, order_ws_bytes(count)))) return st;
+    return ray_query(tree, rays_d, count, static_cast<uint64_t*>(out_d), nullptr, flags, nullptr,
+                     workspace, as_stream(stream));
+}
+
 size_t qk_raycast_host_workspace_bytes(int count, int chunks) {
     if (count <= 0) return 0;
     if (chunks < 1) chunks = 1;

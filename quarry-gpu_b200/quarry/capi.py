@@ -108,6 +108,7 @@ EXPORTS = {
     "qk_ray_t_grad": (_I, [ctypes.POINTER(QkTree), _P, _P, _P, _P, _I, _P, _P, _P, _SZ, _P]),
     "qk_segment_sum": (_I, [_P, _P, _I, _I, _I, _P, _P, _SZ, _P]),
     "qk_raycast_noalloc": (_I, [ctypes.POINTER(QkTree), _P, _I, _P, _U, _P]),
+    "qk_raycast_mapped": (_I, [ctypes.POINTER(QkTree), _P, _I, _P, _U, _P, _SZ, _P]),
     "qk_raycast_host_workspace_bytes": (_SZ, [_I, _I]),
     "qk_raycast_host": (_I, [ctypes.POINTER(QkTree), _P, _I, _P, _P, _P, _I, _U, _P, _SZ, _P, _P,
                              _P, _P]),
@@ -348,6 +349,16 @@ class DeviceTree:
         check(lib().qk_raycast(ctypes.byref(self.t), _ptr(rays), count, _ptr(out), flags,
                                _ptr(stats), _ptr(w), w.numel(), _stream()), "qk_raycast")
         return out
+
+    def raycast_mapped(self, host_rays, host_out, flags: int = 0, ws=None):
+        """Zero-copy ray query: the traversal reads pinned host rays and writes pinned host
+        results directly; synchronise the current stream before reading host_out."""
+        count = host_rays.shape[0]
+        w = ws if ws is not None else self.ws.get(lib().qk_query_workspace_bytes(count, flags))
+        check(lib().qk_raycast_mapped(ctypes.byref(self.t), _ptr(host_rays), count,
+                                      _ptr(host_out), flags, _ptr(w), w.numel(), _stream()),
+              "qk_raycast_mapped")
+        return host_out
 
     def raycast_host(self, host_rays, host_out, dev_rays, dev_out, flags: int = 0,
                      chunks: int = 8, streams=None, ws=None):

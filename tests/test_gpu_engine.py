@@ -344,6 +344,29 @@ def test_raycast_host_pipeline_matches(cuda):
         cuda.cuda.synchronize()
 
 
+def test_raycast_mapped_matches(cuda):
+    """Zero-copy rays: the traversal reads pinned host rays and writes pinned host results;
+    same bits as the device-resident call for input, Morton and coherent order; pageable
+    memory is refused before any launch."""
+    tris = scenes()["city"]
+    lo, hi = workloads.bounds_of(tris)
+    tree = capi.DeviceTree("tri", tris, builder="sah")
+    rays = workloads.cosine_rays(40_001, float(lo[0]), float(hi[0]), float(lo[1]), float(hi[1]),
+                                 float(hi[2]) + 5.0, 9)
+    want = tree.raycast(_dev(rays), 0).cpu().numpy()
+    host_rays = cuda.from_numpy(rays).pin_memory()
+    for flags in (0, capi.QK_ORDER_MORTON, capi.QK_ORDER_COHERENT | capi.QK_TUNE_HIGH_OCC):
+        host_out = cuda.zeros(len(rays), dtype=cuda.int64).pin_memory()
+        tree.raycast_mapped(host_rays, host_out, flags)
+        cuda.cuda.synchronize()
+        assert np.array_equal(host_out.numpy(), want)
+    pageable = cuda.zeros(len(rays), dtype=cuda.int64)
+    with pytest.raises(RuntimeError):
+        tree.raycast_mapped(cuda.from_numpy(rays), pageable, 0)
+    with pytest.raises(RuntimeError):
+        tree.raycast_mapped(host_rays, pageable, 0)
+
+
 @pytest.mark.parametrize("tune", ["dyn", "occ", "dyn_occ", "sm", "occ_sm"])
 @pytest.mark.parametrize("order", [0, capi.QK_ORDER_MORTON, capi.QK_ORDER_COHERENT])
 def test_raycast_tuning_flags_same_bits(cuda, tune, order):

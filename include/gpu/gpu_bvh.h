@@ -138,7 +138,8 @@ void destroyBVHGPU(GpuBVH& bvh);
 GpuRayBuffer uploadRaysGPU(const std::vector<Ray>& rays);
 void destroyRayBufferGPU(GpuRayBuffer& buf);
 
-enum class RayOrder { Input, Morton, MortonDirection };
+// Coherent (engine addition): counting sort on a Morton key of origin and direction
+enum class RayOrder { Input, Morton, MortonDirection, Coherent };
 
 // 4-wide collapse; call again after a refit (the reference contract).  Returns ms.
 double buildWideNodesGPU(GpuBVH& bvh);
@@ -178,7 +179,8 @@ struct GpuQueryStats {
     double sortMs = 0.0;
 };
 
-enum class QueryOrder { Input, Morton };
+// Coherent (engine addition): counting sort on a Morton key of the position
+enum class QueryOrder { Input, Morton, Coherent };
 
 GpuPointBuffer uploadPointsGPU(const std::vector<Vec3>& points, int resultsPerPoint = 1);
 void destroyPointBufferGPU(GpuPointBuffer& buf);

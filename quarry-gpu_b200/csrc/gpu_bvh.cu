@@ -410,7 +410,8 @@ QueryWs queryWs(void* scratch, int count) {
 }
 
 unsigned flagsOf(QueryOrder order, bool wide) {
-    return (order == QueryOrder::Morton ? QK_ORDER_MORTON : 0u) | (wide ? QK_WIDE : 0u);
+    return (order == QueryOrder::Morton ? QK_ORDER_MORTON : 0u) |
+           (order == QueryOrder::Coherent ? QK_ORDER_COHERENT : 0u) | (wide ? QK_WIDE : 0u);
 }
 
 void requireWide(const GpuBVH& bvh, bool wide, const char* who) {
@@ -685,6 +686,7 @@ double raycastGPU(const GpuBVH& bvh, GpuRayBuffer& buf, bool collectStats, RayOr
     unsigned flags = wide ? QK_WIDE : 0u;
     if (order == RayOrder::Morton) flags |= QK_ORDER_MORTON;
     if (order == RayOrder::MortonDirection) flags |= QK_ORDER_DIRECTION;
+    if (order == RayOrder::Coherent) flags |= QK_ORDER_COHERENT;
     if (collectStats) cudaOk(cudaMemset(w.stats, 0, 32), "stats");
     Timer timer;
     qkOk(qk_raycast(&im->t, buf.d_rays, buf.count, static_cast<uint64_t*>(buf.d_results), flags,

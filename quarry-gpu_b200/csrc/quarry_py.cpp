@@ -6,8 +6,8 @@
 // float32 / int32 numpy arrays (cast when needed), results come back as numpy arrays, the
 // GIL is released around device work, bad input raises ValueError (std::invalid_argument)
 // and CUDA failures RuntimeError.  Additive over the reference: wide=True on every query
-// (4-wide traversal, built on first use) and order= on raycast ("input", "morton",
-// "direction").
+// (4-wide traversal, built on first use), order= on raycast ("input", "morton",
+// "direction", "coherent") and order="coherent" on the point queries.
 #include <pybind11/numpy.h>
 #include <pybind11/pybind11.h>
 
@@ -32,14 +32,16 @@ enum class Leaf { Tri, Point, Gauss };
 QueryOrder queryOrder(const std::string& s) {
     if (s == "input") return QueryOrder::Input;
     if (s == "morton") return QueryOrder::Morton;
-    throw std::invalid_argument("order must be 'input' or 'morton'");
+    if (s == "coherent") return QueryOrder::Coherent;
+    throw std::invalid_argument("order must be 'input', 'morton' or 'coherent'");
 }
 
 RayOrder rayOrder(const std::string& s) {
     if (s == "input") return RayOrder::Input;
     if (s == "morton") return RayOrder::Morton;
     if (s == "direction") return RayOrder::MortonDirection;
-    throw std::invalid_argument("order must be 'input', 'morton' or 'direction'");
+    if (s == "coherent") return RayOrder::Coherent;
+    throw std::invalid_argument("order must be 'input', 'morton', 'direction' or 'coherent'");
 }
 
 bool sahBuilder(const std::string& s) {

@@ -57,7 +57,8 @@ def test_scene_basics_and_queries(mesh):
     assert np.array_equal(off, woff)
     assert np.array_equal(_bits(rd2), (wkeys >> np.uint64(32)).astype(np.uint32))
     # order / builder / wide invariance, bit for bit
-    for kw in ({"order": "morton"}, {"wide": True}, {"order": "morton", "wide": True}):
+    for kw in ({"order": "morton"}, {"wide": True}, {"order": "morton", "wide": True},
+               {"order": "coherent"}, {"order": "coherent", "wide": True}):
         m_d2, m_tri = scene.closest(pts, **kw)
         assert np.array_equal(_bits(m_d2), _bits(d2)) and np.array_equal(m_tri, tri)
         m_kd, m_kid = scene.knn(pts, 4, **kw)
@@ -80,7 +81,8 @@ def test_scene_basics_and_queries(mesh):
     assert np.array_equal(hit, (want >> np.uint64(32)) != 0)
     assert np.array_equal(_bits(t[hit]), (want[hit] & np.uint64(0xFFFFFFFF)).astype(np.uint32))
     assert np.all(np.isinf(t[~hit]))
-    for kw in ({"order": "morton"}, {"order": "direction"}, {"wide": True}):
+    for kw in ({"order": "morton"}, {"order": "direction"}, {"wide": True},
+               {"order": "coherent"}, {"order": "coherent", "wide": True}):
         h2, t2 = scene.raycast(origins, dirs, **kw)
         assert np.array_equal(h2, hit) and np.array_equal(_bits(t2), _bits(t))
 

@@ -1181,12 +1181,15 @@ def rays_arm(args, world, rank, local):
             # zero-copy: the traversal reads the pinned rays and writes the pinned results
             with torch.cuda.stream(streams[0]):
                 tree.raycast_mapped(host_rays, host_out, flags, ws)
+        elif chunks < 0:
+            # copy pipeline for the rays; the traversals store results into pinned host_out
+            tree.raycast_host(host_rays, host_out, dev_rays, None, flags, -chunks, streams, ws)
         else:
             tree.raycast_host(host_rays, host_out, dev_rays, out, flags, chunks, streams, ws)
 
     def e2e_times(chunks, steps, flags):
         nb = (capi.lib().qk_query_workspace_bytes(nrays, flags) if chunks == 0 else
-              capi.lib().qk_raycast_host_workspace_bytes(nrays, chunks))
+              capi.lib().qk_raycast_host_workspace_bytes(nrays, abs(chunks)))
         ws = torch.empty(nb, dtype=torch.uint8, device=dev)
         for _ in range(3):
             e2e_call(chunks, flags, ws)
@@ -1212,12 +1215,14 @@ def rays_arm(args, world, rank, local):
     # chunk, an order costs a fixed few tens of microseconds
     orders = {"timed variant": best_flags,
               "input order": best_flags & ~(capi.QK_ORDER_MORTON | capi.QK_ORDER_COHERENT)}
-    schemes = {"zero-copy": 0, **{f"{c} chunks": c for c in (2, 4, 8, 16)}}
+    schemes = {"zero-copy": 0, **{f"{c} chunks": c for c in (2, 4, 8, 16)},
+               **{f"{c} chunks, results stored to host": -c for c in (4, 8, 16)}}
     chunk_ms = {f"{sc}, {o}": float(np.median(e2e_times(c, 10, f)))
                 for o, f in orders.items() for sc, c in schemes.items()}
     e2e_pick = min(chunk_ms, key=chunk_ms.get)
-    chunks = schemes[e2e_pick.split(", ")[0]]
-    e2e_flags = orders[e2e_pick.split(", ", 1)[1]]
+    scheme, order_name = e2e_pick.rsplit(", ", 1)
+    chunks = schemes[scheme]
+    e2e_flags = orders[order_name]
     e2e_t = e2e_times(chunks, min(args.steps, 50), e2e_flags)
     if not np.array_equal(host_out.numpy(), tree.raycast(rays_d, 0).cpu().numpy()):
         raise RuntimeError("e2e results differ from the device-resident run")
@@ -1275,7 +1280,9 @@ def rays_arm(args, world, rank, local):
                     "path": (f"qk_raycast_mapped, {e2e_pick}: the traversal reads pinned "
                              "host rays and writes pinned host results" if chunks == 0 else
                              f"qk_raycast_host, {e2e_pick}: uploads, traversals alternating "
-                             "over two streams, read-backs, pinned host buffers"),
+                             "over two streams, "
+                             + ("results stored by the traversals into pinned host memory"
+                                if chunks < 0 else "read-backs, pinned host buffers")),
                     "flags": e2e_flags,
                     "chunks_ms": {k: round(v, 4) for k, v in chunk_ms.items()}},
             "gpu_launches": None,

@@ -208,8 +208,10 @@ int qk_raycast(const qk_tree* tree, const void* rays, int count, uint64_t* out, 
  * while the one before drains), the read-backs on readback_stream, so the upload of one
  * piece overlaps the traversal of the one before and the read-back of the one before that.
  * host_rays / host_out should be pinned (page-locked) for the copies to be asynchronous;
- * dev_rays (count rays) and dev_out (count results) are device buffers; the workspace holds
- * two chunk workspaces.  Results equal qk_raycast's.  Every read-back waits for its
+ * dev_rays (count rays) and dev_out (count results) are device buffers.  dev_out may be
+ * NULL when host_out is mapped page-locked memory: the traversals then store the results
+ * straight into host_out and no read-back copies run (readback_stream still waits for every
+ * traversal).  The workspace holds two chunk workspaces.  Results equal qk_raycast's.  Every read-back waits for its
  * traversal and follows the earlier read-backs, and every traversal waits for its upload,
  * so synchronising readback_stream covers all the work before host_out is read.  The
  * streams may coincide (the pieces then run one after another). */

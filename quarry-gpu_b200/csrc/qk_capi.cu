@@ -295,8 +295,16 @@ int qk_raycast_host(const qk_tree* tree, const void* host_rays, int count, uint6
     if (tree->kind != QK_TRI) return fail(QK_ERR_INVALID, "raycast needs a triangle tree");
     if (count < 0) return fail(QK_ERR_INVALID, "negative ray count");
     if (count == 0) return QK_OK;
-    if (!host_rays || !host_out || !dev_rays || !dev_out)
+    if (!host_rays || !host_out || !dev_rays)
         return fail(QK_ERR_INVALID, "a ray or result buffer is NULL");
+    // without dev_out the traversals store the results straight into mapped host_out
+    uint64_t* direct = nullptr;
+    if (!dev_out) {
+        direct = static_cast<uint64_t*>(mapped_alias(host_out));
+        if (!direct || (reinterpret_cast<uintptr_t>(direct) & 7u))
+            return fail(QK_ERR_INVALID,
+                        "dev_out is NULL but host_out is not 8-byte aligned, mapped page-locked memory");
+    }
     if ((st = check_wide(tree, flags))) return st;
     if (chunks < 1) chunks = 1;
     if (chunks > count) chunks = count;
@@ -333,11 +341,12 @@ int qk_raycast_host(const qk_tree* tree, const void* host_rays, int count, uint6
             st = cuda_status(e, "ray upload");
             break;
         }
-        st = ray_query(tree, dr, m, dev_out + b, nullptr, flags, nullptr, ws, ts);
+        st = ray_query(tree, dr, m, (direct ? direct : dev_out) + b, nullptr, flags, nullptr, ws,
+                       ts);
         if (st) break;
         e = cudaEventRecord(traced, ts);
         if (e == cudaSuccess) e = cudaStreamWaitEvent(rb, traced, 0);
-        if (e == cudaSuccess)
+        if (e == cudaSuccess && !direct)
             e = cudaMemcpyAsync(host_out + b, dev_out + b, static_cast<size_t>(m) * 8,
                                 cudaMemcpyDeviceToHost, rb);
         if (e != cudaSuccess) st = cuda_status(e, "result read-back");

@@ -342,6 +342,14 @@ def test_raycast_host_pipeline_matches(cuda):
         streams[3].synchronize()
         assert np.array_equal(host_out.numpy().view(np.uint64), want)
         cuda.cuda.synchronize()
+        # without dev_out the traversals store into the pinned host_out themselves
+        host_out.zero_()
+        streams = tree.raycast_host(host_rays, host_out, dev_rays, None, 0, chunks, streams)
+        streams[3].synchronize()
+        assert np.array_equal(host_out.numpy().view(np.uint64), want)
+        cuda.cuda.synchronize()
+    with pytest.raises(RuntimeError):  # pageable host_out cannot take direct stores
+        tree.raycast_host(host_rays, cuda.zeros(len(rays), dtype=cuda.int64), dev_rays, None, 0, 4)
 
 
 def test_raycast_mapped_matches(cuda):

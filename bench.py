@@ -1126,9 +1126,12 @@ def rays_arm(args, world, rank, local):
     k_out = torch.empty((q_d.shape[0], 8, 2), dtype=torch.int32, device=dev)
     knn_base = tree.knn(q_d, 8, 0).clone()
     knn_ms_by = {}
-    for kname, kf in (("layout_of_rays", best_flags & (capi.QK_WIDE | capi.QK_ORDER_MORTON)),
+    for kname, kf in (("layout_of_rays", best_flags & (capi.QK_WIDE | capi.QK_ORDER_MORTON |
+                                                       capi.QK_ORDER_COHERENT)),
+                      ("input", 0),
                       ("split", capi.QK_TUNE_SPLIT),
                       ("split_morton", capi.QK_TUNE_SPLIT | capi.QK_ORDER_MORTON),
+                      ("split_coherent", capi.QK_TUNE_SPLIT | capi.QK_ORDER_COHERENT),
                       ("leaf4", capi.QK_TUNE_LEAF4),
                       ("leaf4_morton", capi.QK_TUNE_LEAF4 | capi.QK_ORDER_MORTON)):
         for _ in range(3):

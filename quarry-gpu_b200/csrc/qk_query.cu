@@ -62,11 +62,24 @@ __global__ __launch_bounds__(kBlock) void k_pos_bounds(const float* __restrict__
             hi[a] = fmaxf(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], o));
         }
     }
-    if ((threadIdx.x & 31) == 0) {
+    // one atomic per block and bound: the warps' partial bounds meet in shared memory first
+    // (thousands of warps hitting six words serialise at the L2)
+    __shared__ float part[kBlock / 32][6];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) {
         for (int a = 0; a < 3; ++a) {
-            atomicMin(&h->lo[a], ord_f(lo[a]));
-            atomicMax(&h->hi[a], ord_f(hi[a]));
+            part[warp][a] = lo[a];
+            part[warp][3 + a] = hi[a];
         }
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        const int a = threadIdx.x % 3;
+        float m = part[0][threadIdx.x];
+        for (int w = 1; w < kBlock / 32; ++w)
+            m = threadIdx.x < 3 ? fminf(m, part[w][threadIdx.x]) : fmaxf(m, part[w][threadIdx.x]);
+        if (threadIdx.x < 3) atomicMin(&h->lo[a], ord_f(m));
+        else atomicMax(&h->hi[a], ord_f(m));
     }
 }
 

@@ -1118,6 +1118,10 @@ def rays_arm(args, world, rank, local):
                            "k_ray_bin_dyn" if trav_flags & capi.QK_TUNE_DYNAMIC else "k_ray_bin"),
                 "tree": best_builder,
                 "kernel_ms": round(kernel_ms, 4),
+                "kernel_timing": ("the traversal alone, CUDA events, on rays already in the "
+                                  "variant's order (contiguous)"),
+                # the same bytes over the whole timed step (ordering kernels included)
+                "frac_step": round(bytes_per_ray * nrays / (ms * 1e-3) / 1e9 / pk["hbm_gbs"], 4),
                 "bytes_per_ray": round(bytes_per_ray, 1),
                 "canonical_counts": {"node_tests_per_ray": round(node_tests / nrays, 3),
                                      "tri_tests_per_ray": round(p_leaf, 3)}}

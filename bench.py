@@ -1069,8 +1069,8 @@ def rays_arm(args, world, rank, local):
     value = world * nrays / (ms * 1e-3) / 1e6
 
     # ---- roofline: traversal kernel alone on pre-sorted rays ----
-    # the engine's Morton order, recomputed on the host (quantize10 of src/gpu/morton.h), so
-    # the kernel alone can be timed on rays that are already in that order
+    # the engine's coherent or Morton order (quantize10 of src/gpu/morton.h), recomputed on
+    # the host, so the kernel alone can be timed on rays that are already in that order
     trav_flags = best_flags & ~(capi.QK_ORDER_MORTON | capi.QK_ORDER_COHERENT)
     if best_flags & capi.QK_ORDER_COHERENT:
         sorted_rays = capi.to_device(cfg.rays[coherent_order(cfg.rays)], np.float32)

@@ -1267,6 +1267,7 @@ def rays_arm(args, world, rank, local):
         line = {
             "metric": METRIC, "value": round(value, 2), "unit": "Mrays/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 4),
+            "median_ms_per_step": round(float(np.median(step_ms)), 4),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded generators, identical bytes on every host)",
             "config": {**desc, "builder": best_builder, "sah_bins": 32, "variant": best,

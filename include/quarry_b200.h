@@ -304,9 +304,10 @@ int qk_segment_sum(const int32_t* keys, const float* values, int count, int chan
  * forbids later allocations, or code without an allocator): same results as qk_raycast with
  * the same flags, but the Morton-order scratch lives in a fixed array inside this library
  * (4.5 MB per GPU that loads it, held until exit), so no workspace is passed.  At most
- * 262,144 rays per call; larger counts return QK_ERR_INVALID.  The first call on each device
- * looks the array up (make it before any stream capture).  Calls share the array: calls that
- * overlap on the GPU race. */
+ * 262,144 rays per call; larger counts return QK_ERR_INVALID.  The array's address belongs to
+ * the current CUDA context, so every call looks it up (a host-side query that allocates
+ * nothing); the first call on a device may load the library's device code, so make it before
+ * any stream capture.  Calls share the array: calls that overlap on the GPU race. */
 int qk_raycast_noalloc(const qk_tree* tree, const void* rays, int count, uint64_t* out,
                        unsigned flags, void* stream);
 

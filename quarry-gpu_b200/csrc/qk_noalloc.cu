@@ -9,13 +9,14 @@
 //
 // The array is a file-scope __device__ variable: every GPU that loads the library holds
 // kNoAllocScratchBytes of it until the process exits.  Host code cannot use the variable's
-// name as a device address, so the first call on each device looks the address up with
-// cudaGetSymbolAddress (with that device current) and keeps it; that first call should come
+// name as a device address, so each call looks the address up with cudaGetSymbolAddress,
+// with the caller's device current.  The address belongs to the current CUDA context (it
+// changes after cudaDeviceReset, and differs under another driver context on the same
+// device), so it is not kept between calls; the lookup is a host-side query that allocates
+// nothing.  The first call on a device may load the library's device code, so make it
 // before any stream capture.  All calls share the one array: calls whose work overlaps on
-// the GPU (different streams, no ordering between them) race on it.  Each call rewrites every
-// scratch word it reads before reading it, so nothing has to start at zero.
-#include <mutex>
-
+// the GPU (different streams, no ordering between them) race on it.  Each call rewrites
+// every scratch word it reads before reading it, so nothing has to start at zero.
 #include "qk_internal.cuh"
 
 namespace qk {
@@ -28,23 +29,15 @@ constexpr size_t kNoAllocScratchBytes = 4608 * 1024;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_noalloc_mutex;
-void* g_noalloc_ptr[kMaxDevices] = {};
-
-int scratch_for_current_device(void** out) {
+// The scratch address in the current context (looked up on every call, see above).
+int scratch_for_current_context(void** out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return cuda_status(e, "noalloc: current device");
-    if (dev < 0 || dev >= kMaxDevices) return fail(QK_ERR_INVALID, "noalloc: device %d out of range", dev);
-    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (g_noalloc_ptr[dev] == nullptr) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) return cuda_status(e, "noalloc: scratch address");
-        g_noalloc_ptr[dev] = p;
-    }
-    *out = g_noalloc_ptr[dev];
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_status(e, "noalloc: scratch address");
+    *out = p;
     return QK_OK;
 }
 
@@ -75,7 +68,7 @@ extern "C" int qk_raycast_noalloc(const qk_tree* tree, const void* rays, int cou
     if (order_ws_bytes(count) > kNoAllocScratchBytes)
         return fail(QK_ERR_WORKSPACE, "noalloc scratch too small for %d rays", count);
     void* scratch = nullptr;
-    const int st = scratch_for_current_device(&scratch);
+    const int st = scratch_for_current_context(&scratch);
     if (st != QK_OK) return st;
     return ray_query(tree, rays, count, out, nullptr, flags, nullptr, scratch,
                      static_cast<cudaStream_t>(stream));

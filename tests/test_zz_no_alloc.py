@@ -40,7 +40,10 @@ def test_noalloc_matches_raycast_on_two_calls(cuda):
                                            float(hi[1]), 50.0, 3), np.float32)
     b = capi.to_device(workloads.cosine_rays(150_000, float(lo[0]), float(hi[0]), float(lo[1]),
                                              float(hi[1]), 40.0, 4), np.float32)
-    for flags in (capi.QK_ORDER_MORTON, capi.QK_ORDER_MORTON | capi.QK_WIDE,
+    # input order (no order scratch), Morton (+ 4-wide), the dynamic-fetch schedule (its work
+    # counter is a word of the shared scratch, zeroed by the call) and the coherent order
+    for flags in (0, capi.QK_ORDER_MORTON, capi.QK_ORDER_MORTON | capi.QK_WIDE,
+                  capi.QK_ORDER_MORTON | capi.QK_TUNE_DYNAMIC,
                   capi.QK_ORDER_COHERENT | capi.QK_TUNE_HIGH_OCC):
         want_a = tree.raycast(a, flags)
         want_b = tree.raycast(b, flags)

@@ -37,7 +37,9 @@ extern "C" {
 #define QK_ERR_CUDA 2        /* a CUDA call failed */
 #define QK_ERR_WORKSPACE 3   /* workspace smaller than the matching *_bytes query */
 #define QK_ERR_OVERFLOW 4    /* a traversal stack or a fixed table overflowed */
-#define QK_ERR_DEPTH 5       /* tree deeper than the traversal stacks support */
+#define QK_ERR_DEPTH 5       /* tree deeper than the traversal stacks support: every traversal
+                                entry point returns it, launching nothing, when tree->depth is
+                                outside [0, 63] (trees from qk_build never are) */
 
 /* ---- primitive kinds and builders ---- */
 #define QK_TRI 0

@@ -36,6 +36,12 @@ def build(reference: bool = True) -> None:
     subprocess.run(["make", "-s", "-C", str(HERE), "all"], check=True)
     if reference and REFERENCE_SRC.is_dir():
         subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF={REFERENCE_SRC}"], check=True)
+        # quarry's own callers against the engine's header and library (drop-in check); they
+        # link libquarry_b200.so, so the engine is built first
+        engine = HERE.parent / "quarry-gpu_b200" / "quarry" / "libquarry_b200.so"
+        if engine.exists():
+            subprocess.run(["make", "-s", "-C", str(HERE), "callers", f"REF={REFERENCE_SRC}"],
+                           check=True)
 
 
 def _ptr(a: np.ndarray | None):

@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include "gpu/gpu_bvh.h"
+#include "qk_internal.cuh"
 #include "quarry_b200.h"
 #include "scenes.h"
 
@@ -61,6 +62,33 @@ struct Timer {
         float ms = 0.0f;
         cudaOk(cudaEventElapsedTime(&ms, a, b), "elapsed");
         return static_cast<double>(ms);
+    }
+};
+
+// Installs a qk::StageClock on this host thread for one engine call, so the builders, refits
+// and topology edits record an event at each stage boundary; ms(a, b) reads a stage's device
+// time (0 when a mark was not reached).  The role of quarry's StageClock
+// (src/gpu/lbvh.cu:173-190).
+struct StageScope {
+    qk::StageClock c;
+    StageScope() {
+        for (cudaEvent_t& e : c.ev) cudaOk(cudaEventCreate(&e), "event");
+        for (cudaEvent_t& e : c.lv) cudaOk(cudaEventCreate(&e), "event");
+        qk::stage_clock() = &c;
+    }
+    ~StageScope() {
+        qk::stage_clock() = nullptr;
+        for (cudaEvent_t& e : c.ev) cudaEventDestroy(e);
+        for (cudaEvent_t& e : c.lv) cudaEventDestroy(e);
+    }
+    StageScope(const StageScope&) = delete;
+    StageScope& operator=(const StageScope&) = delete;
+    double ms(int a, int b) const {
+        if (!c.hit[a] || !c.hit[b]) return 0.0;
+        cudaOk(cudaEventSynchronize(c.ev[b]), "event sync");
+        float v = 0.0f;
+        cudaOk(cudaEventElapsedTime(&v, c.ev[a], c.ev[b]), "elapsed");
+        return static_cast<double>(v);
     }
 };
 
@@ -165,13 +193,33 @@ GpuBVH buildImpl(int kind, const void* host, size_t itemBytes, int n, int builde
         void* src = stageOf(im, itemBytes * static_cast<size_t>(n));
         cudaOk(cudaMemcpy(src, host, itemBytes * static_cast<size_t>(n), cudaMemcpyHostToDevice),
                "H2D prims");
+        StageScope clock;
         Timer timer;
         qkOk(qk_build(&t, builder, im->bins, src, im->ws, im->wsBytes, nullptr), "build");
         const double ms = timer.stop();
         if (timings) {
-            *timings = GpuBuildTimings{};
-            timings->treeMs = ms;
-            timings->totalMs = ms;
+            // stage times as quarry reports them (src/gpu/lbvh.cu:2027-2034, 2105-2115)
+            using namespace qk;
+            GpuBuildTimings& bt = *timings;
+            bt = GpuBuildTimings{};
+            if (builder == QK_BUILD_SAH) {
+                // topology (levels + lower tiers) and depths; the leaf scatter; the boxes
+                bt.treeMs = clock.ms(kMarkStart, kMarkTopo) + clock.ms(kMarkBoxes, kMarkEnd);
+                bt.scatterMs = clock.ms(kMarkTopo, kMarkScatter);
+                bt.refitMs = clock.ms(kMarkScatter, kMarkBoxes);
+                bt.sahBinMs = clock.c.sah_bin;
+                bt.sahSplitMs = clock.c.sah_split;
+                bt.sahPartMs = clock.c.sah_part;
+            } else {
+                // the emit kernel writes the leaves (the scatter) and the internal nodes in
+                // one pass, so its time is in treeMs and scatterMs stays 0
+                bt.mortonMs = clock.ms(kMarkStart, kMarkMorton);
+                bt.sortMs = clock.ms(kMarkMorton, kMarkSort);
+                bt.treeMs = clock.ms(kMarkSort, kMarkTopo) + clock.ms(kMarkBoxes, kMarkEnd);
+                bt.refitMs = clock.ms(kMarkTopo, kMarkBoxes);
+            }
+            bt.totalMs = clock.ms(kMarkStart, kMarkEnd);
+            if (bt.totalMs <= 0.0) bt.totalMs = ms;
         }
         bvh.sah = builder == QK_BUILD_SAH;
         im->baseDepth = t.depth;
@@ -196,6 +244,8 @@ double refitImpl(GpuBVH& bvh, const std::vector<Item>& items, const std::vector<
     GpuRefitTimings* tm = timings ? timings : &local;
     *tm = GpuRefitTimings{};
     Timer timer;
+    StageScope clock;
+    double uploadMs = 0.0;
     if (dirty) {
         // unique, in range; the engine writes each dirty leaf once
         std::vector<int> ids = *dirty;
@@ -211,23 +261,42 @@ double refitImpl(GpuBVH& bvh, const std::vector<Item>& items, const std::vector<
             char* st = static_cast<char*>(stageOf(im, sizeof(int) * count + 256 + sizeof(Item) * count));
             int* dIds = reinterpret_cast<int*>(st);
             void* dItems = st + ((sizeof(int) * count + 255) / 256) * 256;
+            Timer up;
             cudaOk(cudaMemcpy(dIds, ids.data(), sizeof(int) * count, cudaMemcpyHostToDevice), "H2D ids");
             cudaOk(cudaMemcpy(dItems, moved.data(), sizeof(Item) * count, cudaMemcpyHostToDevice), "H2D prims");
+            uploadMs = up.stop();
             qkOk(qk_refit_dirty(&im->t, dIds, dItems, count, im->ws, im->wsBytes, nullptr), "refit");
         }
         tm->updated = count;
     } else {
         void* src = stageOf(im, sizeof(Item) * static_cast<size_t>(n));
+        Timer up;
         cudaOk(cudaMemcpy(src, items.data(), sizeof(Item) * static_cast<size_t>(n),
                           cudaMemcpyHostToDevice),
                "H2D prims");
+        uploadMs = up.stop();
         qkOk(qk_refit(&im->t, src, im->ws, im->wsBytes, nullptr), "refit");
         tm->updated = n;
     }
     const double ms = timer.stop();
-    tm->totalMs = ms;
-    tm->treeMs = ms;
-    tm->mergeMs = ms;
+    // stage times as quarry reports them (src/gpu/gpu_bvh.h:129-138): the full refit gathers
+    // the leaves then merges; the dirty refit rewrites the dirty leaves and marks their
+    // ancestors in one kernel (markMs), then merges them
+    {
+        using namespace qk;
+        tm->uploadMs = uploadMs;
+        const double first = clock.ms(kMarkStart, kMarkScatter);
+        tm->mergeMs = clock.ms(kMarkScatter, kMarkBoxes);
+        if (dirty) {
+            tm->markMs = first;
+            tm->treeMs = first + tm->mergeMs;
+        } else {
+            tm->gatherMs = first;
+            tm->treeMs = tm->mergeMs;
+        }
+        tm->wideMs = clock.ms(kMarkBoxes, kMarkEnd);
+        tm->totalMs = ms;
+    }
     syncPublic(bvh, im);
     return ms;
 }
@@ -364,10 +433,25 @@ double updateImpl(GpuBVH& bvh, int kind, const std::vector<Item>& items, const G
     ed.extra_items = dScript + oExtra;
     ed.moved_items = dScript + oMoved;
     qk_topo_info info{};
-    qkOk(qk_update_topology(&im->t, &nt, &ed, 0, im->bins, &info, im->upd, wsBytes, nullptr),
-         "topology update");
+    double planMs = 0.0, relayoutMs = 0.0, forestMs = 0.0, mergeMs = 0.0;
+    {
+        StageScope clock;
+        qkOk(qk_update_topology(&im->t, &nt, &ed, 0, im->bins, &info, im->upd, wsBytes, nullptr),
+             "topology update");
+        using namespace qk;
+        planMs = clock.ms(kMarkStart, kMarkPlan);
+        relayoutMs = clock.ms(kMarkPlan, kMarkRelayout);
+        forestMs = clock.ms(kMarkRelayout, kMarkTopo);
+        mergeMs = clock.ms(kMarkTopo, kMarkEnd);
+    }
     if (info.rebuild || nt.depth > im->baseDepth + kTopoDepthSlack) return rebuildAll();
-    t->surgeryMs = surgery.stop();
+    // the whole device call; its stages: cut plan, renumbering + leaf staging, the forest
+    // builds of the touched subtrees, and the box merge of the new tree (with depths)
+    const double deviceMs = surgery.stop();
+    t->planMs = planMs;
+    t->relayoutMs = relayoutMs;
+    t->mergeMs = mergeMs;
+    t->surgeryMs = forestMs > 0.0 ? forestMs : deviceMs;
 
     nt.wide = im->t.wide;  // reused by the wide rebuild below (or freed with the tree)
     nt.wide_count = 0;
@@ -384,7 +468,7 @@ double updateImpl(GpuBVH& bvh, int kind, const std::vector<Item>& items, const G
     if (wide) wideMs = buildWideNodesGPU(bvh);
     t->totalMs = timer.stop();
     t->wideMs = wideMs;
-    t->uploadMs = t->totalMs - t->surgeryMs - wideMs;
+    t->uploadMs = std::max(0.0, t->totalMs - deviceMs - wideMs);
     t->surgeryRoots = info.cuts;
     t->rebuiltLeaves = info.new_leaves;
     t->newDepth = bvh.depth;

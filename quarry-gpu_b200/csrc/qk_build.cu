@@ -449,12 +449,14 @@ int finish_tree(qk_tree* t, Header* h, int2* ranges, bool ranges_ready, cudaStre
     if (!ranges_ready) k_ranges_descent<<<blocks_for(n - 1), kBlock, 0, s>>>(nodes, n, ranges);
     k_bottom_up_ranged<<<blocks_for(n), kBlock, 0, s>>>(nodes, static_cast<BNode*>(t->bnodes),
                                                         t->parent, t->flags, n, ranges);
+    stage_mark(kMarkBoxes, s);
     cudaMemsetAsync(&h->max_depth, 0, sizeof(int), s);
     k_depth<<<blocks_for(2 * n - 1), kBlock, 0, s>>>(t->parent, 2 * n - 1, t->depth_arr, h);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_status(e, "tree boxes");
     int depth = 0;
     e = cudaMemcpyAsync(&depth, &h->max_depth, sizeof(int), cudaMemcpyDeviceToHost, s);
+    stage_mark(kMarkEnd, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return cuda_status(e, "build depth readback");
     t->depth = depth;
@@ -481,13 +483,17 @@ int build_lbvh(qk_tree* t, const void* items_v, void* ws, cudaStream_t s) {
     const int grid = min(blocks_for(n), 148 * 8);
     k_centroid_bounds<Ops><<<grid, kBlock, 0, s>>>(items, n, h);
     k_morton<Ops><<<blocks_for(n), kBlock, 0, s>>>(items, n, h, codes, idx);
+    stage_mark(kMarkMorton, s);
     cudaError_t e = sort_pairs(codes, idx, codes_s, idx_s, n, 30, sort_ws, s);
     if (e != cudaSuccess) return cuda_status(e, "build sort");
+    stage_mark(kMarkSort, s);
     int2* ranges = build_ranges(ws, t->kind, n, QK_BUILD_LBVH);
+    // leaves (the scatter into leaf order) and internal nodes in one pass
     k_emit<Ops><<<blocks_for(n), kBlock, 0, s>>>(items, n, codes_s, idx_s, nodes,
                                                   static_cast<float*>(t->items), t->prim_ids,
                                                   t->slot_of, t->parent, bn,
                                                   static_cast<float4*>(t->leaves), t->flags, ranges);
+    stage_mark(kMarkTopo, s);
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_status(e, "build kernels");
     return finish_tree(t, h, ranges, true, s);
@@ -496,16 +502,20 @@ int build_lbvh(qk_tree* t, const void* items_v, void* ws, cudaStream_t s) {
 template <class Ops>
 int refit_impl(qk_tree* t, const void* items, cudaStream_t s) {
     const int n = t->n;
+    stage_mark(kMarkStart, s);
     k_refit_leaves<Ops><<<blocks_for(n), kBlock, 0, s>>>(
         static_cast<const float*>(items), n, t->prim_ids, static_cast<Node*>(t->nodes),
         static_cast<float*>(t->items), static_cast<float4*>(t->leaves));
+    stage_mark(kMarkScatter, s);
     k_bottom_up<<<blocks_for(n), kBlock, 0, s>>>(static_cast<Node*>(t->nodes),
                                                  static_cast<BNode*>(t->bnodes), t->parent,
                                                  t->flags, n, nullptr);
+    stage_mark(kMarkBoxes, s);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_status(e, "refit");
-    if (t->wide_count > 0 && t->wide) return wide_emit_all(t, s);
-    return QK_OK;
+    const int st = (t->wide_count > 0 && t->wide) ? wide_emit_all(t, s) : QK_OK;
+    stage_mark(kMarkEnd, s);
+    return st;
 }
 
 template <class Ops>
@@ -516,19 +526,23 @@ int refit_dirty_impl(qk_tree* t, const int* ids, const void* items, int count, v
     Carve c{static_cast<char*>(ws)};
     Header* h = c.take<Header>(1);
     int* skip = c.take<int>(count);
+    stage_mark(kMarkStart, s);
     k_header_init<<<1, 32, 0, s>>>(h);
     k_dirty_mark<Ops><<<blocks_for(count), kBlock, 0, s>>>(
         ids, static_cast<const float*>(items), count, n, t->slot_of, t->parent,
         static_cast<Node*>(t->nodes), static_cast<float*>(t->items),
         static_cast<float4*>(t->leaves), t->flags, skip, h);
+    stage_mark(kMarkScatter, s);
     k_dirty_merge<<<blocks_for(count), kBlock, 0, s>>>(ids, count, n, t->slot_of, t->parent,
                                                        static_cast<Node*>(t->nodes),
                                                        static_cast<BNode*>(t->bnodes), t->flags,
                                                        skip);
+    stage_mark(kMarkBoxes, s);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_status(e, "refit dirty");
-    if (t->wide_count > 0 && t->wide) return wide_emit_all(t, s);
-    return QK_OK;
+    const int st = (t->wide_count > 0 && t->wide) ? wide_emit_all(t, s) : QK_OK;
+    stage_mark(kMarkEnd, s);
+    return st;
 }
 
 template <class Ops>
@@ -601,6 +615,7 @@ int2* build_ranges(void* ws, int kind, int n, int builder) {
 int build_tree(qk_tree* t, int builder, int bins, const void* items, void* ws, size_t ws_bytes,
                cudaStream_t s) {
     (void)ws_bytes;
+    stage_mark(kMarkStart, s);
     if (builder == QK_BUILD_SAH) {
         cudaMemsetAsync(t->flags, 0, sizeof(int) * static_cast<size_t>(t->n - 1), s);
         const int st = build_sah(t, bins, items, ws, s);

@@ -33,6 +33,11 @@ int cuda_status(cudaError_t e, const char* what) {
     return QK_ERR_CUDA;
 }
 
+StageClock*& stage_clock() {
+    static thread_local StageClock* clock = nullptr;
+    return clock;
+}
+
 }  // namespace qk
 
 using namespace qk;
@@ -56,7 +61,13 @@ int check_ws(void* ws, size_t have, size_t need) {
     return QK_OK;
 }
 
+// Every traversal entry point: the tree's recorded depth must fit the traversal stacks (a
+// tree from qk_build / qk_update_topology always does; one assembled by the caller may not),
+// so nothing is launched on a tree the stacks cannot hold.
 int check_wide(const qk_tree* t, unsigned flags) {
+    if (t->depth < 0 || t->depth >= kStack)
+        return fail(QK_ERR_DEPTH, "tree depth %d exceeds the traversal stack (%d levels)",
+                    t->depth, kStack - 1);
     if ((flags & QK_WIDE) && (t->wide == nullptr || t->wide_count <= 0))
         return fail(QK_ERR_INVALID, "wide nodes not built");
     if (__builtin_popcount(flags & (QK_ORDER_MORTON | QK_ORDER_DIRECTION | QK_ORDER_COHERENT)) > 1)

@@ -29,6 +29,36 @@ void set_error(const char* fmt, ...);
 int fail(int status, const char* fmt, ...);
 int cuda_status(cudaError_t e, const char* what);
 
+// Per-stage device timing behind the C++ API's timing structs (GpuBuildTimings,
+// GpuRefitTimings, GpuTopoUpdateTimings).  A host thread installs a StageClock for the
+// duration of one call; the builders, refits and topology edits then record an event on their
+// stream at each stage boundary (stage_mark), and the SAH builder adds its per-level binning,
+// split and partition times.  With no clock installed (every C-ABI call) nothing is recorded.
+enum StageMark {
+    kMarkStart,     // call begins
+    kMarkMorton,    // LBVH: centroid bounds + Morton codes done
+    kMarkSort,      // LBVH: radix sort done
+    kMarkPlan,      // topology edit: cut plan chosen (host synchronisation)
+    kMarkRelayout,  // topology edit: kept nodes renumbered, kept leaves and new items staged
+    kMarkTopo,      // links done (LBVH emit, SAH levels + lower tiers, edit forests)
+    kMarkScatter,   // leaves written (SAH leaf scatter; refit leaf gather / dirty marking)
+    kMarkBoxes,     // bottom-up boxes (or the refit merge) done
+    kMarkEnd,       // depths read back / wide nodes re-emitted: call done
+    kMarkCount
+};
+struct StageClock {
+    cudaEvent_t ev[kMarkCount] = {};
+    bool hit[kMarkCount] = {};
+    cudaEvent_t lv[4] = {};  // SAH global-tier level: start, binned, split, partitioned
+    double sah_bin = 0.0, sah_split = 0.0, sah_part = 0.0;
+};
+// the calling host thread's installed clock (nullptr when none)
+StageClock*& stage_clock();
+inline void stage_mark(int m, cudaStream_t s) {
+    StageClock* c = stage_clock();
+    if (c != nullptr && cudaEventRecord(c->ev[m], s) == cudaSuccess) c->hit[m] = true;
+}
+
 // Carves aligned sub-buffers out of one workspace.  With base == nullptr it only measures.
 struct Carve {
     char* base = nullptr;

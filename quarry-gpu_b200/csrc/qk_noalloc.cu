@@ -59,6 +59,9 @@ extern "C" int qk_raycast_noalloc(const qk_tree* tree, const void* rays, int cou
                     "batch or use qk_raycast with a caller workspace",
                     kNoAllocMaxRays, count);
     if (count > 0 && (!rays || !out)) return fail(QK_ERR_INVALID, "rays or out is NULL");
+    if (tree->depth < 0 || tree->depth >= kStack)
+        return fail(QK_ERR_DEPTH, "tree depth %d exceeds the traversal stack (%d levels)",
+                    tree->depth, kStack - 1);
     if ((flags & QK_WIDE) && (tree->wide == nullptr || tree->wide_count <= 0))
         return fail(QK_ERR_INVALID, "wide nodes not built");
     if (__builtin_popcount(flags & (QK_ORDER_MORTON | QK_ORDER_DIRECTION | QK_ORDER_COHERENT)) > 1)

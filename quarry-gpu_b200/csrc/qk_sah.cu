@@ -1261,9 +1261,15 @@ int build_sah_impl(qk_tree* t, int bins, const void* items_v, void* ws, cudaStre
         // size / kChunk + 1 chunks); blocks beyond the count k_level_prep wrote return at once
         const int nch = n / kChunk + nbig + 1;
         cudaError_t e;
+        // per-level stage times when a StageClock is installed: binning (centroid bounds +
+        // bins), split selection, partition (+ child assignment)
+        StageClock* clk = stage_clock();
+        if (clk) cudaEventRecord(clk->lv[0], s);
         k_level_cbounds<<<nch, kBlock, 0, s>>>(w.L, ord, w.cen);
         k_level_bins<<<nch, kBlock, 0, s>>>(w.L, ord, w.cen, w.plo, w.phi, bins);
+        if (clk) cudaEventRecord(clk->lv[1], s);
         k_level_split<<<blocks_for(static_cast<long long>(nbig) * 32), kBlock, 0, s>>>(w.L, nbig, bins);
+        if (clk) cudaEventRecord(clk->lv[2], s);
         k_level_count_left<<<nch, kBlock, 0, s>>>(w.L, ord, w.cen, bins);
         k_level_prefix_left<<<blocks_for(nbig), kBlock, 0, s>>>(w.L, nbig);
         k_level_partition<<<nch, kBlock, 0, s>>>(w.L, ord, alt, w.cen, bins);
@@ -1271,10 +1277,21 @@ int build_sah_impl(qk_tree* t, int bins, const void* items_v, void* ws, cudaStre
         // next big tasks start from zero each level; block tasks accumulate
         cudaMemsetAsync(w.L.counters + 1, 0, sizeof(int), s);
         k_level_assign<<<1, 1024, 0, s>>>(w.L, nbig, nxt, w.blocks, nodes, bn, t->parent, n);
+        if (clk) cudaEventRecord(clk->lv[3], s);
         int cnt[4] = {0, 0, 0, 0};
         e = cudaMemcpyAsync(cnt, w.L.counters, sizeof(cnt), cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) return cuda_status(e, "SAH level");
+        if (clk) {
+            float a = 0.f, b = 0.f, c3 = 0.f;
+            if (cudaEventElapsedTime(&a, clk->lv[0], clk->lv[1]) == cudaSuccess &&
+                cudaEventElapsedTime(&b, clk->lv[1], clk->lv[2]) == cudaSuccess &&
+                cudaEventElapsedTime(&c3, clk->lv[2], clk->lv[3]) == cudaSuccess) {
+                clk->sah_bin += a;
+                clk->sah_split += b;
+                clk->sah_part += c3;
+            }
+        }
         nbig = cnt[1];
         nblk = cnt[2];
         Task* tmpt = cur;
@@ -1305,9 +1322,12 @@ int build_sah_impl(qk_tree* t, int bins, const void* items_v, void* ws, cudaStre
         cudaStreamSynchronize(s);
         if (base != n - 1) return fail(QK_ERR_INVALID, "SAH node accounting: %d != %d", base, n - 1);
     }
+    stage_mark(kMarkTopo, s);
+    // the scatter: items, leaf payloads and prim ids in leaf order
     k_sah_leaves<Ops><<<blocks_for(n), kBlock, 0, s>>>(items, n, ord, nodes,
                                                        static_cast<float*>(t->items), t->prim_ids,
                                                        t->slot_of, static_cast<float4*>(t->leaves));
+    stage_mark(kMarkScatter, s);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_status(e, "SAH kernels");
     int errors = 0;

@@ -611,6 +611,7 @@ int update_impl(const qk_tree* old_t, qk_tree* new_t, const qk_topo_edit* ed, in
               static_cast<const float*>(ed->moved_items), n_old, n_new};
     const int nn = 2 * n_old - 1;
 
+    stage_mark(kMarkStart, s);
     cudaMemsetAsync(w.plan, 0, sizeof(TopoPlan), s);
     cudaMemsetAsync(w.del_flag, 0, sizeof(int) * n_old, s);
     cudaMemsetAsync(w.cut_mark, 0, sizeof(int) * 2 * static_cast<size_t>(n_old), s);
@@ -647,6 +648,7 @@ int update_impl(const qk_tree* old_t, qk_tree* new_t, const qk_topo_edit* ed, in
     err = scan_exclusive(w.wnode, w.wnode, nn, true, w.scan_ws, s);
     if (err != cudaSuccess) return cuda_status(err, "topology id scan");
     k_topo_totals<<<1, 1, 0, s>>>(w.plan, w.wslot, n_old, w.cut_mark, w.wnode);
+    stage_mark(kMarkPlan, s);
     TopoPlan plan{};
     err = cudaGetLastError();
     if (err == cudaSuccess) err = cudaMemcpyAsync(&plan, w.plan, sizeof(plan), cudaMemcpyDeviceToHost, s);
@@ -708,6 +710,7 @@ int update_impl(const qk_tree* old_t, qk_tree* new_t, const qk_topo_edit* ed, in
             e, *old_t, w.ext_key_s, w.ext_val_s, w.cut_list, w.range, w.wslot, w.del_flag,
             w.st_items, w.st_id, w.cen, w.plo, w.phi, w.order, eerr);
     }
+    stage_mark(kMarkRelayout, s);
     if (plan.cuts > 0) {
         const int st = sah_forest(w.tasks, plan.cuts, plan.max_new, w.id_base, w.order, w.tmp,
                                   w.cen, w.plo, w.phi, new_t, bins, eerr, s);
@@ -716,6 +719,7 @@ int update_impl(const qk_tree* old_t, qk_tree* new_t, const qk_topo_edit* ed, in
                                                        w.st_id, *new_t, eerr);
     }
     if (e.n_mov > 0) k_topo_moved<Ops><<<blocks_for(e.n_mov), kBlock, 0, s>>>(e, *new_t, eerr);
+    stage_mark(kMarkTopo, s);
     err = cudaGetLastError();
     // every emit write was checked; the bottom-up pass only runs over a fully linked tree
     int emit_errors = 0;

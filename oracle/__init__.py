@@ -128,8 +128,44 @@ def ref():
         _sig(R, "qr_ray_hash", _U64, [_P, _I64, _P])
         _sig(R, "qr_closest_hash", _U64, [_P, _I64])
         _sig(R, "qr_list_hash", _U64, [_P, _P, _I64])
+        _sig(R, "qr_scene", _P, [_I, _P, _I, _P, _I, _P, _P, _I, _I, _P, _P, _I, _F, _P, _I, _P,
+                                 _I, _P, _P])
         _ref = R
     return _ref
+
+
+SCENES_PATH = HERE / "_build" / "libqscenes.so"
+_scenes = None
+
+
+def scenes_lib() -> ctypes.CDLL:
+    """The engine's workload generators (quarry-gpu_b200/csrc/scenes.c) compiled on their own
+    by oracle/Makefile, for CPU-side runs that must not load the engine library; the same
+    source and flags as the engine's copy, so the same bytes (tests/test_workloads.py)."""
+    global _scenes
+    if _scenes is None:
+        if not SCENES_PATH.exists():
+            build(reference=False)
+        _scenes = ctypes.CDLL(str(SCENES_PATH))
+    return _scenes
+
+
+def standalone_workloads():
+    """quarry-gpu_b200/quarry/workloads.py loaded as a plain module bound to scenes_lib(): the
+    benchmark inputs without importing the quarry package or its libraries."""
+    import importlib.util
+    import sys
+
+    name = "_qk_workloads_standalone"
+    if name in sys.modules:
+        return sys.modules[name]
+    path = HERE.parent / "quarry-gpu_b200" / "quarry" / "workloads.py"
+    spec = importlib.util.spec_from_file_location(name, path)
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    mod.bind(scenes_lib())
+    return mod
 
 
 def _f32(a) -> np.ndarray:
@@ -348,6 +384,39 @@ class Reference:
         finally:
             self.R.qr_radius_free(h)
         return offsets, keys, qms.value
+
+    def scene(self, kind: str, items, closest_q, knn_q, kk: int, radius_q, r: float, rays=None,
+              threads: int = 0):
+        """Every query set of one scene on one reference structure (built once): returns
+        {closest, knn, radius: (offsets, keys), rays (triangles)} and the times
+        {build_ms, closest_ms, knn_ms, radius_ms, rays_ms}."""
+        k = KIND[kind]
+        items = _f32(items).reshape(-1, STRIDE[k])
+        qc = _f32(closest_q).reshape(-1, 3)
+        qk = _f32(knn_q).reshape(-1, 3)
+        qr = _f32(radius_q).reshape(-1, 3)
+        rays = np.zeros((0, 8), np.float32) if rays is None else _f32(rays).reshape(-1, 8)
+        oc = np.zeros((qc.shape[0], 2), dtype=np.uint32)
+        ok = np.zeros((qk.shape[0], kk, 2), dtype=np.uint32)
+        orr = np.zeros(rays.shape[0], dtype=np.uint64)
+        bms = ctypes.c_double(0.0)
+        ms = (ctypes.c_double * 4)()
+        h = self.R.qr_scene(k, _ptr(items), items.shape[0], _ptr(qc), qc.shape[0], _ptr(oc),
+                            _ptr(qk), qk.shape[0], kk, _ptr(ok), _ptr(qr), qr.shape[0], r,
+                            _ptr(rays), rays.shape[0], _ptr(orr), threads, ctypes.byref(bms), ms)
+        try:
+            total = self.R.qr_radius_total(h)
+            offsets = np.zeros(qr.shape[0] + 1, dtype=np.int64)
+            keys = np.zeros(total, dtype=np.uint64)
+            self.R.qr_radius_copy(h, _ptr(offsets), _ptr(keys))
+        finally:
+            self.R.qr_radius_free(h)
+        out = {"closest": oc, "knn": ok, "radius": (offsets, keys)}
+        if k == 0:
+            out["rays"] = orr
+        times = {"build_ms": bms.value, "closest_ms": ms[0], "knn_ms": ms[1], "radius_ms": ms[2],
+                 "rays_ms": ms[3]}
+        return out, times
 
     def closest_brute(self, kind: str, items, q):
         k = KIND[kind]

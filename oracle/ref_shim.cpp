@@ -282,6 +282,73 @@ void qr_radius_copy(void* h, int64_t* offsets, uint64_t* keys) {
 
 void qr_radius_free(void* h) { delete static_cast<RadiusResult*>(h); }
 
+// One scene, every query set: the reference structure is built once (*build_ms) and answers
+// nc closest points, nk k-nearest (k per query, padded with id -1), nr radius queries
+// (returned as a handle like qr_radius) and, for triangles, nrays rays; each set fans out
+// over `threads`.  ms[0..3]: closest, kNN, radius and ray query times.
+void* qr_scene(int kind, const float* items, int n, const float* qc, int nc, uint32_t* out_c,
+               const float* qk, int nk, int k, uint32_t* out_k, const float* qr, int nr,
+               float radius, const float* rays8, int nrays, uint64_t* out_r, int threads,
+               double* build_ms, double* ms) {
+    const double t0 = nowMs();
+    const Index idx(kind, items, n);
+    const double t1 = nowMs();
+    if (build_ms) *build_ms = t1 - t0;
+    parallelChunks(nc, threads, [&](int b, int e) {
+        for (int i = b; i < e; ++i) {
+            Vec3 p;
+            std::memcpy(&p, qc + 3 * static_cast<size_t>(i), sizeof(Vec3));
+            putHit(out_c + 2 * static_cast<size_t>(i), idx.closest(p));
+        }
+    });
+    const double t2 = nowMs();
+    parallelChunks(nk, threads, [&](int b, int e) {
+        for (int i = b; i < e; ++i) {
+            Vec3 p;
+            std::memcpy(&p, qk + 3 * static_cast<size_t>(i), sizeof(Vec3));
+            const std::vector<ClosestHit> list = idx.knn(p, k);
+            uint32_t* dst = out_k + 2 * static_cast<size_t>(i) * static_cast<size_t>(k);
+            for (int j = 0; j < k; ++j) {
+                if (j < static_cast<int>(list.size())) {
+                    putHit(dst + 2 * j, list[static_cast<size_t>(j)]);
+                } else {
+                    dst[2 * j] = 0u;
+                    dst[2 * j + 1] = static_cast<uint32_t>(-1);
+                }
+            }
+        }
+    });
+    const double t3 = nowMs();
+    auto* res = new RadiusResult;
+    res->lists.resize(static_cast<size_t>(nr));
+    parallelChunks(nr, threads, [&](int b, int e) {
+        for (int i = b; i < e; ++i) {
+            Vec3 p;
+            std::memcpy(&p, qr + 3 * static_cast<size_t>(i), sizeof(Vec3));
+            res->lists[static_cast<size_t>(i)] = idx.radius(p, radius);
+        }
+    });
+    const double t4 = nowMs();
+    if (kind == 0 && nrays > 0) {
+        parallelChunks(nrays, threads, [&](int b, int e) {
+            for (int i = b; i < e; ++i) {
+                Ray r;
+                std::memcpy(&r, rays8 + 8 * static_cast<size_t>(i), sizeof(Ray));
+                const RayHit h = raycastBVH(idx.tri, r);
+                out_r[i] = h.hit ? ((uint64_t{1} << 32) | bitsOf(h.t)) : 0ull;
+            }
+        });
+    }
+    const double t5 = nowMs();
+    if (ms) {
+        ms[0] = t2 - t1;
+        ms[1] = t3 - t2;
+        ms[2] = t4 - t3;
+        ms[3] = t5 - t4;
+    }
+    return res;
+}
+
 // ---- brute force point queries (src/cpu/brute.cpp:62-197) ----
 void qr_closest_brute(int kind, const float* items, int n, const float* q3, int nq,
                       uint32_t* out2) {

@@ -22,10 +22,13 @@ from . import capi
 __all__ = ["gaussian_distance", "triangle_distance", "ray_hit_t"]
 
 
+_ORDERS = {"input": 0, "morton": capi.QK_ORDER_MORTON, "coherent": capi.QK_ORDER_COHERENT}
+
+
 def _order_flags(order: str, wide: bool) -> int:
-    if order not in ("input", "morton"):
-        raise ValueError("order must be 'input' or 'morton'")
-    return (capi.QK_ORDER_MORTON if order == "morton" else 0) | (capi.QK_WIDE if wide else 0)
+    if order not in _ORDERS:
+        raise ValueError("order must be 'input', 'morton' or 'coherent'")
+    return _ORDERS[order] | (capi.QK_WIDE if wide else 0)
 
 
 def _tree(kind, items, builder, wide):
@@ -92,8 +95,11 @@ class _RayHitT(torch.autograd.Function):
         rays[:, 6] = 1e-6
         rays[:, 7] = tmax
         tree = _tree("tri", tris, builder, wide)
-        flags = (capi.QK_WIDE if wide else 0) | {"input": 0, "morton": capi.QK_ORDER_MORTON,
-                                                 "direction": capi.QK_ORDER_DIRECTION}[order]
+        orders = {"input": 0, "morton": capi.QK_ORDER_MORTON,
+                  "direction": capi.QK_ORDER_DIRECTION, "coherent": capi.QK_ORDER_COHERENT}
+        if order not in orders:
+            raise ValueError("order must be 'input', 'morton', 'direction' or 'coherent'")
+        flags = (capi.QK_WIDE if wide else 0) | orders[order]
         out, ids = tree.raycast_ids(rays, flags)
         hit = (out >> 32) != 0
         t = (out & 0xFFFFFFFF).to(torch.int32).view(torch.float32)

@@ -2,6 +2,8 @@
 
 The generators live in csrc/scenes.c (exported by libquarry_b200.so) and compute every
 transcendental from basic IEEE operations, so a seed yields the same bytes on any host.
+bind() points this module at another library exporting the same qs_* functions (a
+stand-alone build of scenes.c), so inputs can be made without loading the engine.
 
 Workloads (sizes are the benchmark's; every generator takes smaller sizes for tests):
   terrain   z-up height field on a grid x grid unit lattice, 2 triangles per cell
@@ -25,15 +27,26 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from . import capi
-
 _P = ctypes.c_void_p
 _sig_done = False
+_bound = None
+
+
+def bind(library: ctypes.CDLL) -> None:
+    """Use `library` (any build of csrc/scenes.c) for the generators instead of the engine's."""
+    global _bound, _sig_done
+    _bound = library
+    _sig_done = False
 
 
 def _lib():
     global _sig_done
-    L = capi.lib()
+    if _bound is not None:
+        L = _bound
+    else:
+        from . import capi
+
+        L = capi.lib()
     if not _sig_done:
         L.qs_cfg_terrain.restype = ctypes.c_int64
         L.qs_cfg_terrain.argtypes = [ctypes.c_int, ctypes.c_uint64, _P]

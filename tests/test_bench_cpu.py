@@ -48,3 +48,30 @@ def test_coherent_order_is_a_grouping_permutation():
     # flat input (every ray equal) keeps input order
     same = np.repeat(rays[:1], 100, axis=0)
     assert np.array_equal(bench.coherent_order(same), np.arange(100))
+
+
+def test_reference_arm_loads_only_checker_libraries_and_matches_the_config():
+    """The CPU arm must not load any library of the engine (its inputs come from the
+    stand-alone generator build under oracle/_build), and its `config` must be the engine
+    arm's (both come from bench.make_workload)."""
+    code = (
+        "import sys, json\n"
+        "sys.argv = ['bench.py', '--impl', 'reference', '--small', '--steps', '1', '--warmup', '1']\n"
+        "sys.path.insert(0, '.')\n"
+        "import bench\n"
+        "bench.main()\n"
+        "maps = open('/proc/self/maps').read().splitlines()\n"
+        "libs = sorted({l.split()[-1] for l in maps if l.split()[-1].endswith('.so')})\n"
+        "print(json.dumps({'libs': libs, 'mods': [m for m in sys.modules if m.startswith('quarry')]}))\n")
+    out = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True,
+                         timeout=600, check=True)
+    lines = out.stdout.strip().splitlines()
+    line, loaded = json.loads(lines[-2]), json.loads(lines[-1])
+    ours = [p for p in loaded["libs"] if str(ROOT) in p]
+    assert ours and all("/oracle/" in p for p in ours), ours
+    assert loaded["mods"] == []
+    sys.path.insert(0, str(ROOT))
+    import bench
+    import oracle
+
+    assert line["config"] == bench.make_workload(oracle.standalone_workloads(), "city", True, 0)[1]

@@ -56,3 +56,19 @@ def test_clouds():
     g = w.gaussians(5000, 0.05, 1.0, 1)
     assert np.all(g[:, 7:10] >= 0.0499) and np.all(g[:, 7:10] <= 1.0001)
     assert np.allclose(np.linalg.norm(g[:, 3:7], axis=1), 1, atol=1e-5)
+
+
+def test_standalone_generators_match_the_engine_library():
+    """bench.py's CPU arm makes its inputs from oracle/_build/libqscenes.so (scenes.c built on
+    its own) so it never loads the engine; the bytes must equal the engine library's."""
+    import oracle
+
+    alone = oracle.standalone_workloads()
+    a, b = alone.city_config(2048, 5000, 300, 1), w.city_config(2048, 5000, 300, 1)
+    assert np.array_equal(a.tris, b.tris) and np.array_equal(a.rays, b.rays)
+    assert np.array_equal(a.queries, b.queries) and a.top == b.top
+    a, b = alone.terrain_config(40, 5000, 300, 1), w.terrain_config(40, 5000, 300, 1)
+    assert np.array_equal(a.tris, b.tris) and np.array_equal(a.rays, b.rays)
+    assert np.array_equal(a.queries, b.queries)
+    assert np.array_equal(alone.gaussians(500, 0.05, 1.0, 3), w.gaussians(500, 0.05, 1.0, 3))
+    assert np.array_equal(alone.point_cloud("surface", 1000, 2), w.point_cloud("surface", 1000, 2))

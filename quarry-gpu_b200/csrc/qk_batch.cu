@@ -506,8 +506,13 @@ struct QRadius {
     unsigned long long* keys;
     const int* total;      // offsets + queries
     long long cap;
+    const int* pool_first = nullptr;  // fill pass after a single-pass count: only the queries
+                                      // whose keys did not fit the pool
     __device__ bool enabled() const { return !kFill || static_cast<long long>(*total) <= cap; }
     __device__ __forceinline__ void run(const BScene& sc, int s, int q, Stack& st, Trav& tv) const {
+        if (kFill && pool_first != nullptr &&
+            (offsets[q + 1] - offsets[q] <= kRadiusStash || pool_first[q] != kPoolLost))
+            return;
         const float3 p = f3(pts[3 * q], pts[3 * q + 1], pts[3 * q + 2]);
         const float r = __ldg(radius + s);
         const float r2 = r * r;
@@ -524,6 +529,37 @@ struct QRadius {
                                                root_box(static_cast<const Node*>(sc.t.nodes)), p,
                                                r2, write, end, keys, max_iter_of(sc.t), st, tv);
         if (!kFill) counts[q] = found;
+    }
+};
+
+// Single-pass radius count (QK_TUNE_STASH): every key found goes to the query's stash slots
+// and pool chain (PoolSink), so the fill only copies.
+template <class Ops, bool kWide>
+struct QRadiusPool {
+    using Stack = SplitStack<kWide ? kStackWide : kStack>;
+    const float* pts;
+    const float* radius;   // per scene
+    int* counts;
+    RadiusPool pool;
+    __device__ bool enabled() const { return true; }
+    __device__ __forceinline__ void run(const BScene& sc, int s, int q, Stack& st, Trav& tv) const {
+        const float3 p = f3(pts[3 * q], pts[3 * q + 1], pts[3 * q + 2]);
+        const float r = __ldg(radius + s);
+        const float r2 = r * r;
+        pool.first[q] = -1;
+        PoolSink sink{pool.stash + static_cast<size_t>(q) * kRadiusStash, pool.keys, pool.next,
+                      pool.taken, pool.chunks, pool.first + q, 0, -1};
+        int found;
+        if (kWide)
+            found = radius_wide_visit<Ops, true>(static_cast<const WideNode*>(sc.t.wide),
+                                                 static_cast<const float4*>(sc.t.leaves), p, r2,
+                                                 sink, max_iter_of(sc.t), st, tv);
+        else
+            found = radius_bin_visit<Ops, true, Stack, false>(
+                static_cast<const BNode*>(sc.t.bnodes), static_cast<const float4*>(sc.t.leaves),
+                root_box(static_cast<const Node*>(sc.t.nodes)), p, r2, sink, max_iter_of(sc.t), st,
+                tv);
+        counts[q] = found;
     }
 };
 
@@ -616,6 +652,7 @@ struct qk_batch_plan {
     int* medium = nullptr;
     int* large = nullptr;
     int* lane_counts = nullptr;
+    qk::RadiusPool pool{};  // single-pass radius (QK_TUNE_STASH)
     void* loop_ws = nullptr;
     size_t loop_ws_bytes = 0;
     int sms = 148;
@@ -753,7 +790,7 @@ int batch_build_loop(qk_batch* b, int builder, int bins, cudaStream_t s) {
 // ---- queries ----
 struct PlanLayout {
     size_t qoff, chunks, counter, params, stats, hdr, keys, idx, keys_s, idx_s, sort_ws, counts,
-        scan_ws, medium, large, lane_counts, loop_ws, loop_ws_bytes, total;
+        scan_ws, medium, large, lane_counts, pool, loop_ws, loop_ws_bytes, total;
     int nchunks;
 };
 
@@ -792,6 +829,12 @@ PlanLayout plan_layout(int op, const int32_t* counts, int scenes, unsigned flags
         L.medium = take(sizeof(int) * n);
         L.large = take(sizeof(int) * n);
         L.lane_counts = take(sizeof(int) * static_cast<size_t>(n) * 32);
+        if (flags & QK_TUNE_STASH) {
+            // the single-pass radius's stash and key pool, carved at the plan creation
+            Carve pc;
+            carve_pool(pc, n);
+            L.pool = take(pc.used);
+        }
     }
     L.loop_ws_bytes = op == QK_OP_RADIUS ? radius_ws_bytes(max_q, flags) : order_ws_bytes(max_q);
     L.loop_ws = take(L.loop_ws_bytes);
@@ -904,6 +947,24 @@ int batch_query_kind(qk_batch_plan* p, const qk_batch_io& io, const qk_batch_tun
         case QK_OP_RADIUS: {
             const float* pts = static_cast<const float*>(io.input);
             auto* keys = static_cast<unsigned long long*>(io.out);
+            if (p->flags & QK_TUNE_STASH) {
+                // single pass: count + keep every key, scan, copy; traverse again only the
+                // queries whose keys did not fit the pool
+                cudaMemsetAsync(p->pool.taken, 0, sizeof(int), s);
+                QRadiusPool<Ops, kWide> qc{pts, p->d_params, p->counts, p->pool};
+                int st = launch_bq(qc, p, tune, s);
+                if (st != QK_OK) return st;
+                const cudaError_t e = scan_exclusive(p->counts, io.offsets, N, true, p->scan_ws, s);
+                if (e != cudaSuccess) return cuda_status(e, "batched radius scan");
+                k_radius_gather<<<blocks_for(static_cast<long long>(N) * 32), kBlock, 0, s>>>(
+                    p->pool, io.offsets, N, keys, io.capacity);
+                QRadius<Ops, true, kWide> qf{pts, p->d_params, nullptr, io.offsets, keys,
+                                             io.offsets + N, io.capacity, p->pool.first};
+                st = launch_bq(qf, p, tune, s);
+                if (st != QK_OK) return st;
+                return radius_sort_segments(io.offsets, N, io.out ? static_cast<uint64_t*>(io.out) : nullptr,
+                                            p->medium, p->large, p->d_hdr, io.capacity, s);
+            }
             QRadius<Ops, false, kWide> qc{pts, p->d_params, p->counts, nullptr, nullptr, nullptr, -1};
             int st = launch_bq(qc, p, tune, s);
             if (st != QK_OK) return st;
@@ -923,7 +984,8 @@ int batch_query_kind(qk_batch_plan* p, const qk_batch_io& io, const qk_batch_tun
 
 int batch_query_loop(qk_batch_plan* p, const qk_batch_io& io, cudaStream_t s) {
     const qk_batch* b = p->b;
-    const unsigned f = p->flags & (QK_ORDER_MORTON | QK_WIDE);
+    // the same layout, order and radius algorithm as the batched schedule
+    const unsigned f = p->flags & (QK_ORDER_MORTON | QK_WIDE | QK_TUNE_STASH);
     long long base = 0;
     for (int i = 0; i < b->scenes; ++i) {
         const int count = p->q_off[i + 1] - p->q_off[i];
@@ -1158,7 +1220,10 @@ int qk_batch_plan_create(qk_batch_plan** out, const qk_batch* b, int op, const i
     if (op < QK_OP_RAY || op > QK_OP_RADIUS) return fail(QK_ERR_INVALID, "unknown batch operation %d", op);
     if (op == QK_OP_RAY && b->kind != kTri) return fail(QK_ERR_INVALID, "rays need triangle scenes");
     if (op == QK_OP_RADIUS && !params) return fail(QK_ERR_INVALID, "radius queries need per-scene radii");
-    if (flags & ~(QK_ORDER_MORTON | QK_WIDE)) return fail(QK_ERR_INVALID, "unknown plan flags 0x%x", flags);
+    if (flags & ~(QK_ORDER_MORTON | QK_WIDE | QK_TUNE_STASH))
+        return fail(QK_ERR_INVALID, "unknown plan flags 0x%x", flags);
+    if ((flags & QK_TUNE_STASH) && op != QK_OP_RADIUS)
+        return fail(QK_ERR_INVALID, "QK_TUNE_STASH applies to radius plans");
     if ((flags & QK_WIDE) && !(b->flags & QK_WIDE))
         return fail(QK_ERR_INVALID, "the batch was created without 4-wide nodes");
     if (reinterpret_cast<uintptr_t>(mem) % 256 != 0)
@@ -1205,6 +1270,10 @@ int qk_batch_plan_create(qk_batch_plan** out, const qk_batch* b, int op, const i
         p->medium = reinterpret_cast<int*>(base + L.medium);
         p->large = reinterpret_cast<int*>(base + L.large);
         p->lane_counts = reinterpret_cast<int*>(base + L.lane_counts);
+        if (flags & QK_TUNE_STASH) {
+            Carve pc{base + L.pool};
+            p->pool = carve_pool(pc, static_cast<int>(total));
+        }
     }
     p->loop_ws = base + L.loop_ws;
     p->loop_ws_bytes = L.loop_ws_bytes;

@@ -631,17 +631,16 @@ __global__ __launch_bounds__(kBlock) void k_radius_bin(
     flush_stats<kStats>(active, tv.nodes, tv.leaves, tv.overflow, stats);
 }
 
-// Radius with a stash (QK_TUNE_STASH): the count pass also keeps each query's first kStash
-// keys (the traversal runs in fill mode into the query's stash slots and counts every match);
-// the fill pass then copies the stash for queries with at most kStash results and traverses
-// again only for the others.  The keys are the same, and the segment sort orders them.
-constexpr int kStash = 16;
-
+// Single-pass radius (QK_TUNE_STASH): the count pass stores every key it finds -- the first
+// kRadiusStash of a query in its stash slots, the rest in chained chunks of a shared pool
+// (PoolSink, qk_traverse.cuh) -- so the fill pass only copies each query's keys into its CSR
+// segment.  A query whose keys did not fit the pool is traversed again by the fill pass.  The
+// keys are the same either way, and the segment sort orders them.
 template <class Ops, bool kStats, bool kLeaf4 = false>
-__global__ __launch_bounds__(kBlock) void k_radius_count_stash(
+__global__ __launch_bounds__(kBlock) void k_radius_count_pool(
     const BNode* __restrict__ bn, const float4* __restrict__ leaves, const Node* __restrict__ nodes,
     const float* __restrict__ pts, const uint32_t* __restrict__ order, int count, float r2,
-    int* __restrict__ counts, unsigned long long* __restrict__ stash, int max_iter,
+    int* __restrict__ counts, RadiusPool pool, int max_iter,
     unsigned long long* __restrict__ stats, const Node* __restrict__ lnodes = nullptr) {
     const int i = blockIdx.x * kBlock + threadIdx.x;
     const bool active = i < count;
@@ -649,28 +648,27 @@ __global__ __launch_bounds__(kBlock) void k_radius_count_stash(
     if (active) {
         const int q = order ? static_cast<int>(order[i]) : i;
         const float3 p = f3(pts[3 * q], pts[3 * q + 1], pts[3 * q + 2]);
-        const int write = q * kStash;
+        pool.first[q] = -1;
+        PoolSink sink{pool.stash + static_cast<size_t>(q) * kRadiusStash, pool.keys, pool.next,
+                      pool.taken, pool.chunks, pool.first + q, 0, -1};
         LocalStack<kStack> st;
-        counts[q] = radius_bin_one<Ops, true, LocalStack<kStack>, kLeaf4>(
-            bn, leaves, root_box(nodes), p, r2, write, write + kStash, stash, max_iter, st, tv, lnodes);
+        counts[q] = radius_bin_visit<Ops, true, LocalStack<kStack>, kLeaf4>(
+            bn, leaves, root_box(nodes), p, r2, sink, max_iter, st, tv, lnodes);
     }
     flush_stats<kStats>(active, tv.nodes, tv.leaves, tv.overflow, stats);
 }
 
+// the single-pass radius's second traversal: only queries whose keys the pool could not hold
 template <class Ops, bool kLeaf4 = false>
-__global__ __launch_bounds__(kBlock) void k_radius_fill_stash(
+__global__ __launch_bounds__(kBlock) void k_radius_fill_lost(
     const BNode* __restrict__ bn, const float4* __restrict__ leaves, const Node* __restrict__ nodes,
-    const float* __restrict__ pts, const uint32_t* __restrict__ order, int count, float r2,
-    const int* __restrict__ offsets, const unsigned long long* __restrict__ stash,
-    unsigned long long* __restrict__ keys, int max_iter, const Node* __restrict__ lnodes = nullptr) {
-    const int i = blockIdx.x * kBlock + threadIdx.x;
-    if (i >= count) return;
-    const int q = order ? static_cast<int>(order[i]) : i;
+    const float* __restrict__ pts, int count, float r2, const int* __restrict__ offsets,
+    RadiusPool pool, unsigned long long* __restrict__ keys, int max_iter,
+    const Node* __restrict__ lnodes = nullptr) {
+    const int q = blockIdx.x * kBlock + threadIdx.x;
+    if (q >= count) return;
     const int begin = offsets[q], end = offsets[q + 1];
-    if (end - begin <= kStash) {
-        for (int j = 0; j < end - begin; ++j) keys[begin + j] = stash[static_cast<size_t>(q) * kStash + j];
-        return;
-    }
+    if (end - begin <= kRadiusStash || pool.first[q] != kPoolLost) return;
     const float3 p = f3(pts[3 * q], pts[3 * q + 1], pts[3 * q + 2]);
     Trav tv;
     LocalStack<kStack> st;
@@ -1193,7 +1191,7 @@ int knn_query(const qk_tree* t, const float* pts, int count, int k, int stride, 
     }
 }
 
-// the stash applies to the binary thread-per-query traversal only
+// the single-pass pool applies to the binary thread-per-query traversal only
 bool use_stash(unsigned flags) {
     return (flags & QK_TUNE_STASH) && !(flags & (QK_TUNE_SPLIT | QK_WIDE));
 }
@@ -1206,15 +1204,15 @@ size_t radius_ws_bytes(int count, unsigned flags) {
     c.take<int>(count);            // medium segment list
     c.take<int>(count);            // large segment list
     if (flags & QK_TUNE_SPLIT) c.take<int>(static_cast<size_t>(count) * 32);  // lane counts
-    if (use_stash(flags)) c.take<unsigned long long>(static_cast<size_t>(count) * kStash);
+    if (use_stash(flags)) carve_pool(c, count);
     return c.used;
 }
 
 template <class Ops>
-int radius_stash_launch(const qk_tree* t, const float* pts, int count, float r2, int* counts,
-                        const int* offsets, unsigned long long* stash, unsigned long long* keys,
-                        unsigned flags, unsigned long long* stats, const uint32_t* order,
-                        bool fill, cudaStream_t s) {
+int radius_pool_launch(const qk_tree* t, const float* pts, int count, float r2, int* counts,
+                       const int* offsets, const RadiusPool& pool, unsigned long long* keys,
+                       unsigned flags, unsigned long long* stats, const uint32_t* order,
+                       bool fill, cudaStream_t s) {
     const BNode* bn = static_cast<const BNode*>(t->bnodes);
     const Node* nodes = static_cast<const Node*>(t->nodes);
     const float4* leaves = static_cast<const float4*>(t->leaves);
@@ -1222,27 +1220,32 @@ int radius_stash_launch(const qk_tree* t, const float* pts, int count, float r2,
     const int it = t->n * 2 + 64;
     const bool leaf4 = (flags & QK_TUNE_LEAF4) != 0;
     if (fill) {
-        if (leaf4) k_radius_fill_stash<Ops, true><<<g, kBlock, 0, s>>>(bn, leaves, nodes, pts, order, count, r2, offsets, stash, keys, it, leaf_nodes(t));
-        else k_radius_fill_stash<Ops><<<g, kBlock, 0, s>>>(bn, leaves, nodes, pts, order, count, r2, offsets, stash, keys, it);
-    } else if (leaf4) {
-        if (stats) k_radius_count_stash<Ops, true, true><<<g, kBlock, 0, s>>>(bn, leaves, nodes, pts, order, count, r2, counts, stash, it, stats, leaf_nodes(t));
-        else k_radius_count_stash<Ops, false, true><<<g, kBlock, 0, s>>>(bn, leaves, nodes, pts, order, count, r2, counts, stash, it, stats, leaf_nodes(t));
+        k_radius_gather<<<blocks_for(static_cast<long long>(count) * 32), kBlock, 0, s>>>(
+            pool, offsets, count, keys, -1);
+        if (leaf4) k_radius_fill_lost<Ops, true><<<g, kBlock, 0, s>>>(bn, leaves, nodes, pts, count, r2, offsets, pool, keys, it, leaf_nodes(t));
+        else k_radius_fill_lost<Ops><<<g, kBlock, 0, s>>>(bn, leaves, nodes, pts, count, r2, offsets, pool, keys, it);
     } else {
-        if (stats) k_radius_count_stash<Ops, true><<<g, kBlock, 0, s>>>(bn, leaves, nodes, pts, order, count, r2, counts, stash, it, stats);
-        else k_radius_count_stash<Ops, false><<<g, kBlock, 0, s>>>(bn, leaves, nodes, pts, order, count, r2, counts, stash, it, stats);
+        cudaMemsetAsync(pool.taken, 0, sizeof(int), s);
+        if (leaf4) {
+            if (stats) k_radius_count_pool<Ops, true, true><<<g, kBlock, 0, s>>>(bn, leaves, nodes, pts, order, count, r2, counts, pool, it, stats, leaf_nodes(t));
+            else k_radius_count_pool<Ops, false, true><<<g, kBlock, 0, s>>>(bn, leaves, nodes, pts, order, count, r2, counts, pool, it, stats, leaf_nodes(t));
+        } else {
+            if (stats) k_radius_count_pool<Ops, true><<<g, kBlock, 0, s>>>(bn, leaves, nodes, pts, order, count, r2, counts, pool, it, stats);
+            else k_radius_count_pool<Ops, false><<<g, kBlock, 0, s>>>(bn, leaves, nodes, pts, order, count, r2, counts, pool, it, stats);
+        }
     }
     const cudaError_t e = cudaGetLastError();
-    return e == cudaSuccess ? QK_OK : cuda_status(e, "radius traversal (stash)");
+    return e == cudaSuccess ? QK_OK : cuda_status(e, "radius traversal (single pass)");
 }
 
-int radius_stash_dispatch(const qk_tree* t, const float* pts, int count, float r2, int* counts,
-                          const int* offsets, unsigned long long* stash, unsigned long long* keys,
-                          unsigned flags, unsigned long long* stats, const uint32_t* order,
-                          bool fill, cudaStream_t s) {
+int radius_pool_dispatch(const qk_tree* t, const float* pts, int count, float r2, int* counts,
+                         const int* offsets, const RadiusPool& pool, unsigned long long* keys,
+                         unsigned flags, unsigned long long* stats, const uint32_t* order,
+                         bool fill, cudaStream_t s) {
     switch (t->kind) {
-        case kTri: return radius_stash_launch<TriOps>(t, pts, count, r2, counts, offsets, stash, keys, flags, stats, order, fill, s);
-        case kPoint: return radius_stash_launch<PointOps>(t, pts, count, r2, counts, offsets, stash, keys, flags, stats, order, fill, s);
-        case kGauss: return radius_stash_launch<GaussOps>(t, pts, count, r2, counts, offsets, stash, keys, flags, stats, order, fill, s);
+        case kTri: return radius_pool_launch<TriOps>(t, pts, count, r2, counts, offsets, pool, keys, flags, stats, order, fill, s);
+        case kPoint: return radius_pool_launch<PointOps>(t, pts, count, r2, counts, offsets, pool, keys, flags, stats, order, fill, s);
+        case kGauss: return radius_pool_launch<GaussOps>(t, pts, count, r2, counts, offsets, pool, keys, flags, stats, order, fill, s);
         default: return fail(QK_ERR_INVALID, "unknown primitive kind %d", t->kind);
     }
 }
@@ -1261,14 +1264,14 @@ int radius_count(const qk_tree* t, const float* pts, int count, float r, int* of
     c.take<int>(count);
     c.take<int>(count);
     int* lane_counts = (flags & QK_TUNE_SPLIT) ? c.take<int>(static_cast<size_t>(count) * 32) : nullptr;
-    unsigned long long* stash =
-        use_stash(flags) ? c.take<unsigned long long>(static_cast<size_t>(count) * kStash) : nullptr;
+    const bool pooled = use_stash(flags);
+    const RadiusPool pool = pooled ? carve_pool(c, count) : RadiusPool{};
     int st = QK_OK;
     const uint32_t* order = make_order(pts, 3, 0, count, flags, o, s, &st);
     if (st != QK_OK) return st;
-    if (stash)
-        st = radius_stash_dispatch(t, pts, count, r * r, counts, nullptr, stash, nullptr, flags,
-                                   reinterpret_cast<unsigned long long*>(stats), order, false, s);
+    if (pooled)
+        st = radius_pool_dispatch(t, pts, count, r * r, counts, nullptr, pool, nullptr, flags,
+                                  reinterpret_cast<unsigned long long*>(stats), order, false, s);
     else
         st = radius_dispatch<false>(t, pts, count, r * r, counts, lane_counts, nullptr, nullptr, flags,
                                     reinterpret_cast<unsigned long long*>(stats), order, s);
@@ -1293,15 +1296,22 @@ int radius_fill(const qk_tree* t, const float* pts, int count, float r, const in
     int* medium = c.take<int>(count);
     int* large = c.take<int>(count);
     int* lane_counts = (flags & QK_TUNE_SPLIT) ? c.take<int>(static_cast<size_t>(count) * 32) : nullptr;
-    unsigned long long* stash =
-        use_stash(flags) ? c.take<unsigned long long>(static_cast<size_t>(count) * kStash) : nullptr;
+    const bool pooled = use_stash(flags);
+    const RadiusPool pool = pooled ? carve_pool(c, count) : RadiusPool{};
+    auto* k64 = reinterpret_cast<unsigned long long*>(keys);
     int st = QK_OK;
+    if (pooled) {
+        // the fill pass only copies (and traverses again the queries the pool could not hold,
+        // in query order): no ray order is needed
+        st = radius_pool_dispatch(t, pts, count, r * r, nullptr, offsets, pool, k64, flags, nullptr,
+                                  nullptr, true, s);
+        if (st != QK_OK) return st;
+        return radius_sort_segments(offsets, count, keys, medium, large, o.h, -1, s);
+    }
     const uint32_t* order = make_order(pts, 3, 0, count, flags, o, s, &st);
     if (st != QK_OK) return st;
-    auto* k64 = reinterpret_cast<unsigned long long*>(keys);
-    if (stash)
-        st = radius_stash_dispatch(t, pts, count, r * r, nullptr, offsets, stash, k64, flags, nullptr,
-                                   order, true, s);
+    if (false)
+        ;
     else
         st = radius_dispatch<true>(t, pts, count, r * r, nullptr, lane_counts, offsets, k64, flags,
                                    nullptr, order, s);

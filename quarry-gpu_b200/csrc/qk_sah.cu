@@ -1088,7 +1088,9 @@ __global__ __launch_bounds__(kBlock) void k_block_build(const Task* __restrict__
 // to primitive indices (cen / plo / phi), `tmp` is partition scratch of the same size.  A task
 // of up to 32 goes straight to warp_build, a larger one through warp_piece_tree; node ids come
 // from the task's reserved range, so the tree does not depend on scheduling.  No block-wide
-// barriers: each warp works on its own task.
+// barriers: each warp works on its own task.  A task of more than kTaskRange primitives is an
+// error unless `large_ok` says that the block builder (k_block_build) takes those tasks after
+// this launch (the forest of a topology edit, whose cuts grow by the primitives they receive).
 __global__ __launch_bounds__(kBlock, 4) void k_warp_tasks(const Task* __restrict__ tasks, int ntask,
                                                       const int* __restrict__ id_base,
                                                       int* __restrict__ order, int* __restrict__ tmp,
@@ -1096,7 +1098,7 @@ __global__ __launch_bounds__(kBlock, 4) void k_warp_tasks(const Task* __restrict
                                                       const float4* __restrict__ plo,
                                                       const float4* __restrict__ phi, Node* nodes,
                                                       BNode* bn, int* parent, int n, int bins,
-                                                      int* __restrict__ err) {
+                                                      int* __restrict__ err, int large_ok) {
     extern __shared__ unsigned wsm[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned* wb = wsm + static_cast<size_t>(warp) * 3 * bins * kBinWords;
@@ -1109,7 +1111,7 @@ __global__ __launch_bounds__(kBlock, 4) void k_warp_tasks(const Task* __restrict
         const Task tk = tasks[ti];
         const int count = tk.end - tk.begin;
         if (tk.node < 0 || count < 2 || count > kTaskRange) {
-            if (tk.node >= 0 && count > kTaskRange && lane == 0) atomicAdd(err, 1);
+            if (tk.node >= 0 && count > kTaskRange && !large_ok && lane == 0) atomicAdd(err, 1);
             continue;
         }
         if (count <= kWarpRange) {
@@ -1315,7 +1317,8 @@ int build_sah_impl(qk_tree* t, int bins, const void* items_v, void* ws, cudaStre
         // every range of at most kTaskRange primitives: one warp each (`alt` is free scratch)
         k_warp_tasks<<<min(blocks_for(static_cast<long long>(nblk) * 32), 148 * 8), kBlock,
                        warp_tasks_smem(bins), s>>>(w.blocks, nblk, w.id_base, ord, alt, w.cen,
-                                                   w.plo, w.phi, nodes, bn, t->parent, n, bins, err);
+                                                   w.plo, w.phi, nodes, bn, t->parent, n, bins, err,
+                                                   0);
     } else {
         int base = 0;
         cudaMemcpyAsync(&base, w.L.counters + 3, sizeof(int), cudaMemcpyDeviceToHost, s);
@@ -1357,7 +1360,8 @@ int sah_forest(const int4* tasks, int ntask, int max_count, const int* id_base, 
     BNode* bn = static_cast<BNode*>(t->bnodes);
     k_warp_tasks<<<min(blocks_for(static_cast<long long>(ntask) * 32), 148 * 8), kBlock,
                    warp_tasks_smem(bins), s>>>(tk, ntask, id_base, order, tmp, cen, plo, phi, nodes,
-                                               bn, t->parent, t->n, bins, err);
+                                               bn, t->parent, t->n, bins, err,
+                                               max_count > kTaskRange ? 1 : 0);
     if (max_count > kTaskRange) {
         cudaFuncSetAttribute(k_block_build, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              static_cast<int>(block_smem(kMaxBins)));

@@ -47,10 +47,30 @@ struct TopoPlan {
     int depth_need;  // deepest forest bound: cut depth + ceil(log2(m))
     int spliced;     // internal nodes spliced out
     int slots;       // new slot total (must be n_new)
-    int emit_err;    // out-of-range writes skipped by the emit (and forest builder errors)
+    int emit_err;    // out-of-range writes skipped by the emit
+    int emit_site;   // which checks fired (EmitSite bits); must follow emit_err
+    int forest_err;  // errors reported by the forest builders
     int noncontig;   // old subtrees whose slots are not contiguous
-    int pad[4];
+    int pad[2];
 };
+
+// The emit checks, one bit each in TopoPlan::emit_site (reported with the error).
+enum EmitSite {
+    kSiteNodes = 1,        // a kept node's new id or relinked child out of range
+    kSiteKeptLeaf = 2,     // a surviving leaf outside the cuts: slot or index out of range
+    kSiteStageCut = 4,     // a cut survivor's staging position out of range
+    kSiteStageExtra = 8,   // a new primitive's staging position out of range
+    kSiteCutOrder = 16,    // a forest position whose staged entry is out of range
+    kSiteCutLeaf = 32,     // a forest leaf: slot or index out of range
+    kSiteMovedId = 64,     // a moved index out of range
+    kSiteMovedLeaf = 128,  // a moved primitive's slot out of range
+};
+
+// Counts a failed emit check at `err` (TopoPlan::emit_err) and records its site.
+__device__ __forceinline__ void emit_fault(int* err, int site) {
+    atomicAdd(err, 1);
+    atomicOr(err + 1, site);
+}
 
 struct TopoWs {
     TopoPlan* plan;
@@ -190,10 +210,10 @@ __device__ __forceinline__ Box join(const Box& a, const Box& b) {
 // `err` (read back as an error before the tree is used) and skipped.
 template <class Ops>
 __device__ __forceinline__ void write_leaf(const qk_tree& t, int slot, const float* it, int id,
-                                           int* err) {
+                                           int* err, int site) {
     const int n = t.n;
     if (slot < 0 || slot >= n || id < 0 || id >= n) {
-        atomicAdd(err, 1);
+        emit_fault(err, site);
         return;
     }
     float* dst = static_cast<float*>(t.items) + static_cast<size_t>(slot) * Ops::kFloats;
@@ -446,7 +466,7 @@ __global__ __launch_bounds__(kBlock) void k_topo_nodes(Relink R, qk_tree t, int*
     const int r = relink(R, R.nodes[v].right);
     const int n = R.n_new;
     if (id < 0 || id >= n - 1 || l < 0 || l >= 2 * n - 1 || r < 0 || r >= 2 * n - 1) {
-        atomicAdd(err, 1);
+        emit_fault(err, kSiteNodes);
         return;
     }
     Node* nodes = static_cast<Node*>(t.nodes);
@@ -477,15 +497,15 @@ __global__ __launch_bounds__(kBlock) void k_topo_kept_leaves(EditDev e, const qk
     float buf[Ops::kFloats];
 #pragma unroll
     for (int q = 0; q < Ops::kFloats; ++q) buf[q] = it[q];
-    write_leaf<Ops>(t, xs[s], buf, remap_id(e, shifts, j), err);
+    write_leaf<Ops>(t, xs[s], buf, remap_id(e, shifts, j), err, kSiteKeptLeaf);
 }
 
 template <class Ops>
 __device__ __forceinline__ void stage(const float* it, int pos, int id, float* st_items,
                                       int* st_id, float4* cen, float4* plo, float4* phi,
-                                      int* order, int n, int* err) {
+                                      int* order, int n, int* err, int site) {
     if (pos < 0 || pos >= n) {
-        atomicAdd(err, 1);
+        emit_fault(err, site);
         return;
     }
     float buf[Ops::kFloats];
@@ -520,7 +540,7 @@ __global__ __launch_bounds__(kBlock) void k_topo_stage_cuts(
             if (del_flag[j]) continue;
             stage<Ops>(static_cast<const float*>(old_t.items) + static_cast<size_t>(s) * Ops::kFloats,
                        xs[s], remap_id(e, shifts, j), st_items, st_id, cen, plo, phi, order,
-                       e.n_new, err);
+                       e.n_new, err, kSiteStageCut);
         }
         if (threadIdx.x == 0) {
             const int B = xs[r.x], m = xs[r.x + r.y] - B;
@@ -559,7 +579,8 @@ __global__ __launch_bounds__(kBlock) void k_topo_stage_extra(
     const int first_kept = del_flag[old_t.prim_ids[r.x]] ? 0 : 1;
     const int k = static_cast<int>(val[i]);
     stage<Ops>(e.extra + static_cast<size_t>(k) * Ops::kFloats, xs[r.x] + first_kept + (i - lo),
-               extra_id(e, k), st_items, st_id, cen, plo, phi, order, e.n_new, err);
+               extra_id(e, k), st_items, st_id, cen, plo, phi, order, e.n_new, err,
+               kSiteStageExtra);
 }
 
 // per cut: the built order's primitives into the new tree's leaves
@@ -576,11 +597,11 @@ __global__ __launch_bounds__(kBlock) void k_topo_cut_leaves(const int4* __restri
         for (int pos = tk.x + threadIdx.x; pos < tk.y; pos += kBlock) {
             const int src = order[pos];
             if (src < 0 || src >= t.n) {
-                atomicAdd(err, 1);
+                emit_fault(err, kSiteCutOrder);
                 continue;
             }
             write_leaf<Ops>(t, pos, st_items + static_cast<size_t>(src) * Ops::kFloats, st_id[src],
-                            err);
+                            err, kSiteCutLeaf);
         }
     }
 }
@@ -591,11 +612,11 @@ __global__ __launch_bounds__(kBlock) void k_topo_moved(EditDev e, qk_tree t, int
     if (i >= e.n_mov) return;
     const int id = e.moved[i];
     if (id < 0 || id >= t.n) {
-        atomicAdd(err, 1);
+        emit_fault(err, kSiteMovedId);
         return;
     }
     write_leaf<Ops>(t, t.slot_of[id], e.moved_items + static_cast<size_t>(i) * Ops::kFloats, id,
-                    err);
+                    err, kSiteMovedLeaf);
 }
 
 template <class Ops>
@@ -713,7 +734,7 @@ int update_impl(const qk_tree* old_t, qk_tree* new_t, const qk_topo_edit* ed, in
     stage_mark(kMarkRelayout, s);
     if (plan.cuts > 0) {
         const int st = sah_forest(w.tasks, plan.cuts, plan.max_new, w.id_base, w.order, w.tmp,
-                                  w.cen, w.plo, w.phi, new_t, bins, eerr, s);
+                                  w.cen, w.plo, w.phi, new_t, bins, &w.plan->forest_err, s);
         if (st != QK_OK) return st;
         k_topo_cut_leaves<Ops><<<grid, kBlock, 0, s>>>(w.tasks, ncut_p, w.order, w.st_items,
                                                        w.st_id, *new_t, eerr);
@@ -722,12 +743,16 @@ int update_impl(const qk_tree* old_t, qk_tree* new_t, const qk_topo_edit* ed, in
     stage_mark(kMarkTopo, s);
     err = cudaGetLastError();
     // every emit write was checked; the bottom-up pass only runs over a fully linked tree
-    int emit_errors = 0;
+    int emit[3] = {0, 0, 0};  // emit_err, emit_site, forest_err
     if (err == cudaSuccess)
-        err = cudaMemcpyAsync(&emit_errors, eerr, sizeof(int), cudaMemcpyDeviceToHost, s);
+        err = cudaMemcpyAsync(emit, eerr, sizeof(emit), cudaMemcpyDeviceToHost, s);
     if (err == cudaSuccess) err = cudaStreamSynchronize(s);
     if (err != cudaSuccess) return cuda_status(err, "topology emit");
-    if (emit_errors) return fail(QK_ERR_OVERFLOW, "topology emit reported %d errors", emit_errors);
+    if (emit[0] || emit[2])
+        return fail(QK_ERR_OVERFLOW,
+                    "topology emit reported %d failed checks (sites 0x%x) and %d forest builder "
+                    "errors (%d cuts, largest %d primitives)",
+                    emit[0], emit[1], emit[2], plan.cuts, plan.max_new);
     const int st = finish_tree_boxes(new_t, w.h, w.new_range, s);
     if (st != QK_OK) return st;
     info->depth = new_t->depth;

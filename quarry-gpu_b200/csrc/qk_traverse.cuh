@@ -752,13 +752,129 @@ __device__ __forceinline__ unsigned long long radius_key(float d2, int id) {
     return (static_cast<unsigned long long>(__float_as_uint(d2)) << 32) | static_cast<unsigned>(id);
 }
 
-template <class Ops, bool kFill, class St, bool kLeaf4 = false>
-__device__ __forceinline__ int radius_bin_one(const BNode* __restrict__ bn,
-                                              const float4* __restrict__ leaves, const Box& rb,
-                                              float3 p, float r2, int write, int end,
-                                              unsigned long long* __restrict__ keys,
-                                              int max_iter, St& st, Trav& tv,
-                                              const Node* __restrict__ lnodes = nullptr) {
+// Where a radius traversal puts its keys.  SegmentSink: the query's CSR segment
+// keys[write, end) (the fill pass), never past its end.
+struct SegmentSink {
+    unsigned long long* keys;
+    int write;
+    int end;
+    __device__ __forceinline__ void put(unsigned long long k) {
+        if (write < end) keys[write++] = k;
+    }
+};
+
+// PoolSink: the single-pass radius (QK_TUNE_STASH).  A query's first kRadiusStash keys go to
+// its stash slots, later ones to chunks of kPoolChunk keys taken from a shared pool (one
+// atomic per chunk) and chained per query: *first holds the query's first chunk, next[c] the
+// chunk after c; the chain's length follows from the query's count, so it needs no end mark.
+// When the pool runs out, *first becomes kPoolLost and the query's later keys are dropped;
+// the fill pass traverses such a query again.  Only the thread that owns the query writes its
+// stash, its *first and its chain links.
+constexpr int kRadiusStash = 16;
+constexpr int kPoolChunk = 32;
+constexpr int kPoolLost = -2;
+
+// The single-pass radius's buffers for `count` queries, carved from a workspace: the stash
+// (kRadiusStash keys per query), the chain heads, the chunk counter, the chain links and the
+// pool itself (kPoolPerQuery keys per query on average, shared by all queries).
+constexpr int kPoolPerQuery = 128;
+
+struct RadiusPool {
+    unsigned long long* stash;
+    int* first;
+    int* taken;
+    int* next;
+    unsigned long long* keys;
+    int chunks;
+};
+
+inline RadiusPool carve_pool(Carve& c, int count) {
+    RadiusPool p{};
+    p.chunks = static_cast<int>((static_cast<long long>(count) * kPoolPerQuery + kPoolChunk - 1) /
+                                kPoolChunk);
+    p.stash = c.take<unsigned long long>(static_cast<size_t>(count) * kRadiusStash);
+    p.first = c.take<int>(count);
+    p.taken = c.take<int>(1);
+    p.next = c.take<int>(p.chunks);
+    p.keys = c.take<unsigned long long>(static_cast<size_t>(p.chunks) * kPoolChunk);
+    return p;
+}
+
+struct PoolSink {
+    unsigned long long* stash;   // this query's kRadiusStash slots
+    unsigned long long* pool;    // chunks of kPoolChunk keys
+    int* next;                   // chain links, one per chunk
+    int* taken;                  // chunks handed out so far (shared counter)
+    int chunks;                  // pool capacity in chunks
+    int* first;                  // this query's first chunk, or kPoolLost
+    int n;                       // keys seen so far
+    int cur;                     // the chunk being filled, or kPoolLost
+    __device__ __forceinline__ void put(unsigned long long k) {
+        if (n < kRadiusStash) {
+            stash[n++] = k;
+            return;
+        }
+        const int j = (n - kRadiusStash) & (kPoolChunk - 1);
+        const bool fresh = n == kRadiusStash;
+        ++n;
+        if (cur == kPoolLost) return;
+        if (j == 0) {
+            const int c = atomicAdd(taken, 1);
+            if (c >= chunks) {
+                cur = kPoolLost;
+                *first = kPoolLost;
+                return;
+            }
+            if (fresh) *first = c;
+            else next[cur] = c;
+            cur = c;
+        }
+        pool[static_cast<size_t>(cur) * kPoolChunk + j] = k;
+    }
+};
+
+// Copies query q's keys (its stash, then its pool chain) into keys[begin, begin + cnt), one
+// warp per query: lane l moves entry l of the stash and of every 32-key chunk, so the reads and
+// writes are coalesced.  Every lane of the warp calls it for the same q.
+static_assert(kPoolChunk == 32, "a pool chunk is one key per lane");
+__device__ __forceinline__ void copy_pooled_warp(const RadiusPool& pool, int q, int begin, int cnt,
+                                                 unsigned long long* __restrict__ keys, int lane) {
+    const int head = cnt < kRadiusStash ? cnt : kRadiusStash;
+    if (lane < head) keys[begin + lane] = pool.stash[static_cast<size_t>(q) * kRadiusStash + lane];
+    int left = cnt - head;
+    int w = begin + head;
+    int c = left > 0 ? pool.first[q] : -1;
+    while (left > 0) {
+        const int m = left < kPoolChunk ? left : kPoolChunk;
+        if (lane < m) keys[w + lane] = pool.keys[static_cast<size_t>(c) * kPoolChunk + lane];
+        w += m;
+        left -= m;
+        if (left > 0) c = pool.next[c];
+    }
+}
+
+// The copy pass of the single-pass radius: one warp per query whose keys the pool held (the
+// others are traversed again); skipped, as the fill is, when offsets[count] exceeds cap (cap <
+// 0: no limit).
+static __global__ __launch_bounds__(256) void k_radius_gather(RadiusPool pool,
+                                                       const int* __restrict__ offsets, int count,
+                                                       unsigned long long* __restrict__ keys,
+                                                       long long cap) {
+    const int q = static_cast<int>((static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (q >= count) return;
+    if (cap >= 0 && static_cast<long long>(offsets[count]) > cap) return;
+    const int begin = offsets[q], n = offsets[q + 1] - begin;
+    if (n > kRadiusStash && pool.first[q] == kPoolLost) return;
+    copy_pooled_warp(pool, q, begin, n, keys, lane);
+}
+
+template <class Ops, bool kFill, class St, bool kLeaf4, class Sink>
+__device__ __forceinline__ int radius_bin_visit(const BNode* __restrict__ bn,
+                                                const float4* __restrict__ leaves, const Box& rb,
+                                                float3 p, float r2, Sink& sink, int max_iter,
+                                                St& st, Trav& tv,
+                                                const Node* __restrict__ lnodes = nullptr) {
     int found = 0;
     if (!(dist2_box(p, rb.lo, rb.hi) <= r2)) return 0;
     int sp = 0;
@@ -780,7 +896,7 @@ __device__ __forceinline__ int radius_bin_one(const BNode* __restrict__ bn,
             int id;
             const float d2 = Ops::dist2(p, leaves, ~lref, id);
             if (d2 <= r2) {
-                if (kFill && write < end) keys[write++] = radius_key(d2, id);
+                if (kFill) sink.put(radius_key(d2, id));
                 ++found;
             }
             okl = false;
@@ -790,7 +906,7 @@ __device__ __forceinline__ int radius_bin_one(const BNode* __restrict__ bn,
             int id;
             const float d2 = Ops::dist2(p, leaves, ~rref, id);
             if (d2 <= r2) {
-                if (kFill && write < end) keys[write++] = radius_key(d2, id);
+                if (kFill) sink.put(radius_key(d2, id));
                 ++found;
             }
             okr = false;
@@ -808,7 +924,7 @@ __device__ __forceinline__ int radius_bin_one(const BNode* __restrict__ bn,
                         int id;
                         const float d2 = Ops::dist2(p, leaves, first + j, id);
                         if (d2 <= r2) {
-                            if (kFill && write < end) keys[write++] = radius_key(d2, id);
+                            if (kFill) sink.put(radius_key(d2, id));
                             ++found;
                         }
                     }
@@ -836,12 +952,23 @@ __device__ __forceinline__ int radius_bin_one(const BNode* __restrict__ bn,
     return found;
 }
 
-template <class Ops, bool kFill, class St>
-__device__ __forceinline__ int radius_wide_one(const WideNode* __restrict__ wn,
-                                               const float4* __restrict__ leaves, float3 p,
-                                               float r2, int write, int end,
-                                               unsigned long long* __restrict__ keys,
-                                               int max_iter, St& st, Trav& tv) {
+template <class Ops, bool kFill, class St, bool kLeaf4 = false>
+__device__ __forceinline__ int radius_bin_one(const BNode* __restrict__ bn,
+                                              const float4* __restrict__ leaves, const Box& rb,
+                                              float3 p, float r2, int write, int end,
+                                              unsigned long long* __restrict__ keys,
+                                              int max_iter, St& st, Trav& tv,
+                                              const Node* __restrict__ lnodes = nullptr) {
+    SegmentSink sink{keys, write, end};
+    return radius_bin_visit<Ops, kFill, St, kLeaf4>(bn, leaves, rb, p, r2, sink, max_iter, st, tv,
+                                                    lnodes);
+}
+
+template <class Ops, bool kFill, class St, class Sink>
+__device__ __forceinline__ int radius_wide_visit(const WideNode* __restrict__ wn,
+                                                 const float4* __restrict__ leaves, float3 p,
+                                                 float r2, Sink& sink, int max_iter, St& st,
+                                                 Trav& tv) {
     int found = 0;
     int sp = 0;
     int node = 0;
@@ -863,7 +990,7 @@ __device__ __forceinline__ int radius_wide_one(const WideNode* __restrict__ wn,
                 int id;
                 const float d2 = Ops::dist2(p, leaves, ~c, id);
                 if (d2 <= r2) {
-                    if (kFill && write < end) keys[write++] = radius_key(d2, id);
+                    if (kFill) sink.put(radius_key(d2, id));
                     ++found;
                 }
             } else if (next < 0) {
@@ -883,6 +1010,16 @@ __device__ __forceinline__ int radius_wide_one(const WideNode* __restrict__ wn,
         }
     }
     return found;
+}
+
+template <class Ops, bool kFill, class St>
+__device__ __forceinline__ int radius_wide_one(const WideNode* __restrict__ wn,
+                                               const float4* __restrict__ leaves, float3 p,
+                                               float r2, int write, int end,
+                                               unsigned long long* __restrict__ keys,
+                                               int max_iter, St& st, Trav& tv) {
+    SegmentSink sink{keys, write, end};
+    return radius_wide_visit<Ops, kFill>(wn, leaves, p, r2, sink, max_iter, st, tv);
 }
 
 // ---------------------------------------------------------------------------------------

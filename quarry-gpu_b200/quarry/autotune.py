@@ -186,7 +186,8 @@ def _device_name() -> str:
 # the engine's spaces
 # ---------------------------------------------------------------------------------------
 BATCH_SPACE = {
-    "flags": [0, 1, 4, 5],                 # QK_ORDER_MORTON = 1, QK_WIDE = 4
+    # QK_ORDER_MORTON = 1, QK_WIDE = 4; QK_TUNE_STASH = 8192 (single-pass radius, radius only)
+    "flags": [0, 1, 4, 5, 8192, 8193, 8196, 8197],
     "block": [128, 64, 256],
     "blocks_per_sm": [6, 4, 8, 2],
     "short_stack": [8, 0, 16],
@@ -207,8 +208,11 @@ def batch_launch(params: dict) -> dict:
 
 def batch_valid(op: str):
     """Points of BATCH_SPACE an operation accepts: the split schedule serves closest, kNN and
-    radius on binary nodes."""
+    radius on binary nodes; the single-pass flag is for radius plans (and the thread-per-query
+    schedule)."""
     def ok(p: dict) -> bool:
+        if p["flags"] & 8192 and (op != "radius" or p.get("split", 0)):
+            return False
         if not p.get("split", 0):
             return True
         return op != "rays" and not (p["flags"] & 4)

@@ -130,7 +130,7 @@ class BatchPipeline:
     def signature(self, ph: Phase) -> str:
         n = int(sum(s.items.shape[0] for s in self.scenes[ph.kind]))
         return (f"batch:{ph.kind}:{ph.name}:scenes={len(ph.counts)}:prims={n}:"
-                f"queries={int(ph.counts.sum())}:k={self.k}:space=2")
+                f"queries={int(ph.counts.sum())}:k={self.k}:space=3")
 
     def tune(self, tuner: autotune.Autotuner, force: bool = False, repeats: int = 3) -> dict:
         report = {}

@@ -163,6 +163,28 @@ def test_surgery_contiguous_delete_splices(cuda, cut):
     _same_results(tree, "point", new, 5)
 
 
+@pytest.mark.parametrize("kind", ["tri", "point"])
+def test_surgery_cut_grows_past_a_warp(cuda, kind):
+    """New primitives all landing in one cut push it past 256 primitives (the warp builder's
+    largest range): the block builder takes that subtree.  quarry's examples/dynamic_scene.cpp
+    makes such edits (props appended next to a cut of about 256 leaves)."""
+    rng = np.random.default_rng(41)
+    items = _items(kind, 40_000, 12)
+    tree = capi.DeviceTree(kind, items, builder="lbvh")
+    extra = np.repeat(items[100:101], 200, axis=0)
+    shift = rng.normal(0, 1e-3, (200, 3)).astype(np.float32)
+    if kind == "tri":
+        extra += np.tile(shift, 3)
+    else:
+        extra[:, :3] += shift
+    new = np.concatenate([items, extra]).astype(np.float32)
+    info = tree.update_topology(new, [], [], [], cut_size=250)
+    assert info["rebuild"] == 0, info
+    assert info["max_cut"] > 256, info
+    assert tree.validate() == [0] * 8
+    _same_results(tree, kind, new, 17, capi.DeviceTree(kind, new))
+
+
 def test_surgery_declines_large_edits(cuda):
     rng = np.random.default_rng(31)
     items = _items("point", 8_000, 6)

@@ -948,6 +948,11 @@ def points_arm(args, world, rank, local):
                 "leaf4": capi.QK_TUNE_LEAF4, "leaf4_morton": capi.QK_TUNE_LEAF4 | capi.QK_ORDER_MORTON,
                 "bin_coh": capi.QK_ORDER_COHERENT, "split_coh": capi.QK_TUNE_SPLIT | capi.QK_ORDER_COHERENT,
                 "leaf4_coh": capi.QK_TUNE_LEAF4 | capi.QK_ORDER_COHERENT}
+    # the heavy-query tail (closest / kNN): shell queries near the centre go to the shared scan
+    tail = capi.QK_TUNE_TAIL
+    tail_variants = {"bin_tail": tail, "bin_coh_tail": tail | capi.QK_ORDER_COHERENT,
+                     "split_tail": capi.QK_TUNE_SPLIT | tail,
+                     "split_coh_tail": capi.QK_TUNE_SPLIT | capi.QK_ORDER_COHERENT | tail}
     radius_variants = {"stash": capi.QK_TUNE_STASH,
                        "stash_morton": capi.QK_TUNE_STASH | capi.QK_ORDER_MORTON,
                        "stash_leaf4": capi.QK_TUNE_STASH | capi.QK_TUNE_LEAF4,
@@ -957,7 +962,8 @@ def points_arm(args, world, rank, local):
         for op in ops:
             run(kind, op, c["trees"]["lbvh"], 0)
             base = snapshot((kind, op))
-            cands = {**variants, **radius_variants} if op == "radius" else variants
+            cands = ({**variants, **radius_variants} if op == "radius" else
+                     {**variants, **tail_variants})
             for bname, tree in c["trees"].items():
                 for vname, f in cands.items():
                     run(kind, op, tree, f)
@@ -969,6 +975,7 @@ def points_arm(args, world, rank, local):
                         plan[(kind, op)] = (bname, vname, t)
 
     variants.update(radius_variants)
+    variants.update(tail_variants)
 
     def step():
         for (kind, op), (bname, vname, _) in plan.items():

@@ -62,12 +62,22 @@ extern "C" {
 #define QK_TUNE_SHORT_STACK 2048u /* binary rays: top 8 stack entries per thread in shared memory */
 #define QK_TUNE_LEAF4 4096u      /* binary nodes: child subtrees of 2..4 primitives are tested
                                     as leaves (skips their inner boxes) */
-#define QK_TUNE_STASH 8192u     /* radius, binary thread-per-query: the count pass keeps each
-                                    query's first 16 keys in the workspace and the fill pass
-                                    traverses again only for queries with more (pass the same
-                                    workspace and flags to qk_radius_count and qk_radius_fill) */
+#define QK_TUNE_STASH 8192u     /* single-pass radius (binary nodes, one thread per query;
+                                    batched plans on 4-wide nodes too; ignored with
+                                    QK_TUNE_SPLIT): the count pass keeps every key it finds -- a
+                                    query's first 16 in its stash, the rest in chained 32-key
+                                    chunks of a pool of 128 keys per query in the workspace --
+                                    and the fill pass copies them, traversing again only the
+                                    queries the pool could not hold (pass the same workspace
+                                    and flags to qk_radius_count and qk_radius_fill; a batched
+                                    radius plan takes it as a plan flag) */
 #define QK_TUNE_SPLIT 1024u      /* closest / kNN / radius on binary nodes: one warp per query,
                                     lanes on disjoint subtrees sharing the pruning bound */
+#define QK_TUNE_TAIL 16384u      /* closest / kNN on point clouds, binary nodes (thread or warp
+                                    per query): a query still traversing after a step budget is
+                                    answered by a brute-force scan over all points that every
+                                    such query shares, merged per query (the workspace grows by
+                                    33.5 MB + 4 bytes per query; ignored for other kinds) */
 
 /*
  * Device arrays of one tree.  The caller allocates every array (sizes from qk_tree_bytes)
@@ -296,6 +306,24 @@ int qk_ray_t_grad(const qk_tree* tree, const void* items, const void* rays, cons
                   const float* grad_t, int count, float* grad_tris, float* grad_rays,
                   void* workspace, size_t workspace_bytes, void* stream);
 
+/* Vertex form of qk_ray_t_grad and qk_distance_grad (triangle trees), for meshes given as
+ * shared vertices and corner indices: indices holds the n x 3 vertex ids of the tree's
+ * triangles in scene order.  The per-query FP64 terms are summed straight into grad_verts
+ * (nverts x 3) in FP64 and rounded to FP32 once, in a fixed order (deterministic), so a vertex
+ * whose terms cancel keeps its precision; the per-triangle path rounds each triangle's sum
+ * first.  grad_rays / grad_points as in the per-triangle calls. */
+size_t qk_grad_vertices_workspace_bytes(int count);
+int qk_ray_t_grad_vertices(const qk_tree* tree, const void* items, const void* rays,
+                           const int32_t* ids, const float* grad_t, int count,
+                           const int32_t* indices, int nverts, float* grad_verts,
+                           float* grad_rays, void* workspace, size_t workspace_bytes,
+                           void* stream);
+int qk_distance_grad_vertices(const qk_tree* tree, const void* items, const float* points,
+                              const void* results, const float* grad_dist, int count,
+                              const int32_t* indices, int nverts, float* grad_points,
+                              float* grad_verts, void* workspace, size_t workspace_bytes,
+                              void* stream);
+
 /* Deterministic segmented sum: out[k, c] = sum over i in increasing order with keys[i] == k of
  * values[i, c] (FP64 accumulation); keys < 0 are skipped.  1 <= channels <= 10. */
 int qk_segment_sum(const int32_t* keys, const float* values, int count, int channels, int segments,
@@ -377,7 +405,8 @@ void qk_batch_destroy(qk_batch* batch);
 /* A query plan: per-scene query counts of one operation (concatenated by scene in the
  * inputs and outputs) and, for QK_OP_RADIUS, the per-scene radius (host floats).
  * flags: QK_ORDER_MORTON (scene-major Morton order of the inputs, within each scene's
- * bounds) and QK_WIDE (traverse the 4-wide nodes). */
+ * bounds), QK_WIDE (traverse the 4-wide nodes) and, for QK_OP_RADIUS, QK_TUNE_STASH (the
+ * single-pass radius; the plan then holds its stash and key pool). */
 size_t qk_batch_plan_bytes(const qk_batch* batch, int op, const int32_t* counts,
                            unsigned flags);
 int qk_batch_plan_create(qk_batch_plan** out, const qk_batch* batch, int op,

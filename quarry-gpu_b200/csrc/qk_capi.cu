@@ -143,8 +143,7 @@ size_t qk_build_workspace_bytes(int kind, int n, int builder) {
 }
 
 size_t qk_query_workspace_bytes(int count, unsigned flags) {
-    (void)flags;
-    return count > 0 ? order_ws_bytes(count) : 0;
+    return count > 0 ? point_query_ws_bytes(count, flags) : 0;
 }
 
 size_t qk_radius_workspace_bytes(int count, unsigned flags) {
@@ -400,6 +399,42 @@ int qk_ray_t_grad(const qk_tree* tree, const void* items, const void* rays, cons
                       as_stream(stream));
 }
 
+size_t qk_grad_vertices_workspace_bytes(int count) {
+    return count >= 0 ? grad_vertices_ws_bytes(count) : 0;
+}
+
+int qk_ray_t_grad_vertices(const qk_tree* tree, const void* items, const void* rays,
+                           const int32_t* ids, const float* grad_t, int count,
+                           const int32_t* indices, int nverts, float* grad_verts,
+                           float* grad_rays, void* workspace, size_t workspace_bytes,
+                           void* stream) {
+    int st = check_tree(tree);
+    if (st) return st;
+    if (tree->kind != QK_TRI) return fail(QK_ERR_INVALID, "ray gradients need a triangle tree");
+    if (count < 0 || nverts < 1) return fail(QK_ERR_INVALID, "negative ray count or no vertices");
+    if (!items || !indices || !grad_verts || (count > 0 && (!rays || !ids)))
+        return fail(QK_ERR_INVALID, "NULL array");
+    if ((st = check_ws(workspace, workspace_bytes, grad_vertices_ws_bytes(count)))) return st;
+    return ray_t_grad_vertices(tree->n, items, rays, ids, grad_t, count, indices, nverts,
+                               grad_verts, grad_rays, workspace, as_stream(stream));
+}
+
+int qk_distance_grad_vertices(const qk_tree* tree, const void* items, const float* points,
+                              const void* results, const float* grad_dist, int count,
+                              const int32_t* indices, int nverts, float* grad_points,
+                              float* grad_verts, void* workspace, size_t workspace_bytes,
+                              void* stream) {
+    int st = check_tree(tree);
+    if (st) return st;
+    if (tree->kind != QK_TRI) return fail(QK_ERR_INVALID, "vertex gradients need a triangle tree");
+    if (count < 0 || nverts < 1) return fail(QK_ERR_INVALID, "negative query count or no vertices");
+    if (!items || !indices || !grad_verts || (count > 0 && (!points || !results || !grad_points)))
+        return fail(QK_ERR_INVALID, "NULL array");
+    if ((st = check_ws(workspace, workspace_bytes, grad_vertices_ws_bytes(count)))) return st;
+    return distance_grad_vertices(tree->n, items, points, results, grad_dist, count, indices,
+                                  nverts, grad_points, grad_verts, workspace, as_stream(stream));
+}
+
 int qk_segment_sum(const int32_t* keys, const float* values, int count, int channels, int segments,
                    float* out, void* workspace, size_t workspace_bytes, void* stream) {
     if (count < 0 || segments < 0 || channels < 1 || channels > 10)
@@ -419,7 +454,7 @@ int qk_closest(const qk_tree* tree, const float* points, int count, void* out, u
     if (count > 0 && (!points || !out)) return fail(QK_ERR_INVALID, "points or out is NULL");
     if (flags & QK_ORDER_DIRECTION) return fail(QK_ERR_INVALID, "direction order is for rays");
     if ((st = check_wide(tree, flags))) return st;
-    if ((st = check_ws(workspace, workspace_bytes, order_ws_bytes(count)))) return st;
+    if ((st = check_ws(workspace, workspace_bytes, point_query_ws_bytes(count, flags)))) return st;
     return closest_query(tree, points, count, out, flags, stats, workspace, as_stream(stream));
 }
 
@@ -434,7 +469,7 @@ int qk_knn(const qk_tree* tree, const float* points, int count, int k, int strid
     if (count > 0 && (!points || !out)) return fail(QK_ERR_INVALID, "points or out is NULL");
     if (flags & QK_ORDER_DIRECTION) return fail(QK_ERR_INVALID, "direction order is for rays");
     if ((st = check_wide(tree, flags))) return st;
-    if ((st = check_ws(workspace, workspace_bytes, order_ws_bytes(count)))) return st;
+    if ((st = check_ws(workspace, workspace_bytes, point_query_ws_bytes(count, flags)))) return st;
     return knn_query(tree, points, count, k, stride, out, flags, stats, workspace,
                      as_stream(stream));
 }

@@ -130,13 +130,13 @@ __global__ __launch_bounds__(kBlock) void k_dist_grad(const float* __restrict__ 
                                                      const uint2* __restrict__ res,
                                                      const float* __restrict__ gw, int count,
                                                      float* __restrict__ gpts,
-                                                     float* __restrict__ contrib,
+                                                     double* __restrict__ contrib,
                                                      int* __restrict__ keys) {
     const int i = blockIdx.x * kBlock + threadIdx.x;
     if (i >= count) return;
     const int id = static_cast<int>(res[i].y);
-    float* c = contrib + static_cast<size_t>(i) * stride;
-    for (int j = 0; j < stride; ++j) c[j] = 0.0f;
+    double* c = contrib + static_cast<size_t>(i) * stride;
+    for (int j = 0; j < stride; ++j) c[j] = 0.0;
     gpts[3 * i] = gpts[3 * i + 1] = gpts[3 * i + 2] = 0.0f;
     keys[i] = id;  // -1: no primitive, sorts first and is dropped
     if (id < 0) return;
@@ -157,9 +157,9 @@ __global__ __launch_bounds__(kBlock) void k_dist_grad(const float* __restrict__ 
         gpts[3 * i + 2] = static_cast<float>(n.z);
         const double w3[3] = {wa, wb, wc};
         for (int k = 0; k < 3; ++k) {
-            c[3 * k] = static_cast<float>(-w3[k] * n.x);
-            c[3 * k + 1] = static_cast<float>(-w3[k] * n.y);
-            c[3 * k + 2] = static_cast<float>(-w3[k] * n.z);
+            c[3 * k] = -w3[k] * n.x;
+            c[3 * k + 1] = -w3[k] * n.y;
+            c[3 * k + 2] = -w3[k] * n.z;
         }
     } else if (kKind == kPoint) {
         const D3 e = dsub(p, ld3(it));
@@ -169,9 +169,9 @@ __global__ __launch_bounds__(kBlock) void k_dist_grad(const float* __restrict__ 
         gpts[3 * i] = static_cast<float>(n.x);
         gpts[3 * i + 1] = static_cast<float>(n.y);
         gpts[3 * i + 2] = static_cast<float>(n.z);
-        c[0] = static_cast<float>(-n.x);
-        c[1] = static_cast<float>(-n.y);
-        c[2] = static_cast<float>(-n.z);
+        c[0] = -n.x;
+        c[1] = -n.y;
+        c[2] = -n.z;
     } else {
         D3 u, v, w;
         double qn[4], qlen;
@@ -187,13 +187,13 @@ __global__ __launch_bounds__(kBlock) void k_dist_grad(const float* __restrict__ 
         gpts[3 * i] = static_cast<float>(g * nw.x);
         gpts[3 * i + 1] = static_cast<float>(g * nw.y);
         gpts[3 * i + 2] = static_cast<float>(g * nw.z);
-        c[0] = static_cast<float>(-g * nw.x);
-        c[1] = static_cast<float>(-g * nw.y);
-        c[2] = static_cast<float>(-g * nw.z);
+        c[0] = -g * nw.x;
+        c[1] = -g * nw.y;
+        c[2] = -g * nw.z;
         // scales: -n_l,i * x_i / s_i
-        c[7] = static_cast<float>(-g * nl.x * x.x / s.x);
-        c[8] = static_cast<float>(-g * nl.y * x.y / s.y);
-        c[9] = static_cast<float>(-g * nl.z * x.z / s.z);
+        c[7] = -g * nl.x * x.x / s.x;
+        c[8] = -g * nl.y * x.y / s.y;
+        c[9] = -g * nl.z * x.z / s.z;
         // axes: dd/du = n_l.x dp, dd/dv = n_l.y dp, dd/dw = n_l.z dp
         const D3 gu = dmul(dp, nl.x), gv = dmul(dp, nl.y), gwv = dmul(dp, nl.z);
         const double X = qn[0], Y = qn[1], Z = qn[2], W = qn[3];
@@ -210,7 +210,7 @@ __global__ __launch_bounds__(kBlock) void k_dist_grad(const float* __restrict__ 
         // through q_hat = q / |q|: (I - q_hat q_hat^T) / |q|
         const double dotq = gq[0] * X + gq[1] * Y + gq[2] * Z + gq[3] * W;
         const double inv = qlen > 0.0 ? g / qlen : g;
-        for (int k = 0; k < 4; ++k) c[3 + k] = static_cast<float>((gq[k] - dotq * qn[k]) * inv);
+        for (int k = 0; k < 4; ++k) c[3 + k] = (gq[k] - dotq * qn[k]) * inv;
     }
 }
 
@@ -219,14 +219,14 @@ __global__ __launch_bounds__(kBlock) void k_ray_grad(const float* __restrict__ t
                                                     const float* __restrict__ rays,
                                                     const int* __restrict__ ids,
                                                     const float* __restrict__ gw, int count,
-                                                    float* __restrict__ contrib,
+                                                    double* __restrict__ contrib,
                                                     int* __restrict__ keys,
                                                     float* __restrict__ grays) {
     const int i = blockIdx.x * kBlock + threadIdx.x;
     if (i >= count) return;
     const int id = ids[i];
-    float* c = contrib + static_cast<size_t>(i) * 9;
-    for (int j = 0; j < 9; ++j) c[j] = 0.0f;
+    double* c = contrib + static_cast<size_t>(i) * 9;
+    for (int j = 0; j < 9; ++j) c[j] = 0.0;
     if (grays) for (int j = 0; j < 6; ++j) grays[6 * i + j] = 0.0f;
     keys[i] = id;
     if (id < 0) return;
@@ -249,9 +249,9 @@ __global__ __launch_bounds__(kBlock) void k_ray_grad(const float* __restrict__ t
     const double w3[3] = {1.0 - u - v, u, v};
     const D3 k = dmul(n, g / nd);
     for (int j = 0; j < 3; ++j) {
-        c[3 * j] = static_cast<float>(w3[j] * k.x);
-        c[3 * j + 1] = static_cast<float>(w3[j] * k.y);
-        c[3 * j + 2] = static_cast<float>(w3[j] * k.z);
+        c[3 * j] = w3[j] * k.x;
+        c[3 * j + 1] = w3[j] * k.y;
+        c[3 * j + 2] = w3[j] * k.z;
     }
     if (grays) {
         grays[6 * i] = static_cast<float>(-k.x);
@@ -263,10 +263,12 @@ __global__ __launch_bounds__(kBlock) void k_ray_grad(const float* __restrict__ t
     }
 }
 
-// one thread per segment key: sum its run (sorted order = query order) in FP64
+// one thread per segment key: sum its run (sorted order = query order) in FP64; values are
+// the FP64 per-query terms of the adjoints, or a caller's FP32 values (qk_segment_sum)
+template <class V>
 __global__ __launch_bounds__(kBlock) void k_segment_sum(const uint32_t* __restrict__ skeys,
                                                        const uint32_t* __restrict__ sidx,
-                                                       const float* __restrict__ vals, int count,
+                                                       const V* __restrict__ vals, int count,
                                                        int channels, int nseg,
                                                        float* __restrict__ out) {
     const int k = blockIdx.x * kBlock + threadIdx.x;
@@ -280,8 +282,8 @@ __global__ __launch_bounds__(kBlock) void k_segment_sum(const uint32_t* __restri
     }
     double acc[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     for (int j = lo; j < count && skeys[j] == want; ++j) {
-        const float* v = vals + static_cast<size_t>(sidx[j]) * channels;
-        for (int ch = 0; ch < channels && ch < 10; ++ch) acc[ch] += v[ch];
+        const V* v = vals + static_cast<size_t>(sidx[j]) * channels;
+        for (int ch = 0; ch < channels && ch < 10; ++ch) acc[ch] += static_cast<double>(v[ch]);
     }
     for (int ch = 0; ch < channels && ch < 10; ++ch) out[static_cast<size_t>(k) * channels + ch] = static_cast<float>(acc[ch]);
 }
@@ -295,7 +297,7 @@ __global__ void k_shift_keys(const int* __restrict__ keys, int count, uint32_t* 
 }
 
 struct GradWs {
-    float* contrib;
+    double* contrib;
     int* keys;
     uint32_t* k32;
     uint32_t* idx;
@@ -306,7 +308,7 @@ struct GradWs {
 
 GradWs carve_grad(Carve& c, int count, int channels) {
     GradWs g;
-    g.contrib = c.take<float>(static_cast<size_t>(count) * channels);
+    g.contrib = c.take<double>(static_cast<size_t>(count) * channels);
     g.keys = c.take<int>(count);
     g.k32 = c.take<uint32_t>(count);
     g.idx = c.take<uint32_t>(count);
@@ -316,7 +318,8 @@ GradWs carve_grad(Carve& c, int count, int channels) {
     return g;
 }
 
-int segment_sum_impl(const int* keys, const float* vals, int count, int channels, int nseg,
+template <class V>
+int segment_sum_impl(const int* keys, const V* vals, int count, int channels, int nseg,
                      float* out, GradWs& g, cudaStream_t s) {
     if (nseg <= 0) return QK_OK;
     if (count <= 0) {
@@ -328,12 +331,80 @@ int segment_sum_impl(const int* keys, const float* vals, int count, int channels
     while (bits < 32 && (1ull << bits) <= static_cast<unsigned long long>(nseg)) ++bits;
     cudaError_t e = sort_pairs(g.k32, g.idx, g.k32s, g.idxs, count, bits, g.sort_ws, s);
     if (e != cudaSuccess) return cuda_status(e, "gradient sort");
-    k_segment_sum<<<blocks_for(nseg), kBlock, 0, s>>>(g.k32s, g.idxs, vals, count, channels, nseg, out);
+    k_segment_sum<V><<<blocks_for(nseg), kBlock, 0, s>>>(g.k32s, g.idxs, vals, count, channels, nseg, out);
     e = cudaGetLastError();
     return e == cudaSuccess ? QK_OK : cuda_status(e, "segment sum");
 }
 
+// Corner e = 3 q + j of query q's selected triangle -> its vertex (indices, n x 3), or -1.
+__global__ void k_corner_keys(const int* __restrict__ tri_of, const int* __restrict__ indices,
+                              int count, int n, int nverts, int* __restrict__ vkeys) {
+    const int e = blockIdx.x * kBlock + threadIdx.x;
+    if (e >= 3 * count) return;
+    const int t = tri_of[e / 3];
+    int v = -1;
+    if (t >= 0 && t < n) {
+        v = indices[3 * t + e % 3];
+        if (v < 0 || v >= nverts) v = -1;
+    }
+    vkeys[e] = v;
+}
+
+// vertex form: per-query terms (count x 9), their triangles, then the corner keys; the sort
+// and sum run over 3 count corner entries of 3 channels
+GradWs carve_grad_vertices(Carve& c, int count, int** tri_of) {
+    GradWs g;
+    g.contrib = c.take<double>(static_cast<size_t>(count) * 9);
+    *tri_of = c.take<int>(count);
+    g.keys = c.take<int>(3 * static_cast<size_t>(count));
+    g.k32 = c.take<uint32_t>(3 * static_cast<size_t>(count));
+    g.idx = c.take<uint32_t>(3 * static_cast<size_t>(count));
+    g.k32s = c.take<uint32_t>(3 * static_cast<size_t>(count));
+    g.idxs = c.take<uint32_t>(3 * static_cast<size_t>(count));
+    g.sort_ws = c.take<char>(sort_ws_bytes(3 * count));
+    return g;
+}
+
 }  // namespace
+
+size_t grad_vertices_ws_bytes(int count) {
+    Carve c;
+    int* t = nullptr;
+    carve_grad_vertices(c, count, &t);
+    return c.used;
+}
+
+int ray_t_grad_vertices(int n, const void* tris, const void* rays, const int* ids, const float* gw,
+                        int count, const int* indices, int nverts, float* gverts, float* grays,
+                        void* ws, cudaStream_t s) {
+    Carve c{static_cast<char*>(ws)};
+    int* tri_of = nullptr;
+    GradWs g = carve_grad_vertices(c, count, &tri_of);
+    if (count > 0) {
+        k_ray_grad<<<blocks_for(count), kBlock, 0, s>>>(static_cast<const float*>(tris),
+                                                        static_cast<const float*>(rays), ids, gw,
+                                                        count, g.contrib, tri_of, grays);
+        k_corner_keys<<<blocks_for(3ll * count), kBlock, 0, s>>>(tri_of, indices, count, n, nverts,
+                                                                 g.keys);
+    }
+    return segment_sum_impl<double>(g.keys, g.contrib, 3 * count, 3, nverts, gverts, g, s);
+}
+
+int distance_grad_vertices(int n, const void* tris, const float* pts, const void* res,
+                           const float* gw, int count, const int* indices, int nverts,
+                           float* gpts, float* gverts, void* ws, cudaStream_t s) {
+    Carve c{static_cast<char*>(ws)};
+    int* tri_of = nullptr;
+    GradWs g = carve_grad_vertices(c, count, &tri_of);
+    if (count > 0) {
+        k_dist_grad<kTri><<<blocks_for(count), kBlock, 0, s>>>(
+            static_cast<const float*>(tris), 9, pts, static_cast<const uint2*>(res), gw, count, gpts,
+            g.contrib, tri_of);
+        k_corner_keys<<<blocks_for(3ll * count), kBlock, 0, s>>>(tri_of, indices, count, n, nverts,
+                                                                 g.keys);
+    }
+    return segment_sum_impl<double>(g.keys, g.contrib, 3 * count, 3, nverts, gverts, g, s);
+}
 
 size_t grad_ws_bytes(int count, int channels) {
     Carve c;

@@ -149,6 +149,8 @@ int validate_tree(const qk_tree* t, const void* items, int* errors, void* ws, cu
 
 // ---- traversal (qk_query.cu) ----
 size_t order_ws_bytes(int count);
+// closest / kNN workspace: the order buffers plus, with QK_TUNE_TAIL, the heavy-query tail's
+size_t point_query_ws_bytes(int count, unsigned flags);
 int ray_query(const qk_tree* t, const void* rays, int count, uint64_t* out, int* ids,
               unsigned flags, uint64_t* stats, void* ws, cudaStream_t s);
 int closest_query(const qk_tree* t, const float* pts, int count, void* out, unsigned flags,
@@ -174,5 +176,12 @@ int ray_t_grad(int n, const void* tris, const void* rays, const int* ids, const 
                int count, float* gtris, float* grays, void* ws, cudaStream_t s);
 int segment_sum(const int* keys, const float* vals, int count, int channels, int nseg, float* out,
                 void* ws, cudaStream_t s);
+size_t grad_vertices_ws_bytes(int count);
+int ray_t_grad_vertices(int n, const void* tris, const void* rays, const int* ids, const float* gw,
+                        int count, const int* indices, int nverts, float* gverts, float* grays,
+                        void* ws, cudaStream_t s);
+int distance_grad_vertices(int n, const void* tris, const float* pts, const void* res,
+                           const float* gw, int count, const int* indices, int nverts,
+                           float* gpts, float* gverts, void* ws, cudaStream_t s);
 
 }  // namespace qk

@@ -523,6 +523,32 @@ __global__ __launch_bounds__(kBlock) void k_ray_wide(const WideNode* __restrict_
     flush_stats<kStats>(active, tv.nodes, tv.leaves, tv.overflow, stats);
 }
 
+// ---------------------------------------------------------------------------------------
+// heavy-query tail (QK_TUNE_TAIL, point clouds).  A point near the centre of a spherical shell
+// has most of the shell at almost the same distance, so its search ball admits most of the
+// tree: a few such queries take most of a step while the GPU is nearly idle.  With the flag,
+// the binary closest / kNN kernels stop a query after a step budget and list it; the listed
+// queries are then answered by one brute-force scan over all points that every listed query
+// shares (point tiles x heavy-query batches), merged per query.  The scan computes the same
+// dist2 as the leaf test and keeps the same (dist2, id) order, so results are bit-identical.
+// ---------------------------------------------------------------------------------------
+constexpr int kTailCap = 1024;           // heavy queries the scan answers (the rest traverse again)
+constexpr int kTailBatch = 256;          // heavy queries per scan block, one per thread
+constexpr int kTailCands = 4096;         // candidates kept per heavy query (tiles x K)
+constexpr int kTailBudgetThread = 2048;  // traversal steps of a thread-per-query query
+constexpr int kTailBudgetLane = 192;     // traversal steps of each lane of a warp-per-query one
+
+struct TailList {
+    int* count = nullptr;      // heavy queries listed
+    int* list = nullptr;       // their query indices (capacity: every query)
+    uint2* partial = nullptr;  // kTailCap x kTailCands candidates (dist2 bits, id)
+};
+
+__device__ __forceinline__ void tail_append(const TailList& tail, int q) {
+    const int h = atomicAdd(tail.count, 1);
+    tail.list[h] = q;
+}
+
 template <class Ops, bool kStats, bool kLeaf4 = false>
 __global__ __launch_bounds__(kBlock) void k_closest_bin(const BNode* __restrict__ bn,
                                                        const float4* __restrict__ leaves,
@@ -530,7 +556,8 @@ __global__ __launch_bounds__(kBlock) void k_closest_bin(const BNode* __restrict_
                                                        const uint32_t* __restrict__ order,
                                                        int count, uint2* __restrict__ out,
                                                        int max_iter, unsigned long long* __restrict__ stats,
-                                                       const Node* __restrict__ lnodes = nullptr) {
+                                                       const Node* __restrict__ lnodes = nullptr,
+                                                       TailList tail = TailList{}) {
     const int i = blockIdx.x * kBlock + threadIdx.x;
     const bool active = i < count;
     Trav tv;
@@ -540,6 +567,7 @@ __global__ __launch_bounds__(kBlock) void k_closest_bin(const BNode* __restrict_
         LocalStack<kStack> st;
         out[q] = closest_bin_one<Ops, LocalStack<kStack>, kLeaf4>(bn, leaves, p, max_iter, st, tv,
                                                                   lnodes);
+        if (tail.count && tv.overflow) tail_append(tail, q);
     }
     flush_stats<kStats>(active, tv.nodes, tv.leaves, tv.overflow, stats);
 }
@@ -570,7 +598,8 @@ __global__ __launch_bounds__(kBlock) void k_knn_bin(const BNode* __restrict__ bn
                                                    const uint32_t* __restrict__ order, int count,
                                                    int k, int stride, uint2* __restrict__ out,
                                                    int max_iter, unsigned long long* __restrict__ stats,
-                                                   const Node* __restrict__ lnodes = nullptr) {
+                                                   const Node* __restrict__ lnodes = nullptr,
+                                                   TailList tail = TailList{}) {
     const int i = blockIdx.x * kBlock + threadIdx.x;
     const bool active = i < count;
     Trav tv;
@@ -582,6 +611,7 @@ __global__ __launch_bounds__(kBlock) void k_knn_bin(const BNode* __restrict__ bn
         knn_bin_one<Ops, K, LocalStack<kStack>, kLeaf4>(bn, leaves, p, k, max_iter, st, tv, tab,
                                                         lnodes);
         write_knn<K>(tab, k, out + static_cast<size_t>(q) * stride);
+        if (tail.count && tv.overflow) tail_append(tail, q);
     }
     flush_stats<kStats>(active, tv.nodes, tv.leaves, tv.overflow, stats);
 }
@@ -709,7 +739,8 @@ __global__ __launch_bounds__(kBlock) void k_closest_split(const BNode* __restric
                                                          const uint32_t* __restrict__ order,
                                                          int count, uint2* __restrict__ out,
                                                          int max_iter,
-                                                         unsigned long long* __restrict__ stats) {
+                                                         unsigned long long* __restrict__ stats,
+                                                         TailList tail = TailList{}) {
     const int w = (blockIdx.x * kBlock + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (w >= count) return;  // whole warps
@@ -718,6 +749,7 @@ __global__ __launch_bounds__(kBlock) void k_closest_split(const BNode* __restric
     Trav tv;
     const uint2 r = closest_split_one<Ops>(bn, leaves, p, lane, max_iter, tv);
     if (lane == 0) out[q] = r;
+    if (tail.count && __any_sync(0xffffffffu, tv.overflow) && lane == 0) tail_append(tail, q);
     flush_stats<kStats>(true, tv.nodes, tv.leaves, tv.overflow, stats);
 }
 
@@ -728,7 +760,8 @@ __global__ __launch_bounds__(kBlock) void k_knn_split(const BNode* __restrict__ 
                                                      const uint32_t* __restrict__ order,
                                                      int count, int k, int stride,
                                                      uint2* __restrict__ out, int max_iter,
-                                                     unsigned long long* __restrict__ stats) {
+                                                     unsigned long long* __restrict__ stats,
+                                                     TailList tail = TailList{}) {
     const int w = (blockIdx.x * kBlock + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (w >= count) return;
@@ -738,7 +771,113 @@ __global__ __launch_bounds__(kBlock) void k_knn_split(const BNode* __restrict__ 
     WarpTable tab;
     knn_split_one<Ops>(bn, leaves, p, k, lane, max_iter, tv, tab);
     if (lane < k) out[static_cast<size_t>(q) * stride + lane] = warp_table_entry(tab);
+    if (tail.count && __any_sync(0xffffffffu, tv.overflow) && lane == 0) tail_append(tail, q);
     flush_stats<kStats>(true, tv.nodes, tv.leaves, tv.overflow, stats);
+}
+
+// The tail scan: block (tile, batch) runs thread t's heavy query (batch x kTailBatch + t) over
+// the tile's points and keeps the K nearest (dist2, id); the whole block reads the same point at
+// a time, so every load is one broadcast per warp.
+template <class Ops, int K>
+__global__ __launch_bounds__(kTailBatch) void k_tail_scan(const float4* __restrict__ leaves, int n,
+                                                          int ntiles, const float* __restrict__ pts,
+                                                          TailList tail) {
+    const int heavy = min(*tail.count, kTailCap);
+    const int h = blockIdx.y * kTailBatch + threadIdx.x;
+    if (h >= heavy) return;  // no barriers in this kernel
+    const int ti = blockIdx.x;
+    const int begin = static_cast<int>(static_cast<long long>(n) * ti / ntiles);
+    const int end = static_cast<int>(static_cast<long long>(n) * (ti + 1) / ntiles);
+    const int q = tail.list[h];
+    const float3 p = f3(pts[3 * q], pts[3 * q + 1], pts[3 * q + 2]);
+    KnnTable<K> tab;
+    tab.init();
+    for (int slot = begin; slot < end; ++slot) {
+        int id;
+        const float d2 = Ops::dist2(p, leaves, slot, id);
+        tab.insert(d2, id, K);
+    }
+    uint2* dst = tail.partial + static_cast<size_t>(h) * kTailCands + static_cast<size_t>(ti) * K;
+#pragma unroll
+    for (int j = 0; j < K; ++j) dst[j] = make_uint2(__float_as_uint(tab.d[j]), static_cast<unsigned>(tab.id[j]));
+}
+
+// The tail merge: one warp per heavy query; each lane keeps the K best of its share of the
+// query's candidates, then K rounds of a warp-wide (dist2, id) minimum pop the K nearest.
+template <int K>
+__global__ __launch_bounds__(kBlock) void k_tail_merge(TailList tail, int ncand, int k, int stride,
+                                                       uint2* __restrict__ out) {
+    const int h = (blockIdx.x * kBlock + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    const int heavy = min(*tail.count, kTailCap);
+    if (h >= heavy) return;  // whole warps
+    const int q = tail.list[h];
+    KnnTable<K> tab;
+    tab.init();
+    const uint2* cand = tail.partial + static_cast<size_t>(h) * kTailCands;
+    for (int c = lane; c < ncand; c += 32) {
+        const uint2 v = cand[c];
+        if (v.y != 0x7fffffffu) tab.insert(__uint_as_float(v.x), static_cast<int>(v.y), K);
+    }
+    for (int r = 0; r < k; ++r) {
+        float bd = tab.d[0];
+        int bid = tab.id[0];
+        warp_min_lex(bd, bid);
+        if (lane == 0)
+            out[static_cast<size_t>(q) * stride + r] =
+                bid != 0x7fffffff ? make_uint2(__float_as_uint(bd), static_cast<unsigned>(bid))
+                                  : make_uint2(0u, 0xffffffffu);
+        if (bid != 0x7fffffff && tab.id[0] == bid) {  // ids are unique: the owner pops its head
+#pragma unroll
+            for (int j = 0; j + 1 < K; ++j) {
+                tab.d[j] = tab.d[j + 1];
+                tab.id[j] = tab.id[j + 1];
+            }
+            tab.d[K - 1] = kInf;
+            tab.id[K - 1] = 0x7fffffff;
+        }
+    }
+}
+
+// Heavy queries past kTailCap: the ordinary traversal without a budget, one thread each.
+template <class Ops, int K>
+__global__ __launch_bounds__(kBlock) void k_tail_spill(const BNode* __restrict__ bn,
+                                                       const float4* __restrict__ leaves,
+                                                       const float* __restrict__ pts, int count,
+                                                       int k, int stride, uint2* __restrict__ out,
+                                                       int max_iter, TailList tail) {
+    const int h = kTailCap + blockIdx.x * kBlock + threadIdx.x;
+    if (h >= *tail.count || h >= count) return;
+    const int q = tail.list[h];
+    const float3 p = f3(pts[3 * q], pts[3 * q + 1], pts[3 * q + 2]);
+    Trav tv;
+    LocalStack<kStack> st;
+    if (k == 0) {
+        out[q] = closest_bin_one<Ops, LocalStack<kStack>, false>(bn, leaves, p, max_iter, st, tv);
+    } else {
+        KnnTable<K> tab;
+        knn_bin_one<Ops, K, LocalStack<kStack>, false>(bn, leaves, p, k, max_iter, st, tv, tab);
+        write_knn<K>(tab, k, out + static_cast<size_t>(q) * stride);
+    }
+}
+
+// Answers the listed heavy queries (k = 0: closest; else kNN with K >= k table entries).
+template <int K>
+int tail_resolve(const qk_tree* t, const float* pts, int count, int k, int stride, uint2* out,
+                 const TailList& tail, cudaStream_t s) {
+    const int n = t->n;
+    const int ntiles = max(1, min(kTailCands / K, n));
+    dim3 grid(ntiles, kTailCap / kTailBatch);
+    const float4* leaves = static_cast<const float4*>(t->leaves);
+    k_tail_scan<PointOps, K><<<grid, kTailBatch, 0, s>>>(leaves, n, ntiles, pts, tail);
+    k_tail_merge<K><<<blocks_for(static_cast<long long>(kTailCap) * 32), kBlock, 0, s>>>(
+        tail, ntiles * K, k == 0 ? 1 : k, k == 0 ? 1 : stride, out);
+    if (count > kTailCap)
+        k_tail_spill<PointOps, K><<<blocks_for(count - kTailCap), kBlock, 0, s>>>(
+            static_cast<const BNode*>(t->bnodes), leaves, pts, count, k, stride, out, n * 2 + 64,
+            tail);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? QK_OK : cuda_status(e, "heavy-query tail");
 }
 
 // radius, split: the count pass stores every lane's count (lane_counts[q * 32 + lane]) and
@@ -975,11 +1114,26 @@ const uint32_t* make_order(const float* pos, int stride, int offset, int count, 
 
 template <class Ops>
 int closest_impl(const qk_tree* t, const float* pts, int count, uint2* out, unsigned flags,
-                 unsigned long long* stats, const uint32_t* order, cudaStream_t s) {
+                 unsigned long long* stats, const uint32_t* order, cudaStream_t s,
+                 const TailList& tail = TailList{}) {
     const float4* leaves = static_cast<const float4*>(t->leaves);
     const int g = blocks_for(count);
     const bool wide = (flags & QK_WIDE) != 0;
     const bool st = stats != nullptr;
+    if (tail.count) {
+        // budgeted traversal (binary nodes, thread or warp per query), then the shared scan
+        const BNode* bn = static_cast<const BNode*>(t->bnodes);
+        cudaMemsetAsync(tail.count, 0, sizeof(int), s);
+        if (flags & QK_TUNE_SPLIT)
+            k_closest_split<Ops, false><<<blocks_for(static_cast<long long>(count) * 32), kBlock, 0, s>>>(
+                bn, leaves, pts, order, count, out, kTailBudgetLane, nullptr, tail);
+        else
+            k_closest_bin<Ops, false><<<g, kBlock, 0, s>>>(bn, leaves, pts, order, count, out,
+                                                           kTailBudgetThread, nullptr, nullptr, tail);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return cuda_status(e, "closest (tail)");
+        return tail_resolve<1>(t, pts, count, 0, 1, out, tail, s);
+    }
     if (wide) {
         const WideNode* wn = static_cast<const WideNode*>(t->wide);
         if (st) k_closest_wide<Ops, true><<<g, kBlock, 0, s>>>(wn, leaves, pts, order, count, out, t->n * 2 + 64, stats);
@@ -1028,12 +1182,36 @@ void launch_knn(const qk_tree* t, const float* pts, int count, int k, int stride
     }
 }
 
+template <class Ops, int K>
+int knn_tail(const qk_tree* t, const float* pts, int count, int k, int stride, uint2* out,
+             bool split, const uint32_t* order, const TailList& tail, cudaStream_t s) {
+    const BNode* bn = static_cast<const BNode*>(t->bnodes);
+    const float4* leaves = static_cast<const float4*>(t->leaves);
+    cudaMemsetAsync(tail.count, 0, sizeof(int), s);
+    if (split)
+        k_knn_split<Ops, K, false><<<blocks_for(static_cast<long long>(count) * 32), kBlock, 0, s>>>(
+            bn, leaves, pts, order, count, k, stride, out, kTailBudgetLane, nullptr, tail);
+    else
+        k_knn_bin<Ops, K, false><<<blocks_for(count), kBlock, 0, s>>>(
+            bn, leaves, pts, order, count, k, stride, out, kTailBudgetThread, nullptr, nullptr, tail);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_status(e, "knn (tail)");
+    return tail_resolve<K>(t, pts, count, k, stride, out, tail, s);
+}
+
 template <class Ops>
 int knn_impl(const qk_tree* t, const float* pts, int count, int k, int stride, uint2* out,
-             unsigned flags, unsigned long long* stats, const uint32_t* order, cudaStream_t s) {
+             unsigned flags, unsigned long long* stats, const uint32_t* order, cudaStream_t s,
+             const TailList& tail = TailList{}) {
     const bool wide = (flags & QK_WIDE) != 0;
     const bool split = (flags & QK_TUNE_SPLIT) != 0;
     const bool leaf4 = (flags & QK_TUNE_LEAF4) != 0;
+    if (tail.count) {
+        if (k <= 4) return knn_tail<Ops, 4>(t, pts, count, k, stride, out, split, order, tail, s);
+        if (k <= 8) return knn_tail<Ops, 8>(t, pts, count, k, stride, out, split, order, tail, s);
+        if (k <= 16) return knn_tail<Ops, 16>(t, pts, count, k, stride, out, split, order, tail, s);
+        return knn_tail<Ops, 32>(t, pts, count, k, stride, out, split, order, tail, s);
+    }
     if (k <= 4) launch_knn<Ops, 4>(t, pts, count, k, stride, out, wide, split, leaf4, stats, order, s);
     else if (k <= 8) launch_knn<Ops, 8>(t, pts, count, k, stride, out, wide, split, leaf4, stats, order, s);
     else if (k <= 16) launch_knn<Ops, 16>(t, pts, count, k, stride, out, wide, split, leaf4, stats, order, s);
@@ -1085,6 +1263,26 @@ int radius_dispatch(const qk_tree* t, const float* pts, int count, float r2, int
 }
 
 }  // namespace
+
+// the tail's buffers: the heavy count, the heavy list (every query) and the candidates
+TailList carve_tail(Carve& c, int count) {
+    TailList t;
+    t.count = c.take<int>(1);
+    t.list = c.take<int>(count);
+    t.partial = c.take<uint2>(static_cast<size_t>(kTailCap) * kTailCands);
+    return t;
+}
+
+bool use_tail(const qk_tree* t, unsigned flags) {
+    return (flags & QK_TUNE_TAIL) && t->kind == kPoint && !(flags & (QK_WIDE | QK_TUNE_LEAF4));
+}
+
+size_t point_query_ws_bytes(int count, unsigned flags) {
+    Carve c;
+    carve_order(c, count);
+    if (flags & QK_TUNE_TAIL) carve_tail(c, count);
+    return c.used;
+}
 
 size_t order_ws_bytes(int count) {
     Carve c;
@@ -1160,6 +1358,11 @@ int closest_query(const qk_tree* t, const float* pts, int count, void* out, unsi
     if (count <= 0) return QK_OK;
     Carve c{static_cast<char*>(ws)};
     OrderBufs o = carve_order(c, count);
+    TailList tail;
+    if (flags & QK_TUNE_TAIL) {
+        const TailList carved = carve_tail(c, count);
+        if (use_tail(t, flags)) tail = carved;
+    }
     int st = QK_OK;
     const uint32_t* order = make_order(pts, 3, 0, count, flags, o, s, &st);
     if (st != QK_OK) return st;
@@ -1167,7 +1370,7 @@ int closest_query(const qk_tree* t, const float* pts, int count, void* out, unsi
     auto* stt = reinterpret_cast<unsigned long long*>(stats);
     switch (t->kind) {
         case kTri: return closest_impl<TriOps>(t, pts, count, res, flags, stt, order, s);
-        case kPoint: return closest_impl<PointOps>(t, pts, count, res, flags, stt, order, s);
+        case kPoint: return closest_impl<PointOps>(t, pts, count, res, flags, stt, order, s, tail);
         case kGauss: return closest_impl<GaussOps>(t, pts, count, res, flags, stt, order, s);
         default: return fail(QK_ERR_INVALID, "unknown primitive kind %d", t->kind);
     }
@@ -1178,6 +1381,11 @@ int knn_query(const qk_tree* t, const float* pts, int count, int k, int stride, 
     if (count <= 0) return QK_OK;
     Carve c{static_cast<char*>(ws)};
     OrderBufs o = carve_order(c, count);
+    TailList tail;
+    if (flags & QK_TUNE_TAIL) {
+        const TailList carved = carve_tail(c, count);
+        if (use_tail(t, flags)) tail = carved;
+    }
     int st = QK_OK;
     const uint32_t* order = make_order(pts, 3, 0, count, flags, o, s, &st);
     if (st != QK_OK) return st;
@@ -1185,7 +1393,7 @@ int knn_query(const qk_tree* t, const float* pts, int count, int k, int stride, 
     auto* stt = reinterpret_cast<unsigned long long*>(stats);
     switch (t->kind) {
         case kTri: return knn_impl<TriOps>(t, pts, count, k, stride, res, flags, stt, order, s);
-        case kPoint: return knn_impl<PointOps>(t, pts, count, k, stride, res, flags, stt, order, s);
+        case kPoint: return knn_impl<PointOps>(t, pts, count, k, stride, res, flags, stt, order, s, tail);
         case kGauss: return knn_impl<GaussOps>(t, pts, count, k, stride, res, flags, stt, order, s);
         default: return fail(QK_ERR_INVALID, "unknown primitive kind %d", t->kind);
     }

@@ -24,6 +24,7 @@ QK_ORDER_MORTON, QK_ORDER_DIRECTION, QK_WIDE, QK_ORDER_COHERENT = 1, 2, 4, 8
 QK_TUNE_DYNAMIC, QK_TUNE_HIGH_OCC, QK_TUNE_SPLIT, QK_TUNE_SHORT_STACK = 256, 512, 1024, 2048
 QK_TUNE_LEAF4 = 4096
 QK_TUNE_STASH = 8192
+QK_TUNE_TAIL = 16384
 QK_SCHEDULE_BATCHED, QK_SCHEDULE_LOOP = 0, 1
 QK_OP_RAY, QK_OP_CLOSEST, QK_OP_KNN, QK_OP_RADIUS = 0, 1, 2, 3
 KINDS = {"tri": QK_TRI, "point": QK_POINT, "gauss": QK_GAUSS}
@@ -107,6 +108,11 @@ EXPORTS = {
     "qk_distance_grad": (_I, [ctypes.POINTER(QkTree), _P, _P, _P, _P, _I, _P, _P, _P, _SZ, _P]),
     "qk_ray_t_grad": (_I, [ctypes.POINTER(QkTree), _P, _P, _P, _P, _I, _P, _P, _P, _SZ, _P]),
     "qk_segment_sum": (_I, [_P, _P, _I, _I, _I, _P, _P, _SZ, _P]),
+    "qk_grad_vertices_workspace_bytes": (_SZ, [_I]),
+    "qk_ray_t_grad_vertices": (_I, [ctypes.POINTER(QkTree), _P, _P, _P, _P, _I, _P, _I, _P, _P,
+                                    _P, _SZ, _P]),
+    "qk_distance_grad_vertices": (_I, [ctypes.POINTER(QkTree), _P, _P, _P, _P, _I, _P, _I, _P,
+                                       _P, _P, _SZ, _P]),
     "qk_raycast_noalloc": (_I, [ctypes.POINTER(QkTree), _P, _I, _P, _U, _P]),
     "qk_raycast_mapped": (_I, [ctypes.POINTER(QkTree), _P, _I, _P, _U, _P, _SZ, _P]),
     "qk_raycast_host_workspace_bytes": (_SZ, [_I, _I]),
@@ -411,6 +417,37 @@ class DeviceTree:
                                   _ptr(ids), _ptr(grad_t), count, _ptr(gt), _ptr(gr), _ptr(w),
                                   w.numel(), _stream()), "qk_ray_t_grad")
         return gt, gr
+
+    def ray_t_grad_vertices(self, rays, ids, indices, nverts: int, grad_t=None,
+                            with_rays: bool = True):
+        """Adjoint of the first-hit t summed per mesh vertex in FP64: (grad_verts (nverts, 3),
+        grad_rays (count, 6) or None); indices (n, 3) int32 corner vertex ids."""
+        torch = _torch()
+        count = rays.shape[0]
+        gv = torch.empty((nverts, 3), dtype=torch.float32, device="cuda")
+        gr = torch.empty((count, 6), dtype=torch.float32, device="cuda") if with_rays else None
+        idx = indices.to(torch.int32).contiguous()
+        w = _dev_bytes(lib().qk_grad_vertices_workspace_bytes(count))
+        check(lib().qk_ray_t_grad_vertices(ctypes.byref(self.t), _ptr(self.items_scene), _ptr(rays),
+                                           _ptr(ids), _ptr(grad_t), count, _ptr(idx), nverts,
+                                           _ptr(gv), _ptr(gr), _ptr(w), w.numel(), _stream()),
+              "qk_ray_t_grad_vertices")
+        return gv, gr
+
+    def distance_grad_vertices(self, pts, results, indices, nverts: int, grad_dist=None):
+        """Adjoint of the triangle distances summed per mesh vertex in FP64:
+        (grad_points (count, 3), grad_verts (nverts, 3))."""
+        torch = _torch()
+        count = pts.shape[0]
+        gp = torch.empty((count, 3), dtype=torch.float32, device="cuda")
+        gv = torch.empty((nverts, 3), dtype=torch.float32, device="cuda")
+        idx = indices.to(torch.int32).contiguous()
+        w = _dev_bytes(lib().qk_grad_vertices_workspace_bytes(count))
+        check(lib().qk_distance_grad_vertices(ctypes.byref(self.t), _ptr(self.items_scene),
+                                              _ptr(pts), _ptr(results), _ptr(grad_dist), count,
+                                              _ptr(idx), nverts, _ptr(gp), _ptr(gv), _ptr(w),
+                                              w.numel(), _stream()), "qk_distance_grad_vertices")
+        return gp, gv
 
     def closest(self, pts, flags: int = 0, stats=None, out=None):
         torch = _torch()

@@ -8,7 +8,8 @@ Forward: the engine's bit-exact queries (closest primitive / first hit) over a t
 from the current parameters.  Backward: the engine's adjoint kernels, which recompute only
 the selected leaf test in FP64 and differentiate it (envelope theorem for distances, the
 plane-crossing derivative for t); per-primitive and per-vertex sums are deterministic
-(sorted, no float atomics).  Distances are Euclidean (not squared); d = 0 inside a solid
+(sorted, no float atomics) and stay in FP64 until one final rounding to FP32 (mesh vertices
+are summed straight from the per-query terms, not through per-triangle FP32 sums).  Distances are Euclidean (not squared); d = 0 inside a solid
 ellipsoid or on a triangle has gradient 0.  Rays that miss return t = inf and no gradient.
 """
 from __future__ import annotations
@@ -36,12 +37,6 @@ def _tree(kind, items, builder, wide):
     if wide:
         tree.build_wide()
     return tree
-
-
-def _vertex_grad(indices, grad_tris, nverts):
-    keys = indices.reshape(-1).to(torch.int32).contiguous()
-    vals = grad_tris.reshape(-1, 3).contiguous()
-    return capi.segment_sum(keys, vals, nverts)
 
 
 class _GaussianDistance(torch.autograd.Function):
@@ -79,8 +74,8 @@ class _TriangleDistance(torch.autograd.Function):
     @staticmethod
     def backward(ctx, grad_d):
         pts, res, indices = ctx.saved_tensors
-        gp, gt = ctx.tree.distance_grad(pts, res, grad_d.float().contiguous())
-        gv = _vertex_grad(indices, gt, ctx.nverts)
+        gp, gv = ctx.tree.distance_grad_vertices(pts, res, indices, ctx.nverts,
+                                                 grad_d.float().contiguous())
         return gp, gv, None, None, None, None
 
 
@@ -114,8 +109,8 @@ class _RayHitT(torch.autograd.Function):
     def backward(ctx, grad_t, grad_hit):
         rays, ids, indices = ctx.saved_tensors
         g = torch.where(ids >= 0, grad_t.float(), torch.zeros_like(grad_t, dtype=torch.float32))
-        gt, gr = ctx.tree.ray_t_grad(rays, ids, g.contiguous(), with_rays=True)
-        gv = _vertex_grad(indices, gt, ctx.nverts)
+        gv, gr = ctx.tree.ray_t_grad_vertices(rays, ids, indices, ctx.nverts, g.contiguous(),
+                                              with_rays=True)
         return gr[:, 0:3], gr[:, 3:6], gv, None, None, None, None, None
 
 

@@ -615,3 +615,36 @@ def test_radius_segment_sizes_all_sort_paths(cuda):
             assert ((sizes > 32) & (sizes <= 1024)).any()
         if r == 0.75:
             assert ((sizes > 1024) & (sizes <= 4096)).any()
+
+
+def test_point_tail_same_results(cuda):
+    """QK_TUNE_TAIL: queries near the centre of a 1M-point spherical shell (the search ball of
+    such a point admits most of the shell) pass the traversal budget and are answered by the
+    shared brute-force scan; more of them than the scan takes at once (1,024) also exercises
+    the spill path.  Every result equals the plain traversal's bits, and the oracle's."""
+    pts = workloads.point_cloud("surface", 1_048_576, 5)
+    tree = capi.DeviceTree("point", pts)
+    rng = np.random.default_rng(9)
+    centre = rng.normal(0, 2.0, (1_500, 3)).astype(np.float32)  # heavy: near the centre
+    spread = workloads.uniform_points(2_500, pts.min(0), pts.max(0), 5, 13)
+    q = np.concatenate([centre, spread]).astype(np.float32)
+    dq = _dev(q)
+    ref = oracle.LBVH("point", pts)
+    want_c = ref.closest(q[::7])
+    base_c = tree.closest(dq, 0)
+    assert np.array_equal(base_c.cpu().numpy().view(np.uint32)[::7], want_c)
+    for f in (capi.QK_TUNE_TAIL, capi.QK_TUNE_TAIL | capi.QK_TUNE_SPLIT,
+              capi.QK_TUNE_TAIL | capi.QK_TUNE_SPLIT | capi.QK_ORDER_COHERENT,
+              capi.QK_TUNE_TAIL | capi.QK_ORDER_MORTON):
+        assert cuda.equal(tree.closest(dq, f), base_c), f
+    for k in (1, 8, 32):
+        base = tree.knn(dq, k, 0)
+        if k == 8:
+            assert np.array_equal(base.cpu().numpy().view(np.uint32)[::7], ref.knn(q[::7], 8))
+        for f in (capi.QK_TUNE_TAIL, capi.QK_TUNE_TAIL | capi.QK_TUNE_SPLIT,
+                  capi.QK_TUNE_TAIL | capi.QK_ORDER_COHERENT):
+            assert cuda.equal(tree.knn(dq, k, f), base), (k, f)
+    # other kinds ignore the flag
+    g = capi.DeviceTree("gauss", workloads.gaussians(20_000, 0.05, 1.0, 2))
+    gq = _dev(workloads.uniform_points(2_000, [0, 0, 0], [100, 100, 100], 2, 31))
+    assert cuda.equal(g.closest(gq, capi.QK_TUNE_TAIL), g.closest(gq, 0))

@@ -1160,7 +1160,9 @@ def points_arm(args, world, rank, local):
     for (kind, op), (_, vname, _) in plan.items():
         morton = (24 if variants[vname] & capi.QK_ORDER_MORTON else
                   4 if variants[vname] & capi.QK_ORDER_COHERENT else 0)
-        launches += (1 + morton) if op != "radius" else (4 + morton) + (1 + morton) + 4
+        # scan + merge for each round of up to 1,024 queries past the budget (one round here)
+        tail_k = 2 if variants[vname] & capi.QK_TUNE_TAIL else 0
+        launches += (1 + morton + tail_k) if op != "radius" else (4 + morton) + (1 + morton) + 4
     line["gpu_launches"] = args.steps * launches
     return line
 

@@ -76,8 +76,10 @@ extern "C" {
 #define QK_TUNE_TAIL 16384u      /* closest / kNN on point clouds, binary nodes (thread or warp
                                     per query): a query still traversing after a step budget is
                                     answered by a brute-force scan over all points that every
-                                    such query shares, merged per query (the workspace grows by
-                                    33.5 MB + 4 bytes per query; ignored for other kinds) */
+                                    such query shares, merged per query; the call then reads the
+                                    number of such queries back (syncs) and adds it to stats[3]
+                                    (the workspace grows by 33.5 MB + 4 bytes per query; ignored
+                                    for other kinds) */
 
 /*
  * Device arrays of one tree.  The caller allocates every array (sizes from qk_tree_bytes)

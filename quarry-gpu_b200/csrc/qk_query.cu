@@ -523,6 +523,11 @@ __global__ __launch_bounds__(kBlock) void k_ray_wide(const WideNode* __restrict_
     flush_stats<kStats>(active, tv.nodes, tv.leaves, tv.overflow, stats);
 }
 
+// Threads per block of the thread-per-query point-query kernels: a few tens of thousands of
+// queries in blocks of 256 would occupy only some of the 148 SMs, and these latency-bound
+// traversals run faster spread over all of them; large batches keep 256.
+inline int query_block(int count) { return count <= 148 * 512 ? 64 : kBlock; }
+
 // ---------------------------------------------------------------------------------------
 // heavy-query tail (QK_TUNE_TAIL, point clouds).  A point near the centre of a spherical shell
 // has most of the shell at almost the same distance, so its search ball admits most of the
@@ -532,7 +537,7 @@ __global__ __launch_bounds__(kBlock) void k_ray_wide(const WideNode* __restrict_
 // shares (point tiles x heavy-query batches), merged per query.  The scan computes the same
 // dist2 as the leaf test and keeps the same (dist2, id) order, so results are bit-identical.
 // ---------------------------------------------------------------------------------------
-constexpr int kTailCap = 1024;           // heavy queries the scan answers (the rest traverse again)
+constexpr int kTailCap = 1024;           // heavy queries per scan round
 constexpr int kTailBatch = 256;          // heavy queries per scan block, one per thread
 constexpr int kTailCands = 4096;         // candidates kept per heavy query (tiles x K)
 constexpr int kTailBudgetThread = 2048;  // traversal steps of a thread-per-query query
@@ -558,7 +563,7 @@ __global__ __launch_bounds__(kBlock) void k_closest_bin(const BNode* __restrict_
                                                        int max_iter, unsigned long long* __restrict__ stats,
                                                        const Node* __restrict__ lnodes = nullptr,
                                                        TailList tail = TailList{}) {
-    const int i = blockIdx.x * kBlock + threadIdx.x;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool active = i < count;
     Trav tv;
     if (active) {
@@ -579,7 +584,7 @@ __global__ __launch_bounds__(kBlock) void k_closest_wide(const WideNode* __restr
                                                         const uint32_t* __restrict__ order,
                                                         int count, uint2* __restrict__ out,
                                                         int max_iter, unsigned long long* __restrict__ stats) {
-    const int i = blockIdx.x * kBlock + threadIdx.x;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool active = i < count;
     Trav tv;
     if (active) {
@@ -600,7 +605,7 @@ __global__ __launch_bounds__(kBlock) void k_knn_bin(const BNode* __restrict__ bn
                                                    int max_iter, unsigned long long* __restrict__ stats,
                                                    const Node* __restrict__ lnodes = nullptr,
                                                    TailList tail = TailList{}) {
-    const int i = blockIdx.x * kBlock + threadIdx.x;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool active = i < count;
     Trav tv;
     if (active) {
@@ -623,7 +628,7 @@ __global__ __launch_bounds__(kBlock) void k_knn_wide(const WideNode* __restrict_
                                                     const uint32_t* __restrict__ order, int count,
                                                     int k, int stride, uint2* __restrict__ out,
                                                     int max_iter, unsigned long long* __restrict__ stats) {
-    const int i = blockIdx.x * kBlock + threadIdx.x;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool active = i < count;
     Trav tv;
     if (active) {
@@ -645,7 +650,7 @@ __global__ __launch_bounds__(kBlock) void k_radius_bin(
     int* __restrict__ counts, const int* __restrict__ offsets,
     unsigned long long* __restrict__ keys, int max_iter, unsigned long long* __restrict__ stats,
     const Node* __restrict__ lnodes = nullptr) {
-    const int i = blockIdx.x * kBlock + threadIdx.x;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool active = i < count;
     Trav tv;
     if (active) {
@@ -672,7 +677,7 @@ __global__ __launch_bounds__(kBlock) void k_radius_count_pool(
     const float* __restrict__ pts, const uint32_t* __restrict__ order, int count, float r2,
     int* __restrict__ counts, RadiusPool pool, int max_iter,
     unsigned long long* __restrict__ stats, const Node* __restrict__ lnodes = nullptr) {
-    const int i = blockIdx.x * kBlock + threadIdx.x;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool active = i < count;
     Trav tv;
     if (active) {
@@ -695,7 +700,7 @@ __global__ __launch_bounds__(kBlock) void k_radius_fill_lost(
     const float* __restrict__ pts, int count, float r2, const int* __restrict__ offsets,
     RadiusPool pool, unsigned long long* __restrict__ keys, int max_iter,
     const Node* __restrict__ lnodes = nullptr) {
-    const int q = blockIdx.x * kBlock + threadIdx.x;
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= count) return;
     const int begin = offsets[q], end = offsets[q + 1];
     if (end - begin <= kRadiusStash || pool.first[q] != kPoolLost) return;
@@ -713,7 +718,7 @@ __global__ __launch_bounds__(kBlock) void k_radius_wide(
     int* __restrict__ counts, const int* __restrict__ offsets,
     unsigned long long* __restrict__ keys, int max_iter, unsigned long long* __restrict__ stats,
     const Node* __restrict__ lnodes = nullptr) {
-    const int i = blockIdx.x * kBlock + threadIdx.x;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool active = i < count;
     Trav tv;
     if (active) {
@@ -775,20 +780,19 @@ __global__ __launch_bounds__(kBlock) void k_knn_split(const BNode* __restrict__ 
     flush_stats<kStats>(true, tv.nodes, tv.leaves, tv.overflow, stats);
 }
 
-// The tail scan: block (tile, batch) runs thread t's heavy query (batch x kTailBatch + t) over
-// the tile's points and keeps the K nearest (dist2, id); the whole block reads the same point at
-// a time, so every load is one broadcast per warp.
+// The tail scan: block (tile, batch) runs heavy query base + batch x kTailBatch + t of the
+// current round over the tile's points and keeps the K nearest (dist2, id); the whole block
+// reads the same point at a time, so every load is one broadcast per warp.
 template <class Ops, int K>
 __global__ __launch_bounds__(kTailBatch) void k_tail_scan(const float4* __restrict__ leaves, int n,
                                                           int ntiles, const float* __restrict__ pts,
-                                                          TailList tail) {
-    const int heavy = min(*tail.count, kTailCap);
-    const int h = blockIdx.y * kTailBatch + threadIdx.x;
-    if (h >= heavy) return;  // no barriers in this kernel
+                                                          TailList tail, int base, int nround) {
+    const int hl = blockIdx.y * kTailBatch + threadIdx.x;
+    if (hl >= nround) return;  // no barriers in this kernel
     const int ti = blockIdx.x;
     const int begin = static_cast<int>(static_cast<long long>(n) * ti / ntiles);
     const int end = static_cast<int>(static_cast<long long>(n) * (ti + 1) / ntiles);
-    const int q = tail.list[h];
+    const int q = tail.list[base + hl];
     const float3 p = f3(pts[3 * q], pts[3 * q + 1], pts[3 * q + 2]);
     KnnTable<K> tab;
     tab.init();
@@ -797,24 +801,25 @@ __global__ __launch_bounds__(kTailBatch) void k_tail_scan(const float4* __restri
         const float d2 = Ops::dist2(p, leaves, slot, id);
         tab.insert(d2, id, K);
     }
-    uint2* dst = tail.partial + static_cast<size_t>(h) * kTailCands + static_cast<size_t>(ti) * K;
+    uint2* dst = tail.partial + static_cast<size_t>(hl) * kTailCands + static_cast<size_t>(ti) * K;
 #pragma unroll
     for (int j = 0; j < K; ++j) dst[j] = make_uint2(__float_as_uint(tab.d[j]), static_cast<unsigned>(tab.id[j]));
 }
 
-// The tail merge: one warp per heavy query; each lane keeps the K best of its share of the
-// query's candidates, then K rounds of a warp-wide (dist2, id) minimum pop the K nearest.
+// The tail merge: one warp per heavy query of the round; each lane keeps the K best of its
+// share of the query's candidates, then k rounds of a warp-wide (dist2, id) minimum pop the k
+// nearest.
 template <int K>
 __global__ __launch_bounds__(kBlock) void k_tail_merge(TailList tail, int ncand, int k, int stride,
-                                                       uint2* __restrict__ out) {
-    const int h = (blockIdx.x * kBlock + threadIdx.x) >> 5;
+                                                       uint2* __restrict__ out, int base,
+                                                       int nround) {
+    const int hl = (blockIdx.x * kBlock + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
-    const int heavy = min(*tail.count, kTailCap);
-    if (h >= heavy) return;  // whole warps
-    const int q = tail.list[h];
+    if (hl >= nround) return;  // whole warps
+    const int q = tail.list[base + hl];
     KnnTable<K> tab;
     tab.init();
-    const uint2* cand = tail.partial + static_cast<size_t>(h) * kTailCands;
+    const uint2* cand = tail.partial + static_cast<size_t>(hl) * kTailCands;
     for (int c = lane; c < ncand; c += 32) {
         const uint2 v = cand[c];
         if (v.y != 0x7fffffffu) tab.insert(__uint_as_float(v.x), static_cast<int>(v.y), K);
@@ -839,44 +844,30 @@ __global__ __launch_bounds__(kBlock) void k_tail_merge(TailList tail, int ncand,
     }
 }
 
-// Heavy queries past kTailCap: the ordinary traversal without a budget, one thread each.
-template <class Ops, int K>
-__global__ __launch_bounds__(kBlock) void k_tail_spill(const BNode* __restrict__ bn,
-                                                       const float4* __restrict__ leaves,
-                                                       const float* __restrict__ pts, int count,
-                                                       int k, int stride, uint2* __restrict__ out,
-                                                       int max_iter, TailList tail) {
-    const int h = kTailCap + blockIdx.x * kBlock + threadIdx.x;
-    if (h >= *tail.count || h >= count) return;
-    const int q = tail.list[h];
-    const float3 p = f3(pts[3 * q], pts[3 * q + 1], pts[3 * q + 2]);
-    Trav tv;
-    LocalStack<kStack> st;
-    if (k == 0) {
-        out[q] = closest_bin_one<Ops, LocalStack<kStack>, false>(bn, leaves, p, max_iter, st, tv);
-    } else {
-        KnnTable<K> tab;
-        knn_bin_one<Ops, K, LocalStack<kStack>, false>(bn, leaves, p, k, max_iter, st, tv, tab);
-        write_knn<K>(tab, k, out + static_cast<size_t>(q) * stride);
-    }
-}
+__global__ void k_add_u64(unsigned long long* dst, unsigned long long v) { atomicAdd(dst, v); }
 
 // Answers the listed heavy queries (k = 0: closest; else kNN with K >= k table entries).
+// Reads the heavy count back (syncs the stream) and scans in rounds of kTailCap queries.
 template <int K>
-int tail_resolve(const qk_tree* t, const float* pts, int count, int k, int stride, uint2* out,
-                 const TailList& tail, cudaStream_t s) {
+int tail_resolve(const qk_tree* t, const float* pts, int k, int stride, uint2* out,
+                 const TailList& tail, unsigned long long* stats, cudaStream_t s) {
+    int heavy = 0;
+    cudaError_t e = cudaMemcpyAsync(&heavy, tail.count, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_status(e, "heavy-query count");
+    if (stats && heavy > 0) k_add_u64<<<1, 1, 0, s>>>(stats + 3, static_cast<unsigned long long>(heavy));
     const int n = t->n;
     const int ntiles = max(1, min(kTailCands / K, n));
-    dim3 grid(ntiles, kTailCap / kTailBatch);
     const float4* leaves = static_cast<const float4*>(t->leaves);
-    k_tail_scan<PointOps, K><<<grid, kTailBatch, 0, s>>>(leaves, n, ntiles, pts, tail);
-    k_tail_merge<K><<<blocks_for(static_cast<long long>(kTailCap) * 32), kBlock, 0, s>>>(
-        tail, ntiles * K, k == 0 ? 1 : k, k == 0 ? 1 : stride, out);
-    if (count > kTailCap)
-        k_tail_spill<PointOps, K><<<blocks_for(count - kTailCap), kBlock, 0, s>>>(
-            static_cast<const BNode*>(t->bnodes), leaves, pts, count, k, stride, out, n * 2 + 64,
-            tail);
-    const cudaError_t e = cudaGetLastError();
+    for (int base = 0; base < heavy; base += kTailCap) {
+        const int nround = min(kTailCap, heavy - base);
+        dim3 grid(ntiles, (nround + kTailBatch - 1) / kTailBatch);
+        k_tail_scan<PointOps, K><<<grid, kTailBatch, 0, s>>>(leaves, n, ntiles, pts, tail, base,
+                                                             nround);
+        k_tail_merge<K><<<blocks_for(static_cast<long long>(nround) * 32), kBlock, 0, s>>>(
+            tail, ntiles * K, k == 0 ? 1 : k, k == 0 ? 1 : stride, out, base, nround);
+    }
+    e = cudaGetLastError();
     return e == cudaSuccess ? QK_OK : cuda_status(e, "heavy-query tail");
 }
 
@@ -1117,7 +1108,8 @@ int closest_impl(const qk_tree* t, const float* pts, int count, uint2* out, unsi
                  unsigned long long* stats, const uint32_t* order, cudaStream_t s,
                  const TailList& tail = TailList{}) {
     const float4* leaves = static_cast<const float4*>(t->leaves);
-    const int g = blocks_for(count);
+    const int qb = query_block(count);
+    const int g = blocks_for(count, qb);
     const bool wide = (flags & QK_WIDE) != 0;
     const bool st = stats != nullptr;
     if (tail.count) {
@@ -1128,16 +1120,16 @@ int closest_impl(const qk_tree* t, const float* pts, int count, uint2* out, unsi
             k_closest_split<Ops, false><<<blocks_for(static_cast<long long>(count) * 32), kBlock, 0, s>>>(
                 bn, leaves, pts, order, count, out, kTailBudgetLane, nullptr, tail);
         else
-            k_closest_bin<Ops, false><<<g, kBlock, 0, s>>>(bn, leaves, pts, order, count, out,
+            k_closest_bin<Ops, false><<<g, qb, 0, s>>>(bn, leaves, pts, order, count, out,
                                                            kTailBudgetThread, nullptr, nullptr, tail);
         const cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return cuda_status(e, "closest (tail)");
-        return tail_resolve<1>(t, pts, count, 0, 1, out, tail, s);
+        return tail_resolve<1>(t, pts, 0, 1, out, tail, stats, s);
     }
     if (wide) {
         const WideNode* wn = static_cast<const WideNode*>(t->wide);
-        if (st) k_closest_wide<Ops, true><<<g, kBlock, 0, s>>>(wn, leaves, pts, order, count, out, t->n * 2 + 64, stats);
-        else k_closest_wide<Ops, false><<<g, kBlock, 0, s>>>(wn, leaves, pts, order, count, out, t->n * 2 + 64, stats);
+        if (st) k_closest_wide<Ops, true><<<g, qb, 0, s>>>(wn, leaves, pts, order, count, out, t->n * 2 + 64, stats);
+        else k_closest_wide<Ops, false><<<g, qb, 0, s>>>(wn, leaves, pts, order, count, out, t->n * 2 + 64, stats);
     } else if (flags & QK_TUNE_SPLIT) {
         const BNode* bn = static_cast<const BNode*>(t->bnodes);
         const int gs = blocks_for(static_cast<long long>(count) * 32);
@@ -1145,12 +1137,12 @@ int closest_impl(const qk_tree* t, const float* pts, int count, uint2* out, unsi
         else k_closest_split<Ops, false><<<gs, kBlock, 0, s>>>(bn, leaves, pts, order, count, out, t->n * 2 + 64, stats);
     } else if (flags & QK_TUNE_LEAF4) {
         const BNode* bn = static_cast<const BNode*>(t->bnodes);
-        if (st) k_closest_bin<Ops, true, true><<<g, kBlock, 0, s>>>(bn, leaves, pts, order, count, out, t->n * 2 + 64, stats, leaf_nodes(t));
-        else k_closest_bin<Ops, false, true><<<g, kBlock, 0, s>>>(bn, leaves, pts, order, count, out, t->n * 2 + 64, stats, leaf_nodes(t));
+        if (st) k_closest_bin<Ops, true, true><<<g, qb, 0, s>>>(bn, leaves, pts, order, count, out, t->n * 2 + 64, stats, leaf_nodes(t));
+        else k_closest_bin<Ops, false, true><<<g, qb, 0, s>>>(bn, leaves, pts, order, count, out, t->n * 2 + 64, stats, leaf_nodes(t));
     } else {
         const BNode* bn = static_cast<const BNode*>(t->bnodes);
-        if (st) k_closest_bin<Ops, true><<<g, kBlock, 0, s>>>(bn, leaves, pts, order, count, out, t->n * 2 + 64, stats);
-        else k_closest_bin<Ops, false><<<g, kBlock, 0, s>>>(bn, leaves, pts, order, count, out, t->n * 2 + 64, stats);
+        if (st) k_closest_bin<Ops, true><<<g, qb, 0, s>>>(bn, leaves, pts, order, count, out, t->n * 2 + 64, stats);
+        else k_closest_bin<Ops, false><<<g, qb, 0, s>>>(bn, leaves, pts, order, count, out, t->n * 2 + 64, stats);
     }
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? QK_OK : cuda_status(e, "closest");
@@ -1161,7 +1153,8 @@ void launch_knn(const qk_tree* t, const float* pts, int count, int k, int stride
                 bool wide, bool split, bool leaf4, unsigned long long* stats,
                 const uint32_t* order, cudaStream_t s) {
     const float4* leaves = static_cast<const float4*>(t->leaves);
-    const int g = blocks_for(count);
+    const int qb = query_block(count);
+    const int g = blocks_for(count, qb);
     if (split && !wide) {
         const BNode* bn = static_cast<const BNode*>(t->bnodes);
         const int gs = blocks_for(static_cast<long long>(count) * 32);
@@ -1169,22 +1162,23 @@ void launch_knn(const qk_tree* t, const float* pts, int count, int k, int stride
         else k_knn_split<Ops, K, false><<<gs, kBlock, 0, s>>>(bn, leaves, pts, order, count, k, stride, out, t->n * 2 + 64, stats);
     } else if (wide) {
         const WideNode* wn = static_cast<const WideNode*>(t->wide);
-        if (stats) k_knn_wide<Ops, K, true><<<g, kBlock, 0, s>>>(wn, leaves, pts, order, count, k, stride, out, t->n * 2 + 64, stats);
-        else k_knn_wide<Ops, K, false><<<g, kBlock, 0, s>>>(wn, leaves, pts, order, count, k, stride, out, t->n * 2 + 64, stats);
+        if (stats) k_knn_wide<Ops, K, true><<<g, qb, 0, s>>>(wn, leaves, pts, order, count, k, stride, out, t->n * 2 + 64, stats);
+        else k_knn_wide<Ops, K, false><<<g, qb, 0, s>>>(wn, leaves, pts, order, count, k, stride, out, t->n * 2 + 64, stats);
     } else if (leaf4) {
         const BNode* bn = static_cast<const BNode*>(t->bnodes);
-        if (stats) k_knn_bin<Ops, K, true, true><<<g, kBlock, 0, s>>>(bn, leaves, pts, order, count, k, stride, out, t->n * 2 + 64, stats, leaf_nodes(t));
-        else k_knn_bin<Ops, K, false, true><<<g, kBlock, 0, s>>>(bn, leaves, pts, order, count, k, stride, out, t->n * 2 + 64, stats, leaf_nodes(t));
+        if (stats) k_knn_bin<Ops, K, true, true><<<g, qb, 0, s>>>(bn, leaves, pts, order, count, k, stride, out, t->n * 2 + 64, stats, leaf_nodes(t));
+        else k_knn_bin<Ops, K, false, true><<<g, qb, 0, s>>>(bn, leaves, pts, order, count, k, stride, out, t->n * 2 + 64, stats, leaf_nodes(t));
     } else {
         const BNode* bn = static_cast<const BNode*>(t->bnodes);
-        if (stats) k_knn_bin<Ops, K, true><<<g, kBlock, 0, s>>>(bn, leaves, pts, order, count, k, stride, out, t->n * 2 + 64, stats);
-        else k_knn_bin<Ops, K, false><<<g, kBlock, 0, s>>>(bn, leaves, pts, order, count, k, stride, out, t->n * 2 + 64, stats);
+        if (stats) k_knn_bin<Ops, K, true><<<g, qb, 0, s>>>(bn, leaves, pts, order, count, k, stride, out, t->n * 2 + 64, stats);
+        else k_knn_bin<Ops, K, false><<<g, qb, 0, s>>>(bn, leaves, pts, order, count, k, stride, out, t->n * 2 + 64, stats);
     }
 }
 
 template <class Ops, int K>
 int knn_tail(const qk_tree* t, const float* pts, int count, int k, int stride, uint2* out,
-             bool split, const uint32_t* order, const TailList& tail, cudaStream_t s) {
+             bool split, const uint32_t* order, const TailList& tail,
+             unsigned long long* stats, cudaStream_t s) {
     const BNode* bn = static_cast<const BNode*>(t->bnodes);
     const float4* leaves = static_cast<const float4*>(t->leaves);
     cudaMemsetAsync(tail.count, 0, sizeof(int), s);
@@ -1192,11 +1186,11 @@ int knn_tail(const qk_tree* t, const float* pts, int count, int k, int stride, u
         k_knn_split<Ops, K, false><<<blocks_for(static_cast<long long>(count) * 32), kBlock, 0, s>>>(
             bn, leaves, pts, order, count, k, stride, out, kTailBudgetLane, nullptr, tail);
     else
-        k_knn_bin<Ops, K, false><<<blocks_for(count), kBlock, 0, s>>>(
+        k_knn_bin<Ops, K, false><<<blocks_for(count, query_block(count)), query_block(count), 0, s>>>(
             bn, leaves, pts, order, count, k, stride, out, kTailBudgetThread, nullptr, nullptr, tail);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_status(e, "knn (tail)");
-    return tail_resolve<K>(t, pts, count, k, stride, out, tail, s);
+    return tail_resolve<K>(t, pts, k, stride, out, tail, stats, s);
 }
 
 template <class Ops>
@@ -1207,10 +1201,10 @@ int knn_impl(const qk_tree* t, const float* pts, int count, int k, int stride, u
     const bool split = (flags & QK_TUNE_SPLIT) != 0;
     const bool leaf4 = (flags & QK_TUNE_LEAF4) != 0;
     if (tail.count) {
-        if (k <= 4) return knn_tail<Ops, 4>(t, pts, count, k, stride, out, split, order, tail, s);
-        if (k <= 8) return knn_tail<Ops, 8>(t, pts, count, k, stride, out, split, order, tail, s);
-        if (k <= 16) return knn_tail<Ops, 16>(t, pts, count, k, stride, out, split, order, tail, s);
-        return knn_tail<Ops, 32>(t, pts, count, k, stride, out, split, order, tail, s);
+        if (k <= 4) return knn_tail<Ops, 4>(t, pts, count, k, stride, out, split, order, tail, stats, s);
+        if (k <= 8) return knn_tail<Ops, 8>(t, pts, count, k, stride, out, split, order, tail, stats, s);
+        if (k <= 16) return knn_tail<Ops, 16>(t, pts, count, k, stride, out, split, order, tail, stats, s);
+        return knn_tail<Ops, 32>(t, pts, count, k, stride, out, split, order, tail, stats, s);
     }
     if (k <= 4) launch_knn<Ops, 4>(t, pts, count, k, stride, out, wide, split, leaf4, stats, order, s);
     else if (k <= 8) launch_knn<Ops, 8>(t, pts, count, k, stride, out, wide, split, leaf4, stats, order, s);
@@ -1225,7 +1219,8 @@ int radius_launch(const qk_tree* t, const float* pts, int count, float r2, int* 
                   int* lane_counts, const int* offsets, unsigned long long* keys, unsigned flags,
                   unsigned long long* stats, const uint32_t* order, cudaStream_t s) {
     const float4* leaves = static_cast<const float4*>(t->leaves);
-    const int g = blocks_for(count);
+    const int qb = query_block(count);
+    const int g = blocks_for(count, qb);
     if ((flags & QK_TUNE_SPLIT) && !(flags & QK_WIDE)) {
         const BNode* bn = static_cast<const BNode*>(t->bnodes);
         const int gs = blocks_for(static_cast<long long>(count) * 32);
@@ -1233,18 +1228,18 @@ int radius_launch(const qk_tree* t, const float* pts, int count, float r2, int* 
         else k_radius_split<Ops, kFill, false><<<gs, kBlock, 0, s>>>(bn, leaves, pts, order, count, r2, counts, lane_counts, offsets, keys, t->n * 2 + 64, stats);
     } else if (flags & QK_WIDE) {
         const WideNode* wn = static_cast<const WideNode*>(t->wide);
-        if (stats) k_radius_wide<Ops, kFill, true><<<g, kBlock, 0, s>>>(wn, leaves, pts, order, count, r2, counts, offsets, keys, t->n * 2 + 64, stats);
-        else k_radius_wide<Ops, kFill, false><<<g, kBlock, 0, s>>>(wn, leaves, pts, order, count, r2, counts, offsets, keys, t->n * 2 + 64, stats);
+        if (stats) k_radius_wide<Ops, kFill, true><<<g, qb, 0, s>>>(wn, leaves, pts, order, count, r2, counts, offsets, keys, t->n * 2 + 64, stats);
+        else k_radius_wide<Ops, kFill, false><<<g, qb, 0, s>>>(wn, leaves, pts, order, count, r2, counts, offsets, keys, t->n * 2 + 64, stats);
     } else if (flags & QK_TUNE_LEAF4) {
         const BNode* bn = static_cast<const BNode*>(t->bnodes);
         const Node* nodes = static_cast<const Node*>(t->nodes);
-        if (stats) k_radius_bin<Ops, kFill, true, true><<<g, kBlock, 0, s>>>(bn, leaves, nodes, pts, order, count, r2, counts, offsets, keys, t->n * 2 + 64, stats, leaf_nodes(t));
-        else k_radius_bin<Ops, kFill, false, true><<<g, kBlock, 0, s>>>(bn, leaves, nodes, pts, order, count, r2, counts, offsets, keys, t->n * 2 + 64, stats, leaf_nodes(t));
+        if (stats) k_radius_bin<Ops, kFill, true, true><<<g, qb, 0, s>>>(bn, leaves, nodes, pts, order, count, r2, counts, offsets, keys, t->n * 2 + 64, stats, leaf_nodes(t));
+        else k_radius_bin<Ops, kFill, false, true><<<g, qb, 0, s>>>(bn, leaves, nodes, pts, order, count, r2, counts, offsets, keys, t->n * 2 + 64, stats, leaf_nodes(t));
     } else {
         const BNode* bn = static_cast<const BNode*>(t->bnodes);
         const Node* nodes = static_cast<const Node*>(t->nodes);
-        if (stats) k_radius_bin<Ops, kFill, true><<<g, kBlock, 0, s>>>(bn, leaves, nodes, pts, order, count, r2, counts, offsets, keys, t->n * 2 + 64, stats);
-        else k_radius_bin<Ops, kFill, false><<<g, kBlock, 0, s>>>(bn, leaves, nodes, pts, order, count, r2, counts, offsets, keys, t->n * 2 + 64, stats);
+        if (stats) k_radius_bin<Ops, kFill, true><<<g, qb, 0, s>>>(bn, leaves, nodes, pts, order, count, r2, counts, offsets, keys, t->n * 2 + 64, stats);
+        else k_radius_bin<Ops, kFill, false><<<g, qb, 0, s>>>(bn, leaves, nodes, pts, order, count, r2, counts, offsets, keys, t->n * 2 + 64, stats);
     }
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? QK_OK : cuda_status(e, "radius traversal");
@@ -1424,22 +1419,23 @@ int radius_pool_launch(const qk_tree* t, const float* pts, int count, float r2, 
     const BNode* bn = static_cast<const BNode*>(t->bnodes);
     const Node* nodes = static_cast<const Node*>(t->nodes);
     const float4* leaves = static_cast<const float4*>(t->leaves);
-    const int g = blocks_for(count);
+    const int qb = query_block(count);
+    const int g = blocks_for(count, qb);
     const int it = t->n * 2 + 64;
     const bool leaf4 = (flags & QK_TUNE_LEAF4) != 0;
     if (fill) {
         k_radius_gather<<<blocks_for(static_cast<long long>(count) * 32), kBlock, 0, s>>>(
             pool, offsets, count, keys, -1);
-        if (leaf4) k_radius_fill_lost<Ops, true><<<g, kBlock, 0, s>>>(bn, leaves, nodes, pts, count, r2, offsets, pool, keys, it, leaf_nodes(t));
-        else k_radius_fill_lost<Ops><<<g, kBlock, 0, s>>>(bn, leaves, nodes, pts, count, r2, offsets, pool, keys, it);
+        if (leaf4) k_radius_fill_lost<Ops, true><<<g, qb, 0, s>>>(bn, leaves, nodes, pts, count, r2, offsets, pool, keys, it, leaf_nodes(t));
+        else k_radius_fill_lost<Ops><<<g, qb, 0, s>>>(bn, leaves, nodes, pts, count, r2, offsets, pool, keys, it);
     } else {
         cudaMemsetAsync(pool.taken, 0, sizeof(int), s);
         if (leaf4) {
-            if (stats) k_radius_count_pool<Ops, true, true><<<g, kBlock, 0, s>>>(bn, leaves, nodes, pts, order, count, r2, counts, pool, it, stats, leaf_nodes(t));
-            else k_radius_count_pool<Ops, false, true><<<g, kBlock, 0, s>>>(bn, leaves, nodes, pts, order, count, r2, counts, pool, it, stats, leaf_nodes(t));
+            if (stats) k_radius_count_pool<Ops, true, true><<<g, qb, 0, s>>>(bn, leaves, nodes, pts, order, count, r2, counts, pool, it, stats, leaf_nodes(t));
+            else k_radius_count_pool<Ops, false, true><<<g, qb, 0, s>>>(bn, leaves, nodes, pts, order, count, r2, counts, pool, it, stats, leaf_nodes(t));
         } else {
-            if (stats) k_radius_count_pool<Ops, true><<<g, kBlock, 0, s>>>(bn, leaves, nodes, pts, order, count, r2, counts, pool, it, stats);
-            else k_radius_count_pool<Ops, false><<<g, kBlock, 0, s>>>(bn, leaves, nodes, pts, order, count, r2, counts, pool, it, stats);
+            if (stats) k_radius_count_pool<Ops, true><<<g, qb, 0, s>>>(bn, leaves, nodes, pts, order, count, r2, counts, pool, it, stats);
+            else k_radius_count_pool<Ops, false><<<g, qb, 0, s>>>(bn, leaves, nodes, pts, order, count, r2, counts, pool, it, stats);
         }
     }
     const cudaError_t e = cudaGetLastError();

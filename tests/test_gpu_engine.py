@@ -620,8 +620,8 @@ def test_radius_segment_sizes_all_sort_paths(cuda):
 def test_point_tail_same_results(cuda):
     """QK_TUNE_TAIL: queries near the centre of a 1M-point spherical shell (the search ball of
     such a point admits most of the shell) pass the traversal budget and are answered by the
-    shared brute-force scan; more of them than the scan takes at once (1,024) also exercises
-    the spill path.  Every result equals the plain traversal's bits, and the oracle's."""
+    shared brute-force scan, in rounds of 1,024 (1,500 of them make two rounds).  Every result
+    equals the plain traversal's bits, and the oracle's; stats[3] counts the scanned queries."""
     pts = workloads.point_cloud("surface", 1_048_576, 5)
     tree = capi.DeviceTree("point", pts)
     rng = np.random.default_rng(9)
@@ -636,7 +636,11 @@ def test_point_tail_same_results(cuda):
     for f in (capi.QK_TUNE_TAIL, capi.QK_TUNE_TAIL | capi.QK_TUNE_SPLIT,
               capi.QK_TUNE_TAIL | capi.QK_TUNE_SPLIT | capi.QK_ORDER_COHERENT,
               capi.QK_TUNE_TAIL | capi.QK_ORDER_MORTON):
-        assert cuda.equal(tree.closest(dq, f), base_c), f
+        stats = cuda.zeros(4, dtype=cuda.int64, device="cuda")
+        assert cuda.equal(tree.closest(dq, f, stats=stats), base_c), f
+        heavy = int(stats[3].item())
+        assert heavy >= 1_000, (f, heavy)  # the centre queries went to the scan
+        print(f"flags {f}: {heavy} queries scanned")
     for k in (1, 8, 32):
         base = tree.knn(dq, k, 0)
         if k == 8:

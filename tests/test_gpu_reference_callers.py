@@ -145,7 +145,7 @@ def test_reference_example():
 
 def test_reference_python_binding_test():
     """quarry's python/test_quarry.py, unchanged, importing this engine's `quarry` module."""
-    pyc = BIN / "test_quarry.pyc"
+    pyc = BIN / "test_quarry.qbc"
     if not pyc.exists():
         pytest.skip(f"{pyc} not built")
     env = dict(os.environ)

@@ -365,7 +365,8 @@ def rays_arm(args, world, rank, local, workload):
         Path(args.dump).mkdir(parents=True, exist_ok=True)
         dumps.write_qryd(Path(args.dump) / f"{workload}.qryd", cfg.tris, cfg.queries)
 
-    # ---- builds (timed beside the step): LBVH and binned SAH with 32 bins ----
+    # ---- builds (timed beside the step): LBVH, binned SAH with 32 bins, and the leaf-size-4
+    # SAH (whose 4-wide nodes are the leaf-size-4 form) ----
     tris_d = capi.to_device(cfg.tris, np.float32)
 
     def timed_build(builder):
@@ -380,11 +381,11 @@ def rays_arm(args, world, rank, local, workload):
             e1.record()
             torch.cuda.synchronize()
             times.append(e0.elapsed_time(e1))
-        tr.build_wide()
+        tr.build_wide(leaf4=builder == "sah4")
         return tr, float(np.median(times))
 
     trees, build_ms = {}, {}
-    for b in ("lbvh", "sah"):
+    for b in ("lbvh", "sah", "sah4"):
         trees[b], build_ms[b] = timed_build(b)
 
     rays_d = capi.to_device(cfg.rays, np.float32)

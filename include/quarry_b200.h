@@ -47,6 +47,12 @@ extern "C" {
 #define QK_GAUSS 2
 #define QK_BUILD_LBVH 0
 #define QK_BUILD_SAH 1
+#define QK_BUILD_SAH4 2  /* leaf-size-4 binned SAH (the lever quarry names in docs/design.md:203,
+                            207; no quarry counterpart): splits stop at ranges of at most 4
+                            primitives, which are split by count (left half first) down to single
+                            primitives, so the arrays keep the one-primitive-per-leaf format and
+                            every entry point takes the tree; QK_TUNE_LEAF4 and
+                            qk_wide_build_leaf4 then treat each such range as one leaf */
 
 /* ---- query flags ---- */
 #define QK_ORDER_MORTON 1u       /* QueryOrder::Morton / RayOrder::Morton (origin keys) */
@@ -111,6 +117,11 @@ typedef struct qk_tree {
     int32_t* flags;
     void* wide;
     int32_t* wide_id;
+    int32_t wide_leaf;   /* form of the 4-wide nodes, set by the wide builds: 1 from
+                            qk_wide_build (every slot's pad is 0, as quarry writes it), 4 from
+                            qk_wide_build_leaf4 (a leaf slot's pad holds its primitive count);
+                            0 before either */
+    int32_t reserved;
 } qk_tree;
 
 /* Byte sizes of the arrays of a tree with n primitives (same order as qk_tree). */
@@ -207,6 +218,16 @@ int qk_update_topology(const qk_tree* old_tree, qk_tree* new_tree, const qk_topo
  * tree->wide_count.  With tree->wide == NULL the call only computes wide_id and the count, so
  * the caller can allocate wide_count * 128 bytes and call again to emit the nodes. */
 int qk_wide_build(qk_tree* tree, void* workspace, size_t workspace_bytes, void* stream);
+
+/* 4-wide nodes with leaf-size-4 slots (no quarry counterpart; the 4-wide half of the lever in
+ * quarry's docs/design.md:203, 207): as qk_wide_build, but a child or grandchild subtree of 2..4
+ * primitives on contiguous leaf slots (every such range of a QK_BUILD_SAH4 tree) takes one slot
+ * as a leaf range -- child = -(first slot + 1), pad = its primitive count; single leaves have
+ * pad = 1 -- so fewer wide nodes cover the tree and no node level below a range is fetched.
+ * Same two-call pattern; sets tree->wide_leaf = 4.  Every QK_WIDE traversal of the tree reads
+ * the form tree->wide_leaf records, with the same results as any other layout; refits re-emit
+ * the form. */
+int qk_wide_build_leaf4(qk_tree* tree, void* workspace, size_t workspace_bytes, void* stream);
 
 /*
  * First-hit rays (raycastGPU, src/gpu/gpu_bvh.h:233-234).  rays: count rays (device);

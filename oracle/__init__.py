@@ -75,6 +75,7 @@ def lib():
         _sig(L, "qo_prim_bounds", None, [_I, _P, _P])
         _sig(L, "qo_lbvh_build", _I, [_I, _P, _I, _P, _P, _P, _P, _P])
         _sig(L, "qo_wide_collapse", _I, [_P, _P, _I, _P, _P])
+        _sig(L, "qo_wide_collapse_leaf4", _I, [_P, _P, _I, _P, _P])
         _sig(L, "qo_refit", None, [_I, _P, _P, _I])
         _sig(L, "qo_raycast", None, [_P, _P, _P, _I, _P, _I, _P, _I])
         _sig(L, "qo_closest", None, [_I, _P, _P, _P, _I, _P, _I, _P, _I])
@@ -204,6 +205,9 @@ class LBVH:
                                        _ptr(wide))
         return wide[: 4 * count].copy(), wide_id
 
+    def wide_leaf4(self):
+        return wide_collapse_leaf4(self.nodes, self.depth_arr, self.n)
+
     def refit(self, items: np.ndarray) -> None:
         """Topology-frozen refit with scene-ordered items (same count)."""
         items = _f32(items).reshape(-1, STRIDE[self.kind])
@@ -243,6 +247,19 @@ class LBVH:
         lib().qo_radius(self.kind, _ptr(self.nodes), _ptr(self.sorted), _ptr(self.prim_ids),
                         self.n, _ptr(q), nq, r, _ptr(counts), _ptr(offsets), _ptr(keys), threads)
         return offsets, keys
+
+
+def wide_collapse_leaf4(nodes: np.ndarray, depth: np.ndarray, n: int):
+    """Leaf-size-4 4-wide collapse (qo_wide_collapse_leaf4) of any tree in the canonical node
+    format (2n-1 NODE_DTYPE entries, root 0) with its node depths: (wide nodes, wide_id)."""
+    nodes = np.ascontiguousarray(nodes, dtype=NODE_DTYPE)
+    depth = np.ascontiguousarray(depth, dtype=np.int32)
+    wide_id = np.zeros(n - 1, dtype=np.int32)
+    wide = np.zeros((n - 1) * 4, dtype=WIDE_DTYPE)
+    count = lib().qo_wide_collapse_leaf4(_ptr(nodes), _ptr(depth), n, _ptr(wide_id), _ptr(wide))
+    if count < 0:
+        raise MemoryError("qo_wide_collapse_leaf4")
+    return wide[: 4 * count].copy(), wide_id
 
 
 def raycast_brute(tris, rays) -> np.ndarray:

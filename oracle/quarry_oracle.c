@@ -504,6 +504,94 @@ int qo_wide_collapse(const qo_node* nodes, const int32_t* depth, int n, int32_t*
     return count;
 }
 
+/* 4-wide collapse, leaf-size-4 form (the engine's qk_wide_build_leaf4; quarry has no
+ * counterpart: it names leaf-size-4 SAH trees with 4-wide nodes as its next build lever,
+ * docs/design.md:203,207).  A child or grandchild whose subtree holds 2..4 leaves on
+ * contiguous slots is one slot: child = -(first slot + 1), pad = leaves; single leaves have
+ * pad = 1; internal slots pad = 0.  Wide nodes: even-depth internal nodes that are the root or
+ * not such a subtree themselves.  Slot ranges are derived bottom-up from the links: a node's
+ * range is contiguous when both children's are and they abut. */
+int qo_wide_collapse_leaf4(const qo_node* nodes, const int32_t* depth, int n, int32_t* wide_id,
+                           qo_wide_entry* wide) {
+    const int m = n - 1;
+    int32_t* first = (int32_t*)malloc(sizeof(int32_t) * (size_t)m);
+    int32_t* cnt = (int32_t*)malloc(sizeof(int32_t) * (size_t)m);
+    int32_t* stack = (int32_t*)malloc(sizeof(int32_t) * (size_t)(2 * n));
+    uint8_t* seen = (uint8_t*)calloc((size_t)m, 1);
+    if (!first || !cnt || !stack || !seen) {
+        free(first); free(cnt); free(stack); free(seen);
+        return -1;
+    }
+    /* post-order over internal nodes from the root (node 0) */
+    int sp = 0;
+    stack[sp++] = 0;
+    while (sp > 0) {
+        const int i = stack[sp - 1];
+        const int kids[2] = {nodes[i].left, nodes[i].right};
+        if (!seen[i]) {
+            seen[i] = 1;
+            for (int k = 0; k < 2; ++k)
+                if (kids[k] < m) stack[sp++] = kids[k];
+            continue;
+        }
+        --sp;
+        int f[2], c[2];
+        for (int k = 0; k < 2; ++k) {
+            if (kids[k] >= m) {
+                f[k] = kids[k] - m;
+                c[k] = 1;
+            } else {
+                f[k] = first[kids[k]];
+                c[k] = cnt[kids[k]];
+            }
+        }
+        const int lo = f[0] < f[1] ? f[0] : f[1];
+        const int e0 = f[0] + c[0], e1 = f[1] + c[1];
+        const int hi = e0 > e1 ? e0 : e1;
+        first[i] = lo;
+        cnt[i] = (c[0] > 0 && c[1] > 0 && hi - lo == c[0] + c[1]) ? c[0] + c[1] : 0;
+    }
+    /* code of internal node c: (first << 2) | (leaves - 1) for 2..4 contiguous leaves */
+#define SMALL_CODE(c) ((cnt[c] >= 2 && cnt[c] <= 4) ? ((first[c] << 2) | (cnt[c] - 1)) : 0)
+    int count = 0;
+    for (int i = 0; i < m; ++i) {
+        wide_id[i] = count;
+        if ((depth[i] & 1) == 0 && (i == 0 || SMALL_CODE(i) == 0)) ++count;
+    }
+    for (int i = 0; i < m; ++i) {
+        if ((depth[i] & 1) || (i != 0 && SMALL_CODE(i) != 0)) continue;
+        qo_wide_entry* out = wide + 4 * (size_t)wide_id[i];
+        for (int s = 0; s < 4; ++s) {
+            out[s].mn[0] = out[s].mn[1] = out[s].mn[2] = INFINITY;
+            out[s].mx[0] = out[s].mx[1] = out[s].mx[2] = -INFINITY;
+            out[s].child = INT32_MIN;
+            out[s].pad = 0;
+        }
+        int slot = 0;
+        const int kids[2] = {nodes[i].left, nodes[i].right};
+        for (int k = 0; k < 2; ++k) {
+            const int c = kids[k];
+            const int reps = (c >= m || SMALL_CODE(c) != 0) ? 1 : 2;
+            for (int j = 0; j < reps; ++j) {
+                const int x = reps == 1 ? c : (j == 0 ? nodes[c].left : nodes[c].right);
+                qo_wide_entry* e = &out[slot++];
+                if (x >= m) {
+                    wide_fill(e, &nodes[x], nodes[x].left);
+                    e->pad = 1;
+                } else if (SMALL_CODE(x) != 0) {
+                    wide_fill(e, &nodes[x], -(first[x] + 1));
+                    e->pad = cnt[x];
+                } else {
+                    wide_fill(e, &nodes[x], wide_id[x]);
+                }
+            }
+        }
+    }
+#undef SMALL_CODE
+    free(first); free(cnt); free(stack); free(seen);
+    return count;
+}
+
 /* ------------------------------------------------------------------------- */
 /* a tiny parallel-for over query ranges                                       */
 /* ------------------------------------------------------------------------- */

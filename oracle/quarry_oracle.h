@@ -75,6 +75,11 @@ int qo_lbvh_build(int kind, const float* items, int n, qo_node* nodes, float* so
 int qo_wide_collapse(const qo_node* nodes, const int32_t* depth, int n, int32_t* wide_id,
                      qo_wide_entry* wide);
 
+/* 4-wide collapse in the leaf-size-4 form (leaf ranges of 2..4 contiguous slots take one
+ * slot, pad = primitive count); same buffers; -1 when out of host memory. */
+int qo_wide_collapse_leaf4(const qo_node* nodes, const int32_t* depth, int n, int32_t* wide_id,
+                           qo_wide_entry* wide);
+
 /* in-place refit: recompute leaf boxes from sorted items and every internal box */
 void qo_refit(int kind, qo_node* nodes, const float* sorted, int n);
 

@@ -780,7 +780,7 @@ int batch_build_loop(qk_batch* b, int builder, int bins, cudaStream_t s) {
         int st = build_tree(&t, builder, bins, in, b->single_ws, b->single_ws_bytes, s);
         if (st != QK_OK) return st;
         if (b->flags & QK_WIDE) {
-            st = wide_build(&t, b->single_ws, b->single_ws_bytes, s);
+            st = wide_build(&t, 1, b->single_ws, b->single_ws_bytes, s);
             if (st != QK_OK) return st;
         }
     }

@@ -313,6 +313,29 @@ __global__ __launch_bounds__(kBlock) void k_wide_emit(const Node* __restrict__ n
     wide[wide_id[i]] = out;
 }
 
+// ---- 4-wide collapse, leaf-size-4 form (wide4_node_of) ----
+__global__ __launch_bounds__(kBlock) void k_wide4_flags(const Node* __restrict__ nodes,
+                                                       const BNode* __restrict__ bn,
+                                                       const int* __restrict__ parent,
+                                                       const int* __restrict__ depth, int m,
+                                                       int* __restrict__ flags) {
+    const int i = blockIdx.x * kBlock + threadIdx.x;
+    if (i < m) flags[i] = ((depth[i] & 1) == 0 && own_small_code(nodes, bn, parent, i) == 0) ? 1 : 0;
+}
+
+__global__ __launch_bounds__(kBlock) void k_wide4_emit(const Node* __restrict__ nodes,
+                                                      const BNode* __restrict__ bn,
+                                                      const int* __restrict__ parent, int n,
+                                                      const int* __restrict__ depth,
+                                                      const int* __restrict__ wide_id,
+                                                      WideNode* __restrict__ wide) {
+    const int i = blockIdx.x * kBlock + threadIdx.x;
+    if (i >= n - 1 || (depth[i] & 1) != 0 || own_small_code(nodes, bn, parent, i) != 0) return;
+    WideNode out;
+    wide4_node_of(nodes, bn, n, wide_id, i, out);
+    wide[wide_id[i]] = out;
+}
+
 // ---- validation (lbvh.cu:613-729) ----
 __device__ __forceinline__ bool same_box(const Node& a, Box b) {
     return a.mn[0] == b.lo.x && a.mn[1] == b.lo.y && a.mn[2] == b.lo.z && a.mx[0] == b.hi.x &&
@@ -422,15 +445,21 @@ __global__ __launch_bounds__(kBlock) void k_check_depth(const Node* __restrict__
     if (depth[i] >= kStack) atomicAdd(&err[5], 1);
 }
 
-__global__ __launch_bounds__(kBlock) void k_check_wide(const Node* __restrict__ nodes, int n,
+// wide node of every even-depth internal node against a fresh collapse; leaf4: the leaf-size-4
+// form (nodes inside a leaf range have none)
+__global__ __launch_bounds__(kBlock) void k_check_wide(const Node* __restrict__ nodes,
+                                                      const BNode* __restrict__ bn,
+                                                      const int* __restrict__ parent, int n,
                                                       const int* __restrict__ depth,
                                                       const int* __restrict__ wide_id,
                                                       const WideNode* __restrict__ wide,
-                                                      int* __restrict__ err) {
+                                                      int leaf4, int* __restrict__ err) {
     const int i = blockIdx.x * kBlock + threadIdx.x;
     if (i >= n - 1 || (depth[i] & 1) != 0) return;
+    if (leaf4 && own_small_code(nodes, bn, parent, i) != 0) return;
     WideNode want;
-    wide_node_of(nodes, n, wide_id, i, want);
+    if (leaf4) wide4_node_of(nodes, bn, n, wide_id, i, want);
+    else wide_node_of(nodes, n, wide_id, i, want);
     const WideNode got = wide[wide_id[i]];
     const unsigned* a = reinterpret_cast<const unsigned*>(&want);
     const unsigned* b = reinterpret_cast<const unsigned*>(&got);
@@ -461,6 +490,7 @@ int finish_tree(qk_tree* t, Header* h, int2* ranges, bool ranges_ready, cudaStre
     if (e != cudaSuccess) return cuda_status(e, "build depth readback");
     t->depth = depth;
     t->wide_count = 0;
+    t->wide_leaf = 0;
     if (depth >= kStack) return fail(QK_ERR_DEPTH, "tree depth %d exceeds %d", depth, kStack - 1);
     return QK_OK;
 }
@@ -565,9 +595,9 @@ int validate_impl(const qk_tree* t, const void* items, int* err, void* ws, cudaS
     k_check_hist<<<blocks_for(n), kBlock, 0, s>>>(hist, n, err);
     k_check_depth<<<blocks_for(count), kBlock, 0, s>>>(nodes, t->depth_arr, n, err);
     if (t->wide_count > 0 && t->wide) {
-        k_check_wide<<<blocks_for(n - 1), kBlock, 0, s>>>(nodes, n, t->depth_arr, t->wide_id,
-                                                          static_cast<const WideNode*>(t->wide),
-                                                          err);
+        k_check_wide<<<blocks_for(n - 1), kBlock, 0, s>>>(
+            nodes, static_cast<const BNode*>(t->bnodes), t->parent, n, t->depth_arr, t->wide_id,
+            static_cast<const WideNode*>(t->wide), t->wide_leaf == 4 ? 1 : 0, err);
     }
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? QK_OK : cuda_status(e, "validate");
@@ -598,7 +628,7 @@ size_t build_core_bytes(int kind, int n, int builder) {
     Carve w;
     w.take<char>(scan_ws_bytes(n));
     if (w.used > need) need = w.used;
-    if (builder == QK_BUILD_SAH) need = std::max(need, sah_ws_bytes(n));
+    if (builder == QK_BUILD_SAH || builder == QK_BUILD_SAH4) need = std::max(need, sah_ws_bytes(n));
     return need;
 }
 
@@ -616,11 +646,11 @@ int build_tree(qk_tree* t, int builder, int bins, const void* items, void* ws, s
                cudaStream_t s) {
     (void)ws_bytes;
     stage_mark(kMarkStart, s);
-    if (builder == QK_BUILD_SAH) {
+    if (builder == QK_BUILD_SAH || builder == QK_BUILD_SAH4) {
         cudaMemsetAsync(t->flags, 0, sizeof(int) * static_cast<size_t>(t->n - 1), s);
-        const int st = build_sah(t, bins, items, ws, s);
+        const int st = build_sah(t, bins, builder == QK_BUILD_SAH4 ? 4 : 1, items, ws, s);
         if (st != QK_OK) return st;
-        return finish_tree(t, static_cast<Header*>(ws), build_ranges(ws, t->kind, t->n, QK_BUILD_SAH),
+        return finish_tree(t, static_cast<Header*>(ws), build_ranges(ws, t->kind, t->n, builder),
                            false, s);
     }
     switch (t->kind) {
@@ -650,19 +680,32 @@ int refit_tree_dirty(qk_tree* t, const int* ids, const void* items, int count, v
     }
 }
 
+// re-emits the wide nodes in the form tree->wide_leaf records (after a refit)
 int wide_emit_all(qk_tree* t, cudaStream_t s) {
     const int n = t->n;
-    k_wide_emit<<<blocks_for(n - 1), kBlock, 0, s>>>(static_cast<const Node*>(t->nodes), n,
-                                                     t->depth_arr, t->wide_id,
-                                                     static_cast<WideNode*>(t->wide));
+    if (t->wide_leaf == 4) {
+        k_wide4_emit<<<blocks_for(n - 1), kBlock, 0, s>>>(
+            static_cast<const Node*>(t->nodes), static_cast<const BNode*>(t->bnodes), t->parent, n,
+            t->depth_arr, t->wide_id, static_cast<WideNode*>(t->wide));
+    } else {
+        k_wide_emit<<<blocks_for(n - 1), kBlock, 0, s>>>(static_cast<const Node*>(t->nodes), n,
+                                                         t->depth_arr, t->wide_id,
+                                                         static_cast<WideNode*>(t->wide));
+    }
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? QK_OK : cuda_status(e, "wide emit");
 }
 
-int wide_build(qk_tree* t, void* ws, size_t ws_bytes, cudaStream_t s) {
+int wide_build(qk_tree* t, int leaf, void* ws, size_t ws_bytes, cudaStream_t s) {
     (void)ws_bytes;
     const int n = t->n, m = n - 1;
-    k_wide_flags<<<blocks_for(m), kBlock, 0, s>>>(t->depth_arr, m, t->flags);
+    if (leaf == 4) {
+        k_wide4_flags<<<blocks_for(m), kBlock, 0, s>>>(static_cast<const Node*>(t->nodes),
+                                                       static_cast<const BNode*>(t->bnodes),
+                                                       t->parent, t->depth_arr, m, t->flags);
+    } else {
+        k_wide_flags<<<blocks_for(m), kBlock, 0, s>>>(t->depth_arr, m, t->flags);
+    }
     // wide_id = exclusive scan of the flags; count = last prefix + last flag
     cudaError_t e = scan_exclusive(t->flags, t->wide_id, m, false, ws, s);
     if (e != cudaSuccess) return cuda_status(e, "wide scan");
@@ -675,6 +718,7 @@ int wide_build(qk_tree* t, void* ws, size_t ws_bytes, cudaStream_t s) {
     // the flags are scratch of the bottom-up pass, which expects zeros
     cudaMemsetAsync(t->flags, 0, sizeof(int) * static_cast<size_t>(m), s);
     t->wide_count = tail[0] + tail[1];
+    t->wide_leaf = leaf == 4 ? 4 : 1;
     if (t->wide_count <= 0) return fail(QK_ERR_INVALID, "no wide nodes");
     // first call without a node buffer only sizes it
     if (t->wide == nullptr) return QK_OK;

@@ -251,4 +251,63 @@ __device__ __forceinline__ void wide_node_of(const Node* __restrict__ nodes, int
     }
 }
 
+// Small-subtree code of internal node g as its parent's traversal node keeps it (0 for the
+// root, whose subtree is never one leaf slot).
+__device__ __forceinline__ int own_small_code(const Node* __restrict__ nodes,
+                                              const BNode* __restrict__ bn,
+                                              const int* __restrict__ parent, int g) {
+    const int p = parent[g];
+    if (p < 0) return 0;
+    const float4 v3 = bn[p].v3;
+    return __float_as_int(nodes[p].left == g ? v3.z : v3.w);
+}
+
+// 4-wide node of binary node i in the leaf-size-4 form (no quarry counterpart; quarry keeps
+// `pad` zero): as wide_node_of, except that a child or grandchild whose subtree holds 2..4
+// leaves on contiguous slots takes ONE slot as a leaf range -- child = ~first slot (the leaf
+// code of its first slot), pad = its primitive count -- and a single leaf slot has pad = 1.
+// Internal slots keep pad = 0, so a traversal reads max(pad, 1) primitives at every leaf slot
+// of either form.  The wide nodes are the even-depth internal nodes that are not inside such a
+// range (the root always).
+__device__ __forceinline__ void wide4_slot(WideEntry& e, const Node* __restrict__ nodes, int n,
+                                           const int* __restrict__ wide_id, int c, int code) {
+    if (c >= n - 1) {
+        wide_fill(e, nodes[c], nodes[c].left);
+        e.pad = 1;
+    } else if (code != 0) {
+        wide_fill(e, nodes[c], ~(code >> 2));
+        e.pad = (code & 3) + 1;
+    } else {
+        wide_fill(e, nodes[c], wide_id[c]);
+    }
+}
+
+__device__ __forceinline__ void wide4_node_of(const Node* __restrict__ nodes,
+                                              const BNode* __restrict__ bn, int n,
+                                              const int* __restrict__ wide_id, int i,
+                                              WideNode& out) {
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+        out.c[s].mn[0] = out.c[s].mn[1] = out.c[s].mn[2] = kInf;
+        out.c[s].mx[0] = out.c[s].mx[1] = out.c[s].mx[2] = -kInf;
+        out.c[s].child = kEmptySlot;
+        out.c[s].pad = 0;
+    }
+    const int kids[2] = {nodes[i].left, nodes[i].right};
+    const float4 v3 = bn[i].v3;
+    const int codes[2] = {__float_as_int(v3.z), __float_as_int(v3.w)};
+    int slot = 0;
+    for (int k = 0; k < 2; ++k) {
+        const int c = kids[k];
+        if (c >= n - 1 || codes[k] != 0) {
+            wide4_slot(out.c[slot++], nodes, n, wide_id, c, codes[k]);
+            continue;
+        }
+        const float4 w3 = bn[c].v3;
+        const int g[2] = {nodes[c].left, nodes[c].right};
+        const int gcodes[2] = {__float_as_int(w3.z), __float_as_int(w3.w)};
+        for (int j = 0; j < 2; ++j) wide4_slot(out.c[slot++], nodes, n, wide_id, g[j], gcodes[j]);
+    }
+}
+
 }  // namespace qk

@@ -155,9 +155,9 @@ int qk_build(qk_tree* tree, int builder, int sah_bins, const void* items, void* 
     int st = check_tree(tree);
     if (st) return st;
     if (!items) return fail(QK_ERR_INVALID, "items is NULL");
-    if (builder != QK_BUILD_LBVH && builder != QK_BUILD_SAH)
-        return fail(QK_ERR_INVALID, "builder must be QK_BUILD_LBVH or QK_BUILD_SAH");
-    if (builder == QK_BUILD_SAH && (sah_bins < 4 || sah_bins > 64))
+    if (builder != QK_BUILD_LBVH && builder != QK_BUILD_SAH && builder != QK_BUILD_SAH4)
+        return fail(QK_ERR_INVALID, "builder must be QK_BUILD_LBVH, QK_BUILD_SAH or QK_BUILD_SAH4");
+    if (builder != QK_BUILD_LBVH && (sah_bins < 4 || sah_bins > 64))
         return fail(QK_ERR_INVALID, "sah_bins must be in [4, 64]");
     st = check_ws(workspace, workspace_bytes, build_ws_bytes(tree->kind, tree->n, builder));
     if (st) return st;
@@ -230,7 +230,16 @@ int qk_wide_build(qk_tree* tree, void* workspace, size_t workspace_bytes, void* 
     if (!tree->wide_id) return fail(QK_ERR_INVALID, "wide_id is NULL");
     st = check_ws(workspace, workspace_bytes, build_ws_bytes(tree->kind, tree->n, 0));
     if (st) return st;
-    return wide_build(tree, workspace, workspace_bytes, as_stream(stream));
+    return wide_build(tree, 1, workspace, workspace_bytes, as_stream(stream));
+}
+
+int qk_wide_build_leaf4(qk_tree* tree, void* workspace, size_t workspace_bytes, void* stream) {
+    int st = check_tree(tree);
+    if (st) return st;
+    if (!tree->wide_id) return fail(QK_ERR_INVALID, "wide_id is NULL");
+    st = check_ws(workspace, workspace_bytes, build_ws_bytes(tree->kind, tree->n, 0));
+    if (st) return st;
+    return wide_build(tree, 4, workspace, workspace_bytes, as_stream(stream));
 }
 
 int qk_raycast(const qk_tree* tree, const void* rays, int count, uint64_t* out, unsigned flags,

@@ -124,7 +124,7 @@ int build_tree(qk_tree* t, int builder, int bins, const void* items, void* ws, s
                cudaStream_t s);
 // SAH topology (qk_sah.cu): fills links, parents, order-derived leaves; boxes come after
 size_t sah_ws_bytes(int n);
-int build_sah(qk_tree* t, int bins, const void* items, void* ws, cudaStream_t s);
+int build_sah(qk_tree* t, int bins, int leaf_size, const void* items, void* ws, cudaStream_t s);
 // Forest of independent ranges for the SAH builder's lower tiers (qk_sah.cu): task i =
 // {begin, end, node, depth} over positions of `order` (indices into cen / plo / phi), its
 // internal nodes below `node` numbered from id_base[i]; node < 0 skips the task.  Leaf of
@@ -142,7 +142,7 @@ int update_topology(const qk_tree* old_t, qk_tree* new_t, const qk_topo_edit* ed
 int refit_tree(qk_tree* t, const void* items, cudaStream_t s);
 int refit_tree_dirty(qk_tree* t, const int* ids, const void* items, int count, void* ws,
                      cudaStream_t s);
-int wide_build(qk_tree* t, void* ws, size_t ws_bytes, cudaStream_t s);
+int wide_build(qk_tree* t, int leaf, void* ws, size_t ws_bytes, cudaStream_t s);
 int wide_emit_all(qk_tree* t, cudaStream_t s);
 size_t validate_ws_bytes(int n);
 int validate_tree(const qk_tree* t, const void* items, int* errors, void* ws, cudaStream_t s);

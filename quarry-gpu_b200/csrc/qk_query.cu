@@ -501,7 +501,8 @@ __global__ __launch_bounds__(kBlock, kMinBlocks) void k_ray_bin_dyn(
     flush_stats<kStats>(true, ntests, ttests, overflow, stats);
 }
 
-template <bool kStats>
+// kRange: the tree's wide nodes are the leaf-size-4 form (a leaf slot holds up to 4 primitives)
+template <bool kStats, bool kRange = false>
 __global__ __launch_bounds__(kBlock) void k_ray_wide(const WideNode* __restrict__ wn,
                                                     const float4* __restrict__ leaves,
                                                     const float4* __restrict__ rays,
@@ -517,7 +518,7 @@ __global__ __launch_bounds__(kBlock) void k_ray_wide(const WideNode* __restrict_
         const RayPre R = prepare_ray(__ldg(rays + 2 * r), __ldg(rays + 2 * r + 1));
         LocalStack<kStackWide> st;
         int best_id;
-        out[r] = ray_wide_one(wn, leaves, R, max_iter, st, tv, best_id);
+        out[r] = ray_wide_one<kRange>(wn, leaves, R, max_iter, st, tv, best_id);
         if (ids) ids[r] = best_id;
     }
     flush_stats<kStats>(active, tv.nodes, tv.leaves, tv.overflow, stats);
@@ -577,7 +578,7 @@ __global__ __launch_bounds__(kBlock) void k_closest_bin(const BNode* __restrict_
     flush_stats<kStats>(active, tv.nodes, tv.leaves, tv.overflow, stats);
 }
 
-template <class Ops, bool kStats>
+template <class Ops, bool kStats, bool kRange = false>
 __global__ __launch_bounds__(kBlock) void k_closest_wide(const WideNode* __restrict__ wn,
                                                         const float4* __restrict__ leaves,
                                                         const float* __restrict__ pts,
@@ -591,7 +592,7 @@ __global__ __launch_bounds__(kBlock) void k_closest_wide(const WideNode* __restr
         const int q = order ? static_cast<int>(order[i]) : i;
         const float3 p = f3(pts[3 * q], pts[3 * q + 1], pts[3 * q + 2]);
         LocalStack<kStackWide> st;
-        out[q] = closest_wide_one<Ops>(wn, leaves, p, max_iter, st, tv);
+        out[q] = closest_wide_one<Ops, kRange>(wn, leaves, p, max_iter, st, tv);
     }
     flush_stats<kStats>(active, tv.nodes, tv.leaves, tv.overflow, stats);
 }
@@ -621,7 +622,7 @@ __global__ __launch_bounds__(kBlock) void k_knn_bin(const BNode* __restrict__ bn
     flush_stats<kStats>(active, tv.nodes, tv.leaves, tv.overflow, stats);
 }
 
-template <class Ops, int K, bool kStats>
+template <class Ops, int K, bool kStats, bool kRange = false>
 __global__ __launch_bounds__(kBlock) void k_knn_wide(const WideNode* __restrict__ wn,
                                                     const float4* __restrict__ leaves,
                                                     const float* __restrict__ pts,
@@ -636,7 +637,7 @@ __global__ __launch_bounds__(kBlock) void k_knn_wide(const WideNode* __restrict_
         const float3 p = f3(pts[3 * q], pts[3 * q + 1], pts[3 * q + 2]);
         LocalStack<kStackWide> st;
         KnnTable<K> tab;
-        knn_wide_one<Ops, K>(wn, leaves, p, k, max_iter, st, tv, tab);
+        knn_wide_one<Ops, K, kRange>(wn, leaves, p, k, max_iter, st, tv, tab);
         write_knn<K>(tab, k, out + static_cast<size_t>(q) * stride);
     }
     flush_stats<kStats>(active, tv.nodes, tv.leaves, tv.overflow, stats);
@@ -711,7 +712,7 @@ __global__ __launch_bounds__(kBlock) void k_radius_fill_lost(
                                                           end, keys, max_iter, st, tv, lnodes);
 }
 
-template <class Ops, bool kFill, bool kStats>
+template <class Ops, bool kFill, bool kStats, bool kRange = false>
 __global__ __launch_bounds__(kBlock) void k_radius_wide(
     const WideNode* __restrict__ wn, const float4* __restrict__ leaves,
     const float* __restrict__ pts, const uint32_t* __restrict__ order, int count, float r2,
@@ -727,8 +728,8 @@ __global__ __launch_bounds__(kBlock) void k_radius_wide(
         const int write = kFill ? offsets[q] : 0;
         const int end = kFill ? offsets[q + 1] : 0;
         LocalStack<kStackWide> st;
-        const int found = radius_wide_one<Ops, kFill>(wn, leaves, p, r2, write, end, keys,
-                                                      max_iter, st, tv);
+        const int found = radius_wide_one<Ops, kFill, kRange>(wn, leaves, p, r2, write, end,
+                                                              keys, max_iter, st, tv);
         if (!kFill) counts[q] = found;
     }
     flush_stats<kStats>(active, tv.nodes, tv.leaves, tv.overflow, stats);
@@ -1128,8 +1129,13 @@ int closest_impl(const qk_tree* t, const float* pts, int count, uint2* out, unsi
     }
     if (wide) {
         const WideNode* wn = static_cast<const WideNode*>(t->wide);
-        if (st) k_closest_wide<Ops, true><<<g, qb, 0, s>>>(wn, leaves, pts, order, count, out, t->n * 2 + 64, stats);
-        else k_closest_wide<Ops, false><<<g, qb, 0, s>>>(wn, leaves, pts, order, count, out, t->n * 2 + 64, stats);
+        if (t->wide_leaf == 4) {
+            if (st) k_closest_wide<Ops, true, true><<<g, qb, 0, s>>>(wn, leaves, pts, order, count, out, t->n * 2 + 64, stats);
+            else k_closest_wide<Ops, false, true><<<g, qb, 0, s>>>(wn, leaves, pts, order, count, out, t->n * 2 + 64, stats);
+        } else {
+            if (st) k_closest_wide<Ops, true><<<g, qb, 0, s>>>(wn, leaves, pts, order, count, out, t->n * 2 + 64, stats);
+            else k_closest_wide<Ops, false><<<g, qb, 0, s>>>(wn, leaves, pts, order, count, out, t->n * 2 + 64, stats);
+        }
     } else if (flags & QK_TUNE_SPLIT) {
         const BNode* bn = static_cast<const BNode*>(t->bnodes);
         const int gs = blocks_for(static_cast<long long>(count) * 32);
@@ -1162,8 +1168,13 @@ void launch_knn(const qk_tree* t, const float* pts, int count, int k, int stride
         else k_knn_split<Ops, K, false><<<gs, kBlock, 0, s>>>(bn, leaves, pts, order, count, k, stride, out, t->n * 2 + 64, stats);
     } else if (wide) {
         const WideNode* wn = static_cast<const WideNode*>(t->wide);
-        if (stats) k_knn_wide<Ops, K, true><<<g, qb, 0, s>>>(wn, leaves, pts, order, count, k, stride, out, t->n * 2 + 64, stats);
-        else k_knn_wide<Ops, K, false><<<g, qb, 0, s>>>(wn, leaves, pts, order, count, k, stride, out, t->n * 2 + 64, stats);
+        if (t->wide_leaf == 4) {
+            if (stats) k_knn_wide<Ops, K, true, true><<<g, qb, 0, s>>>(wn, leaves, pts, order, count, k, stride, out, t->n * 2 + 64, stats);
+            else k_knn_wide<Ops, K, false, true><<<g, qb, 0, s>>>(wn, leaves, pts, order, count, k, stride, out, t->n * 2 + 64, stats);
+        } else {
+            if (stats) k_knn_wide<Ops, K, true><<<g, qb, 0, s>>>(wn, leaves, pts, order, count, k, stride, out, t->n * 2 + 64, stats);
+            else k_knn_wide<Ops, K, false><<<g, qb, 0, s>>>(wn, leaves, pts, order, count, k, stride, out, t->n * 2 + 64, stats);
+        }
     } else if (leaf4) {
         const BNode* bn = static_cast<const BNode*>(t->bnodes);
         if (stats) k_knn_bin<Ops, K, true, true><<<g, qb, 0, s>>>(bn, leaves, pts, order, count, k, stride, out, t->n * 2 + 64, stats, leaf_nodes(t));
@@ -1228,8 +1239,13 @@ int radius_launch(const qk_tree* t, const float* pts, int count, float r2, int* 
         else k_radius_split<Ops, kFill, false><<<gs, kBlock, 0, s>>>(bn, leaves, pts, order, count, r2, counts, lane_counts, offsets, keys, t->n * 2 + 64, stats);
     } else if (flags & QK_WIDE) {
         const WideNode* wn = static_cast<const WideNode*>(t->wide);
-        if (stats) k_radius_wide<Ops, kFill, true><<<g, qb, 0, s>>>(wn, leaves, pts, order, count, r2, counts, offsets, keys, t->n * 2 + 64, stats);
-        else k_radius_wide<Ops, kFill, false><<<g, qb, 0, s>>>(wn, leaves, pts, order, count, r2, counts, offsets, keys, t->n * 2 + 64, stats);
+        if (t->wide_leaf == 4) {
+            if (stats) k_radius_wide<Ops, kFill, true, true><<<g, qb, 0, s>>>(wn, leaves, pts, order, count, r2, counts, offsets, keys, t->n * 2 + 64, stats);
+            else k_radius_wide<Ops, kFill, false, true><<<g, qb, 0, s>>>(wn, leaves, pts, order, count, r2, counts, offsets, keys, t->n * 2 + 64, stats);
+        } else {
+            if (stats) k_radius_wide<Ops, kFill, true><<<g, qb, 0, s>>>(wn, leaves, pts, order, count, r2, counts, offsets, keys, t->n * 2 + 64, stats);
+            else k_radius_wide<Ops, kFill, false><<<g, qb, 0, s>>>(wn, leaves, pts, order, count, r2, counts, offsets, keys, t->n * 2 + 64, stats);
+        }
     } else if (flags & QK_TUNE_LEAF4) {
         const BNode* bn = static_cast<const BNode*>(t->bnodes);
         const Node* nodes = static_cast<const Node*>(t->nodes);
@@ -1302,8 +1318,13 @@ int ray_query(const qk_tree* t, const void* rays, int count, uint64_t* out, int*
     const int g = blocks_for(count);
     if (flags & QK_WIDE) {
         const WideNode* wn = static_cast<const WideNode*>(t->wide);
-        if (stt) k_ray_wide<true><<<g, kBlock, 0, s>>>(wn, leaves, r4, order, count, res, ids, t->n * 2 + 64, stt);
-        else k_ray_wide<false><<<g, kBlock, 0, s>>>(wn, leaves, r4, order, count, res, ids, t->n * 2 + 64, stt);
+        if (t->wide_leaf == 4) {
+            if (stt) k_ray_wide<true, true><<<g, kBlock, 0, s>>>(wn, leaves, r4, order, count, res, ids, t->n * 2 + 64, stt);
+            else k_ray_wide<false, true><<<g, kBlock, 0, s>>>(wn, leaves, r4, order, count, res, ids, t->n * 2 + 64, stt);
+        } else {
+            if (stt) k_ray_wide<true><<<g, kBlock, 0, s>>>(wn, leaves, r4, order, count, res, ids, t->n * 2 + 64, stt);
+            else k_ray_wide<false><<<g, kBlock, 0, s>>>(wn, leaves, r4, order, count, res, ids, t->n * 2 + 64, stt);
+        }
     } else if (flags & QK_TUNE_DYNAMIC) {
         const BNode* bn = static_cast<const BNode*>(t->bnodes);
         const Node* nodes = static_cast<const Node*>(t->nodes);

@@ -616,9 +616,12 @@ constexpr int kMediumCap = kBlockRange / (kWarpRange + 1) + 1;
 // orders are then stably partitioned by side, so the children own [s, s + k) and
 // [s + k, s + m) again.  Two-item nodes split 1 | 1 without a sweep.  At the end position p
 // of the axis-0 order is leaf slot b + p.  `scratch` holds 32 ints of this warp.
+// Nodes of at most `small` items (2, or 4 for leaf-size-4 trees) are SAH leaves: no sweep,
+// they are split by count (left m / 2 items, in position order) down to single items, so the
+// range keeps the one-primitive-per-leaf node format that every other pass reads.
 __device__ void warp_build(int* perm, const float4* sc, const float4* slo, const float4* shi,
                            int b, int c, int node, int depth, int next_id, Node* nodes, BNode* bn,
-                           int* parent, int n, int gbase, int* scratch) {
+                           int* parent, int n, int gbase, int* scratch, int small) {
     const int lane = threadIdx.x & 31;
     const bool mine = lane < c;
     const int li = perm[b + (mine ? lane : 0)];
@@ -647,8 +650,25 @@ __device__ void warp_build(int* perm, const float4* sc, const float4* slo, const
     while (top > 0 && guard++ < 4 * kWarpRange) {
         --top;
         const int s = stk_s[top], m = stk_m[top], rn = stk_n[top], rd = stk_d[top];
-        if (m == 2) {
-            if (lane == 0) link(nodes, bn, parent, rn, n - 1 + gbase + b + s, n - 1 + gbase + b + s + 1, n);
+        if (m <= small) {
+            const int leaf0 = n - 1 + gbase + b + s;
+            if (m == 2) {
+                if (lane == 0) link(nodes, bn, parent, rn, leaf0, leaf0 + 1, n);
+            } else if (m == 3) {
+                const int rid = next_id++;
+                if (lane == 0) {
+                    link(nodes, bn, parent, rn, leaf0, rid, n);
+                    link(nodes, bn, parent, rid, leaf0 + 1, leaf0 + 2, n);
+                }
+            } else {
+                const int lid = next_id++;
+                const int rid = next_id++;
+                if (lane == 0) {
+                    link(nodes, bn, parent, rn, lid, rid, n);
+                    link(nodes, bn, parent, lid, leaf0, leaf0 + 1, n);
+                    link(nodes, bn, parent, rid, leaf0 + 2, leaf0 + 3, n);
+                }
+            }
             continue;
         }
         float best = kInf;
@@ -764,7 +784,7 @@ __device__ void warp_build(int* perm, const float4* sc, const float4* slo, const
 __device__ void warp_piece_tree(Piece root, int* perm, int* tmp, const float4* sc,
                                 const float4* slo, const float4* shi, unsigned* wb, Piece* wstk,
                                 int* scratch, int bins, Node* nodes, BNode* bn, int* parent, int n,
-                                int gbase, int* err) {
+                                int gbase, int* err, int small) {
     const int lane = threadIdx.x & 31;
     int next = root.ids;
     if (lane == 0) wstk[0] = root;
@@ -849,7 +869,7 @@ __device__ void warp_piece_tree(Piece root, int* perm, int* tmp, const float4* s
             const Piece q = k == 0 ? L : R;
             if (q.count >= 2 && q.count <= kWarpRange) {
                 warp_build(perm, sc, slo, shi, q.begin, q.count, q.node, q.depth, next, nodes, bn,
-                           parent, n, gbase, scratch);
+                           parent, n, gbase, scratch, small);
                 next += q.count - 2;
             }
         }
@@ -1070,13 +1090,13 @@ __global__ __launch_bounds__(kBlock) void k_block_build(const Task* __restrict__
         const int total_m = nm;
         for (int m = warp; m < total_m; m += kBlock / 32)
             warp_piece_tree(mpieces[m], perm, tmp, sc, slo, shi, wbins, wstk, wscratch, bins,
-                            nodes, bn, parent, n, tk.begin, err);
+                            nodes, bn, parent, n, tk.begin, err, 2);
         __syncthreads();
         const int total_w = nw;
         for (int w = warp; w < total_w; w += kBlock / 32) {
             const Piece q = wpieces[w];
             warp_build(perm, sc, slo, shi, q.begin, q.count, q.node, q.depth, q.ids, nodes, bn,
-                       parent, n, tk.begin, wscratch);
+                       parent, n, tk.begin, wscratch, 2);
         }
         __syncthreads();
         for (int i = threadIdx.x; i < count; i += kBlock) order[tk.begin + i] = sid[perm[i]];
@@ -1098,7 +1118,8 @@ __global__ __launch_bounds__(kBlock, 4) void k_warp_tasks(const Task* __restrict
                                                       const float4* __restrict__ plo,
                                                       const float4* __restrict__ phi, Node* nodes,
                                                       BNode* bn, int* parent, int n, int bins,
-                                                      int* __restrict__ err, int large_ok) {
+                                                      int* __restrict__ err, int large_ok,
+                                                      int small) {
     extern __shared__ unsigned wsm[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned* wb = wsm + static_cast<size_t>(warp) * 3 * bins * kBinWords;
@@ -1116,10 +1137,10 @@ __global__ __launch_bounds__(kBlock, 4) void k_warp_tasks(const Task* __restrict
         }
         if (count <= kWarpRange) {
             warp_build(order, cen, plo, phi, tk.begin, count, tk.node, tk.depth, id_base[ti], nodes,
-                       bn, parent, n, 0, scratch);
+                       bn, parent, n, 0, scratch, small);
         } else {
             warp_piece_tree(Piece{tk.begin, count, tk.node, tk.depth, id_base[ti]}, order, tmp, cen,
-                            plo, phi, wb, wstk, scratch, bins, nodes, bn, parent, n, 0, err);
+                            plo, phi, wb, wstk, scratch, bins, nodes, bn, parent, n, 0, err, small);
         }
     }
 }
@@ -1224,7 +1245,8 @@ SahWs carve_sah(Carve& c, int n) {
 }
 
 template <class Ops>
-int build_sah_impl(qk_tree* t, int bins, const void* items_v, void* ws, cudaStream_t s) {
+int build_sah_impl(qk_tree* t, int bins, int small, const void* items_v, void* ws,
+                   cudaStream_t s) {
     const int n = t->n;
     const float* items = static_cast<const float*>(items_v);
     Carve c{static_cast<char*>(ws)};
@@ -1318,7 +1340,7 @@ int build_sah_impl(qk_tree* t, int bins, const void* items_v, void* ws, cudaStre
         k_warp_tasks<<<min(blocks_for(static_cast<long long>(nblk) * 32), 148 * 8), kBlock,
                        warp_tasks_smem(bins), s>>>(w.blocks, nblk, w.id_base, ord, alt, w.cen,
                                                    w.plo, w.phi, nodes, bn, t->parent, n, bins, err,
-                                                   0);
+                                                   0, small);
     } else {
         int base = 0;
         cudaMemcpyAsync(&base, w.L.counters + 3, sizeof(int), cudaMemcpyDeviceToHost, s);
@@ -1361,7 +1383,7 @@ int sah_forest(const int4* tasks, int ntask, int max_count, const int* id_base, 
     k_warp_tasks<<<min(blocks_for(static_cast<long long>(ntask) * 32), 148 * 8), kBlock,
                    warp_tasks_smem(bins), s>>>(tk, ntask, id_base, order, tmp, cen, plo, phi, nodes,
                                                bn, t->parent, t->n, bins, err,
-                                               max_count > kTaskRange ? 1 : 0);
+                                               max_count > kTaskRange ? 1 : 0, 2);
     if (max_count > kTaskRange) {
         cudaFuncSetAttribute(k_block_build, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              static_cast<int>(block_smem(kMaxBins)));
@@ -1372,12 +1394,14 @@ int sah_forest(const int4* tasks, int ntask, int max_count, const int* id_base, 
     return e == cudaSuccess ? QK_OK : cuda_status(e, "SAH forest");
 }
 
-int build_sah(qk_tree* t, int bins, const void* items, void* ws, cudaStream_t s) {
+int build_sah(qk_tree* t, int bins, int leaf_size, const void* items, void* ws, cudaStream_t s) {
     if (bins < 4 || bins > kMaxBins) return fail(QK_ERR_INVALID, "sah_bins must be in [4, 64]");
+    if (leaf_size != 1 && leaf_size != 4) return fail(QK_ERR_INVALID, "SAH leaf size must be 1 or 4");
+    const int small = leaf_size == 4 ? 4 : 2;  // nodes of at most `small` primitives are not swept
     switch (t->kind) {
-        case kTri: return build_sah_impl<TriOps>(t, bins, items, ws, s);
-        case kPoint: return build_sah_impl<PointOps>(t, bins, items, ws, s);
-        case kGauss: return build_sah_impl<GaussOps>(t, bins, items, ws, s);
+        case kTri: return build_sah_impl<TriOps>(t, bins, small, items, ws, s);
+        case kPoint: return build_sah_impl<PointOps>(t, bins, small, items, ws, s);
+        case kGauss: return build_sah_impl<GaussOps>(t, bins, small, items, ws, s);
         default: return fail(QK_ERR_INVALID, "unknown primitive kind %d", t->kind);
     }
 }

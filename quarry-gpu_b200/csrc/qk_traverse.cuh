@@ -116,13 +116,18 @@ __device__ __forceinline__ Box root_box(const Node* __restrict__ nodes) {
     return bx;
 }
 
+// slot s of wide node `node`: box, child and the slot's primitive count -- max(pad, 1): 1 for
+// every leaf slot of quarry's form (pad 0), up to 4 for a leaf range of the leaf-size-4 form
+// (the primitives on slots ~child .. ~child + count - 1); meaningless for internal slots.  The
+// traversals read the count only when instantiated for the leaf-size-4 form (kRange).
 __device__ __forceinline__ void load_wide_entry(const WideNode* __restrict__ w, int node, int s,
-                                                float3& lo, float3& hi, int& child) {
+                                                float3& lo, float3& hi, int& child, int& count) {
     const float4* p = reinterpret_cast<const float4*>(w + node) + 2 * s;
     const float4 a = __ldg(p), b = __ldg(p + 1);
     lo = f3(a.x, a.y, a.z);
     hi = f3(a.w, b.x, b.y);
     child = __float_as_int(b.z);
+    count = max(__float_as_int(b.w), 1);
 }
 
 // statistics: warp-aggregated counters (src/gpu/raycast.cu:147-156)
@@ -270,7 +275,7 @@ __device__ __forceinline__ unsigned long long ray_bin_one(const BNode* __restric
 
 // First hit in a 4-wide tree: hit slots sorted by entry t, leaves tested nearest first,
 // the nearest internal child followed and the others pushed far-first.
-template <class St>
+template <bool kRange = false, class St>
 __device__ __forceinline__ unsigned long long ray_wide_one(const WideNode* __restrict__ wn,
                                                            const float4* __restrict__ leaves,
                                                            const RayPre& R, int max_iter, St& st,
@@ -286,14 +291,14 @@ __device__ __forceinline__ unsigned long long ray_wide_one(const WideNode* __res
             tv.overflow = true;
             break;
         }
-        int child[4];
+        int child[4], cnt[4];
         float key[4];
         int hits = 0;
 #pragma unroll
         for (int s = 0; s < 4; ++s) {
             float3 lo, hi;
-            int c;
-            load_wide_entry(wn, node, s, lo, hi, c);
+            int c, nc;
+            load_wide_entry(wn, node, s, lo, hi, c, nc);
             float t;
             if (c != kEmptySlot && ray_box(R, lo, hi, bound, t)) {
                 ++tv.nodes;
@@ -301,18 +306,23 @@ __device__ __forceinline__ unsigned long long ray_wide_one(const WideNode* __res
                 while (j > 0 && key[j - 1] > t) {
                     key[j] = key[j - 1];
                     child[j] = child[j - 1];
+                    if (kRange) cnt[j] = cnt[j - 1];
                     --j;
                 }
                 key[j] = t;
                 child[j] = c;
+                if (kRange) cnt[j] = nc;
             }
         }
         int next = -1;
         float nextT = 0.0f;
         for (int j = 0; j < hits; ++j) {
             if (child[j] < 0) {
-                ++tv.leaves;
-                test_tri(R, leaves, ~child[j], best, bound, any, best_id);
+                const int nq = kRange ? cnt[j] : 1;
+                for (int q = 0; q < nq; ++q) {
+                    ++tv.leaves;
+                    test_tri(R, leaves, ~child[j] + q, best, bound, any, best_id);
+                }
             }
         }
         for (int j = hits - 1; j >= 0; --j) {
@@ -449,7 +459,7 @@ __device__ __forceinline__ uint2 closest_bin_one(const BNode* __restrict__ bn,
     return pack_closest(best, best_id);
 }
 
-template <class Ops, class St>
+template <class Ops, bool kRange = false, class St>
 __device__ __forceinline__ uint2 closest_wide_one(const WideNode* __restrict__ wn,
                                                   const float4* __restrict__ leaves, float3 p,
                                                   int max_iter, St& st, Trav& tv) {
@@ -462,14 +472,14 @@ __device__ __forceinline__ uint2 closest_wide_one(const WideNode* __restrict__ w
             tv.overflow = true;
             break;
         }
-        int child[4];
+        int child[4], cnt[4];
         float key[4];
         int hits = 0;
 #pragma unroll
         for (int s = 0; s < 4; ++s) {
             float3 lo, hi;
-            int c;
-            load_wide_entry(wn, node, s, lo, hi, c);
+            int c, nc;
+            load_wide_entry(wn, node, s, lo, hi, c, nc);
             if (c == kEmptySlot) continue;
             const float d = dist2_box(p, lo, hi);
             if (best_id >= 0 && d > best) continue;
@@ -478,15 +488,20 @@ __device__ __forceinline__ uint2 closest_wide_one(const WideNode* __restrict__ w
             while (j > 0 && key[j - 1] > d) {
                 key[j] = key[j - 1];
                 child[j] = child[j - 1];
+                if (kRange) cnt[j] = cnt[j - 1];
                 --j;
             }
             key[j] = d;
             child[j] = c;
+            if (kRange) cnt[j] = nc;
         }
         for (int j = 0; j < hits; ++j) {
             if (child[j] < 0 && (best_id < 0 || key[j] <= best)) {
-                ++tv.leaves;
-                leaf_closest<Ops>(p, leaves, ~child[j], best, best_id);
+                const int nq = kRange ? cnt[j] : 1;
+                for (int q = 0; q < nq; ++q) {
+                    ++tv.leaves;
+                    leaf_closest<Ops>(p, leaves, ~child[j] + q, best, best_id);
+                }
             }
         }
         int next = -1;
@@ -672,7 +687,7 @@ __device__ __forceinline__ void knn_bin_one(const BNode* __restrict__ bn,
     }
 }
 
-template <class Ops, int K, class St>
+template <class Ops, int K, bool kRange = false, class St>
 __device__ __forceinline__ void knn_wide_one(const WideNode* __restrict__ wn,
                                              const float4* __restrict__ leaves, float3 p, int k,
                                              int max_iter, St& st, Trav& tv, KnnTable<K>& tab) {
@@ -684,14 +699,14 @@ __device__ __forceinline__ void knn_wide_one(const WideNode* __restrict__ wn,
             tv.overflow = true;
             break;
         }
-        int child[4];
+        int child[4], cnt[4];
         float key[4];
         int hits = 0;
 #pragma unroll
         for (int s = 0; s < 4; ++s) {
             float3 lo, hi;
-            int c;
-            load_wide_entry(wn, node, s, lo, hi, c);
+            int c, nc;
+            load_wide_entry(wn, node, s, lo, hi, c, nc);
             if (c == kEmptySlot) continue;
             const float d = dist2_box(p, lo, hi);
             if (!tab.admits(d)) continue;
@@ -700,15 +715,20 @@ __device__ __forceinline__ void knn_wide_one(const WideNode* __restrict__ wn,
             while (j > 0 && key[j - 1] > d) {
                 key[j] = key[j - 1];
                 child[j] = child[j - 1];
+                if (kRange) cnt[j] = cnt[j - 1];
                 --j;
             }
             key[j] = d;
             child[j] = c;
+            if (kRange) cnt[j] = nc;
         }
         for (int j = 0; j < hits; ++j) {
             if (child[j] < 0 && tab.admits(key[j])) {
-                ++tv.leaves;
-                leaf_knn<Ops, K>(p, leaves, ~child[j], tab, k);
+                const int nq = kRange ? cnt[j] : 1;
+                for (int q = 0; q < nq; ++q) {
+                    ++tv.leaves;
+                    leaf_knn<Ops, K>(p, leaves, ~child[j] + q, tab, k);
+                }
             }
         }
         int next = -1;
@@ -964,7 +984,7 @@ __device__ __forceinline__ int radius_bin_one(const BNode* __restrict__ bn,
                                                     lnodes);
 }
 
-template <class Ops, bool kFill, class St, class Sink>
+template <class Ops, bool kFill, bool kRange = false, class St, class Sink>
 __device__ __forceinline__ int radius_wide_visit(const WideNode* __restrict__ wn,
                                                  const float4* __restrict__ leaves, float3 p,
                                                  float r2, Sink& sink, int max_iter, St& st,
@@ -981,17 +1001,20 @@ __device__ __forceinline__ int radius_wide_visit(const WideNode* __restrict__ wn
 #pragma unroll
         for (int s = 0; s < 4; ++s) {
             float3 lo, hi;
-            int c;
-            load_wide_entry(wn, node, s, lo, hi, c);
+            int c, nc;
+            load_wide_entry(wn, node, s, lo, hi, c, nc);
             if (c == kEmptySlot || !(dist2_box(p, lo, hi) <= r2)) continue;
             ++tv.nodes;
             if (c < 0) {
-                ++tv.leaves;
-                int id;
-                const float d2 = Ops::dist2(p, leaves, ~c, id);
-                if (d2 <= r2) {
-                    if (kFill) sink.put(radius_key(d2, id));
-                    ++found;
+                const int nq = kRange ? nc : 1;
+                for (int q = 0; q < nq; ++q) {
+                    ++tv.leaves;
+                    int id;
+                    const float d2 = Ops::dist2(p, leaves, ~c + q, id);
+                    if (d2 <= r2) {
+                        if (kFill) sink.put(radius_key(d2, id));
+                        ++found;
+                    }
                 }
             } else if (next < 0) {
                 next = c;
@@ -1012,14 +1035,14 @@ __device__ __forceinline__ int radius_wide_visit(const WideNode* __restrict__ wn
     return found;
 }
 
-template <class Ops, bool kFill, class St>
+template <class Ops, bool kFill, bool kRange = false, class St>
 __device__ __forceinline__ int radius_wide_one(const WideNode* __restrict__ wn,
                                                const float4* __restrict__ leaves, float3 p,
                                                float r2, int write, int end,
                                                unsigned long long* __restrict__ keys,
                                                int max_iter, St& st, Trav& tv) {
     SegmentSink sink{keys, write, end};
-    return radius_wide_visit<Ops, kFill>(wn, leaves, p, r2, sink, max_iter, st, tv);
+    return radius_wide_visit<Ops, kFill, kRange>(wn, leaves, p, r2, sink, max_iter, st, tv);
 }
 
 // ---------------------------------------------------------------------------------------

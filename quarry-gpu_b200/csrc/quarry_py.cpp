@@ -130,6 +130,42 @@ GpuTopoEdit topoEdit(const py::object& deleted, const py::object& moved,
     return e;
 }
 
+// The edit names the survivors' new places only through `deleted` and `inserted`; `moved`
+// names those whose geometry changed.  A script that places an insertion one index off
+// (quarry's own edge-insert check passes [0, n] for items that np.insert put at 0 and n + 1)
+// leaves a survivor on an index whose primitive is not the one it was, and the tree would keep
+// the old geometry there.  So every survivor is compared, byte for byte, with the primitive now
+// at its new index, and each one that differs joins `moved`: the tree always describes the
+// scene passed in.  Host work, linear in the scene, beside the conversion the module already
+// does.
+template <class T>
+void addChangedSurvivors(const std::vector<T>& before, const std::vector<T>& after,
+                         GpuTopoEdit& e) {
+    const long long nOld = static_cast<long long>(before.size());
+    const long long nNew = static_cast<long long>(after.size());
+    const long long tail = nNew - e.appended;
+    std::vector<char> named(static_cast<size_t>(nNew), 0);
+    for (int id : e.moved)
+        if (id >= 0 && id < nNew) named[static_cast<size_t>(id)] = 1;
+    size_t di = 0, ii = 0;
+    long long j = 0;  // new index of the next survivor
+    for (long long k = 0; k < nOld; ++k) {
+        if (di < e.deleted.size() && e.deleted[di] == k) {
+            ++di;
+            continue;
+        }
+        while (ii < e.inserted.size() && e.inserted[ii] == j) {
+            ++ii;
+            ++j;
+        }
+        if (j >= tail) break;  // a malformed script: the update itself rejects it
+        if (!named[static_cast<size_t>(j)] &&
+            std::memcmp(&before[static_cast<size_t>(k)], &after[static_cast<size_t>(j)], sizeof(T)) != 0)
+            e.moved.push_back(static_cast<int>(j));
+        ++j;
+    }
+}
+
 py::dict topoDict(const GpuTopoUpdateTimings& t) {
     py::dict d;
     d["upload_ms"] = t.uploadMs;
@@ -395,8 +431,9 @@ public:
     py::dict updateTopology(const F32& tris, const py::object& deleted, const py::object& moved,
                             const py::object& inserted) {
         std::vector<Tri> t = triangles(tris);
-        const GpuTopoEdit e = topoEdit(deleted, moved, inserted, bvh.primCount,
-                                       static_cast<long long>(t.size()));
+        GpuTopoEdit e = topoEdit(deleted, moved, inserted, bvh.primCount,
+                                 static_cast<long long>(t.size()));
+        addChangedSurvivors(tris_, t, e);
         Scene view;
         view.tris = t;
         view.updateBounds();
@@ -482,8 +519,9 @@ public:
     py::dict updateTopology(const F32& points, const py::object& deleted, const py::object& moved,
                             const py::object& inserted) {
         std::vector<Vec3> p = points3(points, "points");
-        const GpuTopoEdit e = topoEdit(deleted, moved, inserted, bvh.primCount,
-                                       static_cast<long long>(p.size()));
+        GpuTopoEdit e = topoEdit(deleted, moved, inserted, bvh.primCount,
+                                 static_cast<long long>(p.size()));
+        addChangedSurvivors(cloud_.pts, p, e);
         PointCloud view;
         view.pts = std::move(p);
         view.updateBounds();
@@ -541,8 +579,9 @@ public:
                             const py::object& deleted, const py::object& moved,
                             const py::object& inserted) {
         std::vector<Gaussian> g = gaussians(means, rot, scale);
-        const GpuTopoEdit e = topoEdit(deleted, moved, inserted, bvh.primCount,
-                                       static_cast<long long>(g.size()));
+        GpuTopoEdit e = topoEdit(deleted, moved, inserted, bvh.primCount,
+                                 static_cast<long long>(g.size()));
+        addChangedSurvivors(cloud_.gaussians, g, e);
         GaussianCloud view;
         view.gaussians = std::move(g);
         view.updateBounds();

@@ -19,7 +19,8 @@ LIB_PATH = HERE / "libquarry_b200.so"
 
 QK_OK = 0
 QK_TRI, QK_POINT, QK_GAUSS = 0, 1, 2
-QK_BUILD_LBVH, QK_BUILD_SAH = 0, 1
+QK_BUILD_LBVH, QK_BUILD_SAH, QK_BUILD_SAH4 = 0, 1, 2
+BUILDERS = {"lbvh": QK_BUILD_LBVH, "sah": QK_BUILD_SAH, "sah4": QK_BUILD_SAH4}
 QK_ORDER_MORTON, QK_ORDER_DIRECTION, QK_WIDE, QK_ORDER_COHERENT = 1, 2, 4, 8
 QK_TUNE_DYNAMIC, QK_TUNE_HIGH_OCC, QK_TUNE_SPLIT, QK_TUNE_SHORT_STACK = 256, 512, 1024, 2048
 QK_TUNE_LEAF4 = 4096
@@ -41,7 +42,8 @@ class QkTree(ctypes.Structure):
     _fields_ = [("kind", ctypes.c_int32), ("n", ctypes.c_int32), ("depth", ctypes.c_int32),
                 ("wide_count", ctypes.c_int32), ("nodes", _P), ("items", _P), ("prim_ids", _P),
                 ("parent", _P), ("depth_arr", _P), ("bnodes", _P), ("leaves", _P),
-                ("slot_of", _P), ("flags", _P), ("wide", _P), ("wide_id", _P)]
+                ("slot_of", _P), ("flags", _P), ("wide", _P), ("wide_id", _P),
+                ("wide_leaf", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 class QkTreeSizes(ctypes.Structure):
@@ -90,6 +92,7 @@ EXPORTS = {
     "qk_refit": (_I, [ctypes.POINTER(QkTree), _P, _P, _SZ, _P]),
     "qk_refit_dirty": (_I, [ctypes.POINTER(QkTree), _P, _P, _I, _P, _SZ, _P]),
     "qk_wide_build": (_I, [ctypes.POINTER(QkTree), _P, _SZ, _P]),
+    "qk_wide_build_leaf4": (_I, [ctypes.POINTER(QkTree), _P, _SZ, _P]),
     "qk_update_workspace_bytes": (_SZ, [_I, _I, _I, _I]),
     "qk_update_topology": (_I, [ctypes.POINTER(QkTree), ctypes.POINTER(QkTree),
                                 ctypes.POINTER(QkTopoEdit), _I, _I, ctypes.POINTER(QkTopoInfo),
@@ -217,7 +220,7 @@ class DeviceTree:
     """One tree: device arrays allocated from torch, filled by qk_build.
 
     kind: "tri" | "point" | "gauss"; items: (n, stride) float32 in scene order (numpy or a
-    CUDA tensor).  builder: "lbvh" or "sah"."""
+    CUDA tensor).  builder: "lbvh", "sah" or "sah4" (leaf-size-4 SAH)."""
 
     def __init__(self, kind: str, items, builder: str = "lbvh", sah_bins: int = 32):
         torch = _torch()
@@ -230,7 +233,9 @@ class DeviceTree:
         self.n = n
         self.arrays, self.t = self._alloc(n)
         self.ws = Workspace()
-        self.builder = QK_BUILD_SAH if builder == "sah" else QK_BUILD_LBVH
+        if builder not in BUILDERS:
+            raise ValueError(f"builder must be one of {sorted(BUILDERS)}")
+        self.builder = BUILDERS[builder]
         self.sah_bins = sah_bins
         self.build()
         del torch, L
@@ -265,15 +270,18 @@ class DeviceTree:
     def depth(self) -> int:
         return self.t.depth
 
-    def build_wide(self) -> int:
+    def build_wide(self, leaf4: bool = False) -> int:
+        """4-wide nodes (qk_wide_build), or with leaf4 the leaf-size-4 form
+        (qk_wide_build_leaf4: subtrees of 2..4 primitives on contiguous slots are one leaf
+        slot).  Returns the node count."""
         ws, _ = self._build_ws()
+        fn = lib().qk_wide_build_leaf4 if leaf4 else lib().qk_wide_build
+        name = "qk_wide_build_leaf4" if leaf4 else "qk_wide_build"
         self.t.wide = None
-        check(lib().qk_wide_build(ctypes.byref(self.t), _ptr(ws), ws.numel(), _stream()),
-              "qk_wide_build (count)")
+        check(fn(ctypes.byref(self.t), _ptr(ws), ws.numel(), _stream()), name + " (count)")
         self.arrays["wide"] = _dev_bytes(self.t.wide_count * 128)
         self.t.wide = self.arrays["wide"].data_ptr()
-        check(lib().qk_wide_build(ctypes.byref(self.t), _ptr(ws), ws.numel(), _stream()),
-              "qk_wide_build")
+        check(fn(ctypes.byref(self.t), _ptr(ws), ws.numel(), _stream()), name)
         return self.t.wide_count
 
     def refit(self, items) -> None:

@@ -559,6 +559,102 @@ def test_leaf4_tiny_trees(cuda, n):
     assert cuda.equal(o1, o0) and cuda.equal(k1, k0)
 
 
+def _slot_ranges(nodes: np.ndarray, n: int, depth: np.ndarray):
+    """(first slot, leaf count) of every node's subtree, children before parents."""
+    first = np.zeros(2 * n - 1, np.int64)
+    count = np.zeros(2 * n - 1, np.int64)
+    first[n - 1:] = np.arange(n)
+    count[n - 1:] = 1
+    for p in sorted(range(n - 1), key=lambda i: -int(depth[i])):
+        l, r = nodes[p, 6], nodes[p, 7]
+        first[p] = min(first[l], first[r])
+        count[p] = count[l] + count[r]
+    return first, count
+
+
+@pytest.mark.parametrize("kind", ["tri", "point", "gauss"])
+def test_sah4_tree_and_wide_leaf4(cuda, kind):
+    """QK_BUILD_SAH4: the SAH decisions stop at ranges of at most 4 primitives, which are split
+    by count (left half first).  Every node above them is the binned SAH tree's own node, byte
+    for byte, and each range holds the SAH tree's primitives.  qk_wide_build_leaf4 then
+    collapses those ranges into single slots: bytes equal the oracle's collapse of the same
+    tree, fewer nodes than the plain collapse, every query result equal to the oracle's
+    (binary, leaf4, wide; input, Morton and coherent order), and the same after a refit, which
+    re-emits the form."""
+    items = _items(kind)
+    tree = capi.DeviceTree(kind, items, builder="sah4")
+    assert tree.validate() == [0] * 8
+    again = capi.DeviceTree(kind, items, builder="sah4")
+    assert again.nodes_bytes().tobytes() == tree.nodes_bytes().tobytes(), "not deterministic"
+    sah = capi.DeviceTree(kind, items, builder="sah")
+    n = tree.n
+    nodes4 = tree.nodes_bytes().view(np.int32).reshape(2 * n - 1, 8)
+    nodes1 = sah.nodes_bytes().view(np.int32).reshape(2 * n - 1, 8)
+    depth4 = tree.host("depth_arr", np.int32, 2 * n - 1)
+    first4, cnt4 = _slot_ranges(nodes4, n, depth4)
+    _, cnt1 = _slot_ranges(nodes1, n, sah.host("depth_arr", np.int32, 2 * n - 1))
+    big = np.nonzero(cnt4[: n - 1] > 4)[0]
+    assert np.array_equal(big, np.nonzero(cnt1[: n - 1] > 4)[0])
+    assert np.array_equal(nodes4[big], nodes1[big])
+    parent = tree.host("parent", np.int32, 2 * n - 1)
+    ids4, ids1 = tree.host("prim_ids", np.int32, n), sah.host("prim_ids", np.int32, n)
+    ranges = 0
+    for p in range(n - 1):
+        m = int(cnt4[p])
+        if m > 4:
+            continue
+        l, r = nodes4[p, 6], nodes4[p, 7]
+        assert cnt4[l] == m // 2 and cnt4[r] == m - m // 2, (p, m)
+        if p == 0 or cnt4[parent[p]] > 4:  # a whole leaf range
+            f = int(first4[p])
+            assert np.array_equal(np.sort(ids4[f:f + m]), np.sort(ids1[f:f + m])), p
+            ranges += 1
+    assert ranges > n // 8
+    assert _check_small_codes(tree) >= ranges
+
+    plain = tree.build_wide()
+    ref = oracle.LBVH(kind, items)
+    qh = _queries(items, kind, 3_001, 5)
+    q = _dev(qh)
+    want_c, want_k = ref.closest(qh), ref.knn(qh, 8)
+    r = 3.0 if kind != "gauss" else 1.0
+    want_off, want_keys = ref.radius(qh, r)
+    lo, hi = qh.min(0), qh.max(0)
+    rays_h = _random_rays(lo, hi, 20_001, 6) if kind == "tri" else None
+    want_r = ref.raycast(rays_h) if kind == "tri" else None
+
+    def same(t):
+        for flags in FLAG_SETS + [capi.QK_TUNE_LEAF4, capi.QK_TUNE_LEAF4 | capi.QK_ORDER_MORTON]:
+            assert np.array_equal(t.closest(q, flags).cpu().numpy().view(np.uint32), want_c), flags
+            assert np.array_equal(t.knn(q, 8, flags).cpu().numpy().view(np.uint32), want_k), flags
+            off, keys = t.radius(q, r, flags)
+            assert np.array_equal(off.cpu().numpy().astype(np.int64), want_off), flags
+            assert np.array_equal(keys.cpu().numpy().view(np.uint64), want_keys), flags
+            if rays_h is not None:
+                got = t.raycast(_dev(rays_h), flags).cpu().numpy().view(np.uint64)
+                assert np.array_equal(got, want_r), flags
+
+    same(tree)  # plain 4-wide form
+    count = tree.build_wide(leaf4=True)
+    assert tree.t.wide_leaf == 4
+    assert count < 0.6 * plain, (count, plain)
+    wide, wide_id = oracle.wide_collapse_leaf4(tree.nodes_bytes().view(oracle.NODE_DTYPE),
+                                               depth4, n)
+    assert count == len(wide) // 4
+    assert tree.arrays["wide"].cpu().numpy()[: count * 128].tobytes() == wide.tobytes()
+    assert tree.validate() == [0] * 8
+    same(tree)  # leaf-size-4 form
+    moved = items.copy()
+    moved[:, :3] += np.random.default_rng(3).normal(0, 0.05, (len(items), 3)).astype(np.float32)
+    tree.refit(moved)
+    assert tree.validate() == [0] * 8  # the wide nodes were re-emitted in the leaf4 form
+    ref.refit(moved)
+    want_c, want_k = ref.closest(qh), ref.knn(qh, 8)
+    want_off, want_keys = ref.radius(qh, r)
+    want_r = ref.raycast(rays_h) if kind == "tri" else None
+    same(tree)
+
+
 def test_split_knn_sphere_matches_oracle(cuda):
     pts = workloads.point_cloud("surface", 100_000, 2)
     q = workloads.uniform_points(2_000, pts.min(0), pts.max(0), 2, 13)

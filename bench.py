@@ -895,9 +895,11 @@ def points_arm(args, world, rank, local):
         lo, hi = pts.min(axis=0), pts.max(axis=0)
         q = w.uniform_points(nq, lo, hi, seed, 13)
         trees = {}
-        for bname, builder, bins in (("lbvh", "lbvh", 32), ("sah8", "sah", 8), ("sah32", "sah", 32)):
+        for bname, builder, bins in (("lbvh", "lbvh", 32), ("sah8", "sah", 8), ("sah32", "sah", 32),
+                                     ("sah4", "sah4", 32)):
             trees[bname] = capi.DeviceTree("point", pts, builder=builder, sah_bins=bins)
-            trees[bname].build_wide()
+            # the leaf-size-4 SAH tree carries the leaf-size-4 4-wide form
+            trees[bname].build_wide(leaf4=builder == "sah4")
         clouds[kind] = {"pts": pts, "q": q, "q_d": capi.to_device(q, np.float32),
                         "tree": trees["lbvh"], "trees": trees}
         if args.dump and rank == 0:

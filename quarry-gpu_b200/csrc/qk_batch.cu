@@ -443,15 +443,20 @@ struct QRay {
     __device__ __forceinline__ void run(const BScene& sc, int, int q, Stack& st, Trav& tv) const {
         const RayPre R = prepare_ray(__ldg(rays + 2 * q), __ldg(rays + 2 * q + 1));
         int best_id;
-        if (kWide)
-            out[q] = ray_wide_one(static_cast<const WideNode*>(sc.t.wide),
-                                  static_cast<const float4*>(sc.t.leaves), R, max_iter_of(sc.t),
-                                  st, tv, best_id);
-        else
-            out[q] = ray_bin_one(static_cast<const BNode*>(sc.t.bnodes),
-                                 static_cast<const float4*>(sc.t.leaves),
-                                 root_box(static_cast<const Node*>(sc.t.nodes)), R,
-                                 max_iter_of(sc.t), st, tv, best_id);
+        // clean rays (all but degenerate ones) take the slab tests without the containment
+        // branch (RayPre::clean)
+        const WideNode* wn = static_cast<const WideNode*>(sc.t.wide);
+        const BNode* bn = static_cast<const BNode*>(sc.t.bnodes);
+        const float4* lv = static_cast<const float4*>(sc.t.leaves);
+        if (kWide) {
+            out[q] = R.clean ? ray_wide_one<false, false>(wn, lv, R, max_iter_of(sc.t), st, tv, best_id)
+                             : ray_wide_one<false, true>(wn, lv, R, max_iter_of(sc.t), st, tv, best_id);
+        } else {
+            const Box rb = root_box(static_cast<const Node*>(sc.t.nodes));
+            out[q] = R.clean
+                         ? ray_bin_one<Stack, false, false>(bn, lv, rb, R, max_iter_of(sc.t), st, tv, best_id)
+                         : ray_bin_one<Stack, false, true>(bn, lv, rb, R, max_iter_of(sc.t), st, tv, best_id);
+        }
     }
 };
 

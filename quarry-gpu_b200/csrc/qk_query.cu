@@ -373,8 +373,14 @@ __global__ __launch_bounds__(kBlock, kMinBlocks) void k_ray_bin(const BNode* __r
             out[r] = ray_bin_one(bn, leaves, root_box(nodes), R, max_iter, st, tv, best_id);
         } else {
             LocalStack<kStack> st;
-            out[r] = ray_bin_one<LocalStack<kStack>, kLeaf4>(bn, leaves, root_box(nodes), R,
-                                                             max_iter, st, tv, best_id, lnodes);
+            // a clean ray (all but degenerate ones) runs the traversal whose slab tests have no
+            // containment branch and use min / max
+            if (!R.clean)
+                out[r] = ray_bin_one<LocalStack<kStack>, kLeaf4, true>(
+                    bn, leaves, root_box(nodes), R, max_iter, st, tv, best_id, lnodes);
+            else
+                out[r] = ray_bin_one<LocalStack<kStack>, kLeaf4, false>(
+                    bn, leaves, root_box(nodes), R, max_iter, st, tv, best_id, lnodes);
         }
         if (ids) ids[r] = best_id;
     }
@@ -518,7 +524,8 @@ __global__ __launch_bounds__(kBlock) void k_ray_wide(const WideNode* __restrict_
         const RayPre R = prepare_ray(__ldg(rays + 2 * r), __ldg(rays + 2 * r + 1));
         LocalStack<kStackWide> st;
         int best_id;
-        out[r] = ray_wide_one<kRange>(wn, leaves, R, max_iter, st, tv, best_id);
+        out[r] = R.clean ? ray_wide_one<kRange, false>(wn, leaves, R, max_iter, st, tv, best_id)
+                         : ray_wide_one<kRange, true>(wn, leaves, R, max_iter, st, tv, best_id);
         if (ids) ids[r] = best_id;
     }
     flush_stats<kStats>(active, tv.nodes, tv.leaves, tv.overflow, stats);

@@ -153,6 +153,41 @@ def test_raycast_parity(cuda, name):
             assert np.array_equal(got, want), f"flags={flags}: {(got != want).sum()} rays differ"
 
 
+def test_degenerate_rays_every_ray_path(cuda):
+    """Clean rays (no axis-parallel direction component, tmin / tmax not NaN) take the
+    traversal whose slab tests drop the containment branch and use min / max; the others
+    (components of |d| < 1e-20, zero directions, NaN tmin or tmax) keep the general one.
+    A mix of both, with infinite tmax, negative tmin and origins inside the scene, through
+    every binary and 4-wide ray schedule and order, gives the oracle's bits."""
+    tris = scenes()["city"]
+    lo, hi = workloads.bounds_of(tris)
+    rays = _random_rays(lo, hi, 20_000, 31)
+    rng = np.random.default_rng(8)
+    rays[0::7, 3] = 0.0                   # parallel to x
+    rays[1::7, 4] = 0.0                   # parallel to y
+    rays[2::7, 3:5] = 0.0                 # vertical
+    rays[3::7, 5] = 1e-21                 # a tiny component counts as parallel
+    rays[4::7, 3:6] = 0.0                 # no direction at all
+    rays[5::11, 6] = np.nan               # NaN tmin
+    rays[6::11, 7] = np.nan               # NaN tmax
+    rays[7::11, 7] = np.inf               # unbounded
+    rays[8::11, 6] = -5.0                 # negative tmin
+    inside = np.arange(9, len(rays), 13)
+    rays[inside, :3] = (lo + (hi - lo) * rng.random((len(inside), 3))).astype(np.float32)
+    want = oracle.LBVH("tri", tris).raycast(rays)
+    assert np.count_nonzero(want >> 32) > 1_000
+    d_rays = _dev(rays)
+    for builder in ("lbvh", "sah"):
+        tree = capi.DeviceTree("tri", tris, builder=builder)
+        tree.build_wide()
+        occ, coh = capi.QK_TUNE_HIGH_OCC, capi.QK_ORDER_COHERENT
+        for flags in (0, occ, coh | occ, capi.QK_ORDER_MORTON, capi.QK_TUNE_DYNAMIC,
+                      capi.QK_TUNE_SHORT_STACK, occ | capi.QK_TUNE_LEAF4, capi.QK_WIDE,
+                      capi.QK_WIDE | coh):
+            got = tree.raycast(d_rays, flags).cpu().numpy().view(np.uint64)
+            assert np.array_equal(got, want), (builder, flags, int((got != want).sum()))
+
+
 def test_raycast_stats_and_no_overflow(cuda):
     tris = scenes()["terrain"]
     tree = capi.DeviceTree("tri", tris)

@@ -443,19 +443,22 @@ struct QRay {
     __device__ __forceinline__ void run(const BScene& sc, int, int q, Stack& st, Trav& tv) const {
         const RayPre R = prepare_ray(__ldg(rays + 2 * q), __ldg(rays + 2 * q + 1));
         int best_id;
-        // clean rays (all but degenerate ones) take the slab tests without the containment
-        // branch (RayPre::clean)
+        // rays with no parallel axis and vertical rays take traversals compiled for their
+        // RayPre::mode; others the general one
         const WideNode* wn = static_cast<const WideNode*>(sc.t.wide);
         const BNode* bn = static_cast<const BNode*>(sc.t.bnodes);
         const float4* lv = static_cast<const float4*>(sc.t.leaves);
         if (kWide) {
-            out[q] = R.clean ? ray_wide_one<false, false>(wn, lv, R, max_iter_of(sc.t), st, tv, best_id)
-                             : ray_wide_one<false, true>(wn, lv, R, max_iter_of(sc.t), st, tv, best_id);
+            out[q] = R.mode == 0 ? ray_wide_one<false, 0>(wn, lv, R, max_iter_of(sc.t), st, tv, best_id)
+                   : R.mode == 3 ? ray_wide_one<false, 3>(wn, lv, R, max_iter_of(sc.t), st, tv, best_id)
+                                 : ray_wide_one<false, -1>(wn, lv, R, max_iter_of(sc.t), st, tv, best_id);
         } else {
             const Box rb = root_box(static_cast<const Node*>(sc.t.nodes));
-            out[q] = R.clean
-                         ? ray_bin_one<Stack, false, false>(bn, lv, rb, R, max_iter_of(sc.t), st, tv, best_id)
-                         : ray_bin_one<Stack, false, true>(bn, lv, rb, R, max_iter_of(sc.t), st, tv, best_id);
+            out[q] = R.mode == 0
+                         ? ray_bin_one<Stack, false, 0>(bn, lv, rb, R, max_iter_of(sc.t), st, tv, best_id)
+                     : R.mode == 3
+                         ? ray_bin_one<Stack, false, 3>(bn, lv, rb, R, max_iter_of(sc.t), st, tv, best_id)
+                         : ray_bin_one<Stack, false, -1>(bn, lv, rb, R, max_iter_of(sc.t), st, tv, best_id);
         }
     }
 };

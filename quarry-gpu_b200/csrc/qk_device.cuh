@@ -93,7 +93,7 @@ struct RayPre {
     float3 o, d, inv;
     float tmin, tmax;
     bool px, py, pz;
-    bool clean;  // no parallel axis, tmin / tmax not NaN
+    int mode;  // tmin / tmax not NaN: the parallel-axis mask px | py << 1 | pz << 2; else -1
 };
 
 __device__ __forceinline__ RayPre prepare_ray(float4 r0, float4 r1) {
@@ -106,19 +106,24 @@ __device__ __forceinline__ RayPre prepare_ray(float4 r0, float4 r1) {
     r.py = fabsf(r.d.y) < 1e-20f;
     r.pz = fabsf(r.d.z) < 1e-20f;
     r.inv = f3(r.px ? 0.0f : 1.0f / r.d.x, r.py ? 0.0f : 1.0f / r.d.y, r.pz ? 0.0f : 1.0f / r.d.z);
-    r.clean = !(r.px || r.py || r.pz) && r.tmin == r.tmin && r.tmax == r.tmax;
+    r.mode = (r.tmin == r.tmin && r.tmax == r.tmax)
+                 ? (static_cast<int>(r.px) | static_cast<int>(r.py) << 1 | static_cast<int>(r.pz) << 2)
+                 : -1;
     return r;
 }
 
-// kPar false: the ray is clean (RayPre::clean: no parallel axis, tmin and tmax not NaN), so
-// the containment branch is compiled out, and t0 / t1, which start at tmin / bound, are never
-// NaN.  Then `x > t0 ? x : t0` is fmaxf(t0, x) and `x < t1 ? x : t1` is fminf(t1, x) for
-// every x, NaN included (both keep t0 / t1); a zero's sign may differ, which no later
-// comparison sees.  The swap keeps its compare: with a NaN slab end it must not reorder.
-template <bool kPar = true>
+// kMode: -1 for any ray (the reference's branch on `par`), else the ray's RayPre::mode known
+// at compile time: tmin / tmax are not NaN and bit kAxis says whether this axis is parallel.
+// Then the branch is compiled out, and t0 / t1, which start at tmin / bound, are never NaN, so
+// `x > t0 ? x : t0` is fmaxf(t0, x) and `x < t1 ? x : t1` is fminf(t1, x) for every x, NaN
+// included (both keep t0 / t1); a zero's sign may differ, which no later comparison sees.
+// The swap keeps its compare: with a NaN slab end it must not reorder.
+template <int kMode = -1, int kAxis = 0>
 __device__ __forceinline__ void slab_axis(bool par, float o, float inv, float lo, float hi,
                                           float& t0, float& t1, bool& ok) {
-    if (!kPar) {
+    if (kMode >= 0 && ((kMode >> kAxis) & 1)) {
+        ok = ok && !(o < lo || o > hi);
+    } else if (kMode >= 0) {
         const float ta = (lo - o) * inv;
         const float tb = (hi - o) * inv;
         const bool sw = ta > tb;
@@ -142,32 +147,32 @@ __device__ __forceinline__ void slab_axis(bool par, float o, float inv, float lo
 // intersectAABB (geometry.h:282-316) with t1 seeded by bound = tMax*(1+1e-6)+1e-6.  The
 // reference's per-axis early exit tests a condition that can only get worse on later axes
 // (t0 grows, t1 shrinks), so one test after all three axes gives the same answer.
-template <bool kPar = true>
+template <int kMode = -1>
 __device__ __forceinline__ bool ray_box(const RayPre& r, float3 lo, float3 hi, float bound,
                                         float& tenter) {
     float t0 = r.tmin, t1 = bound;
     bool ok = true;
-    slab_axis<kPar>(r.px, r.o.x, r.inv.x, lo.x, hi.x, t0, t1, ok);
-    slab_axis<kPar>(r.py, r.o.y, r.inv.y, lo.y, hi.y, t0, t1, ok);
-    slab_axis<kPar>(r.pz, r.o.z, r.inv.z, lo.z, hi.z, t0, t1, ok);
+    slab_axis<kMode, 0>(r.px, r.o.x, r.inv.x, lo.x, hi.x, t0, t1, ok);
+    slab_axis<kMode, 1>(r.py, r.o.y, r.inv.y, lo.y, hi.y, t0, t1, ok);
+    slab_axis<kMode, 2>(r.pz, r.o.z, r.inv.z, lo.z, hi.z, t0, t1, ok);
     tenter = t0;
     return ok && !(t0 > t1 * kMarginMul + kMarginAdd);
 }
 
 // hitParamInsideBox (geometry.h:112-143)
-template <bool kPar = true>
+template <int kMode = -1>
 __device__ __forceinline__ bool hit_inside_box(const RayPre& r, float3 lo, float3 hi, float t) {
     float t0 = r.tmin, t1 = kInf;
     bool ok = true;
-    slab_axis<kPar>(r.px, r.o.x, r.inv.x, lo.x, hi.x, t0, t1, ok);
-    slab_axis<kPar>(r.py, r.o.y, r.inv.y, lo.y, hi.y, t0, t1, ok);
-    slab_axis<kPar>(r.pz, r.o.z, r.inv.z, lo.z, hi.z, t0, t1, ok);
+    slab_axis<kMode, 0>(r.px, r.o.x, r.inv.x, lo.x, hi.x, t0, t1, ok);
+    slab_axis<kMode, 1>(r.py, r.o.y, r.inv.y, lo.y, hi.y, t0, t1, ok);
+    slab_axis<kMode, 2>(r.pz, r.o.z, r.inv.z, lo.z, hi.z, t0, t1, ok);
     if (!ok || t0 > t1) return false;
     return t >= t0 * (1.0f - 1e-6f) - 1e-6f && t <= t1 * (1.0f + 1e-6f) + 1e-6f;
 }
 
 // Moller-Trumbore with the self-box guard (geometry.h:146-176); tMax is the ray's own.
-template <bool kPar = true>
+template <int kMode = -1>
 __device__ __forceinline__ bool ray_tri(const RayPre& r, float3 a, float3 b, float3 c, float& tout) {
     const float3 e1 = sub3(b, a);
     const float3 e2 = sub3(c, a);
@@ -188,7 +193,7 @@ __device__ __forceinline__ bool ray_tri(const RayPre& r, float3 a, float3 b, flo
                          ext_min(ext_min(a.z, b.z), c.z));
     const float3 hi = f3(ext_max(ext_max(a.x, b.x), c.x), ext_max(ext_max(a.y, b.y), c.y),
                          ext_max(ext_max(a.z, b.z), c.z));
-    if (!hit_inside_box<kPar>(r, lo, hi, t)) return false;
+    if (!hit_inside_box<kMode>(r, lo, hi, t)) return false;
     tout = t;
     return true;
 }

@@ -373,14 +373,18 @@ __global__ __launch_bounds__(kBlock, kMinBlocks) void k_ray_bin(const BNode* __r
             out[r] = ray_bin_one(bn, leaves, root_box(nodes), R, max_iter, st, tv, best_id);
         } else {
             LocalStack<kStack> st;
-            // a clean ray (all but degenerate ones) runs the traversal whose slab tests have no
-            // containment branch and use min / max
-            if (!R.clean)
-                out[r] = ray_bin_one<LocalStack<kStack>, kLeaf4, true>(
-                    bn, leaves, root_box(nodes), R, max_iter, st, tv, best_id, lnodes);
+            // rays with no parallel axis and vertical rays (x and y parallel), tmin / tmax not
+            // NaN, run traversals compiled for their mode (RayPre::mode); others the general one
+            const Box rb = root_box(nodes);
+            if (R.mode == 0)
+                out[r] = ray_bin_one<LocalStack<kStack>, kLeaf4, 0>(bn, leaves, rb, R, max_iter,
+                                                                    st, tv, best_id, lnodes);
+            else if (R.mode == 3)
+                out[r] = ray_bin_one<LocalStack<kStack>, kLeaf4, 3>(bn, leaves, rb, R, max_iter,
+                                                                    st, tv, best_id, lnodes);
             else
-                out[r] = ray_bin_one<LocalStack<kStack>, kLeaf4, false>(
-                    bn, leaves, root_box(nodes), R, max_iter, st, tv, best_id, lnodes);
+                out[r] = ray_bin_one<LocalStack<kStack>, kLeaf4, -1>(bn, leaves, rb, R, max_iter,
+                                                                     st, tv, best_id, lnodes);
         }
         if (ids) ids[r] = best_id;
     }
@@ -524,8 +528,9 @@ __global__ __launch_bounds__(kBlock) void k_ray_wide(const WideNode* __restrict_
         const RayPre R = prepare_ray(__ldg(rays + 2 * r), __ldg(rays + 2 * r + 1));
         LocalStack<kStackWide> st;
         int best_id;
-        out[r] = R.clean ? ray_wide_one<kRange, false>(wn, leaves, R, max_iter, st, tv, best_id)
-                         : ray_wide_one<kRange, true>(wn, leaves, R, max_iter, st, tv, best_id);
+        out[r] = R.mode == 0 ? ray_wide_one<kRange, 0>(wn, leaves, R, max_iter, st, tv, best_id)
+               : R.mode == 3 ? ray_wide_one<kRange, 3>(wn, leaves, R, max_iter, st, tv, best_id)
+                             : ray_wide_one<kRange, -1>(wn, leaves, R, max_iter, st, tv, best_id);
         if (ids) ids[r] = best_id;
     }
     flush_stats<kStats>(active, tv.nodes, tv.leaves, tv.overflow, stats);

@@ -154,14 +154,14 @@ __device__ __forceinline__ void flush_stats(bool active, int nodes, int leaves, 
 // Leaf test.  The first hit is taken even at t == tMax (the CPU reference accepts t <= tMax,
 // src/cpu/bvh.cpp:156-168); later hits only when closer.  Among hits at the same t the
 // smallest scene index is kept, so the reported primitive does not depend on visit order.
-template <bool kPar = true>
+template <int kMode = -1>
 __device__ __forceinline__ void test_tri(const RayPre& R, const float4* __restrict__ leaves,
                                          int slot, float& best, float& bound, bool& any,
                                          int& best_id) {
     const float4 a = __ldg(leaves + 3 * slot), b = __ldg(leaves + 3 * slot + 1),
                  c = __ldg(leaves + 3 * slot + 2);
     float t;
-    if (ray_tri<kPar>(R, f3(a.x, a.y, a.z), f3(b.x, b.y, b.z), f3(c.x, c.y, c.z), t)) {
+    if (ray_tri<kMode>(R, f3(a.x, a.y, a.z), f3(b.x, b.y, b.z), f3(c.x, c.y, c.z), t)) {
         const int id = __float_as_int(a.w);
         if (!any || t < best || (t == best && id < best_id)) {
             best = t;
@@ -178,9 +178,9 @@ __device__ __forceinline__ unsigned long long pack_hit(bool any, float best) {
 
 // First hit in a binary tree: near child followed, far child pushed with its entry bound,
 // which is re-checked against the current best when popped (src/cpu/bvh.cpp:147-152).
-// kPar false: the ray is clean (RayPre::clean), so every slab test skips the containment
-// branch and uses min / max.
-template <class St, bool kLeaf4 = false, bool kPar = true>
+// kMode >= 0: the ray's RayPre::mode, known at compile time (the slab tests drop their
+// branch on parallel axes and use min / max); -1 for any ray.
+template <class St, bool kLeaf4 = false, int kMode = -1>
 __device__ __forceinline__ unsigned long long ray_bin_one(const BNode* __restrict__ bn,
                                                           const float4* __restrict__ leaves,
                                                           const Box& rb, const RayPre& R,
@@ -192,7 +192,7 @@ __device__ __forceinline__ unsigned long long ray_bin_one(const BNode* __restric
     bool any = false;
     best_id = -1;
     float te;
-    if (!ray_box<kPar>(R, rb.lo, rb.hi, bound, te)) return 0ull;
+    if (!ray_box<kMode>(R, rb.lo, rb.hi, bound, te)) return 0ull;
     ++tv.nodes;
     int sp = 0;
     int node = 0;
@@ -206,17 +206,17 @@ __device__ __forceinline__ unsigned long long ray_bin_one(const BNode* __restric
         if constexpr (kLeaf4) load_bnode_small(bn, node, llo, lhi, rlo, rhi, lref, rref, lsm, rsm);
         else load_bnode(bn, node, llo, lhi, rlo, rhi, lref, rref);
         float tl, tr;
-        bool hl = ray_box<kPar>(R, llo, lhi, bound, tl);
-        bool hr = ray_box<kPar>(R, rlo, rhi, bound, tr);
+        bool hl = ray_box<kMode>(R, llo, lhi, bound, tl);
+        bool hr = ray_box<kMode>(R, rlo, rhi, bound, tr);
         tv.nodes += static_cast<int>(hl) + static_cast<int>(hr);
         if (hl && lref < 0) {
             ++tv.leaves;
-            test_tri<kPar>(R, leaves, ~lref, best, bound, any, best_id);
+            test_tri<kMode>(R, leaves, ~lref, best, bound, any, best_id);
             hl = false;
         }
         if (hr && rref < 0) {
             ++tv.leaves;
-            test_tri<kPar>(R, leaves, ~rref, best, bound, any, best_id);
+            test_tri<kMode>(R, leaves, ~rref, best, bound, any, best_id);
             hr = false;
         }
         if constexpr (kLeaf4) {
@@ -236,9 +236,9 @@ __device__ __forceinline__ unsigned long long ray_bin_one(const BNode* __restric
                             // the leaf's own box first, as a descent would test it
                             const Box lb = leaf_box(lnodes, first + j);
                             float tb;
-                            if (!ray_box<kPar>(R, lb.lo, lb.hi, bound, tb)) continue;
+                            if (!ray_box<kMode>(R, lb.lo, lb.hi, bound, tb)) continue;
                             ++tv.leaves;
-                            test_tri<kPar>(R, leaves, first + j, best, bound, any, best_id);
+                            test_tri<kMode>(R, leaves, first + j, best, bound, any, best_id);
                         }
                     }
                 }
@@ -278,7 +278,7 @@ __device__ __forceinline__ unsigned long long ray_bin_one(const BNode* __restric
 
 // First hit in a 4-wide tree: hit slots sorted by entry t, leaves tested nearest first,
 // the nearest internal child followed and the others pushed far-first.
-template <bool kRange = false, bool kPar = true, class St>
+template <bool kRange = false, int kMode = -1, class St>
 __device__ __forceinline__ unsigned long long ray_wide_one(const WideNode* __restrict__ wn,
                                                            const float4* __restrict__ leaves,
                                                            const RayPre& R, int max_iter, St& st,
@@ -303,7 +303,7 @@ __device__ __forceinline__ unsigned long long ray_wide_one(const WideNode* __res
             int c, nc;
             load_wide_entry(wn, node, s, lo, hi, c, nc);
             float t;
-            if (c != kEmptySlot && ray_box<kPar>(R, lo, hi, bound, t)) {
+            if (c != kEmptySlot && ray_box<kMode>(R, lo, hi, bound, t)) {
                 ++tv.nodes;
                 int j = hits++;
                 while (j > 0 && key[j - 1] > t) {
@@ -324,7 +324,7 @@ __device__ __forceinline__ unsigned long long ray_wide_one(const WideNode* __res
                 const int nq = kRange ? cnt[j] : 1;
                 for (int q = 0; q < nq; ++q) {
                     ++tv.leaves;
-                    test_tri<kPar>(R, leaves, ~child[j] + q, best, bound, any, best_id);
+                    test_tri<kMode>(R, leaves, ~child[j] + q, best, bound, any, best_id);
                 }
             }
         }

@@ -154,11 +154,12 @@ def test_raycast_parity(cuda, name):
 
 
 def test_degenerate_rays_every_ray_path(cuda):
-    """Clean rays (no axis-parallel direction component, tmin / tmax not NaN) take the
-    traversal whose slab tests drop the containment branch and use min / max; the others
-    (components of |d| < 1e-20, zero directions, NaN tmin or tmax) keep the general one.
-    A mix of both, with infinite tmax, negative tmin and origins inside the scene, through
-    every binary and 4-wide ray schedule and order, gives the oracle's bits."""
+    """Rays with tmin / tmax not NaN and no parallel axis, or only x and y parallel
+    (vertical), take traversals compiled for that case (no branch on parallel axes, min / max
+    slab updates); the others (one parallel axis of x / y, |d| < 1e-20 components, zero
+    directions, NaN tmin or tmax) keep the general one.  A mix of all, with infinite tmax,
+    negative tmin and origins inside the scene, through every binary and 4-wide ray schedule
+    and order, gives the oracle's bits."""
     tris = scenes()["city"]
     lo, hi = workloads.bounds_of(tris)
     rays = _random_rays(lo, hi, 20_000, 31)

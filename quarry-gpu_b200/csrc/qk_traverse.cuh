@@ -24,18 +24,21 @@ struct Trav {
     bool overflow = false;
 };
 
+// Per-thread stack in local memory: entry i is the pair (node, key bits), so a push is one
+// 8-byte store and get() one 8-byte load.
 template <int kCap>
 struct LocalStack {
     static constexpr int kSize = kCap;
-    int node[kCap];
-    float key[kCap];
-    __device__ __forceinline__ void put(int i, int n, float k) {
-        node[i] = n;
-        key[i] = k;
+    int2 e[kCap];
+    __device__ __forceinline__ void put(int i, int n, float k) { e[i] = make_int2(n, __float_as_int(k)); }
+    __device__ __forceinline__ void put_node(int i, int n) { e[i].x = n; }
+    __device__ __forceinline__ int get_node(int i) const { return e[i].x; }
+    __device__ __forceinline__ float get_key(int i) const { return __int_as_float(e[i].y); }
+    __device__ __forceinline__ void get(int i, int& n, float& k) const {
+        const int2 v = e[i];
+        n = v.x;
+        k = __int_as_float(v.y);
     }
-    __device__ __forceinline__ void put_node(int i, int n) { node[i] = n; }
-    __device__ __forceinline__ int get_node(int i) const { return node[i]; }
-    __device__ __forceinline__ float get_key(int i) const { return key[i]; }
 };
 
 template <int kCap>
@@ -62,6 +65,10 @@ struct SplitStack {
     }
     __device__ __forceinline__ int get_node(int i) const { return i < sh ? snode[i * stride] : node[i]; }
     __device__ __forceinline__ float get_key(int i) const { return i < sh ? skey[i * stride] : key[i]; }
+    __device__ __forceinline__ void get(int i, int& n, float& k) const {
+        n = get_node(i);
+        k = get_key(i);
+    }
 };
 
 // ---------------------------------------------------------------------------------------
@@ -265,8 +272,11 @@ __device__ __forceinline__ unsigned long long ray_bin_one(const BNode* __restric
             node = -1;
             while (sp > 0) {
                 --sp;
-                if (!(st.get_key(sp) > limit)) {
-                    node = st.get_node(sp);
+                int pn;
+                float pk;
+                st.get(sp, pn, pk);
+                if (!(pk > limit)) {
+                    node = pn;
                     break;
                 }
             }
@@ -350,8 +360,11 @@ __device__ __forceinline__ unsigned long long ray_wide_one(const WideNode* __res
         node = -1;
         while (sp > 0) {
             --sp;
-            if (!(st.get_key(sp) > limit)) {
-                node = st.get_node(sp);
+            int pn;
+            float pk;
+            st.get(sp, pn, pk);
+            if (!(pk > limit)) {
+                node = pn;
                 break;
             }
         }
@@ -451,8 +464,11 @@ __device__ __forceinline__ uint2 closest_bin_one(const BNode* __restrict__ bn,
             node = -1;
             while (sp > 0) {
                 --sp;
-                if (best_id < 0 || st.get_key(sp) <= best) {
-                    node = st.get_node(sp);
+                int pn;
+                float pk;
+                st.get(sp, pn, pk);
+                if (best_id < 0 || pk <= best) {
+                    node = pn;
                     break;
                 }
             }
@@ -531,8 +547,11 @@ __device__ __forceinline__ uint2 closest_wide_one(const WideNode* __restrict__ w
         node = -1;
         while (sp > 0) {
             --sp;
-            if (best_id < 0 || st.get_key(sp) <= best) {
-                node = st.get_node(sp);
+            int pn;
+            float pk;
+            st.get(sp, pn, pk);
+            if (best_id < 0 || pk <= best) {
+                node = pn;
                 break;
             }
         }
@@ -680,8 +699,11 @@ __device__ __forceinline__ void knn_bin_one(const BNode* __restrict__ bn,
             node = -1;
             while (sp > 0) {
                 --sp;
-                if (tab.admits(st.get_key(sp))) {
-                    node = st.get_node(sp);
+                int pn;
+                float pk;
+                st.get(sp, pn, pk);
+                if (tab.admits(pk)) {
+                    node = pn;
                     break;
                 }
             }
@@ -757,8 +779,11 @@ __device__ __forceinline__ void knn_wide_one(const WideNode* __restrict__ wn,
         node = -1;
         while (sp > 0) {
             --sp;
-            if (tab.admits(st.get_key(sp))) {
-                node = st.get_node(sp);
+            int pn;
+            float pk;
+            st.get(sp, pn, pk);
+            if (tab.admits(pk)) {
+                node = pn;
                 break;
             }
         }
@@ -1157,8 +1182,11 @@ __device__ __forceinline__ uint2 closest_split_one(const BNode* __restrict__ bn,
                     node = -1;
                     while (sp > 0) {
                         --sp;
-                        if (st.get_key(sp) <= best) {
-                            node = st.get_node(sp);
+                        int pn;
+                        float pk;
+                        st.get(sp, pn, pk);
+                        if (pk <= best) {
+                            node = pn;
                             break;
                         }
                     }
@@ -1280,8 +1308,11 @@ __device__ __forceinline__ void knn_split_one(const BNode* __restrict__ bn,
                     node = -1;
                     while (sp > 0) {
                         --sp;
-                        if (tab.admits(st.get_key(sp))) {
-                            node = st.get_node(sp);
+                        int pn;
+                        float pk;
+                        st.get(sp, pn, pk);
+                        if (tab.admits(pk)) {
+                            node = pn;
                             break;
                         }
                     }

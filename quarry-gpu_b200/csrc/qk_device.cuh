@@ -202,14 +202,21 @@ __device__ __forceinline__ bool ray_tri(const RayPre& r, float3 a, float3 b, flo
 // point queries
 // ---------------------------------------------------------------------------------------
 // distanceSquaredToAABB (geometry.h:262-277)
+// Branch-free, with the reference's values: per axis the gap is lo - p below the box, p - hi
+// above it, else 0 (max(max(lo - p, p - hi), 0): below the box p - hi < 0 < lo - p, above it
+// the reverse, inside both <= 0; a NaN end or coordinate leaves the other operand, as the
+// reference's comparisons do), and adding the square of a zero gap to the running sum (never
+// negative) changes nothing, so skipping it and adding it give the same bits.
+__device__ __forceinline__ float dist2_axis(float p, float lo, float hi) {
+    const float d = fmaxf(fmaxf(lo - p, p - hi), 0.0f);
+    return d * d;
+}
+
 __device__ __forceinline__ float dist2_box(float3 p, float3 lo, float3 hi) {
     float d2 = 0.0f;
-    if (p.x < lo.x) { const float d = lo.x - p.x; d2 += d * d; }
-    else if (p.x > hi.x) { const float d = p.x - hi.x; d2 += d * d; }
-    if (p.y < lo.y) { const float d = lo.y - p.y; d2 += d * d; }
-    else if (p.y > hi.y) { const float d = p.y - hi.y; d2 += d * d; }
-    if (p.z < lo.z) { const float d = lo.z - p.z; d2 += d * d; }
-    else if (p.z > hi.z) { const float d = p.z - hi.z; d2 += d * d; }
+    d2 += dist2_axis(p.x, lo.x, hi.x);
+    d2 += dist2_axis(p.y, lo.y, hi.y);
+    d2 += dist2_axis(p.z, lo.z, hi.z);
     return d2;
 }
 

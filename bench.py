@@ -543,6 +543,10 @@ def rays_arm(args, world, rank, local, workload):
                       ("split", capi.QK_TUNE_SPLIT),
                       ("split_morton", capi.QK_TUNE_SPLIT | capi.QK_ORDER_MORTON),
                       ("split_coherent", capi.QK_TUNE_SPLIT | capi.QK_ORDER_COHERENT),
+                      ("split8", capi.QK_TUNE_SPLIT8),
+                      ("split8_coherent", capi.QK_TUNE_SPLIT8 | capi.QK_ORDER_COHERENT),
+                      ("split4", capi.QK_TUNE_SPLIT4),
+                      ("split4_coherent", capi.QK_TUNE_SPLIT4 | capi.QK_ORDER_COHERENT),
                       ("leaf4", capi.QK_TUNE_LEAF4),
                       ("leaf4_morton", capi.QK_TUNE_LEAF4 | capi.QK_ORDER_MORTON)):
         for _ in range(3):
@@ -950,6 +954,8 @@ def points_arm(args, world, rank, local):
                 "split": capi.QK_TUNE_SPLIT, "split_morton": capi.QK_TUNE_SPLIT | capi.QK_ORDER_MORTON,
                 "leaf4": capi.QK_TUNE_LEAF4, "leaf4_morton": capi.QK_TUNE_LEAF4 | capi.QK_ORDER_MORTON,
                 "bin_coh": capi.QK_ORDER_COHERENT, "split_coh": capi.QK_TUNE_SPLIT | capi.QK_ORDER_COHERENT,
+                "split8": capi.QK_TUNE_SPLIT8, "split8_coh": capi.QK_TUNE_SPLIT8 | capi.QK_ORDER_COHERENT,
+                "split4": capi.QK_TUNE_SPLIT4, "split4_coh": capi.QK_TUNE_SPLIT4 | capi.QK_ORDER_COHERENT,
                 "leaf4_coh": capi.QK_TUNE_LEAF4 | capi.QK_ORDER_COHERENT}
     # the heavy-query tail (closest / kNN): shell queries near the centre go to the shared scan
     tail = capi.QK_TUNE_TAIL

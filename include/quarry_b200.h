@@ -79,6 +79,10 @@ extern "C" {
                                     radius plan takes it as a plan flag) */
 #define QK_TUNE_SPLIT 1024u      /* closest / kNN / radius on binary nodes: one warp per query,
                                     lanes on disjoint subtrees sharing the pruning bound */
+#define QK_TUNE_SPLIT8 32768u    /* the same with 8 lanes per query (few queries fill more of the
+                                    GPU); kNN takes at least the next group size >= k (k > 8:
+                                    a warp) */
+#define QK_TUNE_SPLIT4 65536u    /* the same with 4 lanes per query (kNN: at least k lanes) */
 #define QK_TUNE_TAIL 16384u      /* closest / kNN on point clouds, binary nodes (thread or warp
                                     per query): a query still traversing after a step budget is
                                     answered by a brute-force scan over all points that every

@@ -748,9 +748,21 @@ __global__ __launch_bounds__(kBlock) void k_radius_wide(
 }
 
 // ---------------------------------------------------------------------------------------
-// split mode (QK_TUNE_SPLIT): one warp per query (bodies in qk_traverse.cuh)
+// split mode (QK_TUNE_SPLIT: one warp per query; QK_TUNE_SPLIT8 / 4: groups of 8 / 4 lanes;
+// bodies in qk_traverse.cuh)
 // ---------------------------------------------------------------------------------------
-template <class Ops, bool kStats>
+// G lanes per query (32: a warp); a group past the last query traces query 0, writes nothing
+template <int G>
+__device__ __forceinline__ int split_query(int count, const uint32_t* order, bool& valid,
+                                           int& lane) {
+    const long long t = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int w = static_cast<int>(t / G);
+    lane = static_cast<int>(threadIdx.x & (G - 1));
+    valid = w < count;
+    return valid ? (order ? static_cast<int>(order[w]) : w) : 0;
+}
+
+template <class Ops, bool kStats, int G>
 __global__ __launch_bounds__(kBlock) void k_closest_split(const BNode* __restrict__ bn,
                                                          const float4* __restrict__ leaves,
                                                          const float* __restrict__ pts,
@@ -759,19 +771,21 @@ __global__ __launch_bounds__(kBlock) void k_closest_split(const BNode* __restric
                                                          int max_iter,
                                                          unsigned long long* __restrict__ stats,
                                                          TailList tail = TailList{}) {
-    const int w = (blockIdx.x * kBlock + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (w >= count) return;  // whole warps
-    const int q = order ? static_cast<int>(order[w]) : w;
+    if (G == 32 && static_cast<long long>(blockIdx.x * kBlock + threadIdx.x) / 32 >= count)
+        return;  // whole warps
+    bool valid;
+    int lane;
+    const int q = split_query<G>(count, order, valid, lane);
     const float3 p = f3(pts[3 * q], pts[3 * q + 1], pts[3 * q + 2]);
     Trav tv;
-    const uint2 r = closest_split_one<Ops>(bn, leaves, p, lane, max_iter, tv);
-    if (lane == 0) out[q] = r;
-    if (tail.count && __any_sync(0xffffffffu, tv.overflow) && lane == 0) tail_append(tail, q);
-    flush_stats<kStats>(true, tv.nodes, tv.leaves, tv.overflow, stats);
+    const uint2 r = closest_split_one<Ops, G>(bn, leaves, p, lane, max_iter, tv, valid);
+    if (valid && lane == 0) out[q] = r;
+    const bool ovf = group_any<G>(tv.overflow);
+    if (tail.count && valid && ovf && lane == 0) tail_append(tail, q);
+    flush_stats<kStats>(valid, tv.nodes, tv.leaves, tv.overflow, stats);
 }
 
-template <class Ops, int K, bool kStats>
+template <class Ops, bool kStats, int G>
 __global__ __launch_bounds__(kBlock) void k_knn_split(const BNode* __restrict__ bn,
                                                      const float4* __restrict__ leaves,
                                                      const float* __restrict__ pts,
@@ -780,17 +794,19 @@ __global__ __launch_bounds__(kBlock) void k_knn_split(const BNode* __restrict__ 
                                                      uint2* __restrict__ out, int max_iter,
                                                      unsigned long long* __restrict__ stats,
                                                      TailList tail = TailList{}) {
-    const int w = (blockIdx.x * kBlock + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (w >= count) return;
-    const int q = order ? static_cast<int>(order[w]) : w;
+    if (G == 32 && static_cast<long long>(blockIdx.x * kBlock + threadIdx.x) / 32 >= count)
+        return;  // whole warps
+    bool valid;
+    int lane;
+    const int q = split_query<G>(count, order, valid, lane);
     const float3 p = f3(pts[3 * q], pts[3 * q + 1], pts[3 * q + 2]);
     Trav tv;
     WarpTable tab;
-    knn_split_one<Ops>(bn, leaves, p, k, lane, max_iter, tv, tab);
-    if (lane < k) out[static_cast<size_t>(q) * stride + lane] = warp_table_entry(tab);
-    if (tail.count && __any_sync(0xffffffffu, tv.overflow) && lane == 0) tail_append(tail, q);
-    flush_stats<kStats>(true, tv.nodes, tv.leaves, tv.overflow, stats);
+    knn_split_one<Ops, G>(bn, leaves, p, k, lane, max_iter, tv, tab, valid);
+    if (valid && lane < k) out[static_cast<size_t>(q) * stride + lane] = warp_table_entry(tab);
+    const bool ovf = group_any<G>(tv.overflow);
+    if (tail.count && valid && ovf && lane == 0) tail_append(tail, q);
+    flush_stats<kStats>(valid, tv.nodes, tv.leaves, tv.overflow, stats);
 }
 
 // The tail scan: block (tile, batch) runs heavy query base + batch x kTailBatch + t of the
@@ -887,32 +903,37 @@ int tail_resolve(const qk_tree* t, const float* pts, int k, int stride, uint2* o
 // radius, split: the count pass stores every lane's count (lane_counts[q * 32 + lane]) and
 // the query's total; the fill pass writes each lane's keys at the query's offset plus the
 // counts of the lower lanes.
-template <class Ops, bool kFill, bool kStats>
+template <class Ops, bool kFill, bool kStats, int G>
 __global__ __launch_bounds__(kBlock) void k_radius_split(
     const BNode* __restrict__ bn, const float4* __restrict__ leaves, const float* __restrict__ pts,
     const uint32_t* __restrict__ order, int count, float r2, int* __restrict__ counts,
     int* __restrict__ lane_counts, const int* __restrict__ offsets,
     unsigned long long* __restrict__ keys, int max_iter, unsigned long long* __restrict__ stats) {
-    const int w = (blockIdx.x * kBlock + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (w >= count) return;
-    const int q = order ? static_cast<int>(order[w]) : w;
+    if (G == 32 && static_cast<long long>(blockIdx.x * kBlock + threadIdx.x) / 32 >= count)
+        return;  // whole warps
+    bool valid;
+    int lane;
+    const int q = split_query<G>(count, order, valid, lane);
     const float3 p = f3(pts[3 * q], pts[3 * q + 1], pts[3 * q + 2]);
     Trav tv;
     int write = 0, end = 0;
     if (kFill) {
-        const int mine = lane_counts[static_cast<size_t>(q) * 32 + lane];
-        write = offsets[q] + warp_exclusive(mine, lane);
-        end = min(write + mine, offsets[q + 1]);
+        // lane counts of the query: G per query at q * G
+        const int mine = valid ? lane_counts[static_cast<size_t>(q) * G + lane] : 0;
+        const int below = warp_exclusive<G>(mine, lane);  // every lane takes part
+        write = valid ? offsets[q] + below : 0;
+        end = valid ? min(write + mine, offsets[q + 1]) : 0;
     }
-    const int found = radius_split_one<Ops, kFill>(bn, leaves, p, r2, lane, write, end, keys,
-                                                   max_iter, tv);
+    const int found = radius_split_one<Ops, kFill, G>(bn, leaves, p, r2, lane, write, end, keys,
+                                                      max_iter, tv, valid);
     if (!kFill) {
-        lane_counts[static_cast<size_t>(q) * 32 + lane] = found;
-        const int total = __reduce_add_sync(0xffffffffu, found);
-        if (lane == 0) counts[q] = total;
+        const int total = group_sum<G>(found);
+        if (valid) {
+            lane_counts[static_cast<size_t>(q) * G + lane] = found;
+            if (lane == 0) counts[q] = total;
+        }
     }
-    flush_stats<kStats>(true, tv.nodes, tv.leaves, tv.overflow, stats);
+    flush_stats<kStats>(valid, tv.nodes, tv.leaves, tv.overflow, stats);
 }
 
 // ---- segment sort of the radius keys ----
@@ -1116,6 +1137,46 @@ const uint32_t* make_order(const float* pos, int stride, int offset, int count, 
     return o.idx_s;
 }
 
+// lanes per query of the split schedules: QK_TUNE_SPLIT a warp, QK_TUNE_SPLIT8 / 4 groups of
+// 8 / 4 lanes; 0 for one thread per query
+constexpr unsigned kSplitFlags = QK_TUNE_SPLIT | QK_TUNE_SPLIT8 | QK_TUNE_SPLIT4;
+inline int split_lanes(unsigned flags) {
+    return (flags & QK_TUNE_SPLIT) ? 32 : (flags & QK_TUNE_SPLIT8) ? 8 : (flags & QK_TUNE_SPLIT4) ? 4 : 0;
+}
+
+template <class Ops, bool kStats>
+void launch_closest_split(int lanes, const BNode* bn, const float4* leaves, const float* pts,
+                          const uint32_t* order, int count, uint2* out, int max_iter,
+                          unsigned long long* stats, const TailList& tail, cudaStream_t s) {
+    const int g = blocks_for(static_cast<long long>(count) * lanes);
+    if (lanes == 4)
+        k_closest_split<Ops, kStats, 4><<<g, kBlock, 0, s>>>(bn, leaves, pts, order, count, out, max_iter, stats, tail);
+    else if (lanes == 8)
+        k_closest_split<Ops, kStats, 8><<<g, kBlock, 0, s>>>(bn, leaves, pts, order, count, out, max_iter, stats, tail);
+    else
+        k_closest_split<Ops, kStats, 32><<<g, kBlock, 0, s>>>(bn, leaves, pts, order, count, out, max_iter, stats, tail);
+}
+
+// kNN keeps its table one entry per lane: at least k lanes (the next group size up)
+inline int knn_lanes(int requested, int k) {
+    const int need = k <= 4 ? 4 : (k <= 8 ? 8 : 32);
+    return requested > need ? requested : need;
+}
+
+template <class Ops, bool kStats>
+void launch_knn_split(int lanes, const BNode* bn, const float4* leaves, const float* pts,
+                      const uint32_t* order, int count, int k, int stride, uint2* out,
+                      int max_iter, unsigned long long* stats, const TailList& tail,
+                      cudaStream_t s) {
+    const int g = blocks_for(static_cast<long long>(count) * lanes);
+    if (lanes == 4)
+        k_knn_split<Ops, kStats, 4><<<g, kBlock, 0, s>>>(bn, leaves, pts, order, count, k, stride, out, max_iter, stats, tail);
+    else if (lanes == 8)
+        k_knn_split<Ops, kStats, 8><<<g, kBlock, 0, s>>>(bn, leaves, pts, order, count, k, stride, out, max_iter, stats, tail);
+    else
+        k_knn_split<Ops, kStats, 32><<<g, kBlock, 0, s>>>(bn, leaves, pts, order, count, k, stride, out, max_iter, stats, tail);
+}
+
 template <class Ops>
 int closest_impl(const qk_tree* t, const float* pts, int count, uint2* out, unsigned flags,
                  unsigned long long* stats, const uint32_t* order, cudaStream_t s,
@@ -1129,9 +1190,9 @@ int closest_impl(const qk_tree* t, const float* pts, int count, uint2* out, unsi
         // budgeted traversal (binary nodes, thread or warp per query), then the shared scan
         const BNode* bn = static_cast<const BNode*>(t->bnodes);
         cudaMemsetAsync(tail.count, 0, sizeof(int), s);
-        if (flags & QK_TUNE_SPLIT)
-            k_closest_split<Ops, false><<<blocks_for(static_cast<long long>(count) * 32), kBlock, 0, s>>>(
-                bn, leaves, pts, order, count, out, kTailBudgetLane, nullptr, tail);
+        if (flags & kSplitFlags)
+            launch_closest_split<Ops, false>(split_lanes(flags), bn, leaves, pts, order, count, out,
+                                             kTailBudgetLane, nullptr, tail, s);
         else
             k_closest_bin<Ops, false><<<g, qb, 0, s>>>(bn, leaves, pts, order, count, out,
                                                            kTailBudgetThread, nullptr, nullptr, tail);
@@ -1148,11 +1209,10 @@ int closest_impl(const qk_tree* t, const float* pts, int count, uint2* out, unsi
             if (st) k_closest_wide<Ops, true><<<g, qb, 0, s>>>(wn, leaves, pts, order, count, out, t->n * 2 + 64, stats);
             else k_closest_wide<Ops, false><<<g, qb, 0, s>>>(wn, leaves, pts, order, count, out, t->n * 2 + 64, stats);
         }
-    } else if (flags & QK_TUNE_SPLIT) {
+    } else if (flags & kSplitFlags) {
         const BNode* bn = static_cast<const BNode*>(t->bnodes);
-        const int gs = blocks_for(static_cast<long long>(count) * 32);
-        if (st) k_closest_split<Ops, true><<<gs, kBlock, 0, s>>>(bn, leaves, pts, order, count, out, t->n * 2 + 64, stats);
-        else k_closest_split<Ops, false><<<gs, kBlock, 0, s>>>(bn, leaves, pts, order, count, out, t->n * 2 + 64, stats);
+        if (st) launch_closest_split<Ops, true>(split_lanes(flags), bn, leaves, pts, order, count, out, t->n * 2 + 64, stats, TailList{}, s);
+        else launch_closest_split<Ops, false>(split_lanes(flags), bn, leaves, pts, order, count, out, t->n * 2 + 64, stats, TailList{}, s);
     } else if (flags & QK_TUNE_LEAF4) {
         const BNode* bn = static_cast<const BNode*>(t->bnodes);
         if (st) k_closest_bin<Ops, true, true><<<g, qb, 0, s>>>(bn, leaves, pts, order, count, out, t->n * 2 + 64, stats, leaf_nodes(t));
@@ -1168,16 +1228,16 @@ int closest_impl(const qk_tree* t, const float* pts, int count, uint2* out, unsi
 
 template <class Ops, int K>
 void launch_knn(const qk_tree* t, const float* pts, int count, int k, int stride, uint2* out,
-                bool wide, bool split, bool leaf4, unsigned long long* stats,
+                bool wide, int split, bool leaf4, unsigned long long* stats,
                 const uint32_t* order, cudaStream_t s) {
     const float4* leaves = static_cast<const float4*>(t->leaves);
     const int qb = query_block(count);
     const int g = blocks_for(count, qb);
     if (split && !wide) {
         const BNode* bn = static_cast<const BNode*>(t->bnodes);
-        const int gs = blocks_for(static_cast<long long>(count) * 32);
-        if (stats) k_knn_split<Ops, K, true><<<gs, kBlock, 0, s>>>(bn, leaves, pts, order, count, k, stride, out, t->n * 2 + 64, stats);
-        else k_knn_split<Ops, K, false><<<gs, kBlock, 0, s>>>(bn, leaves, pts, order, count, k, stride, out, t->n * 2 + 64, stats);
+        const int lanes = knn_lanes(split, k);
+        if (stats) launch_knn_split<Ops, true>(lanes, bn, leaves, pts, order, count, k, stride, out, t->n * 2 + 64, stats, TailList{}, s);
+        else launch_knn_split<Ops, false>(lanes, bn, leaves, pts, order, count, k, stride, out, t->n * 2 + 64, stats, TailList{}, s);
     } else if (wide) {
         const WideNode* wn = static_cast<const WideNode*>(t->wide);
         if (t->wide_leaf == 4) {
@@ -1200,14 +1260,14 @@ void launch_knn(const qk_tree* t, const float* pts, int count, int k, int stride
 
 template <class Ops, int K>
 int knn_tail(const qk_tree* t, const float* pts, int count, int k, int stride, uint2* out,
-             bool split, const uint32_t* order, const TailList& tail,
+             int split, const uint32_t* order, const TailList& tail,
              unsigned long long* stats, cudaStream_t s) {
     const BNode* bn = static_cast<const BNode*>(t->bnodes);
     const float4* leaves = static_cast<const float4*>(t->leaves);
     cudaMemsetAsync(tail.count, 0, sizeof(int), s);
     if (split)
-        k_knn_split<Ops, K, false><<<blocks_for(static_cast<long long>(count) * 32), kBlock, 0, s>>>(
-            bn, leaves, pts, order, count, k, stride, out, kTailBudgetLane, nullptr, tail);
+        launch_knn_split<Ops, false>(knn_lanes(split, k), bn, leaves, pts, order, count, k,
+                                     stride, out, kTailBudgetLane, nullptr, tail, s);
     else
         k_knn_bin<Ops, K, false><<<blocks_for(count, query_block(count)), query_block(count), 0, s>>>(
             bn, leaves, pts, order, count, k, stride, out, kTailBudgetThread, nullptr, nullptr, tail);
@@ -1221,7 +1281,7 @@ int knn_impl(const qk_tree* t, const float* pts, int count, int k, int stride, u
              unsigned flags, unsigned long long* stats, const uint32_t* order, cudaStream_t s,
              const TailList& tail = TailList{}) {
     const bool wide = (flags & QK_WIDE) != 0;
-    const bool split = (flags & QK_TUNE_SPLIT) != 0;
+    const int split = split_lanes(flags);  // 0: one thread per query
     const bool leaf4 = (flags & QK_TUNE_LEAF4) != 0;
     if (tail.count) {
         if (k <= 4) return knn_tail<Ops, 4>(t, pts, count, k, stride, out, split, order, tail, stats, s);
@@ -1244,11 +1304,20 @@ int radius_launch(const qk_tree* t, const float* pts, int count, float r2, int* 
     const float4* leaves = static_cast<const float4*>(t->leaves);
     const int qb = query_block(count);
     const int g = blocks_for(count, qb);
-    if ((flags & QK_TUNE_SPLIT) && !(flags & QK_WIDE)) {
+    if ((flags & kSplitFlags) && !(flags & QK_WIDE)) {
         const BNode* bn = static_cast<const BNode*>(t->bnodes);
-        const int gs = blocks_for(static_cast<long long>(count) * 32);
-        if (stats) k_radius_split<Ops, kFill, true><<<gs, kBlock, 0, s>>>(bn, leaves, pts, order, count, r2, counts, lane_counts, offsets, keys, t->n * 2 + 64, stats);
-        else k_radius_split<Ops, kFill, false><<<gs, kBlock, 0, s>>>(bn, leaves, pts, order, count, r2, counts, lane_counts, offsets, keys, t->n * 2 + 64, stats);
+        const int lanes = split_lanes(flags);
+        const int gs = blocks_for(static_cast<long long>(count) * lanes);
+        if (lanes == 4) {
+            if (stats) k_radius_split<Ops, kFill, true, 4><<<gs, kBlock, 0, s>>>(bn, leaves, pts, order, count, r2, counts, lane_counts, offsets, keys, t->n * 2 + 64, stats);
+            else k_radius_split<Ops, kFill, false, 4><<<gs, kBlock, 0, s>>>(bn, leaves, pts, order, count, r2, counts, lane_counts, offsets, keys, t->n * 2 + 64, stats);
+        } else if (lanes == 8) {
+            if (stats) k_radius_split<Ops, kFill, true, 8><<<gs, kBlock, 0, s>>>(bn, leaves, pts, order, count, r2, counts, lane_counts, offsets, keys, t->n * 2 + 64, stats);
+            else k_radius_split<Ops, kFill, false, 8><<<gs, kBlock, 0, s>>>(bn, leaves, pts, order, count, r2, counts, lane_counts, offsets, keys, t->n * 2 + 64, stats);
+        } else {
+            if (stats) k_radius_split<Ops, kFill, true, 32><<<gs, kBlock, 0, s>>>(bn, leaves, pts, order, count, r2, counts, lane_counts, offsets, keys, t->n * 2 + 64, stats);
+            else k_radius_split<Ops, kFill, false, 32><<<gs, kBlock, 0, s>>>(bn, leaves, pts, order, count, r2, counts, lane_counts, offsets, keys, t->n * 2 + 64, stats);
+        }
     } else if (flags & QK_WIDE) {
         const WideNode* wn = static_cast<const WideNode*>(t->wide);
         if (t->wide_leaf == 4) {
@@ -1429,7 +1498,7 @@ int knn_query(const qk_tree* t, const float* pts, int count, int k, int stride, 
 
 // the single-pass pool applies to the binary thread-per-query traversal only
 bool use_stash(unsigned flags) {
-    return (flags & QK_TUNE_STASH) && !(flags & (QK_TUNE_SPLIT | QK_WIDE));
+    return (flags & QK_TUNE_STASH) && !(flags & (kSplitFlags | QK_WIDE));
 }
 
 size_t radius_ws_bytes(int count, unsigned flags) {
@@ -1439,7 +1508,7 @@ size_t radius_ws_bytes(int count, unsigned flags) {
     c.take<char>(scan_ws_bytes(count));
     c.take<int>(count);            // medium segment list
     c.take<int>(count);            // large segment list
-    if (flags & QK_TUNE_SPLIT) c.take<int>(static_cast<size_t>(count) * 32);  // lane counts
+    if (flags & kSplitFlags) c.take<int>(static_cast<size_t>(count) * 32);  // lane counts
     if (use_stash(flags)) carve_pool(c, count);
     return c.used;
 }
@@ -1500,7 +1569,7 @@ int radius_count(const qk_tree* t, const float* pts, int count, float r, int* of
     void* scan_ws = c.take<char>(scan_ws_bytes(count));
     c.take<int>(count);
     c.take<int>(count);
-    int* lane_counts = (flags & QK_TUNE_SPLIT) ? c.take<int>(static_cast<size_t>(count) * 32) : nullptr;
+    int* lane_counts = (flags & kSplitFlags) ? c.take<int>(static_cast<size_t>(count) * 32) : nullptr;
     const bool pooled = use_stash(flags);
     const RadiusPool pool = pooled ? carve_pool(c, count) : RadiusPool{};
     int st = QK_OK;
@@ -1532,7 +1601,7 @@ int radius_fill(const qk_tree* t, const float* pts, int count, float r, const in
     c.take<char>(scan_ws_bytes(count));
     int* medium = c.take<int>(count);
     int* large = c.take<int>(count);
-    int* lane_counts = (flags & QK_TUNE_SPLIT) ? c.take<int>(static_cast<size_t>(count) * 32) : nullptr;
+    int* lane_counts = (flags & kSplitFlags) ? c.take<int>(static_cast<size_t>(count) * 32) : nullptr;
     const bool pooled = use_stash(flags);
     const RadiusPool pool = pooled ? carve_pool(c, count) : RadiusPool{};
     auto* k64 = reinterpret_cast<unsigned long long*>(keys);

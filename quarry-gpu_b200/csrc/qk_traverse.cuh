@@ -1082,12 +1082,33 @@ __device__ __forceinline__ int radius_wide_one(const WideNode* __restrict__ wn,
 // the tree (a point near the centre of a spherical shell) is spread over 32 lanes.  The
 // subtrees partition the leaves and the shared bound only ever comes from found candidates,
 // so results equal the one-thread-per-query kernels bit for bit.
+//
+// Groups (QK_TUNE_SPLIT8 / QK_TUNE_SPLIT4): the same with G = 8 or 4 lanes per query, the top
+// log2(G) levels split, every exchange restricted to the query's G aligned lanes (shuffle
+// width G, the group's bits of each ballot).  Few queries then fill more of the GPU without
+// 32-fold redundancy.  Warp-wide loop conditions keep every lane of the warp in the same
+// collectives; a group past the last query traces query 0 and writes nothing.
 // ---------------------------------------------------------------------------------------
 constexpr int kSplitLevels = 5;
 
+constexpr int log2_lanes(int g) { return g <= 1 ? 0 : 1 + log2_lanes(g / 2); }
+
+// first lane of this thread's group of G lanes in its warp, and the group's ballot bits
+template <int G>
+__device__ __forceinline__ int group_base() { return (threadIdx.x & 31) & ~(G - 1); }
+template <int G>
+__device__ __forceinline__ unsigned group_bits(unsigned ballot) {
+    return G == 32 ? ballot : (ballot >> group_base<G>()) & ((1u << G) - 1u);
+}
+template <int G>
+__device__ __forceinline__ bool group_any(bool v) {
+    return group_bits<G>(__ballot_sync(0xffffffffu, v)) != 0u;
+}
+
+template <int G = 32>
 __device__ __forceinline__ void warp_min_lex(float& d, int& id) {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
+    for (int o = G / 2; o > 0; o >>= 1) {
         const float od = __shfl_xor_sync(0xffffffffu, d, o);
         const int oi = __shfl_xor_sync(0xffffffffu, id, o);
         if (closer(od, oi, d, id)) {
@@ -1100,11 +1121,11 @@ __device__ __forceinline__ void warp_min_lex(float& d, int& id) {
 // Forced descent of lane `lane` from the root: returns the subtree root the lane owns (an
 // internal node) or -1; a leaf met on the way is handed to `on_leaf` by its owning lane.
 // `keep(box)` decides whether a child box can still hold a result.
-template <class Leaf, class Keep>
+template <int kLevels = kSplitLevels, class Leaf, class Keep>
 __device__ __forceinline__ int split_descend(const BNode* __restrict__ bn, int lane, Leaf on_leaf,
                                              Keep keep) {
     int node = 0;
-    for (int d = 0; d < kSplitLevels; ++d) {
+    for (int d = 0; d < kLevels; ++d) {
         float3 llo, lhi, rlo, rhi;
         int lref, rref;
         load_bnode(bn, node, llo, lhi, rlo, rhi, lref, rref);
@@ -1122,10 +1143,11 @@ __device__ __forceinline__ int split_descend(const BNode* __restrict__ bn, int l
     return node;
 }
 
-template <class Ops>
+template <class Ops, int G = 32>
 __device__ __forceinline__ uint2 closest_split_one(const BNode* __restrict__ bn,
                                                    const float4* __restrict__ leaves, float3 p,
-                                                   int lane, int max_iter, Trav& tv) {
+                                                   int lane, int max_iter, Trav& tv,
+                                                   bool valid = true) {
     float best = kInf;
     int best_id = 0x7fffffff;
     auto on_leaf = [&](int slot) {
@@ -1137,8 +1159,10 @@ __device__ __forceinline__ uint2 closest_split_one(const BNode* __restrict__ bn,
             best_id = id;
         }
     };
-    int node = split_descend(bn, lane, on_leaf, [](float3, float3) { return true; });
-    warp_min_lex(best, best_id);
+    int node = valid ? split_descend<log2_lanes(G)>(bn, lane, on_leaf,
+                                                    [](float3, float3) { return true; })
+                     : -1;
+    warp_min_lex<G>(best, best_id);
     LocalStack<kStack> st;
     int sp = 0;
     bool active = node >= 0;
@@ -1194,7 +1218,7 @@ __device__ __forceinline__ uint2 closest_split_one(const BNode* __restrict__ bn,
                 }
             }
         }
-        warp_min_lex(best, best_id);
+        warp_min_lex<G>(best, best_id);
     }
     return best_id != 0x7fffffff ? make_uint2(__float_as_uint(best), static_cast<unsigned>(best_id))
                                  : make_uint2(0u, 0xffffffffu);
@@ -1218,8 +1242,30 @@ struct WarpTable {
     __device__ __forceinline__ bool admits(float bound) const {
         return kid == 0x7fffffff || bound <= kd;
     }
-    // whole warp; x is the same on every lane
-    __device__ __forceinline__ void insert(float xd, int xid, int k, int lane) {
+    // whole warp; x is the same on every lane of a group, `lane` the lane in the group; a group
+    // with doit false keeps its table (every lane still takes part in the exchanges)
+    template <int G = 32>
+    __device__ __forceinline__ void insert(float xd, int xid, int k, int lane, bool doit = true) {
+        if constexpr (G < 32) {
+            const bool want = doit && closer(xd, xid, kd, kid);
+            const unsigned before = group_bits<G>(
+                __ballot_sync(0xffffffffu, lane < k && closer(d, id, xd, xid)));
+            const int pos = __popc(before);
+            const float pd = __shfl_up_sync(0xffffffffu, d, 1, G);
+            const int pid = __shfl_up_sync(0xffffffffu, id, 1, G);
+            if (want && lane < k) {
+                if (lane == pos) {
+                    d = xd;
+                    id = xid;
+                } else if (lane > pos) {
+                    d = pd;
+                    id = pid;
+                }
+            }
+            kd = __shfl_sync(0xffffffffu, d, k - 1, G);
+            kid = __shfl_sync(0xffffffffu, id, k - 1, G);
+            return;
+        }
         if (!closer(xd, xid, kd, kid)) return;
         const unsigned before = __ballot_sync(0xffffffffu, lane < k && closer(d, id, xd, xid));
         const int pos = __popc(before);
@@ -1239,11 +1285,12 @@ struct WarpTable {
     }
 };
 
-// the warp's table holds the query's k best on return (entry j in lane j)
-template <class Ops>
+// the warp's (group's) table holds the query's k best on return (entry j in lane j; k <= G)
+template <class Ops, int G = 32>
 __device__ __forceinline__ void knn_split_one(const BNode* __restrict__ bn,
                                               const float4* __restrict__ leaves, float3 p, int k,
-                                              int lane, int max_iter, Trav& tv, WarpTable& tab) {
+                                              int lane, int max_iter, Trav& tv, WarpTable& tab,
+                                              bool valid = true) {
     tab.init();
     tab.init();
     // up to two pending leaf candidates per lane, inserted by the whole warp
@@ -1258,19 +1305,34 @@ __device__ __forceinline__ void knn_split_one(const BNode* __restrict__ bn,
     auto flush = [&]() {
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
-            unsigned m = __ballot_sync(0xffffffffu, has[c]);
-            while (m) {
-                const int src = __ffs(m) - 1;
-                const float xd = __shfl_sync(0xffffffffu, cd[c], src);
-                const int xid = __shfl_sync(0xffffffffu, cid[c], src);
-                tab.insert(xd, xid, k, lane);
-                m &= m - 1;
+            if constexpr (G < 32) {
+                // each group inserts its own candidates, lowest lane first; the rounds run
+                // until no group of the warp has one left
+                unsigned m = group_bits<G>(__ballot_sync(0xffffffffu, has[c]));
+                while (__any_sync(0xffffffffu, m != 0u)) {
+                    const bool doit = m != 0u;
+                    const int src = doit ? __ffs(m) - 1 : 0;
+                    const float xd = __shfl_sync(0xffffffffu, cd[c], src, G);
+                    const int xid = __shfl_sync(0xffffffffu, cid[c], src, G);
+                    tab.insert<G>(xd, xid, k, lane, doit);
+                    if (doit) m &= m - 1;
+                }
+            } else {
+                unsigned m = __ballot_sync(0xffffffffu, has[c]);
+                while (m) {
+                    const int src = __ffs(m) - 1;
+                    const float xd = __shfl_sync(0xffffffffu, cd[c], src);
+                    const int xid = __shfl_sync(0xffffffffu, cid[c], src);
+                    tab.insert(xd, xid, k, lane);
+                    m &= m - 1;
+                }
             }
             has[c] = false;
         }
     };
-    int node = split_descend(bn, lane, [&](int slot) { leaf(slot, 0); },
-                             [](float3, float3) { return true; });
+    int node = valid ? split_descend<log2_lanes(G)>(bn, lane, [&](int slot) { leaf(slot, 0); },
+                                                    [](float3, float3) { return true; })
+                     : -1;
     flush();
     LocalStack<kStack> st;
     int sp = 0;
@@ -1331,12 +1393,12 @@ __device__ __forceinline__ uint2 warp_table_entry(const WarpTable& tab) {
 
 // radius, split: returns this lane's count; the fill pass writes the lane's keys from
 // `write` on, never past `end` (the query's offset plus the counts of the lower lanes)
-template <class Ops, bool kFill>
+template <class Ops, bool kFill, int G = 32>
 __device__ __forceinline__ int radius_split_one(const BNode* __restrict__ bn,
                                                 const float4* __restrict__ leaves, float3 p,
                                                 float r2, int lane, int write, int end,
                                                 unsigned long long* __restrict__ keys,
-                                                int max_iter, Trav& tv) {
+                                                int max_iter, Trav& tv, bool valid = true) {
     int found = 0;
     auto keep = [&](float3 lo, float3 hi) { return dist2_box(p, lo, hi) <= r2; };
     auto on_leaf = [&](int slot) {
@@ -1348,7 +1410,7 @@ __device__ __forceinline__ int radius_split_one(const BNode* __restrict__ bn,
             ++found;
         }
     };
-    int node = split_descend(bn, lane, on_leaf, keep);
+    int node = valid ? split_descend<log2_lanes(G)>(bn, lane, on_leaf, keep) : -1;
     LocalStack<kStack> st;
     int sp = 0;
     for (int iter = 0; node >= 0; ++iter) {
@@ -1388,15 +1450,24 @@ __device__ __forceinline__ int radius_split_one(const BNode* __restrict__ bn,
     return found;
 }
 
-// exclusive prefix over the lanes of `v`
+// exclusive prefix over the lanes of `v` (of the group of G lanes; `lane` the lane in it)
+template <int G = 32>
 __device__ __forceinline__ int warp_exclusive(int v, int lane) {
     int incl = v;
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int u = __shfl_up_sync(0xffffffffu, incl, o);
+    for (int o = 1; o < G; o <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, incl, o, G);
         if (lane >= o) incl += u;
     }
     return incl - v;
+}
+
+// sum of `v` over the group of G lanes (every lane gets it)
+template <int G>
+__device__ __forceinline__ int group_sum(int v) {
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
 }
 
 }  // namespace qk

@@ -26,6 +26,8 @@ QK_TUNE_DYNAMIC, QK_TUNE_HIGH_OCC, QK_TUNE_SPLIT, QK_TUNE_SHORT_STACK = 256, 512
 QK_TUNE_LEAF4 = 4096
 QK_TUNE_STASH = 8192
 QK_TUNE_TAIL = 16384
+QK_TUNE_SPLIT8 = 32768
+QK_TUNE_SPLIT4 = 65536
 QK_SCHEDULE_BATCHED, QK_SCHEDULE_LOOP = 0, 1
 QK_OP_RAY, QK_OP_CLOSEST, QK_OP_KNN, QK_OP_RADIUS = 0, 1, 2, 3
 KINDS = {"tri": QK_TRI, "point": QK_POINT, "gauss": QK_GAUSS}

@@ -477,8 +477,10 @@ def test_coherent_order_same_bits(cuda, count):
 @pytest.mark.parametrize("kind", ["tri", "point", "gauss"])
 @pytest.mark.parametrize("n", [2, 3, 5, 40, 20_000])
 def test_split_queries_same_bits(cuda, kind, n):
-    """One warp per query over 32 disjoint subtrees: closest, kNN and radius equal the
-    one-thread-per-query kernels, including trees shallower than the split levels."""
+    """One warp per query over 32 disjoint subtrees, and groups of 8 and 4 lanes over 8 and 4
+    subtrees: closest, kNN (k from 1 to 16: groups grow to k lanes) and radius equal the
+    one-thread-per-query kernels, including trees shallower than the split levels and a query
+    count (3,001) that leaves the last warp's groups partly past the end."""
     rng = np.random.default_rng(n)
     if kind == "tri":
         items = rng.uniform(0, 10, (n, 9)).astype(np.float32)
@@ -491,18 +493,21 @@ def test_split_queries_same_bits(cuda, kind, n):
     lo = np.asarray(items).reshape(n, -1)[:, :3].min(0) - 1
     hi = np.asarray(items).reshape(n, -1)[:, :3].max(0) + 1
     q = _dev(workloads.uniform_points(3_001, lo, hi, 7, 13))
-    for extra in (0, capi.QK_ORDER_MORTON):
-        f = capi.QK_TUNE_SPLIT | extra
-        assert cuda.equal(tree.closest(q, f), tree.closest(q, 0))
-        for k in (1, 8, 16):
-            assert cuda.equal(tree.knn(q, k, f), tree.knn(q, k, 0)), (k, extra)
-        r = float(np.linalg.norm(hi - lo)) * 0.05
-        o1, k1 = tree.radius(q, r, f)
-        o0, k0 = tree.radius(q, r, 0)
-        assert cuda.equal(o1, o0) and cuda.equal(k1, k0)
-    stats = cuda.zeros(4, dtype=cuda.int64, device="cuda")
-    tree.knn(q, 8, capi.QK_TUNE_SPLIT, stats=stats)
-    assert int(stats[2]) == 0
+    r = float(np.linalg.norm(hi - lo)) * 0.05
+    o0, k0 = tree.radius(q, r, 0)
+    c0 = tree.closest(q, 0)
+    knn0 = {k: tree.knn(q, k, 0) for k in (1, 3, 8, 16)}
+    for split in (capi.QK_TUNE_SPLIT, capi.QK_TUNE_SPLIT8, capi.QK_TUNE_SPLIT4):
+        for extra in (0, capi.QK_ORDER_MORTON, capi.QK_ORDER_COHERENT):
+            f = split | extra
+            assert cuda.equal(tree.closest(q, f), c0), (split, extra)
+            for k, want in knn0.items():
+                assert cuda.equal(tree.knn(q, k, f), want), (split, k, extra)
+            o1, k1 = tree.radius(q, r, f)
+            assert cuda.equal(o1, o0) and cuda.equal(k1, k0), (split, extra)
+        stats = cuda.zeros(4, dtype=cuda.int64, device="cuda")
+        tree.knn(q, 8, split, stats=stats)
+        assert int(stats[2]) == 0
 
 
 def _check_small_codes(tree: capi.DeviceTree):
@@ -767,7 +772,7 @@ def test_point_tail_same_results(cuda):
     assert np.array_equal(base_c.cpu().numpy().view(np.uint32)[::7], want_c)
     for f in (capi.QK_TUNE_TAIL, capi.QK_TUNE_TAIL | capi.QK_TUNE_SPLIT,
               capi.QK_TUNE_TAIL | capi.QK_TUNE_SPLIT | capi.QK_ORDER_COHERENT,
-              capi.QK_TUNE_TAIL | capi.QK_ORDER_MORTON):
+              capi.QK_TUNE_TAIL | capi.QK_TUNE_SPLIT8, capi.QK_TUNE_TAIL | capi.QK_ORDER_MORTON):
         stats = cuda.zeros(4, dtype=cuda.int64, device="cuda")
         assert cuda.equal(tree.closest(dq, f, stats=stats), base_c), f
         heavy = int(stats[3].item())
@@ -778,7 +783,7 @@ def test_point_tail_same_results(cuda):
         if k == 8:
             assert np.array_equal(base.cpu().numpy().view(np.uint32)[::7], ref.knn(q[::7], 8))
         for f in (capi.QK_TUNE_TAIL, capi.QK_TUNE_TAIL | capi.QK_TUNE_SPLIT,
-                  capi.QK_TUNE_TAIL | capi.QK_ORDER_COHERENT):
+                  capi.QK_TUNE_TAIL | capi.QK_TUNE_SPLIT8, capi.QK_TUNE_TAIL | capi.QK_ORDER_COHERENT):
             assert cuda.equal(tree.knn(dq, k, f), base), (k, f)
     # other kinds ignore the flag
     g = capi.DeviceTree("gauss", workloads.gaussians(20_000, 0.05, 1.0, 2))

@@ -1682,11 +1682,13 @@ KERNEL_CASES = {
                  "k_warp_tasks, k_sah_leaves, k_bottom_up_ranged)",
     "refit": "full and 1% dirty refit of the volume cloud's LBVH (k_refit_leaves, k_bottom_up, "
              "k_dirty_mark, k_dirty_merge)",
-    "closest_tri": "20,000 closest-point queries on the terrain's LBVH, 131,072 triangles "
-                   "(k_closest_bin)",
+    "closest_tri": "20,000 closest-point queries on the terrain's LBVH, 131,072 triangles, one "
+                   "thread per query (k_closest_bin) and 4 lanes per query (k_closest_split)",
     "closest_gauss": "262,144 closest-ellipsoid queries on 1,048,576 Gaussians (k_closest_bin)",
-    "knn_points": "kNN k=8, 20,000 queries on each 1,048,576-point cloud (k_knn_split on the "
-                  "sphere shell, k_knn_bin on the uniform cloud)",
+    "knn_points": "kNN k=8, 20,000 queries on each 1,048,576-point cloud (k_knn_split: a warp "
+                  "per query on the sphere shell's SAH tree in coherent order, then 8 lanes per "
+                  "query on the uniform cloud; k_knn_bin: one thread per query on the uniform "
+                  "cloud)",
     "radius_points": "radius 1.0, 20,000 queries on the uniform cloud, single pass "
                      "(k_radius_count_pool, k_radius_gather, k_radius_fill_lost, k_seg_sort_*)",
     "grad": "adjoints: 262,144 Gaussian distances (k_dist_grad, k_segment_sum) and 1,000,000 "
@@ -1733,6 +1735,7 @@ def kernel_case(args):
         qd = dev(cfg.queries, np.float32)
         for _ in range(2):
             t2.closest(qd, 0)
+            t2.closest(qd, capi.QK_TUNE_SPLIT4)
     elif name == "closest_gauss":
         g = capi.DeviceTree("gauss", w.gaussians(1_048_576, 0.05, 1.0, 1))
         qd = dev(w.uniform_points(262_144, [0, 0, 0], [100, 100, 100], 1, 31), np.float32)
@@ -1744,6 +1747,7 @@ def kernel_case(args):
         qs = dev(w.uniform_points(20_000, shell.min(0), shell.max(0), 1, 13), np.float32)
         for _ in range(2):
             ts.knn(qs, 8, capi.QK_TUNE_SPLIT | capi.QK_ORDER_COHERENT)
+            tree.knn(q, 8, capi.QK_TUNE_SPLIT8)
             tree.knn(q, 8, 0)
     elif name == "radius_points":
         for _ in range(2):

@@ -1021,8 +1021,8 @@ def points_arm(args, world, rank, local):
 
     def kernel_of(op, vname):
         f = variants[vname]
-        return ("k_%s_wide" if f & capi.QK_WIDE else "k_%s_split" if f & capi.QK_TUNE_SPLIT
-                else "k_%s_bin") % op
+        split = f & (capi.QK_TUNE_SPLIT | capi.QK_TUNE_SPLIT8 | capi.QK_TUNE_SPLIT4)
+        return ("k_%s_wide" if f & capi.QK_WIDE else "k_%s_split" if split else "k_%s_bin") % op
 
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": pk["hbm_gbs"],
                 "unit": "GB/s", "frac": round(achieved / pk["hbm_gbs"], 4), "traffic": None,

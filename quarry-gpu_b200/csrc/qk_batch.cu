@@ -796,6 +796,13 @@ int batch_build_loop(qk_batch* b, int builder, int bins, cudaStream_t s) {
 }
 
 // ---- queries ----
+// Key pool of a batched single-pass radius plan, in keys per query on average (shared by all
+// queries of the plan).  Larger than the single-tree default: a plan is built once for many
+// replays, and a batch's terrain radius averages about 420 keys per query, so a smaller pool
+// sends most of its keys back through the second traversal.  The plan grows by about 4.3 KB
+// per query (1.3 GB for 300 K queries).
+constexpr int kBatchPoolPerQuery = 512;
+
 struct PlanLayout {
     size_t qoff, chunks, counter, params, stats, hdr, keys, idx, keys_s, idx_s, sort_ws, counts,
         scan_ws, medium, large, lane_counts, pool, loop_ws, loop_ws_bytes, total;
@@ -840,7 +847,7 @@ PlanLayout plan_layout(int op, const int32_t* counts, int scenes, unsigned flags
         if (flags & QK_TUNE_STASH) {
             // the single-pass radius's stash and key pool, carved at the plan creation
             Carve pc;
-            carve_pool(pc, n);
+            carve_pool(pc, n, kBatchPoolPerQuery);
             L.pool = take(pc.used);
         }
     }
@@ -1280,7 +1287,7 @@ int qk_batch_plan_create(qk_batch_plan** out, const qk_batch* b, int op, const i
         p->lane_counts = reinterpret_cast<int*>(base + L.lane_counts);
         if (flags & QK_TUNE_STASH) {
             Carve pc{base + L.pool};
-            p->pool = carve_pool(pc, static_cast<int>(total));
+            p->pool = carve_pool(pc, static_cast<int>(total), kBatchPoolPerQuery);
         }
     }
     p->loop_ws = base + L.loop_ws;

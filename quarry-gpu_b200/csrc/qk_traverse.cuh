@@ -836,9 +836,9 @@ struct RadiusPool {
     int chunks;
 };
 
-inline RadiusPool carve_pool(Carve& c, int count) {
+inline RadiusPool carve_pool(Carve& c, int count, int per_query = kPoolPerQuery) {
     RadiusPool p{};
-    p.chunks = static_cast<int>((static_cast<long long>(count) * kPoolPerQuery + kPoolChunk - 1) /
+    p.chunks = static_cast<int>((static_cast<long long>(count) * per_query + kPoolChunk - 1) /
                                 kPoolChunk);
     p.stash = c.take<unsigned long long>(static_cast<size_t>(count) * kRadiusStash);
     p.first = c.take<int>(count);

@@ -20,6 +20,27 @@ namespace qk {
 
 namespace {
 
+// Launch with programmatic stream serialization: the kernel's blocks may be scheduled while the
+// previous kernel of the stream drains, and the kernel calls cudaGridDependencySynchronize()
+// before it reads anything that kernel wrote.  Used only where the previous operation in the
+// stream is one of this file's own kernels (the chained passes of an ordering and the
+// traversal that reads the order); elsewhere the kernels' wait returns at once.
+template <class... KArgs, class... Args>
+cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t s,
+                       Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 // canonical nodes of the leaves (leaf of slot s at n-1+s): their boxes are the leaf boxes
 inline const Node* leaf_nodes(const qk_tree* t) {
     return static_cast<const Node*>(t->nodes) + (t->n - 1);
@@ -228,6 +249,7 @@ __global__ __launch_bounds__(kBlock) void k_coh_keys(const float* __restrict__ p
                                                     uint32_t* __restrict__ keys,
                                                     uint32_t* __restrict__ ranks,
                                                     uint32_t* __restrict__ hist) {
+    cudaGridDependencySynchronize();  // the grid of k_coh_grid
     float lo[6], scale[6];
 #pragma unroll
     for (int a = 0; a < 6; ++a) {
@@ -284,6 +306,7 @@ __global__ __launch_bounds__(kBlock) void k_coh_keys(const float* __restrict__ p
 // have been scanned
 __global__ __launch_bounds__(kCohThreads) void k_coh_scan(uint32_t* __restrict__ hist,
                                                          int buckets) {
+    cudaGridDependencySynchronize();  // the histogram of k_coh_keys
     constexpr int kWarps = kCohThreads / 32;
     constexpr int kSteps = kCohMaxBuckets / kCohThreads;
     __shared__ uint32_t warp_base[kWarps];
@@ -333,6 +356,7 @@ __global__ __launch_bounds__(kBlock) void k_coh_scatter(const uint32_t* __restri
                                                        int count,
                                                        const uint32_t* __restrict__ start,
                                                        uint32_t* __restrict__ order) {
+    cudaGridDependencySynchronize();  // the bucket starts of k_coh_scan
     const int base = blockIdx.x * (kBlock * kCohItems) + threadIdx.x;
 #pragma unroll
     for (int k = 0; k < kCohItems; ++k) {
@@ -354,6 +378,7 @@ __global__ __launch_bounds__(kBlock, kMinBlocks) void k_ray_bin(const BNode* __r
                                                    int* __restrict__ ids,
                                                    int max_iter, unsigned long long* __restrict__ stats,
                                                    const Node* __restrict__ lnodes = nullptr) {
+    cudaGridDependencySynchronize();  // the order, when the ordering kernels launched it early
     const int i = blockIdx.x * kBlock + threadIdx.x;
     const bool active = i < count;
     Trav tv;
@@ -1108,13 +1133,13 @@ const uint32_t* make_coherent_order(const float* pos, int stride, int count, Ord
     const int g = blocks_for(count, kBlock * kCohItems);
     if (stride == 8) {
         k_coh_grid<6><<<1, kCohThreads, 0, s>>>(pos, count, key_bits, grid);
-        k_coh_keys<6><<<g, kBlock, 0, s>>>(pos, count, grid, o.keys, o.idx, hist);
+        launch_pdl(k_coh_keys<6>, dim3(g), dim3(kBlock), s, pos, count, grid, o.keys, o.idx, hist);
     } else {
         k_coh_grid<3><<<1, kCohThreads, 0, s>>>(pos, count, key_bits, grid);
-        k_coh_keys<3><<<g, kBlock, 0, s>>>(pos, count, grid, o.keys, o.idx, hist);
+        launch_pdl(k_coh_keys<3>, dim3(g), dim3(kBlock), s, pos, count, grid, o.keys, o.idx, hist);
     }
-    k_coh_scan<<<1, kCohThreads, 0, s>>>(hist, buckets);
-    k_coh_scatter<<<g, kBlock, 0, s>>>(o.keys, o.idx, count, hist, o.idx_s);
+    launch_pdl(k_coh_scan, dim3(1), dim3(kCohThreads), s, hist, buckets);
+    launch_pdl(k_coh_scatter, dim3(g), dim3(kBlock), s, o.keys, o.idx, count, hist, o.idx_s);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) *status = cuda_status(e, "coherent order");
     return o.idx_s;
@@ -1438,6 +1463,16 @@ int ray_query(const qk_tree* t, const void* rays, int count, uint64_t* out, int*
         } else if (flags & QK_TUNE_LEAF4) {
             if (stt) k_ray_bin<true, 1, 0, true><<<g, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, ids, t->n * 2 + 64, stt, leaf_nodes(t));
             else k_ray_bin<false, 1, 0, true><<<g, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, ids, t->n * 2 + 64, stt, leaf_nodes(t));
+        } else if (order) {
+            // the previous kernel in the stream wrote the order: start while it drains
+            const Node* no_leaf4 = nullptr;
+            if (flags & QK_TUNE_HIGH_OCC) {
+                if (stt) launch_pdl(k_ray_bin<true, 5>, dim3(g), dim3(kBlock), s, bn, leaves, nodes, r4, order, count, res, ids, t->n * 2 + 64, stt, no_leaf4);
+                else launch_pdl(k_ray_bin<false, 5>, dim3(g), dim3(kBlock), s, bn, leaves, nodes, r4, order, count, res, ids, t->n * 2 + 64, stt, no_leaf4);
+            } else {
+                if (stt) launch_pdl(k_ray_bin<true, 1>, dim3(g), dim3(kBlock), s, bn, leaves, nodes, r4, order, count, res, ids, t->n * 2 + 64, stt, no_leaf4);
+                else launch_pdl(k_ray_bin<false, 1>, dim3(g), dim3(kBlock), s, bn, leaves, nodes, r4, order, count, res, ids, t->n * 2 + 64, stt, no_leaf4);
+            }
         } else if (flags & QK_TUNE_HIGH_OCC) {
             if (stt) k_ray_bin<true, 5><<<g, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, ids, t->n * 2 + 64, stt);
             else k_ray_bin<false, 5><<<g, kBlock, 0, s>>>(bn, leaves, nodes, r4, order, count, res, ids, t->n * 2 + 64, stt);

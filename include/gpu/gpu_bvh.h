@@ -65,6 +65,13 @@ GpuBVH buildBVHGPU(const Scene& scene, GpuBuildTimings* timings = nullptr);
 GpuBVH buildBVHSahGPU(const Scene& scene, GpuBuildTimings* timings = nullptr);
 GpuBVH buildPointBVHSahGPU(const PointCloud& cloud, GpuBuildTimings* timings = nullptr);
 GpuBVH buildGaussianBVHSahGPU(const GaussianCloud& cloud, GpuBuildTimings* timings = nullptr);
+// Engine addition (no quarry counterpart; the leaf-size-4 lever of quarry's docs/design.md):
+// binned SAH whose split search stops at ranges of at most 4 primitives (QK_BUILD_SAH4);
+// buildWideNodesGPU then gives such a tree 4-wide nodes with leaf-range slots.  Same
+// results as every other build.
+GpuBVH buildBVHSah4GPU(const Scene& scene, GpuBuildTimings* timings = nullptr);
+GpuBVH buildPointBVHSah4GPU(const PointCloud& cloud, GpuBuildTimings* timings = nullptr);
+GpuBVH buildGaussianBVHSah4GPU(const GaussianCloud& cloud, GpuBuildTimings* timings = nullptr);
 GpuBVH buildPointBVHGPU(const PointCloud& cloud, GpuBuildTimings* timings = nullptr);
 GpuBVH buildGaussianBVHGPU(const GaussianCloud& cloud, GpuBuildTimings* timings = nullptr);
 

@@ -202,7 +202,7 @@ GpuBVH buildImpl(int kind, const void* host, size_t itemBytes, int n, int builde
             using namespace qk;
             GpuBuildTimings& bt = *timings;
             bt = GpuBuildTimings{};
-            if (builder == QK_BUILD_SAH) {
+            if (builder == QK_BUILD_SAH || builder == QK_BUILD_SAH4) {
                 // topology (levels + lower tiers) and depths; the leaf scatter; the boxes
                 bt.treeMs = clock.ms(kMarkStart, kMarkTopo) + clock.ms(kMarkBoxes, kMarkEnd);
                 bt.scatterMs = clock.ms(kMarkTopo, kMarkScatter);
@@ -221,7 +221,7 @@ GpuBVH buildImpl(int kind, const void* host, size_t itemBytes, int n, int builde
             bt.totalMs = clock.ms(kMarkStart, kMarkEnd);
             if (bt.totalMs <= 0.0) bt.totalMs = ms;
         }
-        bvh.sah = builder == QK_BUILD_SAH;
+        bvh.sah = builder != QK_BUILD_LBVH;
         im->baseDepth = t.depth;
         bvh.impl = im;
         syncPublic(bvh, im);
@@ -676,6 +676,18 @@ GpuBVH buildGaussianBVHSahGPU(const GaussianCloud& cloud, GpuBuildTimings* timin
     return buildImpl(QK_GAUSS, cloud.gaussians.data(), sizeof(Gaussian),
                      static_cast<int>(cloud.gaussians.size()), QK_BUILD_SAH, timings);
 }
+GpuBVH buildBVHSah4GPU(const Scene& scene, GpuBuildTimings* timings) {
+    return buildImpl(QK_TRI, scene.tris.data(), sizeof(Tri), static_cast<int>(scene.tris.size()),
+                     QK_BUILD_SAH4, timings);
+}
+GpuBVH buildPointBVHSah4GPU(const PointCloud& cloud, GpuBuildTimings* timings) {
+    return buildImpl(QK_POINT, cloud.pts.data(), sizeof(Vec3), static_cast<int>(cloud.pts.size()),
+                     QK_BUILD_SAH4, timings);
+}
+GpuBVH buildGaussianBVHSah4GPU(const GaussianCloud& cloud, GpuBuildTimings* timings) {
+    return buildImpl(QK_GAUSS, cloud.gaussians.data(), sizeof(Gaussian),
+                     static_cast<int>(cloud.gaussians.size()), QK_BUILD_SAH4, timings);
+}
 
 void warmupBuildGPU() {
     // a tiny build touches every build kernel once so module loading is not timed later
@@ -731,10 +743,12 @@ double buildWideNodesGPU(GpuBVH& bvh) {
     Timer timer;
     void* old = im->t.wide;
     im->t.wide = nullptr;
-    qkOk(qk_wide_build(&im->t, im->ws, im->wsBytes, nullptr), "wide count");
+    // a leaf-size-4 SAH tree gets the 4-wide form with leaf-range slots
+    auto wide_build = im->builder == QK_BUILD_SAH4 ? qk_wide_build_leaf4 : qk_wide_build;
+    qkOk(wide_build(&im->t, im->ws, im->wsBytes, nullptr), "wide count");
     if (old) cudaFree(old);
     im->t.wide = devAlloc(static_cast<size_t>(im->t.wide_count) * 128, "wide nodes");
-    qkOk(qk_wide_build(&im->t, im->ws, im->wsBytes, nullptr), "wide emit");
+    qkOk(wide_build(&im->t, im->ws, im->wsBytes, nullptr), "wide emit");
     const double ms = timer.stop();
     syncPublic(bvh, im);
     return ms;

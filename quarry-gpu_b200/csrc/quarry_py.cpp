@@ -44,9 +44,11 @@ RayOrder rayOrder(const std::string& s) {
     throw std::invalid_argument("order must be 'input', 'morton', 'direction' or 'coherent'");
 }
 
-bool sahBuilder(const std::string& s) {
-    if (s == "lbvh") return false;
-    if (s == "sah") return true;
+// 0: LBVH, 1: binned SAH, 2: leaf-size-4 binned SAH ("sah4", an engine addition)
+int sahBuilder(const std::string& s) {
+    if (s == "lbvh") return 0;
+    if (s == "sah") return 1;
+    if (s == "sah4") return 2;
     throw std::invalid_argument("builder must be 'lbvh' or 'sah'");
 }
 
@@ -204,7 +206,7 @@ struct Base {
     GpuTopoUpdateTimings topoTimings{};
     AABB bounds;
     double buildMs = 0.0, lastQueryMs = 0.0, refitMs = 0.0;
-    bool sah = false;
+    int sah = 0;  // sahBuilder's code
     bool wideBuilt = false;
     Leaf leaf = Leaf::Tri;
 
@@ -457,7 +459,8 @@ private:
         bounds = scene_.bounds;
         {
             py::gil_scoped_release r;
-            bvh = sah ? buildBVHSahGPU(scene_, &timings) : buildBVHGPU(scene_, &timings);
+            bvh = sah == 2 ? buildBVHSah4GPU(scene_, &timings)
+                  : sah ? buildBVHSahGPU(scene_, &timings) : buildBVHGPU(scene_, &timings);
         }
         buildMs = timings.totalMs;
     }
@@ -492,7 +495,8 @@ public:
         cloud_.updateBounds();
         bounds = cloud_.bounds;
         py::gil_scoped_release r;
-        bvh = sah ? buildPointBVHSahGPU(cloud_, &timings) : buildPointBVHGPU(cloud_, &timings);
+        bvh = sah == 2 ? buildPointBVHSah4GPU(cloud_, &timings)
+              : sah ? buildPointBVHSahGPU(cloud_, &timings) : buildPointBVHGPU(cloud_, &timings);
         buildMs = timings.totalMs;
     }
 
@@ -551,7 +555,8 @@ public:
         cloud_.updateBounds();
         bounds = cloud_.bounds;
         py::gil_scoped_release r;
-        bvh = sah ? buildGaussianBVHSahGPU(cloud_, &timings) : buildGaussianBVHGPU(cloud_, &timings);
+        bvh = sah == 2 ? buildGaussianBVHSah4GPU(cloud_, &timings)
+              : sah ? buildGaussianBVHSahGPU(cloud_, &timings) : buildGaussianBVHGPU(cloud_, &timings);
         buildMs = timings.totalMs;
     }
 

@@ -226,3 +226,62 @@ def test_bad_inputs_raise_value_error(mesh):
     for call in bad:
         with pytest.raises(ValueError):
             call()
+
+
+def test_leaf_size_4_builder_through_the_module(mesh):
+    """builder="sah4" (engine addition): the leaf-size-4 SAH tree, whose 4-wide layer is the
+    leaf-range form, answers every query of every kind with the LBVH's bits, also after a
+    refit and a topology edit."""
+    v, i = mesh
+    base, s4 = quarry.Scene(v, i), quarry.Scene(v, i, builder="sah4")
+    assert s4.validate() == "" and s4.node_count == base.node_count
+    assert "sah_bin_ms" in s4.build_stats
+    lo, hi = np.array(base.bounds["min"]), np.array(base.bounds["max"])
+    rng = np.random.default_rng(21)
+    pts = (lo + (hi - lo) * rng.random((400, 3))).astype(np.float32)
+    radius = 0.2 * float(np.max(hi - lo))
+
+    def same(a, b, kw):
+        for fn in (lambda s: s.closest(pts, **kw), lambda s: s.knn(pts, 4, **kw),
+                   lambda s: s.radius(pts, radius, **kw)):
+            x, y = fn(a), fn(b)
+            for u, w in zip(x, y):
+                assert np.array_equal(np.ascontiguousarray(u).view(np.uint8),
+                                      np.ascontiguousarray(w).view(np.uint8)), kw
+
+    for kw in ({}, {"wide": True}, {"order": "coherent", "wide": True}):
+        same(s4, base, kw)
+    origins = (lo + (hi - lo) * rng.random((300, 3))).astype(np.float32)
+    origins[:, 1] = hi[1] + 1.0
+    dirs = rng.normal(size=(300, 3)).astype(np.float32)
+    dirs[:, 1] = -np.abs(dirs[:, 1]) - 0.5
+    for kw in ({}, {"wide": True}):
+        h1, t1 = s4.raycast(origins, dirs, **kw)
+        h0, t0 = base.raycast(origins, dirs)
+        assert np.array_equal(h1, h0) and np.array_equal(_bits(t1), _bits(t0))
+    lifted = v.copy()
+    lifted[:, 1] += np.float32(0.25)
+    s4.update_vertices(lifted)
+    base.update_vertices(lifted)
+    assert s4.validate() == ""
+    same(s4, base, {"wide": True})
+    pr = np.random.default_rng(5)
+    pc = (pr.random((5000, 3)) * 20).astype(np.float32)
+    c4, c0 = quarry.PointCloud(pc, builder="sah4"), quarry.PointCloud(pc)
+    q = (pr.random((300, 3)) * 20).astype(np.float32)
+    for kw in ({}, {"wide": True}):
+        a, b = c4.knn(q, 8, **kw), c0.knn(q, 8)
+        assert np.array_equal(_bits(a[0]), _bits(b[0])) and np.array_equal(a[1], b[1])
+    keep = np.ones(5000, bool)
+    keep[[3, 99, 4000]] = False
+    newp = np.concatenate([pc[keep], (pr.random((40, 3)) * 20).astype(np.float32)])
+    c4.update_topology(newp, deleted=np.array([3, 99, 4000], np.int32))
+    assert c4.validate() == ""
+    fresh = quarry.PointCloud(newp)
+    a, b = c4.closest(q, wide=True), fresh.closest(q)
+    assert np.array_equal(_bits(a[0]), _bits(b[0])) and np.array_equal(a[1], b[1])
+    m, r, s = quarry.demo_gaussians("sheet", 1500, seed=8)
+    g4, g0 = quarry.GaussianCloud(m, r, s, builder="sah4"), quarry.GaussianCloud(m, r, s)
+    gq = q * np.float32(0.1)
+    a, b = g4.closest(gq, wide=True), g0.closest(gq)
+    assert np.array_equal(_bits(a[0]), _bits(b[0])) and np.array_equal(a[1], b[1])

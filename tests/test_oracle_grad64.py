@@ -1,4 +1,4 @@
-"""The FP64 gradient references (oracle/grad64.py) checked on the CPU before they judge the
+"""The FP64 gradient references (oracle/grad64.py) checked on the CPU before they check the
 engine's adjoints: every analytic gradient against central differences of the FP64 functions
 themselves, with a step small enough (1e-6) that the difference's truncation error is far
 below the tolerance."""

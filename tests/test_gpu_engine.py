@@ -696,6 +696,31 @@ def test_sah4_tree_and_wide_leaf4(cuda, kind):
     same(tree)
 
 
+@pytest.mark.parametrize("n", [2, 3, 4, 5, 6, 9, 33, 257])
+def test_sah4_tiny_trees(cuda, n):
+    """Leaf-size-4 SAH trees small enough that the root, or most of the tree, is one leaf
+    range, with the leaf-range 4-wide layer: every query kind on binary, leaf4 and wide
+    traversal equals the oracle's."""
+    rng = np.random.default_rng(100 + n)
+    pts = rng.uniform(0, 1, (n, 3)).astype(np.float32)
+    tree = capi.DeviceTree("point", pts, builder="sah4")
+    assert tree.validate() == [0] * 8
+    tree.build_wide(leaf4=True)
+    assert tree.validate() == [0] * 8
+    ref = oracle.LBVH("point", pts)
+    qh = rng.uniform(-0.5, 1.5, (513, 3)).astype(np.float32)
+    q = _dev(qh)
+    k = min(n, 4)
+    for f in (0, capi.QK_TUNE_LEAF4, capi.QK_WIDE, capi.QK_WIDE | capi.QK_ORDER_MORTON,
+              capi.QK_TUNE_SPLIT4):
+        assert np.array_equal(tree.closest(q, f).cpu().numpy().view(np.uint32), ref.closest(qh)), f
+        assert np.array_equal(tree.knn(q, k, f).cpu().numpy().view(np.uint32), ref.knn(qh, k)), f
+        off, keys = tree.radius(q, 0.4, f)
+        woff, wkeys = ref.radius(qh, 0.4)
+        assert np.array_equal(off.cpu().numpy().astype(np.int64), woff), f
+        assert np.array_equal(keys.cpu().numpy().view(np.uint64), wkeys), f
+
+
 def test_split_knn_sphere_matches_oracle(cuda):
     pts = workloads.point_cloud("surface", 100_000, 2)
     q = workloads.uniform_points(2_000, pts.min(0), pts.max(0), 2, 13)

@@ -189,6 +189,36 @@ def test_degenerate_rays_every_ray_path(cuda):
             assert np.array_equal(got, want), (builder, flags, int((got != want).sum()))
 
 
+def test_ordered_raycast_captures_in_a_cuda_graph(cuda):
+    """The ordering passes and the traversal after them launch with programmatic stream
+    serialization; captured into a CUDA graph and replayed they give the same bits."""
+    tris = scenes()["city"]
+    lo, hi = workloads.bounds_of(tris)
+    rays = _dev(workloads.cosine_rays(70_001, float(lo[0]), float(hi[0]), float(lo[1]),
+                                      float(hi[1]), float(hi[2]) + 5.0, 3))
+    tree = capi.DeviceTree("tri", tris, builder="sah")
+    for flags in (capi.QK_ORDER_COHERENT | capi.QK_TUNE_HIGH_OCC, capi.QK_ORDER_COHERENT,
+                  capi.QK_ORDER_MORTON | capi.QK_TUNE_HIGH_OCC):
+        want = tree.raycast(rays, 0).clone()
+        out = cuda.empty_like(want)
+        ws = cuda.empty(capi.lib().qk_query_workspace_bytes(rays.shape[0], flags),
+                        dtype=cuda.uint8, device="cuda")
+        side = cuda.cuda.Stream()
+        side.wait_stream(cuda.cuda.current_stream())
+        with cuda.cuda.stream(side):
+            tree.raycast(rays, flags, out=out, ws=ws)  # warm-up outside the capture
+        cuda.cuda.current_stream().wait_stream(side)
+        g = cuda.cuda.CUDAGraph()
+        out.zero_()
+        with cuda.cuda.graph(g):
+            tree.raycast(rays, flags, out=out, ws=ws)
+        for _ in range(3):
+            out.zero_()
+            g.replay()
+            cuda.cuda.synchronize()
+            assert cuda.equal(out, want), flags
+
+
 def test_raycast_stats_and_no_overflow(cuda):
     tris = scenes()["terrain"]
     tree = capi.DeviceTree("tri", tris)

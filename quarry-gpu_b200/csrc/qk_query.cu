@@ -796,8 +796,8 @@ __global__ __launch_bounds__(kBlock) void k_closest_split(const BNode* __restric
                                                          int max_iter,
                                                          unsigned long long* __restrict__ stats,
                                                          TailList tail = TailList{}) {
-    if (G == 32 && static_cast<long long>(blockIdx.x * kBlock + threadIdx.x) / 32 >= count)
-        return;  // whole warps
+    if (static_cast<long long>(blockIdx.x * kBlock + (threadIdx.x & ~31u)) / G >= count)
+        return;  // whole warps past the last query
     bool valid;
     int lane;
     const int q = split_query<G>(count, order, valid, lane);
@@ -807,7 +807,8 @@ __global__ __launch_bounds__(kBlock) void k_closest_split(const BNode* __restric
     if (valid && lane == 0) out[q] = r;
     const bool ovf = group_any<G>(tv.overflow);
     if (tail.count && valid && ovf && lane == 0) tail_append(tail, q);
-    flush_stats<kStats>(valid, tv.nodes, tv.leaves, tv.overflow, stats);
+    // a group past the last query traced query 0: it counts nothing
+    flush_stats<kStats>(valid, valid ? tv.nodes : 0, valid ? tv.leaves : 0, valid && tv.overflow, stats);
 }
 
 template <class Ops, bool kStats, int G>
@@ -819,8 +820,8 @@ __global__ __launch_bounds__(kBlock) void k_knn_split(const BNode* __restrict__ 
                                                      uint2* __restrict__ out, int max_iter,
                                                      unsigned long long* __restrict__ stats,
                                                      TailList tail = TailList{}) {
-    if (G == 32 && static_cast<long long>(blockIdx.x * kBlock + threadIdx.x) / 32 >= count)
-        return;  // whole warps
+    if (static_cast<long long>(blockIdx.x * kBlock + (threadIdx.x & ~31u)) / G >= count)
+        return;  // whole warps past the last query
     bool valid;
     int lane;
     const int q = split_query<G>(count, order, valid, lane);
@@ -831,7 +832,8 @@ __global__ __launch_bounds__(kBlock) void k_knn_split(const BNode* __restrict__ 
     if (valid && lane < k) out[static_cast<size_t>(q) * stride + lane] = warp_table_entry(tab);
     const bool ovf = group_any<G>(tv.overflow);
     if (tail.count && valid && ovf && lane == 0) tail_append(tail, q);
-    flush_stats<kStats>(valid, tv.nodes, tv.leaves, tv.overflow, stats);
+    // a group past the last query traced query 0: it counts nothing
+    flush_stats<kStats>(valid, valid ? tv.nodes : 0, valid ? tv.leaves : 0, valid && tv.overflow, stats);
 }
 
 // The tail scan: block (tile, batch) runs heavy query base + batch x kTailBatch + t of the
@@ -934,8 +936,8 @@ __global__ __launch_bounds__(kBlock) void k_radius_split(
     const uint32_t* __restrict__ order, int count, float r2, int* __restrict__ counts,
     int* __restrict__ lane_counts, const int* __restrict__ offsets,
     unsigned long long* __restrict__ keys, int max_iter, unsigned long long* __restrict__ stats) {
-    if (G == 32 && static_cast<long long>(blockIdx.x * kBlock + threadIdx.x) / 32 >= count)
-        return;  // whole warps
+    if (static_cast<long long>(blockIdx.x * kBlock + (threadIdx.x & ~31u)) / G >= count)
+        return;  // whole warps past the last query
     bool valid;
     int lane;
     const int q = split_query<G>(count, order, valid, lane);
@@ -958,7 +960,8 @@ __global__ __launch_bounds__(kBlock) void k_radius_split(
             if (lane == 0) counts[q] = total;
         }
     }
-    flush_stats<kStats>(valid, tv.nodes, tv.leaves, tv.overflow, stats);
+    // a group past the last query traced query 0: it counts nothing
+    flush_stats<kStats>(valid, valid ? tv.nodes : 0, valid ? tv.leaves : 0, valid && tv.overflow, stats);
 }
 
 // ---- segment sort of the radius keys ----

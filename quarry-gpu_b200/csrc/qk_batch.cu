@@ -188,11 +188,14 @@ __global__ __launch_bounds__(kBlock) void k_bt_gather(const BScene* __restrict__
     }
 }
 
+// ranges: one int2 per primitive of the batch (scene s's internal nodes at prim_off(s)); the
+// emit writes every internal node's slot range (first, count)
 template <class Ops>
 __global__ __launch_bounds__(kBlock) void k_bt_emit(const BScene* __restrict__ tab,
                                                     const int2* __restrict__ chunks,
                                                     const uint32_t* __restrict__ codes_f,
-                                                    const uint32_t* __restrict__ ids_f) {
+                                                    const uint32_t* __restrict__ ids_f,
+                                                    int2* __restrict__ ranges) {
     const int2 ch = chunks[blockIdx.x];
     const BScene& sc = tab[ch.x];
     const qk_tree& t = sc.t;
@@ -202,22 +205,26 @@ __global__ __launch_bounds__(kBlock) void k_bt_emit(const BScene* __restrict__ t
         emit_slot<Ops>(sc.in, n, codes_f + sc.prim_off, ids_f + sc.prim_off,
                        static_cast<Node*>(t.nodes), static_cast<float*>(t.items), t.prim_ids,
                        t.slot_of, t.parent, static_cast<BNode*>(t.bnodes),
-                       static_cast<float4*>(t.leaves), t.flags, k);
+                       static_cast<float4*>(t.leaves), t.flags, k, ranges + sc.prim_off);
     }
 }
 
-// ranges: one int2 per primitive of the batch (scene s's internal nodes at prim_off(s))
+// Bottom-up boxes of every scene: a chunk's block starts the climbs at its kBuildChunk leaf
+// slots, and nodes whose range lies inside the chunk meet in shared memory (climb_ranged).
 __global__ __launch_bounds__(kBlock) void k_bt_bottom_up(const BScene* __restrict__ tab,
                                                          const int2* __restrict__ chunks,
-                                                         int2* __restrict__ ranges) {
+                                                         const int2* __restrict__ ranges) {
+    __shared__ int arrivals[kBuildChunk];
     const int2 ch = chunks[blockIdx.x];
     const BScene& sc = tab[ch.x];
     const qk_tree& t = sc.t;
     const int n = t.n;
     const int end = min(n, ch.y + kBuildChunk);
+    for (int i = threadIdx.x; i < kBuildChunk; i += kBlock) arrivals[i] = 0;
+    __syncthreads();
     for (int k = ch.y + threadIdx.x; k < end; k += kBlock)
-        climb(static_cast<Node*>(t.nodes), static_cast<BNode*>(t.bnodes), t.parent, t.flags, n, k,
-              ranges + sc.prim_off);
+        climb_ranged<kBuildChunk>(static_cast<Node*>(t.nodes), static_cast<BNode*>(t.bnodes),
+                                  t.parent, t.flags, n, k, ch.y, arrivals, ranges + sc.prim_off);
 }
 
 __global__ __launch_bounds__(kBlock) void k_bt_depth(const BScene* __restrict__ tab,
@@ -699,6 +706,11 @@ int check_counts(int kind, const int32_t* counts, int scenes, long long* total, 
     return QK_OK;
 }
 
+// uint32 elements between the five build buffers: 64-aligned, so each starts on 256 bytes
+size_t buf_stride(long long total) {
+    return (static_cast<size_t>(total) + 63) & ~static_cast<size_t>(63);
+}
+
 BatchLayout batch_layout(int kind, const int32_t* counts, int scenes, unsigned flags) {
     BatchLayout L;
     std::memset(&L, 0, sizeof(L));
@@ -733,7 +745,7 @@ BatchLayout batch_layout(int kind, const int32_t* counts, int scenes, unsigned f
     L.chunks = take(sizeof(int2) * nchunks);
     L.hdr = take(sizeof(Header) * scenes);
     L.prim_off = take(sizeof(int) * (scenes + 1));
-    L.bufs = take(sizeof(uint32_t) * n * 5);
+    L.bufs = take(sizeof(uint32_t) * buf_stride(n) * 5);
     L.sort_ws = take(sort_ws_bytes(static_cast<int>(n)));
     const long long span = static_cast<long long>(L.field_bytes[8] / sizeof(int));
     L.scan_ws = take((flags & QK_WIDE) ? scan_ws_bytes(static_cast<int>(span)) : 0);
@@ -764,9 +776,11 @@ int batch_build_impl(qk_batch* b, cudaStream_t s) {
     if (e != cudaSuccess) return cuda_status(e, "batch scene sort");
     // idx_f = codes_s; gather codes into codes, local ids into idx_s
     k_bt_gather<<<C, kBlock, 0, s>>>(b->d_tab, b->d_chunks, keep, codes_s, codes, idx_s);
-    k_bt_emit<Ops><<<C, kBlock, 0, s>>>(b->d_tab, b->d_chunks, codes, idx_s);
-    // the code buffers are free again: their 2N uint32 (256-byte aligned) hold N int2 ranges
-    k_bt_bottom_up<<<C, kBlock, 0, s>>>(b->d_tab, b->d_chunks, reinterpret_cast<int2*>(codes));
+    // keep and idx are free after the gather: their 2N uint32 (adjacent, 256-byte aligned) hold
+    // the N int2 slot ranges
+    int2* ranges = reinterpret_cast<int2*>(keep);
+    k_bt_emit<Ops><<<C, kBlock, 0, s>>>(b->d_tab, b->d_chunks, codes, idx_s, ranges);
+    k_bt_bottom_up<<<C, kBlock, 0, s>>>(b->d_tab, b->d_chunks, ranges);
     k_bt_depth<<<C, kBlock, 0, s>>>(b->d_tab, b->d_chunks, b->d_hdr);
     if (b->flags & QK_WIDE) {
         k_bt_wide_flags<<<C, kBlock, 0, s>>>(b->d_tab, b->d_chunks);
@@ -1097,7 +1111,8 @@ int qk_batch_create(qk_batch** out, int kind, const int32_t* counts, int scenes,
     b->d_hdr = reinterpret_cast<Header*>(base + L.hdr);
     b->d_prim_off = reinterpret_cast<int*>(base + L.prim_off);
     for (int i = 0; i < 5; ++i)
-        b->bufs[i] = reinterpret_cast<uint32_t*>(base + L.bufs) + static_cast<size_t>(i) * total;
+        b->bufs[i] = reinterpret_cast<uint32_t*>(base + L.bufs) +
+                     static_cast<size_t>(i) * buf_stride(total);
     b->sort_ws = base + L.sort_ws;
     b->scan_ws = base + L.scan_ws;
     b->single_ws = base + L.single_ws;

@@ -132,11 +132,8 @@ __global__ __launch_bounds__(kBlock) void k_ranges_descent(const Node* __restric
     ranges[v] = make_int2(first, last >= first ? last - first + 1 : 0);
 }
 
-// Bottom-up boxes with known slot ranges.  Block b's threads start at the leaves of slots
-// [256 b, 256 b + 256).  A node whose whole range lies in those slots has both children
-// finished by this block, so its two arrivals meet in a shared-memory counter (indexed by the
-// node's split gap, the last slot of its left child, unique per internal node) behind block
-// fences; only nodes spanning blocks take the device-scope counter in flags[].
+// Bottom-up boxes with known slot ranges: block b's threads start at the leaves of slots
+// [256 b, 256 b + 256) (climb_ranged in qk_build.cuh).
 __global__ __launch_bounds__(kBlock) void k_bottom_up_ranged(Node* __restrict__ nodes,
                                                             BNode* __restrict__ bnodes,
                                                             const int* __restrict__ parent,
@@ -148,32 +145,7 @@ __global__ __launch_bounds__(kBlock) void k_bottom_up_ranged(Node* __restrict__ 
     __syncthreads();
     const int k = base + threadIdx.x;
     if (k >= n) return;
-    int c = n - 1 + k;
-    int2 rc = make_int2(k, 1);
-    int p = parent[c];
-    for (int guard = 0; p >= 0 && guard < 4096; ++guard) {
-        const int2 rp = ranges[p];
-        const bool local = rp.x >= base && rp.x + rp.y <= base + kBlock;
-        int old;
-        if (local) {
-            const int gap = nodes[p].left == c ? rc.x + rc.y - 1 : rc.x - 1;
-            __threadfence_block();
-            old = atomicAdd(&arrivals[gap - base], 1);
-            __threadfence_block();
-        } else {
-            old = arrive_add(&flags[p], 1);
-        }
-        if (old == 0) return;
-        if (local) {
-            finish_node_ranged<true>(nodes, bnodes, p, n, ranges);
-        } else {
-            finish_node_ranged<false>(nodes, bnodes, p, n, ranges);
-            flags[p] = 0;
-        }
-        c = p;
-        rc = rp;
-        p = parent[p];
-    }
+    climb_ranged<kBlock>(nodes, bnodes, parent, flags, n, k, base, arrivals, ranges);
 }
 
 // One thread per leaf climbs toward the root (climb in qk_build.cuh).

@@ -204,6 +204,45 @@ __device__ __forceinline__ void climb(Node* __restrict__ nodes, BNode* __restric
     }
 }
 
+// One leaf's climb when every internal node's slot range is known (`ranges`).  The calling
+// block starts climbs at the leaves of slots [base, base + kSpan).  A node whose whole range
+// lies in those slots has both children finished by this block, so its two arrivals meet in
+// the shared counter arrivals[gap - base] (gap: the last slot of its left child, unique per
+// internal node) behind block fences; only nodes spanning blocks take the device-scope
+// counter in flags[], which the finishing arrival resets.
+template <int kSpan>
+__device__ __forceinline__ void climb_ranged(Node* __restrict__ nodes, BNode* __restrict__ bnodes,
+                                             const int* __restrict__ parent,
+                                             int* __restrict__ flags, int n, int k, int base,
+                                             int* arrivals, const int2* __restrict__ ranges) {
+    int c = n - 1 + k;
+    int2 rc = make_int2(k, 1);
+    int p = parent[c];
+    for (int guard = 0; p >= 0 && guard < 4096; ++guard) {
+        const int2 rp = ranges[p];
+        const bool local = rp.x >= base && rp.x + rp.y <= base + kSpan;
+        int old;
+        if (local) {
+            const int gap = nodes[p].left == c ? rc.x + rc.y - 1 : rc.x - 1;
+            __threadfence_block();
+            old = atomicAdd(&arrivals[gap - base], 1);
+            __threadfence_block();
+        } else {
+            old = arrive_add(&flags[p], 1);
+        }
+        if (old == 0) return;
+        if (local) {
+            finish_node_ranged<true>(nodes, bnodes, p, n, ranges);
+        } else {
+            finish_node_ranged<false>(nodes, bnodes, p, n, ranges);
+            flags[p] = 0;
+        }
+        c = p;
+        rc = rp;
+        p = parent[p];
+    }
+}
+
 // depth of node i = length of its parent chain (lbvh.cu:419-431), bounded by `limit`
 __device__ __forceinline__ int chain_depth(const int* __restrict__ parent, int i, int limit) {
     int d = 0;

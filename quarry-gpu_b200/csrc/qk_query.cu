@@ -1025,36 +1025,117 @@ __device__ __forceinline__ void bitonic_pair(int t, int size, int stride, int& i
     }
 }
 
-// one warp per listed segment of 33..kWarpSortMax keys, sorted in the warp's shared memory
-// (only warp barriers between stages)
-__global__ __launch_bounds__(kWarpSortBlock) void k_seg_sort_warp_smem(
+// Bitonic sort of 32 E keys held by one warp in registers, striped: key i sits in lane i % 32,
+// register i / 32.  The same all-ascending network as cswap's: for each size, the flip
+// comparator (i, i ^ (size - 1)), then (i, i ^ stride) for shrinking strides, smaller key to
+// the lower index.  Partners 32 or more apart share a lane (register pairs); nearer ones share
+// a register (lane shuffles).  The stage loops stay rolled (the unrolled network of 1024 keys
+// is far larger than the instruction cache); register indices are constants inside each
+// stage body, which a compile-time chain picks by the stage's register distance.
+
+// flip stage of size 64 B: key (r, lane) against (r ^ (2 B - 1), lane ^ 31), the lower key
+// having bit B of r clear
+template <int E, int B>
+__device__ __forceinline__ void bitonic_flip_regs(unsigned long long (&v)[E]) {
+#pragma unroll
+    for (int r = 0; r < E; ++r) {
+        if (r & B) continue;
+        const int rp = r ^ (2 * B - 1);
+        const unsigned long long a = __shfl_xor_sync(0xffffffffu, v[rp], 31);
+        const unsigned long long b = __shfl_xor_sync(0xffffffffu, v[r], 31);
+        v[r] = a < v[r] ? a : v[r];
+        v[rp] = b > v[rp] ? b : v[rp];
+    }
+}
+
+// stride 32 S: key (r, lane) against (r ^ S, lane), inside each lane
+template <int E, int S>
+__device__ __forceinline__ void bitonic_pair_regs(unsigned long long (&v)[E]) {
+#pragma unroll
+    for (int r = 0; r < E; ++r) {
+        if (r & S) continue;
+        const unsigned long long x = v[r], y = v[r ^ S];
+        v[r] = y < x ? y : x;
+        v[r ^ S] = y < x ? x : y;
+    }
+}
+
+template <int E, int B = 1>
+__device__ __forceinline__ void bitonic_flip_at(unsigned long long (&v)[E], int b) {
+    if constexpr (B < E) {
+        if (b == B) bitonic_flip_regs<E, B>(v);
+        else bitonic_flip_at<E, 2 * B>(v, b);
+    }
+}
+
+template <int E, int S = 1>
+__device__ __forceinline__ void bitonic_pair_at(unsigned long long (&v)[E], int s) {
+    if constexpr (S < E) {
+        if (s == S) bitonic_pair_regs<E, S>(v);
+        else bitonic_pair_at<E, 2 * S>(v, s);
+    }
+}
+
+template <int E>
+__device__ __forceinline__ void warp_bitonic(unsigned long long (&v)[E], int lane) {
+#pragma unroll 1
+    for (int size = 2; size <= 32 * E; size <<= 1) {
+        int stride = size >> 1;
+        if (size > 32) {
+            bitonic_flip_at<E>(v, size / 64);
+#pragma unroll 1
+            for (stride = size >> 2; stride >= 32; stride >>= 1) bitonic_pair_at<E>(v, stride / 32);
+        }
+        // strides below 32: lane ^ (size - 1) for the flip of a size up to 32, else lane ^ stride
+#pragma unroll 1
+        for (; stride > 0; stride >>= 1) {
+            const int lx = stride == (size >> 1) ? size - 1 : stride;
+            const bool lower = (lane & stride) == 0;
+#pragma unroll
+            for (int r = 0; r < E; ++r) {
+                const unsigned long long o = __shfl_xor_sync(0xffffffffu, v[r], lx);
+                v[r] = lower ? (o < v[r] ? o : v[r]) : (o > v[r] ? o : v[r]);
+            }
+        }
+    }
+}
+
+// one segment of m (<= 32 E) keys at keys[b..b+m): coalesced striped loads, padded with the
+// largest 64-bit value (which sorts after, or ties with, every real key), sorted in registers
+template <int E>
+__device__ __forceinline__ void warp_sort_segment(unsigned long long* __restrict__ keys, int b,
+                                                  int m, int lane) {
+    unsigned long long v[E];
+#pragma unroll
+    for (int r = 0; r < E; ++r) {
+        const int i = r * 32 + lane;
+        v[r] = i < m ? keys[b + i] : ~0ull;
+    }
+    warp_bitonic<E>(v, lane);
+#pragma unroll
+    for (int r = 0; r < E; ++r) {
+        const int i = r * 32 + lane;
+        if (i < m) keys[b + i] = v[r];
+    }
+}
+
+// one warp per listed segment of 33..kWarpSortMax keys, sorted in registers (the smallest
+// power-of-two network that holds the segment)
+__global__ __launch_bounds__(kWarpSortBlock) void k_seg_sort_warp_reg(
     const int* __restrict__ offsets, unsigned long long* __restrict__ keys,
     const int* __restrict__ list, const Header* __restrict__ h) {
-    __shared__ unsigned long long sm[kWarpSortBlock / 32][kWarpSortMax];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    unsigned long long* a = sm[w];
     const int n_list = h->list_count[0];
     const int warps = gridDim.x * (kWarpSortBlock / 32);
     for (int e = blockIdx.x * (kWarpSortBlock / 32) + w; e < n_list; e += warps) {
         const int q = list[e];
         const int b = offsets[q];
         const int m = min(offsets[q + 1] - b, kWarpSortMax);
-        for (int t = lane; t < m; t += 32) a[t] = keys[b + t];
-        int pow2 = 32;
-        while (pow2 < m) pow2 <<= 1;
-        __syncwarp();
-        for (int size = 2; size <= pow2; size <<= 1) {
-            for (int stride = size >> 1; stride > 0; stride >>= 1) {
-                for (int t = lane; t < pow2 / 2; t += 32) {
-                    int i, j;
-                    bitonic_pair(t, size, stride, i, j);
-                    if (i < m) cswap(a, i, j, m);
-                }
-                __syncwarp();
-            }
-        }
-        for (int t = lane; t < m; t += 32) keys[b + t] = a[t];
-        __syncwarp();
+        if (m <= 64) warp_sort_segment<2>(keys, b, m, lane);
+        else if (m <= 128) warp_sort_segment<4>(keys, b, m, lane);
+        else if (m <= 256) warp_sort_segment<8>(keys, b, m, lane);
+        else if (m <= 512) warp_sort_segment<16>(keys, b, m, lane);
+        else warp_sort_segment<32>(keys, b, m, lane);
     }
 }
 
@@ -1654,11 +1735,8 @@ int radius_fill(const qk_tree* t, const float* pts, int count, float r, const in
     }
     const uint32_t* order = make_order(pts, 3, 0, count, flags, o, s, &st);
     if (st != QK_OK) return st;
-    if (false)
-        ;
-    else
-        st = radius_dispatch<true>(t, pts, count, r * r, nullptr, lane_counts, offsets, k64, flags,
-                                   nullptr, order, s);
+    st = radius_dispatch<true>(t, pts, count, r * r, nullptr, lane_counts, offsets, k64, flags,
+                               nullptr, order, s);
     if (st != QK_OK) return st;
     // reset the segment lists (make_order only resets them on its Morton path)
     return radius_sort_segments(offsets, count, keys, medium, large, o.h, -1, s);
@@ -1670,7 +1748,7 @@ int radius_sort_segments(const int* offsets, int count, uint64_t* keys, int* med
     k_bounds_reset<<<1, 32, 0, s>>>(h, 0);
     k_seg_sort_warp<<<blocks_for(count, kBlock / 32), kBlock, 0, s>>>(offsets, count, k64, medium,
                                                                       large, h, cap);
-    k_seg_sort_warp_smem<<<148 * 8, kWarpSortBlock, 0, s>>>(offsets, k64, medium, h);
+    k_seg_sort_warp_reg<<<148 * 8, kWarpSortBlock, 0, s>>>(offsets, k64, medium, h);
     k_seg_sort_block<<<148 * 2, kBlock, 0, s>>>(offsets, k64, large, h);
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? QK_OK : cuda_status(e, "radius sort");

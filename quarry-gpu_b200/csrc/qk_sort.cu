@@ -9,8 +9,10 @@
 //   downsweep  each warp ranks its 512 keys in input order: __match_any_sync groups lanes
 //              holding the same digit, the rank inside a round is the popcount of lower
 //              peers, and a per-warp running count carries ranks across rounds; warps are
-//              then offset by an exclusive prefix over the per-warp counts.  Equal digits
-//              keep their input order, so the sort is stable.
+//              then offset by an exclusive prefix over the per-warp counts.  The tile is
+//              laid out in digit order in shared memory, and consecutive threads write
+//              consecutive slots of each digit's run (coalesced stores).  Equal digits keep
+//              their input order, so the sort is stable.
 // Stability makes sorting (morton, index) pairs on the 30 Morton bits alone equal to the
 // reference's full 64-bit sort of (morton << 32 | index) keys (src/gpu/lbvh.cu:1995-2003).
 #include "qk_internal.cuh"
@@ -24,86 +26,7 @@ constexpr int kWarps = kBlock / 32;
 constexpr int kItems = kSortTile / kBlock;  // 16 keys per thread
 static_assert(kItems * kBlock == kSortTile, "tile size");
 
-__global__ __launch_bounds__(kBlock) void k_rs_upsweep(const uint32_t* __restrict__ keys, int n,
-                                                       int shift, uint32_t* __restrict__ hist,
-                                                       int tiles) {
-    __shared__ uint32_t wh[kWarps][kRadix];
-    const int warp = threadIdx.x >> 5;
-    for (int i = threadIdx.x; i < kWarps * kRadix; i += kBlock) (&wh[0][0])[i] = 0;
-    __syncthreads();
-    const int tile = blockIdx.x;
-    const int base = tile * kSortTile;
-#pragma unroll 4
-    for (int j = 0; j < kItems; ++j) {
-        const int idx = base + j * kBlock + threadIdx.x;
-        if (idx < n) atomicAdd(&wh[warp][(keys[idx] >> shift) & 0xffu], 1u);
-    }
-    __syncthreads();
-    for (int d = threadIdx.x; d < kRadix; d += kBlock) {
-        uint32_t s = 0;
-#pragma unroll
-        for (int w = 0; w < kWarps; ++w) s += wh[w][d];
-        hist[static_cast<size_t>(d) * tiles + tile] = s;
-    }
-}
-
-__global__ __launch_bounds__(kBlock) void k_rs_downsweep(
-    const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin, uint32_t* __restrict__ kout,
-    uint32_t* __restrict__ vout, int n, int shift, const uint32_t* __restrict__ hist, int tiles) {
-    __shared__ uint32_t wcount[kWarps][kRadix];
-    __shared__ uint32_t gbase[kRadix];
-    const int lane = threadIdx.x & 31;
-    const int warp = threadIdx.x >> 5;
-    for (int i = threadIdx.x; i < kWarps * kRadix; i += kBlock) (&wcount[0][0])[i] = 0;
-    const int tile = blockIdx.x;
-    for (int d = threadIdx.x; d < kRadix; d += kBlock) {
-        gbase[d] = hist[static_cast<size_t>(d) * tiles + tile];
-    }
-    __syncthreads();
-
-    const int wbase = tile * kSortTile + warp * (kSortTile / kWarps);
-    const unsigned lower = (1u << lane) - 1u;
-    uint32_t key[kItems], val[kItems];
-    uint16_t rank[kItems];
-#pragma unroll
-    for (int j = 0; j < kItems; ++j) {
-        const int idx = wbase + j * 32 + lane;
-        const bool ok = idx < n;
-        key[j] = ok ? kin[idx] : 0u;
-        val[j] = ok ? vin[idx] : 0u;
-        const uint32_t d = ok ? ((key[j] >> shift) & 0xffu) : 0x100u;
-        const unsigned peers = __match_any_sync(0xffffffffu, d);
-        const uint32_t before = ok ? wcount[warp][d] : 0u;
-        __syncwarp();
-        if (ok && lane == __ffs(peers) - 1) wcount[warp][d] = before + __popc(peers);
-        __syncwarp();
-        rank[j] = static_cast<uint16_t>(before + __popc(peers & lower));
-    }
-    __syncthreads();
-    // exclusive prefix over warps, per digit
-    for (int d = threadIdx.x; d < kRadix; d += kBlock) {
-        uint32_t run = gbase[d];
-#pragma unroll
-        for (int w = 0; w < kWarps; ++w) {
-            const uint32_t c = wcount[w][d];
-            wcount[w][d] = run;
-            run += c;
-        }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int j = 0; j < kItems; ++j) {
-        const int idx = wbase + j * 32 + lane;
-        if (idx < n) {
-            const uint32_t d = (key[j] >> shift) & 0xffu;
-            const uint32_t dst = wcount[warp][d] + rank[j];
-            kout[dst] = key[j];
-            vout[dst] = val[j];
-        }
-    }
-}
-
-// ---- exclusive scan: block-local scans, a scan of the block sums, then a fix-up ----
+// ---- warp and block scans (the sort's digit runs and the exclusive scan below) ----
 __device__ __forceinline__ int warp_incl_scan(int v) {
     const int lane = threadIdx.x & 31;
 #pragma unroll
@@ -133,6 +56,106 @@ __device__ __forceinline__ int block_excl_scan(int v, int* total) {
     return wprefix + inc - v;
 }
 
+__global__ __launch_bounds__(kBlock) void k_rs_upsweep(const uint32_t* __restrict__ keys, int n,
+                                                       int shift, uint32_t* __restrict__ hist,
+                                                       int tiles) {
+    __shared__ uint32_t wh[kWarps][kRadix];
+    const int warp = threadIdx.x >> 5;
+    for (int i = threadIdx.x; i < kWarps * kRadix; i += kBlock) (&wh[0][0])[i] = 0;
+    __syncthreads();
+    const int tile = blockIdx.x;
+    const int base = tile * kSortTile;
+#pragma unroll 4
+    for (int j = 0; j < kItems; ++j) {
+        const int idx = base + j * kBlock + threadIdx.x;
+        if (idx < n) atomicAdd(&wh[warp][(keys[idx] >> shift) & 0xffu], 1u);
+    }
+    __syncthreads();
+    for (int d = threadIdx.x; d < kRadix; d += kBlock) {
+        uint32_t s = 0;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) s += wh[w][d];
+        hist[static_cast<size_t>(d) * tiles + tile] = s;
+    }
+}
+
+__global__ __launch_bounds__(kBlock) void k_rs_downsweep(
+    const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin, uint32_t* __restrict__ kout,
+    uint32_t* __restrict__ vout, int n, int shift, const uint32_t* __restrict__ hist, int tiles) {
+    __shared__ uint32_t wcount[kWarps][kRadix];
+    __shared__ uint32_t gbase[kRadix];
+    __shared__ uint32_t lstart[kRadix];
+    __shared__ uint32_t skey[kSortTile];
+    __shared__ uint32_t sval[kSortTile];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    for (int i = threadIdx.x; i < kWarps * kRadix; i += kBlock) (&wcount[0][0])[i] = 0;
+    const int tile = blockIdx.x;
+    for (int d = threadIdx.x; d < kRadix; d += kBlock) {
+        gbase[d] = hist[static_cast<size_t>(d) * tiles + tile];
+    }
+    __syncthreads();
+
+    const int wbase = tile * kSortTile + warp * (kSortTile / kWarps);
+    const unsigned lower = (1u << lane) - 1u;
+    uint32_t key[kItems], val[kItems];
+    uint16_t rank[kItems];
+#pragma unroll
+    for (int j = 0; j < kItems; ++j) {
+        const int idx = wbase + j * 32 + lane;
+        const bool ok = idx < n;
+        key[j] = ok ? kin[idx] : 0u;
+        val[j] = ok ? vin[idx] : 0u;
+        const uint32_t d = ok ? ((key[j] >> shift) & 0xffu) : 0x100u;
+        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        const uint32_t before = ok ? wcount[warp][d] : 0u;
+        __syncwarp();
+        if (ok && lane == __ffs(peers) - 1) wcount[warp][d] = before + __popc(peers);
+        __syncwarp();
+        rank[j] = static_cast<uint16_t>(before + __popc(peers & lower));
+    }
+    __syncthreads();
+    // per digit: the tile's count, its run's start inside the tile (a block scan over the
+    // digits) and every warp's offset inside that run
+    static_assert(kRadix == kBlock, "one thread per digit");
+    {
+        const int d = threadIdx.x;
+        uint32_t run = 0;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) {
+            const uint32_t c = wcount[w][d];
+            wcount[w][d] = run;
+            run += c;
+        }
+        int total;
+        lstart[d] = static_cast<uint32_t>(block_excl_scan(static_cast<int>(run), &total));
+    }
+    __syncthreads();
+    // the tile in digit order in shared memory (stable: warps, then items, then lanes)
+#pragma unroll
+    for (int j = 0; j < kItems; ++j) {
+        const int idx = wbase + j * 32 + lane;
+        if (idx < n) {
+            const uint32_t d = (key[j] >> shift) & 0xffu;
+            const uint32_t at = lstart[d] + wcount[warp][d] + rank[j];
+            skey[at] = key[j];
+            sval[at] = val[j];
+        }
+    }
+    __syncthreads();
+    // consecutive threads write consecutive slots of one digit's run
+    const int m = min(kSortTile, n - tile * kSortTile);
+#pragma unroll 4
+    for (int i = threadIdx.x; i < m; i += kBlock) {
+        const uint32_t k = skey[i];
+        const uint32_t d = (k >> shift) & 0xffu;
+        const uint32_t dst = gbase[d] + (static_cast<uint32_t>(i) - lstart[d]);
+        kout[dst] = k;
+        vout[dst] = sval[i];
+    }
+}
+
+// ---- exclusive scan: block-local scans, a scan of the block sums, then a fix-up ----
 // in and out may alias: each thread reads its own four elements before any write
 __global__ __launch_bounds__(kBlock) void k_scan_blocks(const int* in, int* out, int n,
                                                         int* __restrict__ sums) {

@@ -227,28 +227,49 @@ __global__ __launch_bounds__(kBlock) void k_bt_bottom_up(const BScene* __restric
                                   t.parent, t.flags, n, k, ch.y, arrivals, ranges + sc.prim_off);
 }
 
+// depths in two passes, as the single-tree build (anchored_depth in qk_build.cuh): the
+// anchors of every chunk's internal nodes, then every other node and each scene's maximum
+__global__ __launch_bounds__(kBlock) void k_bt_depth_anchors(const BScene* __restrict__ tab,
+                                                             const int2* __restrict__ chunks,
+                                                             const int2* __restrict__ ranges_all) {
+    const int2 ch = chunks[blockIdx.x];
+    const BScene& sc = tab[ch.x];
+    const qk_tree& t = sc.t;
+    const int n = t.n;
+    const int2* ranges = ranges_all + sc.prim_off;
+    const int end = min(n - 1, ch.y + kBuildChunk);
+    for (int k = ch.y + threadIdx.x; k < end; k += kBlock)
+        if (depth_anchor(ranges, k, n)) t.depth_arr[k] = chain_depth(t.parent, k, 2 * n - 1);
+}
+
 __global__ __launch_bounds__(kBlock) void k_bt_depth(const BScene* __restrict__ tab,
                                                      const int2* __restrict__ chunks,
+                                                     const int2* __restrict__ ranges_all,
                                                      Header* __restrict__ hdr) {
     const int2 ch = chunks[blockIdx.x];
-    const qk_tree& t = tab[ch.x].t;
+    const BScene& sc = tab[ch.x];
+    const qk_tree& t = sc.t;
     const int n = t.n;
     const int m = 2 * n - 1;
+    const int2* ranges = ranges_all + sc.prim_off;
     const int end = min(n, ch.y + kBuildChunk);
     int dmax = 0;
     for (int k = ch.y + threadIdx.x; k < end; k += kBlock) {
         if (k < n - 1) {
-            const int d = chain_depth(t.parent, k, m);
-            t.depth_arr[k] = d;
+            int d;
+            if (depth_anchor(ranges, k, n)) {
+                d = t.depth_arr[k];
+            } else {
+                d = anchored_depth(t.parent, ranges, t.depth_arr, n, k, m);
+                t.depth_arr[k] = d;
+            }
             dmax = max(dmax, d);
         }
-        const int d = chain_depth(t.parent, n - 1 + k, m);
+        const int d = anchored_depth(t.parent, ranges, t.depth_arr, n, n - 1 + k, m);
         t.depth_arr[n - 1 + k] = d;
         dmax = max(dmax, d);
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) dmax = max(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
-    if ((threadIdx.x & 31) == 0 && dmax > 0) atomicMax(&hdr[ch.x].max_depth, dmax);
+    block_max_to(dmax, &hdr[ch.x].max_depth);
 }
 
 __global__ __launch_bounds__(kBlock) void k_bt_wide_flags(const BScene* __restrict__ tab,
@@ -781,7 +802,8 @@ int batch_build_impl(qk_batch* b, cudaStream_t s) {
     int2* ranges = reinterpret_cast<int2*>(keep);
     k_bt_emit<Ops><<<C, kBlock, 0, s>>>(b->d_tab, b->d_chunks, codes, idx_s, ranges);
     k_bt_bottom_up<<<C, kBlock, 0, s>>>(b->d_tab, b->d_chunks, ranges);
-    k_bt_depth<<<C, kBlock, 0, s>>>(b->d_tab, b->d_chunks, b->d_hdr);
+    k_bt_depth_anchors<<<C, kBlock, 0, s>>>(b->d_tab, b->d_chunks, ranges);
+    k_bt_depth<<<C, kBlock, 0, s>>>(b->d_tab, b->d_chunks, ranges, b->d_hdr);
     if (b->flags & QK_WIDE) {
         k_bt_wide_flags<<<C, kBlock, 0, s>>>(b->d_tab, b->d_chunks);
         e = scan_exclusive(b->flags_field, b->wide_id_field, static_cast<int>(b->flag_span), false,

@@ -159,18 +159,30 @@ __global__ __launch_bounds__(kBlock) void k_bottom_up(Node* __restrict__ nodes,
     climb(nodes, bnodes, parent, flags, n, k, ranges);
 }
 
-// depth = length of the parent chain (lbvh.cu:419-431); bounded by the node count
-__global__ __launch_bounds__(kBlock) void k_depth(const int* __restrict__ parent, int count,
+// depth = length of the parent chain (lbvh.cu:419-431), bounded by the node count: the
+// anchors' first (anchored_depth in qk_build.cuh), then every other node's and the maximum
+__global__ __launch_bounds__(kBlock) void k_depth_anchors(const int* __restrict__ parent,
+                                                         const int2* __restrict__ ranges, int n,
+                                                         int* __restrict__ depth) {
+    const int i = blockIdx.x * kBlock + threadIdx.x;
+    if (i < n - 1 && depth_anchor(ranges, i, n)) depth[i] = chain_depth(parent, i, 2 * n - 1);
+}
+
+__global__ __launch_bounds__(kBlock) void k_depth(const int* __restrict__ parent,
+                                                 const int2* __restrict__ ranges, int n,
                                                  int* __restrict__ depth, Header* __restrict__ h) {
     const int i = blockIdx.x * kBlock + threadIdx.x;
+    const int count = 2 * n - 1;
     int d = 0;
     if (i < count) {
-        d = chain_depth(parent, i, count);
-        depth[i] = d;
+        if (depth_anchor(ranges, i, n)) {
+            d = depth[i];
+        } else {
+            d = anchored_depth(parent, ranges, depth, n, i, count);
+            depth[i] = d;
+        }
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) d = max(d, __shfl_xor_sync(0xffffffffu, d, o));
-    if ((threadIdx.x & 31) == 0 && d > 0) atomicMax(&h->max_depth, d);
+    block_max_to(d, &h->max_depth);
 }
 
 // ---- refit ----
@@ -452,7 +464,8 @@ int finish_tree(qk_tree* t, Header* h, int2* ranges, bool ranges_ready, cudaStre
                                                         t->parent, t->flags, n, ranges);
     stage_mark(kMarkBoxes, s);
     cudaMemsetAsync(&h->max_depth, 0, sizeof(int), s);
-    k_depth<<<blocks_for(2 * n - 1), kBlock, 0, s>>>(t->parent, 2 * n - 1, t->depth_arr, h);
+    k_depth_anchors<<<blocks_for(n - 1), kBlock, 0, s>>>(t->parent, ranges, n, t->depth_arr);
+    k_depth<<<blocks_for(2 * n - 1), kBlock, 0, s>>>(t->parent, ranges, n, t->depth_arr, h);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_status(e, "tree boxes");
     int depth = 0;

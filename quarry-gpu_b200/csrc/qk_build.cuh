@@ -254,6 +254,47 @@ __device__ __forceinline__ int chain_depth(const int* __restrict__ parent, int i
     return d;
 }
 
+// Depths in two passes.  Anchors, the internal nodes of at least kDepthAnchor leaves (a few
+// per kDepthAnchor leaves, all near the root), walk their whole parent chain; every other node
+// walks only up to its nearest anchor ancestor (a few steps: leaf counts grow toward the root)
+// and adds that anchor's depth.  `ranges` holds each internal node's (first slot, leaves).
+constexpr int kDepthAnchor = 64;
+
+__device__ __forceinline__ bool depth_anchor(const int2* __restrict__ ranges, int i, int n) {
+    return i < n - 1 && ranges[i].y >= kDepthAnchor;
+}
+
+// atomicMax of the block's largest v into *dst, one atomic per block (one per warp on a single
+// address serialises in its L2 slice)
+__device__ __forceinline__ void block_max_to(int v, int* dst) {
+    __shared__ int wmax[kBlock / 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int m = wmax[0];
+#pragma unroll
+        for (int w = 1; w < kBlock / 32; ++w) m = max(m, wmax[w]);
+        if (m > 0) atomicMax(dst, m);
+    }
+}
+
+// depth of a node that is not an anchor (anchors' depths already in `depth`)
+__device__ __forceinline__ int anchored_depth(const int* __restrict__ parent,
+                                              const int2* __restrict__ ranges,
+                                              const int* __restrict__ depth, int n, int i,
+                                              int limit) {
+    int d = 0;
+    int p = i;
+    while (p > 0 && d < limit) {
+        p = parent[p];
+        ++d;
+        if (depth_anchor(ranges, p, n)) return d + depth[p];
+    }
+    return d;
+}
+
 __device__ __forceinline__ void wide_fill(WideEntry& e, const Node& src, int child) {
     e.mn[0] = src.mn[0];
     e.mn[1] = src.mn[1];

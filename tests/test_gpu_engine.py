@@ -785,15 +785,17 @@ def test_radius_stash_same_csr(cuda, kind):
 
 
 def test_radius_segment_sizes_all_sort_paths(cuda):
-    """Segments of 0..32 keys (warp registers), 33..1024 (warp shared memory), 1025..4096
-    (block shared memory) and more (block, global memory) all come out sorted as the oracle's."""
+    """Segments of 0..32 keys (warp registers), 33..1024 (one warp, 32 E keys in registers
+    for E = 2, 4, 8, 16, 32: every class occurs), 1025..4096 (block shared memory) and more
+    (block, global memory) all come out sorted as the oracle's."""
     rng = np.random.default_rng(21)
     pts = rng.uniform(0, 4, (60_000, 3)).astype(np.float32)
     q = rng.uniform(0.5, 3.5, (400, 3)).astype(np.float32)
     tree = capi.DeviceTree("point", pts)
     ref = oracle.LBVH("point", pts)
     dq = _dev(q)
-    for r in (0.15, 0.4, 0.75, 1.1):
+    classes = set()
+    for r in (0.15, 0.25, 0.3, 0.4, 0.55, 0.75, 1.1):
         want_off, want_keys = ref.radius(q, r)
         sizes = np.diff(want_off)
         for flags in (0, capi.QK_TUNE_SPLIT, capi.QK_ORDER_MORTON, capi.QK_TUNE_STASH,
@@ -801,12 +803,13 @@ def test_radius_segment_sizes_all_sort_paths(cuda):
             off, keys = tree.radius(dq, r, flags)
             assert np.array_equal(off.cpu().numpy().astype(np.int64), want_off)
             assert np.array_equal(keys.cpu().numpy().view(np.uint64), want_keys), (r, flags)
+        medium = sizes[(sizes > 32) & (sizes <= 1024)]
+        classes |= {int(np.ceil(np.log2(m / 32))) for m in medium}
         if r == 1.1:
             assert sizes.max() > 4096
-        if r == 0.4:
-            assert ((sizes > 32) & (sizes <= 1024)).any()
         if r == 0.75:
             assert ((sizes > 1024) & (sizes <= 4096)).any()
+    assert classes == {1, 2, 3, 4, 5}
 
 
 def test_point_tail_same_results(cuda):

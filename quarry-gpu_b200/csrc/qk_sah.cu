@@ -33,6 +33,7 @@ constexpr int kTaskRange = 256;    // largest range the global tier hands to one
 constexpr int kWarpRange = 32;     // largest range finished by one warp
 constexpr int kMaxBins = 64;
 constexpr int kMaxDepth = 62;
+constexpr int kLevelsPerSync = 4;  // global-tier levels between host read-backs
 constexpr int kBinWords = 7;       // count, lo xyz, hi xyz
 
 struct Task {
@@ -97,11 +98,13 @@ struct Level {
     int* split;         // per task: axis * 256 + bin (-1 = count split)
     int* left_count;    // per task
     int* chunk_left;    // per chunk: left primitives, then exclusive prefix inside the task
-    int* counters;      // [0] chunks, [1] next big tasks, [2] block tasks, [3] internal base
+    int* counters;      // [0] chunks, [1] next big tasks, [2] block tasks, [3] internal base,
+                        // [4] this level's big tasks (the previous level's [1])
 };
 
 // single block: chunk list of the current tasks
-__global__ __launch_bounds__(1024) void k_level_prep(Level L, int ntask, int bins) {
+__global__ __launch_bounds__(1024) void k_level_prep(Level L, int bins) {
+    const int ntask = L.counters[4];
     __shared__ int carry;
     if (threadIdx.x == 0) carry = 0;
     __syncthreads();
@@ -146,6 +149,7 @@ __global__ __launch_bounds__(1024) void k_level_prep(Level L, int ntask, int bin
 // one block per range: reset its centroid bounds and bins
 __global__ __launch_bounds__(kBlock) void k_level_reset(Level L, int bins) {
     const int t = blockIdx.x;
+    if (t >= L.counters[4]) return;  // grid sized by a bound
     if (threadIdx.x < 6) L.cb[6 * t + threadIdx.x] = threadIdx.x < 3 ? ord_f(kInf) : ord_f(-kInf);
     unsigned* B = L.bins + static_cast<size_t>(t) * 3 * kMaxBins * kBinWords;
     for (int j = threadIdx.x; j < 3 * bins * kBinWords; j += kBlock) {
@@ -177,11 +181,22 @@ __global__ __launch_bounds__(kBlock) void k_level_cbounds(Level L, const int* __
             hi[a] = fmaxf(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], o));
         }
     }
+    // the block's bounds, then six atomics per block (every block of a large range updates
+    // the same six words)
+    __shared__ unsigned wb[kBlock / 32][6];
     if ((threadIdx.x & 31) == 0) {
         for (int a = 0; a < 3; ++a) {
-            atomicMin(&L.cb[6 * t + a], ord_f(lo[a]));
-            atomicMax(&L.cb[6 * t + 3 + a], ord_f(hi[a]));
+            wb[threadIdx.x >> 5][a] = ord_f(lo[a]);
+            wb[threadIdx.x >> 5][3 + a] = ord_f(hi[a]);
         }
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        const int j = threadIdx.x;
+        unsigned v = wb[0][j];
+        for (int w = 1; w < kBlock / 32; ++w) v = j < 3 ? min(v, wb[w][j]) : max(v, wb[w][j]);
+        if (j < 3) atomicMin(&L.cb[6 * t + j], v);
+        else atomicMax(&L.cb[6 * t + j], v);
     }
 }
 
@@ -395,9 +410,9 @@ __device__ int warp_sweep_bins(const unsigned* B, int bins, int count, int* left
 }
 
 // one warp per range
-__global__ __launch_bounds__(kBlock) void k_level_split(Level L, int ntask, int bins) {
+__global__ __launch_bounds__(kBlock) void k_level_split(Level L, int bins) {
     const int t = (blockIdx.x * kBlock + threadIdx.x) >> 5;
-    if (t >= ntask) return;
+    if (t >= L.counters[4]) return;  // grid sized by a bound
     const Task tk = L.tasks[t];
     const int count = tk.end - tk.begin;
     int lc = 0;
@@ -446,9 +461,9 @@ __global__ __launch_bounds__(kBlock) void k_level_count_left(Level L, const int*
 }
 
 // per task: exclusive prefix of the chunk counts inside the task
-__global__ __launch_bounds__(kBlock) void k_level_prefix_left(Level L, int ntask) {
+__global__ __launch_bounds__(kBlock) void k_level_prefix_left(Level L) {
     const int t = blockIdx.x * kBlock + threadIdx.x;
-    if (t >= ntask) return;
+    if (t >= L.counters[4]) return;  // grid sized by a bound
     const int first = L.chunk_first[t];
     const int nch = (L.tasks[t].end - L.tasks[t].begin + kChunk - 1) / kChunk;
     int run = 0;
@@ -521,12 +536,13 @@ __global__ __launch_bounds__(kBlock) void k_level_copy(Level L, const int* __res
 }
 
 // single block: node ids for the children (prefix sums over tasks), next big tasks and the
-// block-tier list
-__global__ __launch_bounds__(1024) void k_level_assign(Level L, int ntask, Task* __restrict__ next,
+// block-tier list; the next level's task count to counters[4]
+__global__ __launch_bounds__(1024) void k_level_assign(Level L, Task* __restrict__ next,
                                                       Task* __restrict__ blocks, Node* nodes,
                                                       BNode* bn, int* parent, int n) {
     __shared__ int carry[3];
     __shared__ int wsum[3][32];
+    const int ntask = L.counters[4];  // read by every thread before the first barrier
     if (threadIdx.x < 3) carry[threadIdx.x] = 0;
     __syncthreads();
     const int base_id = L.counters[3];
@@ -589,6 +605,7 @@ __global__ __launch_bounds__(1024) void k_level_assign(Level L, int ntask, Task*
         L.counters[3] = base_id + carry[0];
         L.counters[1] = base_big + carry[1];
         L.counters[2] = base_blk + carry[2];
+        L.counters[4] = base_big + carry[1];
     }
 }
 
@@ -1258,7 +1275,8 @@ int build_sah_impl(qk_tree* t, int bins, int small, const void* items_v, void* w
     cudaMemsetAsync(t->parent, 0xff, sizeof(int) * (2 * static_cast<size_t>(n) - 1), s);
     k_prim_geom<Ops><<<blocks_for(n), kBlock, 0, s>>>(items, n, w.cen, w.plo, w.phi, w.orderA);
 
-    // counters: [1] next big tasks, [2] block tasks, [3] next internal id
+    // counters: [1] next big tasks, [2] block tasks, [3] next internal id, [4] this level's
+    // big tasks
     int init[8] = {0, 0, 0, 1, 0, 0, 0, 0};
     Task root{0, n, 0, 0};
     int nbig = 0, nblk = 0;
@@ -1270,38 +1288,54 @@ int build_sah_impl(qk_tree* t, int bins, int small, const void* items_v, void* w
         init[2] = 1;
         nblk = 1;
     }
+    init[4] = nbig;
     cudaMemcpyAsync(w.L.counters, init, sizeof(init), cudaMemcpyHostToDevice, s);
     Task* cur = w.tasksA;
     Task* nxt = w.tasksB;
     int* ord = w.orderA;
     int* alt = w.orderB;
     int level = 0;
+    // Levels run in batches between host read-backs of the counters: every level kernel reads
+    // its task count from counters[4] and the grids are sized by a bound (a level has at most
+    // twice the previous level's tasks, and at most n / (kTaskRange + 1)); a level after the
+    // last one has no tasks and every kernel of it returns at once.  With a StageClock
+    // installed every level is read back, so that its stage times are its own.
+    StageClock* clk = stage_clock();
+    const int per_sync = clk ? 1 : kLevelsPerSync;
+    const int max_big = n / (kTaskRange + 1) + 1;
     while (nbig > 0) {
-        if (++level > kMaxDepth) return fail(QK_ERR_DEPTH, "SAH: too many levels");
-        w.L.tasks = cur;
-        k_level_prep<<<1, 1024, 0, s>>>(w.L, nbig, bins);
-        k_level_reset<<<nbig, kBlock, 0, s>>>(w.L, bins);
-        // chunk kernels: grid sized by a bound on the chunk count (every task spans at most
-        // size / kChunk + 1 chunks); blocks beyond the count k_level_prep wrote return at once
-        const int nch = n / kChunk + nbig + 1;
+        if (level >= kMaxDepth) return fail(QK_ERR_DEPTH, "SAH: too many levels");
+        int bound = nbig;
+        const int batch = std::min(per_sync, kMaxDepth - level);
         cudaError_t e;
-        // per-level stage times when a StageClock is installed: binning (centroid bounds +
-        // bins), split selection, partition (+ child assignment)
-        StageClock* clk = stage_clock();
-        if (clk) cudaEventRecord(clk->lv[0], s);
-        k_level_cbounds<<<nch, kBlock, 0, s>>>(w.L, ord, w.cen);
-        k_level_bins<<<nch, kBlock, 0, s>>>(w.L, ord, w.cen, w.plo, w.phi, bins);
-        if (clk) cudaEventRecord(clk->lv[1], s);
-        k_level_split<<<blocks_for(static_cast<long long>(nbig) * 32), kBlock, 0, s>>>(w.L, nbig, bins);
-        if (clk) cudaEventRecord(clk->lv[2], s);
-        k_level_count_left<<<nch, kBlock, 0, s>>>(w.L, ord, w.cen, bins);
-        k_level_prefix_left<<<blocks_for(nbig), kBlock, 0, s>>>(w.L, nbig);
-        k_level_partition<<<nch, kBlock, 0, s>>>(w.L, ord, alt, w.cen, bins);
-        k_level_copy<<<nch, kBlock, 0, s>>>(w.L, alt, ord);
-        // next big tasks start from zero each level; block tasks accumulate
-        cudaMemsetAsync(w.L.counters + 1, 0, sizeof(int), s);
-        k_level_assign<<<1, 1024, 0, s>>>(w.L, nbig, nxt, w.blocks, nodes, bn, t->parent, n);
-        if (clk) cudaEventRecord(clk->lv[3], s);
+        for (int j = 0; j < batch; ++j, ++level) {
+            w.L.tasks = cur;
+            k_level_prep<<<1, 1024, 0, s>>>(w.L, bins);
+            k_level_reset<<<bound, kBlock, 0, s>>>(w.L, bins);
+            // chunk kernels: grid sized by a bound on the chunk count (every task spans at most
+            // size / kChunk + 1 chunks); blocks beyond the count k_level_prep wrote return at once
+            const int nch = n / kChunk + bound + 1;
+            // per-level stage times when a StageClock is installed: binning (centroid bounds +
+            // bins), split selection, partition (+ child assignment)
+            if (clk) cudaEventRecord(clk->lv[0], s);
+            k_level_cbounds<<<nch, kBlock, 0, s>>>(w.L, ord, w.cen);
+            k_level_bins<<<nch, kBlock, 0, s>>>(w.L, ord, w.cen, w.plo, w.phi, bins);
+            if (clk) cudaEventRecord(clk->lv[1], s);
+            k_level_split<<<blocks_for(static_cast<long long>(bound) * 32), kBlock, 0, s>>>(w.L, bins);
+            if (clk) cudaEventRecord(clk->lv[2], s);
+            k_level_count_left<<<nch, kBlock, 0, s>>>(w.L, ord, w.cen, bins);
+            k_level_prefix_left<<<blocks_for(bound), kBlock, 0, s>>>(w.L);
+            k_level_partition<<<nch, kBlock, 0, s>>>(w.L, ord, alt, w.cen, bins);
+            k_level_copy<<<nch, kBlock, 0, s>>>(w.L, alt, ord);
+            // next big tasks start from zero each level; block tasks accumulate
+            cudaMemsetAsync(w.L.counters + 1, 0, sizeof(int), s);
+            k_level_assign<<<1, 1024, 0, s>>>(w.L, nxt, w.blocks, nodes, bn, t->parent, n);
+            if (clk) cudaEventRecord(clk->lv[3], s);
+            Task* tmpt = cur;
+            cur = nxt;
+            nxt = tmpt;
+            bound = std::min(2 * bound, max_big);
+        }
         int cnt[4] = {0, 0, 0, 0};
         e = cudaMemcpyAsync(cnt, w.L.counters, sizeof(cnt), cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -1318,9 +1352,6 @@ int build_sah_impl(qk_tree* t, int bins, int small, const void* items_v, void* w
         }
         nbig = cnt[1];
         nblk = cnt[2];
-        Task* tmpt = cur;
-        cur = nxt;
-        nxt = tmpt;
     }
     if (nblk > 0) {
         // reserved ids for the block subtrees: base + exclusive sum of (count - 2)

@@ -97,7 +97,7 @@ struct Level {
     unsigned* bins;     // per task: 3 * bins * kBinWords
     int* split;         // per task: axis * 256 + bin (-1 = count split)
     int* left_count;    // per task
-    int* chunk_left;    // per chunk: left primitives, then exclusive prefix inside the task
+    int* chunk_left;    // per chunk: left primitives
     int* counters;      // [0] chunks, [1] next big tasks, [2] block tasks, [3] internal base,
                         // [4] this level's big tasks (the previous level's [1])
 };
@@ -460,21 +460,8 @@ __global__ __launch_bounds__(kBlock) void k_level_count_left(Level L, const int*
     }
 }
 
-// per task: exclusive prefix of the chunk counts inside the task
-__global__ __launch_bounds__(kBlock) void k_level_prefix_left(Level L) {
-    const int t = blockIdx.x * kBlock + threadIdx.x;
-    if (t >= L.counters[4]) return;  // grid sized by a bound
-    const int first = L.chunk_first[t];
-    const int nch = (L.tasks[t].end - L.tasks[t].begin + kChunk - 1) / kChunk;
-    int run = 0;
-    for (int c = 0; c < nch; ++c) {
-        const int v = L.chunk_left[first + c];
-        L.chunk_left[first + c] = run;
-        run += v;
-    }
-}
-
-// stable partition of each chunk into `out` (left block first, then right block)
+// stable partition of each chunk into `out` (left block first, then right block); the lefts
+// of the task's earlier chunks are summed from their counts by the whole block
 __global__ __launch_bounds__(kBlock) void k_level_partition(Level L, const int* __restrict__ order,
                                                            int* __restrict__ out,
                                                            const float4* __restrict__ cen,
@@ -486,13 +473,19 @@ __global__ __launch_bounds__(kBlock) void k_level_partition(Level L, const int* 
     const int b = L.chunk_begin[c];
     const int e = min(b + kChunk, tk.end);
     const int split = L.split[t], lc = L.left_count[t];
-    const int left_before = L.chunk_left[c];        // lefts in earlier chunks of this task
-    const int right_before = (b - tk.begin) - left_before;
     __shared__ int wsum[kBlock / 32];
     __shared__ int carry;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int before = 0;
+    for (int j = L.chunk_first[t] + threadIdx.x; j < c; j += kBlock) before += L.chunk_left[j];
+    before = __reduce_add_sync(0xffffffffu, before);
+    if (lane == 0) wsum[warp] = before;
     if (threadIdx.x == 0) carry = 0;
     __syncthreads();
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int left_before = 0;                            // lefts in earlier chunks of this task
+    for (int w = 0; w < kBlock / 32; ++w) left_before += wsum[w];
+    __syncthreads();
+    const int right_before = (b - tk.begin) - left_before;
     for (int base = b; base < e; base += kBlock) {
         const int i = base + threadIdx.x;
         int p = 0;
@@ -1324,7 +1317,6 @@ int build_sah_impl(qk_tree* t, int bins, int small, const void* items_v, void* w
             k_level_split<<<blocks_for(static_cast<long long>(bound) * 32), kBlock, 0, s>>>(w.L, bins);
             if (clk) cudaEventRecord(clk->lv[2], s);
             k_level_count_left<<<nch, kBlock, 0, s>>>(w.L, ord, w.cen, bins);
-            k_level_prefix_left<<<blocks_for(bound), kBlock, 0, s>>>(w.L);
             k_level_partition<<<nch, kBlock, 0, s>>>(w.L, ord, alt, w.cen, bins);
             k_level_copy<<<nch, kBlock, 0, s>>>(w.L, alt, ord);
             // next big tasks start from zero each level; block tasks accumulate

@@ -27,7 +27,7 @@ namespace qk {
 
 namespace {
 
-constexpr int kChunk = 4096;       // primitives binned per block at the global tier
+constexpr int kChunk = 2048;       // primitives binned per block at the global tier
 constexpr int kBlockRange = 1024;  // largest range built by one block (forest tasks)
 constexpr int kTaskRange = 256;    // largest range the global tier hands to one warp
 constexpr int kWarpRange = 32;     // largest range finished by one warp
@@ -460,10 +460,13 @@ __global__ __launch_bounds__(kBlock) void k_level_count_left(Level L, const int*
     }
 }
 
-// stable partition of each chunk into `out` (left block first, then right block); the lefts
-// of the task's earlier chunks are summed from their counts by the whole block
+// stable partition of each chunk (left block first, then right block) into `out` where the
+// child stays in the global tier (more than kTaskRange primitives) and into `fin`, the final
+// order the warp tier and the leaves read, where the child's range is final; the lefts of the
+// task's earlier chunks are summed from their counts by the whole block
 __global__ __launch_bounds__(kBlock) void k_level_partition(Level L, const int* __restrict__ order,
                                                            int* __restrict__ out,
+                                                           int* __restrict__ fin,
                                                            const float4* __restrict__ cen,
                                                            int bins) {
     if (static_cast<int>(blockIdx.x) >= L.counters[0]) return;  // grid sized by a bound
@@ -510,22 +513,13 @@ __global__ __launch_bounds__(kBlock) void k_level_partition(Level L, const int* 
         if (i < e) {
             const int dst = f ? tk.begin + left_before + lrank
                               : tk.begin + lc + right_before + (i - b - lrank);
-            out[dst] = p;
+            const int child = f ? lc : tk.end - tk.begin - lc;
+            (child > kTaskRange ? out : fin)[dst] = p;
         }
         __syncthreads();
         if (threadIdx.x == 0) carry += tot;
         __syncthreads();
     }
-}
-
-__global__ __launch_bounds__(kBlock) void k_level_copy(Level L, const int* __restrict__ src,
-                                                      int* __restrict__ dst) {
-    if (static_cast<int>(blockIdx.x) >= L.counters[0]) return;  // grid sized by a bound
-    const int c = blockIdx.x;
-    const int t = L.chunk_task[c];
-    const int b = L.chunk_begin[c];
-    const int e = min(b + kChunk, L.tasks[t].end);
-    for (int i = b + threadIdx.x; i < e; i += kBlock) dst[i] = src[i];
 }
 
 // single block: node ids for the children (prefix sums over tasks), next big tasks and the
@@ -1214,6 +1208,7 @@ struct SahWs {
     Header* h;
     int* orderA;
     int* orderB;
+    int* orderF;  // final order: each primitive's position once its range leaves the global tier
     float4* cen;
     float4* plo;
     float4* phi;
@@ -1233,6 +1228,7 @@ SahWs carve_sah(Carve& c, int n) {
     w.h = c.take<Header>(1);
     w.orderA = c.take<int>(n);
     w.orderB = c.take<int>(n);
+    w.orderF = c.take<int>(n);
     w.cen = c.take<float4>(n);
     w.plo = c.take<float4>(n);
     w.phi = c.take<float4>(n);
@@ -1317,8 +1313,7 @@ int build_sah_impl(qk_tree* t, int bins, int small, const void* items_v, void* w
             k_level_split<<<blocks_for(static_cast<long long>(bound) * 32), kBlock, 0, s>>>(w.L, bins);
             if (clk) cudaEventRecord(clk->lv[2], s);
             k_level_count_left<<<nch, kBlock, 0, s>>>(w.L, ord, w.cen, bins);
-            k_level_partition<<<nch, kBlock, 0, s>>>(w.L, ord, alt, w.cen, bins);
-            k_level_copy<<<nch, kBlock, 0, s>>>(w.L, alt, ord);
+            k_level_partition<<<nch, kBlock, 0, s>>>(w.L, ord, alt, w.orderF, w.cen, bins);
             // next big tasks start from zero each level; block tasks accumulate
             cudaMemsetAsync(w.L.counters + 1, 0, sizeof(int), s);
             k_level_assign<<<1, 1024, 0, s>>>(w.L, nxt, w.blocks, nodes, bn, t->parent, n);
@@ -1326,6 +1321,9 @@ int build_sah_impl(qk_tree* t, int bins, int small, const void* items_v, void* w
             Task* tmpt = cur;
             cur = nxt;
             nxt = tmpt;
+            int* tmpo = ord;  // the next level reads what this one partitioned
+            ord = alt;
+            alt = tmpo;
             bound = std::min(2 * bound, max_big);
         }
         int cnt[4] = {0, 0, 0, 0};
@@ -1345,6 +1343,10 @@ int build_sah_impl(qk_tree* t, int bins, int small, const void* items_v, void* w
         nbig = cnt[1];
         nblk = cnt[2];
     }
+    // the final order: written by the partitions, or the initial order when the root went
+    // straight to the warp tier; either order buffer is then free scratch
+    int* fin = n > kTaskRange ? w.orderF : w.orderA;
+    int* scratch = n > kTaskRange ? w.orderA : w.orderB;
     if (nblk > 0) {
         // reserved ids for the block subtrees: base + exclusive sum of (count - 2)
         k_task_sizes<<<blocks_for(nblk), kBlock, 0, s>>>(w.blocks, nblk, w.id_base);
@@ -1359,9 +1361,9 @@ int build_sah_impl(qk_tree* t, int bins, int small, const void* items_v, void* w
             return fail(QK_ERR_INVALID, "SAH node accounting: %d + %d != %d", tail[1], tail[0], n - 1);
         }
         k_add_base<<<blocks_for(nblk), kBlock, 0, s>>>(w.id_base, nblk, w.L.counters);
-        // every range of at most kTaskRange primitives: one warp each (`alt` is free scratch)
+        // every range of at most kTaskRange primitives: one warp each
         k_warp_tasks<<<min(blocks_for(static_cast<long long>(nblk) * 32), 148 * 8), kBlock,
-                       warp_tasks_smem(bins), s>>>(w.blocks, nblk, w.id_base, ord, alt, w.cen,
+                       warp_tasks_smem(bins), s>>>(w.blocks, nblk, w.id_base, fin, scratch, w.cen,
                                                    w.plo, w.phi, nodes, bn, t->parent, n, bins, err,
                                                    0, small);
     } else {
@@ -1372,7 +1374,7 @@ int build_sah_impl(qk_tree* t, int bins, int small, const void* items_v, void* w
     }
     stage_mark(kMarkTopo, s);
     // the scatter: items, leaf payloads and prim ids in leaf order
-    k_sah_leaves<Ops><<<blocks_for(n), kBlock, 0, s>>>(items, n, ord, nodes,
+    k_sah_leaves<Ops><<<blocks_for(n), kBlock, 0, s>>>(items, n, fin, nodes,
                                                        static_cast<float*>(t->items), t->prim_ids,
                                                        t->slot_of, static_cast<float4*>(t->leaves));
     stage_mark(kMarkScatter, s);

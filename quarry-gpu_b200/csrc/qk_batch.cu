@@ -196,16 +196,23 @@ __global__ __launch_bounds__(kBlock) void k_bt_emit(const BScene* __restrict__ t
                                                     const uint32_t* __restrict__ codes_f,
                                                     const uint32_t* __restrict__ ids_f,
                                                     int2* __restrict__ ranges) {
+    __shared__ __align__(16) float stage[kBlock / 32][emit_stage_floats<Ops>()];
     const int2 ch = chunks[blockIdx.x];
     const BScene& sc = tab[ch.x];
     const qk_tree& t = sc.t;
     const int n = t.n;
     const int end = min(n, ch.y + kBuildChunk);
-    for (int k = ch.y + threadIdx.x; k < end; k += kBlock) {
-        emit_slot<Ops>(sc.in, n, codes_f + sc.prim_off, ids_f + sc.prim_off,
-                       static_cast<Node*>(t.nodes), static_cast<float*>(t.items), t.prim_ids,
-                       t.slot_of, t.parent, static_cast<BNode*>(t.bnodes),
-                       static_cast<float4*>(t.leaves), t.flags, k, ranges + sc.prim_off);
+    const uint32_t* codes = codes_f + sc.prim_off;
+    const uint32_t* ids = ids_f + sc.prim_off;
+    for (int k0 = ch.y + (threadIdx.x & ~31); k0 < end; k0 += kBlock) {  // whole warps
+        emit_leaves_warp<Ops>(sc.in, n, ids, static_cast<Node*>(t.nodes),
+                              static_cast<float*>(t.items), t.prim_ids, t.slot_of,
+                              static_cast<float4*>(t.leaves), k0, min(32, end - k0),
+                              stage[threadIdx.x >> 5]);
+        const int k = k0 + (threadIdx.x & 31);
+        if (k < end)
+            emit_internal(n, codes, ids, static_cast<Node*>(t.nodes), t.parent,
+                          static_cast<BNode*>(t.bnodes), t.flags, k, ranges + sc.prim_off);
     }
 }
 

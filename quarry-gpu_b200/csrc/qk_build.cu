@@ -113,10 +113,13 @@ __global__ __launch_bounds__(kBlock) void k_emit(
     int* __restrict__ prim_ids, int* __restrict__ slot_of, int* __restrict__ parent,
     BNode* __restrict__ bnodes, float4* __restrict__ leaves, int* __restrict__ flags,
     int2* __restrict__ ranges) {
-    const int k = blockIdx.x * kBlock + threadIdx.x;
-    if (k >= n) return;
-    emit_slot<Ops>(items, n, codes, ids, nodes, sorted, prim_ids, slot_of, parent, bnodes, leaves,
-                   flags, k, ranges);
+    __shared__ __align__(16) float stage[kBlock / 32][emit_stage_floats<Ops>()];
+    const int k0 = blockIdx.x * kBlock + (threadIdx.x & ~31);
+    if (k0 >= n) return;  // whole warps
+    emit_leaves_warp<Ops>(items, n, ids, nodes, sorted, prim_ids, slot_of, leaves, k0,
+                          min(32, n - k0), stage[threadIdx.x >> 5]);
+    const int k = k0 + (threadIdx.x & 31);
+    if (k < n) emit_internal(n, codes, ids, nodes, parent, bnodes, flags, k, ranges);
 }
 
 // (first slot, leaves) of every internal node of a tree whose subtrees cover ordered

@@ -21,7 +21,7 @@
 //            prefix and suffix boxes, and evaluate every split position.
 // Depth stays below the 64-entry traversal stacks: a split is only taken while
 // depth + ceil(log2(larger child)) <= kMaxDepth, otherwise the range is halved by count.
-#include "qk_internal.cuh"
+#include "qk_build.cuh"
 
 namespace qk {
 
@@ -1174,24 +1174,12 @@ __global__ __launch_bounds__(kBlock) void k_sah_leaves(const float* __restrict__
                                                       int* __restrict__ prim_ids,
                                                       int* __restrict__ slot_of,
                                                       float4* __restrict__ leaves) {
-    const int k = blockIdx.x * kBlock + threadIdx.x;
-    if (k >= n) return;
-    const int src = order[k];
-    float it[Ops::kFloats];
-#pragma unroll
-    for (int j = 0; j < Ops::kFloats; ++j) it[j] = items[static_cast<size_t>(src) * Ops::kFloats + j];
-#pragma unroll
-    for (int j = 0; j < Ops::kFloats; ++j) sorted[static_cast<size_t>(k) * Ops::kFloats + j] = it[j];
-    prim_ids[k] = src;
-    slot_of[src] = k;
-    const Box b = Ops::bounds(it);
-    float4* leaf = reinterpret_cast<float4*>(nodes + (n - 1 + k));
-    leaf[0] = make_float4(b.lo.x, b.lo.y, b.lo.z, b.hi.x);
-    leaf[1] = make_float4(b.hi.y, b.hi.z, __int_as_float(-(k + 1)), __int_as_float(1));
-    float4 pay[Ops::kVec4];
-    Ops::pack(it, src, pay);
-#pragma unroll
-    for (int j = 0; j < Ops::kVec4; ++j) leaves[static_cast<size_t>(k) * Ops::kVec4 + j] = pay[j];
+    // the LBVH emit's leaf writer (per-warp staging for triangles and Gaussians)
+    __shared__ __align__(16) float stage[kBlock / 32][emit_stage_floats<Ops>()];
+    const int k0 = blockIdx.x * kBlock + (threadIdx.x & ~31);
+    if (k0 >= n) return;  // whole warps
+    emit_leaves_warp<Ops>(items, n, reinterpret_cast<const uint32_t*>(order), nodes, sorted,
+                          prim_ids, slot_of, leaves, k0, min(32, n - k0), stage[threadIdx.x >> 5]);
 }
 
 __global__ void k_task_sizes(const Task* __restrict__ t, int m, int* __restrict__ out) {

@@ -238,31 +238,49 @@ __global__ __launch_bounds__(kBlock) void k_level_bins(Level L, const int* __res
         atomicMax(&w[5], acc[a][5]);
         atomicMax(&w[6], acc[a][6]);
     };
-    for (int i = i0; i < i1; ++i) {
-        const int p = order[i];
-        const float4 cc = cen[p], lo = plo[p], hi = phi[p];
-        const float cv[3] = {cc.x, cc.y, cc.z};
+    // the run in pairs: both primitives' gathers are issued together (groups of four held 108
+    // registers and ran slower at the lower occupancy)
+    constexpr int kGroup = 2;
+    for (int g = i0; g < i1; g += kGroup) {
+        int pg[kGroup];
 #pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            const int bin = bin_of(cv[a], clo[a], chi[a], bins);
-            if (bin != cur[a]) {
-                if (cur[a] >= 0) flush(a);
-                cur[a] = bin;
-                acc[a][0] = 1u;
-                acc[a][1] = ord_f(lo.x);
-                acc[a][2] = ord_f(lo.y);
-                acc[a][3] = ord_f(lo.z);
-                acc[a][4] = ord_f(hi.x);
-                acc[a][5] = ord_f(hi.y);
-                acc[a][6] = ord_f(hi.z);
-            } else {
-                acc[a][0] += 1u;
-                acc[a][1] = min(acc[a][1], ord_f(lo.x));
-                acc[a][2] = min(acc[a][2], ord_f(lo.y));
-                acc[a][3] = min(acc[a][3], ord_f(lo.z));
-                acc[a][4] = max(acc[a][4], ord_f(hi.x));
-                acc[a][5] = max(acc[a][5], ord_f(hi.y));
-                acc[a][6] = max(acc[a][6], ord_f(hi.z));
+        for (int u = 0; u < kGroup; ++u) pg[u] = g + u < i1 ? order[g + u] : -1;
+        float4 cg[kGroup], lg[kGroup], hg[kGroup];
+#pragma unroll
+        for (int u = 0; u < kGroup; ++u) {
+            if (pg[u] >= 0) {
+                cg[u] = cen[pg[u]];
+                lg[u] = plo[pg[u]];
+                hg[u] = phi[pg[u]];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kGroup; ++u) {
+            if (pg[u] < 0) break;
+            const float4 lo = lg[u], hi = hg[u];
+            const float cv[3] = {cg[u].x, cg[u].y, cg[u].z};
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                const int bin = bin_of(cv[a], clo[a], chi[a], bins);
+                if (bin != cur[a]) {
+                    if (cur[a] >= 0) flush(a);
+                    cur[a] = bin;
+                    acc[a][0] = 1u;
+                    acc[a][1] = ord_f(lo.x);
+                    acc[a][2] = ord_f(lo.y);
+                    acc[a][3] = ord_f(lo.z);
+                    acc[a][4] = ord_f(hi.x);
+                    acc[a][5] = ord_f(hi.y);
+                    acc[a][6] = ord_f(hi.z);
+                } else {
+                    acc[a][0] += 1u;
+                    acc[a][1] = min(acc[a][1], ord_f(lo.x));
+                    acc[a][2] = min(acc[a][2], ord_f(lo.y));
+                    acc[a][3] = min(acc[a][3], ord_f(lo.z));
+                    acc[a][4] = max(acc[a][4], ord_f(hi.x));
+                    acc[a][5] = max(acc[a][5], ord_f(hi.y));
+                    acc[a][6] = max(acc[a][6], ord_f(hi.z));
+                }
             }
         }
     }

@@ -51,25 +51,23 @@ constexpr int emit_stage_floats() {
                                   : (8 > 4 * Ops::kVec4 ? 8 : 4 * Ops::kVec4));
 }
 
-// Leaves k0 .. k0 + m - 1 (m <= 32) of the LBVH over sorted (code, id) pairs, by the whole
-// warp: each lane gathers one primitive, and for triangles and Gaussians (36- and 40-byte
-// items, 48-byte payloads) the sorted items, leaf nodes and leaf payloads go out through the
-// warp's shared staging (16-byte aligned, emit_stage_floats<Ops>() floats) so that each store
-// instruction covers consecutive whole lines instead of one strided piece per lane (city LBVH
-// build 0.587 -> 0.572 ms); points store per lane.
+// Leaves k0 .. k0 + m - 1 (m <= 32) of a tree of n leaves, by the whole warp: lane i < m holds
+// the item (it) and scene index (src) of slot k0 + i.  For triangles and Gaussians (36- and
+// 40-byte items, 48-byte payloads) the sorted items, leaf nodes and leaf payloads go out
+// through the warp's shared staging (16-byte aligned, emit_stage_floats<Ops>() floats) so that
+// each store instruction covers consecutive whole lines instead of one strided piece per lane
+// (city LBVH build 0.587 -> 0.572 ms); points store per lane.
 template <class Ops>
-__device__ __forceinline__ void emit_leaves_warp(
-    const float* __restrict__ items, int n, const uint32_t* __restrict__ ids,
-    Node* __restrict__ nodes, float* __restrict__ sorted, int* __restrict__ prim_ids,
-    int* __restrict__ slot_of, float4* __restrict__ leaves, int k0, int m, float* stage) {
+__device__ __forceinline__ void store_leaves_warp(const float (&it)[Ops::kFloats], int src, int n,
+                                                  Node* __restrict__ nodes,
+                                                  float* __restrict__ sorted,
+                                                  int* __restrict__ prim_ids,
+                                                  int* __restrict__ slot_of,
+                                                  float4* __restrict__ leaves, int k0, int m,
+                                                  float* stage) {
     const int lane = threadIdx.x & 31;
     const int k = k0 + lane;
     const bool ok = lane < m;
-    const int src = ok ? static_cast<int>(ids[k]) : 0;
-    float it[Ops::kFloats];
-#pragma unroll
-    for (int j = 0; j < Ops::kFloats; ++j)
-        it[j] = ok ? items[static_cast<size_t>(src) * Ops::kFloats + j] : 0.0f;
     if (ok) {
         prim_ids[k] = src;
         slot_of[src] = k;
@@ -114,6 +112,23 @@ __device__ __forceinline__ void emit_leaves_warp(
     float4* ldst = leaves + static_cast<size_t>(k0) * Ops::kVec4;
     for (int t = lane; t < m * Ops::kVec4; t += 32) ldst[t] = st4[t];
     __syncwarp();
+}
+
+// Leaves k0 .. k0 + m - 1 (m <= 32) of the LBVH over sorted (code, id) pairs, by the whole
+// warp: each lane gathers one primitive, then store_leaves_warp writes them.
+template <class Ops>
+__device__ __forceinline__ void emit_leaves_warp(
+    const float* __restrict__ items, int n, const uint32_t* __restrict__ ids,
+    Node* __restrict__ nodes, float* __restrict__ sorted, int* __restrict__ prim_ids,
+    int* __restrict__ slot_of, float4* __restrict__ leaves, int k0, int m, float* stage) {
+    const int lane = threadIdx.x & 31;
+    const bool ok = lane < m;
+    const int src = ok ? static_cast<int>(ids[k0 + lane]) : 0;
+    float it[Ops::kFloats];
+#pragma unroll
+    for (int j = 0; j < Ops::kFloats; ++j)
+        it[j] = ok ? items[static_cast<size_t>(src) * Ops::kFloats + j] : 0.0f;
+    store_leaves_warp<Ops>(it, src, n, nodes, sorted, prim_ids, slot_of, leaves, k0, m, stage);
 }
 
 // Internal node k (k < n - 1) of the LBVH over sorted (code, id) pairs, its children's parent

@@ -28,7 +28,7 @@
 // the new leaves, or a forest could pass the depth limit.
 #include <algorithm>
 
-#include "qk_internal.cuh"
+#include "qk_build.cuh"
 
 namespace qk {
 namespace {
@@ -489,15 +489,35 @@ __global__ __launch_bounds__(kBlock) void k_topo_kept_leaves(EditDev e, const qk
                                                             const int* __restrict__ xs,
                                                             const int* __restrict__ shifts,
                                                             int* err) {
+    __shared__ __align__(16) float stage[kBlock / 32][emit_stage_floats<Ops>()];
     const int s = blockIdx.x * kBlock + threadIdx.x;
-    if (s >= e.n_old) return;
-    const int j = old_t.prim_ids[s];
-    if (del_flag[j] || cut_of_slot[s] >= 0) return;
-    const float* it = static_cast<const float*>(old_t.items) + static_cast<size_t>(s) * Ops::kFloats;
+    const int lane = threadIdx.x & 31;
+    if ((s & ~31) >= e.n_old) return;  // whole warps
+    int j = 0;
+    bool mine = s < e.n_old;
+    if (mine) {
+        j = old_t.prim_ids[s];
+        mine = !del_flag[j] && cut_of_slot[s] < 0;
+    }
     float buf[Ops::kFloats];
+    const float* it = static_cast<const float*>(old_t.items) + static_cast<size_t>(mine ? s : 0) * Ops::kFloats;
 #pragma unroll
-    for (int q = 0; q < Ops::kFloats; ++q) buf[q] = it[q];
-    write_leaf<Ops>(t, xs[s], buf, remap_id(e, shifts, j), err, kSiteKeptLeaf);
+    for (int q = 0; q < Ops::kFloats; ++q) buf[q] = mine ? it[q] : 0.0f;
+    const int slot = mine ? xs[s] : -1;
+    const int id = mine ? remap_id(e, shifts, j) : 0;
+    // a warp whose 32 slots all survive into 32 consecutive in-range new slots (most of them,
+    // for small edits) writes through the emit's staged leaf writer; any other lane alone,
+    // with the bounds checks
+    const int slot0 = __shfl_sync(0xffffffffu, slot, 0);
+    const bool run = __all_sync(0xffffffffu, mine && slot == slot0 + lane && id >= 0 && id < t.n) &&
+                     slot0 >= 0 && slot0 + 32 <= t.n;
+    if (run) {
+        store_leaves_warp<Ops>(buf, id, t.n, static_cast<Node*>(t.nodes),
+                               static_cast<float*>(t.items), t.prim_ids, t.slot_of,
+                               static_cast<float4*>(t.leaves), slot0, 32, stage[threadIdx.x >> 5]);
+    } else if (mine) {
+        write_leaf<Ops>(t, slot, buf, id, err, kSiteKeptLeaf);
+    }
 }
 
 template <class Ops>

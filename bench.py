@@ -770,11 +770,11 @@ def rays_parity(cfg, result, q_result, city: bool, threads: int, report_cpu: boo
 # ---------------------------------------------------------------------------------------
 # topology edits: subtree surgery against a rebuild of the edited scene
 # ---------------------------------------------------------------------------------------
-def topology_timing(kind, items, builder, bins, queries_d, seed, timed_ms, rays_d=None):
-    """1% edits of quarry's GpuTopoEdit kind (a quarter each deleted, inserted, appended and
-    moved), "cluster" (around one spot) and "scatter" (uniform): qk_update_topology on the
-    built tree against qk_build of the edited scene, both device-timed with the scripts
-    already resident.  The edited tree must answer closest / kNN (and rays) like the rebuild."""
+def topology_surgery(kind, items, builder, bins, mode, seed):
+    """A 1% edit script of quarry's GpuTopoEdit kind (a quarter each deleted, inserted,
+    appended and moved; "cluster" around one spot or "scatter" uniform) for a tree built from
+    `items`: returns the tree, the edited scene and the script on the device, the QkTopoInfo
+    the surgery fills and a function that runs qk_update_topology once on the built tree."""
     import ctypes
 
     import torch
@@ -782,33 +782,50 @@ def topology_timing(kind, items, builder, bins, queries_d, seed, timed_ms, rays_
     from quarry import capi
     from quarry import workloads as w
 
+    new, dele, ins, mov = w.topology_edit(items, 0.01, mode, seed)
+    base = capi.DeviceTree(kind, items, builder=builder, sah_bins=bins)
+    n_new = len(new)
+    new_d = capi.to_device(new, np.float32)
+    dele_d, ins_d, mov_d = (capi.to_device(a, np.int32) for a in (dele, ins, mov))
+    app = n_new - len(items) + len(dele) - len(ins)
+    tail = torch.arange(n_new - app, n_new, device="cuda")
+    extra = new_d[torch.cat([ins_d.long(), tail])].contiguous()
+    moved_items = new_d[mov_d.long()].contiguous()
+    e = capi.QkTopoEdit(dele_d.data_ptr(), len(dele), ins_d.data_ptr(), len(ins), app,
+                        mov_d.data_ptr(), len(mov), extra.data_ptr(), moved_items.data_ptr())
+    arrays, nt = base._alloc(n_new)
+    nb = capi.lib().qk_update_workspace_bytes(base.kind, base.n, n_new, int(extra.shape[0]))
+    ws = torch.empty(nb, dtype=torch.uint8, device="cuda")
+    info = capi.QkTopoInfo()
+    keep = (dele_d, ins_d, mov_d, extra, moved_items, arrays, nt, ws, e)
+
+    def surgery():
+        capi.check(capi.lib().qk_update_topology(
+            ctypes.byref(base.t), ctypes.byref(nt), ctypes.byref(e), 0, bins,
+            ctypes.byref(info), ws.data_ptr(), nb, capi._stream()), "qk_update_topology")
+
+    script = (new, dele, ins, mov, int(len(dele) + len(ins) + app + len(mov)))
+    return base, new_d, script, info, surgery, keep
+
+
+def topology_timing(kind, items, builder, bins, queries_d, seed, timed_ms, rays_d=None):
+    """1% edits of quarry's GpuTopoEdit kind (a quarter each deleted, inserted, appended and
+    moved), "cluster" (around one spot) and "scatter" (uniform): qk_update_topology on the
+    built tree against qk_build of the edited scene, both device-timed with the scripts
+    already resident.  The edited tree must answer closest / kNN (and rays) like the rebuild."""
+    import torch
+
+    from quarry import capi
+
     out = {}
     for mode in ("cluster", "scatter"):
-        new, dele, ins, mov = w.topology_edit(items, 0.01, mode, seed)
-        base = capi.DeviceTree(kind, items, builder=builder, sah_bins=bins)
-        n_new = len(new)
-        new_d = capi.to_device(new, np.float32)
-        dele_d, ins_d, mov_d = (capi.to_device(a, np.int32) for a in (dele, ins, mov))
-        app = n_new - len(items) + len(dele) - len(ins)
-        tail = torch.arange(n_new - app, n_new, device="cuda")
-        extra = new_d[torch.cat([ins_d.long(), tail])].contiguous()
-        moved_items = new_d[mov_d.long()].contiguous()
-        e = capi.QkTopoEdit(dele_d.data_ptr(), len(dele), ins_d.data_ptr(), len(ins), app,
-                            mov_d.data_ptr(), len(mov), extra.data_ptr(), moved_items.data_ptr())
-        arrays, nt = base._alloc(n_new)
-        nb = capi.lib().qk_update_workspace_bytes(base.kind, base.n, n_new, int(extra.shape[0]))
-        ws = torch.empty(nb, dtype=torch.uint8, device="cuda")
-        info = capi.QkTopoInfo()
-
-        def surgery():
-            capi.check(capi.lib().qk_update_topology(
-                ctypes.byref(base.t), ctypes.byref(nt), ctypes.byref(e), 0, bins,
-                ctypes.byref(info), ws.data_ptr(), nb, capi._stream()), "qk_update_topology")
-
+        base, new_d, script, info, surgery, keep = topology_surgery(kind, items, builder, bins,
+                                                                    mode, seed)
+        new, dele, ins, mov, edited = script
         s_ms = timed_ms(surgery)
         fresh = capi.DeviceTree(kind, new_d, builder=builder, sah_bins=bins)
         b_ms = timed_ms(fresh.build)
-        entry = {"edited": int(len(dele) + len(ins) + app + len(mov)), "surgery_ms": round(s_ms, 4),
+        entry = {"edited": edited, "surgery_ms": round(s_ms, 4),
                  "rebuild_ms": round(b_ms, 4), "ratio": round(s_ms / b_ms, 3),
                  "rebuilt_subtrees": info.cuts, "rebuilt_leaves": info.new_leaves,
                  "spliced": info.spliced, "fallback": bool(info.rebuild)}
@@ -825,7 +842,7 @@ def topology_timing(kind, items, builder, bins, queries_d, seed, timed_ms, rays_
         if mode == "cluster":
             entry["api"] = topology_api_wall(kind, items, new, dele, ins, mov, builder)
         out[f"{mode}_1pct"] = entry
-        del base, fresh, arrays, ws
+        del base, fresh, keep
     return out
 
 
@@ -1697,6 +1714,9 @@ KERNEL_CASES = {
                     "(k_ray_bin)",
     "rays_city": "1,000,000 cosine rays on the city's SAH tree, coherent order, 5 blocks/SM "
                  "(k_ray_bin)",
+    "topology_city": "qk_update_topology with the bench's 1% cluster edit on the city's SAH tree, "
+                     "three calls (k_topo_*, the forest's k_warp_tasks, k_bottom_up_ranged, "
+                     "k_depth*)",
 }
 
 
@@ -1763,6 +1783,11 @@ def kernel_case(args):
         for _ in range(2):
             gt.distance_grad(qd, res)
             tt.ray_t_grad(rd, rid, None, with_rays=True)
+    elif name == "topology_city":
+        cfg = w.city_config(131072, 1000, 100, 1)
+        _, _, _, _, surgery, keep = topology_surgery("tri", cfg.tris, "sah", 32, "cluster", 1)
+        for _ in range(3):
+            surgery()
     elif name in ("rays_terrain", "rays_city"):
         if name == "rays_city":
             cfg = w.city_config(131072, 1_000_000, 10, 1)

@@ -233,31 +233,6 @@ __device__ __forceinline__ Box load_box_ca(const Node* nd) {
     return bx;
 }
 
-// Complete internal node p from its two final children when every internal node's slot range
-// is already known (`ranges`): box, traversal node and the children's small-subtree codes.
-// kLocal: both children were finished by threads of this block, whose writes a plain load
-// sees after the block fence; otherwise they are read from L2.
-template <bool kLocal>
-__device__ __forceinline__ void finish_node_ranged(Node* __restrict__ nodes,
-                                                   BNode* __restrict__ bnodes, int p, int n,
-                                                   const int2* __restrict__ ranges) {
-    const int l = nodes[p].left, r = nodes[p].right;
-    const int2 rl = l >= n - 1 ? make_int2(l - (n - 1), 1) : ranges[l];
-    const int2 rr = r >= n - 1 ? make_int2(r - (n - 1), 1) : ranges[r];
-    *reinterpret_cast<float2*>(&bnodes[p].v3.z) =
-        make_float2(__int_as_float(small_code(l, n, rl)), __int_as_float(small_code(r, n, rr)));
-    const Box a = kLocal ? load_box_ca(nodes + l) : load_box_cg(nodes + l);
-    const Box b = kLocal ? load_box_ca(nodes + r) : load_box_cg(nodes + r);
-    Box u;
-    u.lo = f3(fmin_t(a.lo.x, b.lo.x), fmin_t(a.lo.y, b.lo.y), fmin_t(a.lo.z, b.lo.z));
-    u.hi = f3(fmax_t(a.hi.x, b.hi.x), fmax_t(a.hi.y, b.hi.y), fmax_t(a.hi.z, b.hi.z));
-    write_box(nodes + p, u);
-    BNode& bn = bnodes[p];
-    bn.v0 = make_float4(a.lo.x, a.lo.y, a.lo.z, a.hi.x);
-    bn.v1 = make_float4(a.hi.y, a.hi.z, b.lo.x, b.lo.y);
-    bn.v2 = make_float4(b.lo.z, b.hi.x, b.hi.y, b.hi.z);
-}
-
 // One leaf's climb toward the root; flags[p] counts arrivals at internal node p.  The
 // second arrival finishes p (both children final), resets the counter and continues.
 __device__ __forceinline__ void climb(Node* __restrict__ nodes, BNode* __restrict__ bnodes,
@@ -273,26 +248,66 @@ __device__ __forceinline__ void climb(Node* __restrict__ nodes, BNode* __restric
     }
 }
 
+// Complete internal node p from its final children given its links lr = (left, right) and the
+// children's slot ranges (all static during the pass): box and traversal node, with the
+// children's small-subtree codes.  kLocal: both children were finished by threads of this
+// block, whose writes a plain load sees after the block fence; otherwise they are read from L2.
+template <bool kLocal>
+__device__ __forceinline__ void finish_node_links(Node* __restrict__ nodes,
+                                                  BNode* __restrict__ bnodes, int p, int n,
+                                                  int2 lr, int2 rl, int2 rr) {
+    const int l = lr.x, r = lr.y;
+    *reinterpret_cast<float2*>(&bnodes[p].v3.z) =
+        make_float2(__int_as_float(small_code(l, n, rl)), __int_as_float(small_code(r, n, rr)));
+    const Box a = kLocal ? load_box_ca(nodes + l) : load_box_cg(nodes + l);
+    const Box b = kLocal ? load_box_ca(nodes + r) : load_box_cg(nodes + r);
+    Box u;
+    u.lo = f3(fmin_t(a.lo.x, b.lo.x), fmin_t(a.lo.y, b.lo.y), fmin_t(a.lo.z, b.lo.z));
+    u.hi = f3(fmax_t(a.hi.x, b.hi.x), fmax_t(a.hi.y, b.hi.y), fmax_t(a.hi.z, b.hi.z));
+    float4* np = reinterpret_cast<float4*>(nodes + p);
+    np[0] = make_float4(u.lo.x, u.lo.y, u.lo.z, u.hi.x);
+    np[1] = make_float4(u.hi.y, u.hi.z, __int_as_float(l), __int_as_float(r));
+    BNode& bn = bnodes[p];
+    bn.v0 = make_float4(a.lo.x, a.lo.y, a.lo.z, a.hi.x);
+    bn.v1 = make_float4(a.hi.y, a.hi.z, b.lo.x, b.lo.y);
+    bn.v2 = make_float4(b.lo.z, b.hi.x, b.hi.y, b.hi.z);
+}
+
 // One leaf's climb when every internal node's slot range is known (`ranges`).  The calling
 // block starts climbs at the leaves of slots [base, base + kSpan).  A node whose whole range
 // lies in those slots has both children finished by this block, so its two arrivals meet in
 // the shared counter arrivals[gap - base] (gap: the last slot of its left child, unique per
 // internal node) behind block fences; only nodes spanning blocks take the device-scope
-// counter in flags[], which the finishing arrival resets.
+// counter in flags[], which the finishing arrival resets.  Links, parents and ranges do not
+// change during the pass, so the next level's are loaded while this level's arrival and box
+// wait: after an arrival only the children's boxes remain on the chain of dependent loads.
 template <int kSpan>
 __device__ __forceinline__ void climb_ranged(Node* __restrict__ nodes, BNode* __restrict__ bnodes,
                                              const int* __restrict__ parent,
                                              int* __restrict__ flags, int n, int k, int base,
                                              int* arrivals, const int2* __restrict__ ranges) {
+    // plain loads: the pass rewrites the links' 16-byte word (with the same values)
+    auto links = [&](int v) { return *reinterpret_cast<const int2*>(&nodes[v].left); };
+    auto crange = [&](int v) { return v >= n - 1 ? make_int2(v - (n - 1), 1) : __ldg(ranges + v); };
     int c = n - 1 + k;
     int2 rc = make_int2(k, 1);
     int p = parent[c];
-    for (int guard = 0; p >= 0 && guard < 4096; ++guard) {
-        const int2 rp = ranges[p];
+    if (p < 0) return;
+    int2 rp = __ldg(ranges + p), lr = links(p);
+    int pn = parent[p];
+    for (int guard = 0; guard < 4096; ++guard) {
+        int2 rpn = make_int2(0, 0), lrn = make_int2(0, 0);
+        int pnn = -1;
+        if (pn >= 0) {
+            rpn = __ldg(ranges + pn);
+            lrn = links(pn);
+            pnn = parent[pn];
+        }
+        const int2 rl = crange(lr.x), rr = crange(lr.y);
         const bool local = rp.x >= base && rp.x + rp.y <= base + kSpan;
         int old;
         if (local) {
-            const int gap = nodes[p].left == c ? rc.x + rc.y - 1 : rc.x - 1;
+            const int gap = lr.x == c ? rc.x + rc.y - 1 : rc.x - 1;
             __threadfence_block();
             old = atomicAdd(&arrivals[gap - base], 1);
             __threadfence_block();
@@ -301,14 +316,18 @@ __device__ __forceinline__ void climb_ranged(Node* __restrict__ nodes, BNode* __
         }
         if (old == 0) return;
         if (local) {
-            finish_node_ranged<true>(nodes, bnodes, p, n, ranges);
+            finish_node_links<true>(nodes, bnodes, p, n, lr, rl, rr);
         } else {
-            finish_node_ranged<false>(nodes, bnodes, p, n, ranges);
+            finish_node_links<false>(nodes, bnodes, p, n, lr, rl, rr);
             flags[p] = 0;
         }
+        if (pn < 0) return;
         c = p;
         rc = rp;
-        p = parent[p];
+        p = pn;
+        rp = rpn;
+        lr = lrn;
+        pn = pnn;
     }
 }
 

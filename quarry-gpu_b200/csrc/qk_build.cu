@@ -155,15 +155,14 @@ __global__ __launch_bounds__(kSpan) void k_bottom_up_ranged(Node* __restrict__ n
     climb_ranged<kSpan>(nodes, bnodes, parent, flags, n, k, base, arrivals, ranges);
 }
 
-// One thread per leaf climbs toward the root (climb in qk_build.cuh).
+// Refit: one thread per leaf climbs toward the root (climb_refit in qk_build.cuh).
 __global__ __launch_bounds__(kBlock) void k_bottom_up(Node* __restrict__ nodes,
                                                      BNode* __restrict__ bnodes,
                                                      const int* __restrict__ parent,
-                                                     int* __restrict__ flags, int n,
-                                                     int2* __restrict__ ranges) {
+                                                     int* __restrict__ flags, int n) {
     const int k = blockIdx.x * kBlock + threadIdx.x;
     if (k >= n) return;
-    climb(nodes, bnodes, parent, flags, n, k, ranges);
+    climb_refit(nodes, bnodes, parent, flags, n, k);
 }
 
 // depth = length of the parent chain (lbvh.cu:419-431), bounded by the node count: the
@@ -274,15 +273,29 @@ __global__ __launch_bounds__(kBlock) void k_dirty_merge(const int* __restrict__ 
                                                        const int* __restrict__ skip) {
     const int i = blockIdx.x * kBlock + threadIdx.x;
     if (i >= count || skip[i]) return;
+    auto links = [&](int v) { return *reinterpret_cast<const int2*>(&nodes[v].left); };
     int p = parent[n - 1 + slot_of[ids[i]]];
-    int guard = 0;
-    while (p >= 0 && guard++ < 4096) {
+    if (p < 0) return;
+    int2 lr = links(p);
+    int pn = parent[p];
+    const int2 none = make_int2(0, 0);
+    for (int guard = 0; guard < 4096; ++guard) {
+        // the next level's parent and links (static) load while this arrival and box wait
+        int2 lrn = none;
+        int pnn = -1;
+        if (pn >= 0) {
+            lrn = links(pn);
+            pnn = parent[pn];
+        }
         const int old = arrive_add(&flags[p], 4);
         const int need = __popc(old & 3);
         if ((old >> 2) + 1 < need) return;
-        finish_node(nodes, bnodes, p, n, nullptr);
+        finish_node_links<false, false>(nodes, bnodes, p, n, lr, none, none);
         flags[p] = 0;
-        p = parent[p];
+        if (pn < 0) return;
+        p = pn;
+        lr = lrn;
+        pn = pnn;
     }
 }
 
@@ -531,7 +544,7 @@ int refit_impl(qk_tree* t, const void* items, cudaStream_t s) {
     stage_mark(kMarkScatter, s);
     k_bottom_up<<<blocks_for(n), kBlock, 0, s>>>(static_cast<Node*>(t->nodes),
                                                  static_cast<BNode*>(t->bnodes), t->parent,
-                                                 t->flags, n, nullptr);
+                                                 t->flags, n);
     stage_mark(kMarkBoxes, s);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_status(e, "refit");

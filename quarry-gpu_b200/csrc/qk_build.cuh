@@ -192,38 +192,6 @@ __device__ __forceinline__ int small_code(int c, int n, int2 range) {
     return (c < n - 1 && range.y >= 2 && range.y <= kLeafMax) ? ((range.x << 2) | (range.y - 1)) : 0;
 }
 
-__device__ __forceinline__ int2 child_range(const int2* ranges, int c, int n) {
-    return c >= n - 1 ? make_int2(c - (n - 1), 1) : __ldcg(ranges + c);
-}
-
-// Complete internal node p from its two (final) children: canonical box + traversal node.
-// With `ranges` (one int2 per internal node) the node's leaf-slot range (first, count; count
-// 0 when the slots are not contiguous) is recorded and the children's small-subtree codes
-// are written; without (refit) the codes are kept.
-__device__ __forceinline__ void finish_node(Node* __restrict__ nodes, BNode* __restrict__ bnodes,
-                                            int p, int n, int2* __restrict__ ranges) {
-    const int l = nodes[p].left, r = nodes[p].right;
-    if (ranges) {
-        const int2 rl = child_range(ranges, l, n), rr = child_range(ranges, r, n);
-        const int first = min(rl.x, rr.x);
-        int count = rl.y + rr.y;
-        if (rl.y <= 0 || rr.y <= 0 || max(rl.x + rl.y, rr.x + rr.y) - first != count) count = 0;
-        ranges[p] = make_int2(first, count);
-        *reinterpret_cast<float2*>(&bnodes[p].v3.z) =
-            make_float2(__int_as_float(small_code(l, n, rl)), __int_as_float(small_code(r, n, rr)));
-    }
-    const Box a = load_box_cg(nodes + l);
-    const Box b = load_box_cg(nodes + r);
-    Box u;
-    u.lo = f3(fmin_t(a.lo.x, b.lo.x), fmin_t(a.lo.y, b.lo.y), fmin_t(a.lo.z, b.lo.z));
-    u.hi = f3(fmax_t(a.hi.x, b.hi.x), fmax_t(a.hi.y, b.hi.y), fmax_t(a.hi.z, b.hi.z));
-    write_box(nodes + p, u);
-    BNode& bn = bnodes[p];
-    bn.v0 = make_float4(a.lo.x, a.lo.y, a.lo.z, a.hi.x);
-    bn.v1 = make_float4(a.hi.y, a.hi.z, b.lo.x, b.lo.y);
-    bn.v2 = make_float4(b.lo.z, b.hi.x, b.hi.y, b.hi.z);
-}
-
 __device__ __forceinline__ Box load_box_ca(const Node* nd) {
     const float4* p = reinterpret_cast<const float4*>(nd);
     const float4 a = __ldca(p), b = __ldca(p + 1);
@@ -233,32 +201,19 @@ __device__ __forceinline__ Box load_box_ca(const Node* nd) {
     return bx;
 }
 
-// One leaf's climb toward the root; flags[p] counts arrivals at internal node p.  The
-// second arrival finishes p (both children final), resets the counter and continues.
-__device__ __forceinline__ void climb(Node* __restrict__ nodes, BNode* __restrict__ bnodes,
-                                      const int* __restrict__ parent, int* __restrict__ flags,
-                                      int n, int k, int2* __restrict__ ranges) {
-    int p = parent[n - 1 + k];
-    int guard = 0;
-    while (p >= 0 && guard++ < 4096) {
-        if (arrive_add(&flags[p], 1) == 0) return;
-        finish_node(nodes, bnodes, p, n, ranges);
-        flags[p] = 0;
-        p = parent[p];
-    }
-}
-
 // Complete internal node p from its final children given its links lr = (left, right) and the
 // children's slot ranges (all static during the pass): box and traversal node, with the
 // children's small-subtree codes.  kLocal: both children were finished by threads of this
 // block, whose writes a plain load sees after the block fence; otherwise they are read from L2.
-template <bool kLocal>
+// kCodes false (refits): the small-subtree codes, which depend on the topology only, are kept.
+template <bool kLocal, bool kCodes = true>
 __device__ __forceinline__ void finish_node_links(Node* __restrict__ nodes,
                                                   BNode* __restrict__ bnodes, int p, int n,
                                                   int2 lr, int2 rl, int2 rr) {
     const int l = lr.x, r = lr.y;
-    *reinterpret_cast<float2*>(&bnodes[p].v3.z) =
-        make_float2(__int_as_float(small_code(l, n, rl)), __int_as_float(small_code(r, n, rr)));
+    if (kCodes)
+        *reinterpret_cast<float2*>(&bnodes[p].v3.z) = make_float2(
+            __int_as_float(small_code(l, n, rl)), __int_as_float(small_code(r, n, rr)));
     const Box a = kLocal ? load_box_ca(nodes + l) : load_box_cg(nodes + l);
     const Box b = kLocal ? load_box_ca(nodes + r) : load_box_cg(nodes + r);
     Box u;
@@ -271,6 +226,36 @@ __device__ __forceinline__ void finish_node_links(Node* __restrict__ nodes,
     bn.v0 = make_float4(a.lo.x, a.lo.y, a.lo.z, a.hi.x);
     bn.v1 = make_float4(a.hi.y, a.hi.z, b.lo.x, b.lo.y);
     bn.v2 = make_float4(b.lo.z, b.hi.x, b.hi.y, b.hi.z);
+}
+
+// Refit: one leaf's climb toward the root of a tree whose topology is unchanged; flags[p]
+// counts arrivals at internal node p, the second arrival finishes p's box and traversal node
+// (its small-subtree codes kept), resets the counter and continues.  The next level's parent
+// and links (static) are loaded while this level's arrival and boxes wait.
+__device__ __forceinline__ void climb_refit(Node* __restrict__ nodes, BNode* __restrict__ bnodes,
+                                            const int* __restrict__ parent,
+                                            int* __restrict__ flags, int n, int k) {
+    auto links = [&](int v) { return *reinterpret_cast<const int2*>(&nodes[v].left); };
+    int p = parent[n - 1 + k];
+    if (p < 0) return;
+    int2 lr = links(p);
+    int pn = parent[p];
+    const int2 none = make_int2(0, 0);
+    for (int guard = 0; guard < 4096; ++guard) {
+        int2 lrn = none;
+        int pnn = -1;
+        if (pn >= 0) {
+            lrn = links(pn);
+            pnn = parent[pn];
+        }
+        if (arrive_add(&flags[p], 1) == 0) return;
+        finish_node_links<false, false>(nodes, bnodes, p, n, lr, none, none);
+        flags[p] = 0;
+        if (pn < 0) return;
+        p = pn;
+        lr = lrn;
+        pn = pnn;
+    }
 }
 
 // One leaf's climb when every internal node's slot range is known (`ranges`).  The calling

@@ -99,7 +99,8 @@ struct Level {
     int* left_count;    // per task
     int* chunk_left;    // per chunk: left primitives
     int* counters;      // [0] chunks, [1] next big tasks, [2] block tasks, [3] internal base,
-                        // [4] this level's big tasks (the previous level's [1])
+                        // [4] this level's big tasks (the previous level's [1]), [5] the warp
+                        // tier's next task
 };
 
 // single block: chunk list of the current tasks
@@ -1141,7 +1142,7 @@ __global__ __launch_bounds__(kBlock, 4) void k_warp_tasks(const Task* __restrict
                                                       const float4* __restrict__ phi, Node* nodes,
                                                       BNode* bn, int* parent, int n, int bins,
                                                       int* __restrict__ err, int large_ok,
-                                                      int small) {
+                                                      int small, int* __restrict__ fetch) {
     extern __shared__ unsigned wsm[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned* wb = wsm + static_cast<size_t>(warp) * 3 * bins * kBinWords;
@@ -1150,7 +1151,15 @@ __global__ __launch_bounds__(kBlock, 4) void k_warp_tasks(const Task* __restrict
     int* scratch = reinterpret_cast<int*>(wstk_all + (kBlock / 32) * kWarpStack) + warp * 32;
     const int w = (blockIdx.x * kBlock + threadIdx.x) >> 5;
     const int nw = (gridDim.x * kBlock) >> 5;
-    for (int ti = w; ti < ntask; ti += nw) {
+    // with `fetch` (a zeroed counter) each warp takes its next task from it, so warps that drew
+    // small ranges take more of them; without, warp w takes tasks w, w + nw, ...
+    for (int ti = w;; ti += nw) {
+        if (fetch) {
+            int next = 0;
+            if (lane == 0) next = atomicAdd(fetch, 1);
+            ti = __shfl_sync(0xffffffffu, next, 0);
+        }
+        if (ti >= ntask) break;
         const Task tk = tasks[ti];
         const int count = tk.end - tk.begin;
         if (tk.node < 0 || count < 2 || count > kTaskRange) {
@@ -1368,10 +1377,11 @@ int build_sah_impl(qk_tree* t, int bins, int small, const void* items_v, void* w
         }
         k_add_base<<<blocks_for(nblk), kBlock, 0, s>>>(w.id_base, nblk, w.L.counters);
         // every range of at most kTaskRange primitives: one warp each
-        k_warp_tasks<<<min(blocks_for(static_cast<long long>(nblk) * 32), 148 * 8), kBlock,
+        // a resident grid (4 blocks per SM) whose warps fetch tasks from counters[5]
+        k_warp_tasks<<<min(blocks_for(static_cast<long long>(nblk) * 32), 148 * 4), kBlock,
                        warp_tasks_smem(bins), s>>>(w.blocks, nblk, w.id_base, fin, scratch, w.cen,
                                                    w.plo, w.phi, nodes, bn, t->parent, n, bins, err,
-                                                   0, small);
+                                                   0, small, w.L.counters + 5);
     } else {
         int base = 0;
         cudaMemcpyAsync(&base, w.L.counters + 3, sizeof(int), cudaMemcpyDeviceToHost, s);
@@ -1414,7 +1424,7 @@ int sah_forest(const int4* tasks, int ntask, int max_count, const int* id_base, 
     k_warp_tasks<<<min(blocks_for(static_cast<long long>(ntask) * 32), 148 * 8), kBlock,
                    warp_tasks_smem(bins), s>>>(tk, ntask, id_base, order, tmp, cen, plo, phi, nodes,
                                                bn, t->parent, t->n, bins, err,
-                                               max_count > kTaskRange ? 1 : 0, 2);
+                                               max_count > kTaskRange ? 1 : 0, 2, nullptr);
     if (max_count > kTaskRange) {
         cudaFuncSetAttribute(k_block_build, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              static_cast<int>(block_smem(kMaxBins)));

@@ -103,16 +103,17 @@ struct Level {
                         // tier's next task
 };
 
-// single block: chunk list of the current tasks
-__global__ __launch_bounds__(1024) void k_level_prep(Level L, int bins) {
-    const int ntask = L.counters[4];
+// One block of 1024 threads: the chunk list of `ntask` tasks (kChunk primitives per chunk):
+// each task's first chunk, every chunk's task and first position, the chunk count.
+__device__ __forceinline__ void level_chunks(const Level& L, const Task* __restrict__ tasks,
+                                             int ntask) {
     __shared__ int carry;
     if (threadIdx.x == 0) carry = 0;
     __syncthreads();
     for (int base = 0; base < ntask; base += 1024) {
         const int t = base + threadIdx.x;
         int nch = 0;
-        if (t < ntask) nch = (L.tasks[t].end - L.tasks[t].begin + kChunk - 1) / kChunk;
+        if (t < ntask) nch = (tasks[t].end - tasks[t].begin + kChunk - 1) / kChunk;
         // block exclusive scan of nch (warp shuffles + shared totals)
         __shared__ int wsum[32];
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -137,7 +138,7 @@ __global__ __launch_bounds__(1024) void k_level_prep(Level L, int bins) {
             L.chunk_first[t] = excl;
             for (int c = 0; c < nch; ++c) {
                 L.chunk_task[excl + c] = t;
-                L.chunk_begin[excl + c] = L.tasks[t].begin + c * kChunk;
+                L.chunk_begin[excl + c] = tasks[t].begin + c * kChunk;
             }
         }
         __syncthreads();
@@ -145,6 +146,11 @@ __global__ __launch_bounds__(1024) void k_level_prep(Level L, int bins) {
         __syncthreads();
     }
     if (threadIdx.x == 0) L.counters[0] = carry;
+}
+
+// single block: chunk list of the first level's tasks (later levels' come from k_level_assign)
+__global__ __launch_bounds__(1024) void k_level_prep(Level L) {
+    level_chunks(L, L.tasks, L.counters[4]);
 }
 
 // one block per range: reset its centroid bounds and bins
@@ -613,6 +619,9 @@ __global__ __launch_bounds__(1024) void k_level_assign(Level L, Task* __restrict
         L.counters[2] = base_blk + carry[2];
         L.counters[4] = base_big + carry[1];
     }
+    // the next level's chunk list, from the tasks this block wrote above
+    __syncthreads();
+    level_chunks(L, next, base_big + carry[1]);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -1307,6 +1316,8 @@ int build_sah_impl(qk_tree* t, int bins, int small, const void* items_v, void* w
     StageClock* clk = stage_clock();
     const int per_sync = clk ? 1 : kLevelsPerSync;
     const int max_big = n / (kTaskRange + 1) + 1;
+    // the first level's chunk list; each level's k_level_assign writes the next one's
+    if (nbig > 0) k_level_prep<<<1, 1024, 0, s>>>(w.L);
     while (nbig > 0) {
         if (level >= kMaxDepth) return fail(QK_ERR_DEPTH, "SAH: too many levels");
         int bound = nbig;
@@ -1314,7 +1325,6 @@ int build_sah_impl(qk_tree* t, int bins, int small, const void* items_v, void* w
         cudaError_t e;
         for (int j = 0; j < batch; ++j, ++level) {
             w.L.tasks = cur;
-            k_level_prep<<<1, 1024, 0, s>>>(w.L, bins);
             k_level_reset<<<bound, kBlock, 0, s>>>(w.L, bins);
             // chunk kernels: grid sized by a bound on the chunk count (every task spans at most
             // size / kChunk + 1 chunks); blocks beyond the count k_level_prep wrote return at once
